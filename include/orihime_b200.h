@@ -1,0 +1,103 @@
+/*
+ * orihime_b200 — C ABI of the B200 (sm_100a) soft Smith–Waterman kernels.
+ *
+ * This is the drop-in boundary for the CUDA path of megure-labs/orihime's
+ * soft Smith–Waterman operators.  Each entry point replaces one CUDA op body
+ * of the reference (the C++ functions registered under
+ * TORCH_LIBRARY_IMPL(orihime, CUDA)) together with the extern "C" launchers it
+ * calls; references are to files of that project.
+ *
+ * Conventions
+ *   - All pointers are device pointers unless stated; float32 data, int32
+ *     lengths, row-major.
+ *   - scores / map use the reference's padded layout [B, L1max, L2max].
+ *     lengths is [B, 2] (rows, cols used by pair b) or NULL for full lengths;
+ *     0 <= lengths[b][k] <= L{1,2}max is the caller's responsibility (the
+ *     Python host checks it with the reference's error messages).
+ *   - Every call is asynchronous on `stream` (a cudaStream_t, NULL = legacy
+ *     default stream), allocates nothing and never synchronises, so it can be
+ *     captured in a CUDA graph.  Device scratch is passed as `workspace`,
+ *     at least *_workspace_bytes() bytes, 256-byte aligned; calls that share a
+ *     workspace must be ordered on one stream.
+ *   - Outputs: value [B] (soft alignment score S), map [B, L1max, L2max]
+ *     (dS/dscores; exactly 0 outside lengths), and per-pair dS/dparameter [B].
+ *   - Return value: SWB_OK or a negative SWB_ERR_* code (nothing launched).
+ *     A bounded cross-warp wait that expires inside a kernel is reported in the
+ *     workspace status word (swb_read_status), not by the return value.
+ */
+#ifndef ORIHIME_B200_H
+#define ORIHIME_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWB_ABI_VERSION 1
+
+#define SWB_OK 0
+#define SWB_ERR_ARG (-1)
+#define SWB_ERR_WORKSPACE (-2)
+#define SWB_ERR_CUDA (-3)
+
+/* Status bits written by kernels into the workspace status word. */
+#define SWB_STATUS_WAIT_TIMEOUT 1u
+
+/* Optional launch knobs (pass NULL for defaults). */
+typedef struct swb_options {
+    int max_ctas;                      /* cap on persistent CTAs (0 = occupancy-derived) */
+    unsigned long long spin_limit_ns;  /* bound on every cross-warp wait (0 = 20 s)      */
+    int fault_inject;                  /* 1: band>0 waits on a word nobody writes (tests) */
+} swb_options;
+
+/* Workspace bytes for swb_sw_affine_forward on a [B, L1max, L2max] batch. */
+size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max);
+
+/*
+ * Soft Smith–Waterman, affine gaps: value, marginal map and dS/d(gap_open,
+ * gap_ext, temp) in one call (forward wavefront + checkpointed adjoint).
+ * Replaces orihime_sw_affine_forward_cuda / soft_sw_affine_cuda_float
+ * (src/sw_affine/torch_cuda.cpp:820, :419 -> SoftSWAffineCUDAFunction::forward
+ * :128-206) and orihime_sw_affine_value_grad_params_cuda (:842 ->
+ * soft_sw_affine_cuda_with_grads :446), i.e. the launchers sw_affine_forward +
+ * sw_affine_backward (src/sw_affine/kernels_gpu.cuh:165, :193).
+ */
+int swb_sw_affine_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap_open, float gap_ext, float temp,
+                          float* value, float* map,
+                          float* grad_open, float* grad_ext, float* grad_temp,
+                          void* workspace, size_t workspace_bytes, void* stream,
+                          const swb_options* opt);
+
+/* Workspace bytes for swb_sw_forward on a [B, L1max, L2max] batch. */
+size_t swb_sw_workspace_bytes(int B, int L1max, int L2max);
+
+/*
+ * Soft Smith–Waterman, linear gap: value, marginal map, dS/dgap, dS/dT.
+ * Replaces orihime_sw_forward_cuda / soft_sw_cuda_float and
+ * orihime_sw_value_grad_params_cuda (src/sw/torch_cuda.cpp:364-450,
+ * :803-830 registration), i.e. the launchers sw_regular_forward +
+ * sw_regular_backward (src/sw/kernels_gpu.cuh:139, :165).
+ */
+int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                   float gap, float temp,
+                   float* value, float* map, float* grad_gap, float* grad_temp,
+                   void* workspace, size_t workspace_bytes, void* stream,
+                   const swb_options* opt);
+
+/* Copies the workspace status word to *status (synchronises `stream`).
+ * No reference counterpart: the reference synchronises inside every op. */
+int swb_read_status(const void* workspace, void* stream, unsigned* status);
+
+/* Human-readable text for a SWB_ERR_* code. */
+const char* swb_error_string(int code);
+
+/* SWB_ABI_VERSION of the loaded library. */
+int swb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORIHIME_B200_H */

@@ -1,0 +1,880 @@
+/*
+ * TEST INFRASTRUCTURE ONLY — never linked into the product.
+ *
+ * Body of the CPU oracle for soft Smith–Waterman (linear and affine gaps).
+ * sw_oracle.c includes this file twice: once with REAL=float (a restatement
+ * that follows the reference CPU kernels operation by operation, so it can be
+ * compared bit-for-bit with them) and once with REAL=double (the FP64 truth
+ * that errors are reported against).
+ *
+ * Every function states which reference routine it restates; paths are inside
+ * megure-labs/orihime.
+ *
+ * Semantics shared by all routines (src/common/numerics.h:29-127):
+ *   NEG_BIG = -1e30 stands for "no path"; an LSE whose max is <= NEG_BIG is
+ *   NEG_BIG; exp arguments below -88 give 0 and are clamped to 88 above;
+ *   sums of exponentials are Kahan-compensated.
+ * DP indices are 1-based: cell (i,j) uses score s[i-1][j-1]; row 0 / column 0
+ * are boundary cells (only M[0,0] = 0 is a live value).
+ */
+
+#ifndef REAL
+#error "define REAL before including sw_oracle_impl.h"
+#endif
+
+#define CAT2(a, b) a##b
+#define CAT(a, b) CAT2(a, b)
+#define FN(name) CAT(name, SFX)
+
+/* ---- scalar helpers ---------------------------------------------------- */
+
+static REAL FN(clip_exp)(REAL x) {
+    if (x < (REAL)-88.0) return (REAL)0;
+    if (x > (REAL)88.0) x = (REAL)88.0;
+    return EXPF(x);
+}
+
+typedef struct { REAL s, c; } FN(ksum_t);
+
+static void FN(kadd)(FN(ksum_t) *k, REAL v) {
+    REAL y = v - k->c;
+    REAL t = k->s + y;
+    k->c = (t - k->s) - y;
+    k->s = t;
+}
+
+static REAL FN(vmax)(const REAL *v, int n) {
+    REAL m = v[0];
+    for (int q = 1; q < n; ++q) if (v[q] > m) m = v[q];
+    return m;
+}
+
+/* T*log(sum exp(v/T)) over n terms (numerics.h:75-127). */
+static REAL FN(tlse)(const REAL *v, int n, REAL T) {
+    REAL m = FN(vmax)(v, n);
+    if (m <= (REAL)NEG_BIG) return (REAL)NEG_BIG;
+    FN(ksum_t) k = {0, 0};
+    for (int q = 0; q < n; ++q) FN(kadd)(&k, FN(clip_exp)((v[q] - m) / T));
+    return m + T * LOGF(k.s);
+}
+
+/* Normalised softmax weights, zero for NEG_BIG terms
+ * (src/sw_affine/kernels_cpu.cpp:56-88, src/sw/kernels_cpu.cpp:42-63). */
+static void FN(tsoftmax)(const REAL *v, int n, REAL T, REAL *w) {
+    REAL m = FN(vmax)(v, n);
+    if (m <= (REAL)NEG_BIG) { for (int q = 0; q < n; ++q) w[q] = 0; return; }
+    FN(ksum_t) k = {0, 0};
+    for (int q = 0; q < n; ++q) {
+        if (v[q] > (REAL)NEG_BIG) { w[q] = FN(clip_exp)((v[q] - m) / T); FN(kadd)(&k, w[q]); }
+        else w[q] = 0;
+    }
+    if (k.s > 0) for (int q = 0; q < n; ++q) w[q] /= k.s;
+}
+
+/* exp(min((a - S)/T, 0)), or 0 for a dead cell (kernels_cpu.cpp:43-52). */
+static REAL FN(end_weight)(REAL a, REAL S, REAL T) {
+    if (a <= (REAL)NEG_BIG) return 0;
+    REAL lp = (a - S) / T;
+    if (lp > 0) lp = 0;
+    return FN(clip_exp)(lp);
+}
+
+static int FN(live)(REAL b) { return !(isinf(b) || isnan(b) || b == 0); }
+
+/* ---- affine model ------------------------------------------------------ */
+
+/* Tables of one pair: plane 0 = M, 1 = I, 2 = D, each (L1+1) x (L2+1). */
+typedef struct {
+    int L1, L2, ld;          /* ld = row pitch of the score slab */
+    const REAL *s;
+    REAL go, ge, T;
+    size_t plane, cols;
+    REAL *a;                 /* 3 planes */
+} FN(aff_t);
+
+#define AIX(c, st, i, j) ((size_t)(st) * (c)->plane + (size_t)(i) * (c)->cols + (size_t)(j))
+#define SC(c, i, j) ((c)->s[(size_t)((i) - 1) * (c)->ld + (size_t)((j) - 1)])
+
+/* The three candidate vectors of cell (i,j): M (diag M,I,D + s, sky s),
+ * I (up M + go, up I + ge), D (left M + go, left D + ge). */
+static void FN(aff_cands)(const FN(aff_t) *c, const REAL *tab, int i, int j,
+                          REAL vm[4], REAL vi[2], REAL vd[2]) {
+    REAL s = SC(c, i, j);
+    int dg = (i > 1 && j > 1);
+    vm[0] = dg ? tab[AIX(c, 0, i - 1, j - 1)] + s : (REAL)NEG_BIG;
+    vm[1] = dg ? tab[AIX(c, 1, i - 1, j - 1)] + s : (REAL)NEG_BIG;
+    vm[2] = dg ? tab[AIX(c, 2, i - 1, j - 1)] + s : (REAL)NEG_BIG;
+    vm[3] = s;
+    vi[0] = (i > 1) ? tab[AIX(c, 0, i - 1, j)] + c->go : (REAL)NEG_BIG;
+    vi[1] = (i > 1) ? tab[AIX(c, 1, i - 1, j)] + c->ge : (REAL)NEG_BIG;
+    vd[0] = (j > 1) ? tab[AIX(c, 0, i, j - 1)] + c->go : (REAL)NEG_BIG;
+    vd[1] = (j > 1) ? tab[AIX(c, 2, i, j - 1)] + c->ge : (REAL)NEG_BIG;
+}
+
+/* Forward tables and log-partition (src/sw_affine/kernels_cpu.cpp:94-195).
+ * Cells are visited row-major; every cell reads only cells with smaller
+ * i+j, so the values equal the reference's anti-diagonal order bit for bit. */
+static REAL FN(aff_forward)(FN(aff_t) *c) {
+    size_t n = 3 * c->plane;
+    for (size_t q = 0; q < n; ++q) c->a[q] = (REAL)NEG_BIG;
+    c->a[0] = 0;
+    REAL vm[4], vi[2], vd[2];
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            FN(aff_cands)(c, c->a, i, j, vm, vi, vd);
+            c->a[AIX(c, 0, i, j)] = FN(tlse)(vm, 4, c->T);
+            c->a[AIX(c, 1, i, j)] = FN(tlse)(vi, 2, c->T);
+            c->a[AIX(c, 2, i, j)] = FN(tlse)(vd, 2, c->T);
+        }
+    REAL m = (REAL)NEG_BIG;
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j)
+            for (int st = 0; st < 3; ++st) {
+                REAL v = c->a[AIX(c, st, i, j)];
+                if (v > m) m = v;
+            }
+    FN(ksum_t) k = {0, 0};
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j)
+            for (int st = 0; st < 3; ++st) {
+                REAL v = c->a[AIX(c, st, i, j)];
+                if (v > (REAL)NEG_BIG) FN(kadd)(&k, FN(clip_exp)((v - m) / c->T));
+            }
+    return m + c->T * LOGF(k.s);
+}
+
+/* Adjoint pass (src/sw_affine/kernels_cpu.cpp:201-356): beta starts at the
+ * clamped end weight of every state, then flows to predecessors in reverse
+ * anti-diagonal order (i ascending within a diagonal; per cell M, then I,
+ * then D).  post is the pair's padded [L1max x ld] slab, zeroed here.
+ * g[0]=dS/dgo, g[1]=dS/dge, g[2]=dS/dT. */
+static void FN(aff_adjoint)(const FN(aff_t) *c, REAL S, REAL *be, REAL *post,
+                            int L1max, REAL g[3]) {
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < nsc; ++q) post[q] = 0;
+    size_t n = 3 * c->plane;
+    for (size_t q = 0; q < n; ++q) be[q] = 0;
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j)
+            for (int st = 0; st < 3; ++st) {
+                REAL lp = (c->a[AIX(c, st, i, j)] - S) / c->T;
+                if (lp > 0) lp = 0;
+                be[AIX(c, st, i, j)] = FN(clip_exp)(lp);
+            }
+    REAL gopen = 0, gext = 0;
+    REAL vm[4], vi[2], vd[2], wm[4], wi[2], wd[2];
+    for (int k = c->L1 + c->L2; k >= 2; --k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            FN(aff_cands)(c, c->a, i, j, vm, vi, vd);
+            REAL bm = be[AIX(c, 0, i, j)];
+            if (FN(live)(bm)) {
+                FN(tsoftmax)(vm, 4, c->T, wm);
+                post[(size_t)(i - 1) * c->ld + (j - 1)] += bm * (wm[0] + wm[1] + wm[2] + wm[3]);
+                if (i > 1 && j > 1)
+                    for (int st = 0; st < 3; ++st)
+                        if (wm[st] > 0) be[AIX(c, st, i - 1, j - 1)] += bm * wm[st];
+            }
+            REAL bi = be[AIX(c, 1, i, j)];
+            if (FN(live)(bi)) {
+                FN(tsoftmax)(vi, 2, c->T, wi);
+                if (i > 1) {
+                    if (wi[0] > 0) { be[AIX(c, 0, i - 1, j)] += bi * wi[0]; gopen += bi * wi[0]; }
+                    if (wi[1] > 0) { be[AIX(c, 1, i - 1, j)] += bi * wi[1]; gext += bi * wi[1]; }
+                }
+            }
+            REAL bd = be[AIX(c, 2, i, j)];
+            if (FN(live)(bd)) {
+                FN(tsoftmax)(vd, 2, c->T, wd);
+                if (j > 1) {
+                    if (wd[0] > 0) { be[AIX(c, 0, i, j - 1)] += bd * wd[0]; gopen += bd * wd[0]; }
+                    if (wd[1] > 0) { be[AIX(c, 2, i, j - 1)] += bd * wd[1]; gext += bd * wd[1]; }
+                }
+            }
+        }
+    }
+    /* Expected match score over the whole padded slab, as the reference does. */
+    FN(ksum_t) ms = {0, 0};
+    for (int r = 0; r < L1max; ++r)
+        for (int q = 0; q < c->ld; ++q) {
+            size_t o = (size_t)r * c->ld + q;
+            FN(kadd)(&ms, post[o] * c->s[o]);
+        }
+    REAL gap_cost = gopen * c->go + gext * c->ge;
+    REAL total = ms.s + gap_cost;
+    g[0] = gopen;
+    g[1] = gext;
+    g[2] = (S - total) / c->T;
+}
+
+/* Hessian-vector product d(post)/d(scores) . V
+ * (src/sw_affine/kernels_cpu.cpp:362-631): tangent forward of alpha along V,
+ * tangent of the partition, then beta and its tangent pushed backwards. */
+static void FN(aff_hvp)(const FN(aff_t) *c, REAL S, const REAL *V, REAL *da,
+                        REAL *be, REAL *dbe, REAL *H, int L1max) {
+    size_t n = 3 * c->plane;
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < n; ++q) { da[q] = 0; dbe[q] = 0; be[q] = 0; }
+    for (size_t q = 0; q < nsc; ++q) H[q] = 0;
+    REAL vm[4], vi[2], vd[2], wm[4], wi[2], wd[2];
+#define VV(i, j) V[(size_t)((i) - 1) * c->ld + (size_t)((j) - 1)]
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            REAL v = VV(i, j);
+            int dg = (i > 1 && j > 1);
+            FN(aff_cands)(c, c->a, i, j, vm, vi, vd);
+            FN(tsoftmax)(vm, 4, c->T, wm);
+            REAL t0 = dg ? da[AIX(c, 0, i - 1, j - 1)] + v : 0;
+            REAL t1 = dg ? da[AIX(c, 1, i - 1, j - 1)] + v : 0;
+            REAL t2 = dg ? da[AIX(c, 2, i - 1, j - 1)] + v : 0;
+            da[AIX(c, 0, i, j)] = wm[0] * t0 + wm[1] * t1 + wm[2] * t2 + wm[3] * v;
+            FN(tsoftmax)(vi, 2, c->T, wi);
+            REAL u0 = (i > 1) ? da[AIX(c, 0, i - 1, j)] : 0;
+            REAL u1 = (i > 1) ? da[AIX(c, 1, i - 1, j)] : 0;
+            da[AIX(c, 1, i, j)] = wi[0] * u0 + wi[1] * u1;
+            FN(tsoftmax)(vd, 2, c->T, wd);
+            REAL l0 = (j > 1) ? da[AIX(c, 0, i, j - 1)] : 0;
+            REAL l2 = (j > 1) ? da[AIX(c, 2, i, j - 1)] : 0;
+            da[AIX(c, 2, i, j)] = wd[0] * l0 + wd[1] * l2;
+        }
+    }
+    FN(ksum_t) dk = {0, 0};
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j)
+            for (int st = 0; st < 3; ++st) {
+                REAL lp = (c->a[AIX(c, st, i, j)] - S) / c->T;
+                if (lp > 0) lp = 0;
+                FN(kadd)(&dk, FN(clip_exp)(lp) * da[AIX(c, st, i, j)]);
+            }
+    REAL dS = dk.s;
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j)
+            for (int st = 0; st < 3; ++st) {
+                size_t o = AIX(c, st, i, j);
+                REAL lp = (c->a[o] - S) / c->T;
+                if (lp > 0) lp = 0;
+                be[o] = FN(clip_exp)(lp);
+            }
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j)
+            for (int st = 0; st < 3; ++st) {
+                size_t o = AIX(c, st, i, j);
+                dbe[o] = be[o] * (da[o] - dS) / c->T;
+            }
+    for (int k = c->L1 + c->L2; k >= 2; --k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            REAL v = VV(i, j);
+            int dg = (i > 1 && j > 1);
+            FN(aff_cands)(c, c->a, i, j, vm, vi, vd);
+            /* M */
+            REAL bm = be[AIX(c, 0, i, j)], dbm = dbe[AIX(c, 0, i, j)];
+            FN(tsoftmax)(vm, 4, c->T, wm);
+            REAL tm[4];
+            tm[0] = dg ? da[AIX(c, 0, i - 1, j - 1)] + v : 0;
+            tm[1] = dg ? da[AIX(c, 1, i - 1, j - 1)] + v : 0;
+            tm[2] = dg ? da[AIX(c, 2, i - 1, j - 1)] + v : 0;
+            tm[3] = v;
+            REAL swm = wm[0] * tm[0] + wm[1] * tm[1] + wm[2] * tm[2] + wm[3] * tm[3];
+            REAL dwm[4];
+            for (int q = 0; q < 4; ++q) dwm[q] = wm[q] * (tm[q] - swm) / c->T;
+            H[(size_t)(i - 1) * c->ld + (j - 1)] += dbm * (wm[0] + wm[1] + wm[2] + wm[3]) +
+                                                   bm * (dwm[0] + dwm[1] + dwm[2] + dwm[3]);
+            if (dg) {
+                for (int st = 0; st < 3; ++st) be[AIX(c, st, i - 1, j - 1)] += bm * wm[st];
+                for (int st = 0; st < 3; ++st)
+                    dbe[AIX(c, st, i - 1, j - 1)] += dbm * wm[st] + bm * dwm[st];
+            }
+            /* I */
+            REAL bi = be[AIX(c, 1, i, j)], dbi = dbe[AIX(c, 1, i, j)];
+            FN(tsoftmax)(vi, 2, c->T, wi);
+            REAL ui[2];
+            ui[0] = (i > 1) ? da[AIX(c, 0, i - 1, j)] : 0;
+            ui[1] = (i > 1) ? da[AIX(c, 1, i - 1, j)] : 0;
+            REAL swi = wi[0] * ui[0] + wi[1] * ui[1];
+            REAL dwi0 = wi[0] * (ui[0] - swi) / c->T, dwi1 = wi[1] * (ui[1] - swi) / c->T;
+            if (i > 1) {
+                be[AIX(c, 0, i - 1, j)] += bi * wi[0];
+                be[AIX(c, 1, i - 1, j)] += bi * wi[1];
+                dbe[AIX(c, 0, i - 1, j)] += dbi * wi[0] + bi * dwi0;
+                dbe[AIX(c, 1, i - 1, j)] += dbi * wi[1] + bi * dwi1;
+            }
+            /* D */
+            REAL bd = be[AIX(c, 2, i, j)], dbd = dbe[AIX(c, 2, i, j)];
+            FN(tsoftmax)(vd, 2, c->T, wd);
+            REAL ud[2];
+            ud[0] = (j > 1) ? da[AIX(c, 0, i, j - 1)] : 0;
+            ud[1] = (j > 1) ? da[AIX(c, 2, i, j - 1)] : 0;
+            REAL swd = wd[0] * ud[0] + wd[1] * ud[1];
+            REAL dwd0 = wd[0] * (ud[0] - swd) / c->T, dwd1 = wd[1] * (ud[1] - swd) / c->T;
+            if (j > 1) {
+                be[AIX(c, 0, i, j - 1)] += bd * wd[0];
+                be[AIX(c, 2, i, j - 1)] += bd * wd[1];
+                dbe[AIX(c, 0, i, j - 1)] += dbd * wd[0] + bd * dwd0;
+                dbe[AIX(c, 2, i, j - 1)] += dbd * wd[1] + bd * dwd1;
+            }
+        }
+    }
+#undef VV
+}
+
+/* d(post)/d(theta), theta in {gap_open, gap_ext, T}
+ * (src/sw_affine/kernels_cpu.cpp:637-921): U = d(alpha)/d(theta) forward,
+ * then beta and W = d(beta)/d(theta) backward; dP/dtheta += W_M. */
+static void FN(aff_param)(const FN(aff_t) *c, REAL S, REAL dSdt, int pt, REAL *u,
+                          REAL *be, REAL *w, REAL *dP, int L1max) {
+    size_t n = 3 * c->plane;
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < n; ++q) { u[q] = 0; be[q] = 0; w[q] = 0; }
+    for (size_t q = 0; q < nsc; ++q) dP[q] = 0;
+    const REAL T = c->T;
+    REAL vm[4], vi[2], vd[2], wm[4], wi[2], wd[2];
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            int dg = (i > 1 && j > 1);
+            FN(aff_cands)(c, c->a, i, j, vm, vi, vd);
+            FN(tsoftmax)(vm, 4, T, wm);
+            REAL a0 = dg ? u[AIX(c, 0, i - 1, j - 1)] : 0;
+            REAL a1 = dg ? u[AIX(c, 1, i - 1, j - 1)] : 0;
+            REAL a2 = dg ? u[AIX(c, 2, i - 1, j - 1)] : 0;
+            REAL um = wm[0] * a0 + wm[1] * a1 + wm[2] * a2;
+            if (pt == 2) {
+                REAL e = wm[0] * vm[0] + wm[1] * vm[1] + wm[2] * vm[2] + wm[3] * vm[3];
+                um += (c->a[AIX(c, 0, i, j)] - e) / T;
+            }
+            u[AIX(c, 0, i, j)] = um;
+            FN(tsoftmax)(vi, 2, T, wi);
+            REAL b0 = (i > 1) ? u[AIX(c, 0, i - 1, j)] : 0;
+            REAL b1 = (i > 1) ? u[AIX(c, 1, i - 1, j)] : 0;
+            if (pt == 0) b0 += 1;
+            if (pt == 1) b1 += 1;
+            REAL ui = wi[0] * b0 + wi[1] * b1;
+            if (pt == 2) {
+                REAL e = wi[0] * vi[0] + wi[1] * vi[1];
+                ui += (c->a[AIX(c, 1, i, j)] - e) / T;
+            }
+            u[AIX(c, 1, i, j)] = ui;
+            FN(tsoftmax)(vd, 2, T, wd);
+            REAL c0 = (j > 1) ? u[AIX(c, 0, i, j - 1)] : 0;
+            REAL c2 = (j > 1) ? u[AIX(c, 2, i, j - 1)] : 0;
+            if (pt == 0) c0 += 1;
+            if (pt == 1) c2 += 1;
+            REAL ud = wd[0] * c0 + wd[1] * c2;
+            if (pt == 2) {
+                REAL e = wd[0] * vd[0] + wd[1] * vd[1];
+                ud += (c->a[AIX(c, 2, i, j)] - e) / T;
+            }
+            u[AIX(c, 2, i, j)] = ud;
+        }
+    }
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j)
+            for (int st = 0; st < 3; ++st)
+                be[AIX(c, st, i, j)] = FN(end_weight)(c->a[AIX(c, st, i, j)], S, T);
+    for (int k = c->L1 + c->L2; k >= 2; --k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            int dg = (i > 1 && j > 1);
+            size_t om = AIX(c, 0, i, j), oi = AIX(c, 1, i, j), od = AIX(c, 2, i, j);
+            FN(aff_cands)(c, c->a, i, j, vm, vi, vd);
+            /* M */
+            REAL bm = be[om];
+            REAL bim = FN(end_weight)(c->a[om], S, T);
+            REAL Wm = w[om] + bim * (u[om] - dSdt) / T;
+            if (pt == 2 && c->a[om] > (REAL)NEG_BIG) Wm -= bim * (c->a[om] - S) / (T * T);
+            FN(tsoftmax)(vm, 4, T, wm);
+            REAL du[4];
+            du[0] = dg ? u[AIX(c, 0, i - 1, j - 1)] : 0;
+            du[1] = dg ? u[AIX(c, 1, i - 1, j - 1)] : 0;
+            du[2] = dg ? u[AIX(c, 2, i - 1, j - 1)] : 0;
+            du[3] = 0;
+            REAL sw = wm[0] * du[0] + wm[1] * du[1] + wm[2] * du[2] + wm[3] * du[3];
+            REAL dw[4];
+            for (int q = 0; q < 4; ++q) dw[q] = wm[q] * (du[q] - sw) / T;
+            if (pt == 2) {
+                REAL e = wm[0] * vm[0] + wm[1] * vm[1] + wm[2] * vm[2] + wm[3] * vm[3];
+                REAL it2 = (REAL)1 / (T * T);
+                for (int q = 0; q < 4; ++q) dw[q] += wm[q] * (e - vm[q]) * it2;
+            }
+            dP[(size_t)(i - 1) * c->ld + (j - 1)] += Wm;
+            if (dg) {
+                for (int st = 0; st < 3; ++st) be[AIX(c, st, i - 1, j - 1)] += bm * wm[st];
+                for (int st = 0; st < 3; ++st)
+                    w[AIX(c, st, i - 1, j - 1)] += Wm * wm[st] + bm * dw[st];
+            }
+            /* I */
+            REAL bi = be[oi];
+            REAL bii = FN(end_weight)(c->a[oi], S, T);
+            REAL Wi = w[oi] + bii * (u[oi] - dSdt) / T;
+            if (pt == 2 && c->a[oi] > (REAL)NEG_BIG) Wi -= bii * (c->a[oi] - S) / (T * T);
+            if (i > 1) {
+                FN(tsoftmax)(vi, 2, T, wi);
+                REAL e0 = u[AIX(c, 0, i - 1, j)], e1 = u[AIX(c, 1, i - 1, j)];
+                if (pt == 0) e0 += 1;
+                if (pt == 1) e1 += 1;
+                REAL sI = wi[0] * e0 + wi[1] * e1;
+                REAL d0 = wi[0] * (e0 - sI) / T, d1 = wi[1] * (e1 - sI) / T;
+                if (pt == 2) {
+                    REAL e = wi[0] * vi[0] + wi[1] * vi[1];
+                    REAL it2 = (REAL)1 / (T * T);
+                    d0 += wi[0] * (e - vi[0]) * it2;
+                    d1 += wi[1] * (e - vi[1]) * it2;
+                }
+                be[AIX(c, 0, i - 1, j)] += bi * wi[0];
+                be[AIX(c, 1, i - 1, j)] += bi * wi[1];
+                w[AIX(c, 0, i - 1, j)] += Wi * wi[0] + bi * d0;
+                w[AIX(c, 1, i - 1, j)] += Wi * wi[1] + bi * d1;
+            }
+            /* D */
+            REAL bd = be[od];
+            REAL bid = FN(end_weight)(c->a[od], S, T);
+            REAL Wd = w[od] + bid * (u[od] - dSdt) / T;
+            if (pt == 2 && c->a[od] > (REAL)NEG_BIG) Wd -= bid * (c->a[od] - S) / (T * T);
+            if (j > 1) {
+                FN(tsoftmax)(vd, 2, T, wd);
+                REAL e0 = u[AIX(c, 0, i, j - 1)], e2 = u[AIX(c, 2, i, j - 1)];
+                if (pt == 0) e0 += 1;
+                if (pt == 1) e2 += 1;
+                REAL sD = wd[0] * e0 + wd[1] * e2;
+                REAL d0 = wd[0] * (e0 - sD) / T, d2 = wd[1] * (e2 - sD) / T;
+                if (pt == 2) {
+                    REAL e = wd[0] * vd[0] + wd[1] * vd[1];
+                    REAL it2 = (REAL)1 / (T * T);
+                    d0 += wd[0] * (e - vd[0]) * it2;
+                    d2 += wd[1] * (e - vd[1]) * it2;
+                }
+                be[AIX(c, 0, i, j - 1)] += bd * wd[0];
+                be[AIX(c, 2, i, j - 1)] += bd * wd[1];
+                w[AIX(c, 0, i, j - 1)] += Wd * wd[0] + bd * d0;
+                w[AIX(c, 2, i, j - 1)] += Wd * wd[1] + bd * d2;
+            }
+        }
+    }
+}
+
+/* ---- linear model ------------------------------------------------------ */
+
+#define LIX(c, i, j) ((size_t)(i) * (c)->cols + (size_t)(j))
+
+typedef struct {
+    int L1, L2, ld;
+    const REAL *s;
+    REAL g, T;
+    size_t cols;
+    REAL *a;
+} FN(lin_t);
+
+/* align, up, left, sky candidates of cell (i,j) (src/sw/kernels_cpu.cpp:112-121). */
+static void FN(lin_cands)(const FN(lin_t) *c, const REAL *tab, int i, int j, REAL v[4]) {
+    REAL s = SC(c, i, j);
+    v[0] = (i > 1 && j > 1) ? tab[LIX(c, i - 1, j - 1)] + s : (REAL)NEG_BIG;
+    v[1] = (i > 1) ? tab[LIX(c, i - 1, j)] + c->g : (REAL)NEG_BIG;
+    v[2] = (j > 1) ? tab[LIX(c, i, j - 1)] + c->g : (REAL)NEG_BIG;
+    v[3] = s;
+}
+
+/* src/sw/kernels_cpu.cpp:70-148 */
+static REAL FN(lin_forward)(FN(lin_t) *c) {
+    size_t n = (size_t)(c->L1 + 1) * c->cols;
+    for (size_t q = 0; q < n; ++q) c->a[q] = (REAL)NEG_BIG;
+    c->a[0] = 0;
+    REAL v[4];
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            FN(lin_cands)(c, c->a, i, j, v);
+            c->a[LIX(c, i, j)] = FN(tlse)(v, 4, c->T);
+        }
+    REAL m = (REAL)NEG_BIG;
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j)
+            if (c->a[LIX(c, i, j)] > m) m = c->a[LIX(c, i, j)];
+    FN(ksum_t) k = {0, 0};
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j) {
+            REAL x = c->a[LIX(c, i, j)];
+            if (x > (REAL)NEG_BIG) FN(kadd)(&k, FN(clip_exp)((x - m) / c->T));
+        }
+    return m + c->T * LOGF(k.s);
+}
+
+/* src/sw/kernels_cpu.cpp:154-271; g[0]=dS/dgap, g[1]=dS/dT. */
+static void FN(lin_adjoint)(const FN(lin_t) *c, REAL S, REAL *be, REAL *post, int L1max,
+                            REAL g[2]) {
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < nsc; ++q) post[q] = 0;
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j) {
+            REAL lp = (c->a[LIX(c, i, j)] - S) / c->T;
+            if (lp > 0) lp = 0;
+            be[LIX(c, i, j)] = FN(clip_exp)(lp);
+        }
+    REAL ggap = 0;
+    REAL v[4], w[4];
+    for (int k = c->L1 + c->L2; k >= 2; --k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            REAL b = be[LIX(c, i, j)];
+            if (!FN(live)(b)) continue;
+            FN(lin_cands)(c, c->a, i, j, v);
+            FN(tsoftmax)(v, 4, c->T, w);
+            post[(size_t)(i - 1) * c->ld + (j - 1)] += b * (w[0] + w[3]);
+            if (i > 1 && j > 1 && w[0] > 0) be[LIX(c, i - 1, j - 1)] += b * w[0];
+            if (i > 1 && w[1] > 0) { be[LIX(c, i - 1, j)] += b * w[1]; ggap += b * w[1]; }
+            if (j > 1 && w[2] > 0) { be[LIX(c, i, j - 1)] += b * w[2]; ggap += b * w[2]; }
+        }
+    }
+    FN(ksum_t) ms = {0, 0};
+    for (size_t q = 0; q < nsc; ++q) FN(kadd)(&ms, post[q] * c->s[q]);
+    REAL total = ms.s + ggap * c->g;
+    g[0] = ggap;
+    g[1] = (S - total) / c->T;
+}
+
+/* Softmax of the four linear candidates with a plain (uncompensated) sum and
+ * a 1e-20 guard, as the linear parameter-Jacobian uses
+ * (src/sw/kernels_cpu.cpp:547-560).  Returns 0 when every candidate is dead. */
+static int FN(lin_plain_softmax)(const REAL v[4], REAL T, REAL w[4]) {
+    REAL m = FN(vmax)(v, 4);
+    if (m <= (REAL)NEG_BIG) return 0;
+    for (int q = 0; q < 4; ++q) w[q] = FN(clip_exp)((v[q] - m) / T);
+    REAL sum = w[0] + w[1] + w[2] + w[3];
+    REAL inv = (sum > (REAL)1e-20) ? (REAL)1 / sum : (REAL)0;
+    for (int q = 0; q < 4; ++q) w[q] *= inv;
+    return 1;
+}
+
+/* src/sw/kernels_cpu.cpp:279-485 (HVP of the linear model). */
+static void FN(lin_hvp)(const FN(lin_t) *c, REAL S, const REAL *V, REAL *da, REAL *be,
+                        REAL *dbe, REAL *H, int L1max) {
+    size_t n = (size_t)(c->L1 + 1) * c->cols;
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < n; ++q) { da[q] = 0; be[q] = 0; dbe[q] = 0; }
+    for (size_t q = 0; q < nsc; ++q) H[q] = 0;
+    REAL v[4], w[4];
+#define VV(i, j) V[(size_t)((i) - 1) * c->ld + (size_t)((j) - 1)]
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            REAL vv = VV(i, j);
+            FN(lin_cands)(c, c->a, i, j, v);
+            FN(tsoftmax)(v, 4, c->T, w);
+            REAL t0 = (i > 1 && j > 1) ? da[LIX(c, i - 1, j - 1)] + vv : 0;
+            REAL t1 = (i > 1) ? da[LIX(c, i - 1, j)] : 0;
+            REAL t2 = (j > 1) ? da[LIX(c, i, j - 1)] : 0;
+            da[LIX(c, i, j)] = w[0] * t0 + w[1] * t1 + w[2] * t2 + w[3] * vv;
+        }
+    }
+    FN(ksum_t) dk = {0, 0};
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j) {
+            REAL lp = (c->a[LIX(c, i, j)] - S) / c->T;
+            if (lp > 0) lp = 0;
+            FN(kadd)(&dk, FN(clip_exp)(lp) * da[LIX(c, i, j)]);
+        }
+    REAL dS = dk.s;
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j) {
+            size_t o = LIX(c, i, j);
+            REAL lp = (c->a[o] - S) / c->T;
+            if (lp > 0) lp = 0;
+            be[o] = FN(clip_exp)(lp);
+        }
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j) {
+            size_t o = LIX(c, i, j);
+            dbe[o] = be[o] * (da[o] - dS) / c->T;
+        }
+    for (int k = c->L1 + c->L2; k >= 2; --k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            REAL vv = VV(i, j);
+            size_t o = LIX(c, i, j);
+            REAL b = be[o], db = dbe[o];
+            if (!FN(live)(b)) continue;
+            FN(lin_cands)(c, c->a, i, j, v);
+            FN(tsoftmax)(v, 4, c->T, w);
+            REAL t[4];
+            t[0] = (i > 1 && j > 1) ? da[LIX(c, i - 1, j - 1)] + vv : 0;
+            t[1] = (i > 1) ? da[LIX(c, i - 1, j)] : 0;
+            t[2] = (j > 1) ? da[LIX(c, i, j - 1)] : 0;
+            t[3] = vv;
+            REAL sw = w[0] * t[0] + w[1] * t[1] + w[2] * t[2] + w[3] * t[3];
+            REAL dw[4];
+            for (int q = 0; q < 4; ++q) dw[q] = w[q] * (t[q] - sw) / c->T;
+            H[(size_t)(i - 1) * c->ld + (j - 1)] += db * (w[0] + w[3]) + b * (dw[0] + dw[3]);
+            if (i > 1 && j > 1 && w[0] > 0) be[LIX(c, i - 1, j - 1)] += b * w[0];
+            if (i > 1 && w[1] > 0) be[LIX(c, i - 1, j)] += b * w[1];
+            if (j > 1 && w[2] > 0) be[LIX(c, i, j - 1)] += b * w[2];
+            if (i > 1 && j > 1 && w[0] > 0) dbe[LIX(c, i - 1, j - 1)] += db * w[0] + b * dw[0];
+            if (i > 1 && w[1] > 0) dbe[LIX(c, i - 1, j)] += db * w[1] + b * dw[1];
+            if (j > 1 && w[2] > 0) dbe[LIX(c, i, j - 1)] += db * w[2] + b * dw[2];
+        }
+    }
+#undef VV
+}
+
+/* src/sw/kernels_cpu.cpp:491-710 (dP/dtheta, theta in {gap, T}). */
+static void FN(lin_param)(const FN(lin_t) *c, REAL S, REAL dSdt, int pt, REAL *u, REAL *be,
+                          REAL *wt, REAL *dP, int L1max) {
+    size_t n = (size_t)(c->L1 + 1) * c->cols;
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < n; ++q) { u[q] = 0; be[q] = 0; wt[q] = 0; }
+    for (size_t q = 0; q < nsc; ++q) dP[q] = 0;
+    const REAL T = c->T;
+    REAL v[4], w[4];
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            FN(lin_cands)(c, c->a, i, j, v);
+            if (!FN(lin_plain_softmax)(v, T, w)) { u[LIX(c, i, j)] = 0; continue; }
+            REAL a0 = (i > 1 && j > 1) ? u[LIX(c, i - 1, j - 1)] : 0;
+            REAL a1 = (i > 1) ? u[LIX(c, i - 1, j)] : 0;
+            REAL a2 = (j > 1) ? u[LIX(c, i, j - 1)] : 0;
+            if (pt == 0) { a1 += 1; a2 += 1; }
+            REAL du = w[0] * a0 + w[1] * a1 + w[2] * a2 + w[3] * 0;
+            if (pt == 1) {
+                REAL e = w[0] * v[0] + w[1] * v[1] + w[2] * v[2] + w[3] * v[3];
+                du += (c->a[LIX(c, i, j)] - e) / T;
+            }
+            u[LIX(c, i, j)] = du;
+        }
+    }
+    for (int i = 0; i <= c->L1; ++i)
+        for (int j = 0; j <= c->L2; ++j) {
+            REAL lp = (c->a[LIX(c, i, j)] - S) / T;
+            if (lp > 0) lp = 0;
+            be[LIX(c, i, j)] = FN(clip_exp)(lp);
+        }
+    for (int k = c->L1 + c->L2; k >= 2; --k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            if (j < 1 || j > c->L2) continue;
+            size_t o = LIX(c, i, j);
+            REAL b = be[o];
+            REAL b0 = 0;
+            if (c->a[o] > (REAL)NEG_BIG) {
+                REAL lp = (c->a[o] - S) / T;
+                if (lp > 0) lp = 0;
+                b0 = FN(clip_exp)(lp);
+            }
+            REAL dW = b0 * (u[o] - dSdt) / T;
+            if (pt == 1 && c->a[o] > (REAL)NEG_BIG) dW -= b0 * (c->a[o] - S) / (T * T);
+            REAL W = wt[o] + dW;
+            if (b <= (REAL)1e-20 && FABS(W) <= (REAL)1e-20) continue;
+            FN(lin_cands)(c, c->a, i, j, v);
+            if (!FN(lin_plain_softmax)(v, T, w)) continue;
+            REAL du[4];
+            du[0] = (i > 1 && j > 1) ? u[LIX(c, i - 1, j - 1)] : 0;
+            du[1] = (i > 1) ? u[LIX(c, i - 1, j)] : 0;
+            du[2] = (j > 1) ? u[LIX(c, i, j - 1)] : 0;
+            du[3] = 0;
+            if (pt == 0) { du[1] += 1; du[2] += 1; }
+            REAL sw = w[0] * du[0] + w[1] * du[1] + w[2] * du[2] + w[3] * du[3];
+            REAL dw[4];
+            for (int q = 0; q < 4; ++q) dw[q] = w[q] * (du[q] - sw) / T;
+            if (pt == 1) {
+                REAL e = w[0] * v[0] + w[1] * v[1] + w[2] * v[2] + w[3] * v[3];
+                REAL it2 = (REAL)1 / (T * T);
+                for (int q = 0; q < 4; ++q) dw[q] += w[q] * (e - v[q]) * it2;
+            }
+            dP[(size_t)(i - 1) * c->ld + (j - 1)] += W * (w[0] + w[3]) + b * (dw[0] + dw[3]);
+            if (v[0] > (REAL)NEG_BIG) {
+                be[LIX(c, i - 1, j - 1)] += b * w[0];
+                wt[LIX(c, i - 1, j - 1)] += W * w[0] + b * dw[0];
+            }
+            if (v[1] > (REAL)NEG_BIG) {
+                be[LIX(c, i - 1, j)] += b * w[1];
+                wt[LIX(c, i - 1, j)] += W * w[1] + b * dw[1];
+            }
+            if (v[2] > (REAL)NEG_BIG) {
+                be[LIX(c, i, j - 1)] += b * w[2];
+                wt[LIX(c, i, j - 1)] += W * w[2] + b * dw[2];
+            }
+        }
+    }
+}
+
+/* ---- batched entry points (padded [B, L1max, L2max] layout) ------------ */
+
+static int FN(pair_len)(const int *lengths, int b, int which, int dflt) {
+    return lengths ? lengths[2 * b + which] : dflt;
+}
+
+/* value + map + dS/d(go, ge, T), like orihime::sw_affine_forward plus
+ * value_grad_params.  grads may be NULL. */
+int FN(oracle_sw_affine_forward)(const REAL *scores, const int *lengths, int B, int L1m,
+                                 int L2m, REAL go, REAL ge, REAL T, REAL *value, REAL *map,
+                                 REAL *gopen, REAL *gext, REAL *gT) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 3 * plane);
+    REAL *be = (REAL *)malloc(sizeof(REAL) * 3 * plane);
+    if (!a || !be) { free(a); free(be); return -1; }
+    for (int b = 0; b < B; ++b) {
+        FN(aff_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.go = go; c.ge = ge; c.T = T;
+        c.plane = plane; c.cols = (size_t)L2m + 1; c.a = a;
+        REAL S = FN(aff_forward)(&c);
+        REAL g[3];
+        FN(aff_adjoint)(&c, S, be, map + b * slab, L1m, g);
+        value[b] = S;
+        if (gopen) gopen[b] = g[0];
+        if (gext) gext[b] = g[1];
+        if (gT) gT[b] = g[2];
+    }
+    free(a); free(be);
+    return 0;
+}
+
+int FN(oracle_sw_affine_hvp)(const REAL *scores, const REAL *V, const int *lengths, int B,
+                             int L1m, int L2m, REAL go, REAL ge, REAL T, REAL *out) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *buf = (REAL *)malloc(sizeof(REAL) * 12 * plane);
+    if (!buf) return -1;
+    REAL *a = buf, *be = buf + 3 * plane, *da = buf + 6 * plane, *dbe = buf + 9 * plane;
+    for (int b = 0; b < B; ++b) {
+        FN(aff_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.go = go; c.ge = ge; c.T = T;
+        c.plane = plane; c.cols = (size_t)L2m + 1; c.a = a;
+        REAL S = FN(aff_forward)(&c);
+        FN(aff_hvp)(&c, S, V + b * slab, da, be, dbe, out + b * slab, L1m);
+    }
+    free(buf);
+    return 0;
+}
+
+/* pt: 0 = gap_open, 1 = gap_ext, 2 = temperature. */
+int FN(oracle_sw_affine_param_grad)(const REAL *scores, const int *lengths, int B, int L1m,
+                                    int L2m, REAL go, REAL ge, REAL T, int pt, REAL *out) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *buf = (REAL *)malloc(sizeof(REAL) * (15 * plane + slab));
+    if (!buf) return -1;
+    REAL *a = buf, *be = buf + 3 * plane, *u = buf + 6 * plane, *w = buf + 9 * plane;
+    REAL *be2 = buf + 12 * plane, *post = buf + 15 * plane;
+    for (int b = 0; b < B; ++b) {
+        FN(aff_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.go = go; c.ge = ge; c.T = T;
+        c.plane = plane; c.cols = (size_t)L2m + 1; c.a = a;
+        REAL S = FN(aff_forward)(&c);
+        REAL g[3];
+        FN(aff_adjoint)(&c, S, be2, post, L1m, g);
+        FN(aff_param)(&c, S, g[pt], pt, u, be, w, out + b * slab, L1m);
+    }
+    free(buf);
+    return 0;
+}
+
+int FN(oracle_sw_linear_forward)(const REAL *scores, const int *lengths, int B, int L1m,
+                                 int L2m, REAL gap, REAL T, REAL *value, REAL *map,
+                                 REAL *ggap, REAL *gT) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 2 * plane);
+    if (!a) return -1;
+    REAL *be = a + plane;
+    for (int b = 0; b < B; ++b) {
+        FN(lin_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.g = gap; c.T = T;
+        c.cols = (size_t)L2m + 1; c.a = a;
+        REAL S = FN(lin_forward)(&c);
+        REAL g[2];
+        FN(lin_adjoint)(&c, S, be, map + b * slab, L1m, g);
+        value[b] = S;
+        if (ggap) ggap[b] = g[0];
+        if (gT) gT[b] = g[1];
+    }
+    free(a);
+    return 0;
+}
+
+int FN(oracle_sw_linear_hvp)(const REAL *scores, const REAL *V, const int *lengths, int B,
+                             int L1m, int L2m, REAL gap, REAL T, REAL *out) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *buf = (REAL *)malloc(sizeof(REAL) * 4 * plane);
+    if (!buf) return -1;
+    REAL *a = buf, *be = buf + plane, *da = buf + 2 * plane, *dbe = buf + 3 * plane;
+    for (int b = 0; b < B; ++b) {
+        FN(lin_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.g = gap; c.T = T;
+        c.cols = (size_t)L2m + 1; c.a = a;
+        REAL S = FN(lin_forward)(&c);
+        FN(lin_hvp)(&c, S, V + b * slab, da, be, dbe, out + b * slab, L1m);
+    }
+    free(buf);
+    return 0;
+}
+
+/* pt: 0 = gap, 1 = temperature. */
+int FN(oracle_sw_linear_param_grad)(const REAL *scores, const int *lengths, int B, int L1m,
+                                    int L2m, REAL gap, REAL T, int pt, REAL *out) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *buf = (REAL *)malloc(sizeof(REAL) * (5 * plane + slab));
+    if (!buf) return -1;
+    REAL *a = buf, *be = buf + plane, *u = buf + 2 * plane, *w = buf + 3 * plane;
+    REAL *be2 = buf + 4 * plane, *post = buf + 5 * plane;
+    for (int b = 0; b < B; ++b) {
+        FN(lin_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.g = gap; c.T = T;
+        c.cols = (size_t)L2m + 1; c.a = a;
+        REAL S = FN(lin_forward)(&c);
+        REAL g[2];
+        FN(lin_adjoint)(&c, S, be2, post, L1m, g);
+        FN(lin_param)(&c, S, g[pt], pt, u, be, w, out + b * slab, L1m);
+    }
+    free(buf);
+    return 0;
+}
+
+#undef AIX
+#undef SC
+#undef LIX
+#undef FN
+#undef CAT
+#undef CAT2

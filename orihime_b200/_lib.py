@@ -1,0 +1,79 @@
+"""ctypes binding of the CUDA library ``_swb.so`` (C ABI: include/orihime_b200.h).
+
+The library is required: there is no CPU or pure-PyTorch fallback.  Importing
+the op layer on a machine without the built library raises ImportError with
+the build command.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+_SO = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_swb.so")
+
+ABI_VERSION = 1
+
+OK = 0
+ERR_ARG = -1
+ERR_WORKSPACE = -2
+ERR_CUDA = -3
+
+STATUS_WAIT_TIMEOUT = 1
+
+
+class Options(ctypes.Structure):
+    """Mirror of ``swb_options``."""
+
+    _fields_ = [
+        ("max_ctas", ctypes.c_int),
+        ("spin_limit_ns", ctypes.c_ulonglong),
+        ("fault_inject", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def path() -> str:
+    return _SO
+
+
+def load() -> ctypes.CDLL:
+    """Load (once) and return the CUDA library, or raise ImportError."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_SO):
+        raise ImportError(
+            f"orihime_b200 CUDA library not found at {_SO}; build it with "
+            "`python -m orihime_b200.build` (needs nvcc)"
+        )
+    lib = ctypes.CDLL(_SO)
+    vp, sz, i, f = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_float
+    lib.swb_abi_version.restype = i
+    lib.swb_error_string.restype = ctypes.c_char_p
+    lib.swb_error_string.argtypes = [i]
+    lib.swb_sw_affine_workspace_bytes.restype = sz
+    lib.swb_sw_affine_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sw_workspace_bytes.restype = sz
+    lib.swb_sw_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sw_affine_forward.restype = i
+    lib.swb_sw_affine_forward.argtypes = [vp, vp, i, i, i, f, f, f, vp, vp, vp, vp, vp, vp, sz,
+                                          vp, ctypes.POINTER(Options)]
+    lib.swb_sw_forward.restype = i
+    lib.swb_sw_forward.argtypes = [vp, vp, i, i, i, f, f, vp, vp, vp, vp, vp, sz, vp,
+                                   ctypes.POINTER(Options)]
+    lib.swb_read_status.restype = i
+    lib.swb_read_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_uint)]
+    got = lib.swb_abi_version()
+    if got != ABI_VERSION:
+        raise ImportError(f"orihime_b200 library ABI {got} != expected {ABI_VERSION}; rebuild it")
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != OK:
+        msg = load().swb_error_string(rc).decode()
+        raise RuntimeError(f"{what} failed: {msg} (code {rc})")

@@ -1,0 +1,275 @@
+"""CUDA implementations of the ``torch.ops.orihime`` soft Smith-Waterman ops.
+
+This module is the drop-in seam.  The reference registers its CUDA kernels
+with ``TORCH_LIBRARY_IMPL(orihime, CUDA / AutogradCUDA, m)``
+(src/sw/torch_cuda.cpp:803-830, src/sw_affine/torch_cuda.cpp:917-946); here
+the same operator names get implementations that call the B200 kernels
+through the C ABI (``_lib``).
+
+* If the reference's own extension is already loaded in the process, its
+  schemas exist and only the CUDA / AutogradCUDA kernels are replaced.
+* Otherwise the schemas are defined here, character for character as in
+  src/sw/registry.cpp:38-44 and src/sw_affine/registry.cpp:35-42.
+
+Validation mirrors the reference op bodies (same conditions, same messages)
+so that error-path tests read the same.  Like the reference, the value ops
+read ``lengths`` on the host to range-check them.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+
+_LIB = _lib.load()  # fail loudly at import if the CUDA library is missing
+
+SCHEMAS = {
+    # src/sw/registry.cpp:38-44
+    "sw_forward": "sw_forward(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor[]",
+    "sw_forward_t": "sw_forward_t(Tensor scores, Tensor gap, Tensor temp, Tensor lengths) -> Tensor[]",
+    "sw_value_grad_params": "sw_value_grad_params(Tensor scores, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor)",
+    "sw_marginals_backward": "sw_marginals_backward(Tensor scores, Tensor grad_marginals, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
+    "sw_marginals_hvp": "sw_marginals_hvp(Tensor scores, Tensor v, float gap, float temp, Tensor? lengths) -> Tensor",
+    "sw_marginals_grad_gap": "sw_marginals_grad_gap(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
+    "sw_marginals_grad_temp": "sw_marginals_grad_temp(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
+    # src/sw_affine/registry.cpp:35-42
+    "sw_affine_forward": "sw_affine_forward(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor[]",
+    "sw_affine_forward_t": "sw_affine_forward_t(Tensor scores, Tensor gap_open, Tensor gap_ext, Tensor temp, Tensor lengths) -> Tensor[]",
+    "sw_affine_value_grad_params": "sw_affine_value_grad_params(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
+    "sw_affine_marginals_backward": "sw_affine_marginals_backward(Tensor scores, Tensor grad_marginals, float gap_open, float gap_ext, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
+    "sw_affine_marginals_hvp": "sw_affine_marginals_hvp(Tensor scores, Tensor v, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "sw_affine_marginals_grad_gap_open": "sw_affine_marginals_grad_gap_open(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "sw_affine_marginals_grad_gap_ext": "sw_affine_marginals_grad_gap_ext(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "sw_affine_marginals_grad_temp": "sw_affine_marginals_grad_temp(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+}
+
+_INT32_MAX = 2**31 - 1
+
+
+def _op_exists(name: str) -> bool:
+    try:
+        torch._C._dispatch_find_schema_or_throw(f"orihime::{name}", "")
+        return True
+    except RuntimeError:
+        return False
+
+
+_DEF_LIB = torch.library.Library("orihime", "FRAGMENT")
+DEFINED_HERE = []
+for _name, _schema in SCHEMAS.items():
+    if not _op_exists(_name):
+        _DEF_LIB.define(_schema)
+        DEFINED_HERE.append(_name)
+
+_IMPL_LIB = torch.library.Library("orihime", "IMPL")
+
+
+# ---------------------------------------------------------------------------
+# validation (src/common/torch_utils.h:31-110, src/sw*/torch_cuda.cpp:35-110)
+# ---------------------------------------------------------------------------
+
+_SCALAR_NAMES = {
+    torch.float32: "Float", torch.float64: "Double", torch.float16: "Half",
+    torch.bfloat16: "BFloat16", torch.int32: "Int", torch.int64: "Long", torch.bool: "Bool",
+    torch.int16: "Short", torch.int8: "Char", torch.uint8: "Byte",
+}
+
+
+def _stype(t: torch.Tensor) -> str:
+    return _SCALAR_NAMES.get(t.dtype, str(t.dtype))
+
+
+def check_input_cuda(x: torch.Tensor, name: str) -> None:
+    if not x.is_cuda:
+        raise RuntimeError(f"{name} must be a CUDA tensor")
+    if not x.is_contiguous():
+        raise RuntimeError(f"{name} must be contiguous")
+    if x.dtype != torch.float32:
+        raise RuntimeError(f"{name} must be float32, got {_stype(x)}")
+
+
+def _checked_dim(v: int, what: str) -> int:
+    if v < 0:
+        raise RuntimeError(f"{what} must be non-negative, got {v}")
+    if v > _INT32_MAX:
+        raise RuntimeError(f"{what} exceeds CUDA int index range: {v}")
+    return int(v)
+
+
+def check_shape(scores: torch.Tensor, family: str) -> tuple[int, int, int]:
+    """3-D check plus the reference's index-range guards (torch_cuda.cpp:35-67)."""
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    B = _checked_dim(scores.size(0), "scores.size(0)")
+    L1 = _checked_dim(scores.size(1), "scores.size(1)")
+    L2 = _checked_dim(scores.size(2), "scores.size(2)")
+    if L1 > _INT32_MAX - L2:
+        raise RuntimeError(f"{family} dimensions too large: L1 + L2 exceeds CUDA int index range")
+    return B, L1, L2
+
+
+def resolve_lengths(lengths, B: int, L1: int, L2: int, device) -> torch.Tensor:
+    """Default or validate [B, 2] int32 lengths (validate_sw_affine_lengths_cuda)."""
+    if lengths is None:
+        return torch.tensor([[L1, L2]] * B, dtype=torch.int32, device=device).reshape(B, 2)
+    if not lengths.is_cuda:
+        raise RuntimeError("lengths must be a CUDA tensor")
+    if not lengths.is_contiguous():
+        raise RuntimeError("lengths must be contiguous")
+    if not (lengths.dim() == 2 and lengths.size(0) == B and lengths.size(1) == 2):
+        raise RuntimeError(
+            "Expected lengths.dim() == 2 && lengths.size(0) == B && lengths.size(1) == 2 "
+            "to be true, but got false."
+        )
+    if lengths.dtype != torch.int32:
+        raise RuntimeError("lengths must be int32")
+    if lengths.device != device:
+        raise RuntimeError(f"lengths must be on same device as scores, got {lengths.device} vs {device}")
+    host = lengths.cpu().tolist()
+    for b, (l1, l2) in enumerate(host):
+        if not (0 <= l1 <= L1):
+            raise RuntimeError(f"lengths[{b},0] must be between 0 and {L1}, got {l1}")
+        if not (0 <= l2 <= L2):
+            raise RuntimeError(f"lengths[{b},1] must be between 0 and {L2}, got {l2}")
+    return lengths
+
+
+def _scalar_param(t: torch.Tensor, name: str) -> float:
+    if t.numel() != 1:
+        raise RuntimeError(f"{name} must be a scalar tensor")
+    return float(t.detach().cpu().reshape(()).item())
+
+
+# ---------------------------------------------------------------------------
+# kernel calls
+# ---------------------------------------------------------------------------
+
+def _stream(device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def run_affine(scores, lengths, go, ge, temp, options=None):
+    """value, map, grad_open, grad_ext, grad_temp for a validated padded batch."""
+    B, L1, L2 = scores.shape
+    dev = scores.device
+    value = torch.empty(B, dtype=torch.float32, device=dev)
+    amap = torch.empty_like(scores)
+    g_open = torch.empty(B, dtype=torch.float32, device=dev)
+    g_ext = torch.empty(B, dtype=torch.float32, device=dev)
+    g_T = torch.empty(B, dtype=torch.float32, device=dev)
+    if B == 0:
+        return value, amap, g_open, g_ext, g_T
+    nbytes = _LIB.swb_sw_affine_workspace_bytes(B, L1, L2)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    with torch.cuda.device(dev):
+        rc = _LIB.swb_sw_affine_forward(
+            _ptr(scores), _ptr(lengths), B, L1, L2, float(go), float(ge), float(temp),
+            _ptr(value), _ptr(amap), _ptr(g_open), _ptr(g_ext), _ptr(g_T), _ptr(ws), nbytes,
+            _stream(dev), options)
+    _lib.check(rc, "swb_sw_affine_forward")
+    return value, amap, g_open, g_ext, g_T
+
+
+def run_linear(scores, lengths, gap, temp, options=None):
+    """value, map, grad_gap, grad_temp for a validated padded batch."""
+    B, L1, L2 = scores.shape
+    dev = scores.device
+    value = torch.empty(B, dtype=torch.float32, device=dev)
+    amap = torch.empty_like(scores)
+    g_gap = torch.empty(B, dtype=torch.float32, device=dev)
+    g_T = torch.empty(B, dtype=torch.float32, device=dev)
+    if B == 0:
+        return value, amap, g_gap, g_T
+    nbytes = _LIB.swb_sw_workspace_bytes(B, L1, L2)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    with torch.cuda.device(dev):
+        rc = _LIB.swb_sw_forward(
+            _ptr(scores), _ptr(lengths), B, L1, L2, float(gap), float(temp), _ptr(value),
+            _ptr(amap), _ptr(g_gap), _ptr(g_T), _ptr(ws), nbytes, _stream(dev), options)
+    _lib.check(rc, "swb_sw_forward")
+    return value, amap, g_gap, g_T
+
+
+def _prep(scores, lengths, family):
+    check_input_cuda(scores, "scores")
+    B, L1, L2 = check_shape(scores, family)
+    return resolve_lengths(lengths, B, L1, L2, scores.device)
+
+
+# ---- affine ----------------------------------------------------------------
+
+def sw_affine_forward(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::sw_affine_forward -> [value [B], marginals [B, L1, L2]]
+    (src/sw_affine/torch_cuda.cpp:820 -> :419 -> :128-206)."""
+    ln = _prep(scores, lengths, "sw_affine")
+    v, m, *_ = run_affine(scores, ln, gap_open, gap_ext, temp)
+    return [v, m]
+
+
+def sw_affine_forward_t(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::sw_affine_forward_t (src/sw_affine/torch_cuda.cpp:830 -> :126-206)."""
+    check_input_cuda(scores, "scores")
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    go = _scalar_param(gap_open, "gap_open")
+    ge = _scalar_param(gap_ext, "gap_ext")
+    T = _scalar_param(temp, "temperature")
+    B, L1, L2 = check_shape(scores, "sw_affine")
+    ln = resolve_lengths(lengths, B, L1, L2, scores.device)
+    v, m, *_ = run_affine(scores, ln, go, ge, T)
+    return [v, m]
+
+
+def sw_affine_value_grad_params(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::sw_affine_value_grad_params -> (dS/dgo, dS/dge, dS/dT), each [B]
+    (src/sw_affine/torch_cuda.cpp:842 -> soft_sw_affine_cuda_with_grads :446)."""
+    ln = _prep(scores, lengths, "sw_affine")
+    _, _, go, ge, gT = run_affine(scores, ln, gap_open, gap_ext, temp)
+    return go, ge, gT
+
+
+# ---- linear ----------------------------------------------------------------
+
+def sw_forward(scores, gap, temp, lengths):
+    """orihime::sw_forward -> [value [B], marginals [B, L1, L2]] (src/sw/torch_cuda.cpp:364-402)."""
+    ln = _prep(scores, lengths, "sw")
+    v, m, *_ = run_linear(scores, ln, gap, temp)
+    return [v, m]
+
+
+def sw_forward_t(scores, gap, temp, lengths):
+    """orihime::sw_forward_t (src/sw/torch_cuda.cpp:124-210)."""
+    check_input_cuda(scores, "scores")
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    g = _scalar_param(gap, "gap")
+    T = _scalar_param(temp, "temperature")
+    B, L1, L2 = check_shape(scores, "sw")
+    ln = resolve_lengths(lengths, B, L1, L2, scores.device)
+    v, m, *_ = run_linear(scores, ln, g, T)
+    return [v, m]
+
+
+def sw_value_grad_params(scores, gap, temp, lengths):
+    """orihime::sw_value_grad_params -> (dS/dgap, dS/dT), each [B] (src/sw/torch_cuda.cpp:404-450)."""
+    ln = _prep(scores, lengths, "sw")
+    _, _, gg, gT = run_linear(scores, ln, gap, temp)
+    return gg, gT
+
+
+IMPLS = {
+    "sw_forward": sw_forward,
+    "sw_forward_t": sw_forward_t,
+    "sw_value_grad_params": sw_value_grad_params,
+    "sw_affine_forward": sw_affine_forward,
+    "sw_affine_forward_t": sw_affine_forward_t,
+    "sw_affine_value_grad_params": sw_affine_value_grad_params,
+}
+
+for _name, _fn in IMPLS.items():
+    _IMPL_LIB.impl(_name, _fn, "CUDA")

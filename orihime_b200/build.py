@@ -1,0 +1,59 @@
+"""Build the CUDA library ``orihime_b200/_swb.so`` in-tree with nvcc (sm_100a).
+
+    python -m orihime_b200.build
+
+The library is a plain C ABI (``include/orihime_b200.h``): no torch headers,
+so it builds in seconds and loads with ctypes.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+SO = os.path.join(PKG, "_swb.so")
+SOURCES = [os.path.join(PKG, "csrc", "sw_capi.cu")]
+DEPS = SOURCES + [
+    os.path.join(PKG, "csrc", "sw_kernels.cu"),
+    os.path.join(PKG, "csrc", "sw_kernels.cuh"),
+    os.path.join(ROOT, "include", "orihime_b200.h"),
+]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build orihime_b200")
+    return cand
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(SO):
+        return False
+    t = os.path.getmtime(SO)
+    return all(os.path.getmtime(d) <= t for d in DEPS)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return SO
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+           "-I", os.path.join(ROOT, "include"), "-o", SO + ".tmp", *SOURCES]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+    if verbose:
+        sys.stderr.write(res.stdout + res.stderr)
+    os.replace(SO + ".tmp", SO)
+    return SO
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

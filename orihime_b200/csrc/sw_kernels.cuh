@@ -1,0 +1,81 @@
+// Soft Smith-Waterman wavefront kernels for sm_100a (linear and affine gaps).
+//
+// Work decomposition
+// ------------------
+// A pair (L1 x L2 scores) is cut into column *bands* of 32*R columns.  One
+// warp owns one band: lane l owns the R consecutive columns
+// [band*32R + l*R, +R) and the warp sweeps the rows top to bottom as a skewed
+// wavefront -- at step t lane l works on row i = t - l + 1 (1-based), so the
+// band takes L1 + 31 steps.  The values of a lane's last column reach lane l+1
+// one step later through __shfl_up_sync; the last lane of a band writes them
+// to a global "edge" buffer that lane 0 of the next band polls.
+//
+// All DP values live in a scaled log2 domain: x' = x * log2(e) / T, so every
+// exp/log of the reference recurrence is one MUFU ex2/lg2.
+//
+// Forward kernel (one launch per op call): alpha, the partition partials and,
+// every C steps, a per-lane checkpoint of the DP state (3R+3 floats affine,
+// R+1 linear).  No alpha table is ever stored.
+//
+// Adjoint kernel: per band, time chunks in reverse.  Each chunk restores its
+// checkpoint, recomputes C steps of alpha into shared memory, then runs the
+// adjoint (beta) recurrence backwards in "push" form: a finished cell pushes
+// beta*w to its predecessors -- within the lane through registers, to the
+// left lane through __shfl_down_sync, to the left band through a global
+// buffer.  No atomics; the map is written row by row.
+//
+// Cross-band buffers are filled with a NaN sentinel before each call; a
+// consumer polls the value itself until it is not the sentinel, so no memory
+// fence is needed on the producer side.  Every poll is bounded by a
+// globaltimer deadline; on expiry the kernel records SWB_ERR_WAIT_TIMEOUT in
+// the status word, substitutes a neutral value and carries on, so no warp can
+// hang.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace swb {
+
+constexpr float NEG = -1e30f;           // "no path" in the scaled domain
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int C_STEPS = 8;              // checkpoint stride (steps)
+constexpr int PF = 4;                   // prefetch distance (steps); C_STEPS % PF == 0
+constexpr uint32_t SENTINEL_BITS = 0xffffffffu;
+
+enum : unsigned {
+  ERR_WAIT_TIMEOUT = 1u,
+};
+
+// Launch arguments shared by the forward and adjoint kernels.
+struct Args {
+  // problem
+  const float* scores;        // layout 0: [B, Lmax1, Lmax2]; layout 1: flat ragged
+  float* map;                 // same layout as scores
+  const int* lengths;         // [B, 2] or null (= full padded lengths)
+  const long long* offsets;   // layout 1: [B+1] element offsets (multiples of 4)
+  const int* order;           // optional pair order of the task queue (null = 0..B-1)
+  int B, Lmax1, Lmax2;
+  int layout;                 // 0 padded, 1 ragged packed (row pitch = round4(L2))
+  float go, ge, T, k;         // gaps in natural units, temperature, k = log2(e)/T
+  int nb;                     // bands per pair (uniform, >= ceil(max L2 / 32R))
+  int nchunks;                // checkpoint chunks per band (>= ceil((max L1+31)/C))
+  // outputs [B]
+  float* value;
+  float* g_open;              // affine: dS/dgo ; linear: dS/dgap
+  float* g_ext;               // affine: dS/dge ; linear: unused
+  float* g_T;
+  // workspace (see workspace_layout in sw_capi.cu)
+  unsigned* counters;         // [0] forward task counter, [1] adjoint task counter
+  unsigned* status;           // error bits
+  unsigned* pair_done;        // [B]
+  float* part;                // [B*nb][2] partition partials (ref, sum)
+  float* gpart;               // [B*nb][4] gradient partials
+  float* edge;                // [B*nb][NS][Lmax1] sentinel-initialised
+  float* bpush;               // [B*nb][NP][Lmax1+1] sentinel-initialised
+  float* ckpt;                // [B*nb][nchunks][CKF][32]
+  unsigned long long spin_limit_ns;
+  int fault_inject;           // 1: band>0 waits on a word nobody writes (tests only)
+  float* never_written;       // target of fault_inject polls
+};
+
+}  // namespace swb

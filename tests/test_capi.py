@@ -1,0 +1,79 @@
+"""The C ABI library loads and exports exactly what include/orihime_b200.h declares (CPU)."""
+
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "orihime_b200.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(swb_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from orihime_b200 import _lib
+
+    return _lib.load()
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    assert "swb_sw_affine_forward" in names and "swb_sw_forward" in names
+    assert len(names) >= 7
+
+
+def test_library_exports_every_declared_symbol(lib):
+    from orihime_b200 import _lib
+
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.path()], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (swb_[a-z0-9_]+)", out))
+    missing = [n for n in _declared() if n not in exported]
+    assert not missing, missing
+    for n in _declared():
+        assert hasattr(lib, n)
+
+
+def test_abi_version_and_errors(lib):
+    assert lib.swb_abi_version() == 1
+    assert lib.swb_error_string(0) == b"ok"
+    assert b"workspace" in lib.swb_error_string(-2)
+
+
+def test_workspace_sizes_monotone(lib):
+    a = lib.swb_sw_affine_workspace_bytes(4, 100, 100)
+    b = lib.swb_sw_affine_workspace_bytes(8, 100, 100)
+    c = lib.swb_sw_affine_workspace_bytes(4, 200, 300)
+    assert 0 < a < b and a < c
+    assert lib.swb_sw_affine_workspace_bytes(0, 10, 10) == 0
+    assert 0 < lib.swb_sw_workspace_bytes(4, 100, 100) < a
+    # checkpoint storage is O(cells / chunk), far below a full 3-state table
+    full = 3 * 4 * 16385 * 16385 * 4
+    assert lib.swb_sw_affine_workspace_bytes(4, 16384, 16384) < full / 4
+
+
+def test_argument_errors_return_before_any_launch(lib):
+    # these return before touching CUDA, so they run on a CPU-only host too
+    f = ctypes.c_float
+    rc = lib.swb_sw_affine_forward(None, None, 1, 4, 4, f(-2), f(-0.5), f(0.0), None, None, None,
+                                   None, None, None, 0, None, None)
+    assert rc == -1  # temperature must be > 0
+    rc = lib.swb_sw_affine_forward(None, None, -1, 4, 4, f(-2), f(-0.5), f(1.0), None, None, None,
+                                   None, None, None, 0, None, None)
+    assert rc == -1
+    rc = lib.swb_sw_forward(None, None, 0, 4, 4, f(-1), f(1.0), None, None, None, None, None, 0,
+                            None, None)
+    assert rc == 0  # empty batch: nothing to do
+    buf = (ctypes.c_float * 16)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    rc = lib.swb_sw_affine_forward(p, None, 1, 4, 4, f(-2), f(-0.5), f(1.0), p, p, p, p, p, p, 16,
+                                   None, None)
+    assert rc == -2  # workspace too small

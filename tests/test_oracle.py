@@ -1,0 +1,160 @@
+"""The oracle is pinned before it is trusted (CPU only).
+
+1. Against the golden fixtures recorded from the reference's public API
+   (tests/golden/make_golden.py): value, map, entropy, value/map/entropy
+   gradients, parameter sensitivities and the map VJP.
+2. Against the reference's own CPU kernels compiled from source
+   (oracle/_ref, when present): the float restatement must agree bit for bit.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+CASES = ["sq", "rect", "ragged", "unit", "row"]
+T0 = 0.7
+
+
+def _case(golden, case):
+    s = golden[f"{case}/scores"]
+    ln = golden[f"{case}/lengths"] if f"{case}/lengths" in golden.files else None
+    return s, ln, golden[f"{case}/cot"]
+
+
+def _close(a, b, rtol=2e-5, atol=2e-6):
+    np.testing.assert_allclose(np.asarray(a, np.float64), np.asarray(b, np.float64), rtol=rtol,
+                               atol=atol)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_affine_oracle_vs_golden(golden, case):
+    s, ln, cot = _case(golden, case)
+    g = lambda k: golden[f"{case}/aff/{k}"]
+    B = s.shape[0]
+    o = O.affine(s, ln, -2.0, -0.5, T0)
+    _close(o["value"], g("value"))
+    _close(o["map"], g("map"))
+    _close(-o["map"] / B, g("dvalue"))
+    _close(o["grad_temp"], g("entropy"), atol=2e-5)
+    sens = {p: O.affine_param_grad(s, ln, -2.0, -0.5, T0, p) for p in range(3)}
+    _close(sens[0], g("sens_gap_open_score"), atol=1e-5)
+    _close(sens[1], g("sens_gap_extend_score"), atol=1e-5)
+    _close(sens[2], g("sens_temperature"), atol=1e-5)
+    _close(sens[2], g("dentropy"), atol=1e-5)
+    hv = O.affine_hvp(s, cot, ln, -2.0, -0.5, T0)
+    _close(hv, g("dmap"), atol=1e-5)
+    _close(hv, g("bw_pair_scores"), atol=1e-5)
+    _close((cot * sens[0]).sum(), g("bw_gap_open_score"), atol=1e-4)
+    _close((cot * sens[1]).sum(), g("bw_gap_extend_score"), atol=1e-4)
+    _close((cot * sens[2]).sum(), g("bw_temperature"), atol=1e-4)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_linear_oracle_vs_golden(golden, case):
+    s, ln, cot = _case(golden, case)
+    g = lambda k: golden[f"{case}/lin/{k}"]
+    B = s.shape[0]
+    o = O.linear(s, ln, -1.0, T0)
+    _close(o["value"], g("value"))
+    _close(o["map"], g("map"))
+    _close(-o["map"] / B, g("dvalue"))
+    _close(o["grad_temp"], g("entropy"), atol=2e-5)
+    sens = {p: O.linear_param_grad(s, ln, -1.0, T0, p) for p in range(2)}
+    _close(sens[0], g("sens_gap_score"), atol=1e-5)
+    _close(sens[1], g("sens_temperature"), atol=1e-5)
+    _close(sens[1], g("dentropy"), atol=1e-5)
+    hv = O.linear_hvp(s, cot, ln, -1.0, T0)
+    _close(hv, g("dmap"), atol=1e-5)
+    _close(hv, g("bw_pair_scores"), atol=1e-5)
+    _close((cot * sens[0]).sum(), g("bw_gap_score"), atol=1e-4)
+    _close((cot * sens[1]).sum(), g("bw_temperature"), atol=1e-4)
+
+
+def _mask_sentinel(scores, mask, T):
+    """orihime/operator.py:334-386: masked cells -> amax - (sum(shape[1:])*80 + 200)*T."""
+    x = np.where(mask, -np.inf, scores).astype(np.float32)
+    amax = x.reshape(x.shape[0], -1).max(axis=1)
+    amax = np.where(np.isfinite(amax), amax, 0.0)
+    off = (float(sum(x.shape[1:])) * 80.0 + 200.0) * T
+    sent = (amax - np.float32(off)).astype(np.float32)[:, None, None]
+    return np.where(mask, sent, x).astype(np.float32)
+
+
+def test_masked_batches_vs_golden(golden):
+    s = golden["mask/scores"]
+    mask = golden["mask/mask"].astype(bool)
+    x = _mask_sentinel(s, mask, 0.8)
+    o = O.affine(x, None, -2.0, -0.5, 0.8)
+    _close(o["value"], golden["mask/aff/value"])
+    _close(o["map"], golden["mask/aff/map"])
+    _close(o["map"], golden["mask/aff/dx"])
+    _close(o["grad_open"].sum(), golden["mask/aff/dgap_open"], atol=1e-4)
+    _close(o["grad_ext"].sum(), golden["mask/aff/dgap_ext"], atol=1e-4)
+    _close(o["grad_temp"].sum(), golden["mask/aff/dtemp"], atol=1e-4)
+    o = O.linear(x, None, -1.0, 0.8)
+    _close(o["value"], golden["mask/lin/value"])
+    _close(o["map"], golden["mask/lin/map"])
+    _close(o["grad_gap"].sum(), golden["mask/lin/dgap"], atol=1e-4)
+    _close(o["grad_temp"].sum(), golden["mask/lin/dtemp"], atol=1e-4)
+    assert np.all(o["map"][mask] == 0.0)
+
+
+def test_fp64_oracle_close_to_fp32(golden):
+    s, ln, _ = _case(golden, "ragged")
+    a = O.affine(s, ln, -2.0, -0.5, T0, dtype=np.float32)
+    b = O.affine(s, ln, -2.0, -0.5, T0, dtype=np.float64)
+    _close(a["value"], b["value"], rtol=1e-6)
+    _close(a["map"], b["map"], atol=1e-6)
+
+
+ref_only = pytest.mark.skipif(not O.ref_available(), reason="reference CPU kernels not built")
+
+
+@ref_only
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_oracle_bit_exact_vs_reference_kernels(seed):
+    rng = np.random.default_rng(seed)
+    B, L1, L2 = 3, int(rng.integers(1, 17)), int(rng.integers(1, 17))
+    s = (rng.standard_normal((B, L1, L2)) * 2).astype(np.float32)
+    ln = np.stack([rng.integers(0, L1 + 1, B), rng.integers(0, L2 + 1, B)], 1).astype(np.int32)
+    V = rng.standard_normal(s.shape).astype(np.float32)
+    for lens in (None, ln):
+        for T in (0.3, 1.0, 2.0):
+            a, r = O.affine(s, lens, -2.0, -0.5, T), O.ref_affine(s, lens, -2.0, -0.5, T)
+            for k in a:
+                assert np.array_equal(a[k], r[k]), k
+            assert np.array_equal(O.affine_hvp(s, V, lens, -2.0, -0.5, T),
+                                  O.ref_affine_hvp(s, V, lens, -2.0, -0.5, T))
+            for p in range(3):
+                assert np.array_equal(O.affine_param_grad(s, lens, -2.0, -0.5, T, p),
+                                      O.ref_affine_param_grad(s, lens, -2.0, -0.5, T, p))
+            a, r = O.linear(s, lens, -1.0, T), O.ref_linear(s, lens, -1.0, T)
+            for k in a:
+                assert np.array_equal(a[k], r[k]), k
+            assert np.array_equal(O.linear_hvp(s, V, lens, -1.0, T),
+                                  O.ref_linear_hvp(s, V, lens, -1.0, T))
+            for p in range(2):
+                assert np.array_equal(O.linear_param_grad(s, lens, -1.0, T, p),
+                                      O.ref_linear_param_grad(s, lens, -1.0, T, p))
+
+
+def test_finite_difference_of_fp64_value():
+    """dS/dscores (the map) and dS/dgap against central differences of the FP64 oracle."""
+    rng = np.random.default_rng(5)
+    s = rng.standard_normal((1, 6, 7))
+    base = O.affine(s, None, -2.0, -0.5, 0.5, dtype=np.float64)
+    eps = 1e-5
+    for (i, j) in [(0, 0), (2, 3), (5, 6), (3, 1)]:
+        sp, sm = s.copy(), s.copy()
+        sp[0, i, j] += eps
+        sm[0, i, j] -= eps
+        fd = (O.affine(sp, None, -2.0, -0.5, 0.5, dtype=np.float64)["value"][0] -
+              O.affine(sm, None, -2.0, -0.5, 0.5, dtype=np.float64)["value"][0]) / (2 * eps)
+        assert abs(fd - base["map"][0, i, j]) < 1e-6
+    fd = (O.affine(s, None, -2.0 + eps, -0.5, 0.5, dtype=np.float64)["value"][0] -
+          O.affine(s, None, -2.0 - eps, -0.5, 0.5, dtype=np.float64)["value"][0]) / (2 * eps)
+    assert abs(fd - base["grad_open"][0]) < 1e-6
+    fd = (O.affine(s, None, -2.0, -0.5, 0.5 + eps, dtype=np.float64)["value"][0] -
+          O.affine(s, None, -2.0, -0.5, 0.5 - eps, dtype=np.float64)["value"][0]) / (2 * eps)
+    assert abs(fd - base["grad_temp"][0]) < 1e-5
