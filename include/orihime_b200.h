@@ -96,6 +96,11 @@ const char* swb_error_string(int code);
 /* SWB_ABI_VERSION of the loaded library. */
 int swb_abi_version(void);
 
+/* Roofline probe (no reference counterpart): launches `blocks` x 256 threads,
+ * each issuing iters * 8 dependent-chain ex2.approx operations on the MUFU
+ * pipe; `scratch` needs blocks * 256 floats.  Time it with events on `stream`. */
+int swb_mufu_probe(float* scratch, int blocks, int iters, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,7 +47,7 @@ def load() -> ctypes.CDLL:
     if not os.path.exists(_SO):
         raise ImportError(
             f"orihime_b200 CUDA library not found at {_SO}; build it with "
-            "`python -m orihime_b200.build` (needs nvcc)"
+            "`python orihime_b200/build.py` (needs nvcc)"
         )
     lib = ctypes.CDLL(_SO)
     vp, sz, i, f = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_float
@@ -66,6 +66,8 @@ def load() -> ctypes.CDLL:
                                    ctypes.POINTER(Options)]
     lib.swb_read_status.restype = i
     lib.swb_read_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_uint)]
+    lib.swb_mufu_probe.restype = i
+    lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()
     if got != ABI_VERSION:
         raise ImportError(f"orihime_b200 library ABI {got} != expected {ABI_VERSION}; rebuild it")

@@ -1,6 +1,9 @@
 """Build the CUDA library ``orihime_b200/_swb.so`` in-tree with nvcc (sm_100a).
 
-    python -m orihime_b200.build
+    python orihime_b200/build.py [--force] [-v]
+
+Standalone on purpose: importing the package needs the library, so this file
+must not import the package.
 
 The library is a plain C ABI (``include/orihime_b200.h``): no torch headers,
 so it builds in seconds and loads with ctypes.
@@ -20,6 +23,7 @@ SOURCES = [os.path.join(PKG, "csrc", "sw_capi.cu")]
 DEPS = SOURCES + [
     os.path.join(PKG, "csrc", "sw_kernels.cu"),
     os.path.join(PKG, "csrc", "sw_kernels.cuh"),
+    os.path.join(PKG, "csrc", "sw_probe.cuh"),
     os.path.join(ROOT, "include", "orihime_b200.h"),
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

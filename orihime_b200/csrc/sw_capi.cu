@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "sw_kernels.cu"
+#include "sw_probe.cuh"
 #include "../../include/orihime_b200.h"
 
 namespace {
@@ -19,14 +20,15 @@ namespace {
 using swb::Args;
 
 constexpr int kR = 4;                 // columns per lane
-constexpr int kWarpsPerCta = 4;
+constexpr int kWarpsFwd = 4;          // forward CTA: 4 independent warps
+constexpr int kWarpsBwd = 1;          // adjoint CTA: 1 warp (shared memory bound)
 constexpr size_t kAlign = 256;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
-template <int NS> constexpr int np() { return NS == 3 ? 5 : 2; }
-template <int NS> constexpr int ckf() { return NS * kR + NS; }
-template <int NS> constexpr int ef() { return NS * kR + NS + kR; }
+template <int NS> constexpr int np() { return swb::Dims<NS, kR>::NP; }
+template <int NS> constexpr int ckf() { return swb::Dims<NS, kR>::CKF; }
+template <int NS> constexpr int ne() { return swb::Dims<NS, kR>::NE; }
 
 struct Layout {
   int nb, nchunks;
@@ -40,7 +42,7 @@ Layout layout_for(long long B, long long L1m, long long L2m) {
   Layout l{};
   l.nb = (int)((L2m + 32 * kR - 1) / (32 * kR));
   if (l.nb < 1) l.nb = 1;
-  l.nchunks = (int)((L1m + 31 + swb::C_STEPS - 1) / swb::C_STEPS);
+  l.nchunks = (int)((L1m + 31 + swb::C_STEPS - 1) / swb::C_STEPS);  // = band_chunks(L1m)
   const size_t slots = (size_t)B * l.nb;
   size_t o = 0;
   l.off_hdr = o;        o = align_up(o + 64);
@@ -48,7 +50,7 @@ Layout layout_for(long long B, long long L1m, long long L2m) {
   l.off_part = o;       o = align_up(o + sizeof(float) * 2 * slots);
   l.off_gpart = o;      o = align_up(o + sizeof(float) * 4 * slots);
   l.off_sent = o;       o = o + kAlign;   // never_written word lives here
-  l.off_edge = o;       o = align_up(o + sizeof(float) * slots * NS * (size_t)L1m);
+  l.off_edge = o;       o = align_up(o + sizeof(float) * slots * ne<NS>() * (size_t)L1m);
   l.off_bpush = o;      o = align_up(o + sizeof(float) * slots * np<NS>() * (size_t)(L1m + 1));
   l.sent_bytes = o - l.off_sent;
   l.off_ckpt = o;       o = align_up(o + sizeof(float) * slots * l.nchunks * ckf<NS>() * 32);
@@ -66,7 +68,7 @@ DevInfo g_dev[64];
 std::mutex g_mu;
 
 template <int NS>
-size_t bwd_smem() { return (size_t)kWarpsPerCta * (swb::C_STEPS + 1) * ef<NS>() * 32 * sizeof(float); }
+size_t bwd_smem() { return (size_t)kWarpsBwd * swb::bwd_smem_floats<NS, kR>() * sizeof(float); }
 
 int dev_info(DevInfo** out) {
   int dev = 0;
@@ -76,18 +78,18 @@ int dev_info(DevInfo** out) {
   if (!d.ready) {
     if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       return SWB_ERR_CUDA;
-    if (cudaFuncSetAttribute(swb::bwd_kernel<3, kR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(swb::bwd_kernel<3, kR, kWarpsBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bwd_smem<3>()) != cudaSuccess)
       return SWB_ERR_CUDA;
-    if (cudaFuncSetAttribute(swb::bwd_kernel<1, kR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(swb::bwd_kernel<1, kR, kWarpsBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bwd_smem<1>()) != cudaSuccess)
       return SWB_ERR_CUDA;
-    const int tpb = 32 * kWarpsPerCta;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_fwd[0], swb::fwd_kernel<1, kR>, tpb, 0) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_fwd[1], swb::fwd_kernel<3, kR>, tpb, 0) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_bwd[0], swb::bwd_kernel<1, kR>, tpb,
+    const int tf = 32 * kWarpsFwd, tb = 32 * kWarpsBwd;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_fwd[0], swb::fwd_kernel<1, kR>, tf, 0) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_fwd[1], swb::fwd_kernel<3, kR>, tf, 0) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_bwd[0], swb::bwd_kernel<1, kR, kWarpsBwd>, tb,
                                                       bwd_smem<1>()) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_bwd[1], swb::bwd_kernel<3, kR>, tpb,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_bwd[1], swb::bwd_kernel<3, kR, kWarpsBwd>, tb,
                                                       bwd_smem<3>()))
       return SWB_ERR_CUDA;
     d.ready = true;
@@ -104,7 +106,8 @@ int launch(const float* scores, const int* lengths, const long long* offsets, co
   if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   if (B == 0) return SWB_OK;
-  if (!scores || !map || !value || !g_open || !g_T || (NS == 3 && !g_ext)) return SWB_ERR_ARG;
+  if (!value || !g_open || !g_T || (NS == 3 && !g_ext)) return SWB_ERR_ARG;
+  if (map_elems > 0 && (!scores || !map)) return SWB_ERR_ARG;
   if (layout == 1 && (!offsets || !lengths)) return SWB_ERR_ARG;
   const Layout l = layout_for<NS>(B, L1m, L2m);
   if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
@@ -136,21 +139,23 @@ int launch(const float* scores, const int* lengths, const long long* offsets, co
   // buffers to the NaN sentinel, the map to 0 (cells outside lengths stay 0)
   if (cudaMemsetAsync(w, 0, l.off_part, st) != cudaSuccess) return SWB_ERR_CUDA;
   if (cudaMemsetAsync(w + l.off_sent, 0xff, l.sent_bytes, st) != cudaSuccess) return SWB_ERR_CUDA;
-  if (cudaMemsetAsync(map, 0, map_elems * sizeof(float), st) != cudaSuccess) return SWB_ERR_CUDA;
+  if (map_elems > 0 && cudaMemsetAsync(map, 0, map_elems * sizeof(float), st) != cudaSuccess)
+    return SWB_ERR_CUDA;
 
   const long long ntasks = (long long)B * l.nb;
   const int cta_cap_f = d->sms * (d->occ_fwd[NS == 3] > 0 ? d->occ_fwd[NS == 3] : 1);
   const int cta_cap_b = d->sms * (d->occ_bwd[NS == 3] > 0 ? d->occ_bwd[NS == 3] : 1);
-  long long need = (ntasks + kWarpsPerCta - 1) / kWarpsPerCta;
-  int grid_f = (int)(need < cta_cap_f ? need : cta_cap_f);
-  int grid_b = (int)(need < cta_cap_b ? need : cta_cap_b);
+  const long long need_f = (ntasks + kWarpsFwd - 1) / kWarpsFwd;
+  const long long need_b = (ntasks + kWarpsBwd - 1) / kWarpsBwd;
+  int grid_f = (int)(need_f < cta_cap_f ? need_f : cta_cap_f);
+  int grid_b = (int)(need_b < cta_cap_b ? need_b : cta_cap_b);
   if (opt && opt->max_ctas > 0) {
     if (grid_f > opt->max_ctas) grid_f = opt->max_ctas;
     if (grid_b > opt->max_ctas) grid_b = opt->max_ctas;
   }
-  swb::fwd_kernel<NS, kR><<<grid_f, 32 * kWarpsPerCta, 0, st>>>(a);
+  swb::fwd_kernel<NS, kR><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
-  swb::bwd_kernel<NS, kR><<<grid_b, 32 * kWarpsPerCta, bwd_smem<NS>(), st>>>(a);
+  swb::bwd_kernel<NS, kR, kWarpsBwd><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS>(), st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   return SWB_OK;
 }
@@ -208,5 +213,11 @@ const char* swb_error_string(int code) {
 }
 
 int swb_abi_version(void) { return SWB_ABI_VERSION; }
+
+int swb_mufu_probe(float* scratch, int blocks, int iters, void* stream) {
+  if (!scratch || blocks <= 0 || iters <= 0) return SWB_ERR_ARG;
+  swb::mufu_probe_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(scratch, iters);
+  return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+}
 
 }  // extern "C"

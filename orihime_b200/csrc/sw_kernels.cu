@@ -148,72 +148,118 @@ __device__ __forceinline__ void store_row(const Pair& pr, int i, int jl, const f
   }
 }
 
-// Number of values crossing a band edge forward (NS) and pushes crossing it
-// backward (NP), checkpoint fields per lane (CKF) and shared-memory fields per
-// lane per recomputed step (EF).
+// Values crossing a band edge forward (2*NS: hi and lo of each state), pushes
+// crossing it backward (NP), checkpoint floats per lane (CKF) and shared-memory
+// floats per lane per recomputed step (EF: alpha pairs + scaled scores).
 template <int NS> struct Shape;
 template <> struct Shape<3> { static constexpr int NP = 5; };
 template <> struct Shape<1> { static constexpr int NP = 2; };
 
 template <int NS, int R> struct Dims {
+  static constexpr int NE = 2 * NS;
   static constexpr int NP = Shape<NS>::NP;
-  static constexpr int CKF = NS * R + NS;
-  static constexpr int EF = NS * R + NS + R;
+  static constexpr int CKF = 2 * NS * R + 2 * NS;
+  static constexpr int EF = 2 * NS * R + R;
 };
+
+// checkpoint field indices
+template <int NS, int R> __device__ __forceinline__ int ck_h(int q, int c) { return q * R + c; }
+template <int NS, int R> __device__ __forceinline__ int ck_l(int q, int c) { return NS * R + q * R + c; }
+template <int NS, int R> __device__ __forceinline__ int ck_lh(int q) { return 2 * NS * R + q; }
+template <int NS, int R> __device__ __forceinline__ int ck_ll(int q) { return 2 * NS * R + NS + q; }
+// shared-memory entry field indices
+template <int NS, int R> __device__ __forceinline__ int en_h(int q, int c) { return q * R + c; }
+template <int NS, int R> __device__ __forceinline__ int en_l(int q, int c) { return NS * R + q * R + c; }
+template <int NS, int R> __device__ __forceinline__ int en_s(int c) { return 2 * NS * R + c; }
 
 // ---------------------------------------------------------------------------
 // forward cell
 // ---------------------------------------------------------------------------
 
-// One step of the forward wavefront for one lane: consumes the previous-row
-// values pv, the left values of this row lf (already received), the diag
-// values dg of column 0 (left lane, previous row) and the scaled scores s.
-// Writes the new row into pv when act.  Returns per-column new values in nv.
+// r + t as a pair when r is the large part: hi = r + t, lo = exact error
+// (Fast2Sum; exact whenever |r| >= |t|, and only ever inexact at the scale of
+// small values).
+__device__ __forceinline__ void fast2(float r, float t, float& h, float& l) {
+  h = r + t;
+  l = (r - h) + t;
+}
+
+// a + b as an exact pair (TwoSum).
+__device__ __forceinline__ void two_sum(float a, float b, float& h, float& l) {
+  h = a + b;
+  const float bb = h - a;
+  l = (a - (h - bb)) + (b - bb);
+}
+
+// One step of the forward wavefront for one lane.  Inputs: previous-row pairs
+// (ph, pl), left pairs of this row (lfh, lfl, already received), diag pairs of
+// column 0 (dgh0, dgl0: left lane, previous row) and the scaled scores s.
+// Writes the new row into (ph, pl) when act and returns it in (nh, nl).
 template <int NS, int R>
-__device__ __forceinline__ void fwd_cells(float (&pv)[NS][R], const float (&lf)[NS],
-                                          const float (&dg0)[NS], const float (&s)[R],
-                                          float g0, float g1, bool act, float (&nv)[NS][R]) {
-  float dg[NS], left[NS];
+__device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R],
+                                          const float (&lfh)[NS], const float (&lfl)[NS],
+                                          const float (&dgh0)[NS], const float (&dgl0)[NS],
+                                          const float (&s)[R], float g0, float g1, bool act,
+                                          float (&nh)[NS][R], float (&nl)[NS][R]) {
+  float dgh[NS], dgl[NS], lh[NS], ll[NS];
 #pragma unroll
-  for (int q = 0; q < NS; ++q) { dg[q] = dg0[q]; left[q] = lf[q]; }
+  for (int q = 0; q < NS; ++q) { dgh[q] = dgh0[q]; dgl[q] = dgl0[q]; lh[q] = lfh[q]; ll[q] = lfl[q]; }
 #pragma unroll
   for (int c = 0; c < R; ++c) {
     if constexpr (NS == 3) {
-      const float upM = pv[0][c], upI = pv[1][c], upD = pv[2][c];
+      const float uMh = ph[0][c], uMl = pl[0][c], uIh = ph[1][c], uIl = pl[1][c];
+      const float uDh = ph[2][c], uDl = pl[2][c];
       // M = s + LSE(M, I, D at diag, 0)
-      float mx = fmaxf(fmaxf(dg[0], dg[1]), fmaxf(dg[2], 0.f));
-      float sm = ex2(dg[0] - mx) + ex2(dg[1] - mx) + ex2(dg[2] - mx) + ex2(-mx);
-      float M = s[c] + (mx + lg2(sm));
+      const float r = fmaxf(fmaxf(dgh[0] + dgl[0], dgh[1] + dgl[1]),
+                            fmaxf(dgh[2] + dgl[2], 0.f));
+      const float sm = (ex2((dgh[0] - r) + dgl[0]) + ex2((dgh[1] - r) + dgl[1])) +
+                       (ex2((dgh[2] - r) + dgl[2]) + ex2(-r));
+      float Mh, Ml;
+      two_sum(r, s[c], Mh, Ml);
+      Ml += lg2(sm);
       // I = LSE(M up + go, I up + ge)
-      float ia = upM + g0, ib = upI + g1;
-      float im = fmaxf(ia, ib);
-      float I = im + lg2(1.f + ex2(fminf(ia, ib) - im));
+      const float ru = fmaxf((uMh + uMl) + g0, (uIh + uIl) + g1);
+      const float ia = ((uMh - ru) + g0) + uMl, ib = ((uIh - ru) + g1) + uIl;
+      const float im = fmaxf(ia, ib);
+      float Ih, Il;
+      fast2(ru, im + lg2(1.f + ex2(fminf(ia, ib) - im)), Ih, Il);
       // D = LSE(M left + go, D left + ge)
-      float da = left[0] + g0, db = left[2] + g1;
-      float dm = fmaxf(da, db);
-      float D = dm + lg2(1.f + ex2(fminf(da, db) - dm));
-      nv[0][c] = M; nv[1][c] = I; nv[2][c] = D;
-      dg[0] = upM; dg[1] = upI; dg[2] = upD;
-      left[0] = M; left[1] = I; left[2] = D;
+      const float rl = fmaxf((lh[0] + ll[0]) + g0, (lh[2] + ll[2]) + g1);
+      const float da = ((lh[0] - rl) + g0) + ll[0], db = ((lh[2] - rl) + g1) + ll[2];
+      const float dm = fmaxf(da, db);
+      float Dh, Dl;
+      fast2(rl, dm + lg2(1.f + ex2(fminf(da, db) - dm)), Dh, Dl);
+      nh[0][c] = Mh; nl[0][c] = Ml; nh[1][c] = Ih; nl[1][c] = Il; nh[2][c] = Dh; nl[2][c] = Dl;
+      dgh[0] = uMh; dgl[0] = uMl; dgh[1] = uIh; dgl[1] = uIl; dgh[2] = uDh; dgl[2] = uDl;
+      lh[0] = Mh; ll[0] = Ml; lh[1] = Ih; ll[1] = Il; lh[2] = Dh; ll[2] = Dl;
     } else {
-      const float up = pv[0][c];
+      const float uh = ph[0][c], ul = pl[0][c];
       // A = LSE(diag + s, up + g, left + g, s)
-      float va = dg[0] + s[c], vu = up + g0, vl = left[0] + g0, vs = s[c];
-      float mx = fmaxf(fmaxf(va, vu), fmaxf(vl, vs));
-      float sm = ex2(va - mx) + ex2(vu - mx) + ex2(vl - mx) + ex2(vs - mx);
-      float A = mx + lg2(sm);
-      nv[0][c] = A;
-      dg[0] = up;
-      left[0] = A;
+      const float r = fmaxf(fmaxf((dgh[0] + dgl[0]) + s[c], (uh + ul) + g0),
+                            fmaxf((lh[0] + ll[0]) + g0, s[c]));
+      const float va = ((dgh[0] - r) + s[c]) + dgl[0];
+      const float vu = ((uh - r) + g0) + ul;
+      const float vl = ((lh[0] - r) + g0) + ll[0];
+      const float vs = s[c] - r;
+      const float sm = (ex2(va) + ex2(vu)) + (ex2(vl) + ex2(vs));
+      float Ah, Al;
+      fast2(r, lg2(sm), Ah, Al);
+      nh[0][c] = Ah; nl[0][c] = Al;
+      dgh[0] = uh; dgl[0] = ul;
+      lh[0] = Ah; ll[0] = Al;
     }
   }
   if (act) {
 #pragma unroll
     for (int q = 0; q < NS; ++q)
 #pragma unroll
-      for (int c = 0; c < R; ++c) pv[q][c] = nv[q][c];
+      for (int c = 0; c < R; ++c) { ph[q][c] = nh[q][c]; pl[q][c] = nl[q][c]; }
   }
 }
+
+// Steps of a band, padded to whole checkpoint chunks (the padding steps find
+// every lane past the last row and do nothing).
+__device__ __forceinline__ int band_chunks(int L1) { return (L1 + 31 + C_STEPS - 1) / C_STEPS; }
 
 // ---------------------------------------------------------------------------
 // forward band task
@@ -222,6 +268,7 @@ __device__ __forceinline__ void fwd_cells(float (&pv)[NS][R], const float (&lf)[
 template <int NS, int R>
 __device__ void fwd_band(const Args& a, int p, int band, int lane, uint64_t deadline) {
   using D = Dims<NS, R>;
+  constexpr int NE = D::NE;
   const Pair pr = pair_of(a, p);
   const int L1 = pr.L1, L2 = pr.L2;
   const int slot = p * a.nb + band;
@@ -234,111 +281,135 @@ __device__ void fwd_band(const Args& a, int p, int band, int lane, uint64_t dead
   const int jl = col0 + lane * R;
   const float k = a.k, g0 = a.go * k, g1 = a.ge * k;
   const size_t Lm = (size_t)a.Lmax1;
-  float* eout = a.edge + (size_t)slot * NS * Lm;
-  const float* ein = (band > 0) ? a.edge + (size_t)(slot - 1) * NS * Lm : nullptr;
-  if (a.fault_inject && band > 0) ein = nullptr;
+  float* eout = a.edge + (size_t)slot * NE * Lm;
+  const float* ein = (band > 0) ? a.edge + (size_t)(slot - 1) * NE * Lm : nullptr;
+  const bool fault = a.fault_inject && band > 0;
+  if (fault) ein = nullptr;
   float* ck = a.ckpt + (size_t)slot * a.nchunks * D::CKF * 32;
-  const int nsteps = L1 + 31;
+  const int nch = band_chunks(L1);
 
-  float pv[NS][R], lv[NS];
+  float ph[NS][R], pl[NS][R], lh[NS], ll[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
-    lv[q] = NEG;
+    lh[q] = NEG; ll[q] = 0.f;
 #pragma unroll
-    for (int c = 0; c < R; ++c) pv[q][c] = NEG;
+    for (int c = 0; c < R; ++c) { ph[q][c] = NEG; pl[q][c] = 0.f; }
   }
   float ref = 0.f;
   KSum acc;
   if (band == 0 && lane == 0) acc.s = 1.f;  // the M[0,0] = 0 origin term
 
-  float sb[PF][R], eb[PF][NS];
+  // Lane u < C holds the left band's edge values that lane 0 needs at step u
+  // of a chunk, loaded one chunk ahead; lane 0 takes them by shuffle.
+  float eb[NE], ebn[NE];
+  auto load_edge = [&](int kc, float (&dst)[NE]) {
+    const int i = kc * C_STEPS + lane + 1;  // lane 0's row at step kc*C + lane
+    const bool ok = ein && lane < C_STEPS && i <= L1;
+#pragma unroll
+    for (int f = 0; f < NE; ++f) dst[f] = ok ? ld_poll(ein + f * Lm + (i - 1)) : 0.f;
+  };
+  load_edge(0, eb);
+  float sb[PF][R];  // per-lane score ring, PF steps ahead
 #pragma unroll
   for (int u = 0; u < PF; ++u) {
     const int i = u - lane + 1;
     load_row<R>(pr, i, jl, i >= 1 && i <= L1, sb[u]);
-#pragma unroll
-    for (int q = 0; q < NS; ++q)
-      eb[u][q] = (lane == 0 && ein && i >= 1 && i <= L1) ? ld_poll(ein + q * Lm + (i - 1)) : NEG;
   }
 
-  for (int tb = 0; tb < nsteps; tb += PF) {
+  for (int kc = 0; kc < nch; ++kc) {
+    {  // checkpoint: state before step kc*C
+      float* dst = ck + (size_t)kc * D::CKF * 32 + lane;
 #pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      const int t = tb + u;
-      if (t < nsteps) {
-        if (u == 0 && (tb % C_STEPS) == 0) {
-          float* dst = ck + (size_t)(tb / C_STEPS) * D::CKF * 32 + lane;
+      for (int q = 0; q < NS; ++q) {
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+          dst[ck_h<NS, R>(q, c) * 32] = ph[q][c];
+          dst[ck_l<NS, R>(q, c) * 32] = pl[q][c];
+        }
+        dst[ck_lh<NS, R>(q) * 32] = lh[q];
+        dst[ck_ll<NS, R>(q) * 32] = ll[q];
+      }
+    }
+    if (kc + 1 < nch) load_edge(kc + 1, ebn);
+#pragma unroll
+    for (int cu = 0; cu < C_STEPS; ++cu) {
+      const int u = cu % PF;
+      const int t = kc * C_STEPS + cu;
+      const int i = t - lane + 1;
+      const bool act = (i >= 1) && (i <= L1);
+      float xh[NS], xl[NS], ev[NE];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        xh[q] = __shfl_up_sync(FULL, ph[q][R - 1], 1);
+        xl[q] = __shfl_up_sync(FULL, pl[q][R - 1], 1);
+      }
+#pragma unroll
+      for (int f = 0; f < NE; ++f) ev[f] = __shfl_sync(FULL, eb[f], cu);
+      if (lane == 0) {
+        if (fault && act) {
+          float v = poll_value(a.never_written, ld_poll(a.never_written), deadline, a.status, NEG);
+#pragma unroll
+          for (int q = 0; q < NS; ++q) { xh[q] = v; xl[q] = 0.f; }
+        } else if (ein && act) {
+#pragma unroll
+          for (int f = 0; f < NE; ++f)
+            if (is_sentinel(ev[f]))
+              ev[f] = poll_value(ein + f * Lm + (i - 1), ld_poll(ein + f * Lm + (i - 1)), deadline,
+                                 a.status, f < NS ? NEG : 0.f);
+#pragma unroll
+          for (int q = 0; q < NS; ++q) { xh[q] = ev[q]; xl[q] = ev[NS + q]; }
+        } else {
+#pragma unroll
+          for (int q = 0; q < NS; ++q) { xh[q] = NEG; xl[q] = 0.f; }
+        }
+      }
+      float dgh[NS], dgl[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        dgh[q] = lh[q]; dgl[q] = ll[q];
+        lh[q] = xh[q]; ll[q] = xl[q];
+      }
+      float s[R];
+#pragma unroll
+      for (int c = 0; c < R; ++c) s[c] = sb[u][c] * k;
+      {
+        const int ip = i + PF;
+        load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
+      }
+      float nh[NS][R], nl[NS][R];
+      fwd_cells<NS, R>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, act, nh, nl);
+      if (act) {
+        // partition: lazily rescaled Kahan sum of ex2(x - ref)
+        float mx = NEG;
+#pragma unroll
+        for (int c = 0; c < R; ++c)
+          if (jl + c < L2)
+#pragma unroll
+            for (int q = 0; q < NS; ++q) mx = fmaxf(mx, nh[q][c] + nl[q][c]);
+        if (mx > ref + 64.f) {
+          float f = ex2(ref - mx);
+          acc.s *= f;
+          acc.c *= f;
+          ref = mx;
+        }
+        float tsum = 0.f;
+#pragma unroll
+        for (int c = 0; c < R; ++c)
+          if (jl + c < L2)
+#pragma unroll
+            for (int q = 0; q < NS; ++q) tsum += ex2((nh[q][c] - ref) + nl[q][c]);
+        acc.add(tsum);
+        if (lane == 31) {
 #pragma unroll
           for (int q = 0; q < NS; ++q) {
-#pragma unroll
-            for (int c = 0; c < R; ++c) dst[(q * R + c) * 32] = pv[q][c];
-            dst[(NS * R + q) * 32] = lv[q];
-          }
-        }
-        const int i = t - lane + 1;
-        const bool act = (i >= 1) && (i <= L1);
-        float x[NS];
-#pragma unroll
-        for (int q = 0; q < NS; ++q) x[q] = __shfl_up_sync(FULL, pv[q][R - 1], 1);
-        if (lane == 0) {
-          if (a.fault_inject && band > 0 && act) {
-            float v = poll_value(a.never_written, ld_poll(a.never_written), deadline, a.status,
-                                 NEG);
-#pragma unroll
-            for (int q = 0; q < NS; ++q) x[q] = v;
-          } else if (ein && act) {
-#pragma unroll
-            for (int q = 0; q < NS; ++q)
-              x[q] = poll_value(ein + q * Lm + (i - 1), eb[u][q], deadline, a.status, NEG);
-          } else {
-#pragma unroll
-            for (int q = 0; q < NS; ++q) x[q] = NEG;
-          }
-        }
-        float dg[NS];
-#pragma unroll
-        for (int q = 0; q < NS; ++q) { dg[q] = lv[q]; lv[q] = x[q]; }
-        float s[R];
-#pragma unroll
-        for (int c = 0; c < R; ++c) s[c] = sb[u][c] * k;
-        {  // prefetch step t + PF
-          const int ip = i + PF;
-          load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
-#pragma unroll
-          for (int q = 0; q < NS; ++q)
-            eb[u][q] = (lane == 0 && ein && ip >= 1 && ip <= L1) ? ld_poll(ein + q * Lm + (ip - 1))
-                                                                  : NEG;
-        }
-        float nv[NS][R];
-        fwd_cells<NS, R>(pv, lv, dg, s, g0, g1, act, nv);
-        if (act) {
-          // partition: lazily rescaled Kahan sum of ex2(x - ref)
-          float mx = NEG;
-#pragma unroll
-          for (int c = 0; c < R; ++c)
-            if (jl + c < L2)
-#pragma unroll
-              for (int q = 0; q < NS; ++q) mx = fmaxf(mx, nv[q][c]);
-          if (mx > ref + 64.f) {
-            float f = ex2(ref - mx);
-            acc.s *= f;
-            acc.c *= f;
-            ref = mx;
-          }
-          float tsum = 0.f;
-#pragma unroll
-          for (int c = 0; c < R; ++c)
-            if (jl + c < L2)
-#pragma unroll
-              for (int q = 0; q < NS; ++q) tsum += ex2(nv[q][c] - ref);
-          acc.add(tsum);
-          if (lane == 31) {
-#pragma unroll
-            for (int q = 0; q < NS; ++q) eout[q * Lm + (i - 1)] = pv[q][R - 1];
+            eout[q * Lm + (i - 1)] = ph[q][R - 1];
+            eout[(NS + q) * Lm + (i - 1)] = pl[q][R - 1];
           }
         }
       }
     }
+#pragma unroll
+    for (int f = 0; f < NE; ++f) eb[f] = ebn[f];
   }
   // warp-combine (ref, sum) pairs
   float s_ = acc.s;
@@ -373,8 +444,9 @@ __global__ void __launch_bounds__(128) fwd_kernel(Args a) {
 // adjoint band task
 // ---------------------------------------------------------------------------
 
-// Combine the forward partials of pair p into the scaled log-partition S'.
-__device__ __forceinline__ float pair_logz(const Args& a, int p, int lane) {
+// Combine the forward partials of pair p into the scaled log-partition
+// S' = Sh + Sl.
+__device__ __forceinline__ void pair_logz(const Args& a, int p, int lane, float& Sh, float& Sl) {
   float ref = NEG, s = 0.f;
   for (int b = lane; b < a.nb; b += 32) {
     const float* q = a.part + 2 * ((size_t)p * a.nb + b);
@@ -393,14 +465,15 @@ __device__ __forceinline__ float pair_logz(const Args& a, int p, int lane) {
     s = s * ex2(ref - m) + s2 * ex2(r2 - m);
     ref = m;
   }
-  return ref + lg2(s);
+  Sh = ref;
+  Sl = lg2(s);
 }
 
 // Last band task of a pair to finish folds the per-band gradient partials (in
 // band order, so the result is deterministic) into the outputs.
 template <int NS>
-__device__ void finish_pair(const Args& a, int p, int slot, int lane, float S2, float g0sum,
-                            float g1sum, float pssum) {
+__device__ void finish_pair(const Args& a, int p, int slot, int lane, float Sh, float Sl,
+                            float g0sum, float g1sum, float pssum) {
   if (lane == 0) {
     float* gp = a.gpart + 4 * (size_t)slot;
     gp[0] = g0sum; gp[1] = g1sum; gp[2] = pssum; gp[3] = 0.f;
@@ -416,7 +489,7 @@ __device__ void finish_pair(const Args& a, int p, int slot, int lane, float S2, 
         ps += ld_poll(q + 2);
       }
       const float inv_k = 1.f / a.k;          // = T * ln 2
-      const float S = S2 * inv_k;
+      const float S = (Sh + Sl) * inv_k;
       const float match = ps * inv_k;
       a.value[p] = S;
       if (NS == 3) {
@@ -432,31 +505,76 @@ __device__ void finish_pair(const Args& a, int p, int slot, int lane, float S2, 
   }
 }
 
+// Weight of a predecessor: ex2(((pred_h - cell_h) + edge) + (pred_l - cell_l)),
+// guarded against overflow for cells that do not exist (their beta is 0).
+__device__ __forceinline__ float wgt(float ph_, float pl_, float xh, float xl, float e) {
+  return ex2(fminf(((ph_ - xh) + e) + (pl_ - xl), 64.f));
+}
+
 template <int NS, int R>
-__device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, uint64_t deadline) {
+__device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, float* ea,
+                         uint64_t deadline) {
   using D = Dims<NS, R>;
-  constexpr int NP = D::NP, EF = D::EF, CKF = D::CKF;
+  constexpr int NP = D::NP, EF = D::EF, CKF = D::CKF, NE = D::NE;
   const Pair pr = pair_of(a, p);
   const int L1 = pr.L1, L2 = pr.L2;
   const int slot = p * a.nb + band;
   const int col0 = band * 32 * R;
-  const float S2 = pair_logz(a, p, lane);
+  float Sh, Sl;
+  pair_logz(a, p, lane, Sh, Sl);
   if (!(L1 > 0 && col0 < L2)) {
-    finish_pair<NS>(a, p, slot, lane, S2, 0.f, 0.f, 0.f);
+    finish_pair<NS>(a, p, slot, lane, Sh, Sl, 0.f, 0.f, 0.f);
     return;
   }
   const int jl = col0 + lane * R;
   const float k = a.k, g0 = a.go * k, g1 = a.ge * k;
   const size_t Lm = (size_t)a.Lmax1;
-  const float* ein = (band > 0) ? a.edge + (size_t)(slot - 1) * NS * Lm : nullptr;
+  const float* ein = (band > 0) ? a.edge + (size_t)(slot - 1) * NE * Lm : nullptr;
   float* pout = (band > 0) ? a.bpush + (size_t)slot * NP * (Lm + 1) : nullptr;
   const bool right_live = (col0 + 32 * R) < L2 && (band + 1) < a.nb;
   const float* pin = right_live ? a.bpush + (size_t)(slot + 1) * NP * (Lm + 1) : nullptr;
   const float* ck = a.ckpt + (size_t)slot * a.nchunks * CKF * 32;
-  const int nsteps = L1 + 31;
-  const int nch = (nsteps + C_STEPS - 1) / C_STEPS;
+  const int nch = band_chunks(L1);
+  const int left_lane = (lane + 31) & 31;
 
-  // adjoint state
+  // ---- chunk-ahead prefetch state ----
+  float ckr[CKF];           // checkpoint of the next chunk to recompute
+  float ebr[NE];            // lane u < C: left-band edge pair of lane 0's row at recompute step u
+  float pbc[NP], pbn[NP];   // lane u < C: right-band pushes lane 31 needs at adjoint step u
+  float sb[PF][R];          // per-lane scores of the first PF recompute steps
+  auto load_ck = [&](int kc) {
+    const float* src = ck + (size_t)kc * CKF * 32 + lane;
+#pragma unroll
+    for (int f = 0; f < CKF; ++f) ckr[f] = src[f * 32];
+  };
+  auto load_eb = [&](int kc) {
+    const int i = kc * C_STEPS + lane + 1;
+    const bool ok = ein && lane < C_STEPS && i <= L1;
+#pragma unroll
+    for (int f = 0; f < NE; ++f) ebr[f] = ok ? ein[f * Lm + (i - 1)] : (f < NS ? NEG : 0.f);
+  };
+  auto load_pb = [&](int kc, float (&dst)[NP]) {
+    const int i = kc * C_STEPS + C_STEPS - 1 - lane - 30;  // lane 31's row at step end-1-lane
+    const bool ok = pin && lane < C_STEPS && i >= 1 && i <= L1;
+#pragma unroll
+    for (int f = 0; f < NP; ++f) {
+      const bool left = (NS == 3) ? (f < 2) : (f < 1);
+      dst[f] = (ok && (left || i < L1)) ? ld_poll(pin + f * (Lm + 1) + i) : 0.f;
+    }
+  };
+  auto load_sb = [&](int kc) {
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int i = kc * C_STEPS + u - lane + 1;
+      load_row<R>(pr, i, jl, i >= 1 && i <= L1, sb[u]);
+    }
+  };
+  load_ck(nch - 1);
+  load_eb(nch - 1);
+  load_sb(nch - 1);
+  load_pb(nch - 1, pbc);
+
+  // ---- adjoint state ----
   float ac[NS][R], nx[NS][R];
 #pragma unroll
   for (int q = 0; q < NS; ++q)
@@ -471,108 +589,110 @@ __device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, ui
 
   for (int kc = nch - 1; kc >= 0; --kc) {
     const int t0 = kc * C_STEPS;
-    const int t1 = min(t0 + C_STEPS, nsteps);
-    // ---- restore checkpoint and recompute the chunk into shared memory ----
-    float pv[NS][R], lv[NS];
-    {
-      const float* src = ck + (size_t)kc * CKF * 32 + lane;
+    // ---- restore the checkpoint and recompute the chunk into shared memory ----
+    // entry e (0..C) holds every lane's row pairs after step t0+e-1 and its
+    // scaled scores of that step; ea[e] holds lane 0's left-band pairs.
+    float ph[NS][R], pl[NS][R], lh[NS], ll[NS];
+    float d0h[NS], d0l[NS];   // diag of column 0 at the chunk's first step
 #pragma unroll
-      for (int q = 0; q < NS; ++q) {
+    for (int q = 0; q < NS; ++q) {
 #pragma unroll
-        for (int c = 0; c < R; ++c) pv[q][c] = src[(q * R + c) * 32];
-        lv[q] = src[(NS * R + q) * 32];
+      for (int c = 0; c < R; ++c) {
+        ph[q][c] = ckr[ck_h<NS, R>(q, c)];
+        pl[q][c] = ckr[ck_l<NS, R>(q, c)];
+        sm[en_h<NS, R>(q, c) * 32 + lane] = ph[q][c];
+        sm[en_l<NS, R>(q, c) * 32 + lane] = pl[q][c];
       }
-      float* e0 = sm + lane;
-#pragma unroll
-      for (int q = 0; q < NS; ++q) {
-#pragma unroll
-        for (int c = 0; c < R; ++c) e0[(q * R + c) * 32] = pv[q][c];
-        e0[(NS * R + q) * 32] = lv[q];
-      }
-    }
-    float sb[PF][R];
-#pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      const int i = t0 + u - lane + 1;
-      load_row<R>(pr, i, jl, (t0 + u < t1) && i >= 1 && i <= L1, sb[u]);
+      lh[q] = ckr[ck_lh<NS, R>(q)];
+      ll[q] = ckr[ck_ll<NS, R>(q)];
+      d0h[q] = lh[q];
+      d0l[q] = ll[q];
+      if (lane == 0) { ea[q] = lh[q]; ea[NS + q] = ll[q]; }
     }
 #pragma unroll
-    for (int u0 = 0; u0 < C_STEPS; u0 += PF) {
+    for (int cu = 0; cu < C_STEPS; ++cu) {
+      const int u = cu % PF;
+      const int t = t0 + cu;
+      const int i = t - lane + 1;
+      const bool act = (i >= 1) && (i <= L1);
+      float xh[NS], xl[NS];
 #pragma unroll
-      for (int u = 0; u < PF; ++u) {
-        const int t = t0 + u0 + u;
-        if (t < t1) {
-          const int i = t - lane + 1;
-          const bool act = (i >= 1) && (i <= L1);
-          float x[NS];
-#pragma unroll
-          for (int q = 0; q < NS; ++q) x[q] = __shfl_up_sync(FULL, pv[q][R - 1], 1);
-          if (lane == 0) {
-#pragma unroll
-            for (int q = 0; q < NS; ++q) x[q] = (ein && act) ? ein[q * Lm + (i - 1)] : NEG;
-          }
-          float dg[NS];
-#pragma unroll
-          for (int q = 0; q < NS; ++q) { dg[q] = lv[q]; lv[q] = x[q]; }
-          float s[R];
-#pragma unroll
-          for (int c = 0; c < R; ++c) s[c] = sb[u][c] * k;
-          {
-            const int tp = t + PF;
-            const int ip = tp - lane + 1;
-            if (u0 + u + PF < C_STEPS) load_row<R>(pr, ip, jl, tp < t1 && ip >= 1 && ip <= L1, sb[u]);
-          }
-          float nv[NS][R];
-          fwd_cells<NS, R>(pv, lv, dg, s, g0, g1, act, nv);
-          float* e = sm + (size_t)(t - t0 + 1) * EF * 32 + lane;
-#pragma unroll
-          for (int q = 0; q < NS; ++q) {
-#pragma unroll
-            for (int c = 0; c < R; ++c) e[(q * R + c) * 32] = pv[q][c];
-            e[(NS * R + q) * 32] = lv[q];
-          }
-#pragma unroll
-          for (int c = 0; c < R; ++c) e[(NS * R + NS + c) * 32] = s[c];
+      for (int q = 0; q < NS; ++q) {
+        xh[q] = __shfl_up_sync(FULL, ph[q][R - 1], 1);
+        xl[q] = __shfl_up_sync(FULL, pl[q][R - 1], 1);
+        const float evh = __shfl_sync(FULL, ebr[q], cu);
+        const float evl = __shfl_sync(FULL, ebr[NS + q], cu);
+        if (lane == 0) {
+          xh[q] = act ? evh : NEG;
+          xl[q] = act ? evl : 0.f;
+          ea[(cu + 1) * NE + q] = xh[q];
+          ea[(cu + 1) * NE + NS + q] = xl[q];
         }
       }
+      float dgh[NS], dgl[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        dgh[q] = lh[q]; dgl[q] = ll[q];
+        lh[q] = xh[q]; ll[q] = xl[q];
+      }
+      float s[R];
+#pragma unroll
+      for (int c = 0; c < R; ++c) s[c] = sb[u][c] * k;
+      if (cu + PF < C_STEPS) {
+        const int ip = i + PF;
+        load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
+      }
+      float nh[NS][R], nl[NS][R];
+      fwd_cells<NS, R>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, act, nh, nl);
+      float* e = sm + (size_t)(cu + 1) * EF * 32 + lane;
+#pragma unroll
+      for (int q = 0; q < NS; ++q)
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+          e[en_h<NS, R>(q, c) * 32] = ph[q][c];
+          e[en_l<NS, R>(q, c) * 32] = pl[q][c];
+        }
+#pragma unroll
+      for (int c = 0; c < R; ++c) e[en_s<NS, R>(c) * 32] = s[c];
+    }
+    if (kc > 0) {  // prefetch the next chunk's inputs while the adjoint runs
+      load_ck(kc - 1);
+      load_eb(kc - 1);
+      load_sb(kc - 1);
+      load_pb(kc - 1, pbn);
     }
     __syncwarp();
     // ---- adjoint over the chunk, last step first ----
-    for (int t = t1 - 1; t >= t0; --t) {
+#pragma unroll 1
+    for (int cu = 0; cu < C_STEPS; ++cu) {
+      const int ent = C_STEPS - cu;            // entry of row i (this step)
+      const int t = t0 + ent - 1;
       const int i = t - lane + 1;
       const bool act = (i >= 1) && (i <= L1);
-      const float* E = sm + (size_t)(t - t0 + 1) * EF * 32 + lane;   // row i
-      const float* P = sm + (size_t)(t - t0) * EF * 32 + lane;       // row i-1
-      float r[NP];
+      const float* E = sm + (size_t)ent * EF * 32;        // row i
+      const float* P = sm + (size_t)(ent - 1) * EF * 32;  // row i-1
+      float r[NP], pw[NP];
 #pragma unroll
-      for (int q = 0; q < NP; ++q) r[q] = __shfl_down_sync(FULL, outp[q], 1);
+      for (int q = 0; q < NP; ++q) {
+        r[q] = __shfl_down_sync(FULL, outp[q], 1);
+        pw[q] = __shfl_sync(FULL, pbc[q], cu);
+      }
       // pushes arriving at column R-1 of row i: left pushes (NS==3: M,D; NS==1: A)
       // and diag pushes (NS==3: M,I,D; NS==1: A)
       float inL[2], inD[NS];
       if (lane == 31) {
-        if (pin && act) {
-          if constexpr (NS == 3) {
-            // left pushes for row i come from the right band's row i; diag
-            // pushes into row i from its row i+1, which exists only below L1
-            inL[0] = poll_value(pin + 0 * (Lm + 1) + i, ld_poll(pin + 0 * (Lm + 1) + i), deadline, a.status, 0.f);
-            inL[1] = poll_value(pin + 1 * (Lm + 1) + i, ld_poll(pin + 1 * (Lm + 1) + i), deadline, a.status, 0.f);
 #pragma unroll
-            for (int q = 0; q < 3; ++q)
-              inD[q] = (i < L1) ? poll_value(pin + (2 + q) * (Lm + 1) + i,
-                                             ld_poll(pin + (2 + q) * (Lm + 1) + i), deadline,
-                                             a.status, 0.f)
-                                : 0.f;
-          } else {
-            inL[0] = poll_value(pin + i, ld_poll(pin + i), deadline, a.status, 0.f);
-            inL[1] = 0.f;
-            inD[0] = (i < L1) ? poll_value(pin + (Lm + 1) + i, ld_poll(pin + (Lm + 1) + i), deadline,
-                                           a.status, 0.f)
-                              : 0.f;
-          }
+        for (int q = 0; q < NP; ++q)
+          if (is_sentinel(pw[q]))
+            pw[q] = poll_value(pin + q * (Lm + 1) + i, ld_poll(pin + q * (Lm + 1) + i), deadline,
+                               a.status, 0.f);
+        if constexpr (NS == 3) {
+          inL[0] = pw[0]; inL[1] = pw[1];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) inD[q] = pw[2 + q];
         } else {
-          inL[0] = inL[1] = 0.f;
-#pragma unroll
-          for (int q = 0; q < NS; ++q) inD[q] = 0.f;
+          inL[0] = pw[0]; inL[1] = 0.f;
+          inD[0] = pw[1];
         }
       } else {
         if constexpr (NS == 3) {
@@ -591,6 +711,28 @@ __device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, ui
       } else {
         ac[0][R - 1] += inL[0] + inD[0];
       }
+      // left neighbour of column 0: the left lane's last column at row i
+      // (entry ent-1) and row i-1 (entry ent-2); lane 0 reads the band edge.
+      float lnh[NS], lnl[NS], dnh[NS], dnl[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        if (lane == 0) {
+          lnh[q] = ea[ent * NE + q];
+          lnl[q] = ea[ent * NE + NS + q];
+          dnh[q] = ea[(ent - 1) * NE + q];
+          dnl[q] = ea[(ent - 1) * NE + NS + q];
+        } else {
+          lnh[q] = P[en_h<NS, R>(q, R - 1) * 32 + left_lane];
+          lnl[q] = P[en_l<NS, R>(q, R - 1) * 32 + left_lane];
+          if (ent >= 2) {
+            dnh[q] = P[(-EF + en_h<NS, R>(q, R - 1)) * 32 + left_lane];
+            dnl[q] = P[(-EF + en_l<NS, R>(q, R - 1)) * 32 + left_lane];
+          } else {
+            dnh[q] = d0h[q];
+            dnl[q] = d0l[q];
+          }
+        }
+      }
 #pragma unroll
       for (int q = 0; q < NP; ++q) outp[q] = 0.f;
       float pm[R];
@@ -599,29 +741,34 @@ __device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, ui
         const bool live = act && (jl + c < L2);
         const bool has_up = i > 1;
         const bool has_left = (jl + c) > 0;
-        const float sp = E[(NS * R + NS + c) * 32];
+        const float sp = E[en_s<NS, R>(c) * 32 + lane];
         if constexpr (NS == 3) {
-          const float M = E[(0 * R + c) * 32], I = E[(1 * R + c) * 32], Dv = E[(2 * R + c) * 32];
-          const float uM = P[(0 * R + c) * 32], uI = P[(1 * R + c) * 32];
-          float dM, dI, dD, lM, lD;
+          const float Mh = E[en_h<NS, R>(0, c) * 32 + lane], Ml = E[en_l<NS, R>(0, c) * 32 + lane];
+          const float Ih = E[en_h<NS, R>(1, c) * 32 + lane], Il = E[en_l<NS, R>(1, c) * 32 + lane];
+          const float Dh = E[en_h<NS, R>(2, c) * 32 + lane], Dl = E[en_l<NS, R>(2, c) * 32 + lane];
+          const float uMh = P[en_h<NS, R>(0, c) * 32 + lane], uMl = P[en_l<NS, R>(0, c) * 32 + lane];
+          const float uIh = P[en_h<NS, R>(1, c) * 32 + lane], uIl = P[en_l<NS, R>(1, c) * 32 + lane];
+          float dMh, dMl, dIh, dIl, dDh, dDl, lMh, lMl, lDh, lDl;
           if (c > 0) {
-            dM = P[(0 * R + c - 1) * 32]; dI = P[(1 * R + c - 1) * 32]; dD = P[(2 * R + c - 1) * 32];
-            lM = E[(0 * R + c - 1) * 32]; lD = E[(2 * R + c - 1) * 32];
+            dMh = P[en_h<NS, R>(0, c - 1) * 32 + lane]; dMl = P[en_l<NS, R>(0, c - 1) * 32 + lane];
+            dIh = P[en_h<NS, R>(1, c - 1) * 32 + lane]; dIl = P[en_l<NS, R>(1, c - 1) * 32 + lane];
+            dDh = P[en_h<NS, R>(2, c - 1) * 32 + lane]; dDl = P[en_l<NS, R>(2, c - 1) * 32 + lane];
+            lMh = E[en_h<NS, R>(0, c - 1) * 32 + lane]; lMl = E[en_l<NS, R>(0, c - 1) * 32 + lane];
+            lDh = E[en_h<NS, R>(2, c - 1) * 32 + lane]; lDl = E[en_l<NS, R>(2, c - 1) * 32 + lane];
           } else {
-            dM = P[(3 * R + 0) * 32]; dI = P[(3 * R + 1) * 32]; dD = P[(3 * R + 2) * 32];
-            lM = E[(3 * R + 0) * 32]; lD = E[(3 * R + 2) * 32];
+            dMh = dnh[0]; dMl = dnl[0]; dIh = dnh[1]; dIl = dnl[1]; dDh = dnh[2]; dDl = dnl[2];
+            lMh = lnh[0]; lMl = lnl[0]; lDh = lnh[2]; lDl = lnl[2];
           }
-          const float bM = live ? ex2(fminf(M - S2, 0.f)) + ac[0][c] : 0.f;
-          const float bI = live ? ex2(fminf(I - S2, 0.f)) + ac[1][c] : 0.f;
-          const float bD = live ? ex2(fminf(Dv - S2, 0.f)) + ac[2][c] : 0.f;
-          const float lse = M - sp;
-          const float wMM = ex2(fminf(dM - lse, 0.f));
-          const float wMI = ex2(fminf(dI - lse, 0.f));
-          const float wMD = ex2(fminf(dD - lse, 0.f));
-          const float wIM = has_up ? ex2(fminf(uM + g0 - I, 0.f)) : 0.f;
-          const float wII = has_up ? ex2(fminf(uI + g1 - I, 0.f)) : 0.f;
-          const float wDM = has_left ? ex2(fminf(lM + g0 - Dv, 0.f)) : 0.f;
-          const float wDD = has_left ? ex2(fminf(lD + g1 - Dv, 0.f)) : 0.f;
+          const float bM = live ? ex2(fminf((Mh - Sh) + (Ml - Sl), 0.f)) + ac[0][c] : 0.f;
+          const float bI = live ? ex2(fminf((Ih - Sh) + (Il - Sl), 0.f)) + ac[1][c] : 0.f;
+          const float bD = live ? ex2(fminf((Dh - Sh) + (Dl - Sl), 0.f)) + ac[2][c] : 0.f;
+          const float wMM = wgt(dMh, dMl, Mh, Ml, sp);
+          const float wMI = wgt(dIh, dIl, Mh, Ml, sp);
+          const float wMD = wgt(dDh, dDl, Mh, Ml, sp);
+          const float wIM = has_up ? wgt(uMh, uMl, Ih, Il, g0) : 0.f;
+          const float wII = has_up ? wgt(uIh, uIl, Ih, Il, g1) : 0.f;
+          const float wDM = has_left ? wgt(lMh, lMl, Dh, Dl, g0) : 0.f;
+          const float wDD = has_left ? wgt(lDh, lDl, Dh, Dl, g1) : 0.f;
           pm[c] = bM;
           const float pIM = bI * wIM, pII = bI * wII, pDM = bD * wDM, pDD = bD * wDD;
           gA.add(pIM + pDM);
@@ -637,15 +784,20 @@ __device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, ui
             outp[0] = pDM; outp[1] = pDD; outp[2] = qM; outp[3] = qI; outp[4] = qD;
           }
         } else {
-          const float A = E[c * 32];
-          const float uA = P[c * 32];
-          const float dA = (c > 0) ? P[(c - 1) * 32] : P[R * 32];
-          const float lA = (c > 0) ? E[(c - 1) * 32] : E[R * 32];
-          const float b = live ? ex2(fminf(A - S2, 0.f)) + ac[0][c] : 0.f;
-          const float wA = ex2(fminf(dA + sp - A, 0.f));
-          const float wS = ex2(fminf(sp - A, 0.f));
-          const float wU = has_up ? ex2(fminf(uA + g0 - A, 0.f)) : 0.f;
-          const float wL = has_left ? ex2(fminf(lA + g0 - A, 0.f)) : 0.f;
+          const float Ah = E[en_h<NS, R>(0, c) * 32 + lane], Al = E[en_l<NS, R>(0, c) * 32 + lane];
+          const float uh = P[en_h<NS, R>(0, c) * 32 + lane], ul = P[en_l<NS, R>(0, c) * 32 + lane];
+          float dh, dl, lh_, ll_;
+          if (c > 0) {
+            dh = P[en_h<NS, R>(0, c - 1) * 32 + lane]; dl = P[en_l<NS, R>(0, c - 1) * 32 + lane];
+            lh_ = E[en_h<NS, R>(0, c - 1) * 32 + lane]; ll_ = E[en_l<NS, R>(0, c - 1) * 32 + lane];
+          } else {
+            dh = dnh[0]; dl = dnl[0]; lh_ = lnh[0]; ll_ = lnl[0];
+          }
+          const float b = live ? ex2(fminf((Ah - Sh) + (Al - Sl), 0.f)) + ac[0][c] : 0.f;
+          const float wA = wgt(dh, dl, Ah, Al, sp);
+          const float wS = ex2(fminf((sp - Ah) - Al, 64.f));
+          const float wU = has_up ? wgt(uh, ul, Ah, Al, g0) : 0.f;
+          const float wL = has_left ? wgt(lh_, ll_, Ah, Al, g0) : 0.f;
           const float pv_ = b * (wA + wS);
           pm[c] = pv_;
           const float pU = b * wU, pL = b * wL, pD = b * wA;
@@ -680,6 +832,8 @@ __device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, ui
 #pragma unroll
         for (int c = 0; c < R; ++c) { ac[q][c] = nx[q][c]; nx[q][c] = 0.f; }
     }
+#pragma unroll
+    for (int q = 0; q < NP; ++q) pbc[q] = pbn[q];
     __syncwarp();
   }
   // warp-reduce the gradient partials (fixed shuffle tree: deterministic)
@@ -690,16 +844,22 @@ __device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, ui
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
   }
-  finish_pair<NS>(a, p, slot, lane, S2, v0, v1, v2);
+  finish_pair<NS>(a, p, slot, lane, Sh, Sl, v0, v1, v2);
 }
 
+// Shared memory per adjoint warp (floats): recomputed entries + lane-0 edges.
 template <int NS, int R>
-__global__ void __launch_bounds__(128) bwd_kernel(Args a) {
+__host__ __device__ constexpr int bwd_smem_floats() {
+  return (C_STEPS + 1) * Dims<NS, R>::EF * 32 + (C_STEPS + 1) * Dims<NS, R>::NE;
+}
+
+template <int NS, int R, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
   extern __shared__ float smem[];
-  using D = Dims<NS, R>;
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
-  float* sm = smem + (size_t)w * (C_STEPS + 1) * D::EF * 32;
+  float* sm = smem + (size_t)w * bwd_smem_floats<NS, R>();
+  float* ea = sm + (C_STEPS + 1) * Dims<NS, R>::EF * 32;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
   const int ntasks = a.B * a.nb;
   while (true) {
@@ -710,7 +870,7 @@ __global__ void __launch_bounds__(128) bwd_kernel(Args a) {
     int p = task / a.nb;
     const int band = a.nb - 1 - (task - p * a.nb);
     if (a.order) p = a.order[p];
-    bwd_band<NS, R>(a, p, band, lane, sm, deadline);
+    bwd_band<NS, R>(a, p, band, lane, sm, ea, deadline);
   }
 }
 

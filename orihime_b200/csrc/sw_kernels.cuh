@@ -6,16 +6,24 @@
 // warp owns one band: lane l owns the R consecutive columns
 // [band*32R + l*R, +R) and the warp sweeps the rows top to bottom as a skewed
 // wavefront -- at step t lane l works on row i = t - l + 1 (1-based), so the
-// band takes L1 + 31 steps.  The values of a lane's last column reach lane l+1
-// one step later through __shfl_up_sync; the last lane of a band writes them
-// to a global "edge" buffer that lane 0 of the next band polls.
+// band takes L1 + 31 steps (padded to whole checkpoint chunks).  The values of
+// a lane's last column reach lane l+1 one step later through __shfl_up_sync;
+// the last lane of a band writes them to a global "edge" buffer that lane 0
+// of the next band polls.
 //
-// All DP values live in a scaled log2 domain: x' = x * log2(e) / T, so every
-// exp/log of the reference recurrence is one MUFU ex2/lg2.
+// Arithmetic
+// ----------
+// DP values live in a scaled log2 domain, x' = x * log2(e) / T, so every
+// exp/log of the reference recurrence is one MUFU ex2/lg2.  Each value is a
+// double-float pair (hi, lo) with value = hi + lo: the hi part is an exact
+// copy of a predecessor's hi (or of a TwoSum), and every exponent is formed
+// as ((hi - base) + edge) + lo.  FP32 rounding of the DP values therefore
+// never accumulates along alignment paths, which is what limits the accuracy
+// of a plain FP32 forward-backward (the reference included) on long pairs.
 //
 // Forward kernel (one launch per op call): alpha, the partition partials and,
-// every C steps, a per-lane checkpoint of the DP state (3R+3 floats affine,
-// R+1 linear).  No alpha table is ever stored.
+// every C steps, a per-lane checkpoint of the DP state.  No alpha table is
+// ever stored.
 //
 // Adjoint kernel: per band, time chunks in reverse.  Each chunk restores its
 // checkpoint, recomputes C steps of alpha into shared memory, then runs the
@@ -27,9 +35,9 @@
 // Cross-band buffers are filled with a NaN sentinel before each call; a
 // consumer polls the value itself until it is not the sentinel, so no memory
 // fence is needed on the producer side.  Every poll is bounded by a
-// globaltimer deadline; on expiry the kernel records SWB_ERR_WAIT_TIMEOUT in
-// the status word, substitutes a neutral value and carries on, so no warp can
-// hang.
+// globaltimer deadline; on expiry the kernel records SWB_STATUS_WAIT_TIMEOUT
+// in the status word, substitutes a neutral value and carries on, so no warp
+// can hang.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -39,7 +47,7 @@ namespace swb {
 constexpr float NEG = -1e30f;           // "no path" in the scaled domain
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int C_STEPS = 8;              // checkpoint stride (steps)
-constexpr int PF = 4;                   // prefetch distance (steps); C_STEPS % PF == 0
+constexpr int PF = 4;                   // score prefetch distance (steps); C_STEPS % PF == 0
 constexpr uint32_t SENTINEL_BITS = 0xffffffffu;
 
 enum : unsigned {
@@ -64,13 +72,13 @@ struct Args {
   float* g_open;              // affine: dS/dgo ; linear: dS/dgap
   float* g_ext;               // affine: dS/dge ; linear: unused
   float* g_T;
-  // workspace (see workspace_layout in sw_capi.cu)
+  // workspace (see layout_for in sw_capi.cu)
   unsigned* counters;         // [0] forward task counter, [1] adjoint task counter
   unsigned* status;           // error bits
   unsigned* pair_done;        // [B]
   float* part;                // [B*nb][2] partition partials (ref, sum)
   float* gpart;               // [B*nb][4] gradient partials
-  float* edge;                // [B*nb][NS][Lmax1] sentinel-initialised
+  float* edge;                // [B*nb][2*NS][Lmax1] sentinel-initialised
   float* bpush;               // [B*nb][NP][Lmax1+1] sentinel-initialised
   float* ckpt;                // [B*nb][nchunks][CKF][32]
   unsigned long long spin_limit_ns;
