@@ -1,0 +1,495 @@
+"""Benchmark: fwd+bwd GCUPS of soft Smith-Waterman (affine gaps) over a packed
+ragged batch on B200, against the padded plain launch on the same GPU and the
+reference's own CPU implementation.
+
+Workload (one "step"): 4096 pairs whose lengths N, M are drawn independently
+log-uniform in [32, 2048] (seed 3), pair scores 3 <e_i, f_j> / sqrt(64) with
+e, f ~ N(0, 1) in d = 64 (seeded per pair), gap_open -2, gap_ext -0.5, T 0.5.
+One step = one forward + checkpointed adjoint over the whole packed batch
+(value, marginal map and dS/d(params) for every pair).  Inputs (3.9 GB of
+scores) are larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU (torchrun): every rank runs its own batch (seed 3 + rank): weak
+scaling, no collective on the data path; rank 0 prints the line with the
+max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd GCUPS, soft SW-affine ragged batch, vs padded plain on same B200"
+GO, GE, T = -2.0, -0.5, 0.5
+NPAIRS, LMIN, LMAX, D = 4096, 32, 2048, 64
+MUFU_PER_CELL = 21      # algorithmic MUFU ops per cell, forward 11 + adjoint 10
+MUFU_PER_CELL_BWD = 10  # adjoint kernel alone
+BYTES_PER_CELL = 8      # compulsory HBM bytes per cell (score read + map write)
+
+
+def workload_lengths(seed: int, n: int = NPAIRS) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    ln = np.exp(rng.uniform(np.log(LMIN), np.log(LMAX), size=(n, 2)))
+    return np.rint(ln).astype(np.int64)
+
+
+def make_scores(torch, lengths, offsets, seed, device):
+    """Packed C2-generator scores, built on the device pair by pair."""
+    from orihime_b200 import ragged
+
+    flat = torch.zeros(int(offsets[-1]), dtype=torch.float32, device=device)
+    g = torch.Generator(device=device)
+    for b, (L1, L2) in enumerate(lengths.tolist()):
+        g.manual_seed(seed * 100003 + b)
+        e = torch.randn(L1, D, generator=g, device=device)
+        f = torch.randn(L2, D, generator=g, device=device)
+        p = ragged.pitch_of(L2)
+        flat[int(offsets[b]):int(offsets[b]) + L1 * p].view(L1, p)[:, :L2] = 3.0 * (e @ f.T) / D ** 0.5
+    return flat
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def __enter__(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True,
+                                         text=True, timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._th = threading.Thread(target=run, daemon=True)
+        self._th.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 3 + k and "Active" in s[3 + k] and "Not" not in s[3 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_init(torch):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(torch, world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(torch, world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def mufu_peak(torch, lib) -> float:
+    """Measured ex2 throughput (ops/s) of this GPU: the MUFU roofline denominator."""
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    blocks, iters = sms * 8, 4096
+    scratch = torch.empty(blocks * 256, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        lib.swb_mufu_probe(scratch.data_ptr(), blocks, iters, st)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        lib.swb_mufu_probe(scratch.data_ptr(), blocks, iters, st)
+        b.record()
+        torch.cuda.synchronize()
+        best = max(best, blocks * 256 * iters * 8 / (a.elapsed_time(b) * 1e-3))
+    return best
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(p))
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU arm
+# ---------------------------------------------------------------------------
+
+def reference_cpu_sample(lengths, seed, budget_cells=2.0e8, chunk=None):
+    """A bounded sample of the workload for the reference CPU kernels: every
+    k-th pair (by index) until about `budget_cells` cells, grouped into padded
+    chunks of similar size as the reference's batched API expects."""
+    import torch
+
+    idx = np.arange(len(lengths))
+    cells = lengths[:, 0] * lengths[:, 1]
+    order = idx[np.argsort(-cells, kind="stable")]
+    step = max(1, int(cells.sum() / budget_cells))
+    pick = np.sort(order[::step])
+    chunks, cur = [], []
+    chunk = chunk or min(64, max(8, os.cpu_count() or 8))
+    cap = 4e9 / 40  # padded cells per chunk: scores, map and the 3-plane alpha/beta in RAM
+    for b in sorted(pick, key=lambda b: -cells[b]):
+        if cur:
+            L1m = max(int(lengths[x, 0]) for x in cur + [b])
+            L2m = max(int(lengths[x, 1]) for x in cur + [b])
+            if (len(cur) + 1) * L1m * L2m > cap:
+                chunks.append(cur)
+                cur = []
+        cur.append(b)
+        if len(cur) == chunk:
+            chunks.append(cur)
+            cur = []
+    if cur:
+        chunks.append(cur)
+    data = []
+    for ch in chunks:
+        L1m = int(max(lengths[b, 0] for b in ch))
+        L2m = int(max(lengths[b, 1] for b in ch))
+        s = np.zeros((len(ch), L1m, L2m), np.float32)
+        for k, b in enumerate(ch):
+            g = torch.Generator().manual_seed(seed * 100003 + int(b))
+            L1, L2 = int(lengths[b, 0]), int(lengths[b, 1])
+            e = torch.randn(L1, D, generator=g)
+            f = torch.randn(L2, D, generator=g)
+            s[k, :L1, :L2] = (3.0 * (e @ f.T) / D ** 0.5).numpy()
+        ln = np.array([[lengths[b, 0], lengths[b, 1]] for b in ch], np.int32)
+        data.append((s, ln))
+    return data, int(cells[pick].sum()), len(pick)
+
+
+def run_reference(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        try:
+            O.build(ref=True)
+        except Exception:
+            pass
+    lengths = workload_lengths(3)
+    data, cells, npairs = reference_cpu_sample(lengths, 3)
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    if O.ref_available():
+        kind, fn = "reference", lambda s, ln: O.ref_affine(s, ln, GO, GE, T)
+    else:
+        kind, fn = "port", lambda s, ln: O.affine(s, ln, GO, GE, T)
+        threads = 1
+
+    def step():
+        for s, ln in data:
+            fn(s, ln)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    gcups = cells / dt / 1e9
+    sample = (f"{npairs} of the {NPAIRS} pairs (every k-th by size, {cells:.3g} cells) in padded "
+              f"chunks of up to {min(64, max(8, threads))}; reference CPU kernels (src/sw_affine/kernels_cpu.cpp) forward+backward")
+    line = {"impl": "reference", "metric": METRIC, "value": gcups, "unit": "GCUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"ragged C3: {NPAIRS} affine pairs, N,M log-uniform "
+                                   f"[{LMIN},{LMAX}], go {GO} ge {GE} T {T}", "sample": sample},
+            "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": gcups, "unit": "GCUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--pairs", type=int, default=NPAIRS, help="pairs per GPU (profiling cases)")
+    ap.add_argument("--quick", action="store_true",
+                    help="timed steps only: no e2e, plain, CPU legs (profiling cases)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    import orihime_b200
+    from orihime_b200 import _lib, ragged
+
+    world, rank, local = dist_init(torch)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+
+    lengths = workload_lengths(3 + rank, args.pairs)
+    offsets, ln32 = ragged.layout(lengths)
+    cells = int((lengths[:, 0] * lengths[:, 1]).sum())
+    flat = make_scores(torch, lengths, offsets, 3 + rank, dev)
+    plan = ragged.Plan(ln32, offsets, family="affine", device=dev)
+    out = plan.outputs()
+
+    def step():
+        plan.run(flat, gap_open=GO, gap_ext=GE, temp=T, out=out)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if plan.status() != 0:
+        raise RuntimeError("kernel reported a bounded-wait timeout")
+
+    # ---- timed region: K steps, events on the launching stream ----
+    # Each step records three events: before the call, between the forward and
+    # the adjoint kernel (recorded by the library on the launch stream), after.
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    for trio in ev:           # create the underlying CUDA events before timing
+        for e_ in trio:
+            e_.record()
+    torch.cuda.synchronize()
+    opts = [_lib.Options(0, 0, 0, trio[1].cuda_event) for trio in ev]
+    with ClockSampler(local) as clk:
+        barrier(torch, world)
+        torch.cuda.synchronize()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record()
+        for k in range(args.steps):
+            ev[k][0].record()
+            plan.run(flat, gap_open=GO, gap_ext=GE, temp=T, out=out, options=opts[k])
+            ev[k][2].record()
+        t_end.record()
+        torch.cuda.synchronize()
+        barrier(torch, world)
+    total_ms = max_over_ranks(torch, world, t_start.elapsed_time(t_end))
+    ms = total_ms / args.steps
+    gcups_all = cells * world / (ms * 1e-3) / 1e9
+    per_step = sorted(ev[k][0].elapsed_time(ev[k][2]) for k in range(args.steps))
+    kernel_split = {
+        "fwd_ms": float(np.mean([ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)])),
+        "bwd_ms": float(np.mean([ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps)])),
+        "note": "fwd_ms includes the per-call workspace memsets",
+    }
+
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "pairs": args.pairs, "cells": cells, "ms_per_step": ms,
+                              "gcups": gcups_all, "kernel_ms": kernel_split}))
+        return 0
+
+    # ---- e2e through the public API: pinned H2D of the scores, D2H of values ----
+    host = torch.empty(flat.numel(), dtype=torch.float32, pin_memory=True)
+    host.copy_(flat.cpu())
+    host_val = torch.empty(plan.B, dtype=torch.float32, pin_memory=True)
+    dflat = torch.empty_like(flat)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(2):
+        dflat.copy_(host, non_blocking=True)
+        plan.run(dflat, gap_open=GO, gap_ext=GE, temp=T, out=out)
+        host_val.copy_(out.value, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(torch, world)
+    e0.record()
+    for _ in range(args.steps):
+        dflat.copy_(host, non_blocking=True)
+        plan.run(dflat, gap_open=GO, gap_ext=GE, temp=T, out=out)
+        host_val.copy_(out.value, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(torch, world, e0.elapsed_time(e1)) / args.steps
+    e2e = {"value": cells * world / (e2e_ms * 1e-3) / 1e9, "unit": "GCUPS",
+           "h2d_bytes_per_step": flat.numel() * 4, "d2h_bytes_per_step": plan.B * 4,
+           "ms_per_step": e2e_ms}
+    del dflat, host
+
+    # ---- plain padded launch on a sample of the same pairs ----
+    plain = None if args.no_plain else plain_padded(torch, lengths, offsets, flat, ms, cells)
+
+    line = None
+    if rank == 0:
+        peak = mufu_peak(torch, lib)
+        bwd_ms = kernel_split.get("bwd_ms")
+        roof = None
+        if bwd_ms:
+            achieved = MUFU_PER_CELL_BWD * cells / (bwd_ms * 1e-3)
+            roof = {"bound": "mufu", "achieved": achieved / 1e9, "peak": peak / 1e9,
+                    "unit": "Gop/s", "frac": achieved / peak, "traffic": None,
+                    "kernel": "bwd_kernel<3,4,1> (checkpointed adjoint)",
+                    "algorithmic": f"{MUFU_PER_CELL_BWD} ex2/lg2 per cell x {cells} cells",
+                    "peak_source": "measured in-bench (swb_mufu_probe: ex2.approx throughput)",
+                    "step_frac": (MUFU_PER_CELL * cells / (ms * 1e-3)) / peak,
+                    "hbm_frac_of_measured": (BYTES_PER_CELL * cells / (ms * 1e-3)) /
+                                            (measured_peaks().get("hbm_gbs", 6550.0) * 1e9)}
+            prof = os.path.join(ROOT, "profiles", "bench_traffic.json")
+            if os.path.exists(prof):
+                try:
+                    tr = json.load(open(prof))
+                    roof["traffic"] = tr.get("bytes_per_cell_bwd", 0) * cells
+                except Exception:
+                    pass
+        cpu = None if args.no_cpu_baseline else cpu_baseline(lengths)
+        clocks = clk.summary()
+        line = {"metric": METRIC, "value": gcups_all, "unit": "GCUPS", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"ragged C3: {args.pairs} affine pairs per GPU, N,M log-uniform "
+                                       f"[{LMIN},{LMAX}] (seed 3+rank), scores 3<e,f>/sqrt(64)",
+                           "cells_per_gpu": cells, "gap_open": GO, "gap_ext": GE, "temp": T,
+                           "l2": "inputs (3.9 GB) larger than L2; no flush",
+                           "parallelism": f"replicas x{world} (independent pairs)"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 2 * args.steps, "clocks": clocks,
+                "kernel_ms": kernel_split, "step_ms_spread": [per_step[0], per_step[-1]],
+                "plain_padded": plain}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def plain_padded(torch, lengths, offsets, flat, ragged_ms, cells_all, sample_pairs=64):
+    """The plain drop-in on a padded [B, 2048, 2048] batch of the first
+    `sample_pairs` pairs, masked (excluded cells get the mask sentinel, so the
+    full padded area is computed, as ohm.sw_affine(mask=...) does) and with
+    lengths (the kernel skips cells outside each pair)."""
+    from orihime_b200 import operator as op
+    from orihime_b200 import ragged
+
+    pick = list(range(sample_pairs))
+    L1m, L2m = LMAX, LMAX
+    dev = flat.device
+    x = torch.zeros(len(pick), L1m, L2m, device=dev)
+    mask = torch.ones(len(pick), L1m, L2m, dtype=torch.bool, device=dev)
+    for k, b in enumerate(pick):
+        L1, L2 = int(lengths[b, 0]), int(lengths[b, 1])
+        p = ragged.pitch_of(L2)
+        x[k, :L1, :L2] = flat[int(offsets[b]):int(offsets[b]) + L1 * p].view(L1, p)[:, :L2]
+        mask[k, :L1, :L2] = False
+    useful = int(sum(int(lengths[b, 0]) * int(lengths[b, 1]) for b in pick))
+    xm = op.normalize_mask(x.masked_fill(mask, float("-inf")), T).contiguous()
+    ln = torch.tensor([[int(lengths[b, 0]), int(lengths[b, 1])] for b in pick], dtype=torch.int32,
+                      device=dev)
+    res = {}
+    for name, fn in (("masked", lambda: torch.ops.orihime.sw_affine_forward(xm, GO, GE, T, None)),
+                     ("lengths", lambda: torch.ops.orihime.sw_affine_forward(x, GO, GE, T, ln))):
+        fn()
+        torch.cuda.synchronize()
+        a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b2.record()
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b2)
+        res[name] = {"ms": t, "gcups_useful": useful / (t * 1e-3) / 1e9}
+    ragged_gcups = cells_all / (ragged_ms * 1e-3) / 1e9
+    res["sample"] = f"first {sample_pairs} pairs padded to {L1m}x{L2m} ({useful} useful cells)"
+    res["ragged_over_plain_masked"] = ragged_gcups / res["masked"]["gcups_useful"]
+    res["ragged_over_plain_lengths"] = ragged_gcups / res["lengths"]["gcups_useful"]
+    del x, mask, xm
+    torch.cuda.empty_cache()
+    return res
+
+
+def cpu_baseline(lengths):
+    """The reference CPU kernels on a bounded sample of the workload (this host's cores)."""
+    import torch
+
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        try:
+            O.build(ref=True)
+        except Exception:
+            pass
+    data, cells, npairs = reference_cpu_sample(lengths, 3, budget_cells=2e8)
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    if O.ref_available():
+        kind, fn = "reference", lambda s, ln: O.ref_affine(s, ln, GO, GE, T)
+    else:
+        kind, fn = "port", lambda s, ln: O.affine(s, ln, GO, GE, T)
+        threads = 1
+    t0 = time.perf_counter()
+    for s, ln in data:
+        fn(s, ln)
+    dt = time.perf_counter() - t0
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": threads, "kind": kind,
+            "sample": f"{npairs} pairs ({cells:.3g} cells) of the workload, padded chunks of "
+                      f"up to {min(64, max(8, threads))}, "
+                      f"{dt:.1f} s"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -49,6 +49,8 @@ typedef struct swb_options {
     int max_ctas;                      /* cap on persistent CTAs (0 = occupancy-derived) */
     unsigned long long spin_limit_ns;  /* bound on every cross-warp wait (0 = 20 s)      */
     int fault_inject;                  /* 1: band>0 waits on a word nobody writes (tests) */
+    void* split_event;                 /* cudaEvent_t recorded between the forward and the
+                                          adjoint kernel (per-kernel timing), or NULL     */
 } swb_options;
 
 /* Workspace bytes for swb_sw_affine_forward on a [B, L1max, L2max] batch. */
@@ -85,6 +87,43 @@ int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, in
                    float* value, float* map, float* grad_gap, float* grad_temp,
                    void* workspace, size_t workspace_bytes, void* stream,
                    const swb_options* opt);
+
+/*
+ * Packed ragged batch (no reference counterpart: the reference pads every
+ * pair to one shape; this is the batched path beside its drop-in).
+ *
+ * Packing: pair b's scores are an L1_b x L2_b row-major block with row pitch
+ * P_b = L2_b rounded up to a multiple of 4, starting at element offsets[b]
+ * (a multiple of 4) of one flat float buffer; offsets has B+1 entries and
+ * offsets[b+1] - offsets[b] >= L1_b * P_b.  The map uses the same packing;
+ * its pitch padding is written as 0.
+ *
+ * swb_ragged_plan runs on the host: it validates the packing, orders the
+ * pairs longest first (most cells first) for the persistent task queue and
+ * places every band's workspace slice.  Call it once with plan = NULL to get
+ * *plan_bytes (and *workspace_bytes), then with a buffer of that size; copy
+ * the plan bytes to the device unchanged and pass both copies to the launch.
+ * family: 3 = affine, 1 = linear.  host lengths [B, 2], host offsets [B+1].
+ */
+int swb_ragged_plan(int family, const int* lengths, const long long* offsets, int B,
+                    void* plan, size_t plan_capacity, size_t* plan_bytes,
+                    size_t* workspace_bytes);
+
+/* Affine soft Smith–Waterman over a packed ragged batch; outputs as
+ * swb_sw_affine_forward, map in the packed layout. */
+int swb_sw_affine_ragged(const float* scores, const void* host_plan, const void* dev_plan,
+                         float gap_open, float gap_ext, float temp,
+                         float* value, float* map,
+                         float* grad_open, float* grad_ext, float* grad_temp,
+                         void* workspace, size_t workspace_bytes, void* stream,
+                         const swb_options* opt);
+
+/* Linear-gap soft Smith–Waterman over a packed ragged batch. */
+int swb_sw_ragged(const float* scores, const void* host_plan, const void* dev_plan,
+                  float gap, float temp,
+                  float* value, float* map, float* grad_gap, float* grad_temp,
+                  void* workspace, size_t workspace_bytes, void* stream,
+                  const swb_options* opt);
 
 /* Copies the workspace status word to *status (synchronises `stream`).
  * No reference counterpart: the reference synchronises inside every op. */

@@ -29,6 +29,7 @@ class Options(ctypes.Structure):
         ("max_ctas", ctypes.c_int),
         ("spin_limit_ns", ctypes.c_ulonglong),
         ("fault_inject", ctypes.c_int),
+        ("split_event", ctypes.c_void_p),
     ]
 
 
@@ -66,6 +67,16 @@ def load() -> ctypes.CDLL:
                                    ctypes.POINTER(Options)]
     lib.swb_read_status.restype = i
     lib.swb_read_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_uint)]
+    ll = ctypes.c_longlong
+    lib.swb_ragged_plan.restype = i
+    lib.swb_ragged_plan.argtypes = [i, vp, vp, i, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]
+    lib.swb_sw_affine_ragged.restype = i
+    lib.swb_sw_affine_ragged.argtypes = [vp, vp, vp, f, f, f, vp, vp, vp, vp, vp, vp, sz, vp,
+                                         ctypes.POINTER(Options)]
+    lib.swb_sw_ragged.restype = i
+    lib.swb_sw_ragged.argtypes = [vp, vp, vp, f, f, vp, vp, vp, vp, vp, sz, vp,
+                                  ctypes.POINTER(Options)]
+    del ll
     lib.swb_mufu_probe.restype = i
     lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()

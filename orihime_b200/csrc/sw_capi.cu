@@ -8,7 +8,9 @@
 // buffer whose size the *_workspace_bytes functions report.
 #include <cstdint>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "sw_kernels.cu"
@@ -37,25 +39,52 @@ struct Layout {
   size_t total;
 };
 
-template <int NS>
-Layout layout_for(long long B, long long L1m, long long L2m) {
+// Workspace layout for `slots` band slots and the given buffer sizes (floats).
+Layout layout_sizes(long long B, size_t slots, size_t edge_floats, size_t bp_floats,
+                    size_t ck_floats) {
   Layout l{};
-  l.nb = (int)((L2m + 32 * kR - 1) / (32 * kR));
-  if (l.nb < 1) l.nb = 1;
-  l.nchunks = (int)((L1m + 31 + swb::C_STEPS - 1) / swb::C_STEPS);  // = band_chunks(L1m)
-  const size_t slots = (size_t)B * l.nb;
   size_t o = 0;
   l.off_hdr = o;        o = align_up(o + 64);
   l.off_pair_done = o;  o = align_up(o + sizeof(unsigned) * (size_t)B);
   l.off_part = o;       o = align_up(o + sizeof(float) * 2 * slots);
   l.off_gpart = o;      o = align_up(o + sizeof(float) * 4 * slots);
   l.off_sent = o;       o = o + kAlign;   // never_written word lives here
-  l.off_edge = o;       o = align_up(o + sizeof(float) * slots * ne<NS>() * (size_t)L1m);
-  l.off_bpush = o;      o = align_up(o + sizeof(float) * slots * np<NS>() * (size_t)(L1m + 1));
+  l.off_edge = o;       o = align_up(o + sizeof(float) * edge_floats);
+  l.off_bpush = o;      o = align_up(o + sizeof(float) * bp_floats);
   l.sent_bytes = o - l.off_sent;
-  l.off_ckpt = o;       o = align_up(o + sizeof(float) * slots * l.nchunks * ckf<NS>() * 32);
+  l.off_ckpt = o;       o = align_up(o + sizeof(float) * ck_floats);
   l.total = o;
   return l;
+}
+
+int chunks_for(long long L1) { return (int)((L1 + 31 + swb::C_STEPS - 1) / swb::C_STEPS); }
+
+// Padded batch: every pair gets the slices of a Lmax1 x Lmax2 pair.
+template <int NS>
+Layout layout_for(long long B, long long L1m, long long L2m) {
+  int nb = (int)((L2m + 32 * kR - 1) / (32 * kR));
+  if (nb < 1) nb = 1;
+  const int nch = chunks_for(L1m);
+  const size_t slots = (size_t)B * nb;
+  Layout l = layout_sizes(B, slots, slots * ne<NS>() * (size_t)L1m,
+                          slots * np<NS>() * (size_t)(L1m + 1),
+                          slots * (size_t)nch * ckf<NS>() * 32);
+  l.nb = nb;
+  l.nchunks = nch;
+  return l;
+}
+
+// Ragged plan header (int64 words), followed by B * PLAN_PAIR_WORDS pair
+// words and ntasks (pair, band) int32 pairs.
+enum HeaderWord : int {
+  HW_MAGIC = 0, HW_B = 1, HW_NTASKS = 2, HW_SLOTS = 3, HW_CK = 4, HW_EDGE = 5, HW_BP = 6,
+  HW_FAMILY = 7, HW_MAP_ELEMS = 8, HW_WORDS = 10
+};
+constexpr long long kPlanMagic = 0x53574232504c414eLL;  // "SWB2PLAN"
+
+size_t plan_bytes_for(long long B, long long ntasks) {
+  return sizeof(long long) * (HW_WORDS + (size_t)B * swb::PLAN_PAIR_WORDS) +
+         sizeof(int) * 2 * (size_t)ntasks;
 }
 
 struct DevInfo {
@@ -98,31 +127,17 @@ int dev_info(DevInfo** out) {
   return SWB_OK;
 }
 
+// Common launch: per-call resets, then the forward and adjoint kernels.
 template <int NS>
-int launch(const float* scores, const int* lengths, const long long* offsets, const int* order,
-           int layout, int B, int L1m, int L2m, float go, float ge, float T, float* value,
-           float* map, size_t map_elems, float* g_open, float* g_ext, float* g_T, void* ws,
+int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool clear_map, void* ws,
            size_t ws_bytes, void* stream_v, const swb_options* opt) {
-  if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
-  if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
-  if (B == 0) return SWB_OK;
-  if (!value || !g_open || !g_T || (NS == 3 && !g_ext)) return SWB_ERR_ARG;
-  if (map_elems > 0 && (!scores || !map)) return SWB_ERR_ARG;
-  if (layout == 1 && (!offsets || !lengths)) return SWB_ERR_ARG;
-  const Layout l = layout_for<NS>(B, L1m, L2m);
   if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
   DevInfo* d = nullptr;
   int rc = dev_info(&d);
   if (rc != SWB_OK) return rc;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream_v);
   char* w = static_cast<char*>(ws);
-
-  Args a{};
-  a.scores = scores; a.map = map; a.lengths = lengths; a.offsets = offsets; a.order = order;
-  a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = layout;
-  a.go = go; a.ge = ge; a.T = T; a.k = 1.4426950408889634f / T;
-  a.nb = l.nb; a.nchunks = l.nchunks;
-  a.value = value; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
+  a.k = 1.4426950408889634f / a.T;
   a.counters = reinterpret_cast<unsigned*>(w + l.off_hdr);
   a.status = a.counters + 4;
   a.pair_done = reinterpret_cast<unsigned*>(w + l.off_pair_done);
@@ -139,10 +154,10 @@ int launch(const float* scores, const int* lengths, const long long* offsets, co
   // buffers to the NaN sentinel, the map to 0 (cells outside lengths stay 0)
   if (cudaMemsetAsync(w, 0, l.off_part, st) != cudaSuccess) return SWB_ERR_CUDA;
   if (cudaMemsetAsync(w + l.off_sent, 0xff, l.sent_bytes, st) != cudaSuccess) return SWB_ERR_CUDA;
-  if (map_elems > 0 && cudaMemsetAsync(map, 0, map_elems * sizeof(float), st) != cudaSuccess)
+  if (clear_map && map_elems > 0 &&
+      cudaMemsetAsync(a.map, 0, map_elems * sizeof(float), st) != cudaSuccess)
     return SWB_ERR_CUDA;
 
-  const long long ntasks = (long long)B * l.nb;
   const int cta_cap_f = d->sms * (d->occ_fwd[NS == 3] > 0 ? d->occ_fwd[NS == 3] : 1);
   const int cta_cap_b = d->sms * (d->occ_bwd[NS == 3] > 0 ? d->occ_bwd[NS == 3] : 1);
   const long long need_f = (ntasks + kWarpsFwd - 1) / kWarpsFwd;
@@ -153,11 +168,62 @@ int launch(const float* scores, const int* lengths, const long long* offsets, co
     if (grid_f > opt->max_ctas) grid_f = opt->max_ctas;
     if (grid_b > opt->max_ctas) grid_b = opt->max_ctas;
   }
+  if (grid_f < 1) grid_f = 1;
+  if (grid_b < 1) grid_b = 1;
   swb::fwd_kernel<NS, kR><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
+  if (opt && opt->split_event &&
+      cudaEventRecord(reinterpret_cast<cudaEvent_t>(opt->split_event), st) != cudaSuccess)
+    return SWB_ERR_CUDA;
   swb::bwd_kernel<NS, kR, kWarpsBwd><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS>(), st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   return SWB_OK;
+}
+
+template <int NS>
+int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
+                  float ge, float T, float* value, float* map, float* g_open, float* g_ext,
+                  float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
+  if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
+  if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
+  if (B == 0) return SWB_OK;
+  const size_t map_elems = (size_t)B * L1m * L2m;
+  if (!value || !g_open || !g_T || (NS == 3 && !g_ext)) return SWB_ERR_ARG;
+  if (map_elems > 0 && (!scores || !map)) return SWB_ERR_ARG;
+  const Layout l = layout_for<NS>(B, L1m, L2m);
+  Args a{};
+  a.scores = scores; a.map = map; a.lengths = lengths;
+  a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
+  a.go = go; a.ge = ge; a.T = T;
+  a.nb = l.nb; a.nchunks = l.nchunks;
+  a.value = value; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
+  return launch<NS>(a, l, (long long)B * l.nb, map_elems, true, ws, ws_bytes, stream, opt);
+}
+
+template <int NS>
+int launch_ragged(const float* scores, const void* host_plan, const void* dev_plan, float go,
+                  float ge, float T, float* value, float* map, float* g_open, float* g_ext,
+                  float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
+  if (!host_plan || !dev_plan) return SWB_ERR_ARG;
+  const long long* h = static_cast<const long long*>(host_plan);
+  if (h[HW_MAGIC] != kPlanMagic || h[HW_FAMILY] != NS) return SWB_ERR_ARG;
+  if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
+  const long long B = h[HW_B], ntasks = h[HW_NTASKS];
+  if (B == 0) return SWB_OK;
+  if (!value || !g_open || !g_T || (NS == 3 && !g_ext)) return SWB_ERR_ARG;
+  if (h[HW_MAP_ELEMS] > 0 && (!scores || !map)) return SWB_ERR_ARG;
+  const Layout l = layout_sizes(B, (size_t)h[HW_SLOTS], (size_t)h[HW_EDGE], (size_t)h[HW_BP],
+                                (size_t)h[HW_CK]);
+  const long long* dp = static_cast<const long long*>(dev_plan);
+  Args a{};
+  a.scores = scores; a.map = map;
+  a.plan_pairs = dp + HW_WORDS;
+  a.plan_tasks = reinterpret_cast<const int*>(dp + HW_WORDS + B * swb::PLAN_PAIR_WORDS);
+  a.ntasks = (int)ntasks;
+  a.B = (int)B; a.layout = 1;
+  a.go = go; a.ge = ge; a.T = T;
+  a.value = value; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
+  return launch<NS>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt);
 }
 
 }  // namespace
@@ -178,18 +244,102 @@ int swb_sw_affine_forward(const float* scores, const int* lengths, int B, int L1
                           float gap_open, float gap_ext, float temp, float* value, float* map,
                           float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
                           size_t workspace_bytes, void* stream, const swb_options* opt) {
-  return launch<3>(scores, lengths, nullptr, nullptr, 0, B, L1max, L2max, gap_open, gap_ext, temp,
-                   value, map, (size_t)B * L1max * L2max, grad_open, grad_ext, grad_temp,
-                   workspace, workspace_bytes, stream, opt);
+  return launch_padded<3>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value, map,
+                          grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream, opt);
 }
 
 int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
                    float temp, float* value, float* map, float* grad_gap, float* grad_temp,
                    void* workspace, size_t workspace_bytes, void* stream,
                    const swb_options* opt) {
-  return launch<1>(scores, lengths, nullptr, nullptr, 0, B, L1max, L2max, gap, 0.f, temp, value,
-                   map, (size_t)B * L1max * L2max, grad_gap, nullptr, grad_temp, workspace,
-                   workspace_bytes, stream, opt);
+  return launch_padded<1>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, map, grad_gap,
+                          nullptr, grad_temp, workspace, workspace_bytes, stream, opt);
+}
+
+int swb_ragged_plan(int family, const int* lengths, const long long* offsets, int B,
+                    void* plan, size_t plan_capacity, size_t* plan_bytes,
+                    size_t* workspace_bytes) {
+  if ((family != 1 && family != 3) || B < 0 || (B > 0 && (!lengths || !offsets)))
+    return SWB_ERR_ARG;
+  const int NE = 2 * family, NP = (family == 3) ? 5 : 2, CKF = 2 * family * kR + 2 * family;
+  // validate the packing: row pitch round4(L2), offsets multiples of 4 floats
+  long long ntasks = 0;
+  for (int b = 0; b < B; ++b) {
+    const long long L1 = lengths[2 * b], L2 = lengths[2 * b + 1];
+    if (L1 < 0 || L2 < 0 || L1 > (1 << 24) || L2 > (1 << 24)) return SWB_ERR_ARG;
+    const long long pitch = (L2 + 3) & ~3LL;
+    if (offsets[b] < 0 || (offsets[b] & 3) || offsets[b + 1] - offsets[b] < L1 * pitch)
+      return SWB_ERR_ARG;
+    long long nb = (L2 + 32 * kR - 1) / (32 * kR);
+    ntasks += nb < 1 ? 1 : nb;
+  }
+  const size_t need = plan_bytes_for(B, ntasks);
+  if (plan_bytes) *plan_bytes = need;
+  if (!plan) {  // size query
+    if (workspace_bytes) *workspace_bytes = 0;
+    if (!plan_bytes) return SWB_ERR_ARG;
+    // fall through to compute the workspace size without writing a plan
+  } else if (plan_capacity < need) {
+    return SWB_ERR_ARG;
+  }
+  // longest-processing-time order: most cells first, ties by index
+  std::vector<int> order(B);
+  for (int b = 0; b < B; ++b) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return (long long)lengths[2 * x] * lengths[2 * x + 1] >
+           (long long)lengths[2 * y] * lengths[2 * y + 1];
+  });
+  long long* h = static_cast<long long*>(plan);
+  long long* pw = plan ? h + HW_WORDS : nullptr;
+  int* tk = plan ? reinterpret_cast<int*>(h + HW_WORDS + (size_t)B * swb::PLAN_PAIR_WORDS)
+                 : nullptr;
+  size_t slots = 0, ck = 0, ed = 0, bp = 0;
+  long long t = 0;
+  for (int b : order) {
+    const long long L1 = lengths[2 * b], L2 = lengths[2 * b + 1];
+    long long nb = (L2 + 32 * kR - 1) / (32 * kR);
+    if (nb < 1) nb = 1;
+    if (pw) {
+      long long* q = pw + (size_t)b * swb::PLAN_PAIR_WORDS;
+      q[swb::PW_SCORE_OFF] = offsets[b];
+      q[swb::PW_L1] = L1;
+      q[swb::PW_L2] = L2;
+      q[swb::PW_SLOT0] = (long long)slots;
+      q[swb::PW_NB] = nb;
+      q[swb::PW_CK0] = (long long)ck;
+      q[swb::PW_EDGE0] = (long long)ed;
+      q[swb::PW_BP0] = (long long)bp;
+      for (long long j = 0; j < nb; ++j) { tk[2 * t] = b; tk[2 * t + 1] = (int)j; ++t; }
+    }
+    slots += nb;
+    ck += (size_t)nb * chunks_for(L1) * CKF * 32;
+    ed += (size_t)nb * NE * L1;
+    bp += (size_t)nb * NP * (L1 + 1);
+  }
+  const Layout l = layout_sizes(B, slots, ed, bp, ck);
+  if (workspace_bytes) *workspace_bytes = B > 0 ? l.total : 0;
+  if (pw) {
+    h[HW_MAGIC] = kPlanMagic; h[HW_B] = B; h[HW_NTASKS] = ntasks; h[HW_SLOTS] = (long long)slots;
+    h[HW_CK] = (long long)ck; h[HW_EDGE] = (long long)ed; h[HW_BP] = (long long)bp;
+    h[HW_FAMILY] = family; h[HW_MAP_ELEMS] = B > 0 ? offsets[B] : 0; h[9] = 0;
+  }
+  return SWB_OK;
+}
+
+int swb_sw_affine_ragged(const float* scores, const void* host_plan, const void* dev_plan,
+                         float gap_open, float gap_ext, float temp, float* value, float* map,
+                         float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                         size_t workspace_bytes, void* stream, const swb_options* opt) {
+  return launch_ragged<3>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value, map,
+                          grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream, opt);
+}
+
+int swb_sw_ragged(const float* scores, const void* host_plan, const void* dev_plan, float gap,
+                  float temp, float* value, float* map, float* grad_gap, float* grad_temp,
+                  void* workspace, size_t workspace_bytes, void* stream,
+                  const swb_options* opt) {
+  return launch_ragged<1>(scores, host_plan, dev_plan, gap, 0.f, temp, value, map, grad_gap,
+                          nullptr, grad_temp, workspace, workspace_bytes, stream, opt);
 }
 
 int swb_read_status(const void* workspace, void* stream, unsigned* status) {

@@ -84,33 +84,73 @@ struct Pair {
   bool vec;         // row starts are 16-byte aligned and ld % 4 == 0
 };
 
-__device__ __forceinline__ Pair pair_of(const Args& a, int p) {
-  Pair r;
+// Where a band task lives: its pair, band, and the pair's workspace slices.
+struct Place {
+  int p, band, nb;          // pair, band, bands of the pair
+  size_t slot0;             // slot of band 0 (partials, completion count)
+  size_t ck0, ckb;          // checkpoint floats: band 0 offset, per-band stride
+  size_t ed0, edb;          // edge floats
+  size_t bp0, bpb;          // push floats
+  int Lm;                   // row stride of the edge / push buffers (>= L1)
+  Pair pr;
+};
+
+template <int NS, int R>
+__device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_band) {
+  constexpr int NE = 2 * NS, NP = (NS == 3) ? 5 : 2, CKF = 2 * NS * R + 2 * NS;
+  Place w;
+  Pair& r = w.pr;
   if (a.layout == 0) {
-    size_t base = (size_t)p * a.Lmax1 * a.Lmax2;
+    int p = task / a.nb;
+    const int j = task - p * a.nb;
+    if (a.order) p = a.order[p];
+    w.p = p;
+    w.nb = a.nb;
+    w.band = reverse_band ? a.nb - 1 - j : j;
+    w.slot0 = (size_t)p * a.nb;
+    w.Lm = a.Lmax1;
+    w.ckb = (size_t)a.nchunks * CKF * 32;
+    w.edb = (size_t)NE * a.Lmax1;
+    w.bpb = (size_t)NP * (a.Lmax1 + 1);
+    w.ck0 = w.slot0 * w.ckb;
+    w.ed0 = w.slot0 * w.edb;
+    w.bp0 = w.slot0 * w.bpb;
+    const size_t base = (size_t)p * a.Lmax1 * a.Lmax2;
     r.s = a.scores + base;
     r.m = a.map + base;
     r.ld = a.Lmax2;
-  } else {
-    long long off = a.offsets[p];
-    r.s = a.scores + off;
-    r.m = a.map + off;
-  }
-  if (a.lengths) {
-    r.L1 = a.lengths[2 * p];
-    r.L2 = a.lengths[2 * p + 1];
-    if (a.layout == 0) {  // never index outside the padded slab
-      r.L1 = min(max(r.L1, 0), a.Lmax1);
-      r.L2 = min(max(r.L2, 0), a.Lmax2);
+    if (a.lengths) {  // never index outside the padded slab
+      r.L1 = min(max(a.lengths[2 * p], 0), a.Lmax1);
+      r.L2 = min(max(a.lengths[2 * p + 1], 0), a.Lmax2);
+    } else {
+      r.L1 = a.Lmax1;
+      r.L2 = a.Lmax2;
     }
   } else {
-    r.L1 = a.Lmax1;
-    r.L2 = a.Lmax2;
+    const int p = a.plan_tasks[2 * task];
+    const int j = a.plan_tasks[2 * task + 1];
+    const long long* q = a.plan_pairs + (size_t)p * PLAN_PAIR_WORDS;
+    w.p = p;
+    w.nb = (int)q[PW_NB];
+    w.band = reverse_band ? w.nb - 1 - j : j;
+    w.slot0 = (size_t)q[PW_SLOT0];
+    r.L1 = (int)q[PW_L1];
+    r.L2 = (int)q[PW_L2];
+    r.ld = (r.L2 + 3) & ~3;
+    w.Lm = r.L1;
+    const int nch = (r.L1 + 31 + C_STEPS - 1) / C_STEPS;
+    w.ckb = (size_t)nch * CKF * 32;
+    w.edb = (size_t)NE * r.L1;
+    w.bpb = (size_t)NP * (r.L1 + 1);
+    w.ck0 = (size_t)q[PW_CK0];
+    w.ed0 = (size_t)q[PW_EDGE0];
+    w.bp0 = (size_t)q[PW_BP0];
+    r.s = a.scores + q[PW_SCORE_OFF];
+    r.m = a.map + q[PW_SCORE_OFF];
   }
-  if (a.layout == 1) r.ld = (r.L2 + 3) & ~3;
   r.vec = ((r.ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(r.s) & 15) == 0) &&
           ((reinterpret_cast<uintptr_t>(r.m) & 15) == 0);
-  return r;
+  return w;
 }
 
 template <int R>
@@ -134,17 +174,20 @@ __device__ __forceinline__ void load_row(const Pair& pr, int i, int jl, bool ok,
   }
 }
 
+// Writes row i of the map for the lane's columns; columns in [L2, ld) (row
+// pitch padding) receive 0, so a packed map needs no separate clearing.
 template <int R>
 __device__ __forceinline__ void store_row(const Pair& pr, int i, int jl, const float (&v)[R]) {
   float* dst = pr.m + (size_t)(i - 1) * pr.ld + jl;
-  if (R == 4 && pr.vec && jl + 4 <= pr.L2) {
-    *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
-  } else if (R == 2 && pr.vec && jl + 2 <= pr.L2) {
-    *reinterpret_cast<float2*>(dst) = make_float2(v[0], v[1]);
+  if (R == 4 && pr.vec && jl + 4 <= pr.ld) {
+    *reinterpret_cast<float4*>(dst) = make_float4(jl + 0 < pr.L2 ? v[0] : 0.f, jl + 1 < pr.L2 ? v[1] : 0.f,
+                                                  jl + 2 < pr.L2 ? v[2] : 0.f, jl + 3 < pr.L2 ? v[3] : 0.f);
+  } else if (R == 2 && pr.vec && jl + 2 <= pr.ld) {
+    *reinterpret_cast<float2*>(dst) = make_float2(jl + 0 < pr.L2 ? v[0] : 0.f, jl + 1 < pr.L2 ? v[1] : 0.f);
   } else {
 #pragma unroll
     for (int c = 0; c < R; ++c)
-      if (jl + c < pr.L2) dst[c] = v[c];
+      if (jl + c < pr.ld) dst[c] = (jl + c < pr.L2) ? v[c] : 0.f;
   }
 }
 
@@ -266,12 +309,13 @@ __device__ __forceinline__ int band_chunks(int L1) { return (L1 + 31 + C_STEPS -
 // ---------------------------------------------------------------------------
 
 template <int NS, int R>
-__device__ void fwd_band(const Args& a, int p, int band, int lane, uint64_t deadline) {
+__device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadline) {
   using D = Dims<NS, R>;
   constexpr int NE = D::NE;
-  const Pair pr = pair_of(a, p);
+  const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
-  const int slot = p * a.nb + band;
+  const int band = w.band;
+  const size_t slot = w.slot0 + band;
   const int col0 = band * 32 * R;
   float* part = a.part + 2 * (size_t)slot;
   if (!(L1 > 0 && col0 < L2)) {
@@ -280,12 +324,12 @@ __device__ void fwd_band(const Args& a, int p, int band, int lane, uint64_t dead
   }
   const int jl = col0 + lane * R;
   const float k = a.k, g0 = a.go * k, g1 = a.ge * k;
-  const size_t Lm = (size_t)a.Lmax1;
-  float* eout = a.edge + (size_t)slot * NE * Lm;
-  const float* ein = (band > 0) ? a.edge + (size_t)(slot - 1) * NE * Lm : nullptr;
+  const size_t Lm = (size_t)w.Lm;
+  float* eout = a.edge + w.ed0 + (size_t)band * w.edb;
+  const float* ein = (band > 0) ? eout - w.edb : nullptr;
   const bool fault = a.fault_inject && band > 0;
   if (fault) ein = nullptr;
-  float* ck = a.ckpt + (size_t)slot * a.nchunks * D::CKF * 32;
+  float* ck = a.ckpt + w.ck0 + (size_t)band * w.ckb;
   const int nch = band_chunks(L1);
 
   float ph[NS][R], pl[NS][R], lh[NS], ll[NS];
@@ -428,15 +472,13 @@ template <int NS, int R>
 __global__ void __launch_bounds__(128) fwd_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
-  const int ntasks = a.B * a.nb;
+  const int ntasks = (a.layout == 0) ? a.B * a.nb : a.ntasks;
   while (true) {
     int task = 0;
     if (lane == 0) task = (int)atomicAdd(a.counters + 0, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    int p = task / a.nb, band = task - p * a.nb;
-    if (a.order) p = a.order[p];
-    fwd_band<NS, R>(a, p, band, lane, deadline);
+    fwd_band<NS, R>(a, place_of<NS, R>(a, task, false), lane, deadline);
   }
 }
 
@@ -446,10 +488,11 @@ __global__ void __launch_bounds__(128) fwd_kernel(Args a) {
 
 // Combine the forward partials of pair p into the scaled log-partition
 // S' = Sh + Sl.
-__device__ __forceinline__ void pair_logz(const Args& a, int p, int lane, float& Sh, float& Sl) {
+__device__ __forceinline__ void pair_logz(const Args& a, const Place& w, int lane, float& Sh,
+                                          float& Sl) {
   float ref = NEG, s = 0.f;
-  for (int b = lane; b < a.nb; b += 32) {
-    const float* q = a.part + 2 * ((size_t)p * a.nb + b);
+  for (int b = lane; b < w.nb; b += 32) {
+    const float* q = a.part + 2 * (w.slot0 + b);
     float r2 = q[0], s2 = q[1];
     if (s2 > 0.f) {
       float m = fmaxf(ref, r2);
@@ -472,18 +515,19 @@ __device__ __forceinline__ void pair_logz(const Args& a, int p, int lane, float&
 // Last band task of a pair to finish folds the per-band gradient partials (in
 // band order, so the result is deterministic) into the outputs.
 template <int NS>
-__device__ void finish_pair(const Args& a, int p, int slot, int lane, float Sh, float Sl,
+__device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, float Sl,
                             float g0sum, float g1sum, float pssum) {
+  const int p = w.p;
   if (lane == 0) {
-    float* gp = a.gpart + 4 * (size_t)slot;
+    float* gp = a.gpart + 4 * (w.slot0 + w.band);
     gp[0] = g0sum; gp[1] = g1sum; gp[2] = pssum; gp[3] = 0.f;
     __threadfence();
     unsigned done = atomicAdd(a.pair_done + p, 1u);
-    if (done == (unsigned)a.nb - 1) {
+    if (done == (unsigned)w.nb - 1) {
       __threadfence();
       float o = 0.f, e = 0.f, ps = 0.f;
-      for (int b = 0; b < a.nb; ++b) {
-        const float* q = a.gpart + 4 * ((size_t)p * a.nb + b);
+      for (int b = 0; b < w.nb; ++b) {
+        const float* q = a.gpart + 4 * (w.slot0 + b);
         o += ld_poll(q + 0);
         e += ld_poll(q + 1);
         ps += ld_poll(q + 2);
@@ -512,28 +556,28 @@ __device__ __forceinline__ float wgt(float ph_, float pl_, float xh, float xl, f
 }
 
 template <int NS, int R>
-__device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, float* ea,
+__device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, float* ea,
                          uint64_t deadline) {
   using D = Dims<NS, R>;
   constexpr int NP = D::NP, EF = D::EF, CKF = D::CKF, NE = D::NE;
-  const Pair pr = pair_of(a, p);
+  const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
-  const int slot = p * a.nb + band;
+  const int band = w.band;
   const int col0 = band * 32 * R;
   float Sh, Sl;
-  pair_logz(a, p, lane, Sh, Sl);
+  pair_logz(a, w, lane, Sh, Sl);
   if (!(L1 > 0 && col0 < L2)) {
-    finish_pair<NS>(a, p, slot, lane, Sh, Sl, 0.f, 0.f, 0.f);
+    finish_pair<NS>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f);
     return;
   }
   const int jl = col0 + lane * R;
   const float k = a.k, g0 = a.go * k, g1 = a.ge * k;
-  const size_t Lm = (size_t)a.Lmax1;
-  const float* ein = (band > 0) ? a.edge + (size_t)(slot - 1) * NE * Lm : nullptr;
-  float* pout = (band > 0) ? a.bpush + (size_t)slot * NP * (Lm + 1) : nullptr;
-  const bool right_live = (col0 + 32 * R) < L2 && (band + 1) < a.nb;
-  const float* pin = right_live ? a.bpush + (size_t)(slot + 1) * NP * (Lm + 1) : nullptr;
-  const float* ck = a.ckpt + (size_t)slot * a.nchunks * CKF * 32;
+  const size_t Lm = (size_t)w.Lm;
+  const float* ein = (band > 0) ? a.edge + w.ed0 + (size_t)(band - 1) * w.edb : nullptr;
+  float* pout = (band > 0) ? a.bpush + w.bp0 + (size_t)band * w.bpb : nullptr;
+  const bool right_live = (col0 + 32 * R) < L2 && (band + 1) < w.nb;
+  const float* pin = right_live ? a.bpush + w.bp0 + (size_t)(band + 1) * w.bpb : nullptr;
+  const float* ck = a.ckpt + w.ck0 + (size_t)band * w.ckb;
   const int nch = band_chunks(L1);
   const int left_lane = (lane + 31) & 31;
 
@@ -844,7 +888,7 @@ __device__ void bwd_band(const Args& a, int p, int band, int lane, float* sm, fl
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
   }
-  finish_pair<NS>(a, p, slot, lane, Sh, Sl, v0, v1, v2);
+  finish_pair<NS>(a, w, lane, Sh, Sl, v0, v1, v2);
 }
 
 // Shared memory per adjoint warp (floats): recomputed entries + lane-0 edges.
@@ -861,16 +905,13 @@ __global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
   float* sm = smem + (size_t)w * bwd_smem_floats<NS, R>();
   float* ea = sm + (C_STEPS + 1) * Dims<NS, R>::EF * 32;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
-  const int ntasks = a.B * a.nb;
+  const int ntasks = (a.layout == 0) ? a.B * a.nb : a.ntasks;
   while (true) {
     int task = 0;
     if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    int p = task / a.nb;
-    const int band = a.nb - 1 - (task - p * a.nb);
-    if (a.order) p = a.order[p];
-    bwd_band<NS, R>(a, p, band, lane, sm, ea, deadline);
+    bwd_band<NS, R>(a, place_of<NS, R>(a, task, true), lane, sm, ea, deadline);
   }
 }
 

@@ -50,6 +50,14 @@ constexpr int C_STEPS = 8;              // checkpoint stride (steps)
 constexpr int PF = 4;                   // score prefetch distance (steps); C_STEPS % PF == 0
 constexpr uint32_t SENTINEL_BITS = 0xffffffffu;
 
+// Ragged plan: per-pair words.  Offsets are in floats within the respective
+// workspace array; score_off is the pair's element offset in the packed
+// score/map buffers (row pitch = L2 rounded up to a multiple of 4).
+enum PlanWord : int {
+  PW_SCORE_OFF = 0, PW_L1 = 1, PW_L2 = 2, PW_SLOT0 = 3, PW_NB = 4,
+  PW_CK0 = 5, PW_EDGE0 = 6, PW_BP0 = 7, PLAN_PAIR_WORDS = 8
+};
+
 enum : unsigned {
   ERR_WAIT_TIMEOUT = 1u,
 };
@@ -60,10 +68,12 @@ struct Args {
   const float* scores;        // layout 0: [B, Lmax1, Lmax2]; layout 1: flat ragged
   float* map;                 // same layout as scores
   const int* lengths;         // [B, 2] or null (= full padded lengths)
-  const long long* offsets;   // layout 1: [B+1] element offsets (multiples of 4)
-  const int* order;           // optional pair order of the task queue (null = 0..B-1)
+  const int* order;           // layout 0: optional pair order of the task queue (null = 0..B-1)
+  const long long* plan_pairs;// layout 1: [B][PLAN_PAIR_WORDS] per-pair placement (see below)
+  const int* plan_tasks;      // layout 1: [ntasks][2] (pair, band) in queue order
+  int ntasks;                 // layout 1: number of band tasks
   int B, Lmax1, Lmax2;
-  int layout;                 // 0 padded, 1 ragged packed (row pitch = round4(L2))
+  int layout;                 // 0 padded, 1 ragged packed via plan (row pitch = round4(L2))
   float go, ge, T, k;         // gaps in natural units, temperature, k = log2(e)/T
   int nb;                     // bands per pair (uniform, >= ceil(max L2 / 32R))
   int nchunks;                // checkpoint chunks per band (>= ceil((max L1+31)/C))

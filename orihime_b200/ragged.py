@@ -1,0 +1,178 @@
+"""Packed ragged batches of soft Smith-Waterman pairs.
+
+The reference evaluates a batch of pairs of different lengths as one padded
+[B, L1max, L2max] tensor (with ``lengths`` or a mask).  This module runs the
+same DP over a *packed* batch: every pair's scores are stored at their own
+size, one persistent kernel pair (forward + checkpointed adjoint) pulls band
+tasks longest pair first, and the whole call can be captured in a CUDA graph.
+
+Packing (``pack``): pair b is an L1_b x L2_b row-major block with row pitch
+round_up(L2_b, 4) at element offset ``offsets[b]`` (a multiple of 4) of one
+flat float32 buffer.  The map comes back in the same packing.
+
+    flat, offsets, lengths = ragged.pack([s0, s1, ...])      # CPU or CUDA tensors
+    plan = ragged.Plan(lengths, offsets, family="affine", device="cuda")
+    out = plan.run(flat.cuda(), gap_open=-2.0, gap_ext=-0.5, temp=0.5)
+    out.value, out.map, out.grad_open, out.grad_ext, out.grad_temp
+    maps = ragged.unpack(out.map, offsets, lengths)
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_FAMILY = {"affine": 3, "linear": 1}
+
+
+def pitch_of(L2: int) -> int:
+    return (int(L2) + 3) & ~3
+
+
+def layout(lengths) -> tuple[np.ndarray, np.ndarray]:
+    """int64 offsets [B+1] and int32 lengths [B, 2] of the packing of ``lengths``."""
+    ln = np.asarray(lengths, dtype=np.int64).reshape(-1, 2)
+    sizes = ln[:, 0] * ((ln[:, 1] + 3) & ~3)
+    offsets = np.zeros(len(ln) + 1, dtype=np.int64)
+    np.cumsum(sizes, out=offsets[1:])
+    return offsets, ln.astype(np.int32)
+
+
+def pack(mats: Sequence[torch.Tensor]) -> tuple[torch.Tensor, np.ndarray, np.ndarray]:
+    """Pack 2-D float32 score matrices into (flat, offsets [B+1], lengths [B, 2])."""
+    lengths = [(int(m.shape[0]), int(m.shape[1])) for m in mats]
+    offsets, ln = layout(lengths)
+    dev = mats[0].device if len(mats) else torch.device("cpu")
+    flat = torch.zeros(int(offsets[-1]), dtype=torch.float32, device=dev)
+    for b, m in enumerate(mats):
+        L1, L2 = lengths[b]
+        if L1 * L2 == 0:
+            continue
+        p = pitch_of(L2)
+        view = flat[int(offsets[b]):int(offsets[b]) + L1 * p].view(L1, p)
+        view[:, :L2] = m.to(device=dev, dtype=torch.float32)
+    return flat, offsets, ln
+
+
+def unpack(flat: torch.Tensor, offsets, lengths) -> list[torch.Tensor]:
+    """Views [L1_b, L2_b] of each pair in a packed buffer."""
+    out = []
+    for b, (L1, L2) in enumerate(np.asarray(lengths).reshape(-1, 2).tolist()):
+        p = pitch_of(L2)
+        o = int(offsets[b])
+        out.append(flat[o:o + L1 * p].view(L1, p)[:, :L2])
+    return out
+
+
+@dataclass
+class Result:
+    value: torch.Tensor      # [B]
+    map: torch.Tensor        # packed, like the scores
+    grad_open: torch.Tensor  # [B]  (linear: dS/dgap)
+    grad_ext: Optional[torch.Tensor]
+    grad_temp: torch.Tensor  # [B]
+
+
+class Plan:
+    """Launch plan of one packed batch layout (reusable across calls).
+
+    Builds the host plan with the C ABI (validation, longest-pair-first task
+    order, workspace placement), copies it to the device once and owns the
+    workspace, so repeated calls allocate nothing and can be graph-captured.
+    """
+
+    def __init__(self, lengths, offsets, family: str = "affine", device="cuda"):
+        if family not in _FAMILY:
+            raise ValueError(f"family must be 'affine' or 'linear', got {family!r}")
+        self.family = family
+        self.lib = _lib.load()
+        ln = np.ascontiguousarray(np.asarray(lengths, dtype=np.int32).reshape(-1, 2))
+        off = np.ascontiguousarray(np.asarray(offsets, dtype=np.int64).reshape(-1))
+        B = ln.shape[0]
+        if off.shape[0] != B + 1:
+            raise ValueError(f"offsets must have B+1 = {B + 1} entries, got {off.shape[0]}")
+        self.B = B
+        self.lengths = ln
+        self.offsets = off
+        self.cells = int((ln[:, 0].astype(np.int64) * ln[:, 1]).sum())
+        pb, wb = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        fam = _FAMILY[family]
+        rc = self.lib.swb_ragged_plan(fam, ln.ctypes.data, off.ctypes.data, B, None, 0,
+                                      ctypes.byref(pb), ctypes.byref(wb))
+        if rc != _lib.OK:
+            raise ValueError("invalid packed batch: lengths must be >= 0 and offsets multiples of 4 "
+                             "with room for L1 * round_up(L2, 4) elements per pair")
+        self.host_plan = np.zeros(pb.value // 8 + 1, dtype=np.int64)
+        rc = self.lib.swb_ragged_plan(fam, ln.ctypes.data, off.ctypes.data, B,
+                                      self.host_plan.ctypes.data, self.host_plan.nbytes,
+                                      ctypes.byref(pb), ctypes.byref(wb))
+        _lib.check(rc, "swb_ragged_plan")
+        self.device = torch.device(device)
+        self.dev_plan = torch.from_numpy(self.host_plan.view(np.uint8)).to(self.device)
+        self.workspace_bytes = wb.value
+        self.workspace = torch.empty(max(wb.value, 1), dtype=torch.uint8, device=self.device)
+        self.map_elems = int(off[-1]) if B else 0
+
+    def outputs(self) -> Result:
+        dev = self.device
+        e = lambda: torch.empty(self.B, dtype=torch.float32, device=dev)
+        return Result(e(), torch.empty(self.map_elems, dtype=torch.float32, device=dev), e(),
+                      e() if self.family == "affine" else None, e())
+
+    def run(self, flat: torch.Tensor, *, gap_open: float = 0.0, gap_ext: float = 0.0,
+            gap: float = 0.0, temp: float = 1.0, out: Optional[Result] = None,
+            options: Optional[_lib.Options] = None) -> Result:
+        """One forward + adjoint over the packed batch (asynchronous)."""
+        if flat.device != self.device or flat.dtype != torch.float32 or not flat.is_contiguous():
+            raise ValueError("scores must be a contiguous float32 tensor on the plan's device")
+        if flat.numel() < self.map_elems:
+            raise ValueError(f"scores has {flat.numel()} elements, the packing needs {self.map_elems}")
+        if not (temp > 0):
+            raise ValueError("temperature must be finite and strictly positive")
+        out = out or self.outputs()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        hp = self.host_plan.ctypes.data
+        dp = self.dev_plan.data_ptr()
+        ws = self.workspace.data_ptr()
+        with torch.cuda.device(self.device):
+            if self.family == "affine":
+                rc = self.lib.swb_sw_affine_ragged(
+                    flat.data_ptr(), hp, dp, float(gap_open), float(gap_ext), float(temp),
+                    out.value.data_ptr(), out.map.data_ptr(), out.grad_open.data_ptr(),
+                    out.grad_ext.data_ptr(), out.grad_temp.data_ptr(), ws, self.workspace_bytes,
+                    st, options)
+            else:
+                rc = self.lib.swb_sw_ragged(
+                    flat.data_ptr(), hp, dp, float(gap), float(temp), out.value.data_ptr(),
+                    out.map.data_ptr(), out.grad_open.data_ptr(), out.grad_temp.data_ptr(), ws,
+                    self.workspace_bytes, st, options)
+        _lib.check(rc, "ragged soft Smith-Waterman")
+        return out
+
+    def status(self) -> int:
+        st = ctypes.c_uint(0)
+        rc = self.lib.swb_read_status(self.workspace.data_ptr(),
+                                      torch.cuda.current_stream(self.device).cuda_stream,
+                                      ctypes.byref(st))
+        _lib.check(rc, "swb_read_status")
+        return st.value
+
+    def graph(self, flat: torch.Tensor, **params) -> tuple[torch.cuda.CUDAGraph, Result]:
+        """Capture one call on static buffers; replay with ``g.replay()`` after
+        writing new scores into ``flat``."""
+        out = self.outputs()
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.run(flat, out=out, **params)  # warm-up outside capture (device info, modules)
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.run(flat, out=out, **params)
+        return g, out

@@ -1,0 +1,72 @@
+"""Host-side ragged plan: packing helpers and the C ABI plan builder (CPU)."""
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from orihime_b200 import _lib, ragged
+
+
+def _plan(lengths, offsets, family=3):
+    lib = _lib.load()
+    ln = np.ascontiguousarray(np.asarray(lengths, np.int32).reshape(-1, 2))
+    off = np.ascontiguousarray(np.asarray(offsets, np.int64))
+    pb, wb = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    rc = lib.swb_ragged_plan(family, ln.ctypes.data, off.ctypes.data, len(ln), None, 0,
+                             ctypes.byref(pb), ctypes.byref(wb))
+    if rc != 0:
+        return rc, None
+    buf = np.zeros(pb.value // 8 + 1, np.int64)
+    rc = lib.swb_ragged_plan(family, ln.ctypes.data, off.ctypes.data, len(ln), buf.ctypes.data,
+                             buf.nbytes, ctypes.byref(pb), ctypes.byref(wb))
+    return rc, buf
+
+
+def test_pack_unpack_roundtrip():
+    g = torch.Generator().manual_seed(0)
+    mats = [torch.randn(a, b, generator=g) for a, b in [(3, 5), (0, 7), (9, 0), (1, 1), (17, 130)]]
+    flat, off, ln = ragged.pack(mats)
+    assert np.all(off % 4 == 0)
+    assert ln.tolist() == [[3, 5], [0, 7], [9, 0], [1, 1], [17, 130]]
+    for m, v in zip(mats, ragged.unpack(flat, off, ln)):
+        assert torch.equal(m, v)
+
+
+def test_plan_orders_longest_first_and_places_bands():
+    lengths = [[10, 20], [100, 300], [0, 5], [64, 129], [5, 600]]
+    off, ln = ragged.layout(lengths)
+    rc, buf = _plan(ln, off)
+    assert rc == 0
+    B = len(ln)
+    hdr = buf[:10]
+    pairs = buf[10:10 + 8 * B].reshape(B, 8)
+    tasks = buf[10 + 8 * B:].view(np.int32)[:2 * hdr[2]].reshape(-1, 2)
+    cells = [a * b for a, b in lengths]
+    first_of_pair = []
+    for p, _ in tasks:
+        if p not in first_of_pair:
+            first_of_pair.append(int(p))
+    assert first_of_pair == sorted(range(B), key=lambda b: -cells[b])
+    nb = [max(1, -(-b // 128)) for _, b in lengths]
+    assert hdr[2] == sum(nb)
+    for p in range(B):
+        assert pairs[p, 4] == nb[p]
+        bands = [int(j) for q, j in tasks if q == p]
+        assert bands == list(range(nb[p]))
+        assert pairs[p, 0] == off[p]
+
+
+@pytest.mark.parametrize("bad", ["misaligned", "overlap", "negative"])
+def test_plan_rejects_bad_packing(bad):
+    lengths = np.array([[4, 6], [3, 9]], np.int32)
+    off, _ = ragged.layout(lengths)
+    if bad == "misaligned":
+        off = off + np.array([0, 2, 2])
+    elif bad == "overlap":
+        off[1] -= 4
+    else:
+        lengths[1, 0] = -1
+    rc, _ = _plan(lengths, off)
+    assert rc == _lib.ERR_ARG
