@@ -276,6 +276,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--pairs", type=int, default=NPAIRS, help="pairs per GPU (profiling cases)")
+    ap.add_argument("--cols-per-lane", type=int, default=0, help="band columns per lane (2 or 4)")
     ap.add_argument("--quick", action="store_true",
                     help="timed steps only: no e2e, plain, CPU legs (profiling cases)")
     args = ap.parse_args()
@@ -296,7 +297,7 @@ def main():
     offsets, ln32 = ragged.layout(lengths)
     cells = int((lengths[:, 0] * lengths[:, 1]).sum())
     flat = make_scores(torch, lengths, offsets, 3 + rank, dev)
-    plan = ragged.Plan(ln32, offsets, family="affine", device=dev)
+    plan = ragged.Plan(ln32, offsets, family="affine", device=dev, cols_per_lane=args.cols_per_lane)
     out = plan.outputs()
 
     def step():
@@ -316,7 +317,7 @@ def main():
         for e_ in trio:
             e_.record()
     torch.cuda.synchronize()
-    opts = [_lib.Options(0, 0, 0, trio[1].cuda_event) for trio in ev]
+    opts = [_lib.Options(0, 0, 0, trio[1].cuda_event, 0) for trio in ev]
     with ClockSampler(local) as clk:
         barrier(torch, world)
         torch.cuda.synchronize()
@@ -342,7 +343,8 @@ def main():
 
     if args.quick:
         if rank == 0:
-            print(json.dumps({"quick": True, "pairs": args.pairs, "cells": cells, "ms_per_step": ms,
+            print(json.dumps({"quick": True, "pairs": args.pairs, "cols_per_lane": args.cols_per_lane,
+                              "cells": cells, "ms_per_step": ms,
                               "gcups": gcups_all, "kernel_ms": kernel_split}))
         return 0
 

@@ -51,6 +51,7 @@ typedef struct swb_options {
     int fault_inject;                  /* 1: band>0 waits on a word nobody writes (tests) */
     void* split_event;                 /* cudaEvent_t recorded between the forward and the
                                           adjoint kernel (per-kernel timing), or NULL     */
+    int cols_per_lane;                 /* columns per lane of a band: 2 or 4 (0 = default) */
 } swb_options;
 
 /* Workspace bytes for swb_sw_affine_forward on a [B, L1max, L2max] batch. */
@@ -103,10 +104,11 @@ int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, in
  * places every band's workspace slice.  Call it once with plan = NULL to get
  * *plan_bytes (and *workspace_bytes), then with a buffer of that size; copy
  * the plan bytes to the device unchanged and pass both copies to the launch.
- * family: 3 = affine, 1 = linear.  host lengths [B, 2], host offsets [B+1].
+ * family: 3 = affine, 1 = linear; cols_per_lane: 2 or 4 (0 = default).
+ * host lengths [B, 2], host offsets [B+1].
  */
-int swb_ragged_plan(int family, const int* lengths, const long long* offsets, int B,
-                    void* plan, size_t plan_capacity, size_t* plan_bytes,
+int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const long long* offsets,
+                    int B, void* plan, size_t plan_capacity, size_t* plan_bytes,
                     size_t* workspace_bytes);
 
 /* Affine soft Smith–Waterman over a packed ragged batch; outputs as

@@ -30,6 +30,7 @@ class Options(ctypes.Structure):
         ("spin_limit_ns", ctypes.c_ulonglong),
         ("fault_inject", ctypes.c_int),
         ("split_event", ctypes.c_void_p),
+        ("cols_per_lane", ctypes.c_int),
     ]
 
 
@@ -69,7 +70,7 @@ def load() -> ctypes.CDLL:
     lib.swb_read_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_uint)]
     ll = ctypes.c_longlong
     lib.swb_ragged_plan.restype = i
-    lib.swb_ragged_plan.argtypes = [i, vp, vp, i, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]
+    lib.swb_ragged_plan.argtypes = [i, i, vp, vp, i, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]
     lib.swb_sw_affine_ragged.restype = i
     lib.swb_sw_affine_ragged.argtypes = [vp, vp, vp, f, f, f, vp, vp, vp, vp, vp, vp, sz, vp,
                                          ctypes.POINTER(Options)]

@@ -21,16 +21,21 @@ namespace {
 
 using swb::Args;
 
-constexpr int kR = 4;                 // columns per lane
+constexpr int kDefaultR = 4;          // columns per lane unless the caller picks another
 constexpr int kWarpsFwd = 4;          // forward CTA: 4 independent warps
 constexpr int kWarpsBwd = 1;          // adjoint CTA: 1 warp (shared memory bound)
 constexpr size_t kAlign = 256;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
-template <int NS> constexpr int np() { return swb::Dims<NS, kR>::NP; }
-template <int NS> constexpr int ckf() { return swb::Dims<NS, kR>::CKF; }
-template <int NS> constexpr int ne() { return swb::Dims<NS, kR>::NE; }
+template <int NS, int R> constexpr int np() { return swb::Dims<NS, R>::NP; }
+template <int NS, int R> constexpr int ckf() { return swb::Dims<NS, R>::CKF; }
+template <int NS, int R> constexpr int ne() { return swb::Dims<NS, R>::NE; }
+
+bool valid_r(int r) { return r == 2 || r == 4; }
+int pick_r(const swb_options* opt) {
+  return (opt && opt->cols_per_lane) ? opt->cols_per_lane : kDefaultR;
+}
 
 struct Layout {
   int nb, nchunks;
@@ -60,15 +65,15 @@ Layout layout_sizes(long long B, size_t slots, size_t edge_floats, size_t bp_flo
 int chunks_for(long long L1) { return (int)((L1 + 31 + swb::C_STEPS - 1) / swb::C_STEPS); }
 
 // Padded batch: every pair gets the slices of a Lmax1 x Lmax2 pair.
-template <int NS>
+template <int NS, int R>
 Layout layout_for(long long B, long long L1m, long long L2m) {
-  int nb = (int)((L2m + 32 * kR - 1) / (32 * kR));
+  int nb = (int)((L2m + 32 * R - 1) / (32 * R));
   if (nb < 1) nb = 1;
   const int nch = chunks_for(L1m);
   const size_t slots = (size_t)B * nb;
-  Layout l = layout_sizes(B, slots, slots * ne<NS>() * (size_t)L1m,
-                          slots * np<NS>() * (size_t)(L1m + 1),
-                          slots * (size_t)nch * ckf<NS>() * 32);
+  Layout l = layout_sizes(B, slots, slots * ne<NS, R>() * (size_t)L1m,
+                          slots * np<NS, R>() * (size_t)(L1m + 1),
+                          slots * (size_t)nch * ckf<NS, R>() * 32);
   l.nb = nb;
   l.nchunks = nch;
   return l;
@@ -87,17 +92,31 @@ size_t plan_bytes_for(long long B, long long ntasks) {
          sizeof(int) * 2 * (size_t)ntasks;
 }
 
+// Occupancy of each kernel instantiation on one device, computed once.
 struct DevInfo {
   int sms = 0;
-  int occ_fwd[2] = {0, 0};   // [linear, affine]
-  int occ_bwd[2] = {0, 0};
+  int occ[2][2][2] = {};   // [kernel fwd/bwd][NS affine?][R == 4?]
   bool ready = false;
 };
 DevInfo g_dev[64];
 std::mutex g_mu;
 
-template <int NS>
-size_t bwd_smem() { return (size_t)kWarpsBwd * swb::bwd_smem_floats<NS, kR>() * sizeof(float); }
+template <int NS, int R>
+size_t bwd_smem() { return (size_t)kWarpsBwd * swb::bwd_smem_floats<NS, R>() * sizeof(float); }
+
+template <int NS, int R>
+cudaError_t setup_pair(DevInfo& d) {
+  cudaError_t e = cudaFuncSetAttribute(swb::bwd_kernel<NS, R, kWarpsBwd>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bwd_smem<NS, R>());
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ[0][NS == 3][R == 4],
+                                                    swb::fwd_kernel<NS, R>, 32 * kWarpsFwd, 0);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &d.occ[1][NS == 3][R == 4], swb::bwd_kernel<NS, R, kWarpsBwd>, 32 * kWarpsBwd,
+      bwd_smem<NS, R>());
+}
 
 int dev_info(DevInfo** out) {
   int dev = 0;
@@ -107,19 +126,7 @@ int dev_info(DevInfo** out) {
   if (!d.ready) {
     if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       return SWB_ERR_CUDA;
-    if (cudaFuncSetAttribute(swb::bwd_kernel<3, kR, kWarpsBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)bwd_smem<3>()) != cudaSuccess)
-      return SWB_ERR_CUDA;
-    if (cudaFuncSetAttribute(swb::bwd_kernel<1, kR, kWarpsBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)bwd_smem<1>()) != cudaSuccess)
-      return SWB_ERR_CUDA;
-    const int tf = 32 * kWarpsFwd, tb = 32 * kWarpsBwd;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_fwd[0], swb::fwd_kernel<1, kR>, tf, 0) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_fwd[1], swb::fwd_kernel<3, kR>, tf, 0) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_bwd[0], swb::bwd_kernel<1, kR, kWarpsBwd>, tb,
-                                                      bwd_smem<1>()) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_bwd[1], swb::bwd_kernel<3, kR, kWarpsBwd>, tb,
-                                                      bwd_smem<3>()))
+    if (setup_pair<1, 2>(d) || setup_pair<1, 4>(d) || setup_pair<3, 2>(d) || setup_pair<3, 4>(d))
       return SWB_ERR_CUDA;
     d.ready = true;
   }
@@ -128,7 +135,7 @@ int dev_info(DevInfo** out) {
 }
 
 // Common launch: per-call resets, then the forward and adjoint kernels.
-template <int NS>
+template <int NS, int R>
 int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool clear_map, void* ws,
            size_t ws_bytes, void* stream_v, const swb_options* opt) {
   if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
@@ -158,8 +165,9 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
       cudaMemsetAsync(a.map, 0, map_elems * sizeof(float), st) != cudaSuccess)
     return SWB_ERR_CUDA;
 
-  const int cta_cap_f = d->sms * (d->occ_fwd[NS == 3] > 0 ? d->occ_fwd[NS == 3] : 1);
-  const int cta_cap_b = d->sms * (d->occ_bwd[NS == 3] > 0 ? d->occ_bwd[NS == 3] : 1);
+  const int of = d->occ[0][NS == 3][R == 4], ob = d->occ[1][NS == 3][R == 4];
+  const int cta_cap_f = d->sms * (of > 0 ? of : 1);
+  const int cta_cap_b = d->sms * (ob > 0 ? ob : 1);
   const long long need_f = (ntasks + kWarpsFwd - 1) / kWarpsFwd;
   const long long need_b = (ntasks + kWarpsBwd - 1) / kWarpsBwd;
   int grid_f = (int)(need_f < cta_cap_f ? need_f : cta_cap_f);
@@ -170,34 +178,48 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   }
   if (grid_f < 1) grid_f = 1;
   if (grid_b < 1) grid_b = 1;
-  swb::fwd_kernel<NS, kR><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
+  swb::fwd_kernel<NS, R><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   if (opt && opt->split_event &&
       cudaEventRecord(reinterpret_cast<cudaEvent_t>(opt->split_event), st) != cudaSuccess)
     return SWB_ERR_CUDA;
-  swb::bwd_kernel<NS, kR, kWarpsBwd><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS>(), st>>>(a);
+  swb::bwd_kernel<NS, R, kWarpsBwd><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS, R>(), st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   return SWB_OK;
 }
 
-template <int NS>
-int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
-                  float ge, float T, float* value, float* map, float* g_open, float* g_ext,
-                  float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
+template <int NS, int R>
+int launch_padded_r(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
+                    float ge, float T, float* value, float* map, float* g_open, float* g_ext,
+                    float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
   if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   if (B == 0) return SWB_OK;
   const size_t map_elems = (size_t)B * L1m * L2m;
   if (!value || !g_open || !g_T || (NS == 3 && !g_ext)) return SWB_ERR_ARG;
   if (map_elems > 0 && (!scores || !map)) return SWB_ERR_ARG;
-  const Layout l = layout_for<NS>(B, L1m, L2m);
+  const Layout l = layout_for<NS, R>(B, L1m, L2m);
   Args a{};
   a.scores = scores; a.map = map; a.lengths = lengths;
   a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
   a.go = go; a.ge = ge; a.T = T;
   a.nb = l.nb; a.nchunks = l.nchunks;
   a.value = value; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
-  return launch<NS>(a, l, (long long)B * l.nb, map_elems, true, ws, ws_bytes, stream, opt);
+  return launch<NS, R>(a, l, (long long)B * l.nb, map_elems, true, ws, ws_bytes, stream, opt);
+}
+
+template <int NS>
+int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
+                  float ge, float T, float* value, float* map, float* g_open, float* g_ext,
+                  float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
+  const int r = pick_r(opt);
+  if (r == 2)
+    return launch_padded_r<NS, 2>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
+                                  g_ext, g_T, ws, ws_bytes, stream, opt);
+  if (r == 4)
+    return launch_padded_r<NS, 4>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
+                                  g_ext, g_T, ws, ws_bytes, stream, opt);
+  return SWB_ERR_ARG;
 }
 
 template <int NS>
@@ -206,7 +228,8 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
                   float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
   if (!host_plan || !dev_plan) return SWB_ERR_ARG;
   const long long* h = static_cast<const long long*>(host_plan);
-  if (h[HW_MAGIC] != kPlanMagic || h[HW_FAMILY] != NS) return SWB_ERR_ARG;
+  if (h[HW_MAGIC] != kPlanMagic || (h[HW_FAMILY] & 0xff) != NS) return SWB_ERR_ARG;
+  const int r = (int)(h[HW_FAMILY] >> 8);
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   const long long B = h[HW_B], ntasks = h[HW_NTASKS];
   if (B == 0) return SWB_OK;
@@ -223,7 +246,9 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
   a.B = (int)B; a.layout = 1;
   a.go = go; a.ge = ge; a.T = T;
   a.value = value; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
-  return launch<NS>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt);
+  if (r == 2) return launch<NS, 2>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt);
+  if (r == 4) return launch<NS, 4>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt);
+  return SWB_ERR_ARG;
 }
 
 }  // namespace
@@ -232,12 +257,12 @@ extern "C" {
 
 size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;
-  return layout_for<3>(B, L1max, L2max).total;
+  return std::max(layout_for<3, 2>(B, L1max, L2max).total, layout_for<3, 4>(B, L1max, L2max).total);
 }
 
 size_t swb_sw_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;
-  return layout_for<1>(B, L1max, L2max).total;
+  return std::max(layout_for<1, 2>(B, L1max, L2max).total, layout_for<1, 4>(B, L1max, L2max).total);
 }
 
 int swb_sw_affine_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
@@ -256,12 +281,13 @@ int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, in
                           nullptr, grad_temp, workspace, workspace_bytes, stream, opt);
 }
 
-int swb_ragged_plan(int family, const int* lengths, const long long* offsets, int B,
-                    void* plan, size_t plan_capacity, size_t* plan_bytes,
+int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const long long* offsets,
+                    int B, void* plan, size_t plan_capacity, size_t* plan_bytes,
                     size_t* workspace_bytes) {
-  if ((family != 1 && family != 3) || B < 0 || (B > 0 && (!lengths || !offsets)))
+  const int R = cols_per_lane ? cols_per_lane : kDefaultR;
+  if ((family != 1 && family != 3) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
     return SWB_ERR_ARG;
-  const int NE = 2 * family, NP = (family == 3) ? 5 : 2, CKF = 2 * family * kR + 2 * family;
+  const int NE = 2 * family, NP = (family == 3) ? 5 : 2, CKF = 2 * family * R + 2 * family;
   // validate the packing: row pitch round4(L2), offsets multiples of 4 floats
   long long ntasks = 0;
   for (int b = 0; b < B; ++b) {
@@ -270,7 +296,7 @@ int swb_ragged_plan(int family, const int* lengths, const long long* offsets, in
     const long long pitch = (L2 + 3) & ~3LL;
     if (offsets[b] < 0 || (offsets[b] & 3) || offsets[b + 1] - offsets[b] < L1 * pitch)
       return SWB_ERR_ARG;
-    long long nb = (L2 + 32 * kR - 1) / (32 * kR);
+    long long nb = (L2 + 32 * R - 1) / (32 * R);
     ntasks += nb < 1 ? 1 : nb;
   }
   const size_t need = plan_bytes_for(B, ntasks);
@@ -297,7 +323,7 @@ int swb_ragged_plan(int family, const int* lengths, const long long* offsets, in
   long long t = 0;
   for (int b : order) {
     const long long L1 = lengths[2 * b], L2 = lengths[2 * b + 1];
-    long long nb = (L2 + 32 * kR - 1) / (32 * kR);
+    long long nb = (L2 + 32 * R - 1) / (32 * R);
     if (nb < 1) nb = 1;
     if (pw) {
       long long* q = pw + (size_t)b * swb::PLAN_PAIR_WORDS;
@@ -321,7 +347,7 @@ int swb_ragged_plan(int family, const int* lengths, const long long* offsets, in
   if (pw) {
     h[HW_MAGIC] = kPlanMagic; h[HW_B] = B; h[HW_NTASKS] = ntasks; h[HW_SLOTS] = (long long)slots;
     h[HW_CK] = (long long)ck; h[HW_EDGE] = (long long)ed; h[HW_BP] = (long long)bp;
-    h[HW_FAMILY] = family; h[HW_MAP_ELEMS] = B > 0 ? offsets[B] : 0; h[9] = 0;
+    h[HW_FAMILY] = family | (R << 8); h[HW_MAP_ELEMS] = B > 0 ? offsets[B] : 0; h[9] = 0;
   }
   return SWB_OK;
 }

@@ -375,9 +375,11 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
       }
     }
     if (kc + 1 < nch) load_edge(kc + 1, ebn);
+#pragma unroll 1
+    for (int u0 = 0; u0 < C_STEPS; u0 += PF)
 #pragma unroll
-    for (int cu = 0; cu < C_STEPS; ++cu) {
-      const int u = cu % PF;
+    for (int u = 0; u < PF; ++u) {
+      const int cu = u0 + u;
       const int t = kc * C_STEPS + cu;
       const int i = t - lane + 1;
       const bool act = (i >= 1) && (i <= L1);
@@ -389,22 +391,31 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
       }
 #pragma unroll
       for (int f = 0; f < NE; ++f) ev[f] = __shfl_sync(FULL, eb[f], cu);
-      if (lane == 0) {
-        if (fault && act) {
+      // lane 0 takes the left band's values; a value still at the sentinel
+      // (producer not there yet) is polled on a warp-uniform slow path
+      bool miss = false;
+#pragma unroll
+      for (int f = 0; f < NE; ++f) miss |= is_sentinel(ev[f]);
+      miss = (lane == 0) && ein && act && miss;
+      if (__any_sync(FULL, miss) || fault) {
+        if (lane == 0 && fault && act) {
           float v = poll_value(a.never_written, ld_poll(a.never_written), deadline, a.status, NEG);
 #pragma unroll
-          for (int q = 0; q < NS; ++q) { xh[q] = v; xl[q] = 0.f; }
-        } else if (ein && act) {
+          for (int f = 0; f < NE; ++f) ev[f] = (f < NS) ? v : 0.f;
+        } else if (miss) {
 #pragma unroll
           for (int f = 0; f < NE; ++f)
             if (is_sentinel(ev[f]))
               ev[f] = poll_value(ein + f * Lm + (i - 1), ld_poll(ein + f * Lm + (i - 1)), deadline,
                                  a.status, f < NS ? NEG : 0.f);
+        }
+      }
+      if (lane == 0) {
+        const bool take = act && (ein || fault);
 #pragma unroll
-          for (int q = 0; q < NS; ++q) { xh[q] = ev[q]; xl[q] = ev[NS + q]; }
-        } else {
-#pragma unroll
-          for (int q = 0; q < NS; ++q) { xh[q] = NEG; xl[q] = 0.f; }
+        for (int q = 0; q < NS; ++q) {
+          xh[q] = take ? ev[q] : NEG;
+          xl[q] = take ? ev[NS + q] : 0.f;
         }
       }
       float dgh[NS], dgl[NS];
@@ -629,10 +640,11 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
   for (int q = 0; q < NS; ++q) hold[q] = 0.f;
 #pragma unroll
   for (int q = 0; q < NP; ++q) outp[q] = 0.f;
-  KSum gA, gB, gS;
+  KSum gA, gB, gS;   // chunk sums folded in with compensation
 
   for (int kc = nch - 1; kc >= 0; --kc) {
     const int t0 = kc * C_STEPS;
+    float cA = 0.f, cB = 0.f, cS = 0.f;   // this chunk's plain sums
     // ---- restore the checkpoint and recompute the chunk into shared memory ----
     // entry e (0..C) holds every lane's row pairs after step t0+e-1 and its
     // scaled scores of that step; ea[e] holds lane 0's left-band pairs.
@@ -653,9 +665,11 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
       d0l[q] = ll[q];
       if (lane == 0) { ea[q] = lh[q]; ea[NS + q] = ll[q]; }
     }
+#pragma unroll 1
+    for (int u0 = 0; u0 < C_STEPS; u0 += PF)
 #pragma unroll
-    for (int cu = 0; cu < C_STEPS; ++cu) {
-      const int u = cu % PF;
+    for (int u = 0; u < PF; ++u) {
+      const int cu = u0 + u;
       const int t = t0 + cu;
       const int i = t - lane + 1;
       const bool act = (i >= 1) && (i <= L1);
@@ -724,12 +738,20 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
       // pushes arriving at column R-1 of row i: left pushes (NS==3: M,D; NS==1: A)
       // and diag pushes (NS==3: M,I,D; NS==1: A)
       float inL[2], inD[NS];
-      if (lane == 31) {
+      {
+        bool miss = false;
 #pragma unroll
-        for (int q = 0; q < NP; ++q)
-          if (is_sentinel(pw[q]))
-            pw[q] = poll_value(pin + q * (Lm + 1) + i, ld_poll(pin + q * (Lm + 1) + i), deadline,
-                               a.status, 0.f);
+        for (int q = 0; q < NP; ++q) miss |= is_sentinel(pw[q]);
+        miss = miss && (lane == 31);
+        if (__any_sync(FULL, miss) && miss) {
+#pragma unroll
+          for (int q = 0; q < NP; ++q)
+            if (is_sentinel(pw[q]))
+              pw[q] = poll_value(pin + q * (Lm + 1) + i, ld_poll(pin + q * (Lm + 1) + i), deadline,
+                                 a.status, 0.f);
+        }
+      }
+      if (lane == 31) {
         if constexpr (NS == 3) {
           inL[0] = pw[0]; inL[1] = pw[1];
 #pragma unroll
@@ -815,9 +837,9 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
           const float wDD = has_left ? wgt(lDh, lDl, Dh, Dl, g1) : 0.f;
           pm[c] = bM;
           const float pIM = bI * wIM, pII = bI * wII, pDM = bD * wDM, pDD = bD * wDD;
-          gA.add(pIM + pDM);
-          gB.add(pII + pDD);
-          gS.add(bM * sp);
+          cA += pIM + pDM;
+          cB += pII + pDD;
+          cS += bM * sp;
           nx[0][c] += pIM;
           nx[1][c] += pII;
           const float qM = bM * wMM, qI = bM * wMI, qD = bM * wMD;
@@ -845,8 +867,8 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
           const float pv_ = b * (wA + wS);
           pm[c] = pv_;
           const float pU = b * wU, pL = b * wL, pD = b * wA;
-          gA.add(pU + pL);
-          gS.add(pv_ * sp);
+          cA += pU + pL;
+          cS += pv_ * sp;
           nx[0][c] += pU;
           if (c > 0) {
             nx[0][c - 1] += pD;
@@ -878,6 +900,9 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
     }
 #pragma unroll
     for (int q = 0; q < NP; ++q) pbc[q] = pbn[q];
+    gA.add(cA);
+    gB.add(cB);
+    gS.add(cS);
     __syncwarp();
   }
   // warp-reduce the gradient partials (fixed shuffle tree: deterministic)

@@ -87,7 +87,8 @@ class Plan:
     workspace, so repeated calls allocate nothing and can be graph-captured.
     """
 
-    def __init__(self, lengths, offsets, family: str = "affine", device="cuda"):
+    def __init__(self, lengths, offsets, family: str = "affine", device="cuda",
+                 cols_per_lane: int = 0):
         if family not in _FAMILY:
             raise ValueError(f"family must be 'affine' or 'linear', got {family!r}")
         self.family = family
@@ -103,13 +104,14 @@ class Plan:
         self.cells = int((ln[:, 0].astype(np.int64) * ln[:, 1]).sum())
         pb, wb = ctypes.c_size_t(0), ctypes.c_size_t(0)
         fam = _FAMILY[family]
-        rc = self.lib.swb_ragged_plan(fam, ln.ctypes.data, off.ctypes.data, B, None, 0,
-                                      ctypes.byref(pb), ctypes.byref(wb))
+        self.cols_per_lane = int(cols_per_lane)
+        rc = self.lib.swb_ragged_plan(fam, self.cols_per_lane, ln.ctypes.data, off.ctypes.data, B,
+                                      None, 0, ctypes.byref(pb), ctypes.byref(wb))
         if rc != _lib.OK:
             raise ValueError("invalid packed batch: lengths must be >= 0 and offsets multiples of 4 "
                              "with room for L1 * round_up(L2, 4) elements per pair")
         self.host_plan = np.zeros(pb.value // 8 + 1, dtype=np.int64)
-        rc = self.lib.swb_ragged_plan(fam, ln.ctypes.data, off.ctypes.data, B,
+        rc = self.lib.swb_ragged_plan(fam, self.cols_per_lane, ln.ctypes.data, off.ctypes.data, B,
                                       self.host_plan.ctypes.data, self.host_plan.nbytes,
                                       ctypes.byref(pb), ctypes.byref(wb))
         _lib.check(rc, "swb_ragged_plan")

@@ -274,7 +274,7 @@ def test_bounded_wait_reports_timeout_and_context_survives():
     mp = torch.empty_like(s)
     nb = lib.swb_sw_affine_workspace_bytes(B, L1, L2)
     ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
-    opt = _lib.Options(0, 2_000_000, 1, None)
+    opt = _lib.Options(0, 2_000_000, 1, None, 0)
     rc = lib.swb_sw_affine_forward(s.data_ptr(), None, B, L1, L2, -2.0, -0.5, 0.9,
                                    outs[0].data_ptr(), mp.data_ptr(), outs[1].data_ptr(),
                                    outs[2].data_ptr(), outs[3].data_ptr(), ws.data_ptr(), nb,

@@ -14,12 +14,12 @@ def _plan(lengths, offsets, family=3):
     ln = np.ascontiguousarray(np.asarray(lengths, np.int32).reshape(-1, 2))
     off = np.ascontiguousarray(np.asarray(offsets, np.int64))
     pb, wb = ctypes.c_size_t(0), ctypes.c_size_t(0)
-    rc = lib.swb_ragged_plan(family, ln.ctypes.data, off.ctypes.data, len(ln), None, 0,
+    rc = lib.swb_ragged_plan(family, 4, ln.ctypes.data, off.ctypes.data, len(ln), None, 0,
                              ctypes.byref(pb), ctypes.byref(wb))
     if rc != 0:
         return rc, None
     buf = np.zeros(pb.value // 8 + 1, np.int64)
-    rc = lib.swb_ragged_plan(family, ln.ctypes.data, off.ctypes.data, len(ln), buf.ctypes.data,
+    rc = lib.swb_ragged_plan(family, 4, ln.ctypes.data, off.ctypes.data, len(ln), buf.ctypes.data,
                              buf.nbytes, ctypes.byref(pb), ctypes.byref(wb))
     return rc, buf
 
