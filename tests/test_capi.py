@@ -57,7 +57,7 @@ def test_workspace_sizes_monotone(lib):
     assert 0 < lib.swb_sw_workspace_bytes(4, 100, 100) < a
     # checkpoint storage is O(cells / chunk): well below a full 3-state table
     full = 3 * 4 * 16385 * 16385 * 4
-    assert lib.swb_sw_affine_workspace_bytes(4, 16384, 16384) < full / 2.5
+    assert lib.swb_sw_affine_workspace_bytes(4, 16384, 16384) < full / 2
 
 
 def test_argument_errors_return_before_any_launch(lib):
