@@ -312,3 +312,40 @@ def test_validation_messages():
                                               torch.zeros(2, device=dev), torch.zeros(1, device=dev),
                                               torch.ones(1, device=dev),
                                               torch.tensor([[4, 4]], dtype=torch.int32, device=dev))
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (37, 1), (70, 300), (300, 70), (129, 65)])
+@pytest.mark.parametrize("fam", ["aff", "lin"])
+def test_two_columns_per_lane_variant(shape, fam):
+    """The R=2 band layout (64-column bands) through the C ABI, vs the oracle."""
+    from orihime_b200 import _lib
+
+    lib = _lib.load()
+    s = _gen((3, *shape), 21)
+    sd = s.cuda()
+    B, L1, L2 = s.shape
+    outs = [torch.empty(B, device="cuda") for _ in range(4)]
+    mp = torch.empty_like(sd)
+    opt = _lib.Options(0, 0, 0, None, 2)
+    st = torch.cuda.current_stream().cuda_stream
+    if fam == "aff":
+        nb = lib.swb_sw_affine_workspace_bytes(B, L1, L2)
+        ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+        rc = lib.swb_sw_affine_forward(sd.data_ptr(), None, B, L1, L2, -2.0, -0.5, 0.8,
+                                       outs[0].data_ptr(), mp.data_ptr(), outs[1].data_ptr(),
+                                       outs[2].data_ptr(), outs[3].data_ptr(), ws.data_ptr(), nb,
+                                       st, opt)
+        r32 = O.affine(s.numpy(), None, -2.0, -0.5, 0.8)
+        r64 = O.affine(s.numpy(), None, -2.0, -0.5, 0.8, dtype=np.float64)
+    else:
+        nb = lib.swb_sw_workspace_bytes(B, L1, L2)
+        ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+        rc = lib.swb_sw_forward(sd.data_ptr(), None, B, L1, L2, -1.0, 0.8, outs[0].data_ptr(),
+                                mp.data_ptr(), outs[1].data_ptr(), outs[3].data_ptr(),
+                                ws.data_ptr(), nb, st, opt)
+        r32 = O.linear(s.numpy(), None, -1.0, 0.8)
+        r64 = O.linear(s.numpy(), None, -1.0, 0.8, dtype=np.float64)
+    assert rc == 0
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(outs[0].cpu().numpy(), r32["value"], rtol=VAL_RTOL)
+    _check("map", mp.cpu().numpy(), r32["map"], r64["map"], MAP_ATOL)

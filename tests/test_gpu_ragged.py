@@ -32,13 +32,14 @@ def _lengths(B, seed, lo=1, hi=400):
 
 
 @pytest.mark.parametrize("family", ["affine", "linear"])
-def test_ragged_matches_oracle_and_padded(family):
+@pytest.mark.parametrize("cols", [2, 4])
+def test_ragged_matches_oracle_and_padded(family, cols):
     from orihime_b200 import ragged
 
     ln = _lengths(24, 1)
     mats = [_emb(int(a), int(b), 100 + i) for i, (a, b) in enumerate(ln)]
     flat, off, lens = ragged.pack(mats)
-    plan = ragged.Plan(lens, off, family=family, device="cuda")
+    plan = ragged.Plan(lens, off, family=family, device="cuda", cols_per_lane=cols)
     params = dict(gap_open=-2.0, gap_ext=-0.5, temp=0.5) if family == "affine" else dict(gap=-1.0, temp=0.5)
     out = plan.run(flat.cuda(), **params)
     assert plan.status() == 0
@@ -61,9 +62,9 @@ def test_ragged_matches_oracle_and_padded(family):
             v, m = torch.ops.orihime.sw_forward(s.cuda(), -1.0, 0.5, None)
             r32 = O.linear(s.numpy(), None, -1.0, 0.5)
             r64 = O.linear(s.numpy(), None, -1.0, 0.5, dtype=np.float64)
-        # same per-pair schedule as the padded drop-in: identical bits
-        assert torch.equal(v.cpu()[0], out.value.cpu()[b])
-        assert torch.equal(m.cpu()[0], maps[b])
+        if cols == 4:  # same per-pair schedule as the padded drop-in: identical bits
+            assert torch.equal(v.cpu()[0], out.value.cpu()[b])
+            assert torch.equal(m.cpu()[0], maps[b])
         rel = abs(float(out.value[b]) - r32["value"][0]) / abs(r32["value"][0])
         assert rel <= 1e-5
         err = np.abs(maps[b].numpy() - r64["map"][0]).max()
