@@ -116,6 +116,8 @@ class Plan:
                                       ctypes.byref(pb), ctypes.byref(wb))
         _lib.check(rc, "swb_ragged_plan")
         self.device = torch.device(device)
+        if self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self.dev_plan = torch.from_numpy(self.host_plan.view(np.uint8)).to(self.device)
         self.workspace_bytes = wb.value
         self.workspace = torch.empty(max(wb.value, 1), dtype=torch.uint8, device=self.device)
