@@ -106,7 +106,9 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def dist_init(torch):
+def dist_init(torch, backend: str = "nccl"):
+    """One process per GPU (torchrun env).  `backend` "gloo" runs the same
+    host logic on CPU ranks (tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -115,8 +117,9 @@ def dist_init(torch):
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -132,7 +135,8 @@ def max_over_ranks(torch, world, x: float) -> float:
         return x
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
