@@ -73,6 +73,39 @@ int swb_sw_affine_forward(const float* scores, const int* lengths, int B, int L1
                           void* workspace, size_t workspace_bytes, void* stream,
                           const swb_options* opt);
 
+/* Size of the fixed device scratch of swb_sw_affine_forward_static (32 MiB). */
+#define SWB_STATIC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/*
+ * swb_sw_affine_forward without a workspace argument (no reference
+ * counterpart: the reference allocates its scratch through torch inside each
+ * op).  For callers that hold device pointers to their inputs and outputs but
+ * no device allocator of their own, e.g. a plain C or FFI host: it needs no
+ * workspace and makes no allocating call (no cudaMalloc/cudaFree, no library
+ * allocator).  Scratch is one file-scope device array of
+ * SWB_STATIC_SCRATCH_BYTES per device; whatever must start at zero or at the
+ * sentinel is reset with cudaMemsetAsync on `stream` at every call.
+ *   - Limit: returns SWB_ERR_WORKSPACE, before any CUDA call, when the batch
+ *     needs more than SWB_STATIC_SCRATCH_BYTES, i.e. when
+ *     swb_sw_affine_workspace_bytes(B, L1max, L2max) exceeds it (about
+ *     16 x 512 x 512 or one 2048 x 2048 pair fit).
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress, which may load the module) and sets up the
+ *     kernels; make that first call before any stream capture.
+ *   - All calls of one process on one device share the array: calls that
+ *     overlap in time (on different streams, or from several host threads,
+ *     without ordering) race and corrupt each other's results.  Order them on
+ *     one stream.
+ *   - The wait-timeout status word lives in the shared array and is not
+ *     readable with swb_read_status.
+ * Arguments and outputs as swb_sw_affine_forward.
+ */
+int swb_sw_affine_forward_static(const float* scores, const int* lengths, int B, int L1max,
+                                 int L2max, float gap_open, float gap_ext, float temp,
+                                 float* value, float* map,
+                                 float* grad_open, float* grad_ext, float* grad_temp,
+                                 void* stream, const swb_options* opt);
+
 /* Workspace bytes for swb_sw_forward on a [B, L1max, L2max] batch. */
 size_t swb_sw_workspace_bytes(int B, int L1max, int L2max);
 

@@ -63,6 +63,9 @@ def load() -> ctypes.CDLL:
     lib.swb_sw_affine_forward.restype = i
     lib.swb_sw_affine_forward.argtypes = [vp, vp, i, i, i, f, f, f, vp, vp, vp, vp, vp, vp, sz,
                                           vp, ctypes.POINTER(Options)]
+    lib.swb_sw_affine_forward_static.restype = i
+    lib.swb_sw_affine_forward_static.argtypes = [vp, vp, i, i, i, f, f, f, vp, vp, vp, vp, vp,
+                                                 vp, ctypes.POINTER(Options)]
     lib.swb_sw_forward.restype = i
     lib.swb_sw_forward.argtypes = [vp, vp, i, i, i, f, f, vp, vp, vp, vp, vp, sz, vp,
                                    ctypes.POINTER(Options)]

@@ -17,6 +17,11 @@
 #include "sw_probe.cuh"
 #include "../../include/orihime_b200.h"
 
+// Workspace of swb_sw_affine_forward_static: a fixed device array (one copy
+// per device, created when the module loads on that device), so that entry
+// point needs no caller-provided or allocated scratch.
+static __device__ __align__(256) unsigned char g_static_scratch[SWB_STATIC_SCRATCH_BYTES];
+
 namespace {
 
 using swb::Args;
@@ -131,6 +136,23 @@ int dev_info(DevInfo** out) {
     d.ready = true;
   }
   *out = &d;
+  return SWB_OK;
+}
+
+// Device address of g_static_scratch on the current device, looked up once
+// per device (the first lookup may load the module on that device).
+void* g_static_ptr[64];
+
+int static_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWB_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess || !p) return SWB_ERR_CUDA;
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
   return SWB_OK;
 }
 
@@ -271,6 +293,29 @@ int swb_sw_affine_forward(const float* scores, const int* lengths, int B, int L1
                           size_t workspace_bytes, void* stream, const swb_options* opt) {
   return launch_padded<3>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value, map,
                           grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream, opt);
+}
+
+int swb_sw_affine_forward_static(const float* scores, const int* lengths, int B, int L1max,
+                                 int L2max, float gap_open, float gap_ext, float temp,
+                                 float* value, float* map, float* grad_open, float* grad_ext,
+                                 float* grad_temp, void* stream, const swb_options* opt) {
+  // size check first: an oversize batch is rejected before any CUDA call
+  const int r = pick_r(opt);
+  if (B > 0 && L1max >= 0 && L2max >= 0 && valid_r(r)) {
+    const size_t need = r == 2 ? layout_for<3, 2>(B, L1max, L2max).total
+                               : layout_for<3, 4>(B, L1max, L2max).total;
+    if (need > (size_t)SWB_STATIC_SCRATCH_BYTES) return SWB_ERR_WORKSPACE;
+  }
+  void* ws = nullptr;
+  if (B > 0) {
+    const int rc = static_scratch(&ws);
+    if (rc != SWB_OK) return rc;
+  }
+  // the shared launch path resets the counters, status word and completion
+  // counts to 0 and the cross-band buffers to the sentinel on every call
+  return launch_padded<3>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value, map,
+                          grad_open, grad_ext, grad_temp, ws, (size_t)SWB_STATIC_SCRATCH_BYTES,
+                          stream, opt);
 }
 
 int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
