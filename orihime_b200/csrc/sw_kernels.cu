@@ -8,8 +8,8 @@
 //   linear  src/sw/kernels_gpu.cu:175-239, :242-299, :325-460, :463-497.
 // In the scaled domain x' = x*log2(e)/T the reference's
 //   LSE_T(v) = m + T*log(sum exp((v-m)/T))
-// becomes m' + lg2(sum ex2(v'-m')), and its softmax weight of a predecessor
-// is ex2(pred' + edge' - cell'), which is what the adjoint uses.
+// becomes m' + lg2(sum ex2(v'-m')), and the softmax weight of a predecessor
+// is its term ex2(v'-m') divided by the sum, which is what the adjoint uses.
 #include "sw_kernels.cuh"
 
 namespace swb {
@@ -28,6 +28,15 @@ __device__ __forceinline__ float lg2(float x) {
   float y;
   asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
+}
+
+// 1/x for x in [1, 4]: MUFU approximation refined by one Newton-Raphson step
+// (y' = y + y (1 - x y)), which leaves an error of about half an ulp with no
+// systematic sign; the adjoint's per-cell weight normalisation relies on that.
+__device__ __forceinline__ float recip(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return fmaf(y, fmaf(-x, y, 1.f), y);
 }
 
 __device__ __forceinline__ uint64_t gtimer() {
@@ -192,28 +201,35 @@ __device__ __forceinline__ void store_row(const Pair& pr, int i, int jl, const f
 }
 
 // Values crossing a band edge forward (2*NS: hi and lo of each state), pushes
-// crossing it backward (NP), checkpoint floats per lane (CKF) and shared-memory
-// floats per lane per recomputed step (EF: alpha pairs + scaled scores).
+// crossing it backward (NP), checkpoint floats per lane (CKF), adjoint fields
+// per cell (WF: normalised predecessor weights, beta-init terms, scaled score)
+// and shared-memory floats per lane per recomputed step (EW).
 template <int NS> struct Shape;
-template <> struct Shape<3> { static constexpr int NP = 5; };
-template <> struct Shape<1> { static constexpr int NP = 2; };
+template <> struct Shape<3> { static constexpr int NP = 5, WF = 11; };
+template <> struct Shape<1> { static constexpr int NP = 2, WF = 6; };
 
 template <int NS, int R> struct Dims {
   static constexpr int NE = 2 * NS;
   static constexpr int NP = Shape<NS>::NP;
   static constexpr int CKF = 2 * NS * R + 2 * NS;
-  static constexpr int EF = 2 * NS * R + R;
+  static constexpr int WF = Shape<NS>::WF;
+  static constexpr int EW = WF * R;
 };
+
+// Adjoint fields of a cell (kind index; shared-memory field = kind * R + c).
+// affine: weights of M's diagonal predecessors M, I, D; of I's upper
+// predecessors M, I; of D's left predecessors M, D; beta-init of M, I, D;
+// scaled score.
+enum : int { W_MM = 0, W_MI, W_MD, W_IM, W_II, W_DM, W_DD, B_M, B_I, B_D, W_SA };
+// linear: the map factor (diagonal + start weights), weights of the diagonal,
+// upper and left predecessors, beta-init, scaled score.
+enum : int { V_P = 0, V_A, V_U, V_L, V_B, V_S };
 
 // checkpoint field indices
 template <int NS, int R> __device__ __forceinline__ int ck_h(int q, int c) { return q * R + c; }
 template <int NS, int R> __device__ __forceinline__ int ck_l(int q, int c) { return NS * R + q * R + c; }
 template <int NS, int R> __device__ __forceinline__ int ck_lh(int q) { return 2 * NS * R + q; }
 template <int NS, int R> __device__ __forceinline__ int ck_ll(int q) { return 2 * NS * R + NS + q; }
-// shared-memory entry field indices
-template <int NS, int R> __device__ __forceinline__ int en_h(int q, int c) { return q * R + c; }
-template <int NS, int R> __device__ __forceinline__ int en_l(int q, int c) { return NS * R + q * R + c; }
-template <int NS, int R> __device__ __forceinline__ int en_s(int c) { return 2 * NS * R + c; }
 
 // ---------------------------------------------------------------------------
 // forward cell
@@ -238,12 +254,20 @@ __device__ __forceinline__ void two_sum(float a, float b, float& h, float& l) {
 // (ph, pl), left pairs of this row (lfh, lfl, already received), diag pairs of
 // column 0 (dgh0, dgl0: left lane, previous row) and the scaled scores s.
 // Writes the new row into (ph, pl) when act and returns it in (nh, nl).
-template <int NS, int R>
+//
+// WT (adjoint recompute): also writes each cell's adjoint fields to shared
+// memory at wout[(kind * R + c) * 32].  The predecessor weights are the
+// recurrence's own softmax terms divided by their sum, so they add up to 1
+// per cell up to rounding and the adjoint conserves probability flow exactly;
+// beta-init = exp2(min(x - S, 0)) for the first `nlive` columns, 0 beyond.
+template <int NS, int R, bool WT = false>
 __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R],
                                           const float (&lfh)[NS], const float (&lfl)[NS],
                                           const float (&dgh0)[NS], const float (&dgl0)[NS],
                                           const float (&s)[R], float g0, float g1, bool act,
-                                          float (&nh)[NS][R], float (&nl)[NS][R]) {
+                                          float (&nh)[NS][R], float (&nl)[NS][R],
+                                          float Sh = 0.f, float Sl = 0.f, int nlive = 0,
+                                          float* wout = nullptr) {
   float dgh[NS], dgl[NS], lh[NS], ll[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) { dgh[q] = dgh0[q]; dgl[q] = dgl0[q]; lh[q] = lfh[q]; ll[q] = lfl[q]; }
@@ -255,8 +279,9 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       // M = s + LSE(M, I, D at diag, 0)
       const float r = fmaxf(fmaxf(dgh[0] + dgl[0], dgh[1] + dgl[1]),
                             fmaxf(dgh[2] + dgl[2], 0.f));
-      const float sm = (ex2((dgh[0] - r) + dgl[0]) + ex2((dgh[1] - r) + dgl[1])) +
-                       (ex2((dgh[2] - r) + dgl[2]) + ex2(-r));
+      const float tM = ex2((dgh[0] - r) + dgl[0]), tI = ex2((dgh[1] - r) + dgl[1]);
+      const float tD = ex2((dgh[2] - r) + dgl[2]);
+      const float sm = (tM + tI) + (tD + ex2(-r));
       float Mh, Ml;
       two_sum(r, s[c], Mh, Ml);
       Ml += lg2(sm);
@@ -264,14 +289,34 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       const float ru = fmaxf((uMh + uMl) + g0, (uIh + uIl) + g1);
       const float ia = ((uMh - ru) + g0) + uMl, ib = ((uIh - ru) + g1) + uIl;
       const float im = fmaxf(ia, ib);
+      const float ti = ex2(fminf(ia, ib) - im), si = 1.f + ti;
       float Ih, Il;
-      fast2(ru, im + lg2(1.f + ex2(fminf(ia, ib) - im)), Ih, Il);
+      fast2(ru, im + lg2(si), Ih, Il);
       // D = LSE(M left + go, D left + ge)
       const float rl = fmaxf((lh[0] + ll[0]) + g0, (lh[2] + ll[2]) + g1);
       const float da = ((lh[0] - rl) + g0) + ll[0], db = ((lh[2] - rl) + g1) + ll[2];
       const float dm = fmaxf(da, db);
+      const float td = ex2(fminf(da, db) - dm), sd = 1.f + td;
       float Dh, Dl;
-      fast2(rl, dm + lg2(1.f + ex2(fminf(da, db) - dm)), Dh, Dl);
+      fast2(rl, dm + lg2(sd), Dh, Dl);
+      if constexpr (WT) {
+        float* o = wout + c * 32;
+        const float vm = recip(sm);
+        o[W_MM * R * 32] = tM * vm;
+        o[W_MI * R * 32] = tI * vm;
+        o[W_MD * R * 32] = tD * vm;
+        const float vi = recip(si), wi = ti * vi;   // larger term: 1/si, smaller: ti/si
+        o[W_IM * R * 32] = ia >= ib ? vi : wi;
+        o[W_II * R * 32] = ia >= ib ? wi : vi;
+        const float vd = recip(sd), wd = td * vd;
+        o[W_DM * R * 32] = da >= db ? vd : wd;
+        o[W_DD * R * 32] = da >= db ? wd : vd;
+        const bool lv = c < nlive;
+        o[B_M * R * 32] = lv ? ex2(fminf((Mh - Sh) + (Ml - Sl), 0.f)) : 0.f;
+        o[B_I * R * 32] = lv ? ex2(fminf((Ih - Sh) + (Il - Sl), 0.f)) : 0.f;
+        o[B_D * R * 32] = lv ? ex2(fminf((Dh - Sh) + (Dl - Sl), 0.f)) : 0.f;
+        o[W_SA * R * 32] = s[c];
+      }
       nh[0][c] = Mh; nl[0][c] = Ml; nh[1][c] = Ih; nl[1][c] = Il; nh[2][c] = Dh; nl[2][c] = Dl;
       dgh[0] = uMh; dgl[0] = uMl; dgh[1] = uIh; dgl[1] = uIl; dgh[2] = uDh; dgl[2] = uDl;
       lh[0] = Mh; ll[0] = Ml; lh[1] = Ih; ll[1] = Il; lh[2] = Dh; ll[2] = Dl;
@@ -284,9 +329,20 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       const float vu = ((uh - r) + g0) + ul;
       const float vl = ((lh[0] - r) + g0) + ll[0];
       const float vs = s[c] - r;
-      const float sm = (ex2(va) + ex2(vu)) + (ex2(vl) + ex2(vs));
+      const float ta = ex2(va), tu = ex2(vu), tl = ex2(vl), ts = ex2(vs);
+      const float sm = (ta + tu) + (tl + ts);
       float Ah, Al;
       fast2(r, lg2(sm), Ah, Al);
+      if constexpr (WT) {
+        float* o = wout + c * 32;
+        const float v = recip(sm);
+        o[V_P * R * 32] = (ta + ts) * v;
+        o[V_A * R * 32] = ta * v;
+        o[V_U * R * 32] = tu * v;
+        o[V_L * R * 32] = tl * v;
+        o[V_B * R * 32] = c < nlive ? ex2(fminf((Ah - Sh) + (Al - Sl), 0.f)) : 0.f;
+        o[V_S * R * 32] = s[c];
+      }
       nh[0][c] = Ah; nl[0][c] = Al;
       dgh[0] = uh; dgl[0] = ul;
       lh[0] = Ah; ll[0] = Al;
@@ -426,7 +482,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
       }
       float s[R];
 #pragma unroll
-      for (int c = 0; c < R; ++c) s[c] = sb[u][c] * k;
+      for (int c = 0; c < R; ++c) s[c] = __fmul_rn(sb[u][c], k);
       {
         const int ip = i + PF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
@@ -434,14 +490,15 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
       float nh[NS][R], nl[NS][R];
       fwd_cells<NS, R>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, act, nh, nl);
       if (act) {
-        // partition: lazily rescaled Kahan sum of ex2(x - ref)
+        // partition: lazily rescaled Kahan sum of ex2(x - ref); exponents stay
+        // <= 8 so (hi - ref) + lo rounds at <= 2^-21 absolute
         float mx = NEG;
 #pragma unroll
         for (int c = 0; c < R; ++c)
           if (jl + c < L2)
 #pragma unroll
             for (int q = 0; q < NS; ++q) mx = fmaxf(mx, nh[q][c] + nl[q][c]);
-        if (mx > ref + 64.f) {
+        if (mx > ref + 8.f) {
           float f = ex2(ref - mx);
           acc.s *= f;
           acc.c *= f;
@@ -519,8 +576,21 @@ __device__ __forceinline__ void pair_logz(const Args& a, const Place& w, int lan
     s = s * ex2(ref - m) + s2 * ex2(r2 - m);
     ref = m;
   }
-  Sh = ref;
-  Sl = lg2(s);
+  // S = ref + log2(s) as a double-float with a small lo part: with s = m * 2^e,
+  // m in [1, 2), lg2 sees only the mantissa and the integer e joins ref by
+  // TwoSum.  (lg2 of a large s would round at ~1e-6 absolute, which shows up
+  // in every exp2(x - S) of the adjoint.)
+  const unsigned bits = __float_as_uint(s);
+  const int e = (int)((bits >> 23) & 0xffu) - 127;
+  if (s > 0.f && e > -127 && e < 128) {
+    float h, l;
+    two_sum(ref, (float)e, h, l);
+    Sh = h;
+    Sl = l + lg2(__uint_as_float((bits & 0x7fffffu) | 0x3f800000u));
+  } else {
+    Sh = ref;
+    Sl = lg2(s);
+  }
 }
 
 // Last band task of a pair to finish folds the per-band gradient partials (in
@@ -560,17 +630,21 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
   }
 }
 
-// Weight of a predecessor: ex2(((pred_h - cell_h) + edge) + (pred_l - cell_l)),
-// guarded against overflow for cells that do not exist (their beta is 0).
-__device__ __forceinline__ float wgt(float ph_, float pl_, float xh, float xl, float e) {
-  return ex2(fminf(((ph_ - xh) + e) + (pl_ - xl), 64.f));
-}
+// ---------------------------------------------------------------------------
+// adjoint band task
+// ---------------------------------------------------------------------------
 
+// Per band, checkpoint chunks in reverse.  Each chunk restores its checkpoint
+// and recomputes C steps of alpha, writing every cell's adjoint fields
+// (normalised predecessor weights, beta-init, scaled score) to shared memory;
+// then the adjoint runs the same C steps backwards in push form, where a
+// cell's beta = beta-init + pushes received, and it pushes beta * weight to
+// each predecessor: within the lane through registers, to the left lane
+// through __shfl_down_sync, to the left band through the push buffer.
 template <int NS, int R>
-__device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, float* ea,
-                         uint64_t deadline) {
+__device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uint64_t deadline) {
   using D = Dims<NS, R>;
-  constexpr int NP = D::NP, EF = D::EF, CKF = D::CKF, NE = D::NE;
+  constexpr int NP = D::NP, EW = D::EW, CKF = D::CKF, NE = D::NE;
   const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
   const int band = w.band;
@@ -582,6 +656,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
     return;
   }
   const int jl = col0 + lane * R;
+  const int ncols = min(max(L2 - jl, 0), R);  // columns of this lane inside the pair
   const float k = a.k, g0 = a.go * k, g1 = a.ge * k;
   const size_t Lm = (size_t)w.Lm;
   const float* ein = (band > 0) ? a.edge + w.ed0 + (size_t)(band - 1) * w.edb : nullptr;
@@ -590,7 +665,6 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
   const float* pin = right_live ? a.bpush + w.bp0 + (size_t)(band + 1) * w.bpb : nullptr;
   const float* ck = a.ckpt + w.ck0 + (size_t)band * w.ckb;
   const int nch = band_chunks(L1);
-  const int left_lane = (lane + 31) & 31;
 
   // ---- chunk-ahead prefetch state ----
   float ckr[CKF];           // checkpoint of the next chunk to recompute
@@ -630,7 +704,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
   load_pb(nch - 1, pbc);
 
   // ---- adjoint state ----
-  float ac[NS][R], nx[NS][R];
+  float ac[NS][R], nx[NS][R];   // pushes received by this row / the row above
 #pragma unroll
   for (int q = 0; q < NS; ++q)
 #pragma unroll
@@ -645,25 +719,17 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
   for (int kc = nch - 1; kc >= 0; --kc) {
     const int t0 = kc * C_STEPS;
     float cA = 0.f, cB = 0.f, cS = 0.f;   // this chunk's plain sums
-    // ---- restore the checkpoint and recompute the chunk into shared memory ----
-    // entry e (0..C) holds every lane's row pairs after step t0+e-1 and its
-    // scaled scores of that step; ea[e] holds lane 0's left-band pairs.
+    // ---- restore the checkpoint and recompute the chunk's adjoint fields ----
     float ph[NS][R], pl[NS][R], lh[NS], ll[NS];
-    float d0h[NS], d0l[NS];   // diag of column 0 at the chunk's first step
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
 #pragma unroll
       for (int c = 0; c < R; ++c) {
         ph[q][c] = ckr[ck_h<NS, R>(q, c)];
         pl[q][c] = ckr[ck_l<NS, R>(q, c)];
-        sm[en_h<NS, R>(q, c) * 32 + lane] = ph[q][c];
-        sm[en_l<NS, R>(q, c) * 32 + lane] = pl[q][c];
       }
       lh[q] = ckr[ck_lh<NS, R>(q)];
       ll[q] = ckr[ck_ll<NS, R>(q)];
-      d0h[q] = lh[q];
-      d0l[q] = ll[q];
-      if (lane == 0) { ea[q] = lh[q]; ea[NS + q] = ll[q]; }
     }
 #pragma unroll 1
     for (int u0 = 0; u0 < C_STEPS; u0 += PF)
@@ -683,8 +749,6 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
         if (lane == 0) {
           xh[q] = act ? evh : NEG;
           xl[q] = act ? evl : 0.f;
-          ea[(cu + 1) * NE + q] = xh[q];
-          ea[(cu + 1) * NE + NS + q] = xl[q];
         }
       }
       float dgh[NS], dgl[NS];
@@ -695,23 +759,14 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
       }
       float s[R];
 #pragma unroll
-      for (int c = 0; c < R; ++c) s[c] = sb[u][c] * k;
+      for (int c = 0; c < R; ++c) s[c] = __fmul_rn(sb[u][c], k);
       if (cu + PF < C_STEPS) {
         const int ip = i + PF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
       float nh[NS][R], nl[NS][R];
-      fwd_cells<NS, R>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, act, nh, nl);
-      float* e = sm + (size_t)(cu + 1) * EF * 32 + lane;
-#pragma unroll
-      for (int q = 0; q < NS; ++q)
-#pragma unroll
-        for (int c = 0; c < R; ++c) {
-          e[en_h<NS, R>(q, c) * 32] = ph[q][c];
-          e[en_l<NS, R>(q, c) * 32] = pl[q][c];
-        }
-#pragma unroll
-      for (int c = 0; c < R; ++c) e[en_s<NS, R>(c) * 32] = s[c];
+      fwd_cells<NS, R, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, act, nh, nl, Sh, Sl,
+                             act ? ncols : 0, sm + (size_t)cu * EW * 32 + lane);
     }
     if (kc > 0) {  // prefetch the next chunk's inputs while the adjoint runs
       load_ck(kc - 1);
@@ -723,12 +778,11 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
     // ---- adjoint over the chunk, last step first ----
 #pragma unroll 1
     for (int cu = 0; cu < C_STEPS; ++cu) {
-      const int ent = C_STEPS - cu;            // entry of row i (this step)
-      const int t = t0 + ent - 1;
+      const int ent = C_STEPS - 1 - cu;        // entry of this step's row
+      const int t = t0 + ent;
       const int i = t - lane + 1;
       const bool act = (i >= 1) && (i <= L1);
-      const float* E = sm + (size_t)ent * EF * 32;        // row i
-      const float* P = sm + (size_t)(ent - 1) * EF * 32;  // row i-1
+      const float* E = sm + (size_t)ent * EW * 32 + lane;
       float r[NP], pw[NP];
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
@@ -777,72 +831,26 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
       } else {
         ac[0][R - 1] += inL[0] + inD[0];
       }
-      // left neighbour of column 0: the left lane's last column at row i
-      // (entry ent-1) and row i-1 (entry ent-2); lane 0 reads the band edge.
-      float lnh[NS], lnl[NS], dnh[NS], dnl[NS];
-#pragma unroll
-      for (int q = 0; q < NS; ++q) {
-        if (lane == 0) {
-          lnh[q] = ea[ent * NE + q];
-          lnl[q] = ea[ent * NE + NS + q];
-          dnh[q] = ea[(ent - 1) * NE + q];
-          dnl[q] = ea[(ent - 1) * NE + NS + q];
-        } else {
-          lnh[q] = P[en_h<NS, R>(q, R - 1) * 32 + left_lane];
-          lnl[q] = P[en_l<NS, R>(q, R - 1) * 32 + left_lane];
-          if (ent >= 2) {
-            dnh[q] = P[(-EF + en_h<NS, R>(q, R - 1)) * 32 + left_lane];
-            dnl[q] = P[(-EF + en_l<NS, R>(q, R - 1)) * 32 + left_lane];
-          } else {
-            dnh[q] = d0h[q];
-            dnl[q] = d0l[q];
-          }
-        }
-      }
 #pragma unroll
       for (int q = 0; q < NP; ++q) outp[q] = 0.f;
       float pm[R];
 #pragma unroll
       for (int c = R - 1; c >= 0; --c) {
-        const bool live = act && (jl + c < L2);
-        const bool has_up = i > 1;
-        const bool has_left = (jl + c) > 0;
-        const float sp = E[en_s<NS, R>(c) * 32 + lane];
+        const bool live = act && c < ncols;
+        auto F = [&](int kind) { return E[(kind * R + c) * 32]; };
         if constexpr (NS == 3) {
-          const float Mh = E[en_h<NS, R>(0, c) * 32 + lane], Ml = E[en_l<NS, R>(0, c) * 32 + lane];
-          const float Ih = E[en_h<NS, R>(1, c) * 32 + lane], Il = E[en_l<NS, R>(1, c) * 32 + lane];
-          const float Dh = E[en_h<NS, R>(2, c) * 32 + lane], Dl = E[en_l<NS, R>(2, c) * 32 + lane];
-          const float uMh = P[en_h<NS, R>(0, c) * 32 + lane], uMl = P[en_l<NS, R>(0, c) * 32 + lane];
-          const float uIh = P[en_h<NS, R>(1, c) * 32 + lane], uIl = P[en_l<NS, R>(1, c) * 32 + lane];
-          float dMh, dMl, dIh, dIl, dDh, dDl, lMh, lMl, lDh, lDl;
-          if (c > 0) {
-            dMh = P[en_h<NS, R>(0, c - 1) * 32 + lane]; dMl = P[en_l<NS, R>(0, c - 1) * 32 + lane];
-            dIh = P[en_h<NS, R>(1, c - 1) * 32 + lane]; dIl = P[en_l<NS, R>(1, c - 1) * 32 + lane];
-            dDh = P[en_h<NS, R>(2, c - 1) * 32 + lane]; dDl = P[en_l<NS, R>(2, c - 1) * 32 + lane];
-            lMh = E[en_h<NS, R>(0, c - 1) * 32 + lane]; lMl = E[en_l<NS, R>(0, c - 1) * 32 + lane];
-            lDh = E[en_h<NS, R>(2, c - 1) * 32 + lane]; lDl = E[en_l<NS, R>(2, c - 1) * 32 + lane];
-          } else {
-            dMh = dnh[0]; dMl = dnl[0]; dIh = dnh[1]; dIl = dnl[1]; dDh = dnh[2]; dDl = dnl[2];
-            lMh = lnh[0]; lMl = lnl[0]; lDh = lnh[2]; lDl = lnl[2];
-          }
-          const float bM = live ? ex2(fminf((Mh - Sh) + (Ml - Sl), 0.f)) + ac[0][c] : 0.f;
-          const float bI = live ? ex2(fminf((Ih - Sh) + (Il - Sl), 0.f)) + ac[1][c] : 0.f;
-          const float bD = live ? ex2(fminf((Dh - Sh) + (Dl - Sl), 0.f)) + ac[2][c] : 0.f;
-          const float wMM = wgt(dMh, dMl, Mh, Ml, sp);
-          const float wMI = wgt(dIh, dIl, Mh, Ml, sp);
-          const float wMD = wgt(dDh, dDl, Mh, Ml, sp);
-          const float wIM = has_up ? wgt(uMh, uMl, Ih, Il, g0) : 0.f;
-          const float wII = has_up ? wgt(uIh, uIl, Ih, Il, g1) : 0.f;
-          const float wDM = has_left ? wgt(lMh, lMl, Dh, Dl, g0) : 0.f;
-          const float wDD = has_left ? wgt(lDh, lDl, Dh, Dl, g1) : 0.f;
+          const float bM = live ? F(B_M) + ac[0][c] : 0.f;
+          const float bI = live ? F(B_I) + ac[1][c] : 0.f;
+          const float bD = live ? F(B_D) + ac[2][c] : 0.f;
           pm[c] = bM;
-          const float pIM = bI * wIM, pII = bI * wII, pDM = bD * wDM, pDD = bD * wDD;
+          const float pIM = bI * F(W_IM), pII = bI * F(W_II);
+          const float pDM = bD * F(W_DM), pDD = bD * F(W_DD);
           cA += pIM + pDM;
           cB += pII + pDD;
-          cS += bM * sp;
+          cS += bM * F(W_SA);
           nx[0][c] += pIM;
           nx[1][c] += pII;
-          const float qM = bM * wMM, qI = bM * wMI, qD = bM * wMD;
+          const float qM = bM * F(W_MM), qI = bM * F(W_MI), qD = bM * F(W_MD);
           if (c > 0) {
             nx[0][c - 1] += qM; nx[1][c - 1] += qI; nx[2][c - 1] += qD;
             ac[0][c - 1] += pDM; ac[2][c - 1] += pDD;
@@ -850,25 +858,12 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
             outp[0] = pDM; outp[1] = pDD; outp[2] = qM; outp[3] = qI; outp[4] = qD;
           }
         } else {
-          const float Ah = E[en_h<NS, R>(0, c) * 32 + lane], Al = E[en_l<NS, R>(0, c) * 32 + lane];
-          const float uh = P[en_h<NS, R>(0, c) * 32 + lane], ul = P[en_l<NS, R>(0, c) * 32 + lane];
-          float dh, dl, lh_, ll_;
-          if (c > 0) {
-            dh = P[en_h<NS, R>(0, c - 1) * 32 + lane]; dl = P[en_l<NS, R>(0, c - 1) * 32 + lane];
-            lh_ = E[en_h<NS, R>(0, c - 1) * 32 + lane]; ll_ = E[en_l<NS, R>(0, c - 1) * 32 + lane];
-          } else {
-            dh = dnh[0]; dl = dnl[0]; lh_ = lnh[0]; ll_ = lnl[0];
-          }
-          const float b = live ? ex2(fminf((Ah - Sh) + (Al - Sl), 0.f)) + ac[0][c] : 0.f;
-          const float wA = wgt(dh, dl, Ah, Al, sp);
-          const float wS = ex2(fminf((sp - Ah) - Al, 64.f));
-          const float wU = has_up ? wgt(uh, ul, Ah, Al, g0) : 0.f;
-          const float wL = has_left ? wgt(lh_, ll_, Ah, Al, g0) : 0.f;
-          const float pv_ = b * (wA + wS);
+          const float b = live ? F(V_B) + ac[0][c] : 0.f;
+          const float pv_ = b * F(V_P);
           pm[c] = pv_;
-          const float pU = b * wU, pL = b * wL, pD = b * wA;
+          const float pU = b * F(V_U), pL = b * F(V_L), pD = b * F(V_A);
           cA += pU + pL;
-          cS += pv_ * sp;
+          cS += pv_ * F(V_S);
           nx[0][c] += pU;
           if (c > 0) {
             nx[0][c - 1] += pD;
@@ -916,10 +911,10 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, flo
   finish_pair<NS>(a, w, lane, Sh, Sl, v0, v1, v2);
 }
 
-// Shared memory per adjoint warp (floats): recomputed entries + lane-0 edges.
+// Shared memory per adjoint warp (floats): one chunk of adjoint fields.
 template <int NS, int R>
 __host__ __device__ constexpr int bwd_smem_floats() {
-  return (C_STEPS + 1) * Dims<NS, R>::EF * 32 + (C_STEPS + 1) * Dims<NS, R>::NE;
+  return C_STEPS * Dims<NS, R>::EW * 32;
 }
 
 template <int NS, int R, int WARPS>
@@ -928,7 +923,6 @@ __global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
   float* sm = smem + (size_t)w * bwd_smem_floats<NS, R>();
-  float* ea = sm + (C_STEPS + 1) * Dims<NS, R>::EF * 32;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
   const int ntasks = (a.layout == 0) ? a.B * a.nb : a.ntasks;
   while (true) {
@@ -936,8 +930,9 @@ __global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    bwd_band<NS, R>(a, place_of<NS, R>(a, task, true), lane, sm, ea, deadline);
+    bwd_band<NS, R>(a, place_of<NS, R>(a, task, true), lane, sm, deadline);
   }
 }
 
 }  // namespace swb
+

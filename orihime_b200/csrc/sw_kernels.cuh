@@ -26,8 +26,12 @@
 // ever stored.
 //
 // Adjoint kernel: per band, time chunks in reverse.  Each chunk restores its
-// checkpoint, recomputes C steps of alpha into shared memory, then runs the
-// adjoint (beta) recurrence backwards in "push" form: a finished cell pushes
+// checkpoint and recomputes C steps of alpha; every cell writes its adjoint
+// fields to shared memory: the weights of its predecessors (the recurrence's
+// own softmax terms divided by their sum, so they add up to 1 and the adjoint
+// conserves probability flow whatever the MUFU rounding), its beta-init term
+// exp2(min(x - S, 0)) and its scaled score.  The adjoint then runs the chunk
+// backwards in "push" form with multiply-adds only: a finished cell pushes
 // beta*w to its predecessors -- within the lane through registers, to the
 // left lane through __shfl_down_sync, to the left band through a global
 // buffer.  No atomics; the map is written row by row.
