@@ -37,6 +37,7 @@ NPAIRS, LMIN, LMAX, D = 4096, 32, 2048, 64
 MUFU_PER_CELL = 21      # algorithmic MUFU ops per cell, forward 11 + adjoint 10
 MUFU_PER_CELL_BWD = 10  # adjoint kernel alone
 BYTES_PER_CELL = 8      # compulsory HBM bytes per cell (score read + map write)
+BWD_DRAM_BYTES_PER_CELL = 12.65  # measured adjoint DRAM traffic: scores + checkpoints + map
 
 
 def workload_lengths(seed: int, n: int = NPAIRS) -> np.ndarray:
@@ -395,13 +396,11 @@ def main():
                     "step_frac": (MUFU_PER_CELL * cells / (ms * 1e-3)) / peak,
                     "hbm_frac_of_measured": (BYTES_PER_CELL * cells / (ms * 1e-3)) /
                                             (measured_peaks().get("hbm_gbs", 6550.0) * 1e9)}
-            prof = os.path.join(ROOT, "profiles", "bench_traffic.json")
-            if os.path.exists(prof):
-                try:
-                    tr = json.load(open(prof))
-                    roof["traffic"] = tr.get("bytes_per_cell_bwd", 0) * cells
-                except Exception:
-                    pass
+            # DRAM bytes of one adjoint launch: ncu's dram__bytes_read + write per
+            # cell on a 256-pair capture of this kernel, times this launch's cells
+            roof["traffic"] = BWD_DRAM_BYTES_PER_CELL * cells
+            roof["traffic_source"] = ("ncu capture of bwd_kernel<3,4,1> on 256 pairs, "
+                                      f"{BWD_DRAM_BYTES_PER_CELL} B/cell, scaled by cells")
         cpu = None if args.no_cpu_baseline else cpu_baseline(lengths)
         clocks = clk.summary()
         line = {"metric": METRIC, "value": gcups_all, "unit": "GCUPS", "n_gpus": world,
