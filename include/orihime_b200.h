@@ -160,6 +160,50 @@ int swb_sw_ragged(const float* scores, const void* host_plan, const void* dev_pl
                   void* workspace, size_t workspace_bytes, void* stream,
                   const swb_options* opt);
 
+/*
+ * Second-order ops (one CTA per pair sweeping anti-diagonals; the workspace
+ * holds alpha and its tangent for every cell, 9 floats per cell affine,
+ * 3 linear, plus small per-pair push buffers).
+ */
+size_t swb_sw_affine_aux_workspace_bytes(int B, int L1max, int L2max);
+
+/*
+ * Hessian-vector product of the marginal map: out = d(map)/d(scores) . v
+ * [B, L1max, L2max], zero outside lengths.  Replaces soft_sw_affine_hvp_cuda
+ * (src/sw_affine/torch_cuda.cpp:508 -> sw_affine_hvp, kernels_gpu.cu:1566).
+ * grad_tangents (optional, device [B][4]): per pair the tangents along v of
+ * (dS/dgap_open, dS/dgap_ext, dS/dT, S); their batch sums are the parameter
+ * part of the map's VJP with cotangent v, which
+ * orihime_sw_affine_marginals_backward_cuda (torch_cuda.cpp:681-811) gets from
+ * three parameter-Jacobian passes.
+ */
+int swb_sw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
+                      int L2max, float gap_open, float gap_ext, float temp, float* out,
+                      float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * d(map)/d(theta) [B, L1max, L2max], param 0 = gap_open, 1 = gap_ext, 2 = temp.
+ * Replaces soft_sw_affine_param_jacobian_cuda (src/sw_affine/torch_cuda.cpp:580
+ * -> sw_affine_param_grad, kernels_gpu.cu:1638).
+ */
+int swb_sw_affine_param_jacobian(const float* scores, const int* lengths, int B, int L1max,
+                                 int L2max, float gap_open, float gap_ext, float temp, int param,
+                                 float* out, void* workspace, size_t workspace_bytes, void* stream);
+
+size_t swb_sw_aux_workspace_bytes(int B, int L1max, int L2max);
+
+/* Linear-gap HVP (src/sw/torch_cuda.cpp marginals_hvp body); grad_tangents
+ * [B][4] = tangents of (dS/dgap, dS/dT, 0, S). */
+int swb_sw_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
+               int L2max, float gap, float temp, float* out, float* grad_tangents,
+               void* workspace, size_t workspace_bytes, void* stream);
+
+/* Linear-gap d(map)/d(theta), param 0 = gap, 1 = temp
+ * (src/sw/torch_cuda.cpp param-Jacobian body, kernels_cpu.cpp:491-710). */
+int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap, float temp, int param, float* out, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
 /* Copies the workspace status word to *status (synchronises `stream`).
  * No reference counterpart: the reference synchronises inside every op. */
 int swb_read_status(const void* workspace, void* stream, unsigned* status);

@@ -81,6 +81,18 @@ def load() -> ctypes.CDLL:
     lib.swb_sw_ragged.argtypes = [vp, vp, vp, f, f, vp, vp, vp, vp, vp, sz, vp,
                                   ctypes.POINTER(Options)]
     del ll
+    lib.swb_sw_affine_aux_workspace_bytes.restype = sz
+    lib.swb_sw_affine_aux_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sw_aux_workspace_bytes.restype = sz
+    lib.swb_sw_aux_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sw_affine_hvp.restype = i
+    lib.swb_sw_affine_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, f, vp, vp, vp, sz, vp]
+    lib.swb_sw_affine_param_jacobian.restype = i
+    lib.swb_sw_affine_param_jacobian.argtypes = [vp, vp, i, i, i, f, f, f, i, vp, vp, sz, vp]
+    lib.swb_sw_hvp.restype = i
+    lib.swb_sw_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, vp, vp, vp, sz, vp]
+    lib.swb_sw_param_jacobian.restype = i
+    lib.swb_sw_param_jacobian.argtypes = [vp, vp, i, i, i, f, f, i, vp, vp, sz, vp]
     lib.swb_mufu_probe.restype = i
     lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()

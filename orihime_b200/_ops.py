@@ -262,7 +262,149 @@ def sw_value_grad_params(scores, gap, temp, lengths):
     return gg, gT
 
 
+# ---- second-order ops --------------------------------------------------------
+
+def _check_like(scores, other, name, msg_shape):
+    check_input_cuda(other, name)
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D")
+    if other.shape != scores.shape:
+        raise RuntimeError(msg_shape)
+    if other.device != scores.device:
+        raise RuntimeError(f"{name} must be on same device as scores, got {other.device} vs {scores.device}")
+
+
+def _aux_ws(nbytes, dev):
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=dev)
+
+
+def run_hvp(fam, scores, v, lengths, params, want_grads=False):
+    """H.v of the map (and optionally the per-pair tangents of dS/dparams, S)."""
+    B, L1, L2 = scores.shape
+    dev = scores.device
+    out = torch.empty_like(scores)
+    gt = torch.zeros(B, 4, dtype=torch.float32, device=dev) if want_grads else None
+    if B == 0:
+        return out, gt
+    aff = fam == "sw_affine"
+    nbytes = (_LIB.swb_sw_affine_aux_workspace_bytes if aff else _LIB.swb_sw_aux_workspace_bytes)(B, L1, L2)
+    ws = _aux_ws(nbytes, dev)
+    with torch.cuda.device(dev):
+        if aff:
+            rc = _LIB.swb_sw_affine_hvp(_ptr(scores), _ptr(v), _ptr(lengths), B, L1, L2,
+                                        *map(float, params), _ptr(out), _ptr(gt), _ptr(ws), nbytes,
+                                        _stream(dev))
+        else:
+            rc = _LIB.swb_sw_hvp(_ptr(scores), _ptr(v), _ptr(lengths), B, L1, L2, *map(float, params),
+                                 _ptr(out), _ptr(gt), _ptr(ws), nbytes, _stream(dev))
+    _lib.check(rc, "soft Smith-Waterman HVP")
+    return out, gt
+
+
+def run_param_jacobian(fam, scores, lengths, params, which):
+    B, L1, L2 = scores.shape
+    dev = scores.device
+    out = torch.empty_like(scores)
+    if B == 0:
+        return out
+    aff = fam == "sw_affine"
+    nbytes = (_LIB.swb_sw_affine_aux_workspace_bytes if aff else _LIB.swb_sw_aux_workspace_bytes)(B, L1, L2)
+    ws = _aux_ws(nbytes, dev)
+    with torch.cuda.device(dev):
+        fn = _LIB.swb_sw_affine_param_jacobian if aff else _LIB.swb_sw_param_jacobian
+        rc = fn(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params), int(which), _ptr(out),
+                _ptr(ws), nbytes, _stream(dev))
+    _lib.check(rc, "soft Smith-Waterman parameter Jacobian")
+    return out
+
+
+def sw_affine_marginals_hvp(scores, v, gap_open, gap_ext, temp, lengths):
+    """orihime::sw_affine_marginals_hvp (src/sw_affine/torch_cuda.cpp:866 -> :508)."""
+    check_input_cuda(scores, "scores")
+    _check_like(scores, v, "tangent", "scores and tangent must have same shape")
+    ln = _prep(scores, lengths, "sw_affine")
+    return run_hvp("sw_affine", scores, v, ln, (gap_open, gap_ext, temp))[0]
+
+
+def _affine_param(which):
+    def op(scores, gap_open, gap_ext, temp, lengths):
+        ln = _prep(scores, lengths, "sw_affine")
+        return run_param_jacobian("sw_affine", scores, ln, (gap_open, gap_ext, temp), which)
+    op.__doc__ = (f"orihime::sw_affine_marginals_grad_* param {which} "
+                  "(src/sw_affine/torch_cuda.cpp:878-910 -> :580)")
+    return op
+
+
+def sw_affine_marginals_backward(scores, grad_marginals, gap_open, gap_ext, temp, lengths):
+    """orihime::sw_affine_marginals_backward -> (grad_scores, d/dgo [1], d/dge [1], d/dT [1])
+    (src/sw_affine/torch_cuda.cpp:854 -> soft_sw_affine_backward_full_cuda :681-811).
+
+    One tangent pass along the cotangent G: grad_scores = H.G (the Hessian is
+    symmetric) and sum(G * dP/dtheta) = d/dG (dS/dtheta), the tangents of the
+    parameter gradients, summed over the batch."""
+    check_input_cuda(scores, "scores")
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    if grad_marginals.shape != scores.shape:
+        raise RuntimeError("grad_alignment must have same shape as scores")
+    if not grad_marginals.is_cuda:
+        raise RuntimeError("grad_alignment must be a CUDA tensor")
+    if grad_marginals.device != scores.device:
+        raise RuntimeError(f"grad_alignment must be on same device as scores, got "
+                           f"{grad_marginals.device} vs {scores.device}")
+    g = grad_marginals.contiguous().to(torch.float32)
+    ln = _prep(scores, lengths, "sw_affine")
+    out, gt = run_hvp("sw_affine", scores, g, ln, (gap_open, gap_ext, temp), want_grads=True)
+    tot = gt[:, :3].sum(0)
+    return out, tot[0:1].clone(), tot[1:2].clone(), tot[2:3].clone()
+
+
+def sw_marginals_hvp(scores, v, gap, temp, lengths):
+    """orihime::sw_marginals_hvp (src/sw/torch_cuda.cpp:766 -> soft_sw_regular_hvp_cuda :453)."""
+    check_input_cuda(scores, "scores")
+    _check_like(scores, v, "tangent", "scores and tangent must have same shape")
+    ln = _prep(scores, lengths, "sw")
+    return run_hvp("sw", scores, v, ln, (gap, temp))[0]
+
+
+def _linear_param(which):
+    def op(scores, gap, temp, lengths):
+        ln = _prep(scores, lengths, "sw")
+        return run_param_jacobian("sw", scores, ln, (gap, temp), which)
+    op.__doc__ = f"orihime::sw_marginals_grad_* param {which} (src/sw/torch_cuda.cpp:777-796 -> soft_sw_regular_param_jacobian_cuda :519)"
+    return op
+
+
+def sw_marginals_backward(scores, grad_marginals, gap, temp, lengths):
+    """orihime::sw_marginals_backward -> (grad_scores, d/dgap [1], d/dT [1])
+    (src/sw/torch_cuda.cpp:755 -> soft_sw_backward_full_cuda :612)."""
+    check_input_cuda(scores, "scores")
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    if grad_marginals.shape != scores.shape:
+        raise RuntimeError("grad_alignment must have same shape as scores")
+    if not grad_marginals.is_cuda:
+        raise RuntimeError("grad_alignment must be a CUDA tensor")
+    if grad_marginals.device != scores.device:
+        raise RuntimeError(f"grad_alignment must be on same device as scores, got "
+                           f"{grad_marginals.device} vs {scores.device}")
+    g = grad_marginals.contiguous().to(torch.float32)
+    ln = _prep(scores, lengths, "sw")
+    out, gt = run_hvp("sw", scores, g, ln, (gap, temp), want_grads=True)
+    tot = gt[:, :2].sum(0)
+    return out, tot[0:1].clone(), tot[1:2].clone()
+
+
 IMPLS = {
+    "sw_marginals_hvp": sw_marginals_hvp,
+    "sw_marginals_grad_gap": _linear_param(0),
+    "sw_marginals_grad_temp": _linear_param(1),
+    "sw_marginals_backward": sw_marginals_backward,
+    "sw_affine_marginals_hvp": sw_affine_marginals_hvp,
+    "sw_affine_marginals_grad_gap_open": _affine_param(0),
+    "sw_affine_marginals_grad_gap_ext": _affine_param(1),
+    "sw_affine_marginals_grad_temp": _affine_param(2),
+    "sw_affine_marginals_backward": sw_affine_marginals_backward,
     "sw_forward": sw_forward,
     "sw_forward_t": sw_forward_t,
     "sw_value_grad_params": sw_value_grad_params,

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "sw_kernels.cu"
+#include "sw_aux.cu"
 #include "sw_probe.cuh"
 #include "../../include/orihime_b200.h"
 
@@ -273,9 +274,103 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
   return SWB_ERR_ARG;
 }
 
+// ---- second-order ops (sw_aux.cu) ----
+
+template <int NS>
+size_t aux_tab_floats(long long L1m, long long L2m) {
+  return (size_t)3 * NS * swb::aux_cells((int)L1m, (int)L2m);
+}
+template <int NS>
+size_t aux_roll_floats(long long L1m) {
+  return (size_t)3 * (size_t)(L1m + 1) * 2 * swb::AuxShape<NS>::NPUSH;
+}
+template <int NS>
+size_t aux_ws_bytes(long long B, long long L1m, long long L2m) {
+  if (B <= 0) return 0;
+  return align_up(sizeof(float) * (size_t)B * aux_tab_floats<NS>(L1m, L2m)) +
+         align_up(sizeof(float) * (size_t)B * aux_roll_floats<NS>(L1m));
+}
+
+template <int NS, int MODE>
+int launch_aux(const float* scores, const float* v, const int* lengths, int B, int L1m, int L2m,
+               float go, float ge, float T, float* out, float* gt, void* ws, size_t ws_bytes,
+               void* stream_v) {
+  if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
+  if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
+  if (B == 0) return SWB_OK;
+  const size_t map_elems = (size_t)B * L1m * L2m;
+  if (map_elems > 0 && (!scores || !out || (MODE == swb::AUX_HVP && !v))) return SWB_ERR_ARG;
+  const size_t need = aux_ws_bytes<NS>(B, L1m, L2m);
+  if (!ws || ws_bytes < need) return SWB_ERR_WORKSPACE;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream_v);
+  if (map_elems > 0 && cudaMemsetAsync(out, 0, map_elems * sizeof(float), st) != cudaSuccess)
+    return SWB_ERR_CUDA;
+  swb::AuxArgs a{};
+  a.scores = scores; a.v = v; a.lengths = lengths;
+  a.B = B; a.L1m = L1m; a.L2m = L2m;
+  a.go = go; a.ge = ge; a.T = T; a.k = 1.4426950408889634f / T;
+  a.out = out; a.gt = gt;
+  a.tab_pair = aux_tab_floats<NS>(L1m, L2m);
+  a.roll_pair = aux_roll_floats<NS>(L1m);
+  char* w = static_cast<char*>(ws);
+  a.tab = reinterpret_cast<float*>(w);
+  a.roll = reinterpret_cast<float*>(w + align_up(sizeof(float) * (size_t)B * a.tab_pair));
+  swb::aux_kernel<NS, MODE><<<B, swb::AUX_THREADS, 0, st>>>(a);
+  return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+}
+
 }  // namespace
 
 extern "C" {
+
+size_t swb_sw_affine_aux_workspace_bytes(int B, int L1max, int L2max) {
+  return aux_ws_bytes<3>(B, L1max, L2max);
+}
+
+size_t swb_sw_aux_workspace_bytes(int B, int L1max, int L2max) {
+  return aux_ws_bytes<1>(B, L1max, L2max);
+}
+
+int swb_sw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
+                      int L2max, float gap_open, float gap_ext, float temp, float* out,
+                      float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_aux<3, swb::AUX_HVP>(scores, v, lengths, B, L1max, L2max, gap_open, gap_ext, temp,
+                                     out, grad_tangents, workspace, workspace_bytes, stream);
+}
+
+int swb_sw_affine_param_jacobian(const float* scores, const int* lengths, int B, int L1max,
+                                 int L2max, float gap_open, float gap_ext, float temp, int param,
+                                 float* out, void* workspace, size_t workspace_bytes, void* stream) {
+  switch (param) {
+    case 0: return launch_aux<3, swb::AUX_P0>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
+                                              gap_ext, temp, out, nullptr, workspace, workspace_bytes, stream);
+    case 1: return launch_aux<3, swb::AUX_P1>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
+                                              gap_ext, temp, out, nullptr, workspace, workspace_bytes, stream);
+    case 2: return launch_aux<3, swb::AUX_PT>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
+                                              gap_ext, temp, out, nullptr, workspace, workspace_bytes, stream);
+    default: return SWB_ERR_ARG;
+  }
+}
+
+int swb_sw_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max, int L2max,
+               float gap, float temp, float* out, float* grad_tangents, void* workspace,
+               size_t workspace_bytes, void* stream) {
+  return launch_aux<1, swb::AUX_HVP>(scores, v, lengths, B, L1max, L2max, gap, 0.f, temp, out,
+                                     grad_tangents, workspace, workspace_bytes, stream);
+}
+
+int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap, float temp, int param, float* out, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+  switch (param) {
+    case 0: return launch_aux<1, swb::AUX_P0>(scores, nullptr, lengths, B, L1max, L2max, gap, 0.f,
+                                              temp, out, nullptr, workspace, workspace_bytes, stream);
+    case 1: return launch_aux<1, swb::AUX_PT>(scores, nullptr, lengths, B, L1max, L2max, gap, 0.f,
+                                              temp, out, nullptr, workspace, workspace_bytes, stream);
+    default: return SWB_ERR_ARG;
+  }
+}
+
 
 size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;
