@@ -85,10 +85,12 @@ int swb_sw_affine_forward(const float* scores, const int* lengths, int B, int L1
  * allocator).  Scratch is one file-scope device array of
  * SWB_STATIC_SCRATCH_BYTES per device; whatever must start at zero or at the
  * sentinel is reset with cudaMemsetAsync on `stream` at every call.
- *   - Limit: returns SWB_ERR_WORKSPACE, before any CUDA call, when the batch
- *     needs more than SWB_STATIC_SCRATCH_BYTES, i.e. when
- *     swb_sw_affine_workspace_bytes(B, L1max, L2max) exceeds it (about
- *     16 x 512 x 512 or one 2048 x 2048 pair fit).
+ *   - Limit: returns SWB_ERR_WORKSPACE, before any CUDA call, when the
+ *     batch's workspace at the chosen columns per lane exceeds
+ *     SWB_STATIC_SCRATCH_BYTES.  Every batch whose
+ *     swb_sw_affine_workspace_bytes(B, L1max, L2max) is within the limit
+ *     fits (e.g. 8 x 512 x 512); at the default 4 columns per lane about
+ *     12 x 512 x 512 or one 2048 x 2048 pair fit.
  *   - The first call on each device looks up the array's device address
  *     (cudaGetSymbolAddress, which may load the module) and sets up the
  *     kernels; make that first call before any stream capture.

@@ -50,7 +50,10 @@ namespace swb {
 
 constexpr float NEG = -1e30f;           // "no path" in the scaled domain
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int C_STEPS = 8;              // checkpoint stride (steps)
+#ifndef SWB_C_STEPS
+#define SWB_C_STEPS 4
+#endif
+constexpr int C_STEPS = SWB_C_STEPS;    // checkpoint stride (steps)
 constexpr int PF = 4;                   // score prefetch distance (steps); C_STEPS % PF == 0
 constexpr uint32_t SENTINEL_BITS = 0xffffffffu;
 
