@@ -201,9 +201,14 @@ __device__ __forceinline__ void store_row(const Pair& pr, int i, int jl, const f
 }
 
 // Values crossing a band edge forward (2*NS: hi and lo of each state), pushes
-// crossing it backward (NP), checkpoint floats per lane (CKF), adjoint fields
-// per cell (WF: normalised predecessor weights, beta-init terms, scaled score)
-// and shared-memory floats per lane per recomputed step (EW).
+// crossing it backward (NP), checkpoint floats per lane (CKF), and
+// shared-memory floats per lane per recomputed step (EW: WF adjoint fields per
+// cell).
+// WF: adjoint fields per cell.  affine: the weights of M's diagonal
+// predecessors M, I, D, of I's upper predecessors M, I and of D's left
+// predecessors M, D, the beta-init terms of M, I, D and the scaled score.
+// linear: the map factor (diagonal + start weights), the diagonal, upper and
+// left weights, the beta-init term and the scaled score.
 template <int NS> struct Shape;
 template <> struct Shape<3> { static constexpr int NP = 5, WF = 11; };
 template <> struct Shape<1> { static constexpr int NP = 2, WF = 6; };
@@ -211,25 +216,66 @@ template <> struct Shape<1> { static constexpr int NP = 2, WF = 6; };
 template <int NS, int R> struct Dims {
   static constexpr int NE = 2 * NS;
   static constexpr int NP = Shape<NS>::NP;
-  static constexpr int CKF = 2 * NS * R + 2 * NS;
-  static constexpr int WF = Shape<NS>::WF;
-  static constexpr int EW = WF * R;
+  static constexpr int CKF = 2 * NS * R + 2 * NS;   // checkpoint floats per lane (even)
+  static constexpr int CK4 = CKF / 4;               // ... stored as CK4 float4
+  static constexpr int CK2 = (CKF % 4) / 2;         // ... and CK2 (0 or 1) float2
+  static constexpr int WF = Shape<NS>::WF;         // adjoint fields per cell
+  static constexpr int EW = WF * R;                 // shared floats per lane per step
 };
 
-// Adjoint fields of a cell (kind index; shared-memory field = kind * R + c).
-// affine: weights of M's diagonal predecessors M, I, D; of I's upper
-// predecessors M, I; of D's left predecessors M, D; beta-init of M, I, D;
-// scaled score.
-enum : int { W_MM = 0, W_MI, W_MD, W_IM, W_II, W_DM, W_DD, B_M, B_I, B_D, W_SA };
-// linear: the map factor (diagonal + start weights), weights of the diagonal,
-// upper and left predecessors, beta-init, scaled score.
-enum : int { V_P = 0, V_A, V_U, V_L, V_B, V_S };
+// Checkpoint of one lane: hi of its R columns per state, lo of the same, then
+// hi and lo of its left neighbour per state.
+template <int NS, int R>
+__device__ __forceinline__ void ck_pack(const float (&ph)[NS][R], const float (&pl)[NS][R],
+                                        const float (&lh)[NS], const float (&ll)[NS],
+                                        float (&v)[Dims<NS, R>::CKF]) {
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+#pragma unroll
+    for (int c = 0; c < R; ++c) { v[q * R + c] = ph[q][c]; v[NS * R + q * R + c] = pl[q][c]; }
+    v[2 * NS * R + q] = lh[q];
+    v[2 * NS * R + NS + q] = ll[q];
+  }
+}
 
-// checkpoint field indices
-template <int NS, int R> __device__ __forceinline__ int ck_h(int q, int c) { return q * R + c; }
-template <int NS, int R> __device__ __forceinline__ int ck_l(int q, int c) { return NS * R + q * R + c; }
-template <int NS, int R> __device__ __forceinline__ int ck_lh(int q) { return 2 * NS * R + q; }
-template <int NS, int R> __device__ __forceinline__ int ck_ll(int q) { return 2 * NS * R + NS + q; }
+// Checkpoint chunk layout: CK4 groups of [lane][4] floats, then [lane][2].
+template <int NS, int R>
+__device__ __forceinline__ void ck_store(float* chunk, int lane, const float (&v)[Dims<NS, R>::CKF]) {
+  using D = Dims<NS, R>;
+#pragma unroll
+  for (int g = 0; g < D::CK4; ++g)
+    reinterpret_cast<float4*>(chunk + g * 128)[lane] =
+        make_float4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
+  if constexpr (D::CK2 == 1)
+    reinterpret_cast<float2*>(chunk + D::CK4 * 128)[lane] =
+        make_float2(v[4 * D::CK4], v[4 * D::CK4 + 1]);
+}
+
+template <int NS, int R>
+__device__ __forceinline__ void ck_load(const float* chunk, int lane, float (&v)[Dims<NS, R>::CKF]) {
+  using D = Dims<NS, R>;
+#pragma unroll
+  for (int g = 0; g < D::CK4; ++g) {
+    const float4 x = reinterpret_cast<const float4*>(chunk + g * 128)[lane];
+    v[4 * g] = x.x; v[4 * g + 1] = x.y; v[4 * g + 2] = x.z; v[4 * g + 3] = x.w;
+  }
+  if constexpr (D::CK2 == 1) {
+    const float2 x = reinterpret_cast<const float2*>(chunk + D::CK4 * 128)[lane];
+    v[4 * D::CK4] = x.x; v[4 * D::CK4 + 1] = x.y;
+  }
+}
+
+template <int NS, int R>
+__device__ __forceinline__ void ck_unpack(const float (&v)[Dims<NS, R>::CKF], float (&ph)[NS][R],
+                                          float (&pl)[NS][R], float (&lh)[NS], float (&ll)[NS]) {
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+#pragma unroll
+    for (int c = 0; c < R; ++c) { ph[q][c] = v[q * R + c]; pl[q][c] = v[NS * R + q * R + c]; }
+    lh[q] = v[2 * NS * R + q];
+    ll[q] = v[2 * NS * R + NS + q];
+  }
+}
 
 // ---------------------------------------------------------------------------
 // forward cell
@@ -250,24 +296,60 @@ __device__ __forceinline__ void two_sum(float a, float b, float& h, float& l) {
   l = (a - (h - bb)) + (b - bb);
 }
 
+// Adjoint fields of column c in one step's shared-memory entry `ent`, stored
+// column block by column block; inside a block each field group is one
+// vector per lane (lane-contiguous, so every warp access is conflict-free).
+// affine (11 floats): A = (wMM, wMI, wMD, wIM), B = (wII, wDM, wDD, bM0),
+// C = (bI0, bD0), s; linear (6 floats): A = (map factor, wA, wU, wL),
+// C = (b0, s).  s is the cell's scaled score.
+template <int NS, int R>
+__device__ __forceinline__ void put_fields(float* ent, int lane, int c, float4 A, float4 B, float2 C,
+                                           float sc) {
+  float* col = ent + c * Shape<NS>::WF * 32;
+  reinterpret_cast<float4*>(col)[lane] = A;
+  if constexpr (NS == 3) {
+    reinterpret_cast<float4*>(col + 128)[lane] = B;
+    reinterpret_cast<float2*>(col + 256)[lane] = C;
+    col[320 + lane] = sc;
+  } else {
+    reinterpret_cast<float2*>(col + 128)[lane] = make_float2(C.x, sc);
+  }
+}
+template <int NS, int R>
+__device__ __forceinline__ void get_fields(const float* ent, int lane, int c, float4& A, float4& B,
+                                           float2& C, float& sc) {
+  const float* col = ent + c * Shape<NS>::WF * 32;
+  A = reinterpret_cast<const float4*>(col)[lane];
+  if constexpr (NS == 3) {
+    B = reinterpret_cast<const float4*>(col + 128)[lane];
+    C = reinterpret_cast<const float2*>(col + 256)[lane];
+    sc = col[320 + lane];
+  } else {
+    C = reinterpret_cast<const float2*>(col + 128)[lane];
+    sc = C.y;
+  }
+}
+
 // One step of the forward wavefront for one lane.  Inputs: previous-row pairs
 // (ph, pl), left pairs of this row (lfh, lfl, already received), diag pairs of
 // column 0 (dgh0, dgl0: left lane, previous row) and the scaled scores s.
-// Writes the new row into (ph, pl) when act and returns it in (nh, nl).
+// Overwrites (ph, pl) with the new row.  A lane whose row has not started yet
+// gets s = NEG from its caller, which keeps every state at NEG (the row-0
+// boundary); rows past the pair's end compute values nothing reads.
 //
-// WT (adjoint recompute): also writes each cell's adjoint fields to shared
-// memory at wout[(kind * R + c) * 32].  The predecessor weights are the
-// recurrence's own softmax terms divided by their sum, so they add up to 1
-// per cell up to rounding and the adjoint conserves probability flow exactly;
-// beta-init = exp2(min(x - S, 0)) for the first `nlive` columns, 0 beyond.
+// WT (adjoint recompute): also writes each cell's adjoint fields to the
+// shared-memory entry `went` (put_fields).  The
+// predecessor weights are the recurrence's own softmax terms divided by their
+// sum, so they add up to 1 per cell up to rounding and the adjoint conserves
+// probability flow exactly; beta-init = exp2(min(x - S, 0)) for the first
+// `nlive` columns, 0 beyond.
 template <int NS, int R, bool WT = false>
 __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R],
                                           const float (&lfh)[NS], const float (&lfl)[NS],
                                           const float (&dgh0)[NS], const float (&dgl0)[NS],
-                                          const float (&s)[R], float g0, float g1, bool act,
-                                          float (&nh)[NS][R], float (&nl)[NS][R],
+                                          const float (&s)[R], float g0, float g1,
                                           float Sh = 0.f, float Sl = 0.f, int nlive = 0,
-                                          float* wout = nullptr) {
+                                          float* went = nullptr, int lane = 0) {
   float dgh[NS], dgl[NS], lh[NS], ll[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) { dgh[q] = dgh0[q]; dgl[q] = dgl0[q]; lh[q] = lfh[q]; ll[q] = lfl[q]; }
@@ -300,26 +382,20 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       float Dh, Dl;
       fast2(rl, dm + lg2(sd), Dh, Dl);
       if constexpr (WT) {
-        float* o = wout + c * 32;
         const float vm = recip(sm);
-        o[W_MM * R * 32] = tM * vm;
-        o[W_MI * R * 32] = tI * vm;
-        o[W_MD * R * 32] = tD * vm;
         const float vi = recip(si), wi = ti * vi;   // larger term: 1/si, smaller: ti/si
-        o[W_IM * R * 32] = ia >= ib ? vi : wi;
-        o[W_II * R * 32] = ia >= ib ? wi : vi;
         const float vd = recip(sd), wd = td * vd;
-        o[W_DM * R * 32] = da >= db ? vd : wd;
-        o[W_DD * R * 32] = da >= db ? wd : vd;
         const bool lv = c < nlive;
-        o[B_M * R * 32] = lv ? ex2(fminf((Mh - Sh) + (Ml - Sl), 0.f)) : 0.f;
-        o[B_I * R * 32] = lv ? ex2(fminf((Ih - Sh) + (Il - Sl), 0.f)) : 0.f;
-        o[B_D * R * 32] = lv ? ex2(fminf((Dh - Sh) + (Dl - Sl), 0.f)) : 0.f;
-        o[W_SA * R * 32] = s[c];
+        const float bM = lv ? ex2(fminf((Mh - Sh) + (Ml - Sl), 0.f)) : 0.f;
+        const float bI = lv ? ex2(fminf((Ih - Sh) + (Il - Sl), 0.f)) : 0.f;
+        const float bD = lv ? ex2(fminf((Dh - Sh) + (Dl - Sl), 0.f)) : 0.f;
+        put_fields<NS, R>(went, lane, c, make_float4(tM * vm, tI * vm, tD * vm, ia >= ib ? vi : wi),
+                          make_float4(ia >= ib ? wi : vi, da >= db ? vd : wd, da >= db ? wd : vd, bM),
+                          make_float2(bI, bD), s[c]);
       }
-      nh[0][c] = Mh; nl[0][c] = Ml; nh[1][c] = Ih; nl[1][c] = Il; nh[2][c] = Dh; nl[2][c] = Dl;
       dgh[0] = uMh; dgl[0] = uMl; dgh[1] = uIh; dgl[1] = uIl; dgh[2] = uDh; dgl[2] = uDl;
       lh[0] = Mh; ll[0] = Ml; lh[1] = Ih; ll[1] = Il; lh[2] = Dh; ll[2] = Dl;
+      ph[0][c] = Mh; pl[0][c] = Ml; ph[1][c] = Ih; pl[1][c] = Il; ph[2][c] = Dh; pl[2][c] = Dl;
     } else {
       const float uh = ph[0][c], ul = pl[0][c];
       // A = LSE(diag + s, up + g, left + g, s)
@@ -334,25 +410,15 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       float Ah, Al;
       fast2(r, lg2(sm), Ah, Al);
       if constexpr (WT) {
-        float* o = wout + c * 32;
         const float v = recip(sm);
-        o[V_P * R * 32] = (ta + ts) * v;
-        o[V_A * R * 32] = ta * v;
-        o[V_U * R * 32] = tu * v;
-        o[V_L * R * 32] = tl * v;
-        o[V_B * R * 32] = c < nlive ? ex2(fminf((Ah - Sh) + (Al - Sl), 0.f)) : 0.f;
-        o[V_S * R * 32] = s[c];
+        const float bA = c < nlive ? ex2(fminf((Ah - Sh) + (Al - Sl), 0.f)) : 0.f;
+        put_fields<NS, R>(went, lane, c, make_float4((ta + ts) * v, ta * v, tu * v, tl * v),
+                          make_float4(0.f, 0.f, 0.f, 0.f), make_float2(bA, 0.f), s[c]);
       }
-      nh[0][c] = Ah; nl[0][c] = Al;
       dgh[0] = uh; dgl[0] = ul;
       lh[0] = Ah; ll[0] = Al;
+      ph[0][c] = Ah; pl[0][c] = Al;
     }
-  }
-  if (act) {
-#pragma unroll
-    for (int q = 0; q < NS; ++q)
-#pragma unroll
-      for (int c = 0; c < R; ++c) { ph[q][c] = nh[q][c]; pl[q][c] = nl[q][c]; }
   }
 }
 
@@ -418,17 +484,9 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
 
   for (int kc = 0; kc < nch; ++kc) {
     {  // checkpoint: state before step kc*C
-      float* dst = ck + (size_t)kc * D::CKF * 32 + lane;
-#pragma unroll
-      for (int q = 0; q < NS; ++q) {
-#pragma unroll
-        for (int c = 0; c < R; ++c) {
-          dst[ck_h<NS, R>(q, c) * 32] = ph[q][c];
-          dst[ck_l<NS, R>(q, c) * 32] = pl[q][c];
-        }
-        dst[ck_lh<NS, R>(q) * 32] = lh[q];
-        dst[ck_ll<NS, R>(q) * 32] = ll[q];
-      }
+      float v[D::CKF];
+      ck_pack<NS, R>(ph, pl, lh, ll, v);
+      ck_store<NS, R>(ck + (size_t)kc * D::CKF * 32, lane, v);
     }
     if (kc + 1 < nch) load_edge(kc + 1, ebn);
 #pragma unroll 1
@@ -482,13 +540,12 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
       }
       float s[R];
 #pragma unroll
-      for (int c = 0; c < R; ++c) s[c] = __fmul_rn(sb[u][c], k);
+      for (int c = 0; c < R; ++c) s[c] = i >= 1 ? __fmul_rn(sb[u][c], k) : NEG;
       {
         const int ip = i + PF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
-      float nh[NS][R], nl[NS][R];
-      fwd_cells<NS, R>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, act, nh, nl);
+      fwd_cells<NS, R>(ph, pl, lh, ll, dgh, dgl, s, g0, g1);
       if (act) {
         // partition: lazily rescaled Kahan sum of ex2(x - ref); exponents stay
         // <= 8 so (hi - ref) + lo rounds at <= 2^-21 absolute
@@ -497,7 +554,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
         for (int c = 0; c < R; ++c)
           if (jl + c < L2)
 #pragma unroll
-            for (int q = 0; q < NS; ++q) mx = fmaxf(mx, nh[q][c] + nl[q][c]);
+            for (int q = 0; q < NS; ++q) mx = fmaxf(mx, ph[q][c]);
         if (mx > ref + 8.f) {
           float f = ex2(ref - mx);
           acc.s *= f;
@@ -509,7 +566,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
         for (int c = 0; c < R; ++c)
           if (jl + c < L2)
 #pragma unroll
-            for (int q = 0; q < NS; ++q) tsum += ex2((nh[q][c] - ref) + nl[q][c]);
+            for (int q = 0; q < NS; ++q) tsum += ex2((ph[q][c] - ref) + pl[q][c]);
         acc.add(tsum);
         if (lane == 31) {
 #pragma unroll
@@ -671,11 +728,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
   float ebr[NE];            // lane u < C: left-band edge pair of lane 0's row at recompute step u
   float pbc[NP], pbn[NP];   // lane u < C: right-band pushes lane 31 needs at adjoint step u
   float sb[PF][R];          // per-lane scores of the first PF recompute steps
-  auto load_ck = [&](int kc) {
-    const float* src = ck + (size_t)kc * CKF * 32 + lane;
-#pragma unroll
-    for (int f = 0; f < CKF; ++f) ckr[f] = src[f * 32];
-  };
+  auto load_ck = [&](int kc) { ck_load<NS, R>(ck + (size_t)kc * CKF * 32, lane, ckr); };
   auto load_eb = [&](int kc) {
     const int i = kc * C_STEPS + lane + 1;
     const bool ok = ein && lane < C_STEPS && i <= L1;
@@ -721,16 +774,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
     float cA = 0.f, cB = 0.f, cS = 0.f;   // this chunk's plain sums
     // ---- restore the checkpoint and recompute the chunk's adjoint fields ----
     float ph[NS][R], pl[NS][R], lh[NS], ll[NS];
-#pragma unroll
-    for (int q = 0; q < NS; ++q) {
-#pragma unroll
-      for (int c = 0; c < R; ++c) {
-        ph[q][c] = ckr[ck_h<NS, R>(q, c)];
-        pl[q][c] = ckr[ck_l<NS, R>(q, c)];
-      }
-      lh[q] = ckr[ck_lh<NS, R>(q)];
-      ll[q] = ckr[ck_ll<NS, R>(q)];
-    }
+    ck_unpack<NS, R>(ckr, ph, pl, lh, ll);
 #pragma unroll 1
     for (int u0 = 0; u0 < C_STEPS; u0 += PF)
 #pragma unroll
@@ -759,14 +803,13 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
       }
       float s[R];
 #pragma unroll
-      for (int c = 0; c < R; ++c) s[c] = __fmul_rn(sb[u][c], k);
+      for (int c = 0; c < R; ++c) s[c] = i >= 1 ? __fmul_rn(sb[u][c], k) : NEG;
       if (cu + PF < C_STEPS) {
         const int ip = i + PF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
-      float nh[NS][R], nl[NS][R];
-      fwd_cells<NS, R, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, act, nh, nl, Sh, Sl,
-                             act ? ncols : 0, sm + (size_t)cu * EW * 32 + lane);
+      fwd_cells<NS, R, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, Sh, Sl, act ? ncols : 0,
+                             sm + (size_t)cu * EW * 32, lane);
     }
     if (kc > 0) {  // prefetch the next chunk's inputs while the adjoint runs
       load_ck(kc - 1);
@@ -782,7 +825,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
       const int t = t0 + ent;
       const int i = t - lane + 1;
       const bool act = (i >= 1) && (i <= L1);
-      const float* E = sm + (size_t)ent * EW * 32 + lane;
+      const float* E = sm + (size_t)ent * EW * 32;
       float r[NP], pw[NP];
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
@@ -837,20 +880,24 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
 #pragma unroll
       for (int c = R - 1; c >= 0; --c) {
         const bool live = act && c < ncols;
-        auto F = [&](int kind) { return E[(kind * R + c) * 32]; };
         if constexpr (NS == 3) {
-          const float bM = live ? F(B_M) + ac[0][c] : 0.f;
-          const float bI = live ? F(B_I) + ac[1][c] : 0.f;
-          const float bD = live ? F(B_D) + ac[2][c] : 0.f;
+          float4 f0, f1;
+          float2 f2;
+          float sc;
+          get_fields<NS, R>(E, lane, c, f0, f1, f2, sc);
+          // f0 = (wMM, wMI, wMD, wIM), f1 = (wII, wDM, wDD, bM0), f2 = (bI0, bD0)
+          const float bM = live ? f1.w + ac[0][c] : 0.f;
+          const float bI = live ? f2.x + ac[1][c] : 0.f;
+          const float bD = live ? f2.y + ac[2][c] : 0.f;
           pm[c] = bM;
-          const float pIM = bI * F(W_IM), pII = bI * F(W_II);
-          const float pDM = bD * F(W_DM), pDD = bD * F(W_DD);
+          const float pIM = bI * f0.w, pII = bI * f1.x;
+          const float pDM = bD * f1.y, pDD = bD * f1.z;
           cA += pIM + pDM;
           cB += pII + pDD;
-          cS += bM * F(W_SA);
+          cS += bM * sc;
           nx[0][c] += pIM;
           nx[1][c] += pII;
-          const float qM = bM * F(W_MM), qI = bM * F(W_MI), qD = bM * F(W_MD);
+          const float qM = bM * f0.x, qI = bM * f0.y, qD = bM * f0.z;
           if (c > 0) {
             nx[0][c - 1] += qM; nx[1][c - 1] += qI; nx[2][c - 1] += qD;
             ac[0][c - 1] += pDM; ac[2][c - 1] += pDD;
@@ -858,12 +905,17 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
             outp[0] = pDM; outp[1] = pDD; outp[2] = qM; outp[3] = qI; outp[4] = qD;
           }
         } else {
-          const float b = live ? F(V_B) + ac[0][c] : 0.f;
-          const float pv_ = b * F(V_P);
+          float4 f0, f1;
+          float2 f2;
+          float sc;
+          get_fields<NS, R>(E, lane, c, f0, f1, f2, sc);
+          // f0 = (map factor, wA, wU, wL), f2.x = b0
+          const float b = live ? f2.x + ac[0][c] : 0.f;
+          const float pv_ = b * f0.x;
           pm[c] = pv_;
-          const float pU = b * F(V_U), pL = b * F(V_L), pD = b * F(V_A);
+          const float pU = b * f0.z, pL = b * f0.w, pD = b * f0.y;
           cA += pU + pL;
-          cS += pv_ * F(V_S);
+          cS += pv_ * sc;
           nx[0][c] += pU;
           if (c > 0) {
             nx[0][c - 1] += pD;
