@@ -54,7 +54,10 @@ constexpr unsigned FULL = 0xffffffffu;
 #define SWB_C_STEPS 4
 #endif
 constexpr int C_STEPS = SWB_C_STEPS;    // checkpoint stride (steps)
-constexpr int PF = 4;                   // score prefetch distance (steps); C_STEPS % PF == 0
+#ifndef SWB_PF
+#define SWB_PF 2
+#endif
+constexpr int PF = SWB_PF;              // score prefetch distance (steps); C_STEPS % PF == 0
 constexpr uint32_t SENTINEL_BITS = 0xffffffffu;
 
 // Ragged plan: per-pair words.  Offsets are in floats within the respective
