@@ -180,3 +180,92 @@ class Plan:
         with torch.cuda.graph(g):
             self.run(flat, out=out, **params)
         return g, out
+
+
+def split_groups(lengths, parts: int) -> list[tuple[int, int]]:
+    """Contiguous pair ranges [b0, b1) with about equal cells each (at most `parts`)."""
+    ln = np.asarray(lengths, dtype=np.int64).reshape(-1, 2)
+    B = ln.shape[0]
+    if B == 0:
+        return []
+    parts = max(1, min(int(parts), B))
+    cum = np.cumsum(ln[:, 0] * ln[:, 1])
+    total = int(cum[-1])
+    cuts, b0 = [], 0
+    for k in range(1, parts):
+        b = int(np.searchsorted(cum, total * k / parts, side="right"))
+        b = min(max(b, b0 + 1), B - (parts - k))
+        cuts.append((b0, b))
+        b0 = b
+    cuts.append((b0, B))
+    return [c for c in cuts if c[1] > c[0]]
+
+
+class StreamedPlan:
+    """A packed batch run straight from pinned host memory, with the
+    host-to-device copy overlapped with compute.
+
+    The pairs are split into `parts` contiguous groups of about equal cell
+    count, each with its own Plan.  A copy stream moves group k+1's scores
+    while the compute stream runs group k; the compute stream waits only for
+    its own group's copy.  The scores land in one device buffer in the same
+    packing, and the map comes back as one packed device buffer.
+
+        sp = ragged.StreamedPlan(lengths, offsets, parts=8, device="cuda")
+        out = sp.run(host_flat_pinned, gap_open=-2.0, gap_ext=-0.5, temp=0.5)
+    """
+
+    def __init__(self, lengths, offsets, family: str = "affine", device="cuda", parts: int = 8,
+                 cols_per_lane: int = 0):
+        ln = np.asarray(lengths, dtype=np.int32).reshape(-1, 2)
+        off = np.asarray(offsets, dtype=np.int64).reshape(-1)
+        self.device = torch.device(device)
+        if self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.family = family
+        self.B = ln.shape[0]
+        self.map_elems = int(off[-1]) if self.B else 0
+        self.groups = split_groups(ln, parts)
+        self.plans = []
+        for b0, b1 in self.groups:
+            sub_off = off[b0:b1 + 1] - off[b0]
+            self.plans.append(Plan(ln[b0:b1], sub_off, family=family, device=self.device,
+                                   cols_per_lane=cols_per_lane))
+        self.offsets = off
+        self.scores = torch.empty(max(self.map_elems, 1), dtype=torch.float32, device=self.device)
+        self.copy_stream = torch.cuda.Stream(self.device)
+        self.events = [torch.cuda.Event() for _ in self.groups]
+
+    def outputs(self) -> Result:
+        dev = self.device
+        e = lambda: torch.empty(self.B, dtype=torch.float32, device=dev)
+        return Result(e(), torch.empty(self.map_elems, dtype=torch.float32, device=dev), e(),
+                      e() if self.family == "affine" else None, e())
+
+    def run(self, host_flat: torch.Tensor, *, out: Optional[Result] = None, **params) -> Result:
+        """Copy `host_flat` (pinned, packed like `offsets`) group by group and
+        run each group as soon as its scores are on the device (asynchronous)."""
+        if host_flat.device.type != "cpu" or host_flat.dtype != torch.float32:
+            raise ValueError("host_flat must be a float32 CPU tensor (pinned for overlap)")
+        if host_flat.numel() < self.map_elems:
+            raise ValueError(f"host_flat has {host_flat.numel()} elements, the packing needs {self.map_elems}")
+        out = out or self.outputs()
+        compute = torch.cuda.current_stream(self.device)
+        # the copy stream must not overwrite scores a previous call still reads
+        self.copy_stream.wait_stream(compute)
+        for k, ((b0, b1), plan) in enumerate(zip(self.groups, self.plans)):
+            e0, e1 = int(self.offsets[b0]), int(self.offsets[b1])
+            with torch.cuda.stream(self.copy_stream):
+                self.scores[e0:e1].copy_(host_flat[e0:e1], non_blocking=True)
+                self.events[k].record(self.copy_stream)
+            compute.wait_event(self.events[k])
+            sub = Result(out.value[b0:b1], out.map[e0:e1], out.grad_open[b0:b1],
+                         None if out.grad_ext is None else out.grad_ext[b0:b1], out.grad_temp[b0:b1])
+            plan.run(self.scores[e0:e1], out=sub, **params)
+        return out
+
+    def status(self) -> int:
+        st = 0
+        for p in self.plans:
+            st |= p.status()
+        return st

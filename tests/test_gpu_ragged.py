@@ -94,3 +94,23 @@ def test_ragged_cuda_graph_replay():
     torch.cuda.synchronize()
     assert torch.equal(out.value, direct.value) and torch.equal(out.map, direct.map)
     assert not torch.equal(out.value, ref_v)
+
+
+def test_streamed_plan_from_pinned_host_matches_plan():
+    """Copy/compute-overlapped run from pinned host memory: same bits as one Plan."""
+    from orihime_b200 import ragged
+
+    ln = _lengths(37, 3, 16, 500)
+    mats = [_emb(int(a), int(b), 300 + i) for i, (a, b) in enumerate(ln)]
+    flat, off, lens = ragged.pack(mats)
+    host = flat.pin_memory()
+    params = dict(gap_open=-2.0, gap_ext=-0.5, temp=0.5)
+    ref = ragged.Plan(lens, off, family="affine", device="cuda").run(flat.cuda(), **params)
+    sp = ragged.StreamedPlan(lens, off, family="affine", device="cuda", parts=5)
+    assert len(sp.groups) == 5 and sp.groups[0][0] == 0 and sp.groups[-1][1] == len(lens)
+    for _ in range(2):  # the second call reuses the device buffers
+        out = sp.run(host, **params)
+        torch.cuda.synchronize()
+        assert sp.status() == 0
+        assert torch.equal(out.value, ref.value) and torch.equal(out.map, ref.map)
+        assert torch.equal(out.grad_open, ref.grad_open) and torch.equal(out.grad_temp, ref.grad_temp)
