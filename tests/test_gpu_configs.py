@@ -1,0 +1,115 @@
+"""The two remaining benchmark configurations, run on the GPU through the
+public API.
+
+* C5 is a training step. E and F are float32 leaf parameters of shape
+  [256, 512, 128] and the scores are bmm(E, F^T) / sqrt(128). The loss is
+  -sw_affine_value.mean() + 0.01 * sw_affine_entropy.mean(), run at
+  T in {0.25, 0.5, 1.0}. The entropy backward needs the dP/dT map. The
+  gradient reaching the scores is checked on sampled pairs against the fp64
+  oracle.
+* C4 is four 16384 x 16384 pairs with a band mask, |i - j| > 2048 excluded.
+  Its score generator is the same as C2's. The test records the peak device
+  memory against one fp32 three-state table; the reference keeps alpha and
+  beta and clones them. It also checks properties of the map.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA not available")
+    import orihime_b200  # noqa: F401
+
+
+@pytest.mark.parametrize("T", [0.25, 0.5, 1.0])
+def test_c5_training_step_grads_match_oracle(T):
+    import orihime_b200 as ohm
+
+    B, N, d = 256, 512, 128
+    g = torch.Generator().manual_seed(5)
+    E = torch.randn(B, N, d, generator=g).cuda().requires_grad_(True)
+    F = torch.randn(B, N, d, generator=g).cuda().requires_grad_(True)
+    kw = dict(gap_open_score=-2.0, gap_extend_score=-0.5, temperature=T)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    scores = torch.bmm(E, F.transpose(1, 2)) / d ** 0.5
+    scores.retain_grad()
+    loss = -ohm.sw_affine_value(scores, **kw).mean() + 0.01 * ohm.sw_affine_entropy(scores, **kw).mean()
+    loss.backward()
+    t1.record()
+    torch.cuda.synchronize()
+    print(f"  C5 T={T}: forward+backward {t0.elapsed_time(t1):.1f} ms, loss {float(loss):.4f}")
+    assert torch.isfinite(loss)
+    assert torch.isfinite(E.grad).all() and torch.isfinite(F.grad).all()
+    # chain rule into E, F
+    gs = scores.grad
+    assert torch.allclose(E.grad, torch.bmm(gs, F.detach()) / d ** 0.5, rtol=1e-4, atol=1e-7)
+    # dL/dscores = (-map + 0.01 * dP/dT) / B on sampled pairs, against fp64
+    s_np = scores.detach().cpu().numpy()
+    for b in (0, 131, 255):
+        sb = s_np[b:b + 1]
+        m64 = O.affine(sb, None, -2.0, -0.5, T, dtype=np.float64)["map"]
+        m32 = O.affine(sb, None, -2.0, -0.5, T)["map"]
+        p64 = O.affine_param_grad(sb, None, -2.0, -0.5, T, 2, dtype=np.float64)
+        p32 = O.affine_param_grad(sb, None, -2.0, -0.5, T, 2)
+        want64 = (-m64 + 0.01 * p64) / B
+        want32 = (-m32 + 0.01 * p32) / B
+        got = gs[b:b + 1].cpu().numpy().astype(np.float64)
+        e64 = float(np.abs(got - want64).max())
+        eref = float(np.abs(want32 - want64).max())
+        bound = max(1e-4 * float(np.abs(want64).max()), eref)
+        print(f"  pair {b}: ours-fp64 {e64:.2e} ref32-fp64 {eref:.2e} bound {bound:.2e}")
+        assert e64 <= bound
+
+
+def _c4_scores(B, L, band, seed, d=64, chunk=2048):
+    """3 <e_i, f_j> / sqrt(d) computed in row chunks on the device; cells with
+    |i - j| > band set to -inf (the public API's mask convention)."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    s = torch.empty(B, L, L, device="cuda")
+    for b in range(B):
+        e = torch.randn(L, d, generator=g, device="cuda")
+        f = torch.randn(L, d, generator=g, device="cuda")
+        for r0 in range(0, L, chunk):
+            s[b, r0:r0 + chunk] = 3.0 * (e[r0:r0 + chunk] @ f.T) / d ** 0.5
+    return s
+
+
+def test_c4_banded_16k_memory_and_properties():
+    import orihime_b200 as ohm
+
+    B, L, band = 4, 16384, 2048
+    s = _c4_scores(B, L, band, 4)
+    i = torch.arange(L, device="cuda")
+    excl = (i[:, None] - i[None, :]).abs() > band
+    mask = excl.expand(B, L, L)
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats()
+    base = torch.cuda.memory_allocated()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    m = ohm.sw_affine(s, gap_open_score=-2.0, gap_extend_score=-0.5, temperature=0.5, mask=mask)
+    v = ohm.sw_affine_value(s, gap_open_score=-2.0, gap_extend_score=-0.5, temperature=0.5, mask=mask)
+    t1.record()
+    torch.cuda.synchronize()
+    peak = torch.cuda.max_memory_allocated() - base
+    table = 3 * 4 * (L + 1) ** 2 * B          # one fp32 three-state table for the batch
+    print(f"  C4: map + value {t0.elapsed_time(t1):.0f} ms; peak extra device memory "
+          f"{peak / 2**30:.1f} GiB (inputs excluded), one three-state table {table / 2**30:.1f} GiB")
+    assert torch.isfinite(v).all() and torch.isfinite(m).all()
+    # excluded cells carry no probability; the map is a marginal: 0 <= P <= 1
+    for b in range(B):
+        assert float(torch.where(excl, m[b], torch.zeros((), device="cuda")).abs().max()) < 1e-6
+    assert float(m.min()) >= 0.0 and float(m.max()) <= 1.0 + 1e-5
+    # scores + masked copy + map + our workspace stay below the reference's
+    # alpha + beta + clones (about 47 GB for this batch)
+    assert peak < 0.75 * 47e9
