@@ -26,7 +26,10 @@
 namespace swb {
 
 enum : int { AUX_HVP = 0, AUX_P0 = 1, AUX_P1 = 2, AUX_PT = 3 };
-constexpr int AUX_THREADS = 512;
+#ifndef SWB_AUX_THREADS
+#define SWB_AUX_THREADS 256
+#endif
+constexpr int AUX_THREADS = SWB_AUX_THREADS;
 constexpr float LN2 = 0.69314718055994531f;
 
 struct AuxArgs {
@@ -193,11 +196,22 @@ __device__ __forceinline__ void wtan(const float* w, const float* t, float iT, f
   }
 }
 
-template <int NS, int MODE>
+// Shared-memory variant (SM): the forward sweep reads its predecessors from a
+// ring of the last three diagonals' alpha / tangent values in shared memory,
+// and the backward sweep keeps the push ring there, so the diagonal-to-
+// diagonal dependency costs shared-memory latency instead of an L2 round trip.
+// Ring layout [diag % 3][field][slot], slot = i - max(0, d - L2).
+template <int NS>
+__host__ __device__ constexpr int aux_ring_fields() {
+  return (3 * NS > 2 * AuxShape<NS>::NPUSH) ? 3 * NS : 2 * AuxShape<NS>::NPUSH;
+}
+
+template <int NS, int MODE, bool SM>
 __global__ void __launch_bounds__(AUX_THREADS) aux_kernel(AuxArgs a) {
   constexpr int NP = AuxShape<NS>::NPUSH;
   constexpr bool TM = (MODE == AUX_PT);
   __shared__ float red[2 * (AUX_THREADS / 32) * 4];
+  extern __shared__ float ring[];
   const int p = blockIdx.x;
   const int tid = threadIdx.x;
   int L1 = a.L1m, L2 = a.L2m;
@@ -223,6 +237,28 @@ __global__ void __launch_bounds__(AUX_THREADS) aux_kernel(AuxArgs a) {
   float* roll = a.roll + (size_t)p * a.roll_pair;
   const size_t rstride = (size_t)(L1 + 1) * 2 * NP;   // floats per rolling diagonal
   const float k = a.k, g0 = a.go * k, g1 = a.ge * k, T = a.T, iT = 1.f / a.T;
+  const int DLm = min(a.L1m, a.L2m) + 1;               // ring slots per diagonal (SM)
+  auto slot = [&](int i, int d) { return i - max(0, d - L2); };
+  // forward-sweep reads of alpha (hi, lo) and tangent of cell (i, j), state st
+  auto rd = [&](int st, int i, int j, float& h, float& l, float& u) {
+    if constexpr (SM) {
+      const int d = i + j;
+      const float* r = ring + (size_t)(d % 3) * 3 * NS * DLm + slot(i, d);
+      h = r[(size_t)st * DLm]; l = r[(size_t)(NS + st) * DLm]; u = r[(size_t)(2 * NS + st) * DLm];
+    } else {
+      const long long o = ix.at(i, j);
+      h = AH[st * nc + o]; l = AL[st * nc + o]; u = UU[st * nc + o];
+    }
+  };
+  auto wr = [&](int st, int i, int j, float h, float l, float u) {
+    const long long o = ix.at(i, j);
+    AH[st * nc + o] = h; AL[st * nc + o] = l; UU[st * nc + o] = u;
+    if constexpr (SM) {
+      const int d = i + j;
+      float* r = ring + (size_t)(d % 3) * 3 * NS * DLm + slot(i, d);
+      r[(size_t)st * DLm] = h; r[(size_t)(NS + st) * DLm] = l; r[(size_t)(2 * NS + st) * DLm] = u;
+    }
+  };
 
   // boundary cells: alpha = NEG, tangent 0
   for (int q = tid; q <= L1 + L2; q += AUX_THREADS) {
@@ -234,41 +270,55 @@ __global__ void __launch_bounds__(AUX_THREADS) aux_kernel(AuxArgs a) {
   __syncthreads();
 
   // ---- forward sweep: alpha and its tangent ----
-  for (int d = 2; d <= L1 + L2; ++d) {
-    const int i0 = max(1, d - L2), i1 = min(L1, d - 1);
+  // (SM: from diagonal 0, so the ring holds the boundary cells too)
+  for (int d = SM ? 0 : 2; d <= L1 + L2; ++d) {
+    const int i0 = max(SM ? 0 : 1, d - L2), i1 = min(L1, SM ? d : d - 1);
     for (int i = i0 + tid; i <= i1; i += AUX_THREADS) {
       const int j = d - i;
+      if (SM && (i == 0 || j == 0)) {
+#pragma unroll
+        for (int st = 0; st < NS; ++st) {
+          float* r = ring + (size_t)(d % 3) * 3 * NS * DLm + slot(i, d);
+          r[(size_t)st * DLm] = NEG; r[(size_t)(NS + st) * DLm] = 0.f; r[(size_t)(2 * NS + st) * DLm] = 0.f;
+        }
+        continue;
+      }
       const float sc = S_[(size_t)(i - 1) * ld + (j - 1)];
       const float s = __fmul_rn(sc, k);
-      const long long od = ix.at(i - 1, j - 1), ou = ix.at(i - 1, j), ol = ix.at(i, j - 1), o = ix.at(i, j);
       const float vv = (MODE == AUX_HVP) ? V_[(size_t)(i - 1) * ld + (j - 1)] : 0.f;
       if constexpr (NS == 3) {
-        float dh[3], dl[3];
+        float dh[3], dl[3], du[3], uh[2], ul[2], uu[2], lh[2], ll[2], lu[2];
 #pragma unroll
-        for (int st = 0; st < 3; ++st) { dh[st] = AH[st * nc + od]; dl[st] = AL[st * nc + od]; }
+        for (int st = 0; st < 3; ++st) rd(st, i - 1, j - 1, dh[st], dl[st], du[st]);
+        rd(0, i - 1, j, uh[0], ul[0], uu[0]);
+        rd(1, i - 1, j, uh[1], ul[1], uu[1]);
+        rd(0, i, j - 1, lh[0], ll[0], lu[0]);
+        rd(2, i, j - 1, lh[1], ll[1], lu[1]);
         AffCell c;
-        aff_cell(dh, dl, AH[ou], AL[ou], AH[nc + ou], AL[nc + ou], AH[ol], AL[ol], AH[2 * nc + ol],
-                 AL[2 * nc + ol], s, g0, g1, c);
-        AH[o] = c.Mh; AL[o] = c.Ml; AH[nc + o] = c.Ih; AL[nc + o] = c.Il;
-        AH[2 * nc + o] = c.Dh; AL[2 * nc + o] = c.Dl;
-        const float uM = c.wm[0] * UU[od] + c.wm[1] * UU[nc + od] + c.wm[2] * UU[2 * nc + od];
-        float tu0 = UU[ou], tu1 = UU[nc + ou], tl0 = UU[ol], tl1 = UU[2 * nc + ol];
+        aff_cell(dh, dl, uh[0], ul[0], uh[1], ul[1], lh[0], ll[0], lh[1], ll[1], s, g0, g1, c);
+        const float uM = c.wm[0] * du[0] + c.wm[1] * du[1] + c.wm[2] * du[2];
+        float tu0 = uu[0], tu1 = uu[1], tl0 = lu[0], tl1 = lu[1];
         if (MODE == AUX_P0) { tu0 += 1.f; tl0 += 1.f; }
         if (MODE == AUX_P1) { tu1 += 1.f; tl1 += 1.f; }
         float m = uM, ii = c.wi[0] * tu0 + c.wi[1] * tu1, dd = c.wd[0] * tl0 + c.wd[1] * tl1;
         if (MODE == AUX_HVP) m += vv;
         if (TM) { m += ent<4>(c.wm); ii += ent<2>(c.wi); dd += ent<2>(c.wd); }
-        UU[o] = m; UU[nc + o] = ii; UU[2 * nc + o] = dd;
+        wr(0, i, j, c.Mh, c.Ml, m);
+        wr(1, i, j, c.Ih, c.Il, ii);
+        wr(2, i, j, c.Dh, c.Dl, dd);
       } else {
+        float dh, dl, du, uh, ul, uu, lh, ll, lu;
+        rd(0, i - 1, j - 1, dh, dl, du);
+        rd(0, i - 1, j, uh, ul, uu);
+        rd(0, i, j - 1, lh, ll, lu);
         LinCell c;
-        lin_cell(AH[od], AL[od], AH[ou], AL[ou], AH[ol], AL[ol], s, g0, c);
-        AH[o] = c.Ah; AL[o] = c.Al;
-        float tu = UU[ou], tl = UU[ol];
+        lin_cell(dh, dl, uh, ul, lh, ll, s, g0, c);
+        float tu = uu, tl = lu;
         if (MODE == AUX_P0) { tu += 1.f; tl += 1.f; }
-        float u = c.w[0] * UU[od] + c.w[1] * tu + c.w[2] * tl;
+        float u = c.w[0] * du + c.w[1] * tu + c.w[2] * tl;
         if (MODE == AUX_HVP) u += (c.w[0] + c.w[3]) * vv;
         if (TM) u += ent<4>(c.w);
-        UU[o] = u;
+        wr(0, i, j, c.Ah, c.Al, u);
       }
     }
     __syncthreads();
@@ -324,20 +374,27 @@ __global__ void __launch_bounds__(AUX_THREADS) aux_kernel(AuxArgs a) {
   float acc[4] = {0.f, 0.f, 0.f, 0.f};   // tangents of g0, g1; sum Pdot*s; sum P*v
   for (int d = L1 + L2; d >= 2; --d) {
     const int i0 = max(1, d - L2), i1 = min(L1, d - 1);
-    float* rw = roll + (size_t)(d % 3) * rstride;
-    const float* r1 = roll + (size_t)((d + 1) % 3) * rstride;   // successors (i+1, j), (i, j+1)
-    const float* r2 = roll + (size_t)((d + 2) % 3) * rstride;   // successor (i+1, j+1)
+    // push rings: global [diag % 3][i][field] or shared [diag % 3][field][slot]
+    float* rw = SM ? ring + (size_t)(d % 3) * 2 * NP * DLm : roll + (size_t)(d % 3) * rstride;
+    const float* r1 = SM ? ring + (size_t)((d + 1) % 3) * 2 * NP * DLm
+                         : roll + (size_t)((d + 1) % 3) * rstride;   // successors (i+1, j), (i, j+1)
+    const float* r2 = SM ? ring + (size_t)((d + 2) % 3) * 2 * NP * DLm
+                         : roll + (size_t)((d + 2) % 3) * rstride;   // successor (i+1, j+1)
+    const size_t ps = SM ? (size_t)DLm : 1;   // stride between the fields of one cell
+    auto at = [&](const float* r, int i_, int d_) {
+      return SM ? r + slot(i_, d_) : r + (size_t)i_ * 2 * NP;
+    };
     for (int i = i0 + tid; i <= i1; i += AUX_THREADS) {
       const int j = d - i;
       const bool sD = (i < L1 && j < L2), sU = (i < L1), sL = (j < L2);
-      const float* pD = r2 + (size_t)(i + 1) * 2 * NP;   // pushes of (i+1, j+1)
-      const float* pU = r1 + (size_t)(i + 1) * 2 * NP;   // pushes of (i+1, j)
-      const float* pL = r1 + (size_t)i * 2 * NP;         // pushes of (i, j+1)
+      const float* pD = at(r2, i + 1, d + 2);   // pushes of (i+1, j+1)
+      const float* pU = at(r1, i + 1, d + 1);   // pushes of (i+1, j)
+      const float* pL = at(r1, i, d + 1);       // pushes of (i, j+1)
       const float sc = S_[(size_t)(i - 1) * ld + (j - 1)];
       const float s = __fmul_rn(sc, k);
       const float vv = (MODE == AUX_HVP) ? V_[(size_t)(i - 1) * ld + (j - 1)] : 0.f;
       const long long od = ix.at(i - 1, j - 1), ou = ix.at(i - 1, j), ol = ix.at(i, j - 1), o = ix.at(i, j);
-      float* w_out = rw + (size_t)i * 2 * NP;
+      float* w_out = const_cast<float*>(at(rw, i, d));
       if constexpr (NS == 3) {
         float dh[3], dl[3];
 #pragma unroll
@@ -346,10 +403,10 @@ __global__ void __launch_bounds__(AUX_THREADS) aux_kernel(AuxArgs a) {
         aff_cell(dh, dl, AH[ou], AL[ou], AH[nc + ou], AL[nc + ou], AH[ol], AL[ol], AH[2 * nc + ol],
                  AL[2 * nc + ol], s, g0, g1, c);
         // pushes layout: [MM, MI, MD, IM, II, DM, DD] then their tangents
-        float bM = sD ? pD[0] : 0.f, bI = sD ? pD[1] : 0.f, bD = sD ? pD[2] : 0.f;
-        float tM = sD ? pD[NP + 0] : 0.f, tI = sD ? pD[NP + 1] : 0.f, tD = sD ? pD[NP + 2] : 0.f;
-        if (sU) { bM += pU[3]; bI += pU[4]; tM += pU[NP + 3]; tI += pU[NP + 4]; }
-        if (sL) { bM += pL[5]; bD += pL[6]; tM += pL[NP + 5]; tD += pL[NP + 6]; }
+        float bM = sD ? pD[(0) * ps] : 0.f, bI = sD ? pD[(1) * ps] : 0.f, bD = sD ? pD[(2) * ps] : 0.f;
+        float tM = sD ? pD[(NP + 0) * ps] : 0.f, tI = sD ? pD[(NP + 1) * ps] : 0.f, tD = sD ? pD[(NP + 2) * ps] : 0.f;
+        if (sU) { bM += pU[(3) * ps]; bI += pU[(4) * ps]; tM += pU[(NP + 3) * ps]; tI += pU[(NP + 4) * ps]; }
+        if (sL) { bM += pL[(5) * ps]; bD += pL[(6) * ps]; tM += pL[(NP + 5) * ps]; tD += pL[(NP + 6) * ps]; }
         const float xs[3] = {(c.Mh - Sh) + (c.Ml - Sl), (c.Ih - Sh) + (c.Il - Sl), (c.Dh - Sh) + (c.Dl - Sl)};
         const float us[3] = {UU[o], UU[nc + o], UU[2 * nc + o]};
         float b[3] = {bM, bI, bD}, t[3] = {tM, tI, tD};
@@ -374,27 +431,27 @@ __global__ void __launch_bounds__(AUX_THREADS) aux_kernel(AuxArgs a) {
         wtan<2, TM>(c.wd, cd, iT, dwd);
         const float P = b[0], Pd = t[0];
         O_[(size_t)(i - 1) * ld + (j - 1)] = Pd;
-        w_out[0] = b[0] * c.wm[0]; w_out[1] = b[0] * c.wm[1]; w_out[2] = b[0] * c.wm[2];
-        w_out[3] = b[1] * c.wi[0]; w_out[4] = b[1] * c.wi[1];
-        w_out[5] = b[2] * c.wd[0]; w_out[6] = b[2] * c.wd[1];
-        w_out[NP + 0] = t[0] * c.wm[0] + b[0] * dwm[0];
-        w_out[NP + 1] = t[0] * c.wm[1] + b[0] * dwm[1];
-        w_out[NP + 2] = t[0] * c.wm[2] + b[0] * dwm[2];
-        w_out[NP + 3] = t[1] * c.wi[0] + b[1] * dwi[0];
-        w_out[NP + 4] = t[1] * c.wi[1] + b[1] * dwi[1];
-        w_out[NP + 5] = t[2] * c.wd[0] + b[2] * dwd[0];
-        w_out[NP + 6] = t[2] * c.wd[1] + b[2] * dwd[1];
+        w_out[(0) * ps] = b[0] * c.wm[0]; w_out[(1) * ps] = b[0] * c.wm[1]; w_out[(2) * ps] = b[0] * c.wm[2];
+        w_out[(3) * ps] = b[1] * c.wi[0]; w_out[(4) * ps] = b[1] * c.wi[1];
+        w_out[(5) * ps] = b[2] * c.wd[0]; w_out[(6) * ps] = b[2] * c.wd[1];
+        w_out[(NP + 0) * ps] = t[0] * c.wm[0] + b[0] * dwm[0];
+        w_out[(NP + 1) * ps] = t[0] * c.wm[1] + b[0] * dwm[1];
+        w_out[(NP + 2) * ps] = t[0] * c.wm[2] + b[0] * dwm[2];
+        w_out[(NP + 3) * ps] = t[1] * c.wi[0] + b[1] * dwi[0];
+        w_out[(NP + 4) * ps] = t[1] * c.wi[1] + b[1] * dwi[1];
+        w_out[(NP + 5) * ps] = t[2] * c.wd[0] + b[2] * dwd[0];
+        w_out[(NP + 6) * ps] = t[2] * c.wd[1] + b[2] * dwd[1];
         if (MODE == AUX_HVP) {
-          acc[0] += w_out[NP + 3] + w_out[NP + 5];
-          acc[1] += w_out[NP + 4] + w_out[NP + 6];
+          acc[0] += w_out[(NP + 3) * ps] + w_out[(NP + 5) * ps];
+          acc[1] += w_out[(NP + 4) * ps] + w_out[(NP + 6) * ps];
           acc[2] += Pd * sc;
           acc[3] += P * vv;
         }
       } else {
         LinCell c;
         lin_cell(AH[od], AL[od], AH[ou], AL[ou], AH[ol], AL[ol], s, g0, c);
-        float b = (sD ? pD[0] : 0.f) + (sU ? pU[1] : 0.f) + (sL ? pL[2] : 0.f);
-        float t = (sD ? pD[NP + 0] : 0.f) + (sU ? pU[NP + 1] : 0.f) + (sL ? pL[NP + 2] : 0.f);
+        float b = (sD ? pD[(0) * ps] : 0.f) + (sU ? pU[(1) * ps] : 0.f) + (sL ? pL[(2) * ps] : 0.f);
+        float t = (sD ? pD[(NP + 0) * ps] : 0.f) + (sU ? pU[(NP + 1) * ps] : 0.f) + (sL ? pL[(NP + 2) * ps] : 0.f);
         const float xs = (c.Ah - Sh) + (c.Al - Sl);
         const float e0 = ex2(fminf(xs, 0.f));
         b += e0;
@@ -409,12 +466,12 @@ __global__ void __launch_bounds__(AUX_THREADS) aux_kernel(AuxArgs a) {
         const float P = b * (c.w[0] + c.w[3]);
         const float Pd = t * (c.w[0] + c.w[3]) + b * (dw[0] + dw[3]);
         O_[(size_t)(i - 1) * ld + (j - 1)] = Pd;
-        w_out[0] = b * c.w[0]; w_out[1] = b * c.w[1]; w_out[2] = b * c.w[2];
-        w_out[NP + 0] = t * c.w[0] + b * dw[0];
-        w_out[NP + 1] = t * c.w[1] + b * dw[1];
-        w_out[NP + 2] = t * c.w[2] + b * dw[2];
+        w_out[(0) * ps] = b * c.w[0]; w_out[(1) * ps] = b * c.w[1]; w_out[(2) * ps] = b * c.w[2];
+        w_out[(NP + 0) * ps] = t * c.w[0] + b * dw[0];
+        w_out[(NP + 1) * ps] = t * c.w[1] + b * dw[1];
+        w_out[(NP + 2) * ps] = t * c.w[2] + b * dw[2];
         if (MODE == AUX_HVP) {
-          acc[0] += w_out[NP + 1] + w_out[NP + 2];
+          acc[0] += w_out[(NP + 1) * ps] + w_out[(NP + 2) * ps];
           acc[2] += Pd * sc;
           acc[3] += P * vv;
         }

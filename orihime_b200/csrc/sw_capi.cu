@@ -276,6 +276,10 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
 
 // ---- second-order ops (sw_aux.cu) ----
 
+// Largest dynamic shared-memory ring of the second-order kernel (the per-CTA
+// limit, 227 KB, less its static reduction scratch).
+constexpr size_t kAuxRingMax = 227 * 1024 - 1024;
+
 template <int NS>
 size_t aux_tab_floats(long long L1m, long long L2m) {
   return (size_t)3 * NS * swb::aux_cells((int)L1m, (int)L2m);
@@ -315,7 +319,27 @@ int launch_aux(const float* scores, const float* v, const int* lengths, int B, i
   char* w = static_cast<char*>(ws);
   a.tab = reinterpret_cast<float*>(w);
   a.roll = reinterpret_cast<float*>(w + align_up(sizeof(float) * (size_t)B * a.tab_pair));
-  swb::aux_kernel<NS, MODE><<<B, swb::AUX_THREADS, 0, st>>>(a);
+  // shared-memory rings when the longest diagonal fits
+  const size_t ring = sizeof(float) * 3 * swb::aux_ring_fields<NS>() * (size_t)(std::min(L1m, L2m) + 1);
+  if (ring <= kAuxRingMax) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWB_ERR_CUDA;
+    {
+      std::lock_guard<std::mutex> lk(g_mu);
+      static bool ready[64][2][4];
+      bool& r = ready[dev][NS == 3][MODE];
+      if (!r) {
+        if (cudaFuncSetAttribute(swb::aux_kernel<NS, MODE, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAuxRingMax) !=
+            cudaSuccess)
+          return SWB_ERR_CUDA;
+        r = true;
+      }
+    }
+    swb::aux_kernel<NS, MODE, true><<<B, swb::AUX_THREADS, ring, st>>>(a);
+  } else {
+    swb::aux_kernel<NS, MODE, false><<<B, swb::AUX_THREADS, 0, st>>>(a);
+  }
   return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
 }
 
