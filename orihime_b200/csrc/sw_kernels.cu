@@ -67,6 +67,36 @@ struct KSum {
   }
 };
 
+#ifndef SWB_POLL_SLEEP
+#define SWB_POLL_SLEEP 128
+#endif
+// Bounded wait until none of v[0..N) is the sentinel, v[f] read from
+// base[f * stride].  Every round re-reads all missing fields together, so their
+// load latencies overlap.  On timeout it records the error and substitutes
+// fb[f] for the fields still missing.
+template <int N>
+__device__ __noinline__ void poll_fields(float (&v)[N], const float* base, size_t stride,
+                                         uint64_t deadline, unsigned* status,
+                                         const float (&fb)[N]) {
+  while (true) {
+    bool miss = false;
+#pragma unroll
+    for (int f = 0; f < N; ++f)
+      if (is_sentinel(v[f])) v[f] = ld_poll(base + f * stride);
+#pragma unroll
+    for (int f = 0; f < N; ++f) miss |= is_sentinel(v[f]);
+    if (!miss) return;
+    if (gtimer() > deadline) {
+      atomicOr(status, ERR_WAIT_TIMEOUT);
+#pragma unroll
+      for (int f = 0; f < N; ++f)
+        if (is_sentinel(v[f])) v[f] = fb[f];
+      return;
+    }
+    __nanosleep(SWB_POLL_SLEEP);
+  }
+}
+
 // Bounded wait until *p is not the sentinel.  On timeout records the error and
 // returns `fallback`.
 __device__ __noinline__ float poll_value(const float* p, float v, uint64_t deadline,
@@ -517,11 +547,10 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
 #pragma unroll
           for (int f = 0; f < NE; ++f) ev[f] = (f < NS) ? v : 0.f;
         } else if (miss) {
+          float fb[NE];
 #pragma unroll
-          for (int f = 0; f < NE; ++f)
-            if (is_sentinel(ev[f]))
-              ev[f] = poll_value(ein + f * Lm + (i - 1), ld_poll(ein + f * Lm + (i - 1)), deadline,
-                                 a.status, f < NS ? NEG : 0.f);
+          for (int f = 0; f < NE; ++f) fb[f] = f < NS ? NEG : 0.f;
+          poll_fields<NE>(ev, ein + (i - 1), Lm, deadline, a.status, fb);
         }
       }
       if (lane == 0) {
