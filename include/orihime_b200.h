@@ -135,8 +135,9 @@ int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, in
  * its pitch padding is written as 0.
  *
  * swb_ragged_plan runs on the host: it validates the packing, orders the
- * pairs longest first (most cells first) for the persistent task queue and
- * places every band's workspace slice.  Call it once with plan = NULL to get
+ * pairs by critical path (L1 + 31 x bands wavefront steps, then cells) for
+ * the persistent task queue and places every band's workspace slice.  Call
+ * it once with plan = NULL to get
  * *plan_bytes (and *workspace_bytes), then with a buffer of that size; copy
  * the plan bytes to the device unchanged and pass both copies to the launch.
  * family: 3 = affine, 1 = linear; cols_per_lane: 2 or 4 (0 = default).

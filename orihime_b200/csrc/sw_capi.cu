@@ -28,6 +28,7 @@ namespace {
 using swb::Args;
 
 constexpr int kDefaultR = 4;          // columns per lane unless the caller picks another
+constexpr int kChainLag = 31;         // wavefront steps band b+1 trails band b
 constexpr int kWarpsFwd = 4;          // forward CTA: 4 independent warps
 constexpr int kWarpsBwd = 1;          // adjoint CTA: 1 warp (shared memory bound)
 constexpr size_t kAlign = 256;
@@ -472,10 +473,20 @@ int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const lon
   } else if (plan_capacity < need) {
     return SWB_ERR_ARG;
   }
-  // longest-processing-time order: most cells first, ties by index
+  // longest-chain-first order.  A band task lasts L1 + 31 wavefront steps
+  // whatever its width, and band b+1 of a pair trails band b by about 31
+  // steps, so a pair's critical path is L1 + 31 * nb steps: queue pairs by
+  // that (then by cells, then by index), their bands in order.
   std::vector<int> order(B);
   for (int b = 0; b < B; ++b) order[b] = b;
+  auto chain = [&](int b) {
+    const long long L1 = lengths[2 * b], L2 = lengths[2 * b + 1];
+    if (L1 <= 0 || L2 <= 0) return 0LL;
+    return L1 + (long long)kChainLag * ((L2 + 32 * R - 1) / (32 * R));
+  };
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const long long cx = chain(x), cy = chain(y);
+    if (cx != cy) return cx > cy;
     return (long long)lengths[2 * x] * lengths[2 * x + 1] >
            (long long)lengths[2 * y] * lengths[2 * y + 1];
   });

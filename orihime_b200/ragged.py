@@ -4,7 +4,7 @@ The reference evaluates a batch of pairs of different lengths as one padded
 [B, L1max, L2max] tensor (with ``lengths`` or a mask).  This module runs the
 same DP over a *packed* batch: every pair's scores are stored at their own
 size, one persistent kernel pair (forward + checkpointed adjoint) pulls band
-tasks longest pair first, and the whole call can be captured in a CUDA graph.
+tasks longest chain first, and the whole call can be captured in a CUDA graph.
 
 Packing (``pack``): pair b is an L1_b x L2_b row-major block with row pitch
 round_up(L2_b, 4) at element offset ``offsets[b]`` (a multiple of 4) of one
@@ -82,7 +82,7 @@ class Result:
 class Plan:
     """Launch plan of one packed batch layout (reusable across calls).
 
-    Builds the host plan with the C ABI (validation, longest-pair-first task
+    Builds the host plan with the C ABI (validation, longest-chain-first task
     order, workspace placement), copies it to the device once and owns the
     workspace, so repeated calls allocate nothing and can be graph-captured.
     """

@@ -34,8 +34,11 @@ def test_pack_unpack_roundtrip():
         assert torch.equal(m, v)
 
 
-def test_plan_orders_longest_first_and_places_bands():
-    lengths = [[10, 20], [100, 300], [0, 5], [64, 129], [5, 600]]
+def test_plan_orders_longest_chain_first_and_places_bands():
+    # the queue order is the pair's critical path L1 + 31 * bands (in
+    # wavefront steps), then cells: a tall narrow pair goes before a wide
+    # short one with more cells
+    lengths = [[10, 20], [100, 300], [0, 5], [64, 129], [5, 600], [400, 30]]
     off, ln = ragged.layout(lengths)
     rc, buf = _plan(ln, off)
     assert rc == 0
@@ -44,12 +47,14 @@ def test_plan_orders_longest_first_and_places_bands():
     pairs = buf[10:10 + 8 * B].reshape(B, 8)
     tasks = buf[10 + 8 * B:].view(np.int32)[:2 * hdr[2]].reshape(-1, 2)
     cells = [a * b for a, b in lengths]
+    nb = [max(1, -(-b // 128)) for _, b in lengths]
+    chain = [(a + 31 * n) if a * b > 0 else 0 for (a, b), n in zip(lengths, nb)]
     first_of_pair = []
     for p, _ in tasks:
         if p not in first_of_pair:
             first_of_pair.append(int(p))
-    assert first_of_pair == sorted(range(B), key=lambda b: -cells[b])
-    nb = [max(1, -(-b // 128)) for _, b in lengths]
+    assert first_of_pair == sorted(range(B), key=lambda b: (-chain[b], -cells[b], b))
+    assert first_of_pair[0] == 5 and first_of_pair[1] == 1  # 400 x 30 before 100 x 300
     assert hdr[2] == sum(nb)
     for p in range(B):
         assert pairs[p, 4] == nb[p]
