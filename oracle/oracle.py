@@ -8,6 +8,8 @@ Two libraries sit behind this module, both built by ``oracle/Makefile``:
 * ``_ref/libref_swcpu.so`` -- the reference's own CPU kernels
   (``src/sw/kernels_cpu.cpp``, ``src/sw_affine/kernels_cpu.cpp``), compiled
   from their sources.  Present wherever the Makefile's ``ref`` target ran.
+* ``_ref/libref_swcuda.so`` -- the reference's own CUDA extension (target
+  ``refcuda``); ``ref_cuda_path()`` gives its path for a GPU test that loads it.
 
 Only ``tests/``, ``bench.py``'s CPU legs and ``__graft_entry__.smoke()`` may
 import this module.  The product never does.
@@ -36,10 +38,17 @@ _P = ctypes.c_void_p
 
 
 def build(ref: bool = True) -> None:
-    """Compile the oracle (and the reference CPU kernels when their sources exist)."""
+    """Compile the oracle (and the reference CPU kernels and CUDA extension
+    when their sources exist)."""
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
     if ref and os.path.isdir("/root/reference/src"):
         subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", _HERE, "refcuda"], check=True)
+
+
+def ref_cuda_path() -> Optional[str]:
+    p = os.path.join(_HERE, "_ref", "libref_swcuda.so")
+    return p if os.path.exists(p) else None
 
 
 _lib = None

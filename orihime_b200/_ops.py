@@ -415,3 +415,83 @@ IMPLS = {
 
 for _name, _fn in IMPLS.items():
     _IMPL_LIB.impl(_name, _fn, "CUDA")
+
+
+# ---------------------------------------------------------------------------
+# AutogradCUDA kernels of the forward ops
+# ---------------------------------------------------------------------------
+# The reference makes sw_forward(_t) / sw_affine_forward(_t) differentiable
+# with a C++ autograd Function registered at AutogradCUDA
+# (src/sw_affine/torch_cuda.cpp:938-946, src/sw/torch_cuda.cpp:820-830);
+# backward = value cotangent x map + HVP of the map cotangent, plus the
+# parameter gradients for the tensor-parameter (_t) variants.  An AutogradCUDA
+# kernel runs before the CUDA kernel, so these registrations are what make
+# the B200 kernels the ones that run when the reference extension is loaded
+# too.  Forward redispatches below autograd to the CUDA kernels above.
+
+def _below(op, *args):
+    with torch._C._AutoDispatchBelowAutograd():
+        return op(*args)
+
+
+def _pgrad(g, like):
+    return g.reshape(like.shape).to(dtype=like.dtype) if like.requires_grad else None
+
+
+class _ForwardFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, fam, tensor_params, scores, lengths, *params):
+        name = ("sw_affine_forward" if fam == "sw_affine" else "sw_forward") + ("_t" if tensor_params else "")
+        v, m = _below(getattr(torch.ops.orihime, name), scores, *params, lengths)
+        ctx.fam, ctx.tensor_params, ctx.lengths = fam, tensor_params, lengths
+        ctx.vals = tuple(_scalar_param(p, "param") if tensor_params else float(p) for p in params)
+        ctx.params = params
+        ctx.save_for_backward(scores, m)
+        return v, m
+
+    @staticmethod
+    def backward(ctx, gv, gm):
+        scores, m = ctx.saved_tensors
+        fam, vals, ln = ctx.fam, ctx.vals, ctx.lengths
+        ops = torch.ops.orihime
+        gs = torch.zeros_like(scores) if ctx.needs_input_grad[2] else None
+        pg = [None] * len(ctx.params)
+        want_p = ctx.tensor_params and any(ctx.needs_input_grad[4:])
+        if gv is not None:
+            if gs is not None:
+                gs = gs + gv.view(-1, 1, 1) * m
+            if want_p:
+                grads = _below(ops.sw_affine_value_grad_params if fam == "sw_affine"
+                               else ops.sw_value_grad_params, scores, *vals, ln)
+                pg = [(gv * g).sum() for g in grads]
+        if gm is not None:
+            gmc = gm.contiguous()
+            if want_p:
+                mb = _below(ops.sw_affine_marginals_backward if fam == "sw_affine"
+                            else ops.sw_marginals_backward, scores, gmc, *vals, ln)
+                if gs is not None:
+                    gs = gs + mb[0]
+                pg = [mb[1 + k].reshape(()) if pg[k] is None else pg[k] + mb[1 + k].reshape(())
+                      for k in range(len(pg))]
+            elif gs is not None:
+                gs = gs + _below(ops.sw_affine_marginals_hvp if fam == "sw_affine"
+                                 else ops.sw_marginals_hvp, scores, gmc, *vals, ln)
+        out = [None, None, gs, None]
+        for k, p in enumerate(ctx.params):
+            out.append(_pgrad(pg[k], p) if (ctx.tensor_params and pg[k] is not None
+                                             and ctx.needs_input_grad[4 + k]) else None)
+        return tuple(out)
+
+
+def _autograd_forward(fam, tensor_params):
+    def kernel(scores, *rest):
+        *params, lengths = rest
+        v, m = _ForwardFn.apply(fam, tensor_params, scores, lengths, *params)
+        return [v, m]
+    return kernel
+
+
+for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True),
+                        ("sw_affine_forward", "sw_affine", False),
+                        ("sw_affine_forward_t", "sw_affine", True)):
+    _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")

@@ -1,0 +1,109 @@
+"""Our CUDA path against the reference's own CUDA path on the same GPU.
+
+The reference CUDA extension is built by ``make -C oracle refcuda`` from
+``src/sw*/kernels_gpu.cu`` and the op bodies beside them.  It has to be loaded
+before orihime_b200, which then takes over the namespaced ``sw*`` ops; the
+reference's legacy ``soft_sw*`` ops stay the reference's CUDA path.  That
+order is fixed per process, so the comparison runs in a child process.
+
+Bar: values within rel 1e-5 of the reference CUDA path.  Maps and
+second-order outputs must be at least as close to the fp64 oracle as the
+reference CUDA path's own results (or within the 1e-5 / 1e-4 floors).  Our
+distance to the reference CUDA path is printed with each case.
+"""
+
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+pytestmark = pytest.mark.gpu
+
+
+def _worker():
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+
+    torch.ops.load_library(O.ref_cuda_path())
+    import orihime_b200  # noqa: F401  (takes over the namespaced ops)
+    ops = torch.ops.orihime
+    out = []
+
+    def emb(B, N, M, seed, d=64):
+        g = torch.Generator().manual_seed(seed)
+        e, f = torch.randn(B, N, d, generator=g), torch.randn(B, M, d, generator=g)
+        return (3 * torch.bmm(e, f.transpose(1, 2)) / d ** 0.5).float()
+
+    def dist(a, b):
+        return float(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64)).max())
+
+    for (B, N, M, T, seed) in [(3, 64, 80, 0.5, 1), (2, 200, 150, 0.7, 2), (2, 256, 256, 0.5, 3)]:
+        s = emb(B, N, M, seed)
+        sd = s.cuda()
+        ln = torch.tensor([[N, M]] + [[N - 7, M - 13]] * (B - 1), dtype=torch.int32)
+        rv, rm = ops.soft_sw_affine_float(sd, -2.0, -0.5, T, ln.cuda())[:2]
+        ov, om = ops.sw_affine_forward(sd, -2.0, -0.5, T, ln.cuda())
+        t64 = O.affine(s.numpy(), ln.numpy(), -2.0, -0.5, T, dtype=np.float64)
+        rel = float(((ov - rv).abs() / rv.abs()).max())
+        v = torch.randn(B, N, M, generator=torch.Generator().manual_seed(seed + 9))
+        rh = ops.soft_sw_affine_hvp(sd, v.cuda(), -2.0, -0.5, T, ln.cuda())
+        oh = ops.sw_affine_marginals_hvp(sd, v.cuda(), -2.0, -0.5, T, ln.cuda())
+        h64 = O.affine_hvp(s.numpy(), v.numpy(), ln.numpy(), -2.0, -0.5, T, dtype=np.float64)
+        rp = ops.soft_sw_affine_param_jacobian(sd, 2, -2.0, -0.5, T, ln.cuda())
+        op_ = ops.sw_affine_marginals_grad_temp(sd, -2.0, -0.5, T, ln.cuda())
+        p64 = O.affine_param_grad(s.numpy(), ln.numpy(), -2.0, -0.5, T, 2, dtype=np.float64)
+        out.append(dict(case=[B, N, M, T], value_rel=rel,
+                        map_ours_ref=dist(om.cpu(), rm.cpu()), map_ours_64=dist(om.cpu(), t64["map"]),
+                        map_ref_64=dist(rm.cpu(), t64["map"]),
+                        hvp_ours_ref=dist(oh.cpu(), rh.cpu()), hvp_ours_64=dist(oh.cpu(), h64),
+                        hvp_ref_64=dist(rh.cpu(), h64), hvp_scale=float(np.abs(h64).max()),
+                        dpdt_ours_ref=dist(op_.cpu(), rp.cpu()), dpdt_ours_64=dist(op_.cpu(), p64),
+                        dpdt_ref_64=dist(rp.cpu(), p64), dpdt_scale=float(np.abs(p64).max())))
+    # timing: C2 (64 x 1024^2) on both CUDA paths
+    s = emb(64, 1024, 1024, 1).cuda()
+
+    def t(fn, n=3):
+        fn(); torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record(); torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+    cells = 64 * 1024 * 1024
+    tr = t(lambda: ops.soft_sw_affine_float(s, -2.0, -0.5, 0.5, None), 2)
+    to = t(lambda: ops.sw_affine_forward(s, -2.0, -0.5, 0.5, None), 5)
+    out.append(dict(timing="C2 64x1024^2 value+map", ref_ms=tr, ours_ms=to,
+                    ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
+    print("RESULT " + json.dumps(out))
+
+
+def test_against_reference_cuda_path():
+    import torch
+    from oracle import oracle as O
+
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA not available")
+    if O.ref_cuda_path() is None:
+        pytest.skip("reference CUDA extension not built (make -C oracle refcuda)")
+    r = subprocess.run([sys.executable, __file__, "worker"], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-3000:]
+    res = json.loads(r.stdout.split("RESULT ", 1)[1])
+    for c in res:
+        print(" ", c)
+        if "timing" in c:
+            continue
+        assert c["value_rel"] <= 1e-5
+        assert c["map_ours_64"] <= max(1e-5, c["map_ref_64"])
+        assert c["hvp_ours_64"] <= max(1e-4 * c["hvp_scale"], c["hvp_ref_64"])
+        assert c["dpdt_ours_64"] <= max(1e-4 * c["dpdt_scale"], c["dpdt_ref_64"])
+
+
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "worker":
+    _worker()

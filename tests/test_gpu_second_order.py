@@ -164,3 +164,40 @@ def test_hvp_symmetry_and_linearity():
     assert abs(a - b) <= 1e-4 * max(1.0, abs(a)), (a, b)
     lin = H(2.0 * u - 0.5 * v)
     assert torch.allclose(lin, 2.0 * Hu - 0.5 * Hv, rtol=0, atol=2e-5 * float(Hu.abs().max()))
+
+
+@pytest.mark.parametrize("fam", ["affine", "linear"])
+def test_forward_ops_are_differentiable(fam):
+    """The namespaced forward ops carry their own autograd (as the reference's
+    AutogradCUDA registration does): value cotangent x map + HVP of the map
+    cotangent, plus parameter gradients for the tensor-parameter variant."""
+    ops = torch.ops.orihime
+    B, L1, L2, T = 2, 33, 27, 0.6
+    s = _scores(B, L1, L2, 41).cuda().requires_grad_(True)
+    a = torch.randn(B, device="cuda")
+    g = _scores(B, L1, L2, 42, 1.0).cuda()
+    if fam == "affine":
+        v, m = ops.sw_affine_forward(s, *AFF, T, None)
+        ((v * a).sum() + (m * g).sum()).backward()
+        want = a.view(-1, 1, 1) * m.detach() + ops.sw_affine_marginals_hvp(s.detach(), g, *AFF, T, None)
+    else:
+        v, m = ops.sw_forward(s, *LIN, T, None)
+        ((v * a).sum() + (m * g).sum()).backward()
+        want = a.view(-1, 1, 1) * m.detach() + ops.sw_marginals_hvp(s.detach(), g, *LIN, T, None)
+    assert torch.allclose(s.grad, want, rtol=1e-5, atol=1e-6)
+    # tensor-parameter variant: parameter gradients
+    s2 = s.detach().clone().requires_grad_(True)
+    vals = AFF + (T,) if fam == "affine" else LIN + (T,)
+    ps = [torch.tensor(x, device="cuda", requires_grad=True) for x in vals]
+    ln = torch.tensor([[L1, L2]] * B, dtype=torch.int32, device="cuda")
+    fwd_t = ops.sw_affine_forward_t if fam == "affine" else ops.sw_forward_t
+    v2, m2 = fwd_t(s2, *ps, ln)
+    ((v2 * a).sum() + (m2 * g).sum()).backward()
+    vg = (ops.sw_affine_value_grad_params if fam == "affine" else ops.sw_value_grad_params)(
+        s.detach(), *vals, ln)
+    mb = (ops.sw_affine_marginals_backward if fam == "affine" else ops.sw_marginals_backward)(
+        s.detach(), g, *vals, ln)
+    assert torch.allclose(s2.grad, s.grad, rtol=1e-5, atol=1e-6)
+    for k, p in enumerate(ps):
+        want_p = float((a * vg[k]).sum() + mb[1 + k].sum())
+        assert abs(float(p.grad) - want_p) <= 1e-4 * max(1.0, abs(want_p)), (k, float(p.grad), want_p)
