@@ -80,6 +80,42 @@ def _worker():
     to = t(lambda: ops.sw_affine_forward(s, -2.0, -0.5, 0.5, None), 5)
     out.append(dict(timing="C2 64x1024^2 value+map", ref_ms=tr, ours_ms=to,
                     ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
+    del s
+    # C1: linear, 8 x 128^2, N(0,1) scores, gap -1, T 1
+    s1 = torch.randn(8, 128, 128, generator=torch.Generator().manual_seed(0)).cuda()
+    tr = t(lambda: ops.soft_sw_float(s1, -1.0, 1.0, None), 5)
+    to = t(lambda: ops.sw_forward(s1, -1.0, 1.0, None), 5)
+    cells = 8 * 128 * 128
+    out.append(dict(timing="C1 linear 8x128^2 value+map", ref_ms=tr, ours_ms=to,
+                    ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
+    # C3: 4096 pairs, lengths log-uniform [32, 2048] (seed 3).  The reference
+    # runs padded chunks of 64 pairs of similar size (with lengths); ours runs
+    # the packed ragged batch in one plan.
+    from orihime_b200 import ragged
+    rng = np.random.default_rng(3)
+    ln = np.rint(np.exp(rng.uniform(np.log(32), np.log(2048), size=(4096, 2)))).astype(np.int64)
+    order = np.argsort(-(ln[:, 0] * ln[:, 1]), kind="stable")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    chunks = []
+    for c0 in range(0, 4096, 64):
+        idx = order[c0:c0 + 64]
+        L1m, L2m = int(ln[idx, 0].max()), int(ln[idx, 1].max())
+        sc = 3.0 * torch.randn(len(idx), L1m, L2m, generator=g, device="cuda")
+        chunks.append((sc, torch.tensor(ln[idx], dtype=torch.int32, device="cuda")))
+    cells = int((ln[:, 0] * ln[:, 1]).sum())
+
+    def ref_c3():
+        for sc, l in chunks:
+            ops.soft_sw_affine_float(sc, -2.0, -0.5, 0.5, l)
+    tr = t(ref_c3, 1)
+    del chunks
+    off, l32 = ragged.layout(ln)
+    flat = 3.0 * torch.randn(int(off[-1]), generator=g, device="cuda")
+    plan = ragged.Plan(l32, off, family="affine", device="cuda")
+    to = t(lambda: plan.run(flat, gap_open=-2.0, gap_ext=-0.5, temp=0.5), 5)
+    out.append(dict(timing="C3 4096 ragged pairs value+map+grads (reference: padded chunks of 64)",
+                    ref_ms=tr, ours_ms=to, ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
     print("RESULT " + json.dumps(out))
 
 
