@@ -88,6 +88,21 @@ def _worker():
     cells = 8 * 128 * 128
     out.append(dict(timing="C1 linear 8x128^2 value+map", ref_ms=tr, ours_ms=to,
                     ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
+    # second-order ops at C5 shapes (256 x 512^2)
+    s5 = torch.randn(256, 512, 512, generator=torch.Generator().manual_seed(5)).cuda()
+    v5 = torch.randn_like(s5)
+    cells = 256 * 512 * 512
+    for name, rf, of in (
+            ("C5 HVP", lambda: ops.soft_sw_affine_hvp(s5, v5, -2.0, -0.5, 0.5, None),
+             lambda: ops.sw_affine_marginals_hvp(s5, v5, -2.0, -0.5, 0.5, None)),
+            ("C5 dP/dT", lambda: ops.soft_sw_affine_param_jacobian(s5, 2, -2.0, -0.5, 0.5, None),
+             lambda: ops.sw_affine_marginals_grad_temp(s5, -2.0, -0.5, 0.5, None)),
+            ("C5 marginals_backward", lambda: ops.soft_sw_affine_backward_full(s5, v5, -2.0, -0.5, 0.5, None),
+             lambda: ops.sw_affine_marginals_backward(s5, v5, -2.0, -0.5, 0.5, None))):
+        tr, to = t(rf, 1), t(of, 3)
+        out.append(dict(timing=name + " 256x512^2", ref_ms=tr, ours_ms=to,
+                        ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
+    del s5, v5
     # C3: 4096 pairs, lengths log-uniform [32, 2048] (seed 3).  The reference
     # runs padded chunks of 64 pairs of similar size (with lengths); ours runs
     # the packed ragged batch in one plan.
