@@ -388,9 +388,10 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
     if constexpr (NS == 3) {
       const float uMh = ph[0][c], uMl = pl[0][c], uIh = ph[1][c], uIl = pl[1][c];
       const float uDh = ph[2][c], uDl = pl[2][c];
-      // M = s + LSE(M, I, D at diag, 0)
-      const float r = fmaxf(fmaxf(dgh[0] + dgl[0], dgh[1] + dgl[1]),
-                            fmaxf(dgh[2] + dgl[2], 0.f));
+      // M = s + LSE(M, I, D at diag, 0).  The reference point of each LSE
+      // comes from the hi parts only: any r close to the maximum keeps every
+      // term <= ~1, and the lo parts enter the exponents exactly.
+      const float r = fmaxf(fmaxf(dgh[0], dgh[1]), fmaxf(dgh[2], 0.f));
       const float tM = ex2((dgh[0] - r) + dgl[0]), tI = ex2((dgh[1] - r) + dgl[1]);
       const float tD = ex2((dgh[2] - r) + dgl[2]);
       const float sm = (tM + tI) + (tD + ex2(-r));
@@ -398,39 +399,33 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       two_sum(r, s[c], Mh, Ml);
       Ml += lg2(sm);
       // I = LSE(M up + go, I up + ge)
-      const float ru = fmaxf((uMh + uMl) + g0, (uIh + uIl) + g1);
-      const float ia = ((uMh - ru) + g0) + uMl, ib = ((uIh - ru) + g1) + uIl;
-      const float im = fmaxf(ia, ib);
-      const float ti = ex2(fminf(ia, ib) - im), si = 1.f + ti;
+      const float ru = fmaxf(uMh + g0, uIh + g1);
+      const float ta = ex2(((uMh - ru) + g0) + uMl), tb = ex2(((uIh - ru) + g1) + uIl);
+      const float si = ta + tb;
       float Ih, Il;
-      fast2(ru, im + lg2(si), Ih, Il);
+      fast2(ru, lg2(si), Ih, Il);
       // D = LSE(M left + go, D left + ge)
-      const float rl = fmaxf((lh[0] + ll[0]) + g0, (lh[2] + ll[2]) + g1);
-      const float da = ((lh[0] - rl) + g0) + ll[0], db = ((lh[2] - rl) + g1) + ll[2];
-      const float dm = fmaxf(da, db);
-      const float td = ex2(fminf(da, db) - dm), sd = 1.f + td;
+      const float rl = fmaxf(lh[0] + g0, lh[2] + g1);
+      const float tc = ex2(((lh[0] - rl) + g0) + ll[0]), td = ex2(((lh[2] - rl) + g1) + ll[2]);
+      const float sd = tc + td;
       float Dh, Dl;
-      fast2(rl, dm + lg2(sd), Dh, Dl);
+      fast2(rl, lg2(sd), Dh, Dl);
       if constexpr (WT) {
-        const float vm = recip(sm);
-        const float vi = recip(si), wi = ti * vi;   // larger term: 1/si, smaller: ti/si
-        const float vd = recip(sd), wd = td * vd;
+        const float vm = recip(sm), vi = recip(si), vd = recip(sd);
         const bool lv = c < nlive;
         const float bM = lv ? ex2(fminf((Mh - Sh) + (Ml - Sl), 0.f)) : 0.f;
         const float bI = lv ? ex2(fminf((Ih - Sh) + (Il - Sl), 0.f)) : 0.f;
         const float bD = lv ? ex2(fminf((Dh - Sh) + (Dl - Sl), 0.f)) : 0.f;
-        put_fields<NS, R>(went, lane, c, make_float4(tM * vm, tI * vm, tD * vm, ia >= ib ? vi : wi),
-                          make_float4(ia >= ib ? wi : vi, da >= db ? vd : wd, da >= db ? wd : vd, bM),
-                          make_float2(bI, bD), s[c]);
+        put_fields<NS, R>(went, lane, c, make_float4(tM * vm, tI * vm, tD * vm, ta * vi),
+                          make_float4(tb * vi, tc * vd, td * vd, bM), make_float2(bI, bD), s[c]);
       }
       dgh[0] = uMh; dgl[0] = uMl; dgh[1] = uIh; dgl[1] = uIl; dgh[2] = uDh; dgl[2] = uDl;
       lh[0] = Mh; ll[0] = Ml; lh[1] = Ih; ll[1] = Il; lh[2] = Dh; ll[2] = Dl;
       ph[0][c] = Mh; pl[0][c] = Ml; ph[1][c] = Ih; pl[1][c] = Il; ph[2][c] = Dh; pl[2][c] = Dl;
     } else {
       const float uh = ph[0][c], ul = pl[0][c];
-      // A = LSE(diag + s, up + g, left + g, s)
-      const float r = fmaxf(fmaxf((dgh[0] + dgl[0]) + s[c], (uh + ul) + g0),
-                            fmaxf((lh[0] + ll[0]) + g0, s[c]));
+      // A = LSE(diag + s, up + g, left + g, s), reference point from hi parts
+      const float r = fmaxf(fmaxf(dgh[0] + s[c], uh + g0), fmaxf(lh[0] + g0, s[c]));
       const float va = ((dgh[0] - r) + s[c]) + dgl[0];
       const float vu = ((uh - r) + g0) + ul;
       const float vl = ((lh[0] - r) + g0) + ll[0];
