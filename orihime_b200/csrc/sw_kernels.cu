@@ -903,16 +903,18 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
       float pm[R];
 #pragma unroll
       for (int c = R - 1; c >= 0; --c) {
-        const bool live = act && c < ncols;
+        // cells outside the pair carry beta-init 0 and receive only zero
+        // pushes (their successors are outside too, or their weight toward
+        // a NEG predecessor is 0), so beta needs no mask
         if constexpr (NS == 3) {
           float4 f0, f1;
           float2 f2;
           float sc;
           get_fields<NS, R>(E, lane, c, f0, f1, f2, sc);
           // f0 = (wMM, wMI, wMD, wIM), f1 = (wII, wDM, wDD, bM0), f2 = (bI0, bD0)
-          const float bM = live ? f1.w + ac[0][c] : 0.f;
-          const float bI = live ? f2.x + ac[1][c] : 0.f;
-          const float bD = live ? f2.y + ac[2][c] : 0.f;
+          const float bM = f1.w + ac[0][c];
+          const float bI = f2.x + ac[1][c];
+          const float bD = f2.y + ac[2][c];
           pm[c] = bM;
           const float pIM = bI * f0.w, pII = bI * f1.x;
           const float pDM = bD * f1.y, pDD = bD * f1.z;
@@ -934,7 +936,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
           float sc;
           get_fields<NS, R>(E, lane, c, f0, f1, f2, sc);
           // f0 = (map factor, wA, wU, wL), f2.x = b0
-          const float b = live ? f2.x + ac[0][c] : 0.f;
+          const float b = f2.x + ac[0][c];
           const float pv_ = b * f0.x;
           pm[c] = pv_;
           const float pU = b * f0.z, pL = b * f0.w, pD = b * f0.y;
