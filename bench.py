@@ -63,16 +63,50 @@ def make_scores(torch, lengths, offsets, seed, device):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clock, power and clock-event reasons sampled during the timed region
+    (read only; no setting is changed).  NVML is polled every 10 ms on the
+    device matched by PCI bus id; without NVML, nvidia-smi is polled (about
+    one sample per 0.2 s)."""
+
+    _BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+             ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
     def __init__(self, index: int):
         self.index = index
         self.samples = []
+        self.source = None
         self._stop = threading.Event()
         self._th = None
 
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.index)
+        bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
     def __enter__(self):
-        def run():
+        try:
+            nv, h = self._nvml_handle()
+        except Exception:
+            nv = h = None
+
+        def run_nvml():
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append([str(sm), str(mx), f"{pw:.1f}"]
+                                        + ["Active" if bits & b else "Not Active" for _, b in self._BITS])
+                except Exception:
+                    pass
+                self._stop.wait(0.01)
+
+        def run_smi():
             q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
                  "clocks_event_reasons.sw_power_cap")
@@ -87,7 +121,8 @@ class ClockSampler:
                     pass
                 self._stop.wait(0.2)
 
-        self._th = threading.Thread(target=run, daemon=True)
+        self.source = "nvml" if h is not None else "nvidia-smi"
+        self._th = threading.Thread(target=run_nvml if h is not None else run_smi, daemon=True)
         self._th.start()
         return self
 
@@ -100,12 +135,12 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
         mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _ in self._BITS]
         reasons = sorted({names[k] for s in self.samples for k in range(4)
                           if len(s) > 3 + k and "Active" in s[3 + k] and "Not" not in s[3 + k]})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(self.samples), "source": self.source}
 
 
 def dist_init(torch, backend: str = "nccl"):
@@ -276,7 +311,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
