@@ -164,9 +164,13 @@ int swb_sw_ragged(const float* scores, const void* host_plan, const void* dev_pl
                   const swb_options* opt);
 
 /*
- * Second-order ops (one CTA per pair sweeping anti-diagonals; the workspace
- * holds alpha and its tangent for every cell, 9 floats per cell affine,
- * 3 linear, plus small per-pair push buffers).
+ * Second-order ops (band wavefronts: a forward kernel carrying alpha and its
+ * tangent, then a backward kernel carrying beta and its tangent).  The
+ * workspace holds, for every cell the wavefront visits, the fields the
+ * backward reads: 24 floats affine (weights, weight tangents, alpha hi/lo,
+ * tangents), 12 linear, plus per-band edge, push and partial buffers; about
+ * 100 (affine) or 50 (linear) bytes per cell of the padded batch.  Callers
+ * that bound memory split the batch into pair groups.
  */
 size_t swb_sw_affine_aux_workspace_bytes(int B, int L1max, int L2max);
 

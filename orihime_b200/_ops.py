@@ -274,8 +274,32 @@ def _check_like(scores, other, name, msg_shape):
         raise RuntimeError(f"{name} must be on same device as scores, got {other.device} vs {scores.device}")
 
 
-def _aux_ws(nbytes, dev):
-    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=dev)
+# Largest workspace one second-order call takes at once; a batch needing more
+# is processed in pair groups (results identical: pairs are independent).
+AUX_BUDGET_MAX = 16 << 30
+
+
+def _aux_plan(aff, B, L1, L2, dev):
+    """(pairs per group, workspace bytes) for a second-order call: the field
+    table of the band wavefront is about 100 (affine) / 50 (linear) bytes per
+    cell, so large batches are split to stay within min(AUX_BUDGET_MAX,
+    max(2 GiB, half the free device memory))."""
+    fn = _LIB.swb_sw_affine_aux_workspace_bytes if aff else _LIB.swb_sw_aux_workspace_bytes
+    nbytes = int(fn(B, L1, L2))
+    free = torch.cuda.mem_get_info(dev)[0]
+    budget = min(AUX_BUDGET_MAX, max(2 << 30, free // 2))
+    g = B
+    if nbytes > budget:
+        g = max(1, min(B, B * budget // nbytes))
+        while g > 1 and int(fn(g, L1, L2)) > budget:
+            g = max(1, g // 2)
+    last = B - (B - 1) // g * g
+    return g, max(int(fn(g, L1, L2)), int(fn(last, L1, L2)))
+
+
+def _groups(B, g):
+    for b0 in range(0, B, g):
+        yield b0, min(B, b0 + g)
 
 
 def run_hvp(fam, scores, v, lengths, params, want_grads=False):
@@ -287,17 +311,16 @@ def run_hvp(fam, scores, v, lengths, params, want_grads=False):
     if B == 0:
         return out, gt
     aff = fam == "sw_affine"
-    nbytes = (_LIB.swb_sw_affine_aux_workspace_bytes if aff else _LIB.swb_sw_aux_workspace_bytes)(B, L1, L2)
-    ws = _aux_ws(nbytes, dev)
+    g, nbytes = _aux_plan(aff, B, L1, L2, dev)
+    ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    fn = _LIB.swb_sw_affine_hvp if aff else _LIB.swb_sw_hvp
     with torch.cuda.device(dev):
-        if aff:
-            rc = _LIB.swb_sw_affine_hvp(_ptr(scores), _ptr(v), _ptr(lengths), B, L1, L2,
-                                        *map(float, params), _ptr(out), _ptr(gt), _ptr(ws), nbytes,
-                                        _stream(dev))
-        else:
-            rc = _LIB.swb_sw_hvp(_ptr(scores), _ptr(v), _ptr(lengths), B, L1, L2, *map(float, params),
-                                 _ptr(out), _ptr(gt), _ptr(ws), nbytes, _stream(dev))
-    _lib.check(rc, "soft Smith-Waterman HVP")
+        for b0, b1 in _groups(B, g):
+            ln = None if lengths is None else lengths[b0:b1]
+            rc = fn(_ptr(scores[b0:b1]), _ptr(v[b0:b1]), _ptr(ln), b1 - b0, L1, L2, *map(float, params),
+                    _ptr(out[b0:b1]), _ptr(None if gt is None else gt[b0:b1]), _ptr(ws), nbytes,
+                    _stream(dev))
+            _lib.check(rc, "soft Smith-Waterman HVP")
     return out, gt
 
 
@@ -308,13 +331,15 @@ def run_param_jacobian(fam, scores, lengths, params, which):
     if B == 0:
         return out
     aff = fam == "sw_affine"
-    nbytes = (_LIB.swb_sw_affine_aux_workspace_bytes if aff else _LIB.swb_sw_aux_workspace_bytes)(B, L1, L2)
-    ws = _aux_ws(nbytes, dev)
+    g, nbytes = _aux_plan(aff, B, L1, L2, dev)
+    ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    fn = _LIB.swb_sw_affine_param_jacobian if aff else _LIB.swb_sw_param_jacobian
     with torch.cuda.device(dev):
-        fn = _LIB.swb_sw_affine_param_jacobian if aff else _LIB.swb_sw_param_jacobian
-        rc = fn(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params), int(which), _ptr(out),
-                _ptr(ws), nbytes, _stream(dev))
-    _lib.check(rc, "soft Smith-Waterman parameter Jacobian")
+        for b0, b1 in _groups(B, g):
+            ln = None if lengths is None else lengths[b0:b1]
+            rc = fn(_ptr(scores[b0:b1]), _ptr(ln), b1 - b0, L1, L2, *map(float, params), int(which),
+                    _ptr(out[b0:b1]), _ptr(ws), nbytes, _stream(dev))
+            _lib.check(rc, "soft Smith-Waterman parameter Jacobian")
     return out
 
 

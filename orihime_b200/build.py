@@ -23,7 +23,7 @@ SOURCES = [os.path.join(PKG, "csrc", "sw_capi.cu")]
 DEPS = SOURCES + [
     os.path.join(PKG, "csrc", "sw_kernels.cu"),
     os.path.join(PKG, "csrc", "sw_kernels.cuh"),
-    os.path.join(PKG, "csrc", "sw_aux.cu"),
+    os.path.join(PKG, "csrc", "sw_xband.cu"),
     os.path.join(PKG, "csrc", "sw_probe.cuh"),
     os.path.join(ROOT, "include", "orihime_b200.h"),
 ]

@@ -14,7 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "sw_kernels.cu"
-#include "sw_aux.cu"
+#include "sw_xband.cu"
 #include "sw_probe.cuh"
 #include "../../include/orihime_b200.h"
 
@@ -275,73 +275,120 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
   return SWB_ERR_ARG;
 }
 
-// ---- second-order ops (sw_aux.cu) ----
+// ---- second-order ops as band wavefronts ----
 
-// Largest dynamic shared-memory ring of the second-order kernel (the per-CTA
-// limit, 227 KB, less its static reduction scratch).
-constexpr size_t kAuxRingMax = 227 * 1024 - 1024;
+// Columns per lane of the second-order kernels: 4 once the batch has at least
+// kXTasksR4 bands of 128 columns (enough warps to fill the GPU), else 2.
+constexpr long long kXTasksR4 = 2048;
+#ifndef SWB_XR
+#define SWB_XR 0
+#endif
+
+int xpick_r(long long B, long long L2m) {
+  if (SWB_XR == 2 || SWB_XR == 4) return SWB_XR;
+  const long long nb4 = std::max(1LL, (L2m + 127) / 128);
+  return B * nb4 >= kXTasksR4 ? 4 : 2;
+}
+
+struct XLayout {
+  int R, nb, nsteps;
+  size_t off_pair_done, off_part, off_gpart, off_sent, off_edge, off_bpush, off_fld;
+  size_t sent_bytes, total;
+};
 
 template <int NS>
-size_t aux_tab_floats(long long L1m, long long L2m) {
-  return (size_t)3 * NS * swb::aux_cells((int)L1m, (int)L2m);
+XLayout xlayout(long long B, long long L1m, long long L2m) {
+  XLayout l{};
+  l.R = xpick_r(B, L2m);
+  l.nb = (int)std::max(1LL, (L2m + 32 * l.R - 1) / (32 * l.R));
+  l.nsteps = (int)((L1m + 31 + swb::XC - 1) / swb::XC * swb::XC);
+  const size_t slots = (size_t)B * l.nb;
+  const size_t step = (size_t)l.R * swb::XShape<NS>::G * 128;
+  size_t o = align_up(64);   // counters [0, 1], status [4]
+  l.off_pair_done = o; o = align_up(o + sizeof(unsigned) * (size_t)B);
+  l.off_part = o;      o = align_up(o + sizeof(float) * 4 * slots);
+  l.off_gpart = o;     o = align_up(o + sizeof(float) * 4 * slots);
+  l.off_sent = o;
+  l.off_edge = o;      o = align_up(o + sizeof(float) * slots * swb::XShape<NS>::NE * (size_t)L1m);
+  l.off_bpush = o;
+  o = align_up(o + sizeof(float) * slots * 2 * swb::XShape<NS>::NP * (size_t)(L1m + 1));
+  l.sent_bytes = o - l.off_sent;
+  l.off_fld = o;       o = align_up(o + sizeof(float) * slots * (size_t)l.nsteps * step);
+  l.total = o;
+  return l;
 }
-template <int NS>
-size_t aux_roll_floats(long long L1m) {
-  return (size_t)3 * (size_t)(L1m + 1) * 2 * swb::AuxShape<NS>::NPUSH;
-}
-template <int NS>
-size_t aux_ws_bytes(long long B, long long L1m, long long L2m) {
-  if (B <= 0) return 0;
-  return align_up(sizeof(float) * (size_t)B * aux_tab_floats<NS>(L1m, L2m)) +
-         align_up(sizeof(float) * (size_t)B * aux_roll_floats<NS>(L1m));
+
+// Occupancy of each second-order instantiation on one device, computed once.
+struct XOcc {
+  int f = 0, b = 0;
+  bool ready = false;
+};
+XOcc g_xocc[64][2][2][4];   // [device][affine?][R == 4?][mode]
+
+template <int NS, int R, int MODE>
+int launch_xband_r(swb::XArgs a, cudaStream_t st) {
+  DevInfo* d = nullptr;
+  int rc = dev_info(&d);
+  if (rc != SWB_OK) return rc;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWB_ERR_CUDA;
+  const size_t smem = sizeof(float) * swb::XSTAGES * swb::xstep_floats<NS, R>();
+  XOcc& o = g_xocc[dev][NS == 3][R == 4][MODE];
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!o.ready) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.f, swb::xfwd_kernel<NS, R, MODE>, 128, 0) !=
+              cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.b, swb::xbwd_kernel<NS, R, MODE>, 32, smem) !=
+              cudaSuccess)
+        return SWB_ERR_CUDA;
+      o.ready = true;
+    }
+  }
+  const long long ntasks = (long long)a.B * a.nb;
+  const long long cap_f = (long long)d->sms * (o.f > 0 ? o.f : 1);
+  const long long cap_b = (long long)d->sms * (o.b > 0 ? o.b : 1);
+  const int grid_f = (int)std::min((ntasks + 3) / 4, cap_f);
+  const int grid_b = (int)std::min(ntasks, cap_b);
+  swb::xfwd_kernel<NS, R, MODE><<<grid_f, 128, 0, st>>>(a);
+  swb::xbwd_kernel<NS, R, MODE><<<grid_b, 32, smem, st>>>(a);
+  return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
 }
 
 template <int NS, int MODE>
-int launch_aux(const float* scores, const float* v, const int* lengths, int B, int L1m, int L2m,
-               float go, float ge, float T, float* out, float* gt, void* ws, size_t ws_bytes,
-               void* stream_v) {
+int launch_xband(const float* scores, const float* v, const int* lengths, int B, int L1m, int L2m,
+                 float go, float ge, float T, float* out, float* gt, void* ws, size_t ws_bytes,
+                 void* stream_v) {
   if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   if (B == 0) return SWB_OK;
   const size_t map_elems = (size_t)B * L1m * L2m;
   if (map_elems > 0 && (!scores || !out || (MODE == swb::AUX_HVP && !v))) return SWB_ERR_ARG;
-  const size_t need = aux_ws_bytes<NS>(B, L1m, L2m);
-  if (!ws || ws_bytes < need) return SWB_ERR_WORKSPACE;
+  const XLayout l = xlayout<NS>(B, L1m, L2m);
+  if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream_v);
+  char* w = static_cast<char*>(ws);
+  // per-call resets: counters, status, completion counts to 0; cross-band
+  // buffers to the NaN sentinel; the output to 0 (cells outside lengths stay 0)
+  if (cudaMemsetAsync(w, 0, l.off_part, st) != cudaSuccess) return SWB_ERR_CUDA;
+  if (cudaMemsetAsync(w + l.off_sent, 0xff, l.sent_bytes, st) != cudaSuccess) return SWB_ERR_CUDA;
   if (map_elems > 0 && cudaMemsetAsync(out, 0, map_elems * sizeof(float), st) != cudaSuccess)
     return SWB_ERR_CUDA;
-  swb::AuxArgs a{};
+  swb::XArgs a{};
   a.scores = scores; a.v = v; a.lengths = lengths;
-  a.B = B; a.L1m = L1m; a.L2m = L2m;
+  a.B = B; a.L1m = L1m; a.L2m = L2m; a.nb = l.nb; a.nsteps = l.nsteps;
   a.go = go; a.ge = ge; a.T = T; a.k = 1.4426950408889634f / T;
   a.out = out; a.gt = gt;
-  a.tab_pair = aux_tab_floats<NS>(L1m, L2m);
-  a.roll_pair = aux_roll_floats<NS>(L1m);
-  char* w = static_cast<char*>(ws);
-  a.tab = reinterpret_cast<float*>(w);
-  a.roll = reinterpret_cast<float*>(w + align_up(sizeof(float) * (size_t)B * a.tab_pair));
-  // shared-memory rings when the longest diagonal fits
-  const size_t ring = sizeof(float) * 3 * swb::aux_ring_fields<NS>() * (size_t)(std::min(L1m, L2m) + 1);
-  if (ring <= kAuxRingMax) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWB_ERR_CUDA;
-    {
-      std::lock_guard<std::mutex> lk(g_mu);
-      static bool ready[64][2][4];
-      bool& r = ready[dev][NS == 3][MODE];
-      if (!r) {
-        if (cudaFuncSetAttribute(swb::aux_kernel<NS, MODE, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAuxRingMax) !=
-            cudaSuccess)
-          return SWB_ERR_CUDA;
-        r = true;
-      }
-    }
-    swb::aux_kernel<NS, MODE, true><<<B, swb::AUX_THREADS, ring, st>>>(a);
-  } else {
-    swb::aux_kernel<NS, MODE, false><<<B, swb::AUX_THREADS, 0, st>>>(a);
-  }
-  return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+  a.counters = reinterpret_cast<unsigned*>(w);
+  a.status = a.counters + 4;
+  a.pair_done = reinterpret_cast<unsigned*>(w + l.off_pair_done);
+  a.part = reinterpret_cast<float*>(w + l.off_part);
+  a.gpart = reinterpret_cast<float*>(w + l.off_gpart);
+  a.edge = reinterpret_cast<float*>(w + l.off_edge);
+  a.bpush = reinterpret_cast<float*>(w + l.off_bpush);
+  a.fld = reinterpret_cast<float*>(w + l.off_fld);
+  a.spin_limit_ns = 20ull * 1000000000ull;
+  return l.R == 4 ? launch_xband_r<NS, 4, MODE>(a, st) : launch_xband_r<NS, 2, MODE>(a, st);
 }
 
 }  // namespace
@@ -349,17 +396,17 @@ int launch_aux(const float* scores, const float* v, const int* lengths, int B, i
 extern "C" {
 
 size_t swb_sw_affine_aux_workspace_bytes(int B, int L1max, int L2max) {
-  return aux_ws_bytes<3>(B, L1max, L2max);
+  return B > 0 ? xlayout<3>(B, L1max, L2max).total : 0;
 }
 
 size_t swb_sw_aux_workspace_bytes(int B, int L1max, int L2max) {
-  return aux_ws_bytes<1>(B, L1max, L2max);
+  return B > 0 ? xlayout<1>(B, L1max, L2max).total : 0;
 }
 
 int swb_sw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
                       int L2max, float gap_open, float gap_ext, float temp, float* out,
                       float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream) {
-  return launch_aux<3, swb::AUX_HVP>(scores, v, lengths, B, L1max, L2max, gap_open, gap_ext, temp,
+  return launch_xband<3, swb::AUX_HVP>(scores, v, lengths, B, L1max, L2max, gap_open, gap_ext, temp,
                                      out, grad_tangents, workspace, workspace_bytes, stream);
 }
 
@@ -367,11 +414,11 @@ int swb_sw_affine_param_jacobian(const float* scores, const int* lengths, int B,
                                  int L2max, float gap_open, float gap_ext, float temp, int param,
                                  float* out, void* workspace, size_t workspace_bytes, void* stream) {
   switch (param) {
-    case 0: return launch_aux<3, swb::AUX_P0>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
+    case 0: return launch_xband<3, swb::AUX_P0>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
                                               gap_ext, temp, out, nullptr, workspace, workspace_bytes, stream);
-    case 1: return launch_aux<3, swb::AUX_P1>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
+    case 1: return launch_xband<3, swb::AUX_P1>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
                                               gap_ext, temp, out, nullptr, workspace, workspace_bytes, stream);
-    case 2: return launch_aux<3, swb::AUX_PT>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
+    case 2: return launch_xband<3, swb::AUX_PT>(scores, nullptr, lengths, B, L1max, L2max, gap_open,
                                               gap_ext, temp, out, nullptr, workspace, workspace_bytes, stream);
     default: return SWB_ERR_ARG;
   }
@@ -380,7 +427,7 @@ int swb_sw_affine_param_jacobian(const float* scores, const int* lengths, int B,
 int swb_sw_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max, int L2max,
                float gap, float temp, float* out, float* grad_tangents, void* workspace,
                size_t workspace_bytes, void* stream) {
-  return launch_aux<1, swb::AUX_HVP>(scores, v, lengths, B, L1max, L2max, gap, 0.f, temp, out,
+  return launch_xband<1, swb::AUX_HVP>(scores, v, lengths, B, L1max, L2max, gap, 0.f, temp, out,
                                      grad_tangents, workspace, workspace_bytes, stream);
 }
 
@@ -388,9 +435,9 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
                           float gap, float temp, int param, float* out, void* workspace,
                           size_t workspace_bytes, void* stream) {
   switch (param) {
-    case 0: return launch_aux<1, swb::AUX_P0>(scores, nullptr, lengths, B, L1max, L2max, gap, 0.f,
+    case 0: return launch_xband<1, swb::AUX_P0>(scores, nullptr, lengths, B, L1max, L2max, gap, 0.f,
                                               temp, out, nullptr, workspace, workspace_bytes, stream);
-    case 1: return launch_aux<1, swb::AUX_PT>(scores, nullptr, lengths, B, L1max, L2max, gap, 0.f,
+    case 1: return launch_xband<1, swb::AUX_PT>(scores, nullptr, lengths, B, L1max, L2max, gap, 0.f,
                                               temp, out, nullptr, workspace, workspace_bytes, stream);
     default: return SWB_ERR_ARG;
   }

@@ -1,0 +1,832 @@
+// Second-order soft Smith-Waterman ops as band wavefronts (sm_100a): the
+// Hessian-vector product of the marginal map, the map's parameter Jacobians,
+// and the tangents of the parameter gradients that the map's full VJP needs.
+// Compiled as part of sw_capi.cu, after sw_kernels.cu (helpers, band
+// geometry).
+//
+// Reference semantics (megure-labs/orihime):
+//   affine  HVP          src/sw_affine/kernels_gpu.cu:623-785 (launcher :1566)
+//           dP/dtheta    src/sw_affine/kernels_gpu.cu:1011-1473 (launcher :1638)
+//           full VJP     src/sw_affine/torch_cuda.cpp:681-811
+//   linear  HVP          src/sw/kernels_cpu.cpp:279-485 (CUDA twin src/sw/kernels_gpu.cu)
+//           dP/dtheta    src/sw/kernels_cpu.cpp:491-710
+//
+// Decomposition: the first-order band wavefront.  A warp owns 32*R columns of
+// one pair; lane l owns R adjacent columns and at step t works on row
+// t - l + 1; bands hand their right edge to the next band through polled
+// buffers.
+//
+// Forward (xfwd_kernel): alpha (double-float, scaled log2 domain) and its
+// tangent U along the direction (the score direction V for the HVP, one
+// parameter for a Jacobian) per state.  Each cell writes what the backward
+// needs -- its normalised predecessor weights, their tangents, its alpha
+// (hi, lo) and U -- to a wavefront-major table: per step, one float4 per
+// lane per field group, so the warp's stores (and later loads) are whole
+// contiguous lines.  Per band it accumulates the partition sum with its
+// U-weighted and log-weighted sums, from which S and dS follow.
+//
+// Backward (xbwd_kernel): the same steps in reverse order, lane 31 leading
+// as in the first-order adjoint.  A cell's beta and its tangent are its init
+// terms plus the pushes of its successors; it pushes beta * w and
+// tangent * w + beta * dw to each predecessor: in registers within a lane,
+// by __shfl_down_sync to the left lane, through a polled buffer to the left
+// band.  Fields stream in by cp.async through a shared-memory ring of
+// XSTAGES steps; each lane copies, and later reads, only its own vectors.
+//
+// Tangents are in natural units.  A weight's tangent along a direction with
+// candidate tangents c_k is w_k (c_k - sum_l w_l c_l) / T; the temperature
+// direction adds w_k (-ln w_k - H) / T, H the entropy (nats) of the cell's
+// softmax, and a cell's U is sum_l w_l c_l (+ H for the temperature).
+namespace swb {
+
+// Direction of the tangent pass: the score direction V (HVP), gap open (or
+// the linear gap), gap extend, temperature.
+enum : int { AUX_HVP = 0, AUX_P0 = 1, AUX_P1 = 2, AUX_PT = 3 };
+constexpr float LN2 = 0.69314718055994531f;
+// Weights below the smallest normal float count as 0 in the log terms: the
+// MUFU lg2 flushes a subnormal input to 0 and would return -inf.
+constexpr float W_TINY = 1.17549435e-38f;
+
+template <int NS> struct XShape;
+// G: float4 field groups per cell; NE: floats per row crossing a band edge
+// forward (hi, lo, tangent of each state); NP: value push channels crossing a
+// lane or band edge backward (their tangents double it).
+template <> struct XShape<3> { static constexpr int G = 6, NE = 9, NP = 5; };
+template <> struct XShape<1> { static constexpr int G = 3, NE = 3, NP = 2; };
+
+constexpr int XC = 4;   // steps per edge / push prefetch chunk
+static_assert(XC % PF == 0, "the score prefetch distance must divide the chunk");
+#ifndef SWB_XSTAGES
+#define SWB_XSTAGES 3
+#endif
+constexpr int XSTAGES = SWB_XSTAGES;   // field steps in flight per backward warp
+
+// floats of one step of fields for one warp
+template <int NS, int R>
+__host__ __device__ constexpr int xstep_floats() { return R * XShape<NS>::G * 128; }
+
+struct XArgs {
+  const float* scores;     // [B, L1m, L2m]
+  const float* v;          // AUX_HVP: direction [B, L1m, L2m], else null
+  const int* lengths;      // [B, 2] or null
+  int B, L1m, L2m, nb;     // nb: bands per pair
+  int nsteps;              // field steps per band slot (>= L1m + 31, multiple of XC)
+  float go, ge, T, k;      // natural parameters (linear: go = gap), k = log2(e) / T
+  float* out;              // [B, L1m, L2m], zero outside lengths (cleared by the host)
+  float* gt;               // AUX_HVP: [B][4] tangents of (g0, g1, g_T, S), or null
+  float* fld;              // per band slot: nsteps * xstep_floats floats
+  float* edge;             // per band slot: NE * L1m floats (sentinel-filled)
+  float* bpush;            // per band slot: 2 * NP * (L1m + 1) floats (sentinel-filled)
+  float* part;             // per band slot: ref, sum, U-sum, log-sum
+  float* gpart;            // per band slot: HVP parameter-tangent partials
+  unsigned* counters;      // [0] forward tasks, [1] backward tasks
+  unsigned* pair_done;     // per pair: backward bands finished
+  unsigned* status;
+  unsigned long long spin_limit_ns;
+};
+
+__device__ __forceinline__ void xlengths(const XArgs& a, int p, int& L1, int& L2) {
+  L1 = a.L1m;
+  L2 = a.L2m;
+  if (a.lengths) {  // never index outside the padded slab
+    L1 = min(max(a.lengths[2 * p], 0), a.L1m);
+    L2 = min(max(a.lengths[2 * p + 1], 0), a.L2m);
+  }
+}
+
+// Row access to a padded [B, L1m, L2m] tensor (and optionally the output map)
+// through the first-order band helpers load_row / store_row.
+__device__ __forceinline__ Pair xpair_of(const XArgs& a, int p, int L1, int L2, const float* src,
+                                         float* dst) {
+  Pair r;
+  const size_t base = (size_t)p * a.L1m * a.L2m;
+  r.s = src + base;
+  r.m = dst ? dst + base : nullptr;
+  r.L1 = L1;
+  r.L2 = L2;
+  r.ld = a.L2m;
+  r.vec = ((r.ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(r.s) & 15) == 0) &&
+          (!dst || (reinterpret_cast<uintptr_t>(r.m) & 15) == 0);
+  return r;
+}
+
+// Weight tangents dw_k = w_k (c_k - cbar [+ (-ln w_k - H)]) / T; returns the
+// cell's tangent cbar [+ H].
+template <int N, bool TM>
+__device__ __forceinline__ float xwtan(const float (&w)[N], const float (&c)[N], float iT,
+                                       float (&dw)[N]) {
+  float cb = 0.f;
+#pragma unroll
+  for (int q = 0; q < N; ++q) cb = fmaf(w[q], c[q], cb);
+  float h = 0.f, nl[N];
+  if (TM) {
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      nl[q] = w[q] > W_TINY ? -lg2(w[q]) * LN2 : 0.f;
+      h = fmaf(w[q], nl[q], h);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    float x = c[q] - cb;
+    if (TM) x += nl[q] - h;
+    dw[q] = w[q] * x * iT;
+  }
+  return TM ? cb + h : cb;
+}
+
+// One affine cell of the forward: new alpha pairs and tangents of M, I, D in
+// o = (Mh, Ml, Mu, Ih, Il, Iu, Dh, Dl, Du) and its backward fields in f:
+//   f0 = (wMM, wMI, wMD, wIM)   f1 = (wII, wDM, wDD, dwMM)
+//   f2 = (dwMI, dwMD, dwIM, dwII)  f3 = (dwDM, dwDD, Mh, Ih)
+//   f4 = (Dh, Ml, Il, Dl)       f5 = (uM, uI, uD, 0)
+// Predecessors: diag (dh, dl, du) of M, I, D; up M and I; left M and D.
+template <int MODE>
+__device__ __forceinline__ void xcell3(const float (&dh)[3], const float (&dl)[3],
+                                       const float (&du)[3], float uMh, float uMl, float uMu,
+                                       float uIh, float uIl, float uIu, float lMh, float lMl,
+                                       float lMu, float lDh, float lDl, float lDu, float s,
+                                       float vv, float g0, float g1, float iT, float (&o)[9],
+                                       float4 (&f)[6]) {
+  constexpr bool TM = (MODE == AUX_PT);
+  // M = s + LSE(M, I, D at diag, 0)
+  const float r = fmaxf(fmaxf(dh[0], dh[1]), fmaxf(dh[2], 0.f));
+  const float tM = ex2((dh[0] - r) + dl[0]), tI = ex2((dh[1] - r) + dl[1]);
+  const float tD = ex2((dh[2] - r) + dl[2]), tZ = ex2(-r);
+  const float sm = (tM + tI) + (tD + tZ);
+  float Mh, Ml;
+  two_sum(r, s, Mh, Ml);
+  Ml += lg2(sm);
+  const float vm = recip(sm);
+  const float wm[4] = {tM * vm, tI * vm, tD * vm, tZ * vm};
+  // I = LSE(M up + go, I up + ge)
+  const float ru = fmaxf(uMh + g0, uIh + g1);
+  const float ta = ex2(((uMh - ru) + g0) + uMl), tb = ex2(((uIh - ru) + g1) + uIl);
+  const float si = ta + tb;
+  float Ih, Il;
+  fast2(ru, lg2(si), Ih, Il);
+  const float vi = recip(si);
+  const float wi[2] = {ta * vi, tb * vi};
+  // D = LSE(M left + go, D left + ge)
+  const float rl = fmaxf(lMh + g0, lDh + g1);
+  const float tc = ex2(((lMh - rl) + g0) + lMl), td = ex2(((lDh - rl) + g1) + lDl);
+  const float sd = tc + td;
+  float Dh, Dl;
+  fast2(rl, lg2(sd), Dh, Dl);
+  const float vd = recip(sd);
+  const float wd[2] = {tc * vd, td * vd};
+  // candidate tangents: predecessors' U, the score direction on M's terms,
+  // 1 on the gap terms of the differentiated parameter
+  float cm[4] = {du[0], du[1], du[2], 0.f};
+  if (MODE == AUX_HVP) { cm[0] += vv; cm[1] += vv; cm[2] += vv; cm[3] = vv; }
+  float ci[2] = {uMu, uIu}, cd[2] = {lMu, lDu};
+  if (MODE == AUX_P0) { ci[0] += 1.f; cd[0] += 1.f; }
+  if (MODE == AUX_P1) { ci[1] += 1.f; cd[1] += 1.f; }
+  float dwm[4], dwi[2], dwd[2];
+  const float uM = xwtan<4, TM>(wm, cm, iT, dwm);
+  const float uI = xwtan<2, TM>(wi, ci, iT, dwi);
+  const float uD = xwtan<2, TM>(wd, cd, iT, dwd);
+  o[0] = Mh; o[1] = Ml; o[2] = uM;
+  o[3] = Ih; o[4] = Il; o[5] = uI;
+  o[6] = Dh; o[7] = Dl; o[8] = uD;
+  f[0] = make_float4(wm[0], wm[1], wm[2], wi[0]);
+  f[1] = make_float4(wi[1], wd[0], wd[1], dwm[0]);
+  f[2] = make_float4(dwm[1], dwm[2], dwi[0], dwi[1]);
+  f[3] = make_float4(dwd[0], dwd[1], Mh, Ih);
+  f[4] = make_float4(Dh, Ml, Il, Dl);
+  f[5] = make_float4(uM, uI, uD, 0.f);
+}
+
+// One linear cell: o = (Ah, Al, U); fields
+//   f0 = (w_diag, w_up, w_left, w_diag + w_start)
+//   f1 = (dw_diag, dw_up, dw_left, dw_diag + dw_start)   f2 = (Ah, Al, U, 0)
+template <int MODE>
+__device__ __forceinline__ void xcell1(float dh, float dl, float du, float uh, float ul, float uu,
+                                       float lh, float ll, float lu, float s, float vv, float g,
+                                       float iT, float (&o)[3], float4 (&f)[3]) {
+  constexpr bool TM = (MODE == AUX_PT);
+  // A = LSE(diag + s, up + g, left + g, s)
+  const float r = fmaxf(fmaxf(dh + s, uh + g), fmaxf(lh + g, s));
+  const float ta = ex2(((dh - r) + s) + dl), tu = ex2(((uh - r) + g) + ul);
+  const float tl = ex2(((lh - r) + g) + ll), ts = ex2(s - r);
+  const float sm = (ta + tu) + (tl + ts);
+  float Ah, Al;
+  fast2(r, lg2(sm), Ah, Al);
+  const float v = recip(sm);
+  const float w[4] = {ta * v, tu * v, tl * v, ts * v};
+  float c[4] = {du, uu, lu, 0.f};
+  if (MODE == AUX_HVP) { c[0] += vv; c[3] = vv; }
+  if (MODE == AUX_P0) { c[1] += 1.f; c[2] += 1.f; }
+  float dw[4];
+  const float U = xwtan<4, TM>(w, c, iT, dw);
+  o[0] = Ah; o[1] = Al; o[2] = U;
+  f[0] = make_float4(w[0], w[1], w[2], w[0] + w[3]);
+  f[1] = make_float4(dw[0], dw[1], dw[2], dw[0] + dw[3]);
+  f[2] = make_float4(Ah, Al, U, 0.f);
+}
+
+// (ref, sum 2^(x-ref), sum 2^(x-ref) U, sum 2^(x-ref) (x-ref)) merged into
+// the first tuple at the larger reference.
+__device__ __forceinline__ void xcombine(float& r1, float& s1, float& u1, float& x1, float r2,
+                                         float s2, float u2, float x2) {
+  const float m = fmaxf(r1, r2), d1 = r1 - m, d2 = r2 - m;
+  const float f1 = ex2(d1), f2 = ex2(d2);
+  x1 = f1 * fmaf(d1, s1, x1) + f2 * fmaf(d2, s2, x2);
+  s1 = s1 * f1 + s2 * f2;
+  u1 = u1 * f1 + u2 * f2;
+  r1 = m;
+}
+
+// ---------------------------------------------------------------------------
+// forward band task
+// ---------------------------------------------------------------------------
+
+template <int NS, int R, int MODE>
+__device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t deadline) {
+  using XS = XShape<NS>;
+  constexpr int G = XS::G, NE = XS::NE;
+  constexpr int XSTEP = xstep_floats<NS, R>();
+  constexpr bool HV = (MODE == AUX_HVP);
+  int L1, L2;
+  xlengths(a, p, L1, L2);
+  const size_t slot = (size_t)p * a.nb + band;
+  float* part = a.part + 4 * slot;
+  const int col0 = band * 32 * R;
+  if (!(L1 > 0 && col0 < L2)) {
+    if (lane == 0) { part[0] = 0.f; part[1] = (band == 0) ? 1.f : 0.f; part[2] = 0.f; part[3] = 0.f; }
+    return;
+  }
+  const Pair ps = xpair_of(a, p, L1, L2, a.scores, nullptr);
+  const Pair pv = xpair_of(a, p, L1, L2, HV ? a.v : a.scores, nullptr);
+  const int jl = col0 + lane * R;
+  const float k = a.k, g0 = a.go * k, g1 = a.ge * k, iT = 1.f / a.T;
+  const size_t Lm = (size_t)a.L1m;
+  float* eout = a.edge + slot * NE * Lm;
+  const float* ein = (band > 0) ? eout - NE * Lm : nullptr;
+  float* F = a.fld + slot * (size_t)a.nsteps * XSTEP;
+  const int nch = (L1 + 31 + XC - 1) / XC;
+
+  float ph[NS][R], pl[NS][R], pu[NS][R], lh[NS], ll[NS], lu[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    lh[q] = NEG; ll[q] = 0.f; lu[q] = 0.f;
+#pragma unroll
+    for (int c = 0; c < R; ++c) { ph[q][c] = NEG; pl[q][c] = 0.f; pu[q][c] = 0.f; }
+  }
+  float ref = 0.f, su = 0.f, sx = 0.f;
+  KSum acc;
+  if (band == 0 && lane == 0) acc.s = 1.f;  // origin M[0,0] = 0: weight 1, U 0, log term 0
+
+  // Lane u < XC holds the left band's edge values that lane 0 needs at step u
+  // of a chunk, loaded one chunk ahead; lane 0 takes them by shuffle.
+  float eb[NE], ebn[NE];
+  auto load_edge = [&](int kc, float (&dst)[NE]) {
+    const int i = kc * XC + lane + 1;
+    const bool ok = ein && lane < XC && i <= L1;
+#pragma unroll
+    for (int f = 0; f < NE; ++f) dst[f] = ok ? ld_poll(ein + f * Lm + (i - 1)) : 0.f;
+  };
+  load_edge(0, eb);
+  float sb[PF][R], vb[PF][R];
+#pragma unroll
+  for (int u = 0; u < PF; ++u) {
+    const int i = u - lane + 1;
+    load_row<R>(ps, i, jl, i >= 1 && i <= L1, sb[u]);
+    load_row<R>(pv, i, jl, HV && i >= 1 && i <= L1, vb[u]);
+  }
+
+  for (int kc = 0; kc < nch; ++kc) {
+    if (kc + 1 < nch) load_edge(kc + 1, ebn);
+#pragma unroll 1
+    for (int u0 = 0; u0 < XC; u0 += PF)
+#pragma unroll
+      for (int u = 0; u < PF; ++u) {
+        const int cu = u0 + u;
+        const int t = kc * XC + cu;
+        const int i = t - lane + 1;
+        const bool act = (i >= 1) && (i <= L1);
+        float xh[NS], xl[NS], xu[NS], ev[NE];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          xh[q] = __shfl_up_sync(FULL, ph[q][R - 1], 1);
+          xl[q] = __shfl_up_sync(FULL, pl[q][R - 1], 1);
+          xu[q] = __shfl_up_sync(FULL, pu[q][R - 1], 1);
+        }
+#pragma unroll
+        for (int f = 0; f < NE; ++f) ev[f] = __shfl_sync(FULL, eb[f], cu);
+        // a value still at the sentinel (left band not there yet) is polled
+        // on a warp-uniform slow path
+        bool miss = false;
+#pragma unroll
+        for (int f = 0; f < NE; ++f) miss |= is_sentinel(ev[f]);
+        miss = (lane == 0) && ein && act && miss;
+        if (__any_sync(FULL, miss) && miss) {
+          float fb[NE];
+#pragma unroll
+          for (int f = 0; f < NE; ++f) fb[f] = f < NS ? NEG : 0.f;
+          poll_fields<NE>(ev, ein + (i - 1), Lm, deadline, a.status, fb);
+        }
+        if (lane == 0) {
+          const bool take = act && ein;
+#pragma unroll
+          for (int q = 0; q < NS; ++q) {
+            xh[q] = take ? ev[q] : NEG;
+            xl[q] = take ? ev[NS + q] : 0.f;
+            xu[q] = take ? ev[2 * NS + q] : 0.f;
+          }
+        }
+        float dgh[NS], dgl[NS], dgu[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          dgh[q] = lh[q]; dgl[q] = ll[q]; dgu[q] = lu[q];
+          lh[q] = xh[q]; ll[q] = xl[q]; lu[q] = xu[q];
+        }
+        float s[R], vv[R];
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+          s[c] = i >= 1 ? __fmul_rn(sb[u][c], k) : NEG;
+          vv[c] = HV ? vb[u][c] : 0.f;
+        }
+        {
+          const int ip = i + PF;
+          load_row<R>(ps, ip, jl, ip >= 1 && ip <= L1, sb[u]);
+          load_row<R>(pv, ip, jl, HV && ip >= 1 && ip <= L1, vb[u]);
+        }
+        float* Fs = F + (size_t)t * XSTEP;
+        // left values inside the row: start from the left input, which itself
+        // stays as the next step's diagonal of column 0
+        float wh[NS], wl[NS], wu[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) { wh[q] = lh[q]; wl[q] = ll[q]; wu[q] = lu[q]; }
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+          if constexpr (NS == 3) {
+            const float uMh = ph[0][c], uMl = pl[0][c], uMu = pu[0][c];
+            const float uIh = ph[1][c], uIl = pl[1][c], uIu = pu[1][c];
+            const float uDh = ph[2][c], uDl = pl[2][c], uDu = pu[2][c];
+            float o[9];
+            float4 f[6];
+            xcell3<MODE>(dgh, dgl, dgu, uMh, uMl, uMu, uIh, uIl, uIu, wh[0], wl[0], wu[0], wh[2],
+                         wl[2], wu[2], s[c], vv[c], g0, g1, iT, o, f);
+#pragma unroll
+            for (int g = 0; g < G; ++g) reinterpret_cast<float4*>(Fs + (c * G + g) * 128)[lane] = f[g];
+            dgh[0] = uMh; dgl[0] = uMl; dgu[0] = uMu;
+            dgh[1] = uIh; dgl[1] = uIl; dgu[1] = uIu;
+            dgh[2] = uDh; dgl[2] = uDl; dgu[2] = uDu;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              wh[q] = o[3 * q]; wl[q] = o[3 * q + 1]; wu[q] = o[3 * q + 2];
+              ph[q][c] = o[3 * q]; pl[q][c] = o[3 * q + 1]; pu[q][c] = o[3 * q + 2];
+            }
+          } else {
+            const float uh = ph[0][c], ul = pl[0][c], uu = pu[0][c];
+            float o[3];
+            float4 f[3];
+            xcell1<MODE>(dgh[0], dgl[0], dgu[0], uh, ul, uu, wh[0], wl[0], wu[0], s[c], vv[c], g0,
+                         iT, o, f);
+#pragma unroll
+            for (int g = 0; g < G; ++g) reinterpret_cast<float4*>(Fs + (c * G + g) * 128)[lane] = f[g];
+            dgh[0] = uh; dgl[0] = ul; dgu[0] = uu;
+            wh[0] = o[0]; wl[0] = o[1]; wu[0] = o[2];
+            ph[0][c] = o[0]; pl[0][c] = o[1]; pu[0][c] = o[2];
+          }
+        }
+        if (act) {
+          // partition with its U- and log-weighted sums, lazily rescaled:
+          // exponents stay <= 8 so (hi - ref) + lo rounds at <= 2^-21
+          float mx = NEG;
+#pragma unroll
+          for (int c = 0; c < R; ++c)
+            if (jl + c < L2)
+#pragma unroll
+              for (int q = 0; q < NS; ++q) mx = fmaxf(mx, ph[q][c]);
+          if (mx > ref + 8.f) {
+            const float d = ref - mx, f = ex2(d);
+            sx = f * fmaf(d, acc.s, sx);
+            acc.s *= f;
+            acc.c *= f;
+            su *= f;
+            ref = mx;
+          }
+          float ts = 0.f, tu = 0.f, tx = 0.f;
+#pragma unroll
+          for (int c = 0; c < R; ++c)
+            if (jl + c < L2)
+#pragma unroll
+              for (int q = 0; q < NS; ++q) {
+                const float x = (ph[q][c] - ref) + pl[q][c];
+                const float e = ex2(x);
+                ts += e;
+                tu = fmaf(e, pu[q][c], tu);
+                tx = fmaf(e, x, tx);
+              }
+          acc.add(ts);
+          su += tu;
+          sx += tx;
+          if (lane == 31) {
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+              eout[q * Lm + (i - 1)] = ph[q][R - 1];
+              eout[(NS + q) * Lm + (i - 1)] = pl[q][R - 1];
+              eout[(2 * NS + q) * Lm + (i - 1)] = pu[q][R - 1];
+            }
+          }
+        }
+      }
+#pragma unroll
+    for (int f = 0; f < NE; ++f) eb[f] = ebn[f];
+  }
+  // warp-combine the lanes' tuples (fixed shuffle tree: deterministic)
+  float s_ = acc.s;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float r2 = __shfl_xor_sync(FULL, ref, o), s2 = __shfl_xor_sync(FULL, s_, o);
+    const float u2 = __shfl_xor_sync(FULL, su, o), x2 = __shfl_xor_sync(FULL, sx, o);
+    xcombine(ref, s_, su, sx, r2, s2, u2, x2);
+  }
+  if (lane == 0) { part[0] = ref; part[1] = s_; part[2] = su; part[3] = sx; }
+}
+
+template <int NS, int R, int MODE>
+__global__ void __launch_bounds__(128) xfwd_kernel(XArgs a) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t deadline = gtimer() + a.spin_limit_ns;
+  const int ntasks = a.B * a.nb;
+  while (true) {
+    int task = 0;
+    if (lane == 0) task = (int)atomicAdd(a.counters + 0, 1u);
+    task = __shfl_sync(FULL, task, 0);
+    if (task >= ntasks) break;
+    const int p = task / a.nb;
+    xfwd_band<NS, R, MODE>(a, p, task - p * a.nb, lane, deadline);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// backward band task
+// ---------------------------------------------------------------------------
+
+// S' = Sh + Sl (scaled) and dS of pair p from its bands' forward tuples.
+template <bool TM>
+__device__ __forceinline__ void xpair_stats(const XArgs& a, int p, int lane, float& Sh, float& Sl,
+                                            float& dS) {
+  float ref = NEG, s = 0.f, su = 0.f, sx = 0.f;
+  for (int b = lane; b < a.nb; b += 32) {
+    const float* q = a.part + 4 * ((size_t)p * a.nb + b);
+    const float r2 = q[0], s2 = q[1], u2 = q[2], x2 = q[3];
+    if (s2 > 0.f) xcombine(ref, s, su, sx, r2, s2, u2, x2);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float r2 = __shfl_xor_sync(FULL, ref, o), s2 = __shfl_xor_sync(FULL, s, o);
+    const float u2 = __shfl_xor_sync(FULL, su, o), x2 = __shfl_xor_sync(FULL, sx, o);
+    xcombine(ref, s, su, sx, r2, s2, u2, x2);
+  }
+  // S = ref + log2(s) as a double-float: with s = m * 2^e, m in [1, 2), lg2
+  // sees only the mantissa and the integer e joins ref by TwoSum
+  const unsigned bits = __float_as_uint(s);
+  const int e = (int)((bits >> 23) & 0xffu) - 127;
+  float lgs;
+  if (s > 0.f && e > -127 && e < 128) {
+    const float lm = lg2(__uint_as_float((bits & 0x7fffffu) | 0x3f800000u));
+    float h, l;
+    two_sum(ref, (float)e, h, l);
+    Sh = h;
+    Sl = l + lm;
+    lgs = (float)e + lm;
+  } else {
+    Sh = ref;
+    Sl = lg2(s);
+    lgs = Sl;
+  }
+  // dS = sum P U - [T] ln2 sum P log2 P, P = 2^(x - S):
+  // sum P (x - S) = sx / s - log2(s)
+  dS = su / s - (TM ? (sx / s - lgs) * LN2 : 0.f);
+}
+
+__device__ __forceinline__ void cp_async16(float* sdst, const float* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Band partials of the HVP's parameter tangents; the last band of a pair to
+// finish folds them (in band order: deterministic) into grad_tangents.
+template <int NS, int MODE>
+__device__ void xfinish(const XArgs& a, int p, int band, int lane, bool empty, float dS, float ga,
+                        float gb, float gc) {
+  if (MODE != AUX_HVP || !a.gt) return;
+  if (lane == 0) {
+    float* gp = a.gpart + 4 * ((size_t)p * a.nb + band);
+    gp[0] = ga; gp[1] = gb; gp[2] = gc; gp[3] = 0.f;
+    __threadfence();
+    const unsigned done = atomicAdd(a.pair_done + p, 1u);
+    if (done == (unsigned)a.nb - 1) {
+      __threadfence();
+      float o = 0.f, e = 0.f, c = 0.f;
+      for (int b = 0; b < a.nb; ++b) {
+        const float* q = a.gpart + 4 * ((size_t)p * a.nb + b);
+        o += ld_poll(q + 0);
+        e += ld_poll(q + 1);
+        c += ld_poll(q + 2);
+      }
+      float* g = a.gt + 4 * p;
+      if (empty) {
+        g[0] = 0.f; g[1] = 0.f; g[2] = 0.f; g[3] = 0.f;
+      } else {
+        const float gTt = (dS - c - (NS == 3 ? a.go * o + a.ge * e : a.go * o)) * (1.f / a.T);
+        g[0] = o;
+        g[1] = (NS == 3) ? e : gTt;
+        g[2] = (NS == 3) ? gTt : 0.f;
+        g[3] = dS;
+      }
+    }
+  }
+}
+
+template <int NS, int R, int MODE>
+__device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring,
+                          uint64_t deadline) {
+  using XS = XShape<NS>;
+  constexpr int G = XS::G, NP = XS::NP, NQ = 2 * NP;
+  constexpr int XSTEP = xstep_floats<NS, R>();
+  constexpr bool TM = (MODE == AUX_PT), HV = (MODE == AUX_HVP);
+  int L1, L2;
+  xlengths(a, p, L1, L2);
+  const int col0 = band * 32 * R;
+  float Sh, Sl, dS;
+  xpair_stats<TM>(a, p, lane, Sh, Sl, dS);
+  if (!(L1 > 0 && col0 < L2)) {
+    xfinish<NS, MODE>(a, p, band, lane, L1 == 0 || L2 == 0, dS, 0.f, 0.f, 0.f);
+    return;
+  }
+  const size_t slot = (size_t)p * a.nb + band;
+  const Pair po = xpair_of(a, p, L1, L2, a.scores, a.out);
+  const Pair pv = xpair_of(a, p, L1, L2, HV ? a.v : a.scores, nullptr);
+  const int jl = col0 + lane * R;
+  const float iT = 1.f / a.T;
+  const size_t Lm = (size_t)a.L1m;
+  float* pout = (band > 0) ? a.bpush + slot * NQ * (Lm + 1) : nullptr;
+  const bool right_live = (col0 + 32 * R) < L2 && (band + 1) < a.nb;
+  const float* pin = right_live ? a.bpush + (slot + 1) * NQ * (Lm + 1) : nullptr;
+  const float* F = a.fld + slot * (size_t)a.nsteps * XSTEP;
+  const int nch = (L1 + 31 + XC - 1) / XC;
+  const int nst = nch * XC;   // steps, padded to whole chunks (padding steps find no row)
+
+  // field ring: reverse step tt (forward step nst - 1 - tt) in stage tt % XSTAGES
+  auto issue = [&](int tt) {
+    if (tt < nst) {
+      const float* src = F + (size_t)(nst - 1 - tt) * XSTEP;
+      float* dst = ring + (size_t)(tt % XSTAGES) * XSTEP;
+#pragma unroll
+      for (int cg = 0; cg < R * G; ++cg) cp_async16(dst + (cg * 32 + lane) * 4, src + (cg * 32 + lane) * 4);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int q = 0; q < XSTAGES - 1; ++q) issue(q);
+
+  // right-band pushes: lane u < XC holds those lane 31 needs at step u of a chunk
+  float pbc[NQ], pbn[NQ];
+  auto load_pb = [&](int kc, float (&dst)[NQ]) {
+    const int i = kc * XC + XC - 1 - lane - 30;  // lane 31's row at chunk step lane
+    const bool ok = pin && lane < XC && i >= 1 && i <= L1;
+#pragma unroll
+    for (int f = 0; f < NQ; ++f) {
+      const int fc = f % NP;
+      const bool left = (NS == 3) ? (fc < 2) : (fc < 1);
+      dst[f] = (ok && (left || i < L1)) ? ld_poll(pin + f * (Lm + 1) + i) : 0.f;
+    }
+  };
+  load_pb(nch - 1, pbc);
+  // HVP: raw scores and direction of the rows PF steps ahead
+  float sb[PF][R], vb[PF][R];
+#pragma unroll
+  for (int u = 0; u < PF; ++u) {
+    const int i = (nst - 1 - u) - lane + 1;
+    load_row<R>(po, i, jl, HV && i >= 1 && i <= L1, sb[u]);
+    load_row<R>(pv, i, jl, HV && i >= 1 && i <= L1, vb[u]);
+  }
+
+  float ac[NS][R], at[NS][R], nx[NS][R], nt[NS][R];
+#pragma unroll
+  for (int q = 0; q < NS; ++q)
+#pragma unroll
+    for (int c = 0; c < R; ++c) { ac[q][c] = 0.f; at[q][c] = 0.f; nx[q][c] = 0.f; nt[q][c] = 0.f; }
+  float hold[NS], holdt[NS], outp[NQ];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) { hold[q] = 0.f; holdt[q] = 0.f; }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) outp[q] = 0.f;
+  KSum kA, kB, kC;
+
+  for (int kc = nch - 1; kc >= 0; --kc) {
+    if (kc > 0) load_pb(kc - 1, pbn);
+#pragma unroll 1
+    for (int u0 = 0; u0 < XC; u0 += PF)
+#pragma unroll
+      for (int u = 0; u < PF; ++u) {
+        const int cu = u0 + u;
+        const int t = kc * XC + (XC - 1 - cu);
+        const int tt = nst - 1 - t;
+        const int i = t - lane + 1;
+        const bool act = (i >= 1) && (i <= L1);
+        issue(tt + XSTAGES - 1);
+        cp_async_wait<XSTAGES - 1>();
+        const float* E = ring + (size_t)(tt % XSTAGES) * XSTEP + lane * 4;
+        float r[NQ], pw[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          r[q] = __shfl_down_sync(FULL, outp[q], 1);
+          pw[q] = __shfl_sync(FULL, pbc[q], cu);
+        }
+        {
+          bool miss = false;
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) miss |= is_sentinel(pw[q]);
+          miss = miss && (lane == 31);
+          if (__any_sync(FULL, miss) && miss) {
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+              if (is_sentinel(pw[q]))
+                pw[q] = poll_value(pin + q * (Lm + 1) + i, ld_poll(pin + q * (Lm + 1) + i), deadline,
+                                   a.status, 0.f);
+          }
+        }
+        // pushes arriving at column R-1 of row i: from the right lane (or band)
+        // into the left of this cell, and into its diagonal from (i+1, j+1)
+        if constexpr (NS == 3) {
+          float iL0, iL1, tL0, tL1, iD[3], tD[3];
+          if (lane == 31) {
+            iL0 = pw[0]; iL1 = pw[1]; tL0 = pw[NP + 0]; tL1 = pw[NP + 1];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) { iD[q] = pw[2 + q]; tD[q] = pw[NP + 2 + q]; }
+          } else {
+            iL0 = r[0]; iL1 = r[1]; tL0 = r[NP + 0]; tL1 = r[NP + 1];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              iD[q] = hold[q]; hold[q] = r[2 + q];
+              tD[q] = holdt[q]; holdt[q] = r[NP + 2 + q];
+            }
+          }
+          ac[0][R - 1] += iL0 + iD[0]; ac[1][R - 1] += iD[1]; ac[2][R - 1] += iL1 + iD[2];
+          at[0][R - 1] += tL0 + tD[0]; at[1][R - 1] += tD[1]; at[2][R - 1] += tL1 + tD[2];
+        } else {
+          float iL, tL, iD, tD;
+          if (lane == 31) {
+            iL = pw[0]; iD = pw[1]; tL = pw[2]; tD = pw[3];
+          } else {
+            iL = r[0]; tL = r[2];
+            iD = hold[0]; hold[0] = r[1];
+            tD = holdt[0]; holdt[0] = r[3];
+          }
+          ac[0][R - 1] += iL + iD;
+          at[0][R - 1] += tL + tD;
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) outp[q] = 0.f;
+        float sc[R], vv[R];
+#pragma unroll
+        for (int c = 0; c < R; ++c) { sc[c] = sb[u][c]; vv[c] = vb[u][c]; }
+        if (HV) {
+          const int ip = i - PF;
+          load_row<R>(po, ip, jl, ip >= 1 && ip <= L1, sb[u]);
+          load_row<R>(pv, ip, jl, ip >= 1 && ip <= L1, vb[u]);
+        }
+        float cA = 0.f, cB = 0.f, cC = 0.f;
+        float pm[R];
+#pragma unroll
+        for (int c = R - 1; c >= 0; --c) {
+          float4 f[G];
+#pragma unroll
+          for (int g = 0; g < G; ++g) f[g] = *reinterpret_cast<const float4*>(E + (c * G + g) * 128);
+          const bool live = act && (jl + c < L2);
+          if constexpr (NS == 3) {
+            const float xs[3] = {(f[3].z - Sh) + (f[4].y - Sl), (f[3].w - Sh) + (f[4].z - Sl),
+                                 (f[4].x - Sh) + (f[4].w - Sl)};
+            const float us[3] = {f[5].x, f[5].y, f[5].z};
+            float b[3] = {ac[0][c], ac[1][c], ac[2][c]}, tg[3] = {at[0][c], at[1][c], at[2][c]};
+#pragma unroll
+            for (int st = 0; st < 3; ++st) {
+              const float e0 = live ? ex2(fminf(xs[st], 0.f)) : 0.f;
+              b[st] += e0;
+              float x = us[st] - dS;
+              if (TM) x -= (e0 > 0.f ? xs[st] * LN2 : 0.f);
+              tg[st] += e0 * x * iT;
+            }
+            // f0 = (wMM, wMI, wMD, wIM) f1 = (wII, wDM, wDD, dwMM)
+            // f2 = (dwMI, dwMD, dwIM, dwII) f3 = (dwDM, dwDD, ...)
+            const float qM = b[0] * f[0].x, qI = b[0] * f[0].y, qD = b[0] * f[0].z;
+            const float pIM = b[1] * f[0].w, pII = b[1] * f[1].x;
+            const float pDM = b[2] * f[1].y, pDD = b[2] * f[1].z;
+            const float tqM = fmaf(tg[0], f[0].x, b[0] * f[1].w);
+            const float tqI = fmaf(tg[0], f[0].y, b[0] * f[2].x);
+            const float tqD = fmaf(tg[0], f[0].z, b[0] * f[2].y);
+            const float tIM = fmaf(tg[1], f[0].w, b[1] * f[2].z);
+            const float tII = fmaf(tg[1], f[1].x, b[1] * f[2].w);
+            const float tDM = fmaf(tg[2], f[1].y, b[2] * f[3].x);
+            const float tDD = fmaf(tg[2], f[1].z, b[2] * f[3].y);
+            pm[c] = tg[0];
+            if (HV) {
+              cA += tIM + tDM;
+              cB += tII + tDD;
+              cC = fmaf(tg[0], sc[c], fmaf(b[0], vv[c], cC));
+            }
+            nx[0][c] += pIM; nx[1][c] += pII;
+            nt[0][c] += tIM; nt[1][c] += tII;
+            if (c > 0) {
+              nx[0][c - 1] += qM; nx[1][c - 1] += qI; nx[2][c - 1] += qD;
+              nt[0][c - 1] += tqM; nt[1][c - 1] += tqI; nt[2][c - 1] += tqD;
+              ac[0][c - 1] += pDM; ac[2][c - 1] += pDD;
+              at[0][c - 1] += tDM; at[2][c - 1] += tDD;
+            } else {
+              outp[0] = pDM; outp[1] = pDD; outp[2] = qM; outp[3] = qI; outp[4] = qD;
+              outp[NP + 0] = tDM; outp[NP + 1] = tDD;
+              outp[NP + 2] = tqM; outp[NP + 3] = tqI; outp[NP + 4] = tqD;
+            }
+          } else {
+            // f0 = (w_diag, w_up, w_left, map factor) f1 = their tangents
+            // f2 = (Ah, Al, U, 0)
+            const float xs = (f[2].x - Sh) + (f[2].y - Sl);
+            const float e0 = live ? ex2(fminf(xs, 0.f)) : 0.f;
+            const float b = ac[0][c] + e0;
+            float x = f[2].z - dS;
+            if (TM) x -= (e0 > 0.f ? xs * LN2 : 0.f);
+            const float tg = at[0][c] + e0 * x * iT;
+            const float P = b * f[0].w;
+            const float Pd = fmaf(tg, f[0].w, b * f[1].w);
+            const float pD = b * f[0].x, pU = b * f[0].y, pL = b * f[0].z;
+            const float tpD = fmaf(tg, f[0].x, b * f[1].x);
+            const float tpU = fmaf(tg, f[0].y, b * f[1].y);
+            const float tpL = fmaf(tg, f[0].z, b * f[1].z);
+            pm[c] = Pd;
+            if (HV) {
+              cA += tpU + tpL;
+              cC = fmaf(Pd, sc[c], fmaf(P, vv[c], cC));
+            }
+            nx[0][c] += pU;
+            nt[0][c] += tpU;
+            if (c > 0) {
+              nx[0][c - 1] += pD; nt[0][c - 1] += tpD;
+              ac[0][c - 1] += pL; at[0][c - 1] += tpL;
+            } else {
+              outp[0] = pL; outp[1] = pD; outp[2] = tpL; outp[3] = tpD;
+            }
+          }
+        }
+        if (act) {
+          store_row<R>(po, i, jl, pm);
+          if (lane == 0 && pout) {
+#pragma unroll
+            for (int f = 0; f < NQ; ++f) {
+              const int fc = f % NP;
+              const bool left = (NS == 3) ? (fc < 2) : (fc < 1);
+              pout[f * (Lm + 1) + (left ? i : i - 1)] = outp[f];
+            }
+          }
+        }
+        if (HV) { kA.add(cA); kB.add(cB); kC.add(cC); }
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+#pragma unroll
+          for (int c = 0; c < R; ++c) {
+            ac[q][c] = nx[q][c]; nx[q][c] = 0.f;
+            at[q][c] = nt[q][c]; nt[q][c] = 0.f;
+          }
+      }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) pbc[q] = pbn[q];
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncwarp();
+  float v0 = kA.s, v1 = kB.s, v2 = kC.s;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 += __shfl_xor_sync(FULL, v0, o);
+    v1 += __shfl_xor_sync(FULL, v1, o);
+    v2 += __shfl_xor_sync(FULL, v2, o);
+  }
+  xfinish<NS, MODE>(a, p, band, lane, false, dS, v0, v1, v2);
+}
+
+template <int NS, int R, int MODE>
+__global__ void __launch_bounds__(32) xbwd_kernel(XArgs a) {
+  extern __shared__ __align__(16) float xring[];
+  const int lane = threadIdx.x & 31;
+  const uint64_t deadline = gtimer() + a.spin_limit_ns;
+  const int ntasks = a.B * a.nb;
+  while (true) {
+    int task = 0;
+    if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
+    task = __shfl_sync(FULL, task, 0);
+    if (task >= ntasks) break;
+    const int p = task / a.nb;
+    xbwd_band<NS, R, MODE>(a, p, a.nb - 1 - (task - p * a.nb), lane, xring, deadline);
+  }
+}
+
+}  // namespace swb

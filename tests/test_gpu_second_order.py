@@ -201,3 +201,22 @@ def test_forward_ops_are_differentiable(fam):
     for k, p in enumerate(ps):
         want_p = float((a * vg[k]).sum() + mb[1 + k].sum())
         assert abs(float(p.grad) - want_p) <= 1e-4 * max(1.0, abs(want_p)), (k, float(p.grad), want_p)
+
+
+def test_pair_groups_match_single_call(monkeypatch):
+    """A batch whose field table exceeds the memory budget runs in pair
+    groups; pairs are independent, so each group's outputs equal the
+    single-call outputs bit for bit (both use 2 columns per lane here)."""
+    from orihime_b200 import _ops
+
+    s = _scores(5, 40, 70, 11).cuda()
+    v = _scores(5, 40, 70, 12, scale=1.0).cuda()
+    ln = torch.tensor([[40, 70], [17, 33], [0, 5], [40, 1], [23, 70]], dtype=torch.int32).cuda()
+    want, want_gt = _ops.run_hvp("sw_affine", s, v, ln, (*AFF, 0.6), want_grads=True)
+    want_p = _ops.run_param_jacobian("sw", s, ln, (*LIN, 0.6), 1)
+    monkeypatch.setattr(_ops, "AUX_BUDGET_MAX", 1)
+    assert _ops._aux_plan(True, 5, 40, 70, s.device)[0] == 1
+    got, got_gt = _ops.run_hvp("sw_affine", s, v, ln, (*AFF, 0.6), want_grads=True)
+    got_p = _ops.run_param_jacobian("sw", s, ln, (*LIN, 0.6), 1)
+    assert torch.equal(got, want) and torch.equal(got_gt, want_gt) and torch.equal(got_p, want_p)
+    assert float(want[2].abs().max()) == 0.0 and float(want_gt[2].abs().max()) == 0.0
