@@ -278,8 +278,9 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
 // ---- second-order ops as band wavefronts ----
 
 // Columns per lane of the second-order kernels: 4 once the batch has at least
-// kXTasksR4 bands of 128 columns (enough warps to fill the GPU), else 2.
-constexpr long long kXTasksR4 = 2048;
+// kXTasksR4 bands of 128 columns (measured at 256 x 512^2: HVP 3.2 ms at 4
+// against 4.5 ms at 2), else 2, which doubles the warps for small batches.
+constexpr long long kXTasksR4 = 256;
 #ifndef SWB_XR
 #define SWB_XR 0
 #endif

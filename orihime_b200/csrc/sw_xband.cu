@@ -55,11 +55,21 @@ template <> struct XShape<3> { static constexpr int G = 6, NE = 9, NP = 5; };
 template <> struct XShape<1> { static constexpr int G = 3, NE = 3, NP = 2; };
 
 constexpr int XC = 4;   // steps per edge / push prefetch chunk
-static_assert(XC % PF == 0, "the score prefetch distance must divide the chunk");
+#ifndef SWB_XPF
+#define SWB_XPF 2
+#endif
+constexpr int XPF = SWB_XPF;   // rows of scores (and direction) loaded ahead
+static_assert(XC % XPF == 0, "the score prefetch distance must divide the chunk");
 #ifndef SWB_XSTAGES
-#define SWB_XSTAGES 3
+#define SWB_XSTAGES 2
 #endif
 constexpr int XSTAGES = SWB_XSTAGES;   // field steps in flight per backward warp
+#ifndef SWB_XFWD_MINB
+#define SWB_XFWD_MINB 1
+#endif
+#ifndef SWB_XBWD_MINB
+#define SWB_XBWD_MINB 1
+#endif
 
 // floats of one step of fields for one warp
 template <int NS, int R>
@@ -287,9 +297,9 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
     for (int f = 0; f < NE; ++f) dst[f] = ok ? ld_poll(ein + f * Lm + (i - 1)) : 0.f;
   };
   load_edge(0, eb);
-  float sb[PF][R], vb[PF][R];
+  float sb[XPF][R], vb[XPF][R];
 #pragma unroll
-  for (int u = 0; u < PF; ++u) {
+  for (int u = 0; u < XPF; ++u) {
     const int i = u - lane + 1;
     load_row<R>(ps, i, jl, i >= 1 && i <= L1, sb[u]);
     load_row<R>(pv, i, jl, HV && i >= 1 && i <= L1, vb[u]);
@@ -298,9 +308,9 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
   for (int kc = 0; kc < nch; ++kc) {
     if (kc + 1 < nch) load_edge(kc + 1, ebn);
 #pragma unroll 1
-    for (int u0 = 0; u0 < XC; u0 += PF)
+    for (int u0 = 0; u0 < XC; u0 += XPF)
 #pragma unroll
-      for (int u = 0; u < PF; ++u) {
+      for (int u = 0; u < XPF; ++u) {
         const int cu = u0 + u;
         const int t = kc * XC + cu;
         const int i = t - lane + 1;
@@ -324,7 +334,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
           float fb[NE];
 #pragma unroll
           for (int f = 0; f < NE; ++f) fb[f] = f < NS ? NEG : 0.f;
-          poll_fields<NE>(ev, ein + (i - 1), Lm, deadline, a.status, fb);
+poll_fields<NE>(ev, ein + (i - 1), Lm, deadline, a.status, fb);
         }
         if (lane == 0) {
           const bool take = act && ein;
@@ -348,7 +358,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
           vv[c] = HV ? vb[u][c] : 0.f;
         }
         {
-          const int ip = i + PF;
+          const int ip = i + XPF;
           load_row<R>(ps, ip, jl, ip >= 1 && ip <= L1, sb[u]);
           load_row<R>(pv, ip, jl, HV && ip >= 1 && ip <= L1, vb[u]);
         }
@@ -448,7 +458,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
 }
 
 template <int NS, int R, int MODE>
-__global__ void __launch_bounds__(128) xfwd_kernel(XArgs a) {
+__global__ void __launch_bounds__(128, SWB_XFWD_MINB) xfwd_kernel(XArgs a) {
   const int lane = threadIdx.x & 31;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
   const int ntasks = a.B * a.nb;
@@ -603,10 +613,10 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
     }
   };
   load_pb(nch - 1, pbc);
-  // HVP: raw scores and direction of the rows PF steps ahead
-  float sb[PF][R], vb[PF][R];
+  // HVP: raw scores and direction of the rows XPF steps ahead
+  float sb[XPF][R], vb[XPF][R];
 #pragma unroll
-  for (int u = 0; u < PF; ++u) {
+  for (int u = 0; u < XPF; ++u) {
     const int i = (nst - 1 - u) - lane + 1;
     load_row<R>(po, i, jl, HV && i >= 1 && i <= L1, sb[u]);
     load_row<R>(pv, i, jl, HV && i >= 1 && i <= L1, vb[u]);
@@ -627,9 +637,9 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   for (int kc = nch - 1; kc >= 0; --kc) {
     if (kc > 0) load_pb(kc - 1, pbn);
 #pragma unroll 1
-    for (int u0 = 0; u0 < XC; u0 += PF)
+    for (int u0 = 0; u0 < XC; u0 += XPF)
 #pragma unroll
-      for (int u = 0; u < PF; ++u) {
+      for (int u = 0; u < XPF; ++u) {
         const int cu = u0 + u;
         const int t = kc * XC + (XC - 1 - cu);
         const int tt = nst - 1 - t;
@@ -693,7 +703,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
 #pragma unroll
         for (int c = 0; c < R; ++c) { sc[c] = sb[u][c]; vv[c] = vb[u][c]; }
         if (HV) {
-          const int ip = i - PF;
+          const int ip = i - XPF;
           load_row<R>(po, ip, jl, ip >= 1 && ip <= L1, sb[u]);
           load_row<R>(pv, ip, jl, ip >= 1 && ip <= L1, vb[u]);
         }
@@ -814,7 +824,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
 }
 
 template <int NS, int R, int MODE>
-__global__ void __launch_bounds__(32) xbwd_kernel(XArgs a) {
+__global__ void __launch_bounds__(32, SWB_XBWD_MINB) xbwd_kernel(XArgs a) {
   extern __shared__ __align__(16) float xring[];
   const int lane = threadIdx.x & 31;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
