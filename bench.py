@@ -305,6 +305,66 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# second-order ops (not the contract line: a measurement and profiling case)
+# ---------------------------------------------------------------------------
+
+def second_order(args):
+    """The second-order ops at the training-step shapes: `--pairs` pairs
+    (default 256) of 512 x 512, scores <e_i, f_j> / sqrt(128) with N(0, 1)
+    embeddings.  Times the HVP, dP/dT and the map's full VJP (the HVP pass
+    with the parameter tangents) through the C ABI with buffers allocated
+    once, CUDA events on the launching stream, `--warmup` untimed and
+    `--steps` timed calls each; prints one JSON line."""
+    import torch
+
+    import orihime_b200  # noqa: F401
+    from orihime_b200 import _lib
+
+    lib = _lib.load()
+    B = args.pairs if args.pairs != NPAIRS else 256
+    N, d = 512, 128
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    e = torch.randn(B, N, d, generator=g, device="cuda")
+    f = torch.randn(B, N, d, generator=g, device="cuda")
+    s = (torch.bmm(e, f.transpose(1, 2)) / d ** 0.5).contiguous()
+    v = torch.randn(B, N, N, generator=g, device="cuda")
+    del e, f
+    out = torch.empty_like(s)
+    gt = torch.zeros(B, 4, device="cuda")
+    nbytes = int(lib.swb_sw_affine_aux_workspace_bytes(B, N, N))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    P = lambda t: t.data_ptr()  # noqa: E731
+    calls = {
+        "hvp": lambda: lib.swb_sw_affine_hvp(P(s), P(v), None, B, N, N, GO, GE, T, P(out), None,
+                                             P(ws), nbytes, st),
+        "grad_temp": lambda: lib.swb_sw_affine_param_jacobian(P(s), None, B, N, N, GO, GE, T, 2,
+                                                              P(out), P(ws), nbytes, st),
+        "marginals_backward": lambda: lib.swb_sw_affine_hvp(P(s), P(v), None, B, N, N, GO, GE, T,
+                                                            P(out), P(gt), P(ws), nbytes, st),
+    }
+    cells = B * N * N
+    res = {}
+    for name, fn in calls.items():
+        for _ in range(max(args.warmup, 1)):
+            if fn() != 0:
+                raise RuntimeError(f"{name} failed")
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / args.steps
+        res[name] = {"ms": round(ms, 3), "gcups": round(cells / ms / 1e6, 2)}
+    print(json.dumps({"second_order": res, "pairs": B, "shape": [N, N], "workspace_bytes": nbytes,
+                      "params": {"gap_open": GO, "gap_ext": GE, "temp": T}}))
+    return 0
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 
@@ -320,9 +380,13 @@ def main():
     ap.add_argument("--cols-per-lane", type=int, default=0, help="band columns per lane (2 or 4)")
     ap.add_argument("--quick", action="store_true",
                     help="timed steps only: no e2e, plain, CPU legs (profiling cases)")
+    ap.add_argument("--second-order", action="store_true",
+                    help="time the second-order ops at the training-step shapes instead")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.second_order:
+        return second_order(args)
 
     import torch
 
