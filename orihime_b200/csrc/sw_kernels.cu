@@ -329,34 +329,55 @@ __device__ __forceinline__ void two_sum(float a, float b, float& h, float& l) {
 // Adjoint fields of column c in one step's shared-memory entry `ent`, stored
 // column block by column block; inside a block each field group is one
 // vector per lane (lane-contiguous, so every warp access is conflict-free).
-// affine (11 floats): A = (wMM, wMI, wMD, wIM), B = (wII, wDM, wDD, bM0),
-// C = (bI0, bD0), s; linear (6 floats): A = (map factor, wA, wU, wL),
-// C = (b0, s).  s is the cell's scaled score.
+// affine (11 floats): A = (wMM, wMI, wMD, wIM), B = (wII, wDM, wDD, s), then
+// the beta-init terms C = (bM0, bI0) and D = bD0; linear (6 floats):
+// A = (map factor, wA, wU, wL), then s, then the beta-init term b0.  s is the
+// cell's scaled score.  The init terms are written only for steps where some
+// lane's init can be nonzero (fwd_cells returns that flag).
 template <int NS, int R>
-__device__ __forceinline__ void put_fields(float* ent, int lane, int c, float4 A, float4 B, float2 C,
-                                           float sc) {
+__device__ __forceinline__ void put_weights(float* ent, int lane, int c, float4 A, float4 B,
+                                            float sc) {
   float* col = ent + c * Shape<NS>::WF * 32;
   reinterpret_cast<float4*>(col)[lane] = A;
   if constexpr (NS == 3) {
-    reinterpret_cast<float4*>(col + 128)[lane] = B;
-    reinterpret_cast<float2*>(col + 256)[lane] = C;
-    col[320 + lane] = sc;
+    reinterpret_cast<float4*>(col + 128)[lane] = make_float4(B.x, B.y, B.z, sc);
   } else {
-    reinterpret_cast<float2*>(col + 128)[lane] = make_float2(C.x, sc);
+    col[128 + lane] = sc;
   }
 }
 template <int NS, int R>
-__device__ __forceinline__ void get_fields(const float* ent, int lane, int c, float4& A, float4& B,
-                                           float2& C, float& sc) {
+__device__ __forceinline__ void put_inits(float* ent, int lane, int c, float b0, float b1,
+                                          float b2) {
+  float* col = ent + c * Shape<NS>::WF * 32;
+  if constexpr (NS == 3) {
+    reinterpret_cast<float2*>(col + 256)[lane] = make_float2(b0, b1);
+    col[320 + lane] = b2;
+  } else {
+    col[160 + lane] = b0;
+  }
+}
+template <int NS, int R>
+__device__ __forceinline__ void get_weights(const float* ent, int lane, int c, float4& A, float4& B,
+                                            float& sc) {
   const float* col = ent + c * Shape<NS>::WF * 32;
   A = reinterpret_cast<const float4*>(col)[lane];
   if constexpr (NS == 3) {
     B = reinterpret_cast<const float4*>(col + 128)[lane];
-    C = reinterpret_cast<const float2*>(col + 256)[lane];
-    sc = col[320 + lane];
+    sc = B.w;
   } else {
-    C = reinterpret_cast<const float2*>(col + 128)[lane];
-    sc = C.y;
+    sc = col[128 + lane];
+  }
+}
+template <int NS, int R>
+__device__ __forceinline__ void get_inits(const float* ent, int lane, int c, float& b0, float& b1,
+                                          float& b2) {
+  const float* col = ent + c * Shape<NS>::WF * 32;
+  if constexpr (NS == 3) {
+    const float2 x = reinterpret_cast<const float2*>(col + 256)[lane];
+    b0 = x.x; b1 = x.y;
+    b2 = col[320 + lane];
+  } else {
+    b0 = col[160 + lane];
   }
 }
 
@@ -368,13 +389,14 @@ __device__ __forceinline__ void get_fields(const float* ent, int lane, int c, fl
 // boundary); rows past the pair's end compute values nothing reads.
 //
 // WT (adjoint recompute): also writes each cell's adjoint fields to the
-// shared-memory entry `went` (put_fields).  The
-// predecessor weights are the recurrence's own softmax terms divided by their
-// sum, so they add up to 1 per cell up to rounding and the adjoint conserves
+// shared-memory entry `went` (put_weights, put_inits).  The predecessor
+// weights are the recurrence's own softmax terms divided by their sum, so
+// they add up to 1 per cell up to rounding and the adjoint conserves
 // probability flow exactly; beta-init = exp2(min(x - S, 0)) for the first
-// `nlive` columns, 0 beyond.
+// `nlive` columns, 0 beyond.  Returns (warp-uniform) whether the inits were
+// written; when not, every one of them is 0.
 template <int NS, int R, bool WT = false>
-__device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R],
+__device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R],
                                           const float (&lfh)[NS], const float (&lfl)[NS],
                                           const float (&dgh0)[NS], const float (&dgl0)[NS],
                                           const float (&s)[R], float g0, float g1,
@@ -412,12 +434,8 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       fast2(rl, lg2(sd), Dh, Dl);
       if constexpr (WT) {
         const float vm = recip(sm), vi = recip(si), vd = recip(sd);
-        const bool lv = c < nlive;
-        const float bM = lv ? ex2(fminf((Mh - Sh) + (Ml - Sl), 0.f)) : 0.f;
-        const float bI = lv ? ex2(fminf((Ih - Sh) + (Il - Sl), 0.f)) : 0.f;
-        const float bD = lv ? ex2(fminf((Dh - Sh) + (Dl - Sl), 0.f)) : 0.f;
-        put_fields<NS, R>(went, lane, c, make_float4(tM * vm, tI * vm, tD * vm, ta * vi),
-                          make_float4(tb * vi, tc * vd, td * vd, bM), make_float2(bI, bD), s[c]);
+        put_weights<NS, R>(went, lane, c, make_float4(tM * vm, tI * vm, tD * vm, ta * vi),
+                           make_float4(tb * vi, tc * vd, td * vd, 0.f), s[c]);
       }
       dgh[0] = uMh; dgl[0] = uMl; dgh[1] = uIh; dgl[1] = uIl; dgh[2] = uDh; dgl[2] = uDl;
       lh[0] = Mh; ll[0] = Ml; lh[1] = Ih; ll[1] = Il; lh[2] = Dh; ll[2] = Dl;
@@ -436,15 +454,38 @@ __device__ __forceinline__ void fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       fast2(r, lg2(sm), Ah, Al);
       if constexpr (WT) {
         const float v = recip(sm);
-        const float bA = c < nlive ? ex2(fminf((Ah - Sh) + (Al - Sl), 0.f)) : 0.f;
-        put_fields<NS, R>(went, lane, c, make_float4((ta + ts) * v, ta * v, tu * v, tl * v),
-                          make_float4(0.f, 0.f, 0.f, 0.f), make_float2(bA, 0.f), s[c]);
+        put_weights<NS, R>(went, lane, c, make_float4((ta + ts) * v, ta * v, tu * v, tl * v),
+                           make_float4(0.f, 0.f, 0.f, 0.f), s[c]);
       }
       dgh[0] = uh; dgl[0] = ul;
       lh[0] = Ah; ll[0] = Al;
       ph[0][c] = Ah; pl[0][c] = Al;
     }
   }
+  if constexpr (WT) {
+    // beta-init exp2(min(x - S, 0)) of the first `nlive` columns.  The lo
+    // parts stay below ~2.1 (lo of M carries lg2 of a sum of at most four
+    // terms <= 1), so a hi part below S - 135 gives an exponent below -130
+    // and an init of exactly 0 (ex2.approx.ftz flushes it): when that holds
+    // for every lane the step's inits are not computed or stored.
+    bool near = false;
+#pragma unroll
+    for (int c = 0; c < R; ++c)
+#pragma unroll
+      for (int q = 0; q < NS; ++q) near |= (c < nlive) && (ph[q][c] - Sh > -135.f);
+    if (!__any_sync(FULL, near)) return false;
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      const bool lv = c < nlive;
+      float b[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) b[q] = lv ? ex2(fminf((ph[q][c] - Sh) + (pl[q][c] - Sl), 0.f)) : 0.f;
+      if constexpr (NS == 3) put_inits<NS, R>(went, lane, c, b[0], b[1], b[2]);
+      else put_inits<NS, R>(went, lane, c, b[0], 0.f, 0.f);
+    }
+    return true;
+  }
+  return false;
 }
 
 // Steps of a band, padded to whole checkpoint chunks (the padding steps find
@@ -799,6 +840,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
     // ---- restore the checkpoint and recompute the chunk's adjoint fields ----
     float ph[NS][R], pl[NS][R], lh[NS], ll[NS];
     ck_unpack<NS, R>(ckr, ph, pl, lh, ll);
+    unsigned initbits = 0;   // bit u: step u of the chunk wrote its beta-inits
 #pragma unroll 1
     for (int u0 = 0; u0 < C_STEPS; u0 += PF)
 #pragma unroll
@@ -832,8 +874,9 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
         const int ip = i + PF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
-      fwd_cells<NS, R, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, Sh, Sl, act ? ncols : 0,
-                             sm + (size_t)cu * EW * 32, lane);
+      if (fwd_cells<NS, R, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, Sh, Sl, act ? ncols : 0,
+                                 sm + (size_t)cu * EW * 32, lane))
+        initbits |= 1u << cu;
     }
     if (kc > 0) {  // prefetch the next chunk's inputs while the adjoint runs
       load_ck(kc - 1);
@@ -846,6 +889,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
 #pragma unroll 1
     for (int cu = 0; cu < C_STEPS; ++cu) {
       const int ent = C_STEPS - 1 - cu;        // entry of this step's row
+      const bool hasinit = (initbits >> ent) & 1u;   // else every beta-init is 0
       const int t = t0 + ent;
       const int i = t - lane + 1;
       const bool act = (i >= 1) && (i <= L1);
@@ -908,13 +952,14 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
         // a NEG predecessor is 0), so beta needs no mask
         if constexpr (NS == 3) {
           float4 f0, f1;
-          float2 f2;
           float sc;
-          get_fields<NS, R>(E, lane, c, f0, f1, f2, sc);
-          // f0 = (wMM, wMI, wMD, wIM), f1 = (wII, wDM, wDD, bM0), f2 = (bI0, bD0)
-          const float bM = f1.w + ac[0][c];
-          const float bI = f2.x + ac[1][c];
-          const float bD = f2.y + ac[2][c];
+          get_weights<NS, R>(E, lane, c, f0, f1, sc);
+          // f0 = (wMM, wMI, wMD, wIM), f1 = (wII, wDM, wDD, s)
+          float i0 = 0.f, i1 = 0.f, i2 = 0.f;
+          if (hasinit) get_inits<NS, R>(E, lane, c, i0, i1, i2);
+          const float bM = i0 + ac[0][c];
+          const float bI = i1 + ac[1][c];
+          const float bD = i2 + ac[2][c];
           pm[c] = bM;
           const float pIM = bI * f0.w, pII = bI * f1.x;
           const float pDM = bD * f1.y, pDD = bD * f1.z;
@@ -932,11 +977,12 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
           }
         } else {
           float4 f0, f1;
-          float2 f2;
           float sc;
-          get_fields<NS, R>(E, lane, c, f0, f1, f2, sc);
-          // f0 = (map factor, wA, wU, wL), f2.x = b0
-          const float b = f2.x + ac[0][c];
+          get_weights<NS, R>(E, lane, c, f0, f1, sc);
+          // f0 = (map factor, wA, wU, wL)
+          float i0 = 0.f, i1 = 0.f, i2 = 0.f;
+          if (hasinit) get_inits<NS, R>(E, lane, c, i0, i1, i2);
+          const float b = i0 + ac[0][c];
           const float pv_ = b * f0.x;
           pm[c] = pv_;
           const float pU = b * f0.z, pL = b * f0.w, pD = b * f0.y;
