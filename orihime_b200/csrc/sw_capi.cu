@@ -36,7 +36,7 @@ constexpr size_t kAlign = 256;
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 template <int NS, int R> constexpr int np() { return swb::Dims<NS, R>::NP; }
-template <int NS, int R> constexpr int ckf() { return swb::Dims<NS, R>::CKF; }
+template <int NS, int R> constexpr int ckrs() { return swb::Dims<NS, R>::CKRS; }
 template <int NS, int R> constexpr int ne() { return swb::Dims<NS, R>::NE; }
 
 bool valid_r(int r) { return r == 2 || r == 4; }
@@ -80,7 +80,7 @@ Layout layout_for(long long B, long long L1m, long long L2m) {
   const size_t slots = (size_t)B * nb;
   Layout l = layout_sizes(B, slots, slots * ne<NS, R>() * (size_t)L1m,
                           slots * np<NS, R>() * (size_t)(L1m + 1),
-                          slots * (size_t)nch * ckf<NS, R>() * 32);
+                          slots * (size_t)nch * ckrs<NS, R>());
   l.nb = nb;
   l.nchunks = nch;
   return l;
@@ -500,7 +500,7 @@ int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const lon
   const int R = cols_per_lane ? cols_per_lane : kDefaultR;
   if ((family != 1 && family != 3) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
     return SWB_ERR_ARG;
-  const int NE = 2 * family, NP = (family == 3) ? 5 : 2, CKF = 2 * family * R + 2 * family;
+  const int NE = 2 * family, NP = (family == 3) ? 5 : 2, CKRS = (2 * family * R + 2 * family) * 32 + 4;
   // validate the packing: row pitch round4(L2), offsets multiples of 4 floats
   long long ntasks = 0;
   for (int b = 0; b < B; ++b) {
@@ -561,7 +561,7 @@ int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const lon
       for (long long j = 0; j < nb; ++j) { tk[2 * t] = b; tk[2 * t + 1] = (int)j; ++t; }
     }
     slots += nb;
-    ck += (size_t)nb * chunks_for(L1) * CKF * 32;
+    ck += (size_t)nb * chunks_for(L1) * CKRS;
     ed += (size_t)nb * NE * L1;
     bp += (size_t)nb * NP * (L1 + 1);
   }

@@ -136,7 +136,7 @@ struct Place {
 
 template <int NS, int R>
 __device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_band) {
-  constexpr int NE = 2 * NS, NP = (NS == 3) ? 5 : 2, CKF = 2 * NS * R + 2 * NS;
+  constexpr int NE = 2 * NS, NP = (NS == 3) ? 5 : 2, CKRS = (2 * NS * R + 2 * NS) * 32 + 4;
   Place w;
   Pair& r = w.pr;
   if (a.layout == 0) {
@@ -148,7 +148,7 @@ __device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_
     w.band = reverse_band ? a.nb - 1 - j : j;
     w.slot0 = (size_t)p * a.nb;
     w.Lm = a.Lmax1;
-    w.ckb = (size_t)a.nchunks * CKF * 32;
+    w.ckb = (size_t)a.nchunks * CKRS;
     w.edb = (size_t)NE * a.Lmax1;
     w.bpb = (size_t)NP * (a.Lmax1 + 1);
     w.ck0 = w.slot0 * w.ckb;
@@ -178,7 +178,7 @@ __device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_
     r.ld = (r.L2 + 3) & ~3;
     w.Lm = r.L1;
     const int nch = (r.L1 + 31 + C_STEPS - 1) / C_STEPS;
-    w.ckb = (size_t)nch * CKF * 32;
+    w.ckb = (size_t)nch * CKRS;
     w.edb = (size_t)NE * r.L1;
     w.bpb = (size_t)NP * (r.L1 + 1);
     w.ck0 = (size_t)q[PW_CK0];
@@ -247,6 +247,7 @@ template <int NS, int R> struct Dims {
   static constexpr int NE = 2 * NS;
   static constexpr int NP = Shape<NS>::NP;
   static constexpr int CKF = 2 * NS * R + 2 * NS;   // checkpoint floats per lane (even)
+  static constexpr int CKRS = CKF * 32 + 4;         // chunk record floats: checkpoint, chunk max, pad
   static constexpr int CK4 = CKF / 4;               // ... stored as CK4 float4
   static constexpr int CK2 = (CKF % 4) / 2;         // ... and CK2 (0 or 1) float2
   static constexpr int WF = Shape<NS>::WF;         // adjoint fields per cell
@@ -268,7 +269,10 @@ __device__ __forceinline__ void ck_pack(const float (&ph)[NS][R], const float (&
   }
 }
 
-// Checkpoint chunk layout: CK4 groups of [lane][4] floats, then [lane][2].
+// Checkpoint record of a chunk: CK4 groups of [lane][4] floats, then [lane][2]
+// (ck_store / ck_load), then one float: the largest hi alpha of the band's
+// live cells in the chunk (written by the forward at the chunk's end), and
+// 3 floats of padding that keep records 16-byte aligned.
 template <int NS, int R>
 __device__ __forceinline__ void ck_store(float* chunk, int lane, const float (&v)[Dims<NS, R>::CKF]) {
   using D = Dims<NS, R>;
@@ -552,8 +556,9 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
     {  // checkpoint: state before step kc*C
       float v[D::CKF];
       ck_pack<NS, R>(ph, pl, lh, ll, v);
-      ck_store<NS, R>(ck + (size_t)kc * D::CKF * 32, lane, v);
+      ck_store<NS, R>(ck + (size_t)kc * D::CKRS, lane, v);
     }
+    float cmx = NEG;   // largest hi alpha of the lane's live cells in this chunk
     if (kc + 1 < nch) load_edge(kc + 1, ebn);
 #pragma unroll 1
     for (int u0 = 0; u0 < C_STEPS; u0 += PF)
@@ -620,6 +625,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
           if (jl + c < L2)
 #pragma unroll
             for (int q = 0; q < NS; ++q) mx = fmaxf(mx, ph[q][c]);
+        cmx = fmaxf(cmx, mx);
         if (mx > ref + 8.f) {
           float f = ex2(ref - mx);
           acc.s *= f;
@@ -644,6 +650,9 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
     }
 #pragma unroll
     for (int f = 0; f < NE; ++f) eb[f] = ebn[f];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cmx = fmaxf(cmx, __shfl_xor_sync(FULL, cmx, o));
+    if (lane == 0) ck[(size_t)kc * D::CKRS + D::CKF * 32] = cmx;
   }
   // warp-combine (ref, sum) pairs
   float s_ = acc.s;
@@ -766,7 +775,7 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
 template <int NS, int R>
 __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uint64_t deadline) {
   using D = Dims<NS, R>;
-  constexpr int NP = D::NP, EW = D::EW, CKF = D::CKF, NE = D::NE;
+  constexpr int NP = D::NP, EW = D::EW, CKF = D::CKF, CKRS = D::CKRS, NE = D::NE;
   const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
   const int band = w.band;
@@ -790,10 +799,15 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
 
   // ---- chunk-ahead prefetch state ----
   float ckr[CKF];           // checkpoint of the next chunk to recompute
+  float ckm;                // ... and the largest hi alpha of the band's live cells in it
   float ebr[NE];            // lane u < C: left-band edge pair of lane 0's row at recompute step u
   float pbc[NP], pbn[NP];   // lane u < C: right-band pushes lane 31 needs at adjoint step u
   float sb[PF][R];          // per-lane scores of the first PF recompute steps
-  auto load_ck = [&](int kc) { ck_load<NS, R>(ck + (size_t)kc * CKF * 32, lane, ckr); };
+  auto load_ck = [&](int kc) {
+    const float* rec = ck + (size_t)kc * CKRS;
+    ck_load<NS, R>(rec, lane, ckr);
+    ckm = rec[CKF * 32];
+  };
   auto load_eb = [&](int kc) {
     const int i = kc * C_STEPS + lane + 1;
     const bool ok = ein && lane < C_STEPS && i <= L1;
@@ -836,6 +850,75 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
 
   for (int kc = nch - 1; kc >= 0; --kc) {
     const int t0 = kc * C_STEPS;
+    // ---- quiet chunk.  Flows only split or leave (a cell pushes beta * w
+    // with the weights summing to at most 1), so every value inside a chunk
+    // is at most the sum of the flows entering it plus its beta-inits.  When
+    // every entering push is below kFlowTiny and every init is 0 (all hi
+    // alphas of the chunk 135 below S, as in fwd_cells), nothing in the chunk
+    // exceeds ~1e-27: it writes zeros (map rows, pushes to the left band)
+    // instead of restoring and recomputing. ----
+    {
+      // the right band's pushes for this chunk, resolved now so that the
+      // decision does not depend on timing (results are deterministic)
+      {
+        bool miss = false;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) miss |= is_sentinel(pbc[q]);
+        if (__any_sync(FULL, miss) && miss) {
+          const int ir = kc * C_STEPS + C_STEPS - 1 - lane - 30;   // as in load_pb
+#pragma unroll
+          for (int q = 0; q < NP; ++q)
+            if (is_sentinel(pbc[q]))
+              pbc[q] = poll_value(pin + q * (Lm + 1) + ir, ld_poll(pin + q * (Lm + 1) + ir), deadline,
+                                  a.status, 0.f);
+        }
+      }
+      float inmax = 0.f;
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        inmax = fmaxf(inmax, hold[q]);
+#pragma unroll
+        for (int c = 0; c < R; ++c) inmax = fmaxf(inmax, ac[q][c]);
+      }
+#pragma unroll
+      for (int q = 0; q < NP; ++q) inmax = fmaxf(fmaxf(inmax, outp[q]), pbc[q]);
+      const bool ok = inmax < kFlowTiny && ckm - Sh < -135.f;
+      if (__all_sync(FULL, ok)) {
+        float z[R];
+#pragma unroll
+        for (int c = 0; c < R; ++c) z[c] = 0.f;
+        for (int cu = 0; cu < C_STEPS; ++cu) {
+          const int i = t0 + (C_STEPS - 1 - cu) - lane + 1;
+          if (i >= 1 && i <= L1) {
+            store_row<R>(pr, i, jl, z);
+            if (lane == 0 && pout) {
+#pragma unroll
+              for (int f = 0; f < NP; ++f) {
+                const bool left = (NS == 3) ? (f < 2) : (f < 1);
+                pout[f * (Lm + 1) + (left ? i : i - 1)] = 0.f;
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          hold[q] = 0.f;
+#pragma unroll
+          for (int c = 0; c < R; ++c) ac[q][c] = 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < NP; ++q) outp[q] = 0.f;
+        if (kc > 0) {
+          load_ck(kc - 1);
+          load_eb(kc - 1);
+          load_sb(kc - 1);
+          load_pb(kc - 1, pbn);
+        }
+#pragma unroll
+        for (int q = 0; q < NP; ++q) pbc[q] = pbn[q];
+        continue;
+      }
+    }
     float cA = 0.f, cB = 0.f, cS = 0.f;   // this chunk's plain sums
     // ---- restore the checkpoint and recompute the chunk's adjoint fields ----
     float ph[NS][R], pl[NS][R], lh[NS], ll[NS];

@@ -49,6 +49,9 @@
 namespace swb {
 
 constexpr float NEG = -1e30f;           // "no path" in the scaled domain
+// Adjoint flows below this (2^-100) entering a chunk count as none: a chunk
+// whose inflow and beta-inits are all below it holds values below ~1e-27.
+constexpr float kFlowTiny = 7.8886090522101181e-31f;
 constexpr unsigned FULL = 0xffffffffu;
 #ifndef SWB_C_STEPS
 #define SWB_C_STEPS 4
