@@ -853,10 +853,10 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
     // ---- quiet chunk.  Flows only split or leave (a cell pushes beta * w
     // with the weights summing to at most 1), so every value inside a chunk
     // is at most the sum of the flows entering it plus its beta-inits.  When
-    // every entering push is below kFlowTiny and every init is 0 (all hi
-    // alphas of the chunk 135 below S, as in fwd_cells), nothing in the chunk
-    // exceeds ~1e-27: it writes zeros (map rows, pushes to the left band)
-    // instead of restoring and recomputing. ----
+    // every entering push is below kFlowTiny and every init is too (all hi
+    // alphas of the chunk kInitQuiet below S), nothing in the chunk exceeds
+    // ~2e-15: it writes zeros (map rows, pushes to the left band) instead of
+    // restoring and recomputing. ----
     {
       // the right band's pushes for this chunk, resolved now so that the
       // decision does not depend on timing (results are deterministic)
@@ -882,7 +882,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
       }
 #pragma unroll
       for (int q = 0; q < NP; ++q) inmax = fmaxf(fmaxf(inmax, outp[q]), pbc[q]);
-      const bool ok = inmax < kFlowTiny && ckm - Sh < -135.f;
+      const bool ok = inmax < kFlowTiny && ckm - Sh < kInitQuiet;
       if (__all_sync(FULL, ok)) {
         float z[R];
 #pragma unroll

@@ -49,9 +49,14 @@
 namespace swb {
 
 constexpr float NEG = -1e30f;           // "no path" in the scaled domain
-// Adjoint flows below this (2^-100) entering a chunk count as none: a chunk
-// whose inflow and beta-inits are all below it holds values below ~1e-27.
-constexpr float kFlowTiny = 7.8886090522101181e-31f;
+// Adjoint flows below this (2^-60) entering a chunk count as none.  A chunk
+// whose inflow (at most ~660 values) and beta-inits (512 cells x 3 states) are
+// all below it holds less than ~2e-15 of probability in total; summed over
+// every such chunk of a pair, the dropped mass stays below ~1e-10.
+constexpr float kFlowTiny = 8.6736173798840355e-19f;
+// A chunk's beta-inits are all below kFlowTiny when every hi alpha in it lies
+// this far below S (scaled log2 units; 3 of margin for the lo parts).
+constexpr float kInitQuiet = -63.f;
 constexpr unsigned FULL = 0xffffffffu;
 #ifndef SWB_C_STEPS
 #define SWB_C_STEPS 4
