@@ -38,7 +38,7 @@ MUFU_PER_CELL = 21      # algorithmic MUFU ops per cell, forward 11 + adjoint 10
 MUFU_PER_CELL_BWD = 10  # adjoint kernel alone
 BYTES_PER_CELL = 8      # compulsory HBM bytes per cell (score read + map write)
 E2E_PARTS = 8           # pair groups of the end-to-end pipeline
-BWD_DRAM_BYTES_PER_CELL = 17.91  # measured adjoint DRAM traffic: scores + checkpoints + map
+BWD_DRAM_BYTES_PER_CELL = 18.21  # measured adjoint DRAM traffic: scores + checkpoints + map
 
 
 def workload_lengths(seed: int, n: int = NPAIRS) -> np.ndarray:
@@ -505,8 +505,8 @@ def main():
             # DRAM bytes of one adjoint launch: ncu's dram__bytes_read + write per
             # cell on a 256-pair capture of this kernel, times this launch's cells
             roof["traffic"] = BWD_DRAM_BYTES_PER_CELL * cells
-            roof["traffic_source"] = ("ncu capture of bwd_kernel<3,4,1> on 1024 pairs, "
-                                      f"{BWD_DRAM_BYTES_PER_CELL} B/cell, scaled by cells")
+            roof["traffic_source"] = ("ncu capture (1 pass) of bwd_kernel<3,4,1> on this 4096-pair "
+                                      f"batch: {BWD_DRAM_BYTES_PER_CELL} B/cell")
         cpu = None if args.no_cpu_baseline else cpu_baseline(lengths)
         clocks = clk.summary()
         line = {"metric": METRIC, "value": gcups_all, "unit": "GCUPS", "n_gpus": world,
