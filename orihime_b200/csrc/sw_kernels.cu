@@ -70,28 +70,29 @@ struct KSum {
 #ifndef SWB_POLL_SLEEP
 #define SWB_POLL_SLEEP 128
 #endif
-// Bounded wait until none of v[0..N) is the sentinel, v[f] read from
+// Bounded wait until none of x.v[0..N) is the sentinel, x.v[f] read from
 // base[f * stride].  Every round re-reads all missing fields together, so their
-// load latencies overlap.  On timeout it records the error and substitutes
-// fb[f] for the fields still missing.
-template <int N>
-__device__ __noinline__ void poll_fields(float (&v)[N], const float* base, size_t stride,
-                                         uint64_t deadline, unsigned* status,
-                                         const float (&fb)[N]) {
+// load latencies overlap.  The fields travel by value (the caller's values
+// need no memory address).  On timeout it records the error and substitutes
+// NEG for the missing fields f < NSV, 0 for the others.
+template <int N> struct FieldVec { float v[N]; };
+template <int N, int NSV>
+__device__ __noinline__ FieldVec<N> poll_fields_v(FieldVec<N> x, const float* base, size_t stride,
+                                                  uint64_t deadline, unsigned* status) {
   while (true) {
     bool miss = false;
 #pragma unroll
     for (int f = 0; f < N; ++f)
-      if (is_sentinel(v[f])) v[f] = ld_poll(base + f * stride);
+      if (is_sentinel(x.v[f])) x.v[f] = ld_poll(base + f * stride);
 #pragma unroll
-    for (int f = 0; f < N; ++f) miss |= is_sentinel(v[f]);
-    if (!miss) return;
+    for (int f = 0; f < N; ++f) miss |= is_sentinel(x.v[f]);
+    if (!miss) return x;
     if (gtimer() > deadline) {
       atomicOr(status, ERR_WAIT_TIMEOUT);
 #pragma unroll
       for (int f = 0; f < N; ++f)
-        if (is_sentinel(v[f])) v[f] = fb[f];
-      return;
+        if (is_sentinel(x.v[f])) x.v[f] = f < NSV ? NEG : 0.f;
+      return x;
     }
     __nanosleep(SWB_POLL_SLEEP);
   }
@@ -588,10 +589,12 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
 #pragma unroll
           for (int f = 0; f < NE; ++f) ev[f] = (f < NS) ? v : 0.f;
         } else if (miss) {
-          float fb[NE];
+          FieldVec<NE> x;
 #pragma unroll
-          for (int f = 0; f < NE; ++f) fb[f] = f < NS ? NEG : 0.f;
-          poll_fields<NE>(ev, ein + (i - 1), Lm, deadline, a.status, fb);
+          for (int f = 0; f < NE; ++f) x.v[f] = ev[f];
+          x = poll_fields_v<NE, NS>(x, ein + (i - 1), Lm, deadline, a.status);
+#pragma unroll
+          for (int f = 0; f < NE; ++f) ev[f] = x.v[f];
         }
       }
       if (lane == 0) {

@@ -331,10 +331,12 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
         for (int f = 0; f < NE; ++f) miss |= is_sentinel(ev[f]);
         miss = (lane == 0) && ein && act && miss;
         if (__any_sync(FULL, miss) && miss) {
-          float fb[NE];
+          FieldVec<NE> x;
 #pragma unroll
-          for (int f = 0; f < NE; ++f) fb[f] = f < NS ? NEG : 0.f;
-poll_fields<NE>(ev, ein + (i - 1), Lm, deadline, a.status, fb);
+          for (int f = 0; f < NE; ++f) x.v[f] = ev[f];
+          x = poll_fields_v<NE, NS>(x, ein + (i - 1), Lm, deadline, a.status);
+#pragma unroll
+          for (int f = 0; f < NE; ++f) ev[f] = x.v[f];
         }
         if (lane == 0) {
           const bool take = act && ein;
