@@ -293,7 +293,7 @@ int xpick_r(long long B, long long L2m) {
 
 struct XLayout {
   int R, nb, nsteps;
-  size_t off_pair_done, off_part, off_gpart, off_sent, off_edge, off_bpush, off_fld;
+  size_t off_pair_done, off_part, off_gpart, off_cmax, off_sent, off_edge, off_bpush, off_fld;
   size_t sent_bytes, total;
 };
 
@@ -309,6 +309,7 @@ XLayout xlayout(long long B, long long L1m, long long L2m) {
   l.off_pair_done = o; o = align_up(o + sizeof(unsigned) * (size_t)B);
   l.off_part = o;      o = align_up(o + sizeof(float) * 4 * slots);
   l.off_gpart = o;     o = align_up(o + sizeof(float) * 4 * slots);
+  l.off_cmax = o;      o = align_up(o + sizeof(float) * slots * (size_t)(l.nsteps / swb::XC));
   l.off_sent = o;
   l.off_edge = o;      o = align_up(o + sizeof(float) * slots * swb::XShape<NS>::NE * (size_t)L1m);
   l.off_bpush = o;
@@ -385,6 +386,7 @@ int launch_xband(const float* scores, const float* v, const int* lengths, int B,
   a.pair_done = reinterpret_cast<unsigned*>(w + l.off_pair_done);
   a.part = reinterpret_cast<float*>(w + l.off_part);
   a.gpart = reinterpret_cast<float*>(w + l.off_gpart);
+  a.cmax = reinterpret_cast<float*>(w + l.off_cmax);
   a.edge = reinterpret_cast<float*>(w + l.off_edge);
   a.bpush = reinterpret_cast<float*>(w + l.off_bpush);
   a.fld = reinterpret_cast<float*>(w + l.off_fld);

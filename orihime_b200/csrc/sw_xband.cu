@@ -88,6 +88,7 @@ struct XArgs {
   float* edge;             // per band slot: NE * L1m floats (sentinel-filled)
   float* bpush;            // per band slot: 2 * NP * (L1m + 1) floats (sentinel-filled)
   float* part;             // per band slot: ref, sum, U-sum, log-sum
+  float* cmax;             // per band slot: nsteps / XC floats, largest hi alpha of each chunk
   float* gpart;            // per band slot: HVP parameter-tangent partials
   unsigned* counters;      // [0] forward tasks, [1] backward tasks
   unsigned* pair_done;     // per pair: backward bands finished
@@ -305,8 +306,10 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
     load_row<R>(pv, i, jl, HV && i >= 1 && i <= L1, vb[u]);
   }
 
+  float* cm = a.cmax + slot * (size_t)(a.nsteps / XC);
   for (int kc = 0; kc < nch; ++kc) {
     if (kc + 1 < nch) load_edge(kc + 1, ebn);
+    float cmx = NEG;   // largest hi alpha of the lane's live cells in this chunk
 #pragma unroll 1
     for (int u0 = 0; u0 < XC; u0 += XPF)
 #pragma unroll
@@ -412,6 +415,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
             if (jl + c < L2)
 #pragma unroll
               for (int q = 0; q < NS; ++q) mx = fmaxf(mx, ph[q][c]);
+          cmx = fmaxf(cmx, mx);
           if (mx > ref + 8.f) {
             const float d = ref - mx, f = ex2(d);
             sx = f * fmaf(d, acc.s, sx);
@@ -447,6 +451,9 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
       }
 #pragma unroll
     for (int f = 0; f < NE; ++f) eb[f] = ebn[f];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cmx = fmaxf(cmx, __shfl_xor_sync(FULL, cmx, o));
+    if (lane == 0) cm[kc] = cmx;
   }
   // warp-combine the lanes' tuples (fixed shuffle tree: deterministic)
   float s_ = acc.s;
@@ -590,8 +597,8 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   const int nst = nch * XC;   // steps, padded to whole chunks (padding steps find no row)
 
   // field ring: reverse step tt (forward step nst - 1 - tt) in stage tt % XSTAGES
-  auto issue = [&](int tt) {
-    if (tt < nst) {
+  auto issue = [&](int tt, bool copy) {
+    if (copy && tt < nst) {
       const float* src = F + (size_t)(nst - 1 - tt) * XSTEP;
       float* dst = ring + (size_t)(tt % XSTAGES) * XSTEP;
 #pragma unroll
@@ -600,7 +607,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
     cp_async_commit();
   };
 #pragma unroll
-  for (int q = 0; q < XSTAGES - 1; ++q) issue(q);
+  for (int q = 0; q < XSTAGES - 1; ++q) issue(q, true);
 
   // right-band pushes: lane u < XC holds those lane 31 needs at step u of a chunk
   float pbc[NQ], pbn[NQ];
@@ -636,8 +643,80 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   for (int q = 0; q < NQ; ++q) outp[q] = 0.f;
   KSum kA, kB, kC;
 
+  const float* cm = a.cmax + slot * (size_t)(a.nsteps / XC);
+  float ckm = cm[nch - 1];   // the forward's largest hi alpha of the chunk about to run
   for (int kc = nch - 1; kc >= 0; --kc) {
     if (kc > 0) load_pb(kc - 1, pbn);
+    const float ckm_next = kc > 0 ? cm[kc - 1] : NEG;
+    // ---- quiet chunk: as in the first-order adjoint, every value inside a
+    // chunk is bounded by the summed inflow (values and tangents, which a
+    // cell's weights and weight tangents scale by bounded factors) plus its
+    // inits.  With every entering push below kFlowTiny in magnitude and
+    // every hi alpha kInitQuiet below S, the chunk computes nothing (its
+    // output is already 0), pushes zeros to the left band and skips the
+    // field copies of its later steps. ----
+    {
+      bool miss = false;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) miss |= is_sentinel(pbc[q]);
+      if (__any_sync(FULL, miss) && miss) {
+        const int ir = kc * XC + XC - 1 - lane - 30;   // as in load_pb
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+          if (is_sentinel(pbc[q]))
+            pbc[q] = poll_value(pin + q * (Lm + 1) + ir, ld_poll(pin + q * (Lm + 1) + ir), deadline,
+                                a.status, 0.f);
+      }
+    }
+    float inmax = 0.f;
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      inmax = fmaxf(inmax, fmaxf(fabsf(hold[q]), fabsf(holdt[q])));
+#pragma unroll
+      for (int c = 0; c < R; ++c) inmax = fmaxf(inmax, fmaxf(fabsf(ac[q][c]), fabsf(at[q][c])));
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) inmax = fmaxf(inmax, fmaxf(fabsf(outp[q]), fabsf(pbc[q])));
+    if (__all_sync(FULL, inmax < kFlowTiny && ckm - Sh < kInitQuiet)) {
+      // no copy may still be landing in a stage this chunk refills
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      for (int cu = 0; cu < XC; ++cu) {
+        const int t = kc * XC + (XC - 1 - cu);
+        const int tt = nst - 1 - t;
+        // keep one commit group per step; copy only steps of later chunks
+        issue(tt + XSTAGES - 1, nst - 1 - (tt + XSTAGES - 1) < kc * XC);
+        const int i = t - lane + 1;
+        if (lane == 0 && pout && i >= 1 && i <= L1) {
+#pragma unroll
+          for (int f = 0; f < NQ; ++f) {
+            const int fc = f % NP;
+            const bool left = (NS == 3) ? (fc < 2) : (fc < 1);
+            pout[f * (Lm + 1) + (left ? i : i - 1)] = 0.f;
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        hold[q] = 0.f;
+        holdt[q] = 0.f;
+#pragma unroll
+        for (int c = 0; c < R; ++c) { ac[q][c] = 0.f; at[q][c] = 0.f; }
+      }
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) outp[q] = 0.f;
+      if (HV && kc > 0) {   // the score ring for the next chunk's first steps
+#pragma unroll
+        for (int u = 0; u < XPF; ++u) {
+          const int i = (kc - 1) * XC + (XC - 1 - u) - lane + 1;
+          load_row<R>(po, i, jl, i >= 1 && i <= L1, sb[u]);
+          load_row<R>(pv, i, jl, i >= 1 && i <= L1, vb[u]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) pbc[q] = pbn[q];
+      ckm = ckm_next;
+      continue;
+    }
 #pragma unroll 1
     for (int u0 = 0; u0 < XC; u0 += XPF)
 #pragma unroll
@@ -647,7 +726,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
         const int tt = nst - 1 - t;
         const int i = t - lane + 1;
         const bool act = (i >= 1) && (i <= L1);
-        issue(tt + XSTAGES - 1);
+        issue(tt + XSTAGES - 1, true);
         cp_async_wait<XSTAGES - 1>();
         const float* E = ring + (size_t)(tt % XSTAGES) * XSTEP + lane * 4;
         float r[NQ], pw[NQ];
@@ -812,6 +891,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
       }
 #pragma unroll
     for (int q = 0; q < NQ; ++q) pbc[q] = pbn[q];
+    ckm = ckm_next;
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncwarp();

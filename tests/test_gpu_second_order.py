@@ -220,3 +220,33 @@ def test_pair_groups_match_single_call(monkeypatch):
     got_p = _ops.run_param_jacobian("sw", s, ln, (*LIN, 0.6), 1)
     assert torch.equal(got, want) and torch.equal(got_gt, want_gt) and torch.equal(got_p, want_p)
     assert float(want[2].abs().max()) == 0.0 and float(want_gt[2].abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("fam", ["affine", "linear"])
+def test_long_pair_quiet_chunks(fam):
+    """A long pair where most backward chunks carry negligible flow (they push
+    zeros instead of recomputing, dropping values below ~1e-15): the HVP and
+    dP/dT stay within the fp64 bounds, and two runs agree bit for bit."""
+    from orihime_b200 import _ops
+
+    s = _scores(1, 900, 700, 21, scale=3.0).cuda()
+    v = _scores(1, 900, 700, 22, scale=1.0).cuda()
+    sn, vn = s.cpu().numpy(), v.cpu().numpy()
+    T = 0.5
+    if fam == "affine":
+        got = _ops.run_hvp("sw_affine", s, v, None, (*AFF, T))[0]
+        again = _ops.run_hvp("sw_affine", s, v, None, (*AFF, T))[0]
+        _check("hvp", got.cpu().numpy(), O.affine_hvp(sn, vn, None, *AFF, T),
+               O.affine_hvp(sn, vn, None, *AFF, T, dtype=np.float64))
+        pt = _ops.run_param_jacobian("sw_affine", s, None, (*AFF, T), 2)
+        _check("dP/dT", pt.cpu().numpy(), O.affine_param_grad(sn, None, *AFF, T, 2),
+               O.affine_param_grad(sn, None, *AFF, T, 2, dtype=np.float64))
+    else:
+        got = _ops.run_hvp("sw", s, v, None, (*LIN, T))[0]
+        again = _ops.run_hvp("sw", s, v, None, (*LIN, T))[0]
+        _check("hvp", got.cpu().numpy(), O.linear_hvp(sn, vn, None, *LIN, T),
+               O.linear_hvp(sn, vn, None, *LIN, T, dtype=np.float64))
+        pt = _ops.run_param_jacobian("sw", s, None, (*LIN, T), 1)
+        _check("dP/dT", pt.cpu().numpy(), O.linear_param_grad(sn, None, *LIN, T, 1),
+               O.linear_param_grad(sn, None, *LIN, T, 1, dtype=np.float64))
+    assert torch.equal(got, again)
