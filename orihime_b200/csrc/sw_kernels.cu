@@ -107,7 +107,7 @@ __device__ __noinline__ float poll_value(const float* p, float v, uint64_t deadl
       atomicOr(status, ERR_WAIT_TIMEOUT);
       return fallback;
     }
-    __nanosleep(128);
+    __nanosleep(SWB_POLL_SLEEP);
     v = ld_poll(p);
   }
   return v;
