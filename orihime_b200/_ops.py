@@ -360,13 +360,11 @@ def _affine_param(which):
     return op
 
 
-def sw_affine_marginals_backward(scores, grad_marginals, gap_open, gap_ext, temp, lengths):
-    """orihime::sw_affine_marginals_backward -> (grad_scores, d/dgo [1], d/dge [1], d/dT [1])
-    (src/sw_affine/torch_cuda.cpp:854 -> soft_sw_affine_backward_full_cuda :681-811).
-
-    One tangent pass along the cotangent G: grad_scores = H.G (the Hessian is
-    symmetric) and sum(G * dP/dtheta) = d/dG (dS/dtheta), the tangents of the
-    parameter gradients, summed over the batch."""
+def marginals_backward_per_pair(fam, scores, grad_marginals, params, lengths):
+    """Validated map VJP with per-pair parameter tangents: (grad_scores,
+    gt[B][4]).  gt[b] holds the tangents along G of pair b's parameter
+    gradients (affine: go, ge, T, S; linear: gap, T, 0, S); the
+    marginals_backward ops sum them over the batch."""
     check_input_cuda(scores, "scores")
     if scores.dim() != 3:
         raise RuntimeError("scores must be 3D (B, L1, L2)")
@@ -378,8 +376,19 @@ def sw_affine_marginals_backward(scores, grad_marginals, gap_open, gap_ext, temp
         raise RuntimeError(f"grad_alignment must be on same device as scores, got "
                            f"{grad_marginals.device} vs {scores.device}")
     g = grad_marginals.contiguous().to(torch.float32)
-    ln = _prep(scores, lengths, "sw_affine")
-    out, gt = run_hvp("sw_affine", scores, g, ln, (gap_open, gap_ext, temp), want_grads=True)
+    ln = _prep(scores, lengths, fam)
+    return run_hvp(fam, scores, g, ln, params, want_grads=True)
+
+
+def sw_affine_marginals_backward(scores, grad_marginals, gap_open, gap_ext, temp, lengths):
+    """orihime::sw_affine_marginals_backward -> (grad_scores, d/dgo [1], d/dge [1], d/dT [1])
+    (src/sw_affine/torch_cuda.cpp:854 -> soft_sw_affine_backward_full_cuda :681-811).
+
+    One tangent pass along the cotangent G: grad_scores = H.G (the Hessian is
+    symmetric) and sum(G * dP/dtheta) = d/dG (dS/dtheta), the tangents of the
+    parameter gradients, summed over the batch."""
+    out, gt = marginals_backward_per_pair("sw_affine", scores, grad_marginals,
+                                          (gap_open, gap_ext, temp), lengths)
     tot = gt[:, :3].sum(0)
     return out, tot[0:1].clone(), tot[1:2].clone(), tot[2:3].clone()
 
@@ -403,19 +412,7 @@ def _linear_param(which):
 def sw_marginals_backward(scores, grad_marginals, gap, temp, lengths):
     """orihime::sw_marginals_backward -> (grad_scores, d/dgap [1], d/dT [1])
     (src/sw/torch_cuda.cpp:755 -> soft_sw_backward_full_cuda :612)."""
-    check_input_cuda(scores, "scores")
-    if scores.dim() != 3:
-        raise RuntimeError("scores must be 3D (B, L1, L2)")
-    if grad_marginals.shape != scores.shape:
-        raise RuntimeError("grad_alignment must have same shape as scores")
-    if not grad_marginals.is_cuda:
-        raise RuntimeError("grad_alignment must be a CUDA tensor")
-    if grad_marginals.device != scores.device:
-        raise RuntimeError(f"grad_alignment must be on same device as scores, got "
-                           f"{grad_marginals.device} vs {scores.device}")
-    g = grad_marginals.contiguous().to(torch.float32)
-    ln = _prep(scores, lengths, "sw")
-    out, gt = run_hvp("sw", scores, g, ln, (gap, temp), want_grads=True)
+    out, gt = marginals_backward_per_pair("sw", scores, grad_marginals, (gap, temp), lengths)
     tot = gt[:, :2].sum(0)
     return out, tot[0:1].clone(), tot[1:2].clone()
 
@@ -520,3 +517,10 @@ for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True
                         ("sw_affine_forward", "sw_affine", False),
                         ("sw_affine_forward_t", "sw_affine", True)):
     _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
+
+
+# Meta shapes, FP32 autocast and vmap rules for the ops defined here (when the
+# reference extension defined them, its own Python package registers these).
+from . import _registrations  # noqa: E402
+
+_registrations.register(DEFINED_HERE)
