@@ -125,6 +125,22 @@ int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, in
                    const swb_options* opt);
 
 /*
+ * Value only: S per pair, without the marginal map or gradients.  Runs the
+ * forward wavefront alone (no checkpoints, no adjoint) and folds each pair's
+ * band partials, so scoring costs about half a full call; the values equal
+ * those of swb_sw_affine_forward / swb_sw_forward bit for bit.  No reference
+ * counterpart: the reference's forward ops always run forward and backward.
+ * Workspace from swb_sw_affine_value_workspace_bytes / swb_sw_value_workspace_bytes.
+ */
+size_t swb_sw_affine_value_workspace_bytes(int B, int L1max, int L2max);
+int swb_sw_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                        float gap_open, float gap_ext, float temp, float* value, void* workspace,
+                        size_t workspace_bytes, void* stream);
+size_t swb_sw_value_workspace_bytes(int B, int L1max, int L2max);
+int swb_sw_value(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
+                 float temp, float* value, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
  * Packed ragged batch (no reference counterpart: the reference pads every
  * pair to one shape; this is the batched path beside its drop-in).
  *

@@ -85,6 +85,14 @@ def load() -> ctypes.CDLL:
     lib.swb_sw_affine_aux_workspace_bytes.argtypes = [i, i, i]
     lib.swb_sw_aux_workspace_bytes.restype = sz
     lib.swb_sw_aux_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sw_affine_value_workspace_bytes.restype = sz
+    lib.swb_sw_affine_value_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sw_value_workspace_bytes.restype = sz
+    lib.swb_sw_value_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sw_affine_value.restype = i
+    lib.swb_sw_affine_value.argtypes = [vp, vp, i, i, i, f, f, f, vp, vp, sz, vp]
+    lib.swb_sw_value.restype = i
+    lib.swb_sw_value.argtypes = [vp, vp, i, i, i, f, f, vp, vp, sz, vp]
     lib.swb_sw_affine_hvp.restype = i
     lib.swb_sw_affine_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, f, vp, vp, vp, sz, vp]
     lib.swb_sw_affine_param_jacobian.restype = i

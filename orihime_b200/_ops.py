@@ -195,6 +195,26 @@ def run_linear(scores, lengths, gap, temp, options=None):
     return value, amap, g_gap, g_T
 
 
+def run_value(fam, scores, lengths, params):
+    """S per pair of a validated padded batch, forward wavefront only (no map,
+    no gradients); equal bit for bit to the value of run_affine / run_linear."""
+    B, L1, L2 = scores.shape
+    dev = scores.device
+    value = torch.empty(B, dtype=torch.float32, device=dev)
+    if B == 0:
+        return value
+    aff = fam == "sw_affine"
+    nbytes = int((_LIB.swb_sw_affine_value_workspace_bytes if aff else _LIB.swb_sw_value_workspace_bytes)(
+        B, L1, L2))
+    ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    fn = _LIB.swb_sw_affine_value if aff else _LIB.swb_sw_value
+    with torch.cuda.device(dev):
+        rc = fn(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params), _ptr(value), _ptr(ws),
+                nbytes, _stream(dev))
+    _lib.check(rc, "swb_sw_affine_value" if aff else "swb_sw_value")
+    return value
+
+
 def _prep(scores, lengths, family):
     check_input_cuda(scores, "scores")
     B, L1, L2 = check_shape(scores, family)
@@ -519,8 +539,38 @@ for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True
     _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
 
 
+# ---------------------------------------------------------------------------
+# build-owned ops (namespace orihime_b200, no reference counterpart)
+# ---------------------------------------------------------------------------
+# Value only: the forward wavefront without map or gradients, for scoring
+# under no_grad (the reference's forward ops always run forward + backward).
+
+OWN_SCHEMAS = {
+    "sw_value": "sw_value(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
+    "sw_affine_value": "sw_affine_value(Tensor scores, float gap_open, float gap_ext, float temp, "
+                       "Tensor? lengths) -> Tensor",
+}
+_OWN_LIB = torch.library.Library("orihime_b200", "DEF")
+for _name, _schema in OWN_SCHEMAS.items():
+    _OWN_LIB.define(_schema)
+
+
+def _own_sw_value(scores, gap, temp, lengths):
+    ln = _prep(scores, lengths, "sw")
+    return run_value("sw", scores, ln, (gap, temp))
+
+
+def _own_sw_affine_value(scores, gap_open, gap_ext, temp, lengths):
+    ln = _prep(scores, lengths, "sw_affine")
+    return run_value("sw_affine", scores, ln, (gap_open, gap_ext, temp))
+
+
+_OWN_LIB.impl("sw_value", _own_sw_value, "CUDA")
+_OWN_LIB.impl("sw_affine_value", _own_sw_affine_value, "CUDA")
+
 # Meta shapes, FP32 autocast and vmap rules for the ops defined here (when the
 # reference extension defined them, its own Python package registers these).
 from . import _registrations  # noqa: E402
 
 _registrations.register(DEFINED_HERE)
+_registrations.register(list(OWN_SCHEMAS), namespace="orihime_b200")

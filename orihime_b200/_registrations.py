@@ -1,5 +1,6 @@
 """Meta (fake) shapes, FP32 autocast and vmap batch-folding rules of the 15
-soft Smith-Waterman ops, for the ops that orihime_b200 defined itself.
+soft Smith-Waterman ops, for the ops that orihime_b200 defined itself, and of
+its own value-only ops (`orihime_b200::sw_value`, `sw_affine_value`).
 
 The reference registers the same three things for its ops:
 - fake impls: `orihime/_compile.py:25-140`;
@@ -59,8 +60,14 @@ def _fake_backward(n):
     return fake
 
 
+def _fake_value(scores, *rest):
+    return scores.new_empty([scores.size(0)])
+
+
 def _fake_for(name: str):
     n = _NPARAMS[_fam(name)]
+    if name.endswith("_value"):
+        return _fake_value
     if name.endswith("_forward") or name.endswith("_forward_t"):
         return _fake_forward
     if name.endswith("_value_grad_params"):
@@ -72,8 +79,8 @@ def _fake_for(name: str):
 
 # ---- vmap batch folding -----------------------------------------------------
 
-def _vmap_rule(name: str):
-    op = getattr(torch.ops.orihime, name).default
+def _vmap_rule(name: str, namespace: str = "orihime"):
+    op = getattr(getattr(torch.ops, namespace), name).default
     argn = [a.name for a in op._schema.arguments]
     bidx = [k for k, n in enumerate(argn) if n in _BATCH_ARGS]
     fam = _fam(name)
@@ -82,7 +89,7 @@ def _vmap_rule(name: str):
     def rule(info, in_dims, *args):
         for k, d in enumerate(in_dims):
             if d is not None and k not in bidx:
-                raise RuntimeError(f"orihime::{name} does not support mapping scalar argument "
+                raise RuntimeError(f"{namespace}::{name} does not support mapping scalar argument "
                                    f"{argn[k]!r}; keep scalar parameters unbatched")
         V = info.batch_size
         nb = None
@@ -93,16 +100,16 @@ def _vmap_rule(name: str):
                 continue
             x = x.movedim(in_dims[k], 0) if in_dims[k] is not None else x.unsqueeze(0).expand(V, *x.shape)
             if x.ndim < 2:
-                raise RuntimeError(f"orihime::{name} batch argument {argn[k]!r} has no native batch "
+                raise RuntimeError(f"{namespace}::{name} batch argument {argn[k]!r} has no native batch "
                                    "dimension")
             if nb is None:
                 nb = x.shape[1]
             elif x.shape[1] != nb:
-                raise RuntimeError(f"orihime::{name} received inconsistent native batch sizes "
+                raise RuntimeError(f"{namespace}::{name} received inconsistent native batch sizes "
                                    f"{nb} and {x.shape[1]}")
             args[k] = x.reshape(V * nb, *x.shape[2:]).contiguous()
         if nb is None:
-            raise RuntimeError(f"orihime::{name} requires a mapped batch-aligned tensor")
+            raise RuntimeError(f"{namespace}::{name} requires a mapped batch-aligned tensor")
 
         def unfold(t):
             return t.reshape(V, nb, *t.shape[1:])
@@ -125,10 +132,10 @@ def _vmap_rule(name: str):
     return rule
 
 
-def register(names) -> None:
+def register(names, namespace: str = "orihime") -> None:
     """Fake impls, FP32 autocast and vmap rules for the ops in `names`."""
     for name in names:
-        qual = f"orihime::{name}"
+        qual = f"{namespace}::{name}"
         torch.library.register_fake(qual)(_fake_for(name))
         torch.library.register_autocast(qual, "cuda", torch.float32)
-        torch.library.register_vmap(qual, _vmap_rule(name))
+        torch.library.register_vmap(qual, _vmap_rule(name, namespace))

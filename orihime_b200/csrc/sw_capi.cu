@@ -161,7 +161,7 @@ int static_scratch(void** out) {
 // Common launch: per-call resets, then the forward and adjoint kernels.
 template <int NS, int R>
 int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool clear_map, void* ws,
-           size_t ws_bytes, void* stream_v, const swb_options* opt) {
+           size_t ws_bytes, void* stream_v, const swb_options* opt, bool value_only = false) {
   if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
   DevInfo* d = nullptr;
   int rc = dev_info(&d);
@@ -177,7 +177,7 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   a.never_written = reinterpret_cast<float*>(w + l.off_sent);
   a.edge = reinterpret_cast<float*>(w + l.off_edge);
   a.bpush = reinterpret_cast<float*>(w + l.off_bpush);
-  a.ckpt = reinterpret_cast<float*>(w + l.off_ckpt);
+  a.ckpt = value_only ? nullptr : reinterpret_cast<float*>(w + l.off_ckpt);
   a.spin_limit_ns = (opt && opt->spin_limit_ns) ? opt->spin_limit_ns : 20ull * 1000000000ull;
   a.fault_inject = opt ? opt->fault_inject : 0;
 
@@ -207,6 +207,10 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   if (opt && opt->split_event &&
       cudaEventRecord(reinterpret_cast<cudaEvent_t>(opt->split_event), st) != cudaSuccess)
     return SWB_ERR_CUDA;
+  if (value_only) {
+    swb::value_kernel<NS, R><<<(a.B + 3) / 4, 128, 0, st>>>(a);
+    return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+  }
   swb::bwd_kernel<NS, R, kWarpsBwd><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS, R>(), st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   return SWB_OK;
@@ -244,6 +248,38 @@ int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L
     return launch_padded_r<NS, 4>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
                                   g_ext, g_T, ws, ws_bytes, stream, opt);
   return SWB_ERR_ARG;
+}
+
+// Padded value-only batch: the forward wavefront, no checkpoints, no adjoint.
+template <int NS>
+Layout value_layout(long long B, long long L1m, long long L2m) {
+  constexpr int R = kDefaultR;
+  int nb = (int)((L2m + 32 * R - 1) / (32 * R));
+  if (nb < 1) nb = 1;
+  const size_t slots = (size_t)B * nb;
+  Layout l = layout_sizes(B, slots, slots * ne<NS, R>() * (size_t)L1m,
+                          slots * np<NS, R>() * (size_t)(L1m + 1), 0);
+  l.nb = nb;
+  l.nchunks = chunks_for(L1m);
+  return l;
+}
+
+template <int NS>
+int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
+                 float ge, float T, float* value, void* ws, size_t ws_bytes, void* stream) {
+  if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
+  if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
+  if (B == 0) return SWB_OK;
+  if (!value || ((size_t)B * L1m * L2m > 0 && !scores)) return SWB_ERR_ARG;
+  const Layout l = value_layout<NS>(B, L1m, L2m);
+  Args a{};
+  a.scores = scores; a.map = nullptr; a.lengths = lengths;
+  a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
+  a.go = go; a.ge = ge; a.T = T;
+  a.nb = l.nb; a.nchunks = l.nchunks;
+  a.value = value;
+  return launch<NS, kDefaultR>(a, l, (long long)B * l.nb, 0, false, ws, ws_bytes, stream, nullptr,
+                               true);
 }
 
 template <int NS>
@@ -450,6 +486,27 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
 size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;
   return std::max(layout_for<3, 2>(B, L1max, L2max).total, layout_for<3, 4>(B, L1max, L2max).total);
+}
+
+size_t swb_sw_affine_value_workspace_bytes(int B, int L1max, int L2max) {
+  return B > 0 ? value_layout<3>(B, L1max, L2max).total : 0;
+}
+
+size_t swb_sw_value_workspace_bytes(int B, int L1max, int L2max) {
+  return B > 0 ? value_layout<1>(B, L1max, L2max).total : 0;
+}
+
+int swb_sw_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                        float gap_open, float gap_ext, float temp, float* value, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+  return launch_value<3>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value, workspace,
+                         workspace_bytes, stream);
+}
+
+int swb_sw_value(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
+                 float temp, float* value, void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_value<1>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, workspace,
+                         workspace_bytes, stream);
 }
 
 size_t swb_sw_workspace_bytes(int B, int L1max, int L2max) {

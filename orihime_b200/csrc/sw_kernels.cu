@@ -522,7 +522,9 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
   const float* ein = (band > 0) ? eout - w.edb : nullptr;
   const bool fault = a.fault_inject && band > 0;
   if (fault) ein = nullptr;
-  float* ck = a.ckpt + w.ck0 + (size_t)band * w.ckb;
+  // value-only calls (no adjoint to follow) pass no checkpoint buffer
+  const bool keep_ck = a.ckpt != nullptr;
+  float* ck = keep_ck ? a.ckpt + w.ck0 + (size_t)band * w.ckb : nullptr;
   const int nch = band_chunks(L1);
 
   float ph[NS][R], pl[NS][R], lh[NS], ll[NS];
@@ -554,7 +556,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
   }
 
   for (int kc = 0; kc < nch; ++kc) {
-    {  // checkpoint: state before step kc*C
+    if (keep_ck) {  // checkpoint: state before step kc*C
       float v[D::CKF];
       ck_pack<NS, R>(ph, pl, lh, ll, v);
       ck_store<NS, R>(ck + (size_t)kc * D::CKRS, lane, v);
@@ -655,7 +657,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
     for (int f = 0; f < NE; ++f) eb[f] = ebn[f];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cmx = fmaxf(cmx, __shfl_xor_sync(FULL, cmx, o));
-    if (lane == 0) ck[(size_t)kc * D::CKRS + D::CKF * 32] = cmx;
+    if (keep_ck && lane == 0) ck[(size_t)kc * D::CKRS + D::CKF * 32] = cmx;
   }
   // warp-combine (ref, sum) pairs
   float s_ = acc.s;
@@ -725,6 +727,19 @@ __device__ __forceinline__ void pair_logz(const Args& a, const Place& w, int lan
     Sh = ref;
     Sl = lg2(s);
   }
+}
+
+// Value-only calls: one warp per pair folds the forward's band partials into
+// S, as finish_pair does after a full adjoint (padded layout; 4 warps per CTA).
+template <int NS, int R>
+__global__ void __launch_bounds__(128) value_kernel(Args a) {
+  const int lane = threadIdx.x & 31;
+  const int q = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (q >= a.B) return;
+  const Place w = place_of<NS, R>(a, q * a.nb, false);
+  float Sh, Sl;
+  pair_logz(a, w, lane, Sh, Sl);
+  if (lane == 0) a.value[w.p] = (Sh + Sl) * (1.f / a.k);
 }
 
 // Last band task of a pair to finish folds the per-band gradient partials (in

@@ -120,6 +120,7 @@ class Family:
     grads: Callable              # (scores, *floats, lengths) -> per-param dS/dtheta [B] each
     hvp: Callable                # (scores, v, *floats, lengths) -> [B, L1, L2]
     sens: tuple[Callable, ...]   # per param: (scores, *floats, lengths) -> dP/dtheta
+    value: Callable = None       # (scores, *floats, lengths) -> [B], forward wavefront only
 
 
 def _ops():
@@ -133,6 +134,7 @@ SW = Family(
     hvp=lambda *a: _ops().sw_marginals_hvp(*a),
     sens=(lambda *a: _ops().sw_marginals_grad_gap(*a),
           lambda *a: _ops().sw_marginals_grad_temp(*a)),
+    value=lambda *a: torch.ops.orihime_b200.sw_value(*a),
 )
 
 SW_AFFINE = Family(
@@ -143,6 +145,7 @@ SW_AFFINE = Family(
     sens=(lambda *a: _ops().sw_affine_marginals_grad_gap_open(*a),
           lambda *a: _ops().sw_affine_marginals_grad_gap_ext(*a),
           lambda *a: _ops().sw_affine_marginals_grad_temp(*a)),
+    value=lambda *a: torch.ops.orihime_b200.sw_affine_value(*a),
 )
 
 
@@ -308,6 +311,12 @@ class Operator:
 
     def value(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:
         x, params, lengths = self._prepare(primary, params, lengths, mask, dtype)
+        needs_grad = torch.is_grad_enabled() and (
+            x.requires_grad or any(isinstance(p, Tensor) and p.requires_grad for p in params))
+        if not needs_grad:
+            # no gradient can flow: the forward wavefront alone (same values,
+            # no marginal map, about half the work)
+            return self.fam.value(x, *[_as_float(p) for p in params], lengths)
         return _ValueFn.apply(self.fam, lengths, x, *params)
 
     def entropy(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:

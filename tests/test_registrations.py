@@ -54,3 +54,9 @@ def test_vmap_rejects_inconsistent_native_batches():
     v = torch.zeros(2, 4, 4, 5)
     with pytest.raises(RuntimeError, match="inconsistent native batch sizes 3 and 4"):
         torch.func.vmap(lambda a, b: o.sw_marginals_hvp(a, b, *LIN, None))(s, v)
+
+
+def test_fake_shapes_of_value_only_ops():
+    s = torch.empty(3, 5, 7, device="meta")
+    assert torch.ops.orihime_b200.sw_value(s, *LIN, None).shape == (3,)
+    assert torch.ops.orihime_b200.sw_affine_value(s, *AFF, None).shape == (3,)
