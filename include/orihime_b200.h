@@ -227,6 +227,18 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
                           float gap, float temp, int param, float* out, void* workspace,
                           size_t workspace_bytes, void* stream);
 
+/*
+ * One pass over a [B, per_item] fp32 tensor for the Python prelude's input
+ * checks (replaces the reference's separate full-tensor passes in
+ * orihime/operator.py:249-386: isposinf().any(), the domain mask .all(),
+ * isneginf().any() and amax).  words (device, 1 + B unsigned): words[0] gets
+ * flag 1 if some cell is +inf, 2 if some cell is NaN or is finite, not
+ * -sentinel and |x| > limit, 4 if some cell is -inf.  amax (device, B floats)
+ * gets each item's largest cell (-inf if all are -inf).  Asynchronous.
+ */
+int swb_scan_scores(const float* x, int B, long long per_item, float limit, float sentinel,
+                    unsigned* words, float* amax, void* stream);
+
 /* Copies the workspace status word to *status (synchronises `stream`).
  * No reference counterpart: the reference synchronises inside every op. */
 int swb_read_status(const void* workspace, void* stream, unsigned* status);

@@ -195,6 +195,26 @@ def run_linear(scores, lengths, gap, temp, options=None):
     return value, amap, g_gap, g_T
 
 
+SCAN_POSINF, SCAN_DOMAIN, SCAN_NEGINF = 1, 2, 4
+
+
+def scan_scores(x, limit, sentinel):
+    """One device pass over a contiguous fp32 CUDA tensor [B, ...]: (flags,
+    amax[B]).  flags: SCAN_POSINF if some cell is +inf, SCAN_DOMAIN if some
+    cell is NaN or finite with |x| > limit and not -sentinel, SCAN_NEGINF if
+    some cell is -inf; amax: each item's largest cell.  Reading the flags
+    synchronises the stream once."""
+    B = x.shape[0]
+    per = x.numel() // B if B else 0
+    words = torch.empty(1 + 2 * B, dtype=torch.int32, device=x.device)
+    amax = words[1 + B:].view(torch.float32)
+    with torch.cuda.device(x.device):
+        rc = _LIB.swb_scan_scores(_ptr(x), B, per, float(limit), float(sentinel), _ptr(words), _ptr(amax),
+                                  _stream(x.device))
+    _lib.check(rc, "swb_scan_scores")
+    return int(words[0].item()) if B else 0, amax
+
+
 def run_value(fam, scores, lengths, params):
     """S per pair of a validated padded batch, forward wavefront only (no map,
     no gradients); equal bit for bit to the value of run_affine / run_linear."""

@@ -24,6 +24,7 @@ DEPS = SOURCES + [
     os.path.join(PKG, "csrc", "sw_kernels.cu"),
     os.path.join(PKG, "csrc", "sw_kernels.cuh"),
     os.path.join(PKG, "csrc", "sw_xband.cu"),
+    os.path.join(PKG, "csrc", "sw_prelude.cuh"),
     os.path.join(PKG, "csrc", "sw_probe.cuh"),
     os.path.join(ROOT, "include", "orihime_b200.h"),
 ]

@@ -15,6 +15,7 @@
 
 #include "sw_kernels.cu"
 #include "sw_xband.cu"
+#include "sw_prelude.cuh"
 #include "sw_probe.cuh"
 #include "../../include/orihime_b200.h"
 
@@ -486,6 +487,31 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
 size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;
   return std::max(layout_for<3, 2>(B, L1max, L2max).total, layout_for<3, 4>(B, L1max, L2max).total);
+}
+
+int swb_scan_scores(const float* x, int B, long long per_item, float limit, float sentinel,
+                    unsigned* words, float* amax, void* stream) {
+  if (B < 0 || per_item < 0 || !words || !amax) return SWB_ERR_ARG;
+  if (B == 0) return SWB_OK;
+  if (per_item > 0 && !x) return SWB_ERR_ARG;
+  DevInfo* d = nullptr;
+  int rc = dev_info(&d);
+  if (rc != SWB_OK) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  swb::scan_init_kernel<<<(B + 1 + 255) / 256, 256, 0, st>>>(words, B);
+  if (per_item > 0) {
+    // about 8 blocks of 256 threads per SM in all, at least one per item
+    const long long want = (long long)d->sms * 8;
+    long long bpi = (want + B - 1) / B;
+    const long long most = (per_item + 1023) / 1024;
+    if (bpi > most) bpi = most;
+    if (bpi < 1) bpi = 1;
+    if ((long long)B * bpi > 0x7fffffffLL) return SWB_ERR_ARG;
+    swb::scan_kernel<<<(unsigned)(B * bpi), 256, 0, st>>>(x, per_item, (int)bpi, limit, sentinel,
+                                                          words);
+  }
+  swb::scan_finish_kernel<<<(B + 255) / 256, 256, 0, st>>>(words, amax, B);
+  return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
 }
 
 size_t swb_sw_affine_value_workspace_bytes(int B, int L1max, int L2max) {
