@@ -560,6 +560,90 @@ for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True
 
 
 # ---------------------------------------------------------------------------
+# legacy soft_sw* ops (src/sw/registry.cpp:30-35, src/sw_affine/registry.cpp:27-32)
+# ---------------------------------------------------------------------------
+# The reference keeps 12 older schemas beside the namespaced ones; its Python
+# package no longer calls them.  Each is one of the namespaced op bodies under
+# another name (src/sw*/torch_cuda.cpp:803-830, :917-946).  They are defined
+# and given CUDA kernels only when orihime_b200 defines the schemas itself:
+# with the reference extension loaded first, they stay the reference's own.
+
+LEGACY_SCHEMAS = {
+    "soft_sw": "soft_sw(Tensor scores, Tensor gap, Tensor temperature, Tensor lengths) -> Tensor[]",
+    "soft_sw_float": "soft_sw_float(Tensor scores, float gap, float temperature, Tensor? lengths) -> Tensor[]",
+    "soft_sw_with_grads": "soft_sw_with_grads(Tensor scores, float gap, float temperature, Tensor? lengths) "
+                          "-> (Tensor, Tensor, Tensor, Tensor)",
+    "soft_sw_hvp": "soft_sw_hvp(Tensor scores, Tensor tangent, float gap, float temperature, Tensor? lengths) "
+                   "-> Tensor",
+    "soft_sw_param_jacobian": "soft_sw_param_jacobian(Tensor scores, int param_type, float gap, "
+                              "float temperature, Tensor? lengths) -> Tensor",
+    "soft_sw_backward_full": "soft_sw_backward_full(Tensor scores, Tensor grad_alignment, float gap, "
+                             "float temperature, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
+    "soft_sw_affine": "soft_sw_affine(Tensor scores, Tensor gap_open, Tensor gap_ext, Tensor temperature, "
+                      "Tensor lengths) -> Tensor[]",
+    "soft_sw_affine_float": "soft_sw_affine_float(Tensor scores, float gap_open, float gap_ext, "
+                            "float temperature, Tensor? lengths) -> Tensor[]",
+    "soft_sw_affine_with_grads": "soft_sw_affine_with_grads(Tensor scores, float gap_open, float gap_ext, "
+                                 "float temperature, Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor, Tensor)",
+    "soft_sw_affine_hvp": "soft_sw_affine_hvp(Tensor scores, Tensor tangent, float gap_open, float gap_ext, "
+                          "float temperature, Tensor? lengths) -> Tensor",
+    "soft_sw_affine_param_jacobian": "soft_sw_affine_param_jacobian(Tensor scores, int param_type, "
+                                     "float gap_open, float gap_ext, float temperature, Tensor? lengths) -> Tensor",
+    "soft_sw_affine_backward_full": "soft_sw_affine_backward_full(Tensor scores, Tensor grad_alignment, "
+                                    "float gap_open, float gap_ext, float temperature, Tensor? lengths) "
+                                    "-> (Tensor, Tensor, Tensor, Tensor)",
+}
+LEGACY_DEFINED_HERE = []
+if DEFINED_HERE:
+    for _name, _schema in LEGACY_SCHEMAS.items():
+        if not _op_exists(_name):
+            _DEF_LIB.define(_schema)
+            LEGACY_DEFINED_HERE.append(_name)
+
+
+def _legacy_with_grads_linear(scores, gap, temperature, lengths):
+    ln = _prep(scores, lengths, "sw")
+    return tuple(run_linear(scores, ln, gap, temperature))
+
+
+def _legacy_with_grads_affine(scores, gap_open, gap_ext, temperature, lengths):
+    ln = _prep(scores, lengths, "sw_affine")
+    return tuple(run_affine(scores, ln, gap_open, gap_ext, temperature))
+
+
+def _legacy_jacobian(fam, nparams):
+    def op(scores, param_type, *rest):
+        if not 0 <= int(param_type) < nparams:
+            raise RuntimeError(f"param_type must be in [0, {nparams}), got {param_type}")
+        *params, lengths = rest
+        ln = _prep(scores, lengths, fam)
+        return run_param_jacobian(fam, scores, ln, tuple(params), int(param_type))
+    return op
+
+
+LEGACY_IMPLS = {
+    "soft_sw_float": sw_forward,
+    "soft_sw": sw_forward_t,
+    "soft_sw_with_grads": _legacy_with_grads_linear,
+    "soft_sw_hvp": sw_marginals_hvp,
+    "soft_sw_param_jacobian": _legacy_jacobian("sw", 2),
+    "soft_sw_backward_full": sw_marginals_backward,
+    "soft_sw_affine_float": sw_affine_forward,
+    "soft_sw_affine": sw_affine_forward_t,
+    "soft_sw_affine_with_grads": _legacy_with_grads_affine,
+    "soft_sw_affine_hvp": sw_affine_marginals_hvp,
+    "soft_sw_affine_param_jacobian": _legacy_jacobian("sw_affine", 3),
+    "soft_sw_affine_backward_full": sw_affine_marginals_backward,
+}
+for _name in LEGACY_DEFINED_HERE:
+    _IMPL_LIB.impl(_name, LEGACY_IMPLS[_name], "CUDA")
+for _name, _fam, _t in (("soft_sw_float", "sw", False), ("soft_sw", "sw", True),
+                        ("soft_sw_affine_float", "sw_affine", False), ("soft_sw_affine", "sw_affine", True)):
+    if _name in LEGACY_DEFINED_HERE:   # differentiable like the reference (AutogradCUDA)
+        _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
+
+
+# ---------------------------------------------------------------------------
 # build-owned ops (namespace orihime_b200, no reference counterpart)
 # ---------------------------------------------------------------------------
 # Value only: the forward wavefront without map or gradients, for scoring

@@ -60,3 +60,11 @@ def test_fake_shapes_of_value_only_ops():
     s = torch.empty(3, 5, 7, device="meta")
     assert torch.ops.orihime_b200.sw_value(s, *LIN, None).shape == (3,)
     assert torch.ops.orihime_b200.sw_affine_value(s, *AFF, None).shape == (3,)
+
+
+def test_legacy_schemas_defined():
+    """The 12 legacy soft_sw* schemas (src/sw/registry.cpp:30-35,
+    src/sw_affine/registry.cpp:27-32) exist beside the namespaced ones."""
+    assert sorted(_ops.LEGACY_DEFINED_HERE) == sorted(_ops.LEGACY_SCHEMAS)
+    for name in _ops.LEGACY_SCHEMAS:
+        assert getattr(o, name).default._schema.name == f"orihime::{name}"
