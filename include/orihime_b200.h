@@ -180,6 +180,19 @@ int swb_sw_ragged(const float* scores, const void* host_plan, const void* dev_pl
                   const swb_options* opt);
 
 /*
+ * Value only for a packed ragged batch (no map, no gradients): the forward
+ * wavefront and a per-pair fold, with the same plan and workspace as
+ * swb_sw_affine_ragged / swb_sw_ragged (its checkpoint part goes unused).
+ * The values equal the full call's bit for bit.  No reference counterpart.
+ */
+int swb_sw_affine_ragged_value(const float* scores, const void* host_plan, const void* dev_plan,
+                               float gap_open, float gap_ext, float temp, float* value,
+                               void* workspace, size_t workspace_bytes, void* stream);
+int swb_sw_ragged_value(const float* scores, const void* host_plan, const void* dev_plan, float gap,
+                        float temp, float* value, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
+/*
  * Second-order ops (band wavefronts: a forward kernel carrying alpha and its
  * tangent, then a backward kernel carrying beta and its tangent).  The
  * workspace holds, for every cell the wavefront visits, the fields the

@@ -91,6 +91,10 @@ def load() -> ctypes.CDLL:
     lib.swb_sw_value_workspace_bytes.argtypes = [i, i, i]
     lib.swb_scan_scores.restype = i
     lib.swb_scan_scores.argtypes = [vp, i, ctypes.c_longlong, f, f, vp, vp, vp]
+    lib.swb_sw_affine_ragged_value.restype = i
+    lib.swb_sw_affine_ragged_value.argtypes = [vp, vp, vp, f, f, f, vp, vp, sz, vp]
+    lib.swb_sw_ragged_value.restype = i
+    lib.swb_sw_ragged_value.argtypes = [vp, vp, vp, f, f, vp, vp, sz, vp]
     lib.swb_sw_affine_value.restype = i
     lib.swb_sw_affine_value.argtypes = [vp, vp, i, i, i, f, f, f, vp, vp, sz, vp]
     lib.swb_sw_value.restype = i

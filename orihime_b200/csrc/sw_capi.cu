@@ -286,7 +286,8 @@ int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2
 template <int NS>
 int launch_ragged(const float* scores, const void* host_plan, const void* dev_plan, float go,
                   float ge, float T, float* value, float* map, float* g_open, float* g_ext,
-                  float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
+                  float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt,
+                  bool value_only = false) {
   if (!host_plan || !dev_plan) return SWB_ERR_ARG;
   const long long* h = static_cast<const long long*>(host_plan);
   if (h[HW_MAGIC] != kPlanMagic || (h[HW_FAMILY] & 0xff) != NS) return SWB_ERR_ARG;
@@ -294,8 +295,9 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   const long long B = h[HW_B], ntasks = h[HW_NTASKS];
   if (B == 0) return SWB_OK;
-  if (!value || !g_open || !g_T || (NS == 3 && !g_ext)) return SWB_ERR_ARG;
-  if (h[HW_MAP_ELEMS] > 0 && (!scores || !map)) return SWB_ERR_ARG;
+  if (!value) return SWB_ERR_ARG;
+  if (!value_only && (!g_open || !g_T || (NS == 3 && !g_ext))) return SWB_ERR_ARG;
+  if (h[HW_MAP_ELEMS] > 0 && (!scores || (!value_only && !map))) return SWB_ERR_ARG;
   const Layout l = layout_sizes(B, (size_t)h[HW_SLOTS], (size_t)h[HW_EDGE], (size_t)h[HW_BP],
                                 (size_t)h[HW_CK]);
   const long long* dp = static_cast<const long long*>(dev_plan);
@@ -307,8 +309,12 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
   a.B = (int)B; a.layout = 1;
   a.go = go; a.ge = ge; a.T = T;
   a.value = value; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
-  if (r == 2) return launch<NS, 2>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt);
-  if (r == 4) return launch<NS, 4>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt);
+  if (r == 2)
+    return launch<NS, 2>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt,
+                         value_only);
+  if (r == 4)
+    return launch<NS, 4>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt,
+                         value_only);
   return SWB_ERR_ARG;
 }
 
@@ -666,6 +672,20 @@ int swb_sw_affine_ragged(const float* scores, const void* host_plan, const void*
                          size_t workspace_bytes, void* stream, const swb_options* opt) {
   return launch_ragged<3>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value, map,
                           grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream, opt);
+}
+
+int swb_sw_affine_ragged_value(const float* scores, const void* host_plan, const void* dev_plan,
+                               float gap_open, float gap_ext, float temp, float* value,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_ragged<3>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value, nullptr,
+                          nullptr, nullptr, nullptr, workspace, workspace_bytes, stream, nullptr, true);
+}
+
+int swb_sw_ragged_value(const float* scores, const void* host_plan, const void* dev_plan, float gap,
+                        float temp, float* value, void* workspace, size_t workspace_bytes,
+                        void* stream) {
+  return launch_ragged<1>(scores, host_plan, dev_plan, gap, 0.f, temp, value, nullptr, nullptr,
+                          nullptr, nullptr, workspace, workspace_bytes, stream, nullptr, true);
 }
 
 int swb_sw_ragged(const float* scores, const void* host_plan, const void* dev_plan, float gap,

@@ -730,13 +730,22 @@ __device__ __forceinline__ void pair_logz(const Args& a, const Place& w, int lan
 }
 
 // Value-only calls: one warp per pair folds the forward's band partials into
-// S, as finish_pair does after a full adjoint (padded layout; 4 warps per CTA).
+// S, as finish_pair does after a full adjoint (4 warps per CTA).  Only the
+// pair's band count and first partial slot are needed.
 template <int NS, int R>
 __global__ void __launch_bounds__(128) value_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (q >= a.B) return;
-  const Place w = place_of<NS, R>(a, q * a.nb, false);
+  Place w;
+  if (a.layout == 0) {
+    w = place_of<NS, R>(a, q * a.nb, false);
+  } else {
+    const long long* pw = a.plan_pairs + (size_t)q * PLAN_PAIR_WORDS;
+    w.p = q;
+    w.nb = (int)pw[PW_NB];
+    w.slot0 = (size_t)pw[PW_SLOT0];
+  }
   float Sh, Sl;
   pair_logz(a, w, lane, Sh, Sl);
   if (lane == 0) a.value[w.p] = (Sh + Sl) * (1.f / a.k);

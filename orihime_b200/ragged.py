@@ -159,6 +159,35 @@ class Plan:
         _lib.check(rc, "ragged soft Smith-Waterman")
         return out
 
+    def values(self, flat: torch.Tensor, *, gap_open: float = 0.0, gap_ext: float = 0.0,
+               gap: float = 0.0, temp: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """S per pair of the packed batch without map or gradients: the forward
+        wavefront alone, about half the work of `run`, the same values bit for
+        bit (asynchronous).  `out`: optional float32 [B] device tensor."""
+        if flat.device != self.device or flat.dtype != torch.float32 or not flat.is_contiguous():
+            raise ValueError("scores must be a contiguous float32 tensor on the plan's device")
+        if flat.numel() < self.map_elems:
+            raise ValueError(f"scores has {flat.numel()} elements, the packing needs {self.map_elems}")
+        if not (temp > 0):
+            raise ValueError("temperature must be finite and strictly positive")
+        if out is None:
+            out = torch.empty(self.B, dtype=torch.float32, device=self.device)
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        hp = self.host_plan.ctypes.data
+        dp = self.dev_plan.data_ptr()
+        ws = self.workspace.data_ptr()
+        with torch.cuda.device(self.device):
+            if self.family == "affine":
+                rc = self.lib.swb_sw_affine_ragged_value(
+                    flat.data_ptr(), hp, dp, float(gap_open), float(gap_ext), float(temp),
+                    out.data_ptr(), ws, self.workspace_bytes, st)
+            else:
+                rc = self.lib.swb_sw_ragged_value(
+                    flat.data_ptr(), hp, dp, float(gap), float(temp), out.data_ptr(), ws,
+                    self.workspace_bytes, st)
+        _lib.check(rc, "ragged soft Smith-Waterman value")
+        return out
+
     def status(self) -> int:
         st = ctypes.c_uint(0)
         rc = self.lib.swb_read_status(self.workspace.data_ptr(),

@@ -114,3 +114,23 @@ def test_streamed_plan_from_pinned_host_matches_plan():
         assert sp.status() == 0
         assert torch.equal(out.value, ref.value) and torch.equal(out.map, ref.map)
         assert torch.equal(out.grad_open, ref.grad_open) and torch.equal(out.grad_temp, ref.grad_temp)
+
+
+@pytest.mark.parametrize("family", ["affine", "linear"])
+@pytest.mark.parametrize("cols", [2, 4])
+def test_ragged_values_only_equal_full_run(family, cols):
+    """Plan.values (forward wavefront only) gives the full run's values bit
+    for bit, including empty pairs."""
+    from orihime_b200 import ragged
+
+    ln = _lengths(40, 7)
+    mats = [_emb(int(a), int(b), 300 + i) for i, (a, b) in enumerate(ln)]
+    flat, off, lens = ragged.pack(mats)
+    plan = ragged.Plan(lens, off, family=family, device="cuda", cols_per_lane=cols)
+    params = dict(gap_open=-2.0, gap_ext=-0.5, temp=0.5) if family == "affine" else dict(gap=-1.0, temp=0.5)
+    fd = flat.cuda()
+    full = plan.run(fd, **params).value.clone()
+    vals = plan.values(fd, **params)
+    again = plan.values(fd, **params)
+    assert plan.status() == 0
+    assert torch.equal(vals, full) and torch.equal(again, full)
