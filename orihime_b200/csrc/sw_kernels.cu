@@ -911,22 +911,26 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
       for (int q = 0; q < NP; ++q) inmax = fmaxf(fmaxf(inmax, outp[q]), pbc[q]);
       const bool ok = inmax < kFlowTiny && ckm - Sh < kInitQuiet;
       if (__all_sync(FULL, ok)) {
-        float z[R];
+        // zero map rows and pushes to the left band for the rows of chunk kq
+        auto zero_chunk = [&](int kq) {
+          float z[R];
 #pragma unroll
-        for (int c = 0; c < R; ++c) z[c] = 0.f;
-        for (int cu = 0; cu < C_STEPS; ++cu) {
-          const int i = t0 + (C_STEPS - 1 - cu) - lane + 1;
-          if (i >= 1 && i <= L1) {
-            store_row<R>(pr, i, jl, z);
-            if (lane == 0 && pout) {
+          for (int c = 0; c < R; ++c) z[c] = 0.f;
+          for (int cu = 0; cu < C_STEPS; ++cu) {
+            const int i = kq * C_STEPS + (C_STEPS - 1 - cu) - lane + 1;
+            if (i >= 1 && i <= L1) {
+              store_row<R>(pr, i, jl, z);
+              if (lane == 0 && pout) {
 #pragma unroll
-              for (int f = 0; f < NP; ++f) {
-                const bool left = (NS == 3) ? (f < 2) : (f < 1);
-                pout[f * (Lm + 1) + (left ? i : i - 1)] = 0.f;
+                for (int f = 0; f < NP; ++f) {
+                  const bool left = (NS == 3) ? (f < 2) : (f < 1);
+                  pout[f * (Lm + 1) + (left ? i : i - 1)] = 0.f;
+                }
               }
             }
           }
-        }
+        };
+        zero_chunk(kc);
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
           hold[q] = 0.f;
@@ -935,14 +939,49 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
         }
 #pragma unroll
         for (int q = 0; q < NP; ++q) outp[q] = 0.f;
-        if (kc > 0) {
-          load_ck(kc - 1);
-          load_eb(kc - 1);
-          load_sb(kc - 1);
-          load_pb(kc - 1, pbn);
-        }
+        // ---- quiet run.  After a quiet chunk nothing enters the next one
+        // from below or from the right lane, so the following chunks are
+        // quiet when the right band's pushes for their rows are written and
+        // below kFlowTiny and their alpha maxima are low.  One round of loads
+        // checks 32 / C chunks (lane l: chunk kn - l / C, lane 31's row at
+        // its step C - 1 - l % C); a push not written yet ends the run, and
+        // that chunk is then decided above from the same values, so results
+        // do not depend on timing. ----
+        constexpr int RUN = 32 / C_STEPS;
+        int kn = kc - 1;   // first chunk not known to be quiet
+        while (kn >= 0) {
+          const int j = lane / C_STEPS, u = lane - j * C_STEPS;
+          const int kq = kn - j;
+          bool q = kq >= 0;
+          if (q) {
+            const int ir = kq * C_STEPS + C_STEPS - 1 - u - 30;
+            if (pin && ir >= 1 && ir <= L1) {
 #pragma unroll
-        for (int q = 0; q < NP; ++q) pbc[q] = pbn[q];
+              for (int f = 0; f < NP; ++f) {
+                const bool left = (NS == 3) ? (f < 2) : (f < 1);
+                if (left || ir < L1) {
+                  const float v = ld_poll(pin + f * (Lm + 1) + ir);
+                  q = q && !is_sentinel(v) && v < kFlowTiny;
+                }
+              }
+            }
+            q = q && (ck[(size_t)kq * CKRS + CKF * 32] - Sh < kInitQuiet);
+          }
+          const unsigned ball = __ballot_sync(FULL, q);
+          constexpr unsigned grp = (1u << C_STEPS) - 1u;
+          int n = 0;
+          while (n < RUN && kn - n >= 0 && ((ball >> (n * C_STEPS)) & grp) == grp) ++n;
+          for (int m = 0; m < n; ++m) zero_chunk(kn - m);
+          kn -= n;
+          if (n < RUN) break;
+        }
+        if (kn >= 0) {   // inputs of the next chunk to run
+          load_ck(kn);
+          load_eb(kn);
+          load_sb(kn);
+          load_pb(kn, pbc);
+        }
+        kc = kn + 1;     // the loop continues with chunk kn
         continue;
       }
     }
