@@ -141,6 +141,26 @@ int swb_sw_value(const float* scores, const int* lengths, int B, int L1max, int 
                  float temp, float* value, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * Soft Needleman–Wunsch (global alignment), linear gap: value S = A[L1, L2],
+ * marginal map (posterior of each aligned cell), dS/dgap, dS/dT.  Boundaries
+ * A[i,0] = i*gap, A[0,j] = j*gap, no local start.  Replaces nw_forward_cuda /
+ * soft_nw_cuda_float and nw_value_grad_params_cuda (src/nw/torch_cuda.cpp:364,
+ * :716-745, registration :795-821), i.e. the launchers nw_forward +
+ * nw_backward (src/nw/kernels_gpu.cuh:209, :232).  Same band wavefront as swb_sw_forward;
+ * workspace from swb_nw_workspace_bytes.
+ */
+size_t swb_nw_workspace_bytes(int B, int L1max, int L2max);
+int swb_nw_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                   float gap, float temp,
+                   float* value, float* map, float* grad_gap, float* grad_temp,
+                   void* workspace, size_t workspace_bytes, void* stream,
+                   const swb_options* opt);
+/* Value only (forward wavefront alone; equals swb_nw_forward's value bit for bit). */
+size_t swb_nw_value_workspace_bytes(int B, int L1max, int L2max);
+int swb_nw_value(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
+                 float temp, float* value, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
  * Packed ragged batch (no reference counterpart: the reference pads every
  * pair to one shape; this is the batched path beside its drop-in).
  *

@@ -1,13 +1,15 @@
 /*
  * TEST INFRASTRUCTURE ONLY.  CPU oracle for the soft Smith-Waterman path
- * (linear and affine gaps) of megure-labs/orihime: value, marginal map,
- * parameter gradients, Hessian-vector product and parameter Jacobians.
+ * (linear and affine gaps) and the soft Needleman-Wunsch path (linear gap) of
+ * megure-labs/orihime: value, marginal map, parameter gradients,
+ * Hessian-vector product and parameter Jacobians.
  *
  * The product (orihime_b200) never loads this library: only tests/, the CPU
  * legs of bench.py and __graft_entry__.smoke() do, as the checker.
  *
  * Symbols ending in _f32 follow the reference CPU kernels
- * (src/sw/kernels_cpu.cpp, src/sw_affine/kernels_cpu.cpp) operation by
+ * (src/sw/kernels_cpu.cpp, src/sw_affine/kernels_cpu.cpp,
+ * src/nw/kernels_cpu.cpp) operation by
  * operation in float, so that they reproduce the reference bit for bit when
  * built without FMA contraction (gcc -std=c11 implies -ffp-contract=off).
  * Symbols ending in _f64 run the same recurrences in double: the FP64 truth.

@@ -725,6 +725,166 @@ static void FN(lin_param)(const FN(lin_t) *c, REAL S, REAL dSdt, int pt, REAL *u
     }
 }
 
+/* ---- global alignment (Needleman-Wunsch), linear gap -------------------
+ * Same table layout as the linear model (lin_t).  Boundaries A[0,0] = 0,
+ * A[i,0] = i*gap, A[0,j] = j*gap; three candidates (diag + s, up + gap,
+ * left + gap), no local start; S = A[L1, L2]; beta = 1 at the terminal only.
+ * Loop orders follow src/nw/kernels_cpu.cpp so that the float instantiation
+ * accumulates in the same order as the reference. */
+
+static void FN(nw_cands)(const FN(lin_t) *c, const REAL *tab, int i, int j, REAL v[3]) {
+    v[0] = tab[LIX(c, i - 1, j - 1)] + SC(c, i, j);
+    v[1] = tab[LIX(c, i - 1, j)] + c->g;
+    v[2] = tab[LIX(c, i, j - 1)] + c->g;
+}
+
+static void FN(nw_bounds)(FN(lin_t) *c, REAL *tab, int gap_index) {
+    /* gap_index: boundary values i*gap (0) or d/dgap of them, i (1) */
+    tab[0] = 0;
+    for (int i = 1; i <= c->L1; ++i) tab[LIX(c, i, 0)] = gap_index ? (REAL)i : (REAL)i * c->g;
+    for (int j = 1; j <= c->L2; ++j) tab[LIX(c, 0, j)] = gap_index ? (REAL)j : (REAL)j * c->g;
+}
+
+/* src/nw/kernels_cpu.cpp:77-150 */
+static REAL FN(nw_forward)(FN(lin_t) *c) {
+    size_t n = (size_t)(c->L1 + 1) * c->cols;
+    for (size_t q = 0; q < n; ++q) c->a[q] = (REAL)NEG_BIG;
+    FN(nw_bounds)(c, c->a, 0);
+    REAL v[3];
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            FN(nw_cands)(c, c->a, i, j, v);
+            c->a[LIX(c, i, j)] = FN(tlse)(v, 3, c->T);
+        }
+    return c->a[LIX(c, c->L1, c->L2)];
+}
+
+#define NW_DIAGS(c, k, i, j)                                                  \
+    for (int k = (c)->L1 + (c)->L2; k >= 2; --k)                              \
+        for (int i = ((k - (c)->L2 > 1) ? k - (c)->L2 : 1),                   \
+                 i##_end = (((c)->L1 < k - 1) ? (c)->L1 : k - 1);             \
+             i <= i##_end; ++i)                                               \
+            for (int j = k - i, j##_once = 1; j##_once; j##_once = 0)
+
+/* src/nw/kernels_cpu.cpp:156-268; g[0] = dS/dgap, g[1] = dS/dT. */
+static void FN(nw_adjoint)(const FN(lin_t) *c, REAL S, REAL *be, REAL *post, int L1max,
+                           REAL g[2]) {
+    size_t nsc = (size_t)L1max * c->ld;
+    size_t n = (size_t)(c->L1 + 1) * c->cols;
+    for (size_t q = 0; q < nsc; ++q) post[q] = 0;
+    for (size_t q = 0; q < n; ++q) be[q] = 0;
+    be[LIX(c, c->L1, c->L2)] = 1;
+    FN(ksum_t) gs = {0, 0}, ms = {0, 0};
+    REAL v[3], w[3];
+    NW_DIAGS(c, k, i, j) {
+        REAL b = be[LIX(c, i, j)];
+        if (b == 0) continue;
+        REAL sc = SC(c, i, j);
+        FN(nw_cands)(c, c->a, i, j, v);
+        FN(tsoftmax)(v, 3, c->T, w);
+        REAL p = b * w[0];
+        post[(size_t)(i - 1) * c->ld + (j - 1)] = p;
+        FN(kadd)(&ms, p * sc);
+        FN(kadd)(&gs, b * (w[1] + w[2]));
+        if (w[0] > 0) be[LIX(c, i - 1, j - 1)] += b * w[0];
+        if (w[1] > 0) be[LIX(c, i - 1, j)] += b * w[1];
+        if (w[2] > 0) be[LIX(c, i, j - 1)] += b * w[2];
+    }
+    /* boundary cells carry gap costs i*gap and j*gap (kernels_cpu.cpp:250-258) */
+    for (int i = 1; i <= c->L1; ++i) FN(kadd)(&gs, be[LIX(c, i, 0)] * (REAL)i);
+    for (int j = 1; j <= c->L2; ++j) FN(kadd)(&gs, be[LIX(c, 0, j)] * (REAL)j);
+    REAL gg = gs.s;
+    g[0] = gg;
+    g[1] = (S - (ms.s + gg * c->g)) / c->T;
+}
+
+/* src/nw/kernels_cpu.cpp:276-437 (HVP). */
+static void FN(nw_hvp)(const FN(lin_t) *c, const REAL *V, REAL *da, REAL *be, REAL *dbe,
+                       REAL *H, int L1max) {
+    size_t n = (size_t)(c->L1 + 1) * c->cols;
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < n; ++q) { da[q] = 0; be[q] = 0; dbe[q] = 0; }
+    for (size_t q = 0; q < nsc; ++q) H[q] = 0;
+    REAL v[3], w[3];
+#define VV(i, j) V[(size_t)((i) - 1) * c->ld + (size_t)((j) - 1)]
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            FN(nw_cands)(c, c->a, i, j, v);
+            FN(tsoftmax)(v, 3, c->T, w);
+            REAL d0 = da[LIX(c, i - 1, j - 1)] + VV(i, j);
+            REAL d1 = da[LIX(c, i - 1, j)];
+            REAL d2 = da[LIX(c, i, j - 1)];
+            da[LIX(c, i, j)] = w[0] * d0 + w[1] * d1 + w[2] * d2;
+        }
+    be[LIX(c, c->L1, c->L2)] = 1;
+    NW_DIAGS(c, k, i, j) {
+        size_t o = LIX(c, i, j);
+        REAL b = be[o], db = dbe[o];
+        if (b == 0 && FABS(db) < (REAL)1e-20) continue;
+        FN(nw_cands)(c, c->a, i, j, v);
+        FN(tsoftmax)(v, 3, c->T, w);
+        REAL t[3];
+        t[0] = da[LIX(c, i - 1, j - 1)] + VV(i, j);
+        t[1] = da[LIX(c, i - 1, j)];
+        t[2] = da[LIX(c, i, j - 1)];
+        REAL e = w[0] * t[0] + w[1] * t[1] + w[2] * t[2];
+        REAL dw[3];
+        for (int q = 0; q < 3; ++q) dw[q] = w[q] * (t[q] - e) / c->T;
+        H[(size_t)(i - 1) * c->ld + (j - 1)] = db * w[0] + b * dw[0];
+        if (w[0] > 0) { be[LIX(c, i - 1, j - 1)] += b * w[0]; dbe[LIX(c, i - 1, j - 1)] += db * w[0] + b * dw[0]; }
+        if (w[1] > 0) { be[LIX(c, i - 1, j)] += b * w[1]; dbe[LIX(c, i - 1, j)] += db * w[1] + b * dw[1]; }
+        if (w[2] > 0) { be[LIX(c, i, j - 1)] += b * w[2]; dbe[LIX(c, i, j - 1)] += db * w[2] + b * dw[2]; }
+    }
+#undef VV
+}
+
+/* src/nw/kernels_cpu.cpp:445-640 (dP/dtheta, theta in {gap, T}). */
+static void FN(nw_param)(FN(lin_t) *c, int pt, REAL *u, REAL *be, REAL *wt, REAL *dP,
+                         int L1max) {
+    size_t n = (size_t)(c->L1 + 1) * c->cols;
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < n; ++q) { u[q] = 0; be[q] = 0; wt[q] = 0; }
+    for (size_t q = 0; q < nsc; ++q) dP[q] = 0;
+    if (pt == 0) FN(nw_bounds)(c, u, 1);
+    const REAL T = c->T;
+    REAL v[3], w[3];
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            FN(nw_cands)(c, c->a, i, j, v);
+            FN(tsoftmax)(v, 3, T, w);
+            REAL a0 = u[LIX(c, i - 1, j - 1)], a1 = u[LIX(c, i - 1, j)], a2 = u[LIX(c, i, j - 1)];
+            if (pt == 0) { a1 += 1; a2 += 1; }
+            REAL U = w[0] * a0 + w[1] * a1 + w[2] * a2;
+            if (pt == 1) {
+                REAL e = w[0] * v[0] + w[1] * v[1] + w[2] * v[2];
+                U += (c->a[LIX(c, i, j)] - e) / T;
+            }
+            u[LIX(c, i, j)] = U;
+        }
+    be[LIX(c, c->L1, c->L2)] = 1;
+    NW_DIAGS(c, k, i, j) {
+        size_t o = LIX(c, i, j);
+        REAL b = be[o], W = wt[o];
+        if (b == 0 && FABS(W) < (REAL)1e-20) continue;
+        FN(nw_cands)(c, c->a, i, j, v);
+        FN(tsoftmax)(v, 3, T, w);
+        REAL du[3] = {u[LIX(c, i - 1, j - 1)], u[LIX(c, i - 1, j)], u[LIX(c, i, j - 1)]};
+        if (pt == 0) { du[1] += 1; du[2] += 1; }
+        REAL e = w[0] * du[0] + w[1] * du[1] + w[2] * du[2];
+        REAL dw[3];
+        for (int q = 0; q < 3; ++q) dw[q] = w[q] * (du[q] - e) / T;
+        if (pt == 1) {
+            REAL ev = w[0] * v[0] + w[1] * v[1] + w[2] * v[2];
+            REAL it2 = (REAL)1 / (T * T);
+            for (int q = 0; q < 3; ++q) dw[q] += w[q] * (ev - v[q]) * it2;
+        }
+        dP[(size_t)(i - 1) * c->ld + (j - 1)] = W * w[0] + b * dw[0];
+        if (w[0] > 0) { be[LIX(c, i - 1, j - 1)] += b * w[0]; wt[LIX(c, i - 1, j - 1)] += W * w[0] + b * dw[0]; }
+        if (w[1] > 0) { be[LIX(c, i - 1, j)] += b * w[1]; wt[LIX(c, i - 1, j)] += W * w[1] + b * dw[1]; }
+        if (w[2] > 0) { be[LIX(c, i, j - 1)] += b * w[2]; wt[LIX(c, i, j - 1)] += W * w[2] + b * dw[2]; }
+    }
+}
+
 /* ---- batched entry points (padded [B, L1max, L2max] layout) ------------ */
 
 static int FN(pair_len)(const int *lengths, int b, int which, int dflt) {
@@ -872,6 +1032,73 @@ int FN(oracle_sw_linear_param_grad)(const REAL *scores, const int *lengths, int 
     return 0;
 }
 
+int FN(oracle_nw_linear_forward)(const REAL *scores, const int *lengths, int B, int L1m,
+                                 int L2m, REAL gap, REAL T, REAL *value, REAL *map,
+                                 REAL *ggap, REAL *gT) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 2 * plane);
+    if (!a) return -1;
+    REAL *be = a + plane;
+    for (int b = 0; b < B; ++b) {
+        FN(lin_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.g = gap; c.T = T;
+        c.cols = (size_t)L2m + 1; c.a = a;
+        REAL S = FN(nw_forward)(&c);
+        REAL g[2];
+        FN(nw_adjoint)(&c, S, be, map + b * slab, L1m, g);
+        value[b] = S;
+        if (ggap) ggap[b] = g[0];
+        if (gT) gT[b] = g[1];
+    }
+    free(a);
+    return 0;
+}
+
+int FN(oracle_nw_linear_hvp)(const REAL *scores, const REAL *V, const int *lengths, int B,
+                             int L1m, int L2m, REAL gap, REAL T, REAL *out) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *buf = (REAL *)malloc(sizeof(REAL) * 4 * plane);
+    if (!buf) return -1;
+    REAL *a = buf, *be = buf + plane, *da = buf + 2 * plane, *dbe = buf + 3 * plane;
+    for (int b = 0; b < B; ++b) {
+        FN(lin_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.g = gap; c.T = T;
+        c.cols = (size_t)L2m + 1; c.a = a;
+        FN(nw_forward)(&c);
+        FN(nw_hvp)(&c, V + b * slab, da, be, dbe, out + b * slab, L1m);
+    }
+    free(buf);
+    return 0;
+}
+
+/* pt: 0 = gap, 1 = temperature. */
+int FN(oracle_nw_linear_param_grad)(const REAL *scores, const int *lengths, int B, int L1m,
+                                    int L2m, REAL gap, REAL T, int pt, REAL *out) {
+    size_t slab = (size_t)L1m * L2m;
+    size_t plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *buf = (REAL *)malloc(sizeof(REAL) * 4 * plane);
+    if (!buf) return -1;
+    REAL *a = buf, *be = buf + plane, *u = buf + 2 * plane, *w = buf + 3 * plane;
+    for (int b = 0; b < B; ++b) {
+        FN(lin_t) c;
+        c.L1 = FN(pair_len)(lengths, b, 0, L1m);
+        c.L2 = FN(pair_len)(lengths, b, 1, L2m);
+        c.ld = L2m; c.s = scores + b * slab; c.g = gap; c.T = T;
+        c.cols = (size_t)L2m + 1; c.a = a;
+        FN(nw_forward)(&c);
+        FN(nw_param)(&c, pt, u, be, w, out + b * slab, L1m);
+    }
+    free(buf);
+    return 0;
+}
+
+#undef NW_DIAGS
 #undef AIX
 #undef SC
 #undef LIX

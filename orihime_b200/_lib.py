@@ -107,6 +107,15 @@ def load() -> ctypes.CDLL:
     lib.swb_sw_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, vp, vp, vp, sz, vp]
     lib.swb_sw_param_jacobian.restype = i
     lib.swb_sw_param_jacobian.argtypes = [vp, vp, i, i, i, f, f, i, vp, vp, sz, vp]
+    lib.swb_nw_workspace_bytes.restype = sz
+    lib.swb_nw_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_nw_forward.restype = i
+    lib.swb_nw_forward.argtypes = [vp, vp, i, i, i, f, f, vp, vp, vp, vp, vp, sz, vp,
+                                   ctypes.POINTER(Options)]
+    lib.swb_nw_value_workspace_bytes.restype = sz
+    lib.swb_nw_value_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_nw_value.restype = i
+    lib.swb_nw_value.argtypes = [vp, vp, i, i, i, f, f, vp, vp, sz, vp]
     lib.swb_mufu_probe.restype = i
     lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()

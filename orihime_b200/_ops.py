@@ -1,15 +1,18 @@
-"""CUDA implementations of the ``torch.ops.orihime`` soft Smith-Waterman ops.
+"""CUDA implementations of the ``torch.ops.orihime`` soft Smith-Waterman ops
+(linear and affine gaps) and soft Needleman-Wunsch ops (global alignment,
+linear gap).
 
 This module is the drop-in seam.  The reference registers its CUDA kernels
 with ``TORCH_LIBRARY_IMPL(orihime, CUDA / AutogradCUDA, m)``
-(src/sw/torch_cuda.cpp:803-830, src/sw_affine/torch_cuda.cpp:917-946); here
-the same operator names get implementations that call the B200 kernels
-through the C ABI (``_lib``).
+(src/sw/torch_cuda.cpp:803-830, src/sw_affine/torch_cuda.cpp:917-946,
+src/nw/torch_cuda.cpp:795-821); here the same operator names get
+implementations that call the B200 kernels through the C ABI (``_lib``).
 
 * If the reference's own extension is already loaded in the process, its
   schemas exist and only the CUDA / AutogradCUDA kernels are replaced.
 * Otherwise the schemas are defined here, character for character as in
-  src/sw/registry.cpp:38-44 and src/sw_affine/registry.cpp:35-42.
+  src/sw/registry.cpp:38-44, src/sw_affine/registry.cpp:35-42 and
+  src/nw/registry.cpp:45-51.
 
 Validation mirrors the reference op bodies (same conditions, same messages)
 so that error-path tests read the same.  Like the reference, the value ops
@@ -42,6 +45,10 @@ SCHEMAS = {
     "sw_affine_marginals_grad_gap_open": "sw_affine_marginals_grad_gap_open(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
     "sw_affine_marginals_grad_gap_ext": "sw_affine_marginals_grad_gap_ext(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
     "sw_affine_marginals_grad_temp": "sw_affine_marginals_grad_temp(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    # src/nw/registry.cpp:45-47
+    "nw_forward": "nw_forward(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor[]",
+    "nw_forward_t": "nw_forward_t(Tensor scores, Tensor gap, Tensor temp, Tensor lengths) -> Tensor[]",
+    "nw_value_grad_params": "nw_value_grad_params(Tensor scores, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor)",
 }
 
 _INT32_MAX = 2**31 - 1
@@ -175,8 +182,9 @@ def run_affine(scores, lengths, go, ge, temp, options=None):
     return value, amap, g_open, g_ext, g_T
 
 
-def run_linear(scores, lengths, gap, temp, options=None):
-    """value, map, grad_gap, grad_temp for a validated padded batch."""
+def run_linear(scores, lengths, gap, temp, options=None, family="sw"):
+    """value, map, grad_gap, grad_temp for a validated padded batch; family
+    "sw" (local) or "nw" (global alignment)."""
     B, L1, L2 = scores.shape
     dev = scores.device
     value = torch.empty(B, dtype=torch.float32, device=dev)
@@ -185,13 +193,14 @@ def run_linear(scores, lengths, gap, temp, options=None):
     g_T = torch.empty(B, dtype=torch.float32, device=dev)
     if B == 0:
         return value, amap, g_gap, g_T
-    nbytes = _LIB.swb_sw_workspace_bytes(B, L1, L2)
+    nw = family == "nw"
+    nbytes = (_LIB.swb_nw_workspace_bytes if nw else _LIB.swb_sw_workspace_bytes)(B, L1, L2)
     ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    fn = _LIB.swb_nw_forward if nw else _LIB.swb_sw_forward
     with torch.cuda.device(dev):
-        rc = _LIB.swb_sw_forward(
-            _ptr(scores), _ptr(lengths), B, L1, L2, float(gap), float(temp), _ptr(value),
-            _ptr(amap), _ptr(g_gap), _ptr(g_T), _ptr(ws), nbytes, _stream(dev), options)
-    _lib.check(rc, "swb_sw_forward")
+        rc = fn(_ptr(scores), _ptr(lengths), B, L1, L2, float(gap), float(temp), _ptr(value),
+                _ptr(amap), _ptr(g_gap), _ptr(g_T), _ptr(ws), nbytes, _stream(dev), options)
+    _lib.check(rc, "swb_nw_forward" if nw else "swb_sw_forward")
     return value, amap, g_gap, g_T
 
 
@@ -223,15 +232,13 @@ def run_value(fam, scores, lengths, params):
     value = torch.empty(B, dtype=torch.float32, device=dev)
     if B == 0:
         return value
-    aff = fam == "sw_affine"
-    nbytes = int((_LIB.swb_sw_affine_value_workspace_bytes if aff else _LIB.swb_sw_value_workspace_bytes)(
-        B, L1, L2))
+    name = {"sw": "swb_sw_value", "sw_affine": "swb_sw_affine_value", "nw": "swb_nw_value"}[fam]
+    nbytes = int(getattr(_LIB, name + "_workspace_bytes")(B, L1, L2))
     ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
-    fn = _LIB.swb_sw_affine_value if aff else _LIB.swb_sw_value
     with torch.cuda.device(dev):
-        rc = fn(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params), _ptr(value), _ptr(ws),
-                nbytes, _stream(dev))
-    _lib.check(rc, "swb_sw_affine_value" if aff else "swb_sw_value")
+        rc = getattr(_LIB, name)(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params),
+                                 _ptr(value), _ptr(ws), nbytes, _stream(dev))
+    _lib.check(rc, name)
     return value
 
 
@@ -299,6 +306,37 @@ def sw_value_grad_params(scores, gap, temp, lengths):
     """orihime::sw_value_grad_params -> (dS/dgap, dS/dT), each [B] (src/sw/torch_cuda.cpp:404-450)."""
     ln = _prep(scores, lengths, "sw")
     _, _, gg, gT = run_linear(scores, ln, gap, temp)
+    return gg, gT
+
+
+# ---- global alignment (Needleman-Wunsch, linear gap) -----------------------
+
+def nw_forward(scores, gap, temp, lengths):
+    """orihime::nw_forward -> [value [B], marginals [B, L1, L2]]
+    (src/nw/torch_cuda.cpp:716 -> soft_nw_cuda_float :364)."""
+    ln = _prep(scores, lengths, "nw")
+    v, m, *_ = run_linear(scores, ln, gap, temp, family="nw")
+    return [v, m]
+
+
+def nw_forward_t(scores, gap, temp, lengths):
+    """orihime::nw_forward_t (src/nw/torch_cuda.cpp:726 -> SoftNWCUDAFunction :110-200)."""
+    check_input_cuda(scores, "scores")
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    g = _scalar_param(gap, "gap")
+    T = _scalar_param(temp, "temperature")
+    B, L1, L2 = check_shape(scores, "nw")
+    ln = resolve_lengths(lengths, B, L1, L2, scores.device)
+    v, m, *_ = run_linear(scores, ln, g, T, family="nw")
+    return [v, m]
+
+
+def nw_value_grad_params(scores, gap, temp, lengths):
+    """orihime::nw_value_grad_params -> (dS/dgap, dS/dT), each [B]
+    (src/nw/torch_cuda.cpp:736 -> soft_nw_cuda_with_grads :384)."""
+    ln = _prep(scores, lengths, "nw")
+    _, _, gg, gT = run_linear(scores, ln, gap, temp, family="nw")
     return gg, gT
 
 
@@ -473,6 +511,9 @@ IMPLS = {
     "sw_affine_forward": sw_affine_forward,
     "sw_affine_forward_t": sw_affine_forward_t,
     "sw_affine_value_grad_params": sw_affine_value_grad_params,
+    "nw_forward": nw_forward,
+    "nw_forward_t": nw_forward_t,
+    "nw_value_grad_params": nw_value_grad_params,
 }
 
 for _name, _fn in IMPLS.items():
@@ -503,7 +544,7 @@ def _pgrad(g, like):
 class _ForwardFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, fam, tensor_params, scores, lengths, *params):
-        name = ("sw_affine_forward" if fam == "sw_affine" else "sw_forward") + ("_t" if tensor_params else "")
+        name = f"{fam}_forward" + ("_t" if tensor_params else "")
         v, m = _below(getattr(torch.ops.orihime, name), scores, *params, lengths)
         ctx.fam, ctx.tensor_params, ctx.lengths = fam, tensor_params, lengths
         ctx.vals = tuple(_scalar_param(p, "param") if tensor_params else float(p) for p in params)
@@ -523,21 +564,18 @@ class _ForwardFn(torch.autograd.Function):
             if gs is not None:
                 gs = gs + gv.view(-1, 1, 1) * m
             if want_p:
-                grads = _below(ops.sw_affine_value_grad_params if fam == "sw_affine"
-                               else ops.sw_value_grad_params, scores, *vals, ln)
+                grads = _below(getattr(ops, f"{fam}_value_grad_params"), scores, *vals, ln)
                 pg = [(gv * g).sum() for g in grads]
         if gm is not None:
             gmc = gm.contiguous()
             if want_p:
-                mb = _below(ops.sw_affine_marginals_backward if fam == "sw_affine"
-                            else ops.sw_marginals_backward, scores, gmc, *vals, ln)
+                mb = _below(getattr(ops, f"{fam}_marginals_backward"), scores, gmc, *vals, ln)
                 if gs is not None:
                     gs = gs + mb[0]
                 pg = [mb[1 + k].reshape(()) if pg[k] is None else pg[k] + mb[1 + k].reshape(())
                       for k in range(len(pg))]
             elif gs is not None:
-                gs = gs + _below(ops.sw_affine_marginals_hvp if fam == "sw_affine"
-                                 else ops.sw_marginals_hvp, scores, gmc, *vals, ln)
+                gs = gs + _below(getattr(ops, f"{fam}_marginals_hvp"), scores, gmc, *vals, ln)
         out = [None, None, gs, None]
         for k, p in enumerate(ctx.params):
             out.append(_pgrad(pg[k], p) if (ctx.tensor_params and pg[k] is not None
@@ -555,7 +593,8 @@ def _autograd_forward(fam, tensor_params):
 
 for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True),
                         ("sw_affine_forward", "sw_affine", False),
-                        ("sw_affine_forward_t", "sw_affine", True)):
+                        ("sw_affine_forward_t", "sw_affine", True),
+                        ("nw_forward", "nw", False), ("nw_forward_t", "nw", True)):
     _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
 
 
@@ -653,6 +692,7 @@ OWN_SCHEMAS = {
     "sw_value": "sw_value(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
     "sw_affine_value": "sw_affine_value(Tensor scores, float gap_open, float gap_ext, float temp, "
                        "Tensor? lengths) -> Tensor",
+    "nw_value": "nw_value(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
 }
 _OWN_LIB = torch.library.Library("orihime_b200", "DEF")
 for _name, _schema in OWN_SCHEMAS.items():
@@ -669,8 +709,14 @@ def _own_sw_affine_value(scores, gap_open, gap_ext, temp, lengths):
     return run_value("sw_affine", scores, ln, (gap_open, gap_ext, temp))
 
 
+def _own_nw_value(scores, gap, temp, lengths):
+    ln = _prep(scores, lengths, "nw")
+    return run_value("nw", scores, ln, (gap, temp))
+
+
 _OWN_LIB.impl("sw_value", _own_sw_value, "CUDA")
 _OWN_LIB.impl("sw_affine_value", _own_sw_affine_value, "CUDA")
+_OWN_LIB.impl("nw_value", _own_nw_value, "CUDA")
 
 # Meta shapes, FP32 autocast and vmap rules for the ops defined here (when the
 # reference extension defined them, its own Python package registers these).

@@ -1,6 +1,7 @@
-"""Meta (fake) shapes, FP32 autocast and vmap batch-folding rules of the 15
-soft Smith-Waterman ops, for the ops that orihime_b200 defined itself, and of
-its own value-only ops (`orihime_b200::sw_value`, `sw_affine_value`).
+"""Meta (fake) shapes, FP32 autocast and vmap batch-folding rules of the soft
+Smith-Waterman and soft Needleman-Wunsch ops, for the ops that orihime_b200
+defined itself, and of its own value-only ops (`orihime_b200::sw_value`,
+`sw_affine_value`, `nw_value`).
 
 The reference registers the same three things for its ops:
 - fake impls: `orihime/_compile.py:25-140`;
@@ -30,11 +31,13 @@ import torch
 from . import _ops
 
 _BATCH_ARGS = frozenset({"scores", "v", "grad_marginals", "lengths"})
-_NPARAMS = {"sw": 2, "sw_affine": 3}
+_NPARAMS = {"sw": 2, "sw_affine": 3, "nw": 2}
 
 
 def _fam(name: str) -> str:
-    return "sw_affine" if name.startswith("sw_affine") else "sw"
+    if name.startswith("sw_affine"):
+        return "sw_affine"
+    return "nw" if name.startswith("nw") else "sw"
 
 
 # ---- fake impls -------------------------------------------------------------

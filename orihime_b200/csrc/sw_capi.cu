@@ -103,7 +103,7 @@ size_t plan_bytes_for(long long B, long long ntasks) {
 // Occupancy of each kernel instantiation on one device, computed once.
 struct DevInfo {
   int sms = 0;
-  int occ[2][2][2] = {};   // [kernel fwd/bwd][NS affine?][R == 4?]
+  int occ[2][3][2] = {};   // [kernel fwd/bwd][model: linear, affine, global linear][R == 4?]
   bool ready = false;
 };
 DevInfo g_dev[64];
@@ -112,17 +112,20 @@ std::mutex g_mu;
 template <int NS, int R>
 size_t bwd_smem() { return (size_t)kWarpsBwd * swb::bwd_smem_floats<NS, R>() * sizeof(float); }
 
-template <int NS, int R>
+template <int NS, bool G> constexpr int model_index() { return NS == 3 ? 1 : (G ? 2 : 0); }
+
+template <int NS, int R, bool G = false>
 cudaError_t setup_pair(DevInfo& d) {
-  cudaError_t e = cudaFuncSetAttribute(swb::bwd_kernel<NS, R, kWarpsBwd>,
+  constexpr int m = model_index<NS, G>();
+  cudaError_t e = cudaFuncSetAttribute(swb::bwd_kernel<NS, R, kWarpsBwd, G>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)bwd_smem<NS, R>());
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ[0][NS == 3][R == 4],
-                                                    swb::fwd_kernel<NS, R>, 32 * kWarpsFwd, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ[0][m][R == 4],
+                                                    swb::fwd_kernel<NS, R, G>, 32 * kWarpsFwd, 0);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &d.occ[1][NS == 3][R == 4], swb::bwd_kernel<NS, R, kWarpsBwd>, 32 * kWarpsBwd,
+      &d.occ[1][m][R == 4], swb::bwd_kernel<NS, R, kWarpsBwd, G>, 32 * kWarpsBwd,
       bwd_smem<NS, R>());
 }
 
@@ -134,7 +137,8 @@ int dev_info(DevInfo** out) {
   if (!d.ready) {
     if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       return SWB_ERR_CUDA;
-    if (setup_pair<1, 2>(d) || setup_pair<1, 4>(d) || setup_pair<3, 2>(d) || setup_pair<3, 4>(d))
+    if (setup_pair<1, 2>(d) || setup_pair<1, 4>(d) || setup_pair<3, 2>(d) || setup_pair<3, 4>(d) ||
+        setup_pair<1, 2, true>(d) || setup_pair<1, 4, true>(d))
       return SWB_ERR_CUDA;
     d.ready = true;
   }
@@ -160,7 +164,7 @@ int static_scratch(void** out) {
 }
 
 // Common launch: per-call resets, then the forward and adjoint kernels.
-template <int NS, int R>
+template <int NS, int R, bool G = false>
 int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool clear_map, void* ws,
            size_t ws_bytes, void* stream_v, const swb_options* opt, bool value_only = false) {
   if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
@@ -190,7 +194,8 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
       cudaMemsetAsync(a.map, 0, map_elems * sizeof(float), st) != cudaSuccess)
     return SWB_ERR_CUDA;
 
-  const int of = d->occ[0][NS == 3][R == 4], ob = d->occ[1][NS == 3][R == 4];
+  constexpr int m = model_index<NS, G>();
+  const int of = d->occ[0][m][R == 4], ob = d->occ[1][m][R == 4];
   const int cta_cap_f = d->sms * (of > 0 ? of : 1);
   const int cta_cap_b = d->sms * (ob > 0 ? ob : 1);
   const long long need_f = (ntasks + kWarpsFwd - 1) / kWarpsFwd;
@@ -203,21 +208,21 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   }
   if (grid_f < 1) grid_f = 1;
   if (grid_b < 1) grid_b = 1;
-  swb::fwd_kernel<NS, R><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
+  swb::fwd_kernel<NS, R, G><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   if (opt && opt->split_event &&
       cudaEventRecord(reinterpret_cast<cudaEvent_t>(opt->split_event), st) != cudaSuccess)
     return SWB_ERR_CUDA;
   if (value_only) {
-    swb::value_kernel<NS, R><<<(a.B + 3) / 4, 128, 0, st>>>(a);
+    swb::value_kernel<NS, R, G><<<(a.B + 3) / 4, 128, 0, st>>>(a);
     return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
   }
-  swb::bwd_kernel<NS, R, kWarpsBwd><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS, R>(), st>>>(a);
+  swb::bwd_kernel<NS, R, kWarpsBwd, G><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS, R>(), st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   return SWB_OK;
 }
 
-template <int NS, int R>
+template <int NS, int R, bool G = false>
 int launch_padded_r(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
                     float ge, float T, float* value, float* map, float* g_open, float* g_ext,
                     float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
@@ -234,20 +239,20 @@ int launch_padded_r(const float* scores, const int* lengths, int B, int L1m, int
   a.go = go; a.ge = ge; a.T = T;
   a.nb = l.nb; a.nchunks = l.nchunks;
   a.value = value; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
-  return launch<NS, R>(a, l, (long long)B * l.nb, map_elems, true, ws, ws_bytes, stream, opt);
+  return launch<NS, R, G>(a, l, (long long)B * l.nb, map_elems, true, ws, ws_bytes, stream, opt);
 }
 
-template <int NS>
+template <int NS, bool G = false>
 int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
                   float ge, float T, float* value, float* map, float* g_open, float* g_ext,
                   float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
   const int r = pick_r(opt);
   if (r == 2)
-    return launch_padded_r<NS, 2>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
-                                  g_ext, g_T, ws, ws_bytes, stream, opt);
+    return launch_padded_r<NS, 2, G>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
+                                     g_ext, g_T, ws, ws_bytes, stream, opt);
   if (r == 4)
-    return launch_padded_r<NS, 4>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
-                                  g_ext, g_T, ws, ws_bytes, stream, opt);
+    return launch_padded_r<NS, 4, G>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
+                                     g_ext, g_T, ws, ws_bytes, stream, opt);
   return SWB_ERR_ARG;
 }
 
@@ -265,7 +270,7 @@ Layout value_layout(long long B, long long L1m, long long L2m) {
   return l;
 }
 
-template <int NS>
+template <int NS, bool G = false>
 int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
                  float ge, float T, float* value, void* ws, size_t ws_bytes, void* stream) {
   if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
@@ -279,8 +284,8 @@ int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2
   a.go = go; a.ge = ge; a.T = T;
   a.nb = l.nb; a.nchunks = l.nchunks;
   a.value = value;
-  return launch<NS, kDefaultR>(a, l, (long long)B * l.nb, 0, false, ws, ws_bytes, stream, nullptr,
-                               true);
+  return launch<NS, kDefaultR, G>(a, l, (long long)B * l.nb, 0, false, ws, ws_bytes, stream,
+                                  nullptr, true);
 }
 
 template <int NS>
@@ -583,6 +588,27 @@ int swb_sw_forward(const float* scores, const int* lengths, int B, int L1max, in
                    const swb_options* opt) {
   return launch_padded<1>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, map, grad_gap,
                           nullptr, grad_temp, workspace, workspace_bytes, stream, opt);
+}
+
+size_t swb_nw_workspace_bytes(int B, int L1max, int L2max) { return swb_sw_workspace_bytes(B, L1max, L2max); }
+
+int swb_nw_forward(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
+                   float temp, float* value, float* map, float* grad_gap, float* grad_temp,
+                   void* workspace, size_t workspace_bytes, void* stream,
+                   const swb_options* opt) {
+  return launch_padded<1, true>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, map,
+                                grad_gap, nullptr, grad_temp, workspace, workspace_bytes, stream,
+                                opt);
+}
+
+size_t swb_nw_value_workspace_bytes(int B, int L1max, int L2max) {
+  return swb_sw_value_workspace_bytes(B, L1max, L2max);
+}
+
+int swb_nw_value(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
+                 float temp, float* value, void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_value<1, true>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, workspace,
+                               workspace_bytes, stream);
 }
 
 int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const long long* offsets,

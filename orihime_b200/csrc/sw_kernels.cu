@@ -331,6 +331,13 @@ __device__ __forceinline__ void two_sum(float a, float b, float& h, float& l) {
   l = (a - (h - bb)) + (b - bb);
 }
 
+// n * g as an exact pair (the global-alignment boundaries A[i,0] = i * gap,
+// A[0,j] = j * gap in the scaled domain; n < 2^24 is exact in float).
+__device__ __forceinline__ void nmul(int n, float g, float& h, float& l) {
+  h = (float)n * g;
+  l = fmaf((float)n, g, -h);
+}
+
 // Adjoint fields of column c in one step's shared-memory entry `ent`, stored
 // column block by column block; inside a block each field group is one
 // vector per lane (lane-contiguous, so every warp access is conflict-free).
@@ -400,13 +407,19 @@ __device__ __forceinline__ void get_inits(const float* ent, int lane, int c, flo
 // probability flow exactly; beta-init = exp2(min(x - S, 0)) for the first
 // `nlive` columns, 0 beyond.  Returns (warp-uniform) whether the inits were
 // written; when not, every one of them is 0.
-template <int NS, int R, bool WT = false>
+//
+// G (global alignment, NS == 1 only): A = LSE(diag + s, up + g, left + g),
+// no local start, no beta-inits.  `hold` (a row before the lane's first)
+// keeps (ph, pl) at the row-0 boundary values and writes zero weights, so the
+// boundary cells neither change nor push.
+template <int NS, int R, bool WT = false, bool G = false>
 __device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R],
                                           const float (&lfh)[NS], const float (&lfl)[NS],
                                           const float (&dgh0)[NS], const float (&dgl0)[NS],
                                           const float (&s)[R], float g0, float g1,
                                           float Sh = 0.f, float Sl = 0.f, int nlive = 0,
-                                          float* went = nullptr, int lane = 0) {
+                                          float* went = nullptr, int lane = 0, bool hold = false) {
+  static_assert(!G || NS == 1, "global alignment is built for the linear model");
   float dgh[NS], dgl[NS], lh[NS], ll[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) { dgh[q] = dgh0[q]; dgl[q] = dgl0[q]; lh[q] = lfh[q]; ll[q] = lfl[q]; }
@@ -445,6 +458,26 @@ __device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       dgh[0] = uMh; dgl[0] = uMl; dgh[1] = uIh; dgl[1] = uIl; dgh[2] = uDh; dgl[2] = uDl;
       lh[0] = Mh; ll[0] = Ml; lh[1] = Ih; ll[1] = Il; lh[2] = Dh; ll[2] = Dl;
       ph[0][c] = Mh; pl[0][c] = Ml; ph[1][c] = Ih; pl[1][c] = Il; ph[2][c] = Dh; pl[2][c] = Dl;
+    } else if constexpr (G) {
+      const float uh = ph[0][c], ul = pl[0][c];
+      // A = LSE(diag + s, up + g, left + g), reference point from hi parts
+      const float r = fmaxf(dgh[0] + s[c], fmaxf(uh + g0, lh[0] + g0));
+      const float va = ((dgh[0] - r) + s[c]) + dgl[0];
+      const float vu = ((uh - r) + g0) + ul;
+      const float vl = ((lh[0] - r) + g0) + ll[0];
+      const float ta = ex2(va), tu = ex2(vu), tl = ex2(vl);
+      const float sm = (ta + tu) + tl;
+      float Ah, Al;
+      fast2(r, lg2(sm), Ah, Al);
+      if (hold) { Ah = uh; Al = ul; }
+      if constexpr (WT) {
+        const float v = hold ? 0.f : recip(sm);
+        put_weights<NS, R>(went, lane, c, make_float4(ta * v, ta * v, tu * v, tl * v),
+                           make_float4(0.f, 0.f, 0.f, 0.f), s[c]);
+      }
+      dgh[0] = uh; dgl[0] = ul;
+      lh[0] = Ah; ll[0] = Al;
+      ph[0][c] = Ah; pl[0][c] = Al;
     } else {
       const float uh = ph[0][c], ul = pl[0][c];
       // A = LSE(diag + s, up + g, left + g, s), reference point from hi parts
@@ -467,7 +500,7 @@ __device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       ph[0][c] = Ah; pl[0][c] = Al;
     }
   }
-  if constexpr (WT) {
+  if constexpr (WT && !G) {
     // beta-init exp2(min(x - S, 0)) of the first `nlive` columns.  The lo
     // parts stay below ~2.1 (lo of M carries lg2 of a sum of at most four
     // terms <= 1), so a hi part below S - 135 gives an exponent below -130
@@ -501,7 +534,13 @@ __device__ __forceinline__ int band_chunks(int L1) { return (L1 + 31 + C_STEPS -
 // forward band task
 // ---------------------------------------------------------------------------
 
-template <int NS, int R>
+// G: global alignment (see fwd_cells).  Lanes start from the row-0 boundary,
+// band 0's lane 0 takes A[i,0] = i * gap as its left input, and instead of
+// partition partials the band holding the pair's last column writes the
+// terminal value A[L1,L2] (hi, lo) to its partial slot.  The chunk maximum
+// becomes a marker: +1e30 for the chunk holding the terminal, NEG elsewhere,
+// so the adjoint's quiet-chunk test sees the one beta-init there is.
+template <int NS, int R, bool G = false>
 __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadline) {
   using D = Dims<NS, R>;
   constexpr int NE = D::NE;
@@ -512,12 +551,13 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
   const int col0 = band * 32 * R;
   float* part = a.part + 2 * (size_t)slot;
   if (!(L1 > 0 && col0 < L2)) {
-    if (lane == 0) { part[0] = 0.f; part[1] = (band == 0) ? 1.f : 0.f; }
+    if (!G && lane == 0) { part[0] = 0.f; part[1] = (band == 0) ? 1.f : 0.f; }
     return;
   }
   const int jl = col0 + lane * R;
   const float k = a.k, g0 = a.go * k, g1 = a.ge * k;
   const size_t Lm = (size_t)w.Lm;
+  const bool term_lane = G && jl < L2 && L2 <= jl + R;   // holds the pair's last column
   float* eout = a.edge + w.ed0 + (size_t)band * w.edb;
   const float* ein = (band > 0) ? eout - w.edb : nullptr;
   const bool fault = a.fault_inject && band > 0;
@@ -534,18 +574,26 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
 #pragma unroll
     for (int c = 0; c < R; ++c) { ph[q][c] = NEG; pl[q][c] = 0.f; }
   }
+  if constexpr (G) {   // row 0: A[0,j] = j * gap; lh = A[0, jl] (left of the lane)
+    nmul(jl, g0, lh[0], ll[0]);
+#pragma unroll
+    for (int c = 0; c < R; ++c) nmul(jl + c + 1, g0, ph[0][c], pl[0][c]);
+  }
   float ref = 0.f;
   KSum acc;
-  if (band == 0 && lane == 0) acc.s = 1.f;  // the M[0,0] = 0 origin term
+  if (!G && band == 0 && lane == 0) acc.s = 1.f;  // the M[0,0] = 0 origin term
 
   // Lane u < C holds the left band's edge values that lane 0 needs at step u
-  // of a chunk, loaded one chunk ahead; lane 0 takes them by shuffle.
+  // of a chunk, loaded one chunk ahead; lane 0 takes them by shuffle.  Band 0
+  // of a global alignment takes the column-0 boundary i * gap instead.
+  const bool left_bnd = G && band == 0 && !fault;
   float eb[NE], ebn[NE];
   auto load_edge = [&](int kc, float (&dst)[NE]) {
     const int i = kc * C_STEPS + lane + 1;  // lane 0's row at step kc*C + lane
     const bool ok = ein && lane < C_STEPS && i <= L1;
 #pragma unroll
     for (int f = 0; f < NE; ++f) dst[f] = ok ? ld_poll(ein + f * Lm + (i - 1)) : 0.f;
+    if (left_bnd) nmul(i, g0, dst[0], dst[1]);
   };
   load_edge(0, eb);
   float sb[PF][R];  // per-lane score ring, PF steps ahead
@@ -600,7 +648,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
         }
       }
       if (lane == 0) {
-        const bool take = act && (ein || fault);
+        const bool take = act && (ein || fault || left_bnd);
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
           xh[q] = take ? ev[q] : NEG;
@@ -619,6 +667,26 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
       {
         const int ip = i + PF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
+      }
+      if constexpr (G) {
+        fwd_cells<NS, R, false, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, 0.f, 0.f, 0, nullptr,
+                                      lane, i < 1);
+        if (act) {
+          if (term_lane && i == L1) {   // the terminal cell A[L1, L2]
+            float th = 0.f, tl = 0.f;
+#pragma unroll
+            for (int c = 0; c < R; ++c)
+              if (jl + c == L2 - 1) { th = ph[0][c]; tl = pl[0][c]; }
+            part[0] = th;
+            part[1] = tl;
+            cmx = 1e30f;
+          }
+          if (lane == 31) {
+            eout[(i - 1)] = ph[0][R - 1];
+            eout[Lm + (i - 1)] = pl[0][R - 1];
+          }
+        }
+        continue;
       }
       fwd_cells<NS, R>(ph, pl, lh, ll, dgh, dgl, s, g0, g1);
       if (act) {
@@ -659,6 +727,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
     for (int o = 16; o > 0; o >>= 1) cmx = fmaxf(cmx, __shfl_xor_sync(FULL, cmx, o));
     if (keep_ck && lane == 0) ck[(size_t)kc * D::CKRS + D::CKF * 32] = cmx;
   }
+  if constexpr (G) return;
   // warp-combine (ref, sum) pairs
   float s_ = acc.s;
 #pragma unroll
@@ -672,7 +741,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
   if (lane == 0) { part[0] = ref; part[1] = s_; }
 }
 
-template <int NS, int R>
+template <int NS, int R, bool G = false>
 __global__ void __launch_bounds__(128) fwd_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
@@ -682,7 +751,7 @@ __global__ void __launch_bounds__(128) fwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 0, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    fwd_band<NS, R>(a, place_of<NS, R>(a, task, false), lane, deadline);
+    fwd_band<NS, R, G>(a, place_of<NS, R>(a, task, false), lane, deadline);
   }
 }
 
@@ -729,10 +798,25 @@ __device__ __forceinline__ void pair_logz(const Args& a, const Place& w, int lan
   }
 }
 
+// Global alignment: S' = the terminal value the band holding column L2 wrote,
+// or (L1 + L2) * gap when a side is empty (the terminal is a boundary cell).
+template <int R>
+__device__ __forceinline__ void pair_term(const Args& a, const Place& w, float& Sh, float& Sl) {
+  const int L1 = w.pr.L1, L2 = w.pr.L2;
+  if (L1 == 0 || L2 == 0) {
+    nmul(L1 + L2, a.go * a.k, Sh, Sl);
+    return;
+  }
+  const float* q = a.part + 2 * (w.slot0 + (L2 - 1) / (32 * R));
+  Sh = q[0];
+  Sl = q[1];
+}
+
 // Value-only calls: one warp per pair folds the forward's band partials into
 // S, as finish_pair does after a full adjoint (4 warps per CTA).  Only the
-// pair's band count and first partial slot are needed.
-template <int NS, int R>
+// pair's band count and first partial slot (and, for a global alignment, its
+// lengths) are needed.
+template <int NS, int R, bool G = false>
 __global__ void __launch_bounds__(128) value_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * 4 + (threadIdx.x >> 5);
@@ -745,15 +829,29 @@ __global__ void __launch_bounds__(128) value_kernel(Args a) {
     w.p = q;
     w.nb = (int)pw[PW_NB];
     w.slot0 = (size_t)pw[PW_SLOT0];
+    w.pr.L1 = (int)pw[PW_L1];
+    w.pr.L2 = (int)pw[PW_L2];
   }
   float Sh, Sl;
+  if constexpr (G) {
+    if (lane == 0) {
+      const int n = w.pr.L1 + w.pr.L2;
+      if (w.pr.L1 == 0 || w.pr.L2 == 0) {
+        a.value[w.p] = (float)n * a.go;   // exactly the boundary cell's value
+      } else {
+        pair_term<R>(a, w, Sh, Sl);
+        a.value[w.p] = (Sh + Sl) * (1.f / a.k);
+      }
+    }
+    return;
+  }
   pair_logz(a, w, lane, Sh, Sl);
   if (lane == 0) a.value[w.p] = (Sh + Sl) * (1.f / a.k);
 }
 
 // Last band task of a pair to finish folds the per-band gradient partials (in
 // band order, so the result is deterministic) into the outputs.
-template <int NS>
+template <int NS, bool G = false>
 __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, float Sl,
                             float g0sum, float g1sum, float pssum) {
   const int p = w.p;
@@ -774,6 +872,15 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
       const float inv_k = 1.f / a.k;          // = T * ln 2
       const float S = (Sh + Sl) * inv_k;
       const float match = ps * inv_k;
+      if (G && (w.pr.L1 == 0 || w.pr.L2 == 0)) {
+        // the terminal is the boundary cell (L1 + L2) * gap: dS/dgap = L1 + L2, dS/dT = 0
+        const int n = w.pr.L1 + w.pr.L2;
+        a.value[p] = (float)n * a.go;
+        a.g_open[p] = (float)n;
+        if (a.g_ext) a.g_ext[p] = 0.f;
+        a.g_T[p] = 0.f;
+        return;
+      }
       a.value[p] = S;
       if (NS == 3) {
         a.g_open[p] = o;
@@ -799,7 +906,11 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
 // cell's beta = beta-init + pushes received, and it pushes beta * weight to
 // each predecessor: within the lane through registers, to the left lane
 // through __shfl_down_sync, to the left band through the push buffer.
-template <int NS, int R>
+//
+// G (global alignment): the only beta-init is beta = 1 at the terminal cell
+// A[L1, L2]; pushes that leave the grid into the row-0 and column-0 boundary
+// cells (values j * gap and i * gap) add index * push to dS/dgap there.
+template <int NS, int R, bool G = false>
 __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uint64_t deadline) {
   using D = Dims<NS, R>;
   constexpr int NP = D::NP, EW = D::EW, CKF = D::CKF, CKRS = D::CKRS, NE = D::NE;
@@ -808,12 +919,14 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
   const int band = w.band;
   const int col0 = band * 32 * R;
   float Sh, Sl;
-  pair_logz(a, w, lane, Sh, Sl);
+  if constexpr (G) pair_term<R>(a, w, Sh, Sl);
+  else pair_logz(a, w, lane, Sh, Sl);
   if (!(L1 > 0 && col0 < L2)) {
-    finish_pair<NS>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f);
+    finish_pair<NS, G>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f);
     return;
   }
   const int jl = col0 + lane * R;
+  const bool term_lane = G && jl < L2 && L2 <= jl + R;   // holds the pair's last column
   const int ncols = min(max(L2 - jl, 0), R);  // columns of this lane inside the pair
   const float k = a.k, g0 = a.go * k, g1 = a.ge * k;
   const size_t Lm = (size_t)w.Lm;
@@ -840,6 +953,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
     const bool ok = ein && lane < C_STEPS && i <= L1;
 #pragma unroll
     for (int f = 0; f < NE; ++f) ebr[f] = ok ? ein[f * Lm + (i - 1)] : (f < NS ? NEG : 0.f);
+    if (G && band == 0) nmul(i, g0, ebr[0], ebr[1]);   // column-0 boundary i * gap
   };
   auto load_pb = [&](int kc, float (&dst)[NP]) {
     const int i = kc * C_STEPS + C_STEPS - 1 - lane - 30;  // lane 31's row at step end-1-lane
@@ -1023,8 +1137,8 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
         const int ip = i + PF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
-      if (fwd_cells<NS, R, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, Sh, Sl, act ? ncols : 0,
-                                 sm + (size_t)cu * EW * 32, lane))
+      if (fwd_cells<NS, R, true, G>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, Sh, Sl, act ? ncols : 0,
+                                    sm + (size_t)cu * EW * 32, lane, G && i < 1))
         initbits |= 1u << cu;
     }
     if (kc > 0) {  // prefetch the next chunk's inputs while the adjoint runs
@@ -1091,6 +1205,13 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
       } else {
         ac[0][R - 1] += inL[0] + inD[0];
       }
+      if constexpr (G) {
+        if (term_lane && i == L1) {   // beta = 1 at the terminal cell
+#pragma unroll
+          for (int c = 0; c < R; ++c)
+            if (jl + c == L2 - 1) ac[0][c] += 1.f;
+        }
+      }
 #pragma unroll
       for (int q = 0; q < NP; ++q) outp[q] = 0.f;
       float pm[R];
@@ -1137,6 +1258,12 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
           const float pU = b * f0.z, pL = b * f0.w, pD = b * f0.y;
           cA += pU + pL;
           cS += pv_ * sc;
+          if constexpr (G) {
+            // pushes into the boundary: row 0 (up to column j, diag to j - 1)
+            // and column 0 (left to row i, diag to row i - 1)
+            if (i == 1) cA += (float)(jl + c + 1) * pU + (float)(jl + c) * pD;
+            if (band == 0 && lane == 0 && c == 0) cA += (float)i * pL + (float)(i - 1) * pD;
+          }
           nx[0][c] += pU;
           if (c > 0) {
             nx[0][c - 1] += pD;
@@ -1181,7 +1308,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
   }
-  finish_pair<NS>(a, w, lane, Sh, Sl, v0, v1, v2);
+  finish_pair<NS, G>(a, w, lane, Sh, Sl, v0, v1, v2);
 }
 
 // Shared memory per adjoint warp (floats): one chunk of adjoint fields.
@@ -1190,7 +1317,7 @@ __host__ __device__ constexpr int bwd_smem_floats() {
   return C_STEPS * Dims<NS, R>::EW * 32;
 }
 
-template <int NS, int R, int WARPS>
+template <int NS, int R, int WARPS, bool G = false>
 __global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31;
@@ -1203,7 +1330,7 @@ __global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    bwd_band<NS, R>(a, place_of<NS, R>(a, task, true), lane, sm, deadline);
+    bwd_band<NS, R, G>(a, place_of<NS, R>(a, task, true), lane, sm, deadline);
   }
 }
 

@@ -195,6 +195,16 @@ SW_AFFINE = Family(
     value=lambda *a: torch.ops.orihime_b200.sw_affine_value(*a),
 )
 
+NW = Family(
+    "nw", ("gap", "temp"),
+    forward=lambda *a: _ops().nw_forward(*a),
+    grads=lambda *a: _ops().nw_value_grad_params(*a),
+    hvp=lambda *a: _ops().nw_marginals_hvp(*a),
+    sens=(lambda *a: _ops().nw_marginals_grad_gap(*a),
+          lambda *a: _ops().nw_marginals_grad_temp(*a)),
+    value=lambda *a: torch.ops.orihime_b200.nw_value(*a),
+)
+
 
 # ---------------------------------------------------------------------------
 # autograd functions
@@ -279,7 +289,8 @@ class _EntropyFn(torch.autograd.Function):
 # ---------------------------------------------------------------------------
 
 class Operator:
-    """One soft Smith-Waterman family with map / value / entropy observables."""
+    """One soft alignment family (Smith-Waterman or Needleman-Wunsch) with map /
+    value / entropy observables."""
 
     def __init__(self, fam: Family, primary_name: str = "pair_scores"):
         self.fam = fam

@@ -6,12 +6,13 @@ directory under /tmp, compiles the reference's CPU extension there with g++
 (the source list of meson.build's ``cpp_sources``), imports it, and records
 the public soft Smith-Waterman API's outputs on small seeded inputs:
 
-* ``ohm.sw`` / ``sw_value`` / ``sw_entropy`` and the ``sw_affine`` trio:
-  forward results and the gradients of value, map (against a fixed cotangent)
-  and entropy with respect to the pair scores;
+* ``ohm.sw`` / ``sw_value`` / ``sw_entropy``, the ``sw_affine`` trio and the
+  global-alignment ``nw`` trio: forward results and the gradients of value,
+  map (against a fixed cotangent) and entropy with respect to the pair scores;
 * lengths-ragged and boolean-mask batches;
 * tensor-valued (learnable) gap parameters and their gradients;
-* ``ohm.ops.sw*.backward`` (map VJP) and ``.sensitivity`` (parameter fields).
+* ``ohm.ops.sw*.backward`` / ``ohm.ops.nw.backward`` (map VJP) and
+  ``.sensitivity`` (parameter fields).
 
 Output: ``sw_golden.npz`` (float32 arrays, a few hundred KB).
 
@@ -107,9 +108,11 @@ def main() -> None:
             put(f"{name}/lengths", lt)
         for fam, kw in (("lin", dict(gap_score=-1.0, temperature=0.7)),
                         ("aff", dict(gap_open_score=-2.0, gap_extend_score=-0.5,
-                                     temperature=0.7))):
-            fmap, fval, fent = ((ohm.sw, ohm.sw_value, ohm.sw_entropy) if fam == "lin"
-                                else (ohm.sw_affine, ohm.sw_affine_value, ohm.sw_affine_entropy))
+                                     temperature=0.7)),
+                        ("nw", dict(gap_score=-1.0, temperature=0.7))):
+            fmap, fval, fent = {"lin": (ohm.sw, ohm.sw_value, ohm.sw_entropy),
+                                "aff": (ohm.sw_affine, ohm.sw_affine_value, ohm.sw_affine_entropy),
+                                "nw": (ohm.nw, ohm.nw_value, ohm.nw_entropy)}[fam]
             key = f"{name}/{fam}"
             x = x0.clone().requires_grad_(True)
             v = fval(x, lengths=lt, **kw)
@@ -126,7 +129,7 @@ def main() -> None:
             (g,) = torch.autograd.grad(h.sum(), x)
             put(f"{key}/entropy", h)
             put(f"{key}/dentropy", g)
-            op = ohm.ops.sw if fam == "lin" else ohm.ops.sw_affine
+            op = {"lin": ohm.ops.sw, "aff": ohm.ops.sw_affine, "nw": ohm.ops.nw}[fam]
             sens = op.sensitivity(x0, lengths=lt, **kw)
             for k2, t in sens.items():
                 put(f"{key}/sens_{k2}", t)
@@ -142,12 +145,13 @@ def main() -> None:
     mask[1, 2, 3] = True
     put("mask/scores", x0)
     put("mask/mask", mask.to(torch.int32))
-    for fam in ("lin", "aff"):
+    for fam in ("lin", "aff", "nw"):
         x = x0.clone().requires_grad_(True)
-        if fam == "lin":
+        if fam in ("lin", "nw"):
             gp = torch.tensor(-1.0, requires_grad=True)
             tp = torch.tensor(0.8, requires_grad=True)
-            v = ohm.sw_value(x, gap_score=gp, temperature=tp, mask=mask)
+            fv = ohm.sw_value if fam == "lin" else ohm.nw_value
+            v = fv(x, gap_score=gp, temperature=tp, mask=mask)
             grads = torch.autograd.grad(v.sum(), (x, gp, tp))
             names = ("dx", "dgap", "dtemp")
         else:
@@ -161,8 +165,8 @@ def main() -> None:
         put(f"mask/{fam}/value", v)
         for n_, g_ in zip(names, grads):
             put(f"mask/{fam}/{n_}", g_)
-        m = (ohm.sw if fam == "lin" else ohm.sw_affine)(
-            x0, mask=mask, **(dict(gap_score=-1.0, temperature=0.8) if fam == "lin" else
+        m = {"lin": ohm.sw, "aff": ohm.sw_affine, "nw": ohm.nw}[fam](
+            x0, mask=mask, **(dict(gap_score=-1.0, temperature=0.8) if fam != "aff" else
                              dict(gap_open_score=-2.0, gap_extend_score=-0.5, temperature=0.8)))
         put(f"mask/{fam}/map", m)
 

@@ -71,6 +71,28 @@ def test_linear_oracle_vs_golden(golden, case):
     _close((cot * sens[1]).sum(), g("bw_temperature"), atol=1e-4)
 
 
+@pytest.mark.parametrize("case", CASES)
+def test_nw_oracle_vs_golden(golden, case):
+    """Global alignment (ohm.nw trio, ohm.ops.nw) against the recorded fixtures."""
+    s, ln, cot = _case(golden, case)
+    g = lambda k: golden[f"{case}/nw/{k}"]
+    B = s.shape[0]
+    o = O.nw(s, ln, -1.0, T0)
+    _close(o["value"], g("value"))
+    _close(o["map"], g("map"))
+    _close(-o["map"] / B, g("dvalue"))
+    _close(o["grad_temp"], g("entropy"), atol=2e-5)
+    sens = {p: O.nw_param_grad(s, ln, -1.0, T0, p) for p in range(2)}
+    _close(sens[0], g("sens_gap_score"), atol=1e-5)
+    _close(sens[1], g("sens_temperature"), atol=1e-5)
+    _close(sens[1], g("dentropy"), atol=1e-5)
+    hv = O.nw_hvp(s, cot, ln, -1.0, T0)
+    _close(hv, g("dmap"), atol=1e-5)
+    _close(hv, g("bw_pair_scores"), atol=1e-5)
+    _close((cot * sens[0]).sum(), g("bw_gap_score"), atol=1e-4)
+    _close((cot * sens[1]).sum(), g("bw_temperature"), atol=1e-4)
+
+
 def _mask_sentinel(scores, mask, T):
     """orihime/operator.py:334-386: masked cells -> amax - (sum(shape[1:])*80 + 200)*T."""
     x = np.where(mask, -np.inf, scores).astype(np.float32)
@@ -98,6 +120,12 @@ def test_masked_batches_vs_golden(golden):
     _close(o["grad_gap"].sum(), golden["mask/lin/dgap"], atol=1e-4)
     _close(o["grad_temp"].sum(), golden["mask/lin/dtemp"], atol=1e-4)
     assert np.all(o["map"][mask] == 0.0)
+    o = O.nw(x, None, -1.0, 0.8)
+    _close(o["value"], golden["mask/nw/value"])
+    _close(o["map"], golden["mask/nw/map"])
+    _close(o["map"], golden["mask/nw/dx"])
+    _close(o["grad_gap"].sum(), golden["mask/nw/dgap"], atol=1e-4)
+    _close(o["grad_temp"].sum(), golden["mask/nw/dtemp"], atol=1e-4)
 
 
 def test_fp64_oracle_close_to_fp32(golden):
@@ -137,6 +165,13 @@ def test_oracle_bit_exact_vs_reference_kernels(seed):
             for p in range(2):
                 assert np.array_equal(O.linear_param_grad(s, lens, -1.0, T, p),
                                       O.ref_linear_param_grad(s, lens, -1.0, T, p))
+            a, r = O.nw(s, lens, -1.0, T), O.ref_nw(s, lens, -1.0, T)
+            for k in a:
+                assert np.array_equal(a[k], r[k]), k
+            assert np.array_equal(O.nw_hvp(s, V, lens, -1.0, T), O.ref_nw_hvp(s, V, lens, -1.0, T))
+            for p in range(2):
+                assert np.array_equal(O.nw_param_grad(s, lens, -1.0, T, p),
+                                      O.ref_nw_param_grad(s, lens, -1.0, T, p))
 
 
 def test_finite_difference_of_fp64_value():
@@ -158,3 +193,22 @@ def test_finite_difference_of_fp64_value():
     fd = (O.affine(s, None, -2.0, -0.5, 0.5 + eps, dtype=np.float64)["value"][0] -
           O.affine(s, None, -2.0, -0.5, 0.5 - eps, dtype=np.float64)["value"][0]) / (2 * eps)
     assert abs(fd - base["grad_temp"][0]) < 1e-5
+
+
+def test_nw_finite_differences_of_fp64_value():
+    """Global alignment: the map, dS/dgap (boundary cells included) and dS/dT
+    against central differences of the FP64 oracle's value."""
+    rng = np.random.default_rng(6)
+    s = rng.standard_normal((1, 5, 8))
+    ln = np.array([[5, 6]], np.int32)
+    f = lambda x, g, t: O.nw(x, ln, g, t, dtype=np.float64)["value"][0]
+    base = O.nw(s, ln, -0.7, 0.6, dtype=np.float64)
+    eps = 1e-5
+    for (i, j) in [(0, 0), (2, 3), (4, 5), (3, 1)]:
+        sp, sm = s.copy(), s.copy()
+        sp[0, i, j] += eps
+        sm[0, i, j] -= eps
+        assert abs((f(sp, -0.7, 0.6) - f(sm, -0.7, 0.6)) / (2 * eps) - base["map"][0, i, j]) < 1e-6
+    assert abs((f(s, -0.7 + eps, 0.6) - f(s, -0.7 - eps, 0.6)) / (2 * eps) - base["grad_gap"][0]) < 1e-6
+    assert abs((f(s, -0.7, 0.6 + eps) - f(s, -0.7, 0.6 - eps)) / (2 * eps) - base["grad_temp"][0]) < 1e-5
+    assert np.all(base["map"][0, 5:, :] == 0) and np.all(base["map"][0, :, 6:] == 0)

@@ -1,4 +1,4 @@
-"""Meta (fake) shapes and vmap argument checks of the 15 ops, on the CPU
+"""Meta (fake) shapes and vmap argument checks of the namespaced ops, on the CPU
 (reference registrations: orihime/_compile.py:25-140, orihime/_ops.py:178-406)."""
 
 import pytest
@@ -14,7 +14,7 @@ LIN = (-1.0, 0.5)
 
 @pytest.fixture(scope="module", autouse=True)
 def _defined_here():
-    if len(_ops.DEFINED_HERE) != 15:
+    if len(_ops.DEFINED_HERE) != len(_ops.SCHEMAS):
         pytest.skip("the reference extension defined the schemas; its package registers these")
 
 
@@ -38,6 +38,11 @@ def test_fake_shapes_of_all_ops():
     assert [g.shape for g in o.sw_marginals_backward(s, s, *LIN, None)] == [(3, 5, 7), (1,), (1,)]
     assert [g.shape for g in o.sw_affine_marginals_backward(s, s, *AFF, None)] == \
         [(3, 5, 7), (1,), (1,), (1,)]
+    v, m = o.nw_forward(s, *LIN, None)
+    assert v.shape == (3,) and m.shape == (3, 5, 7)
+    v, m = o.nw_forward_t(s, t, t, ln)
+    assert v.shape == (3,) and m.shape == (3, 5, 7)
+    assert [g.shape for g in o.nw_value_grad_params(s, *LIN, None)] == [(3,)] * 2
 
 
 def test_vmap_rejects_a_mapped_scalar_parameter():
@@ -60,6 +65,7 @@ def test_fake_shapes_of_value_only_ops():
     s = torch.empty(3, 5, 7, device="meta")
     assert torch.ops.orihime_b200.sw_value(s, *LIN, None).shape == (3,)
     assert torch.ops.orihime_b200.sw_affine_value(s, *AFF, None).shape == (3,)
+    assert torch.ops.orihime_b200.nw_value(s, *LIN, None).shape == (3,)
 
 
 def test_legacy_schemas_defined():
