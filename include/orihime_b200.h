@@ -261,6 +261,24 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
                           size_t workspace_bytes, void* stream);
 
 /*
+ * Global alignment (soft Needleman–Wunsch, linear gap) second-order ops on the
+ * same band wavefront; workspace from swb_nw_aux_workspace_bytes.
+ * swb_nw_hvp replaces soft_nw_hvp_cuda (src/nw/torch_cuda.cpp:442, launcher
+ * nw_hvp src/nw/kernels_gpu.cuh:258); grad_tangents [B][4] = tangents of
+ * (dS/dgap, dS/dT, 0, S), dS/dgap including the boundary cells, for
+ * soft_nw_backward_full_cuda (:603).  swb_nw_param_jacobian (param 0 = gap,
+ * 1 = temp) replaces soft_nw_param_jacobian_cuda (:509, launcher nw_param_grad
+ * src/nw/kernels_gpu.cuh:285).
+ */
+size_t swb_nw_aux_workspace_bytes(int B, int L1max, int L2max);
+int swb_nw_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
+               int L2max, float gap, float temp, float* out, float* grad_tangents,
+               void* workspace, size_t workspace_bytes, void* stream);
+int swb_nw_param_jacobian(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap, float temp, int param, float* out, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
+/*
  * One pass over a [B, per_item] fp32 tensor for the Python prelude's input
  * checks (replaces the reference's separate full-tensor passes in
  * orihime/operator.py:249-386: isposinf().any(), the domain mask .all(),

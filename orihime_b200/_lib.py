@@ -116,6 +116,12 @@ def load() -> ctypes.CDLL:
     lib.swb_nw_value_workspace_bytes.argtypes = [i, i, i]
     lib.swb_nw_value.restype = i
     lib.swb_nw_value.argtypes = [vp, vp, i, i, i, f, f, vp, vp, sz, vp]
+    lib.swb_nw_aux_workspace_bytes.restype = sz
+    lib.swb_nw_aux_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_nw_hvp.restype = i
+    lib.swb_nw_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, vp, vp, vp, sz, vp]
+    lib.swb_nw_param_jacobian.restype = i
+    lib.swb_nw_param_jacobian.argtypes = [vp, vp, i, i, i, f, f, i, vp, vp, sz, vp]
     lib.swb_mufu_probe.restype = i
     lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()

@@ -49,6 +49,11 @@ SCHEMAS = {
     "nw_forward": "nw_forward(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor[]",
     "nw_forward_t": "nw_forward_t(Tensor scores, Tensor gap, Tensor temp, Tensor lengths) -> Tensor[]",
     "nw_value_grad_params": "nw_value_grad_params(Tensor scores, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor)",
+    # src/nw/registry.cpp:48-51
+    "nw_marginals_backward": "nw_marginals_backward(Tensor scores, Tensor grad_marginals, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
+    "nw_marginals_hvp": "nw_marginals_hvp(Tensor scores, Tensor v, float gap, float temp, Tensor? lengths) -> Tensor",
+    "nw_marginals_grad_gap": "nw_marginals_grad_gap(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
+    "nw_marginals_grad_temp": "nw_marginals_grad_temp(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
 }
 
 _INT32_MAX = 2**31 - 1
@@ -357,12 +362,20 @@ def _check_like(scores, other, name, msg_shape):
 AUX_BUDGET_MAX = 16 << 30
 
 
-def _aux_plan(aff, B, L1, L2, dev):
+_AUX = {  # family -> (workspace bytes, HVP, parameter Jacobian) entry points
+    "sw": ("swb_sw_aux_workspace_bytes", "swb_sw_hvp", "swb_sw_param_jacobian"),
+    "sw_affine": ("swb_sw_affine_aux_workspace_bytes", "swb_sw_affine_hvp",
+                  "swb_sw_affine_param_jacobian"),
+    "nw": ("swb_nw_aux_workspace_bytes", "swb_nw_hvp", "swb_nw_param_jacobian"),
+}
+
+
+def _aux_plan(fam, B, L1, L2, dev):
     """(pairs per group, workspace bytes) for a second-order call: the field
     table of the band wavefront is about 100 (affine) / 50 (linear) bytes per
     cell, so large batches are split to stay within min(AUX_BUDGET_MAX,
     max(2 GiB, half the free device memory))."""
-    fn = _LIB.swb_sw_affine_aux_workspace_bytes if aff else _LIB.swb_sw_aux_workspace_bytes
+    fn = getattr(_LIB, _AUX[fam][0])
     nbytes = int(fn(B, L1, L2))
     free = torch.cuda.mem_get_info(dev)[0]
     budget = min(AUX_BUDGET_MAX, max(2 << 30, free // 2))
@@ -388,17 +401,16 @@ def run_hvp(fam, scores, v, lengths, params, want_grads=False):
     gt = torch.zeros(B, 4, dtype=torch.float32, device=dev) if want_grads else None
     if B == 0:
         return out, gt
-    aff = fam == "sw_affine"
-    g, nbytes = _aux_plan(aff, B, L1, L2, dev)
+    g, nbytes = _aux_plan(fam, B, L1, L2, dev)
     ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
-    fn = _LIB.swb_sw_affine_hvp if aff else _LIB.swb_sw_hvp
+    fn = getattr(_LIB, _AUX[fam][1])
     with torch.cuda.device(dev):
         for b0, b1 in _groups(B, g):
             ln = None if lengths is None else lengths[b0:b1]
             rc = fn(_ptr(scores[b0:b1]), _ptr(v[b0:b1]), _ptr(ln), b1 - b0, L1, L2, *map(float, params),
                     _ptr(out[b0:b1]), _ptr(None if gt is None else gt[b0:b1]), _ptr(ws), nbytes,
                     _stream(dev))
-            _lib.check(rc, "soft Smith-Waterman HVP")
+            _lib.check(rc, _AUX[fam][1])
     return out, gt
 
 
@@ -408,16 +420,15 @@ def run_param_jacobian(fam, scores, lengths, params, which):
     out = torch.empty_like(scores)
     if B == 0:
         return out
-    aff = fam == "sw_affine"
-    g, nbytes = _aux_plan(aff, B, L1, L2, dev)
+    g, nbytes = _aux_plan(fam, B, L1, L2, dev)
     ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
-    fn = _LIB.swb_sw_affine_param_jacobian if aff else _LIB.swb_sw_param_jacobian
+    fn = getattr(_LIB, _AUX[fam][2])
     with torch.cuda.device(dev):
         for b0, b1 in _groups(B, g):
             ln = None if lengths is None else lengths[b0:b1]
             rc = fn(_ptr(scores[b0:b1]), _ptr(ln), b1 - b0, L1, L2, *map(float, params), int(which),
                     _ptr(out[b0:b1]), _ptr(ws), nbytes, _stream(dev))
-            _lib.check(rc, "soft Smith-Waterman parameter Jacobian")
+            _lib.check(rc, _AUX[fam][2])
     return out
 
 
@@ -495,7 +506,37 @@ def sw_marginals_backward(scores, grad_marginals, gap, temp, lengths):
     return out, tot[0:1].clone(), tot[1:2].clone()
 
 
+def nw_marginals_hvp(scores, v, gap, temp, lengths):
+    """orihime::nw_marginals_hvp (src/nw/torch_cuda.cpp:758 -> soft_nw_hvp_cuda :442)."""
+    check_input_cuda(scores, "scores")
+    _check_like(scores, v, "tangent", "scores and tangent must have same shape")
+    ln = _prep(scores, lengths, "nw")
+    return run_hvp("nw", scores, v, ln, (gap, temp))[0]
+
+
+def _nw_param(which):
+    def op(scores, gap, temp, lengths):
+        ln = _prep(scores, lengths, "nw")
+        return run_param_jacobian("nw", scores, ln, (gap, temp), which)
+    op.__doc__ = (f"orihime::nw_marginals_grad_* param {which} "
+                  "(src/nw/torch_cuda.cpp:769-790 -> soft_nw_param_jacobian_cuda :509)")
+    return op
+
+
+def nw_marginals_backward(scores, grad_marginals, gap, temp, lengths):
+    """orihime::nw_marginals_backward -> (grad_scores, d/dgap [1], d/dT [1])
+    (src/nw/torch_cuda.cpp:747 -> soft_nw_backward_full_cuda :603); one
+    tangent pass along the cotangent, as for the local alignment."""
+    out, gt = marginals_backward_per_pair("nw", scores, grad_marginals, (gap, temp), lengths)
+    tot = gt[:, :2].sum(0)
+    return out, tot[0:1].clone(), tot[1:2].clone()
+
+
 IMPLS = {
+    "nw_marginals_hvp": nw_marginals_hvp,
+    "nw_marginals_grad_gap": _nw_param(0),
+    "nw_marginals_grad_temp": _nw_param(1),
+    "nw_marginals_backward": nw_marginals_backward,
     "sw_marginals_hvp": sw_marginals_hvp,
     "sw_marginals_grad_gap": _linear_param(0),
     "sw_marginals_grad_temp": _linear_param(1),
@@ -599,11 +640,13 @@ for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True
 
 
 # ---------------------------------------------------------------------------
-# legacy soft_sw* ops (src/sw/registry.cpp:30-35, src/sw_affine/registry.cpp:27-32)
+# legacy soft_sw* / soft_nw* ops (src/sw/registry.cpp:30-35,
+# src/sw_affine/registry.cpp:27-32, src/nw/registry.cpp:34-39)
 # ---------------------------------------------------------------------------
-# The reference keeps 12 older schemas beside the namespaced ones; its Python
+# The reference keeps 18 older schemas beside the namespaced ones; its Python
 # package no longer calls them.  Each is one of the namespaced op bodies under
-# another name (src/sw*/torch_cuda.cpp:803-830, :917-946).  They are defined
+# another name (src/sw*/torch_cuda.cpp:803-830, :917-946,
+# src/nw/torch_cuda.cpp:795-821).  They are defined
 # and given CUDA kernels only when orihime_b200 defines the schemas itself:
 # with the reference extension loaded first, they stay the reference's own.
 
@@ -631,6 +674,16 @@ LEGACY_SCHEMAS = {
     "soft_sw_affine_backward_full": "soft_sw_affine_backward_full(Tensor scores, Tensor grad_alignment, "
                                     "float gap_open, float gap_ext, float temperature, Tensor? lengths) "
                                     "-> (Tensor, Tensor, Tensor, Tensor)",
+    "soft_nw": "soft_nw(Tensor scores, Tensor gap, Tensor temperature, Tensor lengths) -> Tensor[]",
+    "soft_nw_float": "soft_nw_float(Tensor scores, float gap, float temperature, Tensor? lengths) -> Tensor[]",
+    "soft_nw_with_grads": "soft_nw_with_grads(Tensor scores, float gap, float temperature, Tensor? lengths) "
+                          "-> (Tensor, Tensor, Tensor, Tensor)",
+    "soft_nw_hvp": "soft_nw_hvp(Tensor scores, Tensor tangent, float gap, float temperature, Tensor? lengths) "
+                   "-> Tensor",
+    "soft_nw_param_jacobian": "soft_nw_param_jacobian(Tensor scores, int param_type, float gap, "
+                              "float temperature, Tensor? lengths) -> Tensor",
+    "soft_nw_backward_full": "soft_nw_backward_full(Tensor scores, Tensor grad_alignment, float gap, "
+                             "float temperature, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
 }
 LEGACY_DEFINED_HERE = []
 if DEFINED_HERE:
@@ -645,15 +698,23 @@ def _legacy_with_grads_linear(scores, gap, temperature, lengths):
     return tuple(run_linear(scores, ln, gap, temperature))
 
 
+def _legacy_with_grads_nw(scores, gap, temperature, lengths):
+    ln = _prep(scores, lengths, "nw")
+    return tuple(run_linear(scores, ln, gap, temperature, family="nw"))
+
+
 def _legacy_with_grads_affine(scores, gap_open, gap_ext, temperature, lengths):
     ln = _prep(scores, lengths, "sw_affine")
     return tuple(run_affine(scores, ln, gap_open, gap_ext, temperature))
 
 
 def _legacy_jacobian(fam, nparams):
+    # messages of src/sw/torch_cuda.cpp:528, src/sw_affine/torch_cuda.cpp:591, src/nw/torch_cuda.cpp:519
+    msg = "param_type must be 0 or 1" if nparams == 2 else "param_type must be 0, 1, or 2"
+
     def op(scores, param_type, *rest):
         if not 0 <= int(param_type) < nparams:
-            raise RuntimeError(f"param_type must be in [0, {nparams}), got {param_type}")
+            raise RuntimeError(msg)
         *params, lengths = rest
         ln = _prep(scores, lengths, fam)
         return run_param_jacobian(fam, scores, ln, tuple(params), int(param_type))
@@ -673,11 +734,18 @@ LEGACY_IMPLS = {
     "soft_sw_affine_hvp": sw_affine_marginals_hvp,
     "soft_sw_affine_param_jacobian": _legacy_jacobian("sw_affine", 3),
     "soft_sw_affine_backward_full": sw_affine_marginals_backward,
+    "soft_nw_float": nw_forward,
+    "soft_nw": nw_forward_t,
+    "soft_nw_with_grads": _legacy_with_grads_nw,
+    "soft_nw_hvp": nw_marginals_hvp,
+    "soft_nw_param_jacobian": _legacy_jacobian("nw", 2),
+    "soft_nw_backward_full": nw_marginals_backward,
 }
 for _name in LEGACY_DEFINED_HERE:
     _IMPL_LIB.impl(_name, LEGACY_IMPLS[_name], "CUDA")
 for _name, _fam, _t in (("soft_sw_float", "sw", False), ("soft_sw", "sw", True),
-                        ("soft_sw_affine_float", "sw_affine", False), ("soft_sw_affine", "sw_affine", True)):
+                        ("soft_sw_affine_float", "sw_affine", False), ("soft_sw_affine", "sw_affine", True),
+                        ("soft_nw_float", "nw", False), ("soft_nw", "nw", True)):
     if _name in LEGACY_DEFINED_HERE:   # differentiable like the reference (AutogradCUDA)
         _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
 

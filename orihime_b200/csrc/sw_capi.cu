@@ -373,9 +373,9 @@ struct XOcc {
   int f = 0, b = 0;
   bool ready = false;
 };
-XOcc g_xocc[64][2][2][4];   // [device][affine?][R == 4?][mode]
+XOcc g_xocc[64][3][2][4];   // [device][model: linear, affine, global linear][R == 4?][mode]
 
-template <int NS, int R, int MODE>
+template <int NS, int R, int MODE, bool G = false>
 int launch_xband_r(swb::XArgs a, cudaStream_t st) {
   DevInfo* d = nullptr;
   int rc = dev_info(&d);
@@ -383,14 +383,14 @@ int launch_xband_r(swb::XArgs a, cudaStream_t st) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWB_ERR_CUDA;
   const size_t smem = sizeof(float) * swb::XSTAGES * swb::xstep_floats<NS, R>();
-  XOcc& o = g_xocc[dev][NS == 3][R == 4][MODE];
+  XOcc& o = g_xocc[dev][model_index<NS, G>()][R == 4][MODE];
   {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!o.ready) {
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.f, swb::xfwd_kernel<NS, R, MODE>, 128, 0) !=
-              cudaSuccess ||
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.b, swb::xbwd_kernel<NS, R, MODE>, 32, smem) !=
-              cudaSuccess)
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.f, swb::xfwd_kernel<NS, R, MODE, G>, 128,
+                                                        0) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.b, swb::xbwd_kernel<NS, R, MODE, G>, 32,
+                                                        smem) != cudaSuccess)
         return SWB_ERR_CUDA;
       o.ready = true;
     }
@@ -400,12 +400,12 @@ int launch_xband_r(swb::XArgs a, cudaStream_t st) {
   const long long cap_b = (long long)d->sms * (o.b > 0 ? o.b : 1);
   const int grid_f = (int)std::min((ntasks + 3) / 4, cap_f);
   const int grid_b = (int)std::min(ntasks, cap_b);
-  swb::xfwd_kernel<NS, R, MODE><<<grid_f, 128, 0, st>>>(a);
-  swb::xbwd_kernel<NS, R, MODE><<<grid_b, 32, smem, st>>>(a);
+  swb::xfwd_kernel<NS, R, MODE, G><<<grid_f, 128, 0, st>>>(a);
+  swb::xbwd_kernel<NS, R, MODE, G><<<grid_b, 32, smem, st>>>(a);
   return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
 }
 
-template <int NS, int MODE>
+template <int NS, int MODE, bool G = false>
 int launch_xband(const float* scores, const float* v, const int* lengths, int B, int L1m, int L2m,
                  float go, float ge, float T, float* out, float* gt, void* ws, size_t ws_bytes,
                  void* stream_v) {
@@ -439,7 +439,7 @@ int launch_xband(const float* scores, const float* v, const int* lengths, int B,
   a.bpush = reinterpret_cast<float*>(w + l.off_bpush);
   a.fld = reinterpret_cast<float*>(w + l.off_fld);
   a.spin_limit_ns = 20ull * 1000000000ull;
-  return l.R == 4 ? launch_xband_r<NS, 4, MODE>(a, st) : launch_xband_r<NS, 2, MODE>(a, st);
+  return l.R == 4 ? launch_xband_r<NS, 4, MODE, G>(a, st) : launch_xband_r<NS, 2, MODE, G>(a, st);
 }
 
 }  // namespace
@@ -494,6 +494,31 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
   }
 }
 
+
+size_t swb_nw_aux_workspace_bytes(int B, int L1max, int L2max) {
+  return swb_sw_aux_workspace_bytes(B, L1max, L2max);
+}
+
+int swb_nw_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max, int L2max,
+               float gap, float temp, float* out, float* grad_tangents, void* workspace,
+               size_t workspace_bytes, void* stream) {
+  return launch_xband<1, swb::AUX_HVP, true>(scores, v, lengths, B, L1max, L2max, gap, 0.f, temp,
+                                             out, grad_tangents, workspace, workspace_bytes, stream);
+}
+
+int swb_nw_param_jacobian(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap, float temp, int param, float* out, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+  switch (param) {
+    case 0: return launch_xband<1, swb::AUX_P0, true>(scores, nullptr, lengths, B, L1max, L2max, gap,
+                                                      0.f, temp, out, nullptr, workspace,
+                                                      workspace_bytes, stream);
+    case 1: return launch_xband<1, swb::AUX_PT, true>(scores, nullptr, lengths, B, L1max, L2max, gap,
+                                                      0.f, temp, out, nullptr, workspace,
+                                                      workspace_bytes, stream);
+    default: return SWB_ERR_ARG;
+  }
+}
 
 size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;

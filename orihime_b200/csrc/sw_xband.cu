@@ -211,11 +211,33 @@ __device__ __forceinline__ void xcell3(const float (&dh)[3], const float (&dl)[3
 // One linear cell: o = (Ah, Al, U); fields
 //   f0 = (w_diag, w_up, w_left, w_diag + w_start)
 //   f1 = (dw_diag, dw_up, dw_left, dw_diag + dw_start)   f2 = (Ah, Al, U, 0)
-template <int MODE>
+// GL (global alignment): no start term, map factor w_diag.
+template <int MODE, bool GL = false>
 __device__ __forceinline__ void xcell1(float dh, float dl, float du, float uh, float ul, float uu,
                                        float lh, float ll, float lu, float s, float vv, float g,
                                        float iT, float (&o)[3], float4 (&f)[3]) {
   constexpr bool TM = (MODE == AUX_PT);
+  if constexpr (GL) {
+    // A = LSE(diag + s, up + g, left + g)
+    const float r = fmaxf(dh + s, fmaxf(uh + g, lh + g));
+    const float ta = ex2(((dh - r) + s) + dl), tu = ex2(((uh - r) + g) + ul);
+    const float tl = ex2(((lh - r) + g) + ll);
+    const float sm = (ta + tu) + tl;
+    float Ah, Al;
+    fast2(r, lg2(sm), Ah, Al);
+    const float v = recip(sm);
+    const float w[3] = {ta * v, tu * v, tl * v};
+    float c[3] = {du, uu, lu};
+    if (MODE == AUX_HVP) c[0] += vv;
+    if (MODE == AUX_P0) { c[1] += 1.f; c[2] += 1.f; }
+    float dw[3];
+    const float U = xwtan<3, TM>(w, c, iT, dw);
+    o[0] = Ah; o[1] = Al; o[2] = U;
+    f[0] = make_float4(w[0], w[1], w[2], w[0]);
+    f[1] = make_float4(dw[0], dw[1], dw[2], dw[0]);
+    f[2] = make_float4(Ah, Al, U, 0.f);
+    return;
+  }
   // A = LSE(diag + s, up + g, left + g, s)
   const float r = fmaxf(fmaxf(dh + s, uh + g), fmaxf(lh + g, s));
   const float ta = ex2(((dh - r) + s) + dl), tu = ex2(((uh - r) + g) + ul);
@@ -252,8 +274,15 @@ __device__ __forceinline__ void xcombine(float& r1, float& s1, float& u1, float&
 // forward band task
 // ---------------------------------------------------------------------------
 
-template <int NS, int R, int MODE>
+// GL: global alignment (NS == 1).  Rows start from the row-0 boundary j * gap
+// (tangent j along the gap, else 0) and band 0 takes the column-0 boundary
+// i * gap; a row before the lane's first keeps the boundary and writes zero
+// fields.  The band holding the pair's last column writes the terminal
+// (hi, lo, U) to its partial slot; the chunk maximum is a marker, +1e30 in
+// the chunk holding the terminal and NEG elsewhere.
+template <int NS, int R, int MODE, bool GL = false>
 __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t deadline) {
+  static_assert(!GL || NS == 1, "global alignment is built for the linear model");
   using XS = XShape<NS>;
   constexpr int G = XS::G, NE = XS::NE;
   constexpr int XSTEP = xstep_floats<NS, R>();
@@ -264,7 +293,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
   float* part = a.part + 4 * slot;
   const int col0 = band * 32 * R;
   if (!(L1 > 0 && col0 < L2)) {
-    if (lane == 0) { part[0] = 0.f; part[1] = (band == 0) ? 1.f : 0.f; part[2] = 0.f; part[3] = 0.f; }
+    if (!GL && lane == 0) { part[0] = 0.f; part[1] = (band == 0) ? 1.f : 0.f; part[2] = 0.f; part[3] = 0.f; }
     return;
   }
   const Pair ps = xpair_of(a, p, L1, L2, a.scores, nullptr);
@@ -284,18 +313,35 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
 #pragma unroll
     for (int c = 0; c < R; ++c) { ph[q][c] = NEG; pl[q][c] = 0.f; pu[q][c] = 0.f; }
   }
+  constexpr bool GAPDIR = (MODE == AUX_P0);   // tangent of a boundary n * gap is n
+  if constexpr (GL) {
+    nmul(jl, g0, lh[0], ll[0]);
+    lu[0] = GAPDIR ? (float)jl : 0.f;
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      nmul(jl + c + 1, g0, ph[0][c], pl[0][c]);
+      pu[0][c] = GAPDIR ? (float)(jl + c + 1) : 0.f;
+    }
+  }
+  const bool term_lane = GL && jl < L2 && L2 <= jl + R;   // holds the pair's last column
   float ref = 0.f, su = 0.f, sx = 0.f;
   KSum acc;
-  if (band == 0 && lane == 0) acc.s = 1.f;  // origin M[0,0] = 0: weight 1, U 0, log term 0
+  if (!GL && band == 0 && lane == 0) acc.s = 1.f;  // origin M[0,0] = 0: weight 1, U 0, log term 0
 
   // Lane u < XC holds the left band's edge values that lane 0 needs at step u
-  // of a chunk, loaded one chunk ahead; lane 0 takes them by shuffle.
+  // of a chunk, loaded one chunk ahead; lane 0 takes them by shuffle.  Band 0
+  // of a global alignment takes the column-0 boundary instead.
+  const bool left_bnd = GL && band == 0;
   float eb[NE], ebn[NE];
   auto load_edge = [&](int kc, float (&dst)[NE]) {
     const int i = kc * XC + lane + 1;
     const bool ok = ein && lane < XC && i <= L1;
 #pragma unroll
     for (int f = 0; f < NE; ++f) dst[f] = ok ? ld_poll(ein + f * Lm + (i - 1)) : 0.f;
+    if (left_bnd) {
+      nmul(i, g0, dst[0], dst[1]);
+      dst[2] = GAPDIR ? (float)i : 0.f;
+    }
   };
   load_edge(0, eb);
   float sb[XPF][R], vb[XPF][R];
@@ -342,7 +388,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
           for (int f = 0; f < NE; ++f) ev[f] = x.v[f];
         }
         if (lane == 0) {
-          const bool take = act && ein;
+          const bool take = act && (ein || left_bnd);
 #pragma unroll
           for (int q = 0; q < NS; ++q) {
             xh[q] = take ? ev[q] : NEG;
@@ -397,8 +443,13 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
             const float uh = ph[0][c], ul = pl[0][c], uu = pu[0][c];
             float o[3];
             float4 f[3];
-            xcell1<MODE>(dgh[0], dgl[0], dgu[0], uh, ul, uu, wh[0], wl[0], wu[0], s[c], vv[c], g0,
-                         iT, o, f);
+            xcell1<MODE, GL>(dgh[0], dgl[0], dgu[0], uh, ul, uu, wh[0], wl[0], wu[0], s[c], vv[c],
+                             g0, iT, o, f);
+            if (GL && i < 1) {   // boundary row: keep the values, no fields
+              o[0] = uh; o[1] = ul; o[2] = uu;
+#pragma unroll
+              for (int g = 0; g < G; ++g) f[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
 #pragma unroll
             for (int g = 0; g < G; ++g) reinterpret_cast<float4*>(Fs + (c * G + g) * 128)[lane] = f[g];
             dgh[0] = uh; dgl[0] = ul; dgu[0] = uu;
@@ -406,7 +457,22 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
             ph[0][c] = o[0]; pl[0][c] = o[1]; pu[0][c] = o[2];
           }
         }
-        if (act) {
+        if (GL && act) {
+          if (term_lane && i == L1) {   // the terminal A[L1, L2] with its tangent
+            float th = 0.f, tl = 0.f, tu = 0.f;
+#pragma unroll
+            for (int c = 0; c < R; ++c)
+              if (jl + c == L2 - 1) { th = ph[0][c]; tl = pl[0][c]; tu = pu[0][c]; }
+            part[0] = th; part[1] = tl; part[2] = tu; part[3] = 0.f;
+            cmx = 1e30f;
+          }
+          if (lane == 31) {
+            eout[(i - 1)] = ph[0][R - 1];
+            eout[Lm + (i - 1)] = pl[0][R - 1];
+            eout[2 * Lm + (i - 1)] = pu[0][R - 1];
+          }
+        }
+        if (!GL && act) {
           // partition with its U- and log-weighted sums, lazily rescaled:
           // exponents stay <= 8 so (hi - ref) + lo rounds at <= 2^-21
           float mx = NEG;
@@ -455,6 +521,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
     for (int o = 16; o > 0; o >>= 1) cmx = fmaxf(cmx, __shfl_xor_sync(FULL, cmx, o));
     if (lane == 0) cm[kc] = cmx;
   }
+  if constexpr (GL) return;
   // warp-combine the lanes' tuples (fixed shuffle tree: deterministic)
   float s_ = acc.s;
 #pragma unroll
@@ -466,7 +533,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
   if (lane == 0) { part[0] = ref; part[1] = s_; part[2] = su; part[3] = sx; }
 }
 
-template <int NS, int R, int MODE>
+template <int NS, int R, int MODE, bool GL = false>
 __global__ void __launch_bounds__(128, SWB_XFWD_MINB) xfwd_kernel(XArgs a) {
   const int lane = threadIdx.x & 31;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
@@ -477,7 +544,7 @@ __global__ void __launch_bounds__(128, SWB_XFWD_MINB) xfwd_kernel(XArgs a) {
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
     const int p = task / a.nb;
-    xfwd_band<NS, R, MODE>(a, p, task - p * a.nb, lane, deadline);
+    xfwd_band<NS, R, MODE, GL>(a, p, task - p * a.nb, lane, deadline);
   }
 }
 
@@ -486,9 +553,25 @@ __global__ void __launch_bounds__(128, SWB_XFWD_MINB) xfwd_kernel(XArgs a) {
 // ---------------------------------------------------------------------------
 
 // S' = Sh + Sl (scaled) and dS of pair p from its bands' forward tuples.
-template <bool TM>
+// GL: the terminal tuple of the band holding the last column; an empty side
+// leaves the boundary (L1 + L2) * gap (the caller then returns early).
+template <bool TM, int R = 0, bool GL = false>
 __device__ __forceinline__ void xpair_stats(const XArgs& a, int p, int lane, float& Sh, float& Sl,
                                             float& dS) {
+  if constexpr (GL) {
+    int L1, L2;
+    xlengths(a, p, L1, L2);
+    if (L1 == 0 || L2 == 0) {
+      nmul(L1 + L2, a.go * a.k, Sh, Sl);
+      dS = 0.f;
+      return;
+    }
+    const float* q = a.part + 4 * ((size_t)p * a.nb + (L2 - 1) / (32 * R));
+    Sh = q[0];
+    Sl = q[1];
+    dS = q[2];
+    return;
+  }
   float ref = NEG, s = 0.f, su = 0.f, sx = 0.f;
   for (int b = lane; b < a.nb; b += 32) {
     const float* q = a.part + 4 * ((size_t)p * a.nb + b);
@@ -567,7 +650,9 @@ __device__ void xfinish(const XArgs& a, int p, int band, int lane, bool empty, f
   }
 }
 
-template <int NS, int R, int MODE>
+// GL: the only beta-init is 1 at the terminal (tangent 0); pushes into the
+// row-0 / column-0 boundary add index * tangent to the gap tangent (HVP).
+template <int NS, int R, int MODE, bool GL = false>
 __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring,
                           uint64_t deadline) {
   using XS = XShape<NS>;
@@ -578,7 +663,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   xlengths(a, p, L1, L2);
   const int col0 = band * 32 * R;
   float Sh, Sl, dS;
-  xpair_stats<TM>(a, p, lane, Sh, Sl, dS);
+  xpair_stats<TM, R, GL>(a, p, lane, Sh, Sl, dS);
   if (!(L1 > 0 && col0 < L2)) {
     xfinish<NS, MODE>(a, p, band, lane, L1 == 0 || L2 == 0, dS, 0.f, 0.f, 0.f);
     return;
@@ -587,6 +672,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   const Pair po = xpair_of(a, p, L1, L2, a.scores, a.out);
   const Pair pv = xpair_of(a, p, L1, L2, HV ? a.v : a.scores, nullptr);
   const int jl = col0 + lane * R;
+  const bool term_lane = GL && jl < L2 && L2 <= jl + R;   // holds the pair's last column
   const float iT = 1.f / a.T;
   const size_t Lm = (size_t)a.L1m;
   float* pout = (band > 0) ? a.bpush + slot * NQ * (Lm + 1) : nullptr;
@@ -777,6 +863,11 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
           }
           ac[0][R - 1] += iL + iD;
           at[0][R - 1] += tL + tD;
+          if (GL && term_lane && i == L1) {   // beta = 1 at the terminal
+#pragma unroll
+            for (int c = 0; c < R; ++c)
+              if (jl + c == L2 - 1) ac[0][c] += 1.f;
+          }
         }
 #pragma unroll
         for (int q = 0; q < NQ; ++q) outp[q] = 0.f;
@@ -843,7 +934,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
             // f0 = (w_diag, w_up, w_left, map factor) f1 = their tangents
             // f2 = (Ah, Al, U, 0)
             const float xs = (f[2].x - Sh) + (f[2].y - Sl);
-            const float e0 = live ? ex2(fminf(xs, 0.f)) : 0.f;
+            const float e0 = (!GL && live) ? ex2(fminf(xs, 0.f)) : 0.f;
             const float b = ac[0][c] + e0;
             float x = f[2].z - dS;
             if (TM) x -= (e0 > 0.f ? xs * LN2 : 0.f);
@@ -858,6 +949,10 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
             if (HV) {
               cA += tpU + tpL;
               cC = fmaf(Pd, sc[c], fmaf(P, vv[c], cC));
+              if constexpr (GL) {   // tangents pushed into the boundary cells
+                if (i == 1) cA += (float)(jl + c + 1) * tpU + (float)(jl + c) * tpD;
+                if (band == 0 && lane == 0 && c == 0) cA += (float)i * tpL + (float)(i - 1) * tpD;
+              }
             }
             nx[0][c] += pU;
             nt[0][c] += tpU;
@@ -905,7 +1000,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   xfinish<NS, MODE>(a, p, band, lane, false, dS, v0, v1, v2);
 }
 
-template <int NS, int R, int MODE>
+template <int NS, int R, int MODE, bool GL = false>
 __global__ void __launch_bounds__(32, SWB_XBWD_MINB) xbwd_kernel(XArgs a) {
   extern __shared__ __align__(16) float xring[];
   const int lane = threadIdx.x & 31;
@@ -917,7 +1012,7 @@ __global__ void __launch_bounds__(32, SWB_XBWD_MINB) xbwd_kernel(XArgs a) {
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
     const int p = task / a.nb;
-    xbwd_band<NS, R, MODE>(a, p, a.nb - 1 - (task - p * a.nb), lane, xring, deadline);
+    xbwd_band<NS, R, MODE, GL>(a, p, a.nb - 1 - (task - p * a.nb), lane, xring, deadline);
   }
 }
 

@@ -1,7 +1,8 @@
-"""The 12 legacy soft_sw* ops (src/sw*/registry.cpp, src/sw*/torch_cuda.cpp
-:803-830, :917-946) run the namespaced op bodies under their old names: the
-same results bit for bit, param_type selecting the parameter, autograd
-through the tensor-parameter forward."""
+"""The 18 legacy soft_sw* / soft_nw* ops (src/sw*/registry.cpp,
+src/nw/registry.cpp, src/sw*/torch_cuda.cpp:803-830, :917-946,
+src/nw/torch_cuda.cpp:795-821) run the namespaced op bodies under their old
+names: the same results bit for bit, param_type selecting the parameter,
+autograd through the tensor-parameter forward."""
 
 import pytest
 import torch
@@ -19,7 +20,7 @@ LIN = (-1.0, 0.5)
 def _cuda():
     if not torch.cuda.is_available():
         pytest.skip("CUDA not available")
-    if len(_ops.LEGACY_DEFINED_HERE) != 12:
+    if len(_ops.LEGACY_DEFINED_HERE) != len(_ops.LEGACY_SCHEMAS):
         pytest.skip("the reference extension defined the legacy schemas; they stay its own")
 
 
@@ -58,8 +59,29 @@ def test_legacy_ops_equal_namespaced_ops():
         assert _eq(o.soft_sw_affine_backward_full(s, v, *AFF, lengths),
                    o.sw_affine_marginals_backward(s, v, *AFF, lengths))
         assert _eq(o.soft_sw_backward_full(s, v, *LIN, lengths), o.sw_marginals_backward(s, v, *LIN, lengths))
-    with pytest.raises(RuntimeError, match="param_type must be in"):
+    with pytest.raises(RuntimeError, match="param_type must be 0, 1, or 2"):
         o.soft_sw_affine_param_jacobian(s, 3, *AFF, None)
+    with pytest.raises(RuntimeError, match="param_type must be 0 or 1"):
+        o.soft_nw_param_jacobian(s, 2, *LIN, None)
+
+
+def test_legacy_nw_ops_equal_namespaced_ops():
+    s = _scores(3, 40, 57)
+    v = _scores(3, 40, 57, seed=1)
+    ln = torch.tensor([[40, 57], [13, 9], [0, 30]], dtype=torch.int32).cuda()
+    for lengths in (None, ln):
+        assert _eq(o.soft_nw_float(s, *LIN, lengths), o.nw_forward(s, *LIN, lengths))
+        lg = o.soft_nw_with_grads(s, *LIN, lengths)
+        assert _eq(lg[:2], o.nw_forward(s, *LIN, lengths))
+        assert _eq(lg[2:], o.nw_value_grad_params(s, *LIN, lengths))
+        assert _eq(o.soft_nw_hvp(s, v, *LIN, lengths), o.nw_marginals_hvp(s, v, *LIN, lengths))
+        for k, name in enumerate(("gap", "temp")):
+            assert _eq(o.soft_nw_param_jacobian(s, k, *LIN, lengths),
+                       getattr(o, f"nw_marginals_grad_{name}")(s, *LIN, lengths))
+        assert _eq(o.soft_nw_backward_full(s, v, *LIN, lengths), o.nw_marginals_backward(s, v, *LIN, lengths))
+    full = torch.tensor([[40, 57]] * 3, dtype=torch.int32).cuda()
+    assert _eq(o.soft_nw(s, torch.tensor(-1.0).cuda(), torch.tensor(0.5).cuda(), full),
+               o.nw_forward(s, *LIN, full))
 
 
 def test_legacy_tensor_parameter_forward_is_differentiable():

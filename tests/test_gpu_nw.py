@@ -193,3 +193,135 @@ def test_nw_public_api_vs_golden(golden):
     np.testing.assert_allclose(dx.cpu().numpy(), golden["mask/nw/dx"], atol=1e-5)
     np.testing.assert_allclose(dg.item(), golden["mask/nw/dgap"], atol=1e-4)
     np.testing.assert_allclose(dt.item(), golden["mask/nw/dtemp"], atol=1e-4)
+
+
+# ---- second-order ops: HVP, parameter Jacobians, map VJP --------------------
+
+def _check2(name, got, r32, r64, rel_floor=1e-4):
+    """Bar of the second-order ops: error vs fp64 within the reference's own
+    fp32 error, floor 1e-4 of the largest exact entry."""
+    got, r32, r64 = (np.asarray(x, np.float64) for x in (got, r32, r64))
+    scale = max(float(np.abs(r64).max()), 1e-12)
+    e64 = float(np.abs(got - r64).max())
+    eref = float(np.abs(r32 - r64).max())
+    bound = max(rel_floor * scale, eref)
+    print(f"  {name:14s} ours-fp64 {e64:.2e}  ref32-fp64 {eref:.2e}  bound {bound:.2e}  scale {scale:.2e}")
+    assert e64 <= bound, f"{name}: {e64:.3e} > {bound:.3e}"
+
+
+SECOND = [
+    # (B, L1, L2, lengths or None, gap, T, seed)
+    (2, 24, 31, None, -1.0, 0.7, 1),
+    (4, 10, 12, [[8, 10], [10, 12], [0, 5], [7, 0]], -1.0, 1.0, 2),
+    (2, 64, 48, None, -0.5, 0.3, 3),
+    (1, 130, 300, None, -2.0, 0.5, 4),
+    (3, 5, 7, None, -1.0, 1.0, 7),     # boundary-heavy (below)
+]
+
+
+def _second_inputs(B, L1, L2, seed):
+    s = _gen((B, L1, L2), seed, 1.5)
+    if seed == 7:   # push mass onto the row-0 / column-0 boundary
+        s[:, 0, :] -= 2.5
+        s[:, :, 0] -= 2.5
+    return s, _gen((B, L1, L2), seed + 100)
+
+
+@pytest.mark.parametrize("B,L1,L2,lengths,gap,T,seed", SECOND)
+def test_nw_hvp_matches_oracle(B, L1, L2, lengths, gap, T, seed):
+    s, v = _second_inputs(B, L1, L2, seed)
+    ln = None if lengths is None else torch.tensor(lengths, dtype=torch.int32)
+    lnd = None if ln is None else ln.cuda()
+    lnn = None if ln is None else ln.numpy()
+    got = torch.ops.orihime.nw_marginals_hvp(s.cuda(), v.cuda(), gap, T, lnd).cpu().numpy()
+    _check2("hvp", got, O.nw_hvp(s.numpy(), v.numpy(), lnn, gap, T),
+            O.nw_hvp(s.numpy(), v.numpy(), lnn, gap, T, dtype=np.float64))
+    if lengths is not None:
+        for b, (l1, l2) in enumerate(lengths):
+            assert not got[b, l1:, :].any() and not got[b, :, l2:].any()
+
+
+@pytest.mark.parametrize("B,L1,L2,lengths,gap,T,seed", SECOND)
+@pytest.mark.parametrize("param", [0, 1])
+def test_nw_param_jacobian_matches_oracle(param, B, L1, L2, lengths, gap, T, seed):
+    s, _ = _second_inputs(B, L1, L2, seed)
+    ln = None if lengths is None else torch.tensor(lengths, dtype=torch.int32)
+    lnd = None if ln is None else ln.cuda()
+    lnn = None if ln is None else ln.numpy()
+    fn = (torch.ops.orihime.nw_marginals_grad_gap, torch.ops.orihime.nw_marginals_grad_temp)[param]
+    got = fn(s.cuda(), gap, T, lnd).cpu().numpy()
+    _check2(f"dP/dtheta{param}", got, O.nw_param_grad(s.numpy(), lnn, gap, T, param),
+            O.nw_param_grad(s.numpy(), lnn, gap, T, param, dtype=np.float64))
+
+
+def test_nw_marginals_backward_matches_oracle_contractions():
+    B, L1, L2, gap, T = 3, 37, 145, -0.8, 0.6
+    s, gm = _second_inputs(B, L1, L2, 11)
+    ln = torch.tensor([[37, 145], [20, 45], [37, 9]], dtype=torch.int32)
+    sn, gn, lnn = s.numpy(), gm.numpy(), ln.numpy()
+    out = torch.ops.orihime.nw_marginals_backward(s.cuda(), gm.cuda(), gap, T, ln.cuda())
+    _check2("grad_scores", out[0].cpu().numpy(), O.nw_hvp(sn, gn, lnn, gap, T),
+            O.nw_hvp(sn, gn, lnn, gap, T, dtype=np.float64))
+    for k in range(2):
+        r64 = (gn.astype(np.float64) * O.nw_param_grad(sn, lnn, gap, T, k, dtype=np.float64)).sum()
+        r32 = (gn.astype(np.float64) * O.nw_param_grad(sn, lnn, gap, T, k)).sum()
+        got = float(out[1 + k].item())
+        bound = max(abs(r32 - r64), 1e-4 * (1 + abs(r64)))
+        print(f"  param {k}: ours {got:.6f} fp64 {r64:.6f} ref32 {r32:.6f}")
+        assert abs(got - r64) <= bound
+
+
+def test_nw_second_order_deterministic_and_grouped():
+    s, v = _second_inputs(5, 70, 200, 21)
+    s, v = s.cuda(), v.cuda()
+    a = torch.ops.orihime.nw_marginals_hvp(s, v, -1.0, 0.8, None)
+    b = torch.ops.orihime.nw_marginals_hvp(s, v, -1.0, 0.8, None)
+    assert torch.equal(a, b)
+    for k in range(5):   # pairs are independent: one call per pair gives the same bits
+        assert torch.equal(torch.ops.orihime.nw_marginals_hvp(s[k:k + 1].contiguous(), v[k:k + 1].contiguous(),
+                                                              -1.0, 0.8, None), a[k:k + 1])
+
+
+def test_nw_public_api_second_order_vs_golden(golden):
+    import orihime_b200 as ob
+    for case in ("sq", "rect", "ragged", "unit", "row"):
+        s = torch.from_numpy(golden[f"{case}/scores"]).cuda()
+        cot = torch.from_numpy(golden[f"{case}/cot"]).cuda()
+        ln = (torch.from_numpy(golden[f"{case}/lengths"]).to(torch.int32).cuda()
+              if f"{case}/lengths" in golden.files else None)
+        g = lambda k: golden[f"{case}/nw/{k}"]  # noqa: E731
+        kw = dict(gap_score=-1.0, temperature=0.7, lengths=ln)
+        x = s.clone().requires_grad_(True)
+        (dm,) = torch.autograd.grad((ob.nw(x, **kw) * cot).sum(), x)
+        np.testing.assert_allclose(dm.cpu().numpy(), g("dmap"), atol=1e-5)
+        x = s.clone().requires_grad_(True)
+        (de,) = torch.autograd.grad(ob.nw_entropy(x, **kw).sum(), x)
+        np.testing.assert_allclose(de.cpu().numpy(), g("dentropy"), atol=1e-5)
+        args = (s, -1.0, 0.7, ln)
+        np.testing.assert_allclose(torch.ops.orihime.nw_marginals_grad_gap(*args).cpu().numpy(),
+                                   g("sens_gap_score"), atol=1e-5)
+        np.testing.assert_allclose(torch.ops.orihime.nw_marginals_grad_temp(*args).cpu().numpy(),
+                                   g("sens_temperature"), atol=1e-5)
+        bw = torch.ops.orihime.nw_marginals_backward(s, cot, -1.0, 0.7, ln)
+        np.testing.assert_allclose(bw[0].cpu().numpy(), g("bw_pair_scores"), atol=1e-5)
+        np.testing.assert_allclose(bw[1].item(), g("bw_gap_score"), atol=1e-4)
+        np.testing.assert_allclose(bw[2].item(), g("bw_temperature"), atol=1e-4)
+
+
+def test_nw_tensor_parameter_forward_backward():
+    """orihime::nw_forward_t through AutogradCUDA: value and map cotangents reach
+    the scores and both tensor parameters (value x grads + map VJP)."""
+    s = _gen((2, 30, 41), 31, 1.5).cuda().requires_grad_(True)
+    ln = torch.tensor([[30, 41], [22, 17]], dtype=torch.int32).cuda()
+    gp = torch.tensor(-0.9, device="cuda", requires_grad=True)
+    tp = torch.tensor(0.7, device="cuda", requires_grad=True)
+    v, m = torch.ops.orihime.nw_forward_t(s, gp, tp, ln)
+    cot = _gen((2, 30, 41), 32).cuda()
+    (v.sum() + (m * cot).sum()).backward()
+    sd = s.detach()
+    gg, gT = torch.ops.orihime.nw_value_grad_params(sd, -0.9, 0.7, ln)
+    mb = torch.ops.orihime.nw_marginals_backward(sd, cot, -0.9, 0.7, ln)
+    vm = torch.ops.orihime.nw_forward(sd, -0.9, 0.7, ln)[1]
+    assert torch.allclose(s.grad, vm + mb[0], rtol=1e-5, atol=1e-6)
+    assert torch.allclose(gp.grad, gg.sum() + mb[1][0], rtol=1e-5, atol=1e-5)
+    assert torch.allclose(tp.grad, gT.sum() + mb[2][0], rtol=1e-5, atol=1e-5)

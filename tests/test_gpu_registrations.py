@@ -1,4 +1,4 @@
-"""vmap, autocast and torch.compile through the registrations of the 15 ops,
+"""vmap, autocast and torch.compile through the registrations of the namespaced ops,
 on the GPU (reference: orihime/_ops.py:178-406, orihime/_compile.py:323-452)."""
 
 import pytest
@@ -17,7 +17,7 @@ LIN = (-1.0, 0.5)
 def _cuda():
     if not torch.cuda.is_available():
         pytest.skip("CUDA not available")
-    if len(_ops.DEFINED_HERE) != 15:
+    if len(_ops.DEFINED_HERE) != len(_ops.SCHEMAS):
         pytest.skip("the reference extension defined the schemas; its package registers these")
 
 
@@ -78,3 +78,15 @@ def test_torch_compile_fullgraph_matches_eager():
 
     got = torch.compile(loss, fullgraph=True)(s)
     assert torch.allclose(got, loss(s), rtol=1e-6, atol=1e-5)
+
+
+def test_vmap_global_alignment_ops_match_per_element_calls():
+    s = _scores(2, 3, 29, 41)
+    v = _scores(2, 3, 29, 41, seed=2)
+    val, mp = torch.func.vmap(lambda a: o.nw_forward(a, *LIN, None))(s)
+    h = torch.func.vmap(lambda a, b: o.nw_marginals_hvp(a, b, *LIN, None))(s, v)
+    for k in range(2):
+        v1, m1 = o.nw_forward(s[k].contiguous(), *LIN, None)
+        assert torch.equal(val[k], v1) and torch.equal(mp[k], m1)
+        assert torch.allclose(h[k], o.nw_marginals_hvp(s[k].contiguous(), v[k].contiguous(), *LIN, None),
+                              rtol=1e-5, atol=1e-7)

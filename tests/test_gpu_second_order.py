@@ -215,7 +215,7 @@ def test_pair_groups_match_single_call(monkeypatch):
     want, want_gt = _ops.run_hvp("sw_affine", s, v, ln, (*AFF, 0.6), want_grads=True)
     want_p = _ops.run_param_jacobian("sw", s, ln, (*LIN, 0.6), 1)
     monkeypatch.setattr(_ops, "AUX_BUDGET_MAX", 1)
-    assert _ops._aux_plan(True, 5, 40, 70, s.device)[0] == 1
+    assert _ops._aux_plan("sw_affine", 5, 40, 70, s.device)[0] == 1
     got, got_gt = _ops.run_hvp("sw_affine", s, v, ln, (*AFF, 0.6), want_grads=True)
     got_p = _ops.run_param_jacobian("sw", s, ln, (*LIN, 0.6), 1)
     assert torch.equal(got, want) and torch.equal(got_gt, want_gt) and torch.equal(got_p, want_p)

@@ -38,6 +38,10 @@ def test_fake_shapes_of_all_ops():
     assert [g.shape for g in o.sw_marginals_backward(s, s, *LIN, None)] == [(3, 5, 7), (1,), (1,)]
     assert [g.shape for g in o.sw_affine_marginals_backward(s, s, *AFF, None)] == \
         [(3, 5, 7), (1,), (1,), (1,)]
+    assert o.nw_marginals_hvp(s, s, *LIN, None).shape == (3, 5, 7)
+    for name in ("nw_marginals_grad_gap", "nw_marginals_grad_temp"):
+        assert getattr(o, name)(s, *LIN, None).shape == (3, 5, 7)
+    assert [g.shape for g in o.nw_marginals_backward(s, s, *LIN, None)] == [(3, 5, 7), (1,), (1,)]
     v, m = o.nw_forward(s, *LIN, None)
     assert v.shape == (3,) and m.shape == (3, 5, 7)
     v, m = o.nw_forward_t(s, t, t, ln)
@@ -69,8 +73,13 @@ def test_fake_shapes_of_value_only_ops():
 
 
 def test_legacy_schemas_defined():
-    """The 12 legacy soft_sw* schemas (src/sw/registry.cpp:30-35,
-    src/sw_affine/registry.cpp:27-32) exist beside the namespaced ones."""
+    """The 18 legacy soft_sw* / soft_nw* schemas (src/sw/registry.cpp:30-35,
+    src/sw_affine/registry.cpp:27-32, src/nw/registry.cpp:34-39) exist beside
+    the namespaced ones."""
     assert sorted(_ops.LEGACY_DEFINED_HERE) == sorted(_ops.LEGACY_SCHEMAS)
     for name in _ops.LEGACY_SCHEMAS:
         assert getattr(o, name).default._schema.name == f"orihime::{name}"
+
+
+def test_legacy_schema_count():
+    assert len(_ops.LEGACY_SCHEMAS) == 18
