@@ -38,7 +38,7 @@ MUFU_PER_CELL = 21      # algorithmic MUFU ops per cell, forward 11 + adjoint 10
 MUFU_PER_CELL_BWD = 10  # adjoint kernel alone
 BYTES_PER_CELL = 8      # compulsory HBM bytes per cell (score read + map write)
 E2E_PARTS = 8           # pair groups of the end-to-end pipeline
-BWD_DRAM_BYTES_PER_CELL = 18.21  # measured adjoint DRAM traffic: scores + checkpoints + map
+BWD_DRAM_BYTES_PER_CELL = 13.33  # measured adjoint DRAM traffic: scores + checkpoints + map
 
 
 def workload_lengths(seed: int, n: int = NPAIRS) -> np.ndarray:
@@ -369,11 +369,12 @@ def second_order(args):
 # ---------------------------------------------------------------------------
 
 def global_alignment(args):
-    """Soft Needleman-Wunsch (linear gap) at two shapes: 64 pairs of
+    """Soft Needleman-Wunsch (linear gap) at three workloads: 64 pairs of
     1024 x 1024 (scores 3 <e_i, f_j> / sqrt(64), gap -1, T 0.5) for the
-    forward + adjoint (value, map, dS/dgap, dS/dT) and the value alone, and
+    forward + adjoint (value, map, dS/dgap, dS/dT) and the value alone;
     256 pairs of 512 x 512 (N(0, 1) embeddings, d = 128) for the HVP, dP/dT
-    and the map's full VJP.  Through the C ABI with buffers allocated once,
+    and the map's full VJP; and the contract line's ragged batch (4096
+    pairs) as one packed plan, forward + adjoint and value alone.  Through the C ABI with buffers allocated once,
     CUDA events on the launching stream, `--warmup` untimed and `--steps`
     timed calls each.  The reference's CPU kernels (src/nw/kernels_cpu.cpp)
     run 2 of the 64 pairs on all host threads for the CPU line.  Prints one
@@ -445,6 +446,22 @@ def global_alignment(args):
         ms = timed(fn)
         res[name] = {"ms": round(ms, 3), "gcups": round(c5 / ms / 1e6, 2), "shape": [B5, N5, N5]}
     del s5, v5, out, wx
+
+    # the bench's ragged batch (4096 pairs, log-uniform 32..2048, seed 3) as one packed plan
+    from orihime_b200 import ragged
+    lengths = workload_lengths(3)
+    offsets, ln32 = ragged.layout(lengths)
+    flat = make_scores(torch, lengths, offsets, 3, "cuda")
+    plan = ragged.Plan(ln32, offsets, family="global", device="cuda")
+    outr = plan.outputs()
+    vals = torch.empty(plan.B, device="cuda")
+    rcells = plan.cells
+    ms = timed(lambda: (plan.run(flat, gap=gap, temp=temp, out=outr), 0)[1])
+    res["ragged_forward_adjoint"] = {"ms": round(ms, 3), "gcups": round(rcells / ms / 1e6, 2),
+                                     "pairs": plan.B, "cells": rcells}
+    ms = timed(lambda: (plan.values(flat, gap=gap, temp=temp, out=vals), 0)[1])
+    res["ragged_value_only"] = {"ms": round(ms, 3), "gcups": round(rcells / ms / 1e6, 2)}
+    del flat, plan, outr
 
     line = {"global_alignment": res, "shape": [B, N, N], "params": {"gap": gap, "temp": temp}}
     try:

@@ -176,7 +176,8 @@ int swb_nw_value(const float* scores, const int* lengths, int B, int L1max, int 
  * it once with plan = NULL to get
  * *plan_bytes (and *workspace_bytes), then with a buffer of that size; copy
  * the plan bytes to the device unchanged and pass both copies to the launch.
- * family: 3 = affine, 1 = linear; cols_per_lane: 2 or 4 (0 = default).
+ * family: 3 = affine, 1 = linear, 2 = global alignment (soft Needleman–Wunsch,
+ * linear gap); cols_per_lane: 2 or 4 (0 = default).
  * host lengths [B, 2], host offsets [B+1].
  */
 int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const long long* offsets,
@@ -209,6 +210,13 @@ int swb_sw_affine_ragged_value(const float* scores, const void* host_plan, const
                                float gap_open, float gap_ext, float temp, float* value,
                                void* workspace, size_t workspace_bytes, void* stream);
 int swb_sw_ragged_value(const float* scores, const void* host_plan, const void* dev_plan, float gap,
+                        float temp, float* value, void* workspace, size_t workspace_bytes,
+                        void* stream);
+/* Global alignment over a family-2 plan: as swb_sw_ragged / swb_sw_ragged_value. */
+int swb_nw_ragged(const float* scores, const void* host_plan, const void* dev_plan, float gap,
+                  float temp, float* value, float* map, float* grad_gap, float* grad_temp,
+                  void* workspace, size_t workspace_bytes, void* stream, const swb_options* opt);
+int swb_nw_ragged_value(const float* scores, const void* host_plan, const void* dev_plan, float gap,
                         float temp, float* value, void* workspace, size_t workspace_bytes,
                         void* stream);
 

@@ -122,6 +122,10 @@ def load() -> ctypes.CDLL:
     lib.swb_nw_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, vp, vp, vp, sz, vp]
     lib.swb_nw_param_jacobian.restype = i
     lib.swb_nw_param_jacobian.argtypes = [vp, vp, i, i, i, f, f, i, vp, vp, sz, vp]
+    lib.swb_nw_ragged.restype = i
+    lib.swb_nw_ragged.argtypes = [vp, vp, vp, f, f, vp, vp, vp, vp, vp, sz, vp, ctypes.POINTER(Options)]
+    lib.swb_nw_ragged_value.restype = i
+    lib.swb_nw_ragged_value.argtypes = [vp, vp, vp, f, f, vp, vp, sz, vp]
     lib.swb_mufu_probe.restype = i
     lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()

@@ -288,14 +288,14 @@ int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2
                                   nullptr, true);
 }
 
-template <int NS>
+template <int NS, bool G = false>
 int launch_ragged(const float* scores, const void* host_plan, const void* dev_plan, float go,
                   float ge, float T, float* value, float* map, float* g_open, float* g_ext,
                   float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt,
                   bool value_only = false) {
   if (!host_plan || !dev_plan) return SWB_ERR_ARG;
   const long long* h = static_cast<const long long*>(host_plan);
-  if (h[HW_MAGIC] != kPlanMagic || (h[HW_FAMILY] & 0xff) != NS) return SWB_ERR_ARG;
+  if (h[HW_MAGIC] != kPlanMagic || (h[HW_FAMILY] & 0xff) != (G ? 2 : NS)) return SWB_ERR_ARG;
   const int r = (int)(h[HW_FAMILY] >> 8);
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   const long long B = h[HW_B], ntasks = h[HW_NTASKS];
@@ -315,11 +315,11 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
   a.go = go; a.ge = ge; a.T = T;
   a.value = value; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
   if (r == 2)
-    return launch<NS, 2>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt,
-                         value_only);
+    return launch<NS, 2, G>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream,
+                            opt, value_only);
   if (r == 4)
-    return launch<NS, 4>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream, opt,
-                         value_only);
+    return launch<NS, 4, G>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream,
+                            opt, value_only);
   return SWB_ERR_ARG;
 }
 
@@ -640,9 +640,11 @@ int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const lon
                     int B, void* plan, size_t plan_capacity, size_t* plan_bytes,
                     size_t* workspace_bytes) {
   const int R = cols_per_lane ? cols_per_lane : kDefaultR;
-  if ((family != 1 && family != 3) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
+  // family: 1 linear, 3 affine, 2 global alignment (linear gap; the linear model's buffers)
+  if ((family < 1 || family > 3) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
     return SWB_ERR_ARG;
-  const int NE = 2 * family, NP = (family == 3) ? 5 : 2, CKRS = (2 * family * R + 2 * family) * 32 + 4;
+  const int ns = family == 3 ? 3 : 1;
+  const int NE = 2 * ns, NP = (ns == 3) ? 5 : 2, CKRS = (2 * ns * R + 2 * ns) * 32 + 4;
   // validate the packing: row pitch round4(L2), offsets multiples of 4 floats
   long long ntasks = 0;
   for (int b = 0; b < B; ++b) {
@@ -745,6 +747,22 @@ int swb_sw_ragged(const float* scores, const void* host_plan, const void* dev_pl
                   const swb_options* opt) {
   return launch_ragged<1>(scores, host_plan, dev_plan, gap, 0.f, temp, value, map, grad_gap,
                           nullptr, grad_temp, workspace, workspace_bytes, stream, opt);
+}
+
+int swb_nw_ragged(const float* scores, const void* host_plan, const void* dev_plan, float gap,
+                  float temp, float* value, float* map, float* grad_gap, float* grad_temp,
+                  void* workspace, size_t workspace_bytes, void* stream,
+                  const swb_options* opt) {
+  return launch_ragged<1, true>(scores, host_plan, dev_plan, gap, 0.f, temp, value, map, grad_gap,
+                                nullptr, grad_temp, workspace, workspace_bytes, stream, opt);
+}
+
+int swb_nw_ragged_value(const float* scores, const void* host_plan, const void* dev_plan, float gap,
+                        float temp, float* value, void* workspace, size_t workspace_bytes,
+                        void* stream) {
+  return launch_ragged<1, true>(scores, host_plan, dev_plan, gap, 0.f, temp, value, nullptr,
+                                nullptr, nullptr, nullptr, workspace, workspace_bytes, stream,
+                                nullptr, true);
 }
 
 int swb_read_status(const void* workspace, void* stream, unsigned* status) {

@@ -1,4 +1,4 @@
-"""Packed ragged batches of soft Smith-Waterman pairs.
+"""Packed ragged batches of soft Smith-Waterman (and soft Needleman-Wunsch) pairs.
 
 The reference evaluates a batch of pairs of different lengths as one padded
 [B, L1max, L2max] tensor (with ``lengths`` or a mask).  This module runs the
@@ -15,6 +15,9 @@ flat float32 buffer.  The map comes back in the same packing.
     out = plan.run(flat.cuda(), gap_open=-2.0, gap_ext=-0.5, temp=0.5)
     out.value, out.map, out.grad_open, out.grad_ext, out.grad_temp
     maps = ragged.unpack(out.map, offsets, lengths)
+
+Families: "affine" and "linear" (local alignment), "global" (soft
+Needleman-Wunsch, linear gap; parameters gap and temp as for "linear").
 """
 
 from __future__ import annotations
@@ -28,7 +31,7 @@ import torch
 
 from . import _lib
 
-_FAMILY = {"affine": 3, "linear": 1}
+_FAMILY = {"affine": 3, "linear": 1, "global": 2}
 
 
 def pitch_of(L2: int) -> int:
@@ -90,7 +93,7 @@ class Plan:
     def __init__(self, lengths, offsets, family: str = "affine", device="cuda",
                  cols_per_lane: int = 0):
         if family not in _FAMILY:
-            raise ValueError(f"family must be 'affine' or 'linear', got {family!r}")
+            raise ValueError(f"family must be 'affine', 'linear' or 'global', got {family!r}")
         self.family = family
         self.lib = _lib.load()
         ln = np.ascontiguousarray(np.asarray(lengths, dtype=np.int32).reshape(-1, 2))
@@ -152,11 +155,11 @@ class Plan:
                     out.grad_ext.data_ptr(), out.grad_temp.data_ptr(), ws, self.workspace_bytes,
                     st, options)
             else:
-                rc = self.lib.swb_sw_ragged(
-                    flat.data_ptr(), hp, dp, float(gap), float(temp), out.value.data_ptr(),
-                    out.map.data_ptr(), out.grad_open.data_ptr(), out.grad_temp.data_ptr(), ws,
-                    self.workspace_bytes, st, options)
-        _lib.check(rc, "ragged soft Smith-Waterman")
+                fn = self.lib.swb_nw_ragged if self.family == "global" else self.lib.swb_sw_ragged
+                rc = fn(flat.data_ptr(), hp, dp, float(gap), float(temp), out.value.data_ptr(),
+                        out.map.data_ptr(), out.grad_open.data_ptr(), out.grad_temp.data_ptr(), ws,
+                        self.workspace_bytes, st, options)
+        _lib.check(rc, "ragged soft alignment")
         return out
 
     def values(self, flat: torch.Tensor, *, gap_open: float = 0.0, gap_ext: float = 0.0,
@@ -182,10 +185,11 @@ class Plan:
                     flat.data_ptr(), hp, dp, float(gap_open), float(gap_ext), float(temp),
                     out.data_ptr(), ws, self.workspace_bytes, st)
             else:
-                rc = self.lib.swb_sw_ragged_value(
-                    flat.data_ptr(), hp, dp, float(gap), float(temp), out.data_ptr(), ws,
-                    self.workspace_bytes, st)
-        _lib.check(rc, "ragged soft Smith-Waterman value")
+                fn = (self.lib.swb_nw_ragged_value if self.family == "global"
+                      else self.lib.swb_sw_ragged_value)
+                rc = fn(flat.data_ptr(), hp, dp, float(gap), float(temp), out.data_ptr(), ws,
+                        self.workspace_bytes, st)
+        _lib.check(rc, "ragged soft alignment value")
         return out
 
     def status(self) -> int:

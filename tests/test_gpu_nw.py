@@ -325,3 +325,31 @@ def test_nw_tensor_parameter_forward_backward():
     assert torch.allclose(s.grad, vm + mb[0], rtol=1e-5, atol=1e-6)
     assert torch.allclose(gp.grad, gg.sum() + mb[1][0], rtol=1e-5, atol=1e-5)
     assert torch.allclose(tp.grad, gT.sum() + mb[2][0], rtol=1e-5, atol=1e-5)
+
+
+def test_nw_ragged_plan_equals_padded_bitwise():
+    """The packed ragged path (family "global") computes each pair exactly as
+    the padded op with lengths does."""
+    from orihime_b200 import ragged
+    rng = np.random.default_rng(17)
+    lens = np.stack([rng.integers(0, 300, 40), rng.integers(0, 520, 40)], 1)
+    lens[3] = [0, 50]
+    lens[5] = [70, 0]
+    lens[7] = [1, 1]
+    mats = [_gen((int(a), int(b)), 100 + k, 1.5) for k, (a, b) in enumerate(lens)]
+    flat, off, l32 = ragged.pack([m.cuda() for m in mats])
+    plan = ragged.Plan(l32, off, family="global", device="cuda")
+    out = plan.run(flat.cuda(), gap=-0.9, temp=0.6)
+    vals = plan.values(flat.cuda(), gap=-0.9, temp=0.6)
+    L1m, L2m = int(lens[:, 0].max()), int(lens[:, 1].max())
+    pad = torch.zeros(len(mats), L1m, L2m)
+    for k, m in enumerate(mats):
+        pad[k, :m.shape[0], :m.shape[1]] = m
+    ln = torch.tensor(lens, dtype=torch.int32).cuda()
+    v, m = torch.ops.orihime.nw_forward(pad.cuda(), -0.9, 0.6, ln)
+    gg, gT = torch.ops.orihime.nw_value_grad_params(pad.cuda(), -0.9, 0.6, ln)
+    assert torch.equal(out.value, v) and torch.equal(vals, v)
+    assert torch.equal(out.grad_open, gg) and torch.equal(out.grad_temp, gT)
+    for k, mk in enumerate(ragged.unpack(out.map, off, l32)):
+        a, b = int(lens[k, 0]), int(lens[k, 1])
+        assert torch.equal(mk, m[k, :a, :b]), k

@@ -75,3 +75,17 @@ def test_plan_rejects_bad_packing(bad):
         lengths[1, 0] = -1
     rc, _ = _plan(lengths, off)
     assert rc == _lib.ERR_ARG
+
+
+def test_global_alignment_plan_uses_the_linear_layout():
+    """Family 2 (global alignment, linear gap) places the same buffers as the
+    linear model and records its own family code; an unknown family is refused."""
+    lengths = [[40, 300], [0, 5], [17, 1], [129, 129]]
+    off, _ = ragged.layout(lengths)
+    rc1, lin = _plan(lengths, off, family=1)
+    rc2, glob = _plan(lengths, off, family=2)
+    assert rc1 == 0 and rc2 == 0
+    assert np.array_equal(lin[1:7], glob[1:7])          # B, tasks, slots, ck, edge, push
+    assert glob[7] & 0xff == 2 and lin[7] & 0xff == 1   # family word
+    assert _plan(lengths, off, family=4)[0] != 0
+    assert _plan(lengths, off, family=0)[0] != 0
