@@ -155,6 +155,35 @@ int swb_nw_forward(const float* scores, const int* lengths, int B, int L1max, in
                    float* value, float* map, float* grad_gap, float* grad_temp,
                    void* workspace, size_t workspace_bytes, void* stream,
                    const swb_options* opt);
+/*
+ * Soft Needleman–Wunsch with affine gaps: value S = LSE(M, I, D at (L1, L2)),
+ * marginal map (posterior of M), dS/dgap_open, dS/dgap_ext, dS/dT.  Three
+ * states with I <- (M, I, D) from above and D <- (M, I, D) from the left;
+ * boundaries M(0,0) = 0, I(i,0) = go + (i-1) ge, D(0,j) = go + (j-1) ge.
+ * Replaces soft_nw_affine_cuda_float / soft_nw_affine_cuda_with_grads
+ * (src/nw_affine/torch_cuda.cpp:364, :387; registration :763-786), i.e. the reference
+ * launchers nw_affine_forward + nw_affine_backward
+ * (src/nw_affine/kernels_cpu.cpp:100-347 restated).  Workspace from
+ * swb_nw_affine_workspace_bytes; the value-only call and the packed ragged
+ * calls (plan family 4) follow the linear global ones.
+ */
+size_t swb_nw_affine_workspace_bytes(int B, int L1max, int L2max);
+int swb_nw_affine_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap_open, float gap_ext, float temp, float* value, float* map,
+                          float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                          size_t workspace_bytes, void* stream, const swb_options* opt);
+size_t swb_nw_affine_value_workspace_bytes(int B, int L1max, int L2max);
+int swb_nw_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                        float gap_open, float gap_ext, float temp, float* value, void* workspace,
+                        size_t workspace_bytes, void* stream);
+int swb_nw_affine_ragged(const float* scores, const void* host_plan, const void* dev_plan,
+                         float gap_open, float gap_ext, float temp, float* value, float* map,
+                         float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                         size_t workspace_bytes, void* stream, const swb_options* opt);
+int swb_nw_affine_ragged_value(const float* scores, const void* host_plan, const void* dev_plan,
+                               float gap_open, float gap_ext, float temp, float* value,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
 /* Value only (forward wavefront alone; equals swb_nw_forward's value bit for bit). */
 size_t swb_nw_value_workspace_bytes(int B, int L1max, int L2max);
 int swb_nw_value(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
@@ -177,7 +206,8 @@ int swb_nw_value(const float* scores, const int* lengths, int B, int L1max, int 
  * *plan_bytes (and *workspace_bytes), then with a buffer of that size; copy
  * the plan bytes to the device unchanged and pass both copies to the launch.
  * family: 3 = affine, 1 = linear, 2 = global alignment (soft Needleman–Wunsch,
- * linear gap); cols_per_lane: 2 or 4 (0 = default).
+ * linear gap), 4 = global alignment with affine gaps; cols_per_lane: 2 or 4
+ * (0 = default).
  * host lengths [B, 2], host offsets [B+1].
  */
 int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const long long* offsets,

@@ -217,9 +217,52 @@ def nw_param_grad(scores, lengths, gap, temp, param: int, dtype=np.float32) -> n
     return out
 
 
+def nw_affine(scores, lengths, gap_open, gap_ext, temp, dtype=np.float32) -> dict:
+    """Global alignment with affine gaps: value [B], map, grad_open/grad_ext/
+    grad_temp [B]."""
+    s, ln = _prep(scores, lengths, dtype)
+    B, L1, L2 = s.shape
+    out = {k: np.zeros(B, dtype) for k in ("value", "grad_open", "grad_ext", "grad_temp")}
+    out["map"] = np.zeros_like(s)
+    sc = _scal(dtype)
+    rc = getattr(lib(), "oracle_nw_affine_forward" + _sfx(dtype))(
+        _ptr(s), _ptr(ln), _I(B), _I(L1), _I(L2), sc(gap_open), sc(gap_ext), sc(temp),
+        _ptr(out["value"]), _ptr(out["map"]), _ptr(out["grad_open"]), _ptr(out["grad_ext"]),
+        _ptr(out["grad_temp"]))
+    assert rc == 0
+    return out
+
+
+def nw_affine_hvp(scores, v, lengths, gap_open, gap_ext, temp, dtype=np.float32) -> np.ndarray:
+    s, ln = _prep(scores, lengths, dtype)
+    vv = np.ascontiguousarray(v, dtype=dtype)
+    B, L1, L2 = s.shape
+    out = np.zeros_like(s)
+    sc = _scal(dtype)
+    rc = getattr(lib(), "oracle_nw_affine_hvp" + _sfx(dtype))(
+        _ptr(s), _ptr(vv), _ptr(ln), _I(B), _I(L1), _I(L2), sc(gap_open), sc(gap_ext), sc(temp),
+        _ptr(out))
+    assert rc == 0
+    return out
+
+
+def nw_affine_param_grad(scores, lengths, gap_open, gap_ext, temp, param: int,
+                         dtype=np.float32) -> np.ndarray:
+    """d(map)/d(theta); param 0 = gap_open, 1 = gap_ext, 2 = temperature."""
+    s, ln = _prep(scores, lengths, dtype)
+    B, L1, L2 = s.shape
+    out = np.zeros_like(s)
+    sc = _scal(dtype)
+    rc = getattr(lib(), "oracle_nw_affine_param_grad" + _sfx(dtype))(
+        _ptr(s), _ptr(ln), _I(B), _I(L1), _I(L2), sc(gap_open), sc(gap_ext), sc(temp), _I(param),
+        _ptr(out))
+    assert rc == 0
+    return out
+
+
 # ---------------------------------------------------------------------------
 # the reference's own CPU kernels (src/sw*/kernels_cpu.cpp,
-# src/nw/kernels_cpu.cpp), float32 only
+# src/nw*/kernels_cpu.cpp), float32 only
 # ---------------------------------------------------------------------------
 
 def _full_lengths(B, L1, L2, ln):
@@ -394,4 +437,58 @@ def ref_nw_param_grad(scores, lengths, gap, temp, param: int) -> np.ndarray:
     r.nw_forward_cpu(_ptr(s), _ptr(alpha), _ptr(part), _ptr(ln), *a)
     r.nw_param_grad_cpu(_ptr(alpha), _ptr(s), _ptr(part), _ptr(dS), _ptr(U), _ptr(be), _ptr(W),
                         _ptr(out), _ptr(ln), *a, _I(param))
+    return out
+
+
+def ref_nw_affine(scores, lengths, gap_open, gap_ext, temp) -> dict:
+    """nw_affine_forward_cpu + nw_affine_backward_cpu (src/nw_affine/kernels_cpu.cpp:100, :193)."""
+    s, ln = _prep(scores, lengths, np.float32)
+    B, L1, L2 = s.shape
+    ln = _full_lengths(B, L1, L2, ln)
+    n_alpha = 3 * (L1 + 1) * (L2 + 1)
+    alpha = np.empty((B, n_alpha), np.float32)
+    beta = np.empty((B, n_alpha), np.float32)
+    out = {k: np.zeros(B, np.float32) for k in ("value", "grad_open", "grad_ext", "grad_temp")}
+    out["map"] = np.zeros_like(s)
+    r = ref_lib()
+    a = (_I(B), _I(L1), _I(L2), _F(gap_open), _F(gap_ext), _F(temp))
+    r.nw_affine_forward_cpu(_ptr(s), _ptr(alpha), _ptr(out["value"]), _ptr(ln), *a)
+    r.nw_affine_backward_cpu(_ptr(alpha), _ptr(s), _ptr(out["value"]), _ptr(beta), _ptr(out["map"]),
+                             _ptr(out["grad_open"]), _ptr(out["grad_ext"]), _ptr(out["grad_temp"]),
+                             _ptr(ln), *a)
+    return out
+
+
+def ref_nw_affine_hvp(scores, v, lengths, gap_open, gap_ext, temp) -> np.ndarray:
+    s, ln = _prep(scores, lengths, np.float32)
+    vv = np.ascontiguousarray(v, dtype=np.float32)
+    B, L1, L2 = s.shape
+    ln = _full_lengths(B, L1, L2, ln)
+    n_alpha = 3 * (L1 + 1) * (L2 + 1)
+    alpha, da, be, dbe = (np.empty((B, n_alpha), np.float32) for _ in range(4))
+    part = np.zeros(B, np.float32)
+    dpart = np.zeros(B, np.float32)
+    out = np.zeros_like(s)
+    r = ref_lib()
+    a = (_I(B), _I(L1), _I(L2), _F(gap_open), _F(gap_ext), _F(temp))
+    r.nw_affine_forward_cpu(_ptr(s), _ptr(alpha), _ptr(part), _ptr(ln), *a)
+    r.nw_affine_hvp_cpu(_ptr(alpha), _ptr(s), _ptr(part), _ptr(vv), _ptr(da), _ptr(dpart), _ptr(be),
+                        _ptr(dbe), _ptr(out), _ptr(ln), *a)
+    return out
+
+
+def ref_nw_affine_param_grad(scores, lengths, gap_open, gap_ext, temp, param: int) -> np.ndarray:
+    s, ln = _prep(scores, lengths, np.float32)
+    B, L1, L2 = s.shape
+    ln = _full_lengths(B, L1, L2, ln)
+    n_alpha = 3 * (L1 + 1) * (L2 + 1)
+    alpha, U, be, W = (np.empty((B, n_alpha), np.float32) for _ in range(4))
+    part = np.zeros(B, np.float32)
+    dS = np.zeros(B, np.float32)
+    out = np.zeros_like(s)
+    r = ref_lib()
+    a = (_I(B), _I(L1), _I(L2), _F(gap_open), _F(gap_ext), _F(temp))
+    r.nw_affine_forward_cpu(_ptr(s), _ptr(alpha), _ptr(part), _ptr(ln), *a)
+    r.nw_affine_param_grad_cpu(_ptr(alpha), _ptr(s), _ptr(part), _ptr(dS), _ptr(U), _ptr(be), _ptr(W),
+                               _ptr(out), _ptr(ln), *a, _I(param))
     return out

@@ -885,6 +885,337 @@ static void FN(nw_param)(FN(lin_t) *c, int pt, REAL *u, REAL *be, REAL *wt, REAL
     }
 }
 
+/* ---- global alignment, affine gaps (Needleman-Wunsch affine) ------------
+ * Three states on the affine tables (aff_t): M = s + LSE(M, I, D at diag),
+ * I = LSE(M + go, I + ge, D + go) from above, D = LSE(M + go, I + go, D + ge)
+ * from the left.  Boundaries M(0,0) = 0, I(i,0) = go + (i-1) ge,
+ * D(0,j) = go + (j-1) ge, every other boundary state NEG_BIG.  S = LSE of the
+ * three states at (L1, L2).  The helpers are the file's own
+ * (src/nw_affine/kernels_cpu.cpp:37-98): the LSE skips NEG_BIG terms in its
+ * Kahan sum, the weights use a plain sum. */
+
+static REAL FN(nwa_lse3)(REAL a, REAL b, REAL c, REAL T) {
+    REAL m = a > b ? a : b;
+    if (c > m) m = c;
+    if (m <= (REAL)NEG_BIG) return (REAL)NEG_BIG;
+    FN(ksum_t) k = {0, 0};
+    if (a > (REAL)NEG_BIG) FN(kadd)(&k, FN(clip_exp)((a - m) / T));
+    if (b > (REAL)NEG_BIG) FN(kadd)(&k, FN(clip_exp)((b - m) / T));
+    if (c > (REAL)NEG_BIG) FN(kadd)(&k, FN(clip_exp)((c - m) / T));
+    if (k.s <= 0) return (REAL)NEG_BIG;
+    return m + T * LOGF(k.s);
+}
+
+static void FN(nwa_w3)(REAL a, REAL b, REAL c, REAL T, REAL w[3]) {
+    REAL m = a > b ? a : b;
+    if (c > m) m = c;
+    w[0] = w[1] = w[2] = 0;
+    if (m <= (REAL)NEG_BIG) return;
+    REAL ea = a > (REAL)NEG_BIG ? FN(clip_exp)((a - m) / T) : 0;
+    REAL eb = b > (REAL)NEG_BIG ? FN(clip_exp)((b - m) / T) : 0;
+    REAL ec = c > (REAL)NEG_BIG ? FN(clip_exp)((c - m) / T) : 0;
+    REAL t = ea + eb + ec;
+    if (t > 0) { w[0] = ea / t; w[1] = eb / t; w[2] = ec / t; }
+}
+
+/* candidates of cell (i,j): v[0..2] diag M, I, D; v[3..5] up M+go, I+ge, D+go;
+ * v[6..8] left M+go, I+go, D+ge */
+static void FN(nwa_cands)(const FN(aff_t) *c, const REAL *t, int i, int j, REAL v[9]) {
+    v[0] = t[AIX(c, 0, i - 1, j - 1)]; v[1] = t[AIX(c, 1, i - 1, j - 1)]; v[2] = t[AIX(c, 2, i - 1, j - 1)];
+    v[3] = t[AIX(c, 0, i - 1, j)] + c->go; v[4] = t[AIX(c, 1, i - 1, j)] + c->ge;
+    v[5] = t[AIX(c, 2, i - 1, j)] + c->go;
+    v[6] = t[AIX(c, 0, i, j - 1)] + c->go; v[7] = t[AIX(c, 1, i, j - 1)] + c->go;
+    v[8] = t[AIX(c, 2, i, j - 1)] + c->ge;
+}
+
+/* src/nw_affine/kernels_cpu.cpp:100-187 */
+static REAL FN(nwa_forward)(FN(aff_t) *c) {
+    for (int st = 0; st < 3; ++st)
+        for (int i = 0; i <= c->L1; ++i)
+            for (int j = 0; j <= c->L2; ++j) c->a[AIX(c, st, i, j)] = (REAL)NEG_BIG;
+    c->a[AIX(c, 0, 0, 0)] = 0;
+    for (int i = 1; i <= c->L1; ++i) c->a[AIX(c, 1, i, 0)] = c->go + (REAL)(i - 1) * c->ge;
+    for (int j = 1; j <= c->L2; ++j) c->a[AIX(c, 2, 0, j)] = c->go + (REAL)(j - 1) * c->ge;
+    REAL v[9];
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            FN(nwa_cands)(c, c->a, i, j, v);
+            c->a[AIX(c, 0, i, j)] = SC(c, i, j) + FN(nwa_lse3)(v[0], v[1], v[2], c->T);
+            c->a[AIX(c, 1, i, j)] = FN(nwa_lse3)(v[3], v[4], v[5], c->T);
+            c->a[AIX(c, 2, i, j)] = FN(nwa_lse3)(v[6], v[7], v[8], c->T);
+        }
+    return FN(nwa_lse3)(c->a[AIX(c, 0, c->L1, c->L2)], c->a[AIX(c, 1, c->L1, c->L2)],
+                        c->a[AIX(c, 2, c->L1, c->L2)], c->T);
+}
+
+#define NWA_TH ((REAL)1e-20)
+
+/* src/nw_affine/kernels_cpu.cpp:193-347; g = dS/d(go, ge, T). */
+static void FN(nwa_adjoint)(const FN(aff_t) *c, REAL S, REAL *be, REAL *post, int L1max,
+                            REAL g[3]) {
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < nsc; ++q) post[q] = 0;
+    for (int st = 0; st < 3; ++st)
+        for (int i = 0; i <= c->L1; ++i)
+            for (int j = 0; j <= c->L2; ++j) be[AIX(c, st, i, j)] = 0;
+    const REAL T = c->T;
+    REAL w[3], v[9];
+    FN(nwa_w3)(c->a[AIX(c, 0, c->L1, c->L2)], c->a[AIX(c, 1, c->L1, c->L2)],
+               c->a[AIX(c, 2, c->L1, c->L2)], T, w);
+    for (int st = 0; st < 3; ++st) be[AIX(c, st, c->L1, c->L2)] = w[st];
+    REAL so = 0, se = 0;
+    FN(ksum_t) ms = {0, 0};
+    NW_DIAGS(c, k, i, j) {
+        REAL bM = be[AIX(c, 0, i, j)], bI = be[AIX(c, 1, i, j)], bD = be[AIX(c, 2, i, j)];
+        REAL sc = SC(c, i, j);
+        FN(nwa_cands)(c, c->a, i, j, v);
+        if (bM > NWA_TH && FN(nwa_lse3)(v[0], v[1], v[2], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[0], v[1], v[2], T, w);
+            for (int st = 0; st < 3; ++st)
+                if (v[st] > (REAL)NEG_BIG) be[AIX(c, st, i - 1, j - 1)] += bM * w[st];
+            post[(size_t)(i - 1) * c->ld + (j - 1)] += bM;
+            FN(kadd)(&ms, bM * sc);
+        }
+        if (bI > NWA_TH && FN(nwa_lse3)(v[3], v[4], v[5], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[3], v[4], v[5], T, w);
+            for (int st = 0; st < 3; ++st) be[AIX(c, st, i - 1, j)] += bI * w[st];
+            so += bI * (w[0] + w[2]);
+            se += bI * w[1];
+        }
+        if (bD > NWA_TH && FN(nwa_lse3)(v[6], v[7], v[8], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[6], v[7], v[8], T, w);
+            for (int st = 0; st < 3; ++st) be[AIX(c, st, i, j - 1)] += bD * w[st];
+            so += bD * (w[0] + w[1]);
+            se += bD * w[2];
+        }
+    }
+    /* leading-gap boundary states (kernels_cpu.cpp:318-335) */
+    for (int i = 1; i <= c->L1; ++i) {
+        REAL b = be[AIX(c, 1, i, 0)];
+        if (b > NWA_TH) { so += b; se += b * (REAL)(i - 1); }
+    }
+    for (int j = 1; j <= c->L2; ++j) {
+        REAL b = be[AIX(c, 2, 0, j)];
+        if (b > NWA_TH) { so += b; se += b * (REAL)(j - 1); }
+    }
+    g[0] = so;
+    g[1] = se;
+    g[2] = (S - (ms.s + so * c->go + se * c->ge)) / T;
+}
+
+/* dw = w (t - sum w t) / T over three terms, left to right as the reference */
+static void FN(nwa_dw)(const REAL w[3], const REAL t[3], REAL T, REAL dw[3]) {
+    REAL e = w[0] * t[0] + w[1] * t[1] + w[2] * t[2];
+    for (int q = 0; q < 3; ++q) dw[q] = w[q] * (t[q] - e) / T;
+}
+
+/* src/nw_affine/kernels_cpu.cpp:353-613 (HVP). */
+static void FN(nwa_hvp)(FN(aff_t) *c, const REAL *V, REAL *da, REAL *be, REAL *dbe, REAL *H,
+                        int L1max) {
+    size_t nsc = (size_t)L1max * c->ld;
+    for (int st = 0; st < 3; ++st)
+        for (int i = 0; i <= c->L1; ++i)
+            for (int j = 0; j <= c->L2; ++j) {
+                size_t o = AIX(c, st, i, j);
+                da[o] = 0; be[o] = 0; dbe[o] = 0;
+            }
+    for (size_t q = 0; q < nsc; ++q) H[q] = 0;
+    const REAL T = c->T;
+    REAL w[3], v[9], t[3], dw[3];
+#define VV(i, j) V[(size_t)((i) - 1) * c->ld + (size_t)((j) - 1)]
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            FN(nwa_cands)(c, c->a, i, j, v);
+            if (FN(nwa_lse3)(v[0], v[1], v[2], T) > (REAL)NEG_BIG) {
+                FN(nwa_w3)(v[0], v[1], v[2], T, w);
+                da[AIX(c, 0, i, j)] = VV(i, j) + w[0] * da[AIX(c, 0, i - 1, j - 1)] +
+                                      w[1] * da[AIX(c, 1, i - 1, j - 1)] + w[2] * da[AIX(c, 2, i - 1, j - 1)];
+            } else {
+                da[AIX(c, 0, i, j)] = 0;
+            }
+            if (FN(nwa_lse3)(v[3], v[4], v[5], T) > (REAL)NEG_BIG) {
+                FN(nwa_w3)(v[3], v[4], v[5], T, w);
+                da[AIX(c, 1, i, j)] = w[0] * da[AIX(c, 0, i - 1, j)] + w[1] * da[AIX(c, 1, i - 1, j)] +
+                                      w[2] * da[AIX(c, 2, i - 1, j)];
+            } else {
+                da[AIX(c, 1, i, j)] = 0;
+            }
+            if (FN(nwa_lse3)(v[6], v[7], v[8], T) > (REAL)NEG_BIG) {
+                FN(nwa_w3)(v[6], v[7], v[8], T, w);
+                da[AIX(c, 2, i, j)] = w[0] * da[AIX(c, 0, i, j - 1)] + w[1] * da[AIX(c, 1, i, j - 1)] +
+                                      w[2] * da[AIX(c, 2, i, j - 1)];
+            } else {
+                da[AIX(c, 2, i, j)] = 0;
+            }
+        }
+    }
+    {
+        size_t f0 = AIX(c, 0, c->L1, c->L2), f1 = AIX(c, 1, c->L1, c->L2), f2 = AIX(c, 2, c->L1, c->L2);
+        FN(nwa_w3)(c->a[f0], c->a[f1], c->a[f2], T, w);
+        be[f0] = w[0]; be[f1] = w[1]; be[f2] = w[2];
+        t[0] = da[f0]; t[1] = da[f1]; t[2] = da[f2];
+        FN(nwa_dw)(w, t, T, dw);
+        dbe[f0] = dw[0]; dbe[f1] = dw[1]; dbe[f2] = dw[2];
+    }
+    NW_DIAGS(c, k, i, j) {
+        REAL bM = be[AIX(c, 0, i, j)], bI = be[AIX(c, 1, i, j)], bD = be[AIX(c, 2, i, j)];
+        REAL dM = dbe[AIX(c, 0, i, j)], dI = dbe[AIX(c, 1, i, j)], dD = dbe[AIX(c, 2, i, j)];
+        FN(nwa_cands)(c, c->a, i, j, v);
+        if ((bM > NWA_TH || FABS(dM) > NWA_TH) && FN(nwa_lse3)(v[0], v[1], v[2], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[0], v[1], v[2], T, w);
+            for (int st = 0; st < 3; ++st) t[st] = da[AIX(c, st, i - 1, j - 1)];
+            FN(nwa_dw)(w, t, T, dw);
+            for (int st = 0; st < 3; ++st)
+                if (v[st] > (REAL)NEG_BIG) {
+                    be[AIX(c, st, i - 1, j - 1)] += bM * w[st];
+                    dbe[AIX(c, st, i - 1, j - 1)] += dM * w[st] + bM * dw[st];
+                }
+            H[(size_t)(i - 1) * c->ld + (j - 1)] += dM;
+        }
+        if ((bI > NWA_TH || FABS(dI) > NWA_TH) && FN(nwa_lse3)(v[3], v[4], v[5], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[3], v[4], v[5], T, w);
+            for (int st = 0; st < 3; ++st) t[st] = da[AIX(c, st, i - 1, j)];
+            FN(nwa_dw)(w, t, T, dw);
+            for (int st = 0; st < 3; ++st) {
+                be[AIX(c, st, i - 1, j)] += bI * w[st];
+                dbe[AIX(c, st, i - 1, j)] += dI * w[st] + bI * dw[st];
+            }
+        }
+        if ((bD > NWA_TH || FABS(dD) > NWA_TH) && FN(nwa_lse3)(v[6], v[7], v[8], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[6], v[7], v[8], T, w);
+            for (int st = 0; st < 3; ++st) t[st] = da[AIX(c, st, i, j - 1)];
+            FN(nwa_dw)(w, t, T, dw);
+            for (int st = 0; st < 3; ++st) {
+                be[AIX(c, st, i, j - 1)] += bD * w[st];
+                dbe[AIX(c, st, i, j - 1)] += dD * w[st] + bD * dw[st];
+            }
+        }
+    }
+#undef VV
+}
+
+/* src/nw_affine/kernels_cpu.cpp:619-1000 (dP/dtheta, theta in {go, ge, T}). */
+static void FN(nwa_param)(FN(aff_t) *c, int pt, REAL *u, REAL *be, REAL *wt, REAL *dP,
+                          int L1max) {
+    size_t nsc = (size_t)L1max * c->ld;
+    for (int st = 0; st < 3; ++st)
+        for (int i = 0; i <= c->L1; ++i)
+            for (int j = 0; j <= c->L2; ++j) {
+                size_t o = AIX(c, st, i, j);
+                u[o] = 0; be[o] = 0; wt[o] = 0;
+            }
+    for (size_t q = 0; q < nsc; ++q) dP[q] = 0;
+    if (pt == 0 || pt == 1) {
+        for (int i = 1; i <= c->L1; ++i) u[AIX(c, 1, i, 0)] = pt == 0 ? (REAL)1 : (REAL)(i - 1);
+        for (int j = 1; j <= c->L2; ++j) u[AIX(c, 2, 0, j)] = pt == 0 ? (REAL)1 : (REAL)(j - 1);
+    }
+    const REAL T = c->T;
+    /* direct tangents of the gap terms: I from (M, I, D) up, D from (M, I, D) left */
+    const REAL dI[3] = {pt == 0 ? 1 : 0, pt == 1 ? 1 : 0, pt == 0 ? 1 : 0};
+    const REAL dD[3] = {pt == 0 ? 1 : 0, pt == 0 ? 1 : 0, pt == 1 ? 1 : 0};
+    REAL w[3], v[9], t[3], dw[3];
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            FN(nwa_cands)(c, c->a, i, j, v);
+            if (FN(nwa_lse3)(v[0], v[1], v[2], T) > (REAL)NEG_BIG) {
+                FN(nwa_w3)(v[0], v[1], v[2], T, w);
+                REAL U = w[0] * u[AIX(c, 0, i - 1, j - 1)] + w[1] * u[AIX(c, 1, i - 1, j - 1)] +
+                         w[2] * u[AIX(c, 2, i - 1, j - 1)];
+                if (pt == 2) {
+                    REAL e = w[0] * v[0] + w[1] * v[1] + w[2] * v[2];
+                    U += (c->a[AIX(c, 0, i, j)] - (e + SC(c, i, j))) / T;
+                }
+                u[AIX(c, 0, i, j)] = U;
+            }
+            if (FN(nwa_lse3)(v[3], v[4], v[5], T) > (REAL)NEG_BIG) {
+                FN(nwa_w3)(v[3], v[4], v[5], T, w);
+                REAL U = w[0] * (u[AIX(c, 0, i - 1, j)] + dI[0]) + w[1] * (u[AIX(c, 1, i - 1, j)] + dI[1]) +
+                         w[2] * (u[AIX(c, 2, i - 1, j)] + dI[2]);
+                if (pt == 2) {
+                    REAL e = w[0] * v[3] + w[1] * v[4] + w[2] * v[5];
+                    U += (c->a[AIX(c, 1, i, j)] - e) / T;
+                }
+                u[AIX(c, 1, i, j)] = U;
+            }
+            if (FN(nwa_lse3)(v[6], v[7], v[8], T) > (REAL)NEG_BIG) {
+                FN(nwa_w3)(v[6], v[7], v[8], T, w);
+                REAL U = w[0] * (u[AIX(c, 0, i, j - 1)] + dD[0]) + w[1] * (u[AIX(c, 1, i, j - 1)] + dD[1]) +
+                         w[2] * (u[AIX(c, 2, i, j - 1)] + dD[2]);
+                if (pt == 2) {
+                    REAL e = w[0] * v[6] + w[1] * v[7] + w[2] * v[8];
+                    U += (c->a[AIX(c, 2, i, j)] - e) / T;
+                }
+                u[AIX(c, 2, i, j)] = U;
+            }
+        }
+    }
+    {
+        size_t f[3] = {AIX(c, 0, c->L1, c->L2), AIX(c, 1, c->L1, c->L2), AIX(c, 2, c->L1, c->L2)};
+        FN(nwa_w3)(c->a[f[0]], c->a[f[1]], c->a[f[2]], T, w);
+        for (int st = 0; st < 3; ++st) { be[f[st]] = w[st]; t[st] = u[f[st]]; }
+        FN(nwa_dw)(w, t, T, dw);
+        if (pt == 2) {
+            REAL e = w[0] * c->a[f[0]] + w[1] * c->a[f[1]] + w[2] * c->a[f[2]];
+            REAL it2 = (REAL)1 / (T * T);
+            for (int st = 0; st < 3; ++st) dw[st] += w[st] * (e - c->a[f[st]]) * it2;
+        }
+        for (int st = 0; st < 3; ++st) wt[f[st]] = dw[st];
+    }
+    NW_DIAGS(c, k, i, j) {
+        REAL bM = be[AIX(c, 0, i, j)], bI = be[AIX(c, 1, i, j)], bD = be[AIX(c, 2, i, j)];
+        REAL WM = wt[AIX(c, 0, i, j)], WI = wt[AIX(c, 1, i, j)], WD = wt[AIX(c, 2, i, j)];
+        FN(nwa_cands)(c, c->a, i, j, v);
+        REAL it2 = (REAL)1 / (T * T);
+        if ((bM > NWA_TH || FABS(WM) > NWA_TH) && FN(nwa_lse3)(v[0], v[1], v[2], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[0], v[1], v[2], T, w);
+            for (int st = 0; st < 3; ++st) t[st] = u[AIX(c, st, i - 1, j - 1)];
+            FN(nwa_dw)(w, t, T, dw);
+            if (pt == 2) {
+                REAL e = w[0] * v[0] + w[1] * v[1] + w[2] * v[2];
+                for (int st = 0; st < 3; ++st) dw[st] += w[st] * (e - v[st]) * it2;
+            }
+            for (int st = 0; st < 3; ++st)
+                if (v[st] > (REAL)NEG_BIG) {
+                    be[AIX(c, st, i - 1, j - 1)] += bM * w[st];
+                    wt[AIX(c, st, i - 1, j - 1)] += WM * w[st] + bM * dw[st];
+                }
+            dP[(size_t)(i - 1) * c->ld + (j - 1)] += WM;
+        }
+        if ((bI > NWA_TH || FABS(WI) > NWA_TH) && FN(nwa_lse3)(v[3], v[4], v[5], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[3], v[4], v[5], T, w);
+            for (int st = 0; st < 3; ++st) t[st] = u[AIX(c, st, i - 1, j)] + dI[st];
+            FN(nwa_dw)(w, t, T, dw);
+            if (pt == 2) {
+                REAL e = w[0] * v[3] + w[1] * v[4] + w[2] * v[5];
+                for (int st = 0; st < 3; ++st) dw[st] += w[st] * (e - v[3 + st]) * it2;
+            }
+            for (int st = 0; st < 3; ++st) {
+                be[AIX(c, st, i - 1, j)] += bI * w[st];
+                wt[AIX(c, st, i - 1, j)] += WI * w[st] + bI * dw[st];
+            }
+        }
+        if ((bD > NWA_TH || FABS(WD) > NWA_TH) && FN(nwa_lse3)(v[6], v[7], v[8], T) > (REAL)NEG_BIG) {
+            FN(nwa_w3)(v[6], v[7], v[8], T, w);
+            for (int st = 0; st < 3; ++st) t[st] = u[AIX(c, st, i, j - 1)] + dD[st];
+            FN(nwa_dw)(w, t, T, dw);
+            if (pt == 2) {
+                REAL e = w[0] * v[6] + w[1] * v[7] + w[2] * v[8];
+                for (int st = 0; st < 3; ++st) dw[st] += w[st] * (e - v[6 + st]) * it2;
+            }
+            for (int st = 0; st < 3; ++st) {
+                be[AIX(c, st, i, j - 1)] += bD * w[st];
+                wt[AIX(c, st, i, j - 1)] += WD * w[st] + bD * dw[st];
+            }
+        }
+    }
+}
+
 /* ---- batched entry points (padded [B, L1max, L2max] layout) ------------ */
 
 static int FN(pair_len)(const int *lengths, int b, int which, int dflt) {
@@ -1098,6 +1429,65 @@ int FN(oracle_nw_linear_param_grad)(const REAL *scores, const int *lengths, int 
     return 0;
 }
 
+#define NWA_PAIR()                                                            \
+    FN(aff_t) c;                                                              \
+    c.L1 = FN(pair_len)(lengths, b, 0, L1m);                                  \
+    c.L2 = FN(pair_len)(lengths, b, 1, L2m);                                  \
+    c.ld = L2m; c.s = scores + b * slab; c.go = go; c.ge = ge; c.T = T;       \
+    c.plane = plane; c.cols = (size_t)L2m + 1; c.a = a
+
+int FN(oracle_nw_affine_forward)(const REAL *scores, const int *lengths, int B, int L1m, int L2m,
+                                 REAL go, REAL ge, REAL T, REAL *value, REAL *map, REAL *gopen,
+                                 REAL *gext, REAL *gT) {
+    size_t slab = (size_t)L1m * L2m, plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 6 * plane);
+    if (!a) return -1;
+    REAL *be = a + 3 * plane;
+    for (int b = 0; b < B; ++b) {
+        NWA_PAIR();
+        REAL S = FN(nwa_forward)(&c);
+        REAL g[3];
+        FN(nwa_adjoint)(&c, S, be, map + b * slab, L1m, g);
+        value[b] = S;
+        if (gopen) gopen[b] = g[0];
+        if (gext) gext[b] = g[1];
+        if (gT) gT[b] = g[2];
+    }
+    free(a);
+    return 0;
+}
+
+int FN(oracle_nw_affine_hvp)(const REAL *scores, const REAL *V, const int *lengths, int B, int L1m,
+                             int L2m, REAL go, REAL ge, REAL T, REAL *out) {
+    size_t slab = (size_t)L1m * L2m, plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 12 * plane);
+    if (!a) return -1;
+    for (int b = 0; b < B; ++b) {
+        NWA_PAIR();
+        FN(nwa_forward)(&c);
+        FN(nwa_hvp)(&c, V + b * slab, a + 3 * plane, a + 6 * plane, a + 9 * plane, out + b * slab, L1m);
+    }
+    free(a);
+    return 0;
+}
+
+/* pt: 0 = gap_open, 1 = gap_ext, 2 = temperature. */
+int FN(oracle_nw_affine_param_grad)(const REAL *scores, const int *lengths, int B, int L1m,
+                                    int L2m, REAL go, REAL ge, REAL T, int pt, REAL *out) {
+    size_t slab = (size_t)L1m * L2m, plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 12 * plane);
+    if (!a) return -1;
+    for (int b = 0; b < B; ++b) {
+        NWA_PAIR();
+        FN(nwa_forward)(&c);
+        FN(nwa_param)(&c, pt, a + 3 * plane, a + 6 * plane, a + 9 * plane, out + b * slab, L1m);
+    }
+    free(a);
+    return 0;
+}
+
+#undef NWA_PAIR
+#undef NWA_TH
 #undef NW_DIAGS
 #undef AIX
 #undef SC

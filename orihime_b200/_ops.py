@@ -49,6 +49,10 @@ SCHEMAS = {
     "nw_forward": "nw_forward(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor[]",
     "nw_forward_t": "nw_forward_t(Tensor scores, Tensor gap, Tensor temp, Tensor lengths) -> Tensor[]",
     "nw_value_grad_params": "nw_value_grad_params(Tensor scores, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor)",
+    # src/nw_affine/registry.cpp:37-39
+    "nw_affine_forward": "nw_affine_forward(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor[]",
+    "nw_affine_forward_t": "nw_affine_forward_t(Tensor scores, Tensor gap_open, Tensor gap_ext, Tensor temp, Tensor lengths) -> Tensor[]",
+    "nw_affine_value_grad_params": "nw_affine_value_grad_params(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
     # src/nw/registry.cpp:48-51
     "nw_marginals_backward": "nw_marginals_backward(Tensor scores, Tensor grad_marginals, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
     "nw_marginals_hvp": "nw_marginals_hvp(Tensor scores, Tensor v, float gap, float temp, Tensor? lengths) -> Tensor",
@@ -165,8 +169,9 @@ def _ptr(t):
     return None if t is None else t.data_ptr()
 
 
-def run_affine(scores, lengths, go, ge, temp, options=None):
-    """value, map, grad_open, grad_ext, grad_temp for a validated padded batch."""
+def run_affine(scores, lengths, go, ge, temp, options=None, family="sw_affine"):
+    """value, map, grad_open, grad_ext, grad_temp for a validated padded batch;
+    family "sw_affine" (local) or "nw_affine" (global alignment)."""
     B, L1, L2 = scores.shape
     dev = scores.device
     value = torch.empty(B, dtype=torch.float32, device=dev)
@@ -176,14 +181,15 @@ def run_affine(scores, lengths, go, ge, temp, options=None):
     g_T = torch.empty(B, dtype=torch.float32, device=dev)
     if B == 0:
         return value, amap, g_open, g_ext, g_T
-    nbytes = _LIB.swb_sw_affine_workspace_bytes(B, L1, L2)
+    name = "swb_nw_affine_forward" if family == "nw_affine" else "swb_sw_affine_forward"
+    nbytes = getattr(_LIB, name.replace("_forward", "_workspace_bytes"))(B, L1, L2)
     ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
     with torch.cuda.device(dev):
-        rc = _LIB.swb_sw_affine_forward(
+        rc = getattr(_LIB, name)(
             _ptr(scores), _ptr(lengths), B, L1, L2, float(go), float(ge), float(temp),
             _ptr(value), _ptr(amap), _ptr(g_open), _ptr(g_ext), _ptr(g_T), _ptr(ws), nbytes,
             _stream(dev), options)
-    _lib.check(rc, "swb_sw_affine_forward")
+    _lib.check(rc, name)
     return value, amap, g_open, g_ext, g_T
 
 
@@ -237,7 +243,8 @@ def run_value(fam, scores, lengths, params):
     value = torch.empty(B, dtype=torch.float32, device=dev)
     if B == 0:
         return value
-    name = {"sw": "swb_sw_value", "sw_affine": "swb_sw_affine_value", "nw": "swb_nw_value"}[fam]
+    name = {"sw": "swb_sw_value", "sw_affine": "swb_sw_affine_value", "nw": "swb_nw_value",
+            "nw_affine": "swb_nw_affine_value"}[fam]
     nbytes = int(getattr(_LIB, name + "_workspace_bytes")(B, L1, L2))
     ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     with torch.cuda.device(dev):
@@ -343,6 +350,38 @@ def nw_value_grad_params(scores, gap, temp, lengths):
     ln = _prep(scores, lengths, "nw")
     _, _, gg, gT = run_linear(scores, ln, gap, temp, family="nw")
     return gg, gT
+
+
+# ---- global alignment with affine gaps (Needleman-Wunsch affine) -------------
+
+def nw_affine_forward(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::nw_affine_forward -> [value [B], marginals [B, L1, L2]]
+    (src/nw_affine/torch_cuda.cpp:667 -> soft_nw_affine_cuda_float :364)."""
+    ln = _prep(scores, lengths, "nw_affine")
+    v, m, *_ = run_affine(scores, ln, gap_open, gap_ext, temp, family="nw_affine")
+    return [v, m]
+
+
+def nw_affine_forward_t(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::nw_affine_forward_t (src/nw_affine/torch_cuda.cpp:677 -> :352)."""
+    check_input_cuda(scores, "scores")
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    go = _scalar_param(gap_open, "gap_open")
+    ge = _scalar_param(gap_ext, "gap_ext")
+    T = _scalar_param(temp, "temperature")
+    B, L1, L2 = check_shape(scores, "nw_affine")
+    ln = resolve_lengths(lengths, B, L1, L2, scores.device)
+    v, m, *_ = run_affine(scores, ln, go, ge, T, family="nw_affine")
+    return [v, m]
+
+
+def nw_affine_value_grad_params(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::nw_affine_value_grad_params -> (value, dS/dgo, dS/dge, dS/dT), each [B]
+    (src/nw_affine/torch_cuda.cpp:688-702 -> soft_nw_affine_cuda_with_grads :387)."""
+    ln = _prep(scores, lengths, "nw_affine")
+    v, _, go, ge, gT = run_affine(scores, ln, gap_open, gap_ext, temp, family="nw_affine")
+    return v, go, ge, gT
 
 
 # ---- second-order ops --------------------------------------------------------
@@ -555,6 +594,9 @@ IMPLS = {
     "nw_forward": nw_forward,
     "nw_forward_t": nw_forward_t,
     "nw_value_grad_params": nw_value_grad_params,
+    "nw_affine_forward": nw_affine_forward,
+    "nw_affine_forward_t": nw_affine_forward_t,
+    "nw_affine_value_grad_params": nw_affine_value_grad_params,
 }
 
 for _name, _fn in IMPLS.items():
@@ -606,6 +648,8 @@ class _ForwardFn(torch.autograd.Function):
                 gs = gs + gv.view(-1, 1, 1) * m
             if want_p:
                 grads = _below(getattr(ops, f"{fam}_value_grad_params"), scores, *vals, ln)
+                if fam == "nw_affine":   # (value, grads...): src/nw_affine/torch_cuda.cpp:696
+                    grads = grads[1:]
                 pg = [(gv * g).sum() for g in grads]
         if gm is not None:
             gmc = gm.contiguous()
@@ -635,7 +679,9 @@ def _autograd_forward(fam, tensor_params):
 for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True),
                         ("sw_affine_forward", "sw_affine", False),
                         ("sw_affine_forward_t", "sw_affine", True),
-                        ("nw_forward", "nw", False), ("nw_forward_t", "nw", True)):
+                        ("nw_forward", "nw", False), ("nw_forward_t", "nw", True),
+                        ("nw_affine_forward", "nw_affine", False),
+                        ("nw_affine_forward_t", "nw_affine", True)):
     _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
 
 
@@ -761,6 +807,8 @@ OWN_SCHEMAS = {
     "sw_affine_value": "sw_affine_value(Tensor scores, float gap_open, float gap_ext, float temp, "
                        "Tensor? lengths) -> Tensor",
     "nw_value": "nw_value(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
+    "nw_affine_value": "nw_affine_value(Tensor scores, float gap_open, float gap_ext, float temp, "
+                       "Tensor? lengths) -> Tensor",
 }
 _OWN_LIB = torch.library.Library("orihime_b200", "DEF")
 for _name, _schema in OWN_SCHEMAS.items():
@@ -784,7 +832,13 @@ def _own_nw_value(scores, gap, temp, lengths):
 
 _OWN_LIB.impl("sw_value", _own_sw_value, "CUDA")
 _OWN_LIB.impl("sw_affine_value", _own_sw_affine_value, "CUDA")
+def _own_nw_affine_value(scores, gap_open, gap_ext, temp, lengths):
+    ln = _prep(scores, lengths, "nw_affine")
+    return run_value("nw_affine", scores, ln, (gap_open, gap_ext, temp))
+
+
 _OWN_LIB.impl("nw_value", _own_nw_value, "CUDA")
+_OWN_LIB.impl("nw_affine_value", _own_nw_affine_value, "CUDA")
 
 # Meta shapes, FP32 autocast and vmap rules for the ops defined here (when the
 # reference extension defined them, its own Python package registers these).

@@ -31,13 +31,14 @@ import torch
 from . import _ops
 
 _BATCH_ARGS = frozenset({"scores", "v", "grad_marginals", "lengths"})
-_NPARAMS = {"sw": 2, "sw_affine": 3, "nw": 2}
+_NPARAMS = {"sw": 2, "sw_affine": 3, "nw": 2, "nw_affine": 3}
 
 
 def _fam(name: str) -> str:
-    if name.startswith("sw_affine"):
-        return "sw_affine"
-    return "nw" if name.startswith("nw") else "sw"
+    for f in ("sw_affine", "nw_affine", "nw"):
+        if name.startswith(f):
+            return f
+    return "sw"
 
 
 # ---- fake impls -------------------------------------------------------------
@@ -74,7 +75,8 @@ def _fake_for(name: str):
     if name.endswith("_forward") or name.endswith("_forward_t"):
         return _fake_forward
     if name.endswith("_value_grad_params"):
-        return _fake_grad_params(n)
+        # nw_affine's also returns the value first (src/nw_affine/registry.cpp:39)
+        return _fake_grad_params(n + 1 if name.startswith("nw_affine") else n)
     if name.endswith("_marginals_backward"):
         return _fake_backward(n)
     return _fake_map

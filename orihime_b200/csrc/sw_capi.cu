@@ -36,7 +36,7 @@ constexpr size_t kAlign = 256;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
-template <int NS, int R> constexpr int np() { return swb::Dims<NS, R>::NP; }
+template <int NS, bool G = false> constexpr int np() { return swb::push_channels<NS, G>(); }
 template <int NS, int R> constexpr int ckrs() { return swb::Dims<NS, R>::CKRS; }
 template <int NS, int R> constexpr int ne() { return swb::Dims<NS, R>::NE; }
 
@@ -73,14 +73,14 @@ Layout layout_sizes(long long B, size_t slots, size_t edge_floats, size_t bp_flo
 int chunks_for(long long L1) { return (int)((L1 + 31 + swb::C_STEPS - 1) / swb::C_STEPS); }
 
 // Padded batch: every pair gets the slices of a Lmax1 x Lmax2 pair.
-template <int NS, int R>
+template <int NS, int R, bool G = false>
 Layout layout_for(long long B, long long L1m, long long L2m) {
   int nb = (int)((L2m + 32 * R - 1) / (32 * R));
   if (nb < 1) nb = 1;
   const int nch = chunks_for(L1m);
   const size_t slots = (size_t)B * nb;
   Layout l = layout_sizes(B, slots, slots * ne<NS, R>() * (size_t)L1m,
-                          slots * np<NS, R>() * (size_t)(L1m + 1),
+                          slots * np<NS, G>() * (size_t)(L1m + 1),
                           slots * (size_t)nch * ckrs<NS, R>());
   l.nb = nb;
   l.nchunks = nch;
@@ -103,7 +103,7 @@ size_t plan_bytes_for(long long B, long long ntasks) {
 // Occupancy of each kernel instantiation on one device, computed once.
 struct DevInfo {
   int sms = 0;
-  int occ[2][3][2] = {};   // [kernel fwd/bwd][model: linear, affine, global linear][R == 4?]
+  int occ[2][4][2] = {};   // [kernel fwd/bwd][model: linear, affine, global linear, global affine][R == 4?]
   bool ready = false;
 };
 DevInfo g_dev[64];
@@ -112,7 +112,7 @@ std::mutex g_mu;
 template <int NS, int R>
 size_t bwd_smem() { return (size_t)kWarpsBwd * swb::bwd_smem_floats<NS, R>() * sizeof(float); }
 
-template <int NS, bool G> constexpr int model_index() { return NS == 3 ? 1 : (G ? 2 : 0); }
+template <int NS, bool G> constexpr int model_index() { return NS == 3 ? (G ? 3 : 1) : (G ? 2 : 0); }
 
 template <int NS, int R, bool G = false>
 cudaError_t setup_pair(DevInfo& d) {
@@ -138,7 +138,8 @@ int dev_info(DevInfo** out) {
     if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       return SWB_ERR_CUDA;
     if (setup_pair<1, 2>(d) || setup_pair<1, 4>(d) || setup_pair<3, 2>(d) || setup_pair<3, 4>(d) ||
-        setup_pair<1, 2, true>(d) || setup_pair<1, 4, true>(d))
+        setup_pair<1, 2, true>(d) || setup_pair<1, 4, true>(d) || setup_pair<3, 2, true>(d) ||
+        setup_pair<3, 4, true>(d))
       return SWB_ERR_CUDA;
     d.ready = true;
   }
@@ -232,7 +233,7 @@ int launch_padded_r(const float* scores, const int* lengths, int B, int L1m, int
   const size_t map_elems = (size_t)B * L1m * L2m;
   if (!value || !g_open || !g_T || (NS == 3 && !g_ext)) return SWB_ERR_ARG;
   if (map_elems > 0 && (!scores || !map)) return SWB_ERR_ARG;
-  const Layout l = layout_for<NS, R>(B, L1m, L2m);
+  const Layout l = layout_for<NS, R, G>(B, L1m, L2m);
   Args a{};
   a.scores = scores; a.map = map; a.lengths = lengths;
   a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
@@ -257,14 +258,14 @@ int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L
 }
 
 // Padded value-only batch: the forward wavefront, no checkpoints, no adjoint.
-template <int NS>
+template <int NS, bool G = false>
 Layout value_layout(long long B, long long L1m, long long L2m) {
   constexpr int R = kDefaultR;
   int nb = (int)((L2m + 32 * R - 1) / (32 * R));
   if (nb < 1) nb = 1;
   const size_t slots = (size_t)B * nb;
   Layout l = layout_sizes(B, slots, slots * ne<NS, R>() * (size_t)L1m,
-                          slots * np<NS, R>() * (size_t)(L1m + 1), 0);
+                          slots * np<NS, G>() * (size_t)(L1m + 1), 0);
   l.nb = nb;
   l.nchunks = chunks_for(L1m);
   return l;
@@ -277,7 +278,7 @@ int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   if (B == 0) return SWB_OK;
   if (!value || ((size_t)B * L1m * L2m > 0 && !scores)) return SWB_ERR_ARG;
-  const Layout l = value_layout<NS>(B, L1m, L2m);
+  const Layout l = value_layout<NS, G>(B, L1m, L2m);
   Args a{};
   a.scores = scores; a.map = nullptr; a.lengths = lengths;
   a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
@@ -295,7 +296,8 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
                   bool value_only = false) {
   if (!host_plan || !dev_plan) return SWB_ERR_ARG;
   const long long* h = static_cast<const long long*>(host_plan);
-  if (h[HW_MAGIC] != kPlanMagic || (h[HW_FAMILY] & 0xff) != (G ? 2 : NS)) return SWB_ERR_ARG;
+  if (h[HW_MAGIC] != kPlanMagic || (h[HW_FAMILY] & 0xff) != (G ? (NS == 3 ? 4 : 2) : NS))
+    return SWB_ERR_ARG;
   const int r = (int)(h[HW_FAMILY] >> 8);
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   const long long B = h[HW_B], ntasks = h[HW_NTASKS];
@@ -626,6 +628,49 @@ int swb_nw_forward(const float* scores, const int* lengths, int B, int L1max, in
                                 opt);
 }
 
+size_t swb_nw_affine_workspace_bytes(int B, int L1max, int L2max) {
+  if (B <= 0) return 0;
+  return std::max(layout_for<3, 2, true>(B, L1max, L2max).total,
+                  layout_for<3, 4, true>(B, L1max, L2max).total);
+}
+
+int swb_nw_affine_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap_open, float gap_ext, float temp, float* value, float* map,
+                          float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                          size_t workspace_bytes, void* stream, const swb_options* opt) {
+  return launch_padded<3, true>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value,
+                                map, grad_open, grad_ext, grad_temp, workspace, workspace_bytes,
+                                stream, opt);
+}
+
+size_t swb_nw_affine_value_workspace_bytes(int B, int L1max, int L2max) {
+  return B > 0 ? value_layout<3, true>(B, L1max, L2max).total : 0;
+}
+
+int swb_nw_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                        float gap_open, float gap_ext, float temp, float* value, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+  return launch_value<3, true>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value,
+                               workspace, workspace_bytes, stream);
+}
+
+int swb_nw_affine_ragged(const float* scores, const void* host_plan, const void* dev_plan,
+                         float gap_open, float gap_ext, float temp, float* value, float* map,
+                         float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                         size_t workspace_bytes, void* stream, const swb_options* opt) {
+  return launch_ragged<3, true>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value, map,
+                                grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream,
+                                opt);
+}
+
+int swb_nw_affine_ragged_value(const float* scores, const void* host_plan, const void* dev_plan,
+                               float gap_open, float gap_ext, float temp, float* value,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_ragged<3, true>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value,
+                                nullptr, nullptr, nullptr, nullptr, workspace, workspace_bytes,
+                                stream, nullptr, true);
+}
+
 size_t swb_nw_value_workspace_bytes(int B, int L1max, int L2max) {
   return swb_sw_value_workspace_bytes(B, L1max, L2max);
 }
@@ -640,11 +685,12 @@ int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const lon
                     int B, void* plan, size_t plan_capacity, size_t* plan_bytes,
                     size_t* workspace_bytes) {
   const int R = cols_per_lane ? cols_per_lane : kDefaultR;
-  // family: 1 linear, 3 affine, 2 global alignment (linear gap; the linear model's buffers)
-  if ((family < 1 || family > 3) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
+  // family: 1 linear, 3 affine, 2 global linear, 4 global affine
+  if ((family < 1 || family > 4) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
     return SWB_ERR_ARG;
-  const int ns = family == 3 ? 3 : 1;
-  const int NE = 2 * ns, NP = (ns == 3) ? 5 : 2, CKRS = (2 * ns * R + 2 * ns) * 32 + 4;
+  const int ns = (family == 3 || family == 4) ? 3 : 1;
+  const int NE = 2 * ns, NP = family == 4 ? 6 : (ns == 3 ? 5 : 2);
+  const int CKRS = (2 * ns * R + 2 * ns) * 32 + 4;
   // validate the packing: row pitch round4(L2), offsets multiples of 4 floats
   long long ntasks = 0;
   for (int b = 0; b < B; ++b) {

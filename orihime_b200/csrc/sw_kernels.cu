@@ -135,9 +135,19 @@ struct Place {
   Pair pr;
 };
 
-template <int NS, int R>
+// Push channels crossing a lane or band edge backward: local affine 5 (left
+// M, D; diagonal M, I, D), global affine 6 (left M, I, D; diagonal M, I, D),
+// linear 2 (left, diagonal); the first push_left of them are left pushes.
+template <int NS, bool G> __host__ __device__ constexpr int push_channels() {
+  return NS == 3 ? (G ? 6 : 5) : 2;
+}
+template <int NS, bool G> __host__ __device__ constexpr int push_left() {
+  return NS == 3 ? (G ? 3 : 2) : 1;
+}
+
+template <int NS, int R, bool G = false>
 __device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_band) {
-  constexpr int NE = 2 * NS, NP = (NS == 3) ? 5 : 2, CKRS = (2 * NS * R + 2 * NS) * 32 + 4;
+  constexpr int NE = 2 * NS, NP = push_channels<NS, G>(), CKRS = (2 * NS * R + 2 * NS) * 32 + 4;
   Place w;
   Pair& r = w.pr;
   if (a.layout == 0) {
@@ -338,6 +348,44 @@ __device__ __forceinline__ void nmul(int n, float g, float& h, float& l) {
   l = fmaf((float)n, g, -h);
 }
 
+// go + n * ge as a pair (the affine global boundaries I(i,0), D(0,j) with
+// n = i - 1, j - 1; scaled gaps).
+__device__ __forceinline__ void gpair(int n, float go, float ge, float& h, float& l) {
+  float ph, pl, th, tl;
+  nmul(n, ge, ph, pl);
+  two_sum(go, ph, th, tl);
+  h = th;
+  l = tl + pl;
+}
+
+// Row-0 values of a global alignment at column j (1-based; j = 0 is the
+// origin): linear A = j * gap; affine M = [j == 0] * 0, I = NEG,
+// D = go + (j - 1) ge.  (h, l) per state.
+template <int NS>
+__device__ __forceinline__ void row0(int j, float g0, float g1, float (&h)[NS], float (&l)[NS]) {
+  if constexpr (NS == 1) {
+    nmul(j, g0, h[0], l[0]);
+  } else {
+    h[0] = j == 0 ? 0.f : NEG; l[0] = 0.f;
+    h[1] = NEG; l[1] = 0.f;
+    if (j >= 1) gpair(j - 1, g0, g1, h[2], l[2]);
+    else { h[2] = NEG; l[2] = 0.f; }
+  }
+}
+
+// Column-0 values at row i >= 1 as an edge record (hi of each state, then lo):
+// linear A = i * gap; affine M = NEG, I = go + (i - 1) ge, D = NEG.
+template <int NS>
+__device__ __forceinline__ void col0_edge(int i, float g0, float g1, float (&e)[2 * NS]) {
+  if constexpr (NS == 1) {
+    nmul(i, g0, e[0], e[1]);
+  } else {
+    e[0] = NEG; e[3] = 0.f;
+    gpair(i - 1, g0, g1, e[1], e[4]);
+    e[2] = NEG; e[5] = 0.f;
+  }
+}
+
 // Adjoint fields of column c in one step's shared-memory entry `ent`, stored
 // column block by column block; inside a block each field group is one
 // vector per lane (lane-contiguous, so every warp access is conflict-free).
@@ -419,13 +467,49 @@ __device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
                                           const float (&s)[R], float g0, float g1,
                                           float Sh = 0.f, float Sl = 0.f, int nlive = 0,
                                           float* went = nullptr, int lane = 0, bool hold = false) {
-  static_assert(!G || NS == 1, "global alignment is built for the linear model");
+  // G, NS == 3 (global affine): M = s + LSE(M, I, D at diag);
+  // I = LSE(M + go, I + ge, D + go) from above; D = LSE(M + go, I + go, D + ge)
+  // from the left.  Fields: A = (wMM, wMI, wMD, wIM), B = (wII, wDM, wDD, s),
+  // and the init slots carry (wID, wDI).
   float dgh[NS], dgl[NS], lh[NS], ll[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) { dgh[q] = dgh0[q]; dgl[q] = dgl0[q]; lh[q] = lfh[q]; ll[q] = lfl[q]; }
 #pragma unroll
   for (int c = 0; c < R; ++c) {
-    if constexpr (NS == 3) {
+    if constexpr (NS == 3 && G) {
+      const float uMh = ph[0][c], uMl = pl[0][c], uIh = ph[1][c], uIl = pl[1][c];
+      const float uDh = ph[2][c], uDl = pl[2][c];
+      const float r = fmaxf(fmaxf(dgh[0], dgh[1]), dgh[2]);
+      const float tM = ex2((dgh[0] - r) + dgl[0]), tI = ex2((dgh[1] - r) + dgl[1]);
+      const float tD = ex2((dgh[2] - r) + dgl[2]);
+      const float sm = (tM + tI) + tD;
+      float Mh, Ml;
+      two_sum(r, s[c], Mh, Ml);
+      Ml += lg2(sm);
+      const float ru = fmaxf(fmaxf(uMh + g0, uIh + g1), uDh + g0);
+      const float ta = ex2(((uMh - ru) + g0) + uMl), tb = ex2(((uIh - ru) + g1) + uIl);
+      const float tc = ex2(((uDh - ru) + g0) + uDl);
+      const float si = (ta + tb) + tc;
+      float Ih, Il;
+      fast2(ru, lg2(si), Ih, Il);
+      const float rl = fmaxf(fmaxf(lh[0] + g0, lh[1] + g0), lh[2] + g1);
+      const float td = ex2(((lh[0] - rl) + g0) + ll[0]), te = ex2(((lh[1] - rl) + g0) + ll[1]);
+      const float tf = ex2(((lh[2] - rl) + g1) + ll[2]);
+      const float sd = (td + te) + tf;
+      float Dh, Dl;
+      fast2(rl, lg2(sd), Dh, Dl);
+      if (hold) { Mh = uMh; Ml = uMl; Ih = uIh; Il = uIl; Dh = uDh; Dl = uDl; }
+      if constexpr (WT) {
+        const float vm = hold ? 0.f : recip(sm), vi = hold ? 0.f : recip(si);
+        const float vd = hold ? 0.f : recip(sd);
+        put_weights<NS, R>(went, lane, c, make_float4(tM * vm, tI * vm, tD * vm, ta * vi),
+                           make_float4(tb * vi, td * vd, tf * vd, 0.f), s[c]);
+        put_inits<NS, R>(went, lane, c, tc * vi, te * vd, 0.f);
+      }
+      dgh[0] = uMh; dgl[0] = uMl; dgh[1] = uIh; dgl[1] = uIl; dgh[2] = uDh; dgl[2] = uDl;
+      lh[0] = Mh; ll[0] = Ml; lh[1] = Ih; ll[1] = Il; lh[2] = Dh; ll[2] = Dl;
+      ph[0][c] = Mh; pl[0][c] = Ml; ph[1][c] = Ih; pl[1][c] = Il; ph[2][c] = Dh; pl[2][c] = Dl;
+    } else if constexpr (NS == 3) {
       const float uMh = ph[0][c], uMl = pl[0][c], uIh = ph[1][c], uIl = pl[1][c];
       const float uDh = ph[2][c], uDl = pl[2][c];
       // M = s + LSE(M, I, D at diag, 0).  The reference point of each LSE
@@ -526,6 +610,22 @@ __device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
   return false;
 }
 
+// Value of a global alignment at a terminal cell (column c): linear A;
+// affine LSE(M, I, D) as a pair.
+template <int NS, int R>
+__device__ __forceinline__ void term_value(const float (&ph)[NS][R], const float (&pl)[NS][R], int c,
+                                           float& h, float& l) {
+  if constexpr (NS == 1) {
+    h = ph[0][c];
+    l = pl[0][c];
+  } else {
+    const float r = fmaxf(fmaxf(ph[0][c], ph[1][c]), ph[2][c]);
+    const float sm = (ex2((ph[0][c] - r) + pl[0][c]) + ex2((ph[1][c] - r) + pl[1][c])) +
+                     ex2((ph[2][c] - r) + pl[2][c]);
+    fast2(r, lg2(sm), h, l);
+  }
+}
+
 // Steps of a band, padded to whole checkpoint chunks (the padding steps find
 // every lane past the last row and do nothing).
 __device__ __forceinline__ int band_chunks(int L1) { return (L1 + 31 + C_STEPS - 1) / C_STEPS; }
@@ -574,10 +674,15 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
 #pragma unroll
     for (int c = 0; c < R; ++c) { ph[q][c] = NEG; pl[q][c] = 0.f; }
   }
-  if constexpr (G) {   // row 0: A[0,j] = j * gap; lh = A[0, jl] (left of the lane)
-    nmul(jl, g0, lh[0], ll[0]);
+  if constexpr (G) {   // row 0 (A[0,j] = j * gap, affine D(0,j) = go + (j-1) ge); lh = column jl
+    row0<NS>(jl, g0, g1, lh, ll);
 #pragma unroll
-    for (int c = 0; c < R; ++c) nmul(jl + c + 1, g0, ph[0][c], pl[0][c]);
+    for (int c = 0; c < R; ++c) {
+      float h[NS], l[NS];
+      row0<NS>(jl + c + 1, g0, g1, h, l);
+#pragma unroll
+      for (int q = 0; q < NS; ++q) { ph[q][c] = h[q]; pl[q][c] = l[q]; }
+    }
   }
   float ref = 0.f;
   KSum acc;
@@ -593,7 +698,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
     const bool ok = ein && lane < C_STEPS && i <= L1;
 #pragma unroll
     for (int f = 0; f < NE; ++f) dst[f] = ok ? ld_poll(ein + f * Lm + (i - 1)) : 0.f;
-    if (left_bnd) nmul(i, g0, dst[0], dst[1]);
+    if (left_bnd) col0_edge<NS>(i, g0, g1, dst);
   };
   load_edge(0, eb);
   float sb[PF][R];  // per-lane score ring, PF steps ahead
@@ -672,18 +777,21 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
         fwd_cells<NS, R, false, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, 0.f, 0.f, 0, nullptr,
                                       lane, i < 1);
         if (act) {
-          if (term_lane && i == L1) {   // the terminal cell A[L1, L2]
+          if (term_lane && i == L1) {   // the terminal: A[L1, L2], affine LSE of M, I, D there
             float th = 0.f, tl = 0.f;
 #pragma unroll
             for (int c = 0; c < R; ++c)
-              if (jl + c == L2 - 1) { th = ph[0][c]; tl = pl[0][c]; }
+              if (jl + c == L2 - 1) term_value<NS>(ph, pl, c, th, tl);
             part[0] = th;
             part[1] = tl;
             cmx = 1e30f;
           }
           if (lane == 31) {
-            eout[(i - 1)] = ph[0][R - 1];
-            eout[Lm + (i - 1)] = pl[0][R - 1];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+              eout[q * Lm + (i - 1)] = ph[q][R - 1];
+              eout[(NS + q) * Lm + (i - 1)] = pl[q][R - 1];
+            }
           }
         }
         continue;
@@ -751,7 +859,7 @@ __global__ void __launch_bounds__(128) fwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 0, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    fwd_band<NS, R, G>(a, place_of<NS, R>(a, task, false), lane, deadline);
+    fwd_band<NS, R, G>(a, place_of<NS, R, G>(a, task, false), lane, deadline);
   }
 }
 
@@ -799,17 +907,40 @@ __device__ __forceinline__ void pair_logz(const Args& a, const Place& w, int lan
 }
 
 // Global alignment: S' = the terminal value the band holding column L2 wrote,
-// or (L1 + L2) * gap when a side is empty (the terminal is a boundary cell).
-template <int R>
+// or, when a side is empty, the boundary cell's: linear (L1 + L2) * gap;
+// affine go + (n - 1) ge for n = L1 + L2 > 0, 0 at the origin.
+template <int NS, int R>
 __device__ __forceinline__ void pair_term(const Args& a, const Place& w, float& Sh, float& Sl) {
   const int L1 = w.pr.L1, L2 = w.pr.L2;
   if (L1 == 0 || L2 == 0) {
-    nmul(L1 + L2, a.go * a.k, Sh, Sl);
+    const int n = L1 + L2;
+    if (NS == 1) {
+      nmul(n, a.go * a.k, Sh, Sl);
+    } else if (n > 0) {
+      gpair(n - 1, a.go * a.k, a.ge * a.k, Sh, Sl);
+    } else {
+      Sh = 0.f;
+      Sl = 0.f;
+    }
     return;
   }
   const float* q = a.part + 2 * (w.slot0 + (L2 - 1) / (32 * R));
   Sh = q[0];
   Sl = q[1];
+}
+
+// Natural-unit value and dS/d(go, ge) of a global alignment with an empty
+// side (the reference's float expressions: n * gap; go + (n - 1) * ge).
+template <int NS>
+__device__ __forceinline__ float empty_global_value(const Args& a, int n, float& dgo, float& dge) {
+  if (NS == 1) {
+    dgo = (float)n;
+    dge = 0.f;
+    return (float)n * a.go;
+  }
+  dgo = n > 0 ? 1.f : 0.f;
+  dge = n > 0 ? (float)(n - 1) : 0.f;
+  return n > 0 ? a.go + (float)(n - 1) * a.ge : 0.f;
 }
 
 // Value-only calls: one warp per pair folds the forward's band partials into
@@ -823,7 +954,7 @@ __global__ void __launch_bounds__(128) value_kernel(Args a) {
   if (q >= a.B) return;
   Place w;
   if (a.layout == 0) {
-    w = place_of<NS, R>(a, q * a.nb, false);
+    w = place_of<NS, R, G>(a, q * a.nb, false);
   } else {
     const long long* pw = a.plan_pairs + (size_t)q * PLAN_PAIR_WORDS;
     w.p = q;
@@ -835,11 +966,11 @@ __global__ void __launch_bounds__(128) value_kernel(Args a) {
   float Sh, Sl;
   if constexpr (G) {
     if (lane == 0) {
-      const int n = w.pr.L1 + w.pr.L2;
-      if (w.pr.L1 == 0 || w.pr.L2 == 0) {
-        a.value[w.p] = (float)n * a.go;   // exactly the boundary cell's value
+      if (w.pr.L1 == 0 || w.pr.L2 == 0) {   // exactly the boundary cell's value
+        float dgo, dge;
+        a.value[w.p] = empty_global_value<NS>(a, w.pr.L1 + w.pr.L2, dgo, dge);
       } else {
-        pair_term<R>(a, w, Sh, Sl);
+        pair_term<NS, R>(a, w, Sh, Sl);
         a.value[w.p] = (Sh + Sl) * (1.f / a.k);
       }
     }
@@ -873,11 +1004,11 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
       const float S = (Sh + Sl) * inv_k;
       const float match = ps * inv_k;
       if (G && (w.pr.L1 == 0 || w.pr.L2 == 0)) {
-        // the terminal is the boundary cell (L1 + L2) * gap: dS/dgap = L1 + L2, dS/dT = 0
-        const int n = w.pr.L1 + w.pr.L2;
-        a.value[p] = (float)n * a.go;
-        a.g_open[p] = (float)n;
-        if (a.g_ext) a.g_ext[p] = 0.f;
+        // the terminal is a boundary cell: its value, its gap derivatives, dS/dT = 0
+        float dgo, dge;
+        a.value[p] = empty_global_value<NS>(a, w.pr.L1 + w.pr.L2, dgo, dge);
+        a.g_open[p] = dgo;
+        if (a.g_ext) a.g_ext[p] = dge;
         a.g_T[p] = 0.f;
         return;
       }
@@ -913,13 +1044,14 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
 template <int NS, int R, bool G = false>
 __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uint64_t deadline) {
   using D = Dims<NS, R>;
-  constexpr int NP = D::NP, EW = D::EW, CKF = D::CKF, CKRS = D::CKRS, NE = D::NE;
+  constexpr int NP = push_channels<NS, G>(), NL = push_left<NS, G>();
+  constexpr int EW = D::EW, CKF = D::CKF, CKRS = D::CKRS, NE = D::NE;
   const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
   const int band = w.band;
   const int col0 = band * 32 * R;
   float Sh, Sl;
-  if constexpr (G) pair_term<R>(a, w, Sh, Sl);
+  if constexpr (G) pair_term<NS, R>(a, w, Sh, Sl);
   else pair_logz(a, w, lane, Sh, Sl);
   if (!(L1 > 0 && col0 < L2)) {
     finish_pair<NS, G>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f);
@@ -953,14 +1085,14 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
     const bool ok = ein && lane < C_STEPS && i <= L1;
 #pragma unroll
     for (int f = 0; f < NE; ++f) ebr[f] = ok ? ein[f * Lm + (i - 1)] : (f < NS ? NEG : 0.f);
-    if (G && band == 0) nmul(i, g0, ebr[0], ebr[1]);   // column-0 boundary i * gap
+    if (G && band == 0) col0_edge<NS>(i, g0, g1, ebr);   // column-0 boundary
   };
   auto load_pb = [&](int kc, float (&dst)[NP]) {
     const int i = kc * C_STEPS + C_STEPS - 1 - lane - 30;  // lane 31's row at step end-1-lane
     const bool ok = pin && lane < C_STEPS && i >= 1 && i <= L1;
 #pragma unroll
     for (int f = 0; f < NP; ++f) {
-      const bool left = (NS == 3) ? (f < 2) : (f < 1);
+      const bool left = f < NL;
       dst[f] = (ok && (left || i < L1)) ? ld_poll(pin + f * (Lm + 1) + i) : 0.f;
     }
   };
@@ -1037,7 +1169,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
               if (lane == 0 && pout) {
 #pragma unroll
                 for (int f = 0; f < NP; ++f) {
-                  const bool left = (NS == 3) ? (f < 2) : (f < 1);
+                  const bool left = f < NL;
                   pout[f * (Lm + 1) + (left ? i : i - 1)] = 0.f;
                 }
               }
@@ -1072,7 +1204,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
             if (pin && ir >= 1 && ir <= L1) {
 #pragma unroll
               for (int f = 0; f < NP; ++f) {
-                const bool left = (NS == 3) ? (f < 2) : (f < 1);
+                const bool left = f < NL;
                 if (left || ir < L1) {
                   const float v = ld_poll(pin + f * (Lm + 1) + ir);
                   q = q && !is_sentinel(v) && v < kFlowTiny;
@@ -1104,6 +1236,9 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
     float ph[NS][R], pl[NS][R], lh[NS], ll[NS];
     ck_unpack<NS, R>(ckr, ph, pl, lh, ll);
     unsigned initbits = 0;   // bit u: step u of the chunk wrote its beta-inits
+    float tw[NS];            // G: the terminal's beta-inits (softmax of its states; linear 1)
+#pragma unroll
+    for (int q = 0; q < NS; ++q) tw[q] = 0.f;
 #pragma unroll 1
     for (int u0 = 0; u0 < C_STEPS; u0 += PF)
 #pragma unroll
@@ -1140,6 +1275,14 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
       if (fwd_cells<NS, R, true, G>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, Sh, Sl, act ? ncols : 0,
                                     sm + (size_t)cu * EW * 32, lane, G && i < 1))
         initbits |= 1u << cu;
+      if (G && term_lane && i == L1) {
+#pragma unroll
+        for (int c = 0; c < R; ++c)
+          if (jl + c == L2 - 1)
+#pragma unroll
+            for (int q = 0; q < NS; ++q)
+              tw[q] = NS == 1 ? 1.f : ex2((ph[q][c] - Sh) + (pl[q][c] - Sl));
+      }
     }
     if (kc > 0) {  // prefetch the next chunk's inputs while the adjoint runs
       load_ck(kc - 1);
@@ -1163,9 +1306,9 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
         r[q] = __shfl_down_sync(FULL, outp[q], 1);
         pw[q] = __shfl_sync(FULL, pbc[q], cu);
       }
-      // pushes arriving at column R-1 of row i: left pushes (NS==3: M,D; NS==1: A)
-      // and diag pushes (NS==3: M,I,D; NS==1: A)
-      float inL[2], inD[NS];
+      // pushes arriving at column R-1 of row i: left pushes (local affine: M, D;
+      // global affine: M, I, D; linear: A) and diag pushes (M, I, D; linear: A)
+      float inL[3], inD[NS];
       {
         bool miss = false;
 #pragma unroll
@@ -1179,26 +1322,24 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
                                  a.status, 0.f);
         }
       }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) inL[q] = 0.f;
       if (lane == 31) {
-        if constexpr (NS == 3) {
-          inL[0] = pw[0]; inL[1] = pw[1];
 #pragma unroll
-          for (int q = 0; q < 3; ++q) inD[q] = pw[2 + q];
-        } else {
-          inL[0] = pw[0]; inL[1] = 0.f;
-          inD[0] = pw[1];
-        }
+        for (int q = 0; q < NL; ++q) inL[q] = pw[q];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) inD[q] = pw[NL + q];
       } else {
-        if constexpr (NS == 3) {
-          inL[0] = r[0]; inL[1] = r[1];
 #pragma unroll
-          for (int q = 0; q < 3; ++q) { inD[q] = hold[q]; hold[q] = r[2 + q]; }
-        } else {
-          inL[0] = r[0]; inL[1] = 0.f;
-          inD[0] = hold[0]; hold[0] = r[1];
-        }
+        for (int q = 0; q < NL; ++q) inL[q] = r[q];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) { inD[q] = hold[q]; hold[q] = r[NL + q]; }
       }
-      if constexpr (NS == 3) {
+      if constexpr (NS == 3 && G) {
+        ac[0][R - 1] += inL[0] + inD[0];
+        ac[1][R - 1] += inL[1] + inD[1];
+        ac[2][R - 1] += inL[2] + inD[2];
+      } else if constexpr (NS == 3) {
         ac[0][R - 1] += inL[0] + inD[0];
         ac[1][R - 1] += inD[1];
         ac[2][R - 1] += inL[1] + inD[2];
@@ -1206,10 +1347,12 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
         ac[0][R - 1] += inL[0] + inD[0];
       }
       if constexpr (G) {
-        if (term_lane && i == L1) {   // beta = 1 at the terminal cell
+        if (term_lane && i == L1) {   // the terminal's beta-inits
 #pragma unroll
           for (int c = 0; c < R; ++c)
-            if (jl + c == L2 - 1) ac[0][c] += 1.f;
+            if (jl + c == L2 - 1)
+#pragma unroll
+              for (int q = 0; q < NS; ++q) ac[q][c] += tw[q];
         }
       }
 #pragma unroll
@@ -1220,7 +1363,39 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
         // cells outside the pair carry beta-init 0 and receive only zero
         // pushes (their successors are outside too, or their weight toward
         // a NEG predecessor is 0), so beta needs no mask
-        if constexpr (NS == 3) {
+        if constexpr (NS == 3 && G) {
+          float4 f0, f1;
+          float sc, wID, wDI, unused;
+          get_weights<NS, R>(E, lane, c, f0, f1, sc);
+          get_inits<NS, R>(E, lane, c, wID, wDI, unused);
+          // f0 = (wMM, wMI, wMD, wIM), f1 = (wII, wDM, wDD, s), (wID, wDI)
+          const float bM = ac[0][c], bI = ac[1][c], bD = ac[2][c];
+          pm[c] = bM;
+          const float pIM = bI * f0.w, pII = bI * f1.x, pID = bI * wID;
+          const float pDM = bD * f1.y, pDI = bD * wDI, pDD = bD * f1.z;
+          const float qM = bM * f0.x, qI = bM * f0.y, qD = bM * f0.z;
+          cA += (pIM + pID) + (pDM + pDI);
+          cB += pII + pDD;
+          cS += bM * sc;
+          // pushes into the boundary states D(0, j) (row 0) and I(i, 0)
+          // (column 0): gap_open once, gap_ext (n - 1) times; pushes toward
+          // the NEG boundary states are 0
+          if (i == 1) {
+            cA += pID + qD;
+            cB += (float)(jl + c) * pID + (float)(jl + c - 1) * qD;
+          }
+          if (band == 0 && lane == 0 && c == 0) {
+            cA += pDI + qI;
+            cB += (float)(i - 1) * pDI + (float)(i - 2) * qI;
+          }
+          nx[0][c] += pIM; nx[1][c] += pII; nx[2][c] += pID;
+          if (c > 0) {
+            nx[0][c - 1] += qM; nx[1][c - 1] += qI; nx[2][c - 1] += qD;
+            ac[0][c - 1] += pDM; ac[1][c - 1] += pDI; ac[2][c - 1] += pDD;
+          } else {
+            outp[0] = pDM; outp[1] = pDI; outp[2] = pDD; outp[3] = qM; outp[4] = qI; outp[5] = qD;
+          }
+        } else if constexpr (NS == 3) {
           float4 f0, f1;
           float sc;
           get_weights<NS, R>(E, lane, c, f0, f1, sc);
@@ -1276,16 +1451,8 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
       if (act) {
         store_row<R>(pr, i, jl, pm);
         if (lane == 0 && pout) {
-          if constexpr (NS == 3) {
-            pout[0 * (Lm + 1) + i] = outp[0];
-            pout[1 * (Lm + 1) + i] = outp[1];
-            pout[2 * (Lm + 1) + (i - 1)] = outp[2];
-            pout[3 * (Lm + 1) + (i - 1)] = outp[3];
-            pout[4 * (Lm + 1) + (i - 1)] = outp[4];
-          } else {
-            pout[i] = outp[0];
-            pout[(Lm + 1) + (i - 1)] = outp[1];
-          }
+#pragma unroll
+          for (int f = 0; f < NP; ++f) pout[f * (Lm + 1) + (f < NL ? i : i - 1)] = outp[f];
         }
       }
 #pragma unroll
@@ -1330,7 +1497,7 @@ __global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    bwd_band<NS, R, G>(a, place_of<NS, R>(a, task, true), lane, sm, deadline);
+    bwd_band<NS, R, G>(a, place_of<NS, R, G>(a, task, true), lane, sm, deadline);
   }
 }
 

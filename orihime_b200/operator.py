@@ -205,6 +205,18 @@ NW = Family(
     value=lambda *a: torch.ops.orihime_b200.nw_value(*a),
 )
 
+NW_AFFINE = Family(
+    "nw_affine", ("gap_open", "gap_ext", "temp"),
+    forward=lambda *a: _ops().nw_affine_forward(*a),
+    # (value, dS/dgo, dS/dge, dS/dT): src/nw_affine/torch_cuda.cpp:688-702
+    grads=lambda *a: _ops().nw_affine_value_grad_params(*a)[1:],
+    hvp=lambda *a: _ops().nw_affine_marginals_hvp(*a),
+    sens=(lambda *a: _ops().nw_affine_marginals_grad_gap_open(*a),
+          lambda *a: _ops().nw_affine_marginals_grad_gap_ext(*a),
+          lambda *a: _ops().nw_affine_marginals_grad_temp(*a)),
+    value=lambda *a: torch.ops.orihime_b200.nw_affine_value(*a),
+)
+
 
 # ---------------------------------------------------------------------------
 # autograd functions

