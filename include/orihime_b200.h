@@ -309,6 +309,17 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
  * src/nw/kernels_gpu.cuh:285).
  */
 size_t swb_nw_aux_workspace_bytes(int B, int L1max, int L2max);
+/* Affine global alignment: the same two ops (param 0 = gap_open, 1 = gap_ext,
+ * 2 = temp; grad_tangents [B][4] = tangents of (dS/dgo, dS/dge, dS/dT, S)),
+ * replacing soft_nw_affine_hvp_cuda and soft_nw_affine_param_jacobian_cuda
+ * (src/nw_affine/torch_cuda.cpp:435, :484; backward_full :555). */
+size_t swb_nw_affine_aux_workspace_bytes(int B, int L1max, int L2max);
+int swb_nw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
+                      int L2max, float gap_open, float gap_ext, float temp, float* out,
+                      float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream);
+int swb_nw_affine_param_jacobian(const float* scores, const int* lengths, int B, int L1max,
+                                 int L2max, float gap_open, float gap_ext, float temp, int param,
+                                 float* out, void* workspace, size_t workspace_bytes, void* stream);
 int swb_nw_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
                int L2max, float gap, float temp, float* out, float* grad_tangents,
                void* workspace, size_t workspace_bytes, void* stream);

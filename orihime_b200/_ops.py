@@ -49,10 +49,16 @@ SCHEMAS = {
     "nw_forward": "nw_forward(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor[]",
     "nw_forward_t": "nw_forward_t(Tensor scores, Tensor gap, Tensor temp, Tensor lengths) -> Tensor[]",
     "nw_value_grad_params": "nw_value_grad_params(Tensor scores, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor)",
-    # src/nw_affine/registry.cpp:37-39
+    # src/nw_affine/registry.cpp:43-45
     "nw_affine_forward": "nw_affine_forward(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor[]",
     "nw_affine_forward_t": "nw_affine_forward_t(Tensor scores, Tensor gap_open, Tensor gap_ext, Tensor temp, Tensor lengths) -> Tensor[]",
     "nw_affine_value_grad_params": "nw_affine_value_grad_params(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
+    # src/nw_affine/registry.cpp:46-50
+    "nw_affine_marginals_backward": "nw_affine_marginals_backward(Tensor scores, Tensor grad_marginals, float gap_open, float gap_ext, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
+    "nw_affine_marginals_hvp": "nw_affine_marginals_hvp(Tensor scores, Tensor v, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "nw_affine_marginals_grad_gap_open": "nw_affine_marginals_grad_gap_open(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "nw_affine_marginals_grad_gap_ext": "nw_affine_marginals_grad_gap_ext(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "nw_affine_marginals_grad_temp": "nw_affine_marginals_grad_temp(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
     # src/nw/registry.cpp:48-51
     "nw_marginals_backward": "nw_marginals_backward(Tensor scores, Tensor grad_marginals, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
     "nw_marginals_hvp": "nw_marginals_hvp(Tensor scores, Tensor v, float gap, float temp, Tensor? lengths) -> Tensor",
@@ -406,6 +412,8 @@ _AUX = {  # family -> (workspace bytes, HVP, parameter Jacobian) entry points
     "sw_affine": ("swb_sw_affine_aux_workspace_bytes", "swb_sw_affine_hvp",
                   "swb_sw_affine_param_jacobian"),
     "nw": ("swb_nw_aux_workspace_bytes", "swb_nw_hvp", "swb_nw_param_jacobian"),
+    "nw_affine": ("swb_nw_affine_aux_workspace_bytes", "swb_nw_affine_hvp",
+                  "swb_nw_affine_param_jacobian"),
 }
 
 
@@ -571,7 +579,39 @@ def nw_marginals_backward(scores, grad_marginals, gap, temp, lengths):
     return out, tot[0:1].clone(), tot[1:2].clone()
 
 
+def nw_affine_marginals_hvp(scores, v, gap_open, gap_ext, temp, lengths):
+    """orihime::nw_affine_marginals_hvp (src/nw_affine/torch_cuda.cpp:716 -> soft_nw_affine_hvp_cuda :435)."""
+    check_input_cuda(scores, "scores")
+    _check_like(scores, v, "tangent", "scores and tangent must have same shape")
+    ln = _prep(scores, lengths, "nw_affine")
+    return run_hvp("nw_affine", scores, v, ln, (gap_open, gap_ext, temp))[0]
+
+
+def _nw_affine_param(which):
+    def op(scores, gap_open, gap_ext, temp, lengths):
+        ln = _prep(scores, lengths, "nw_affine")
+        return run_param_jacobian("nw_affine", scores, ln, (gap_open, gap_ext, temp), which)
+    op.__doc__ = (f"orihime::nw_affine_marginals_grad_* param {which} "
+                  "(src/nw_affine/torch_cuda.cpp:727-755 -> soft_nw_affine_param_jacobian_cuda :484)")
+    return op
+
+
+def nw_affine_marginals_backward(scores, grad_marginals, gap_open, gap_ext, temp, lengths):
+    """orihime::nw_affine_marginals_backward -> (grad_scores, d/dgo [1], d/dge [1], d/dT [1])
+    (src/nw_affine/torch_cuda.cpp:704 -> soft_nw_affine_backward_full_cuda :555); one
+    tangent pass along the cotangent."""
+    out, gt = marginals_backward_per_pair("nw_affine", scores, grad_marginals,
+                                          (gap_open, gap_ext, temp), lengths)
+    tot = gt[:, :3].sum(0)
+    return out, tot[0:1].clone(), tot[1:2].clone(), tot[2:3].clone()
+
+
 IMPLS = {
+    "nw_affine_marginals_hvp": nw_affine_marginals_hvp,
+    "nw_affine_marginals_grad_gap_open": _nw_affine_param(0),
+    "nw_affine_marginals_grad_gap_ext": _nw_affine_param(1),
+    "nw_affine_marginals_grad_temp": _nw_affine_param(2),
+    "nw_affine_marginals_backward": nw_affine_marginals_backward,
     "nw_marginals_hvp": nw_marginals_hvp,
     "nw_marginals_grad_gap": _nw_param(0),
     "nw_marginals_grad_temp": _nw_param(1),
@@ -687,12 +727,13 @@ for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True
 
 # ---------------------------------------------------------------------------
 # legacy soft_sw* / soft_nw* ops (src/sw/registry.cpp:30-35,
-# src/sw_affine/registry.cpp:27-32, src/nw/registry.cpp:34-39)
+# src/sw_affine/registry.cpp:27-32, src/nw/registry.cpp:34-39,
+# src/nw_affine/registry.cpp:35-40)
 # ---------------------------------------------------------------------------
-# The reference keeps 18 older schemas beside the namespaced ones; its Python
+# The reference keeps 24 older schemas beside the namespaced ones; its Python
 # package no longer calls them.  Each is one of the namespaced op bodies under
 # another name (src/sw*/torch_cuda.cpp:803-830, :917-946,
-# src/nw/torch_cuda.cpp:795-821).  They are defined
+# src/nw*/torch_cuda.cpp:795-821, :763-786).  They are defined
 # and given CUDA kernels only when orihime_b200 defines the schemas itself:
 # with the reference extension loaded first, they stay the reference's own.
 
@@ -730,6 +771,19 @@ LEGACY_SCHEMAS = {
                               "float temperature, Tensor? lengths) -> Tensor",
     "soft_nw_backward_full": "soft_nw_backward_full(Tensor scores, Tensor grad_alignment, float gap, "
                              "float temperature, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
+    "soft_nw_affine": "soft_nw_affine(Tensor scores, Tensor gap_open, Tensor gap_ext, Tensor temperature, "
+                      "Tensor lengths) -> Tensor[]",
+    "soft_nw_affine_float": "soft_nw_affine_float(Tensor scores, float gap_open, float gap_ext, "
+                            "float temperature, Tensor? lengths) -> Tensor[]",
+    "soft_nw_affine_with_grads": "soft_nw_affine_with_grads(Tensor scores, float gap_open, float gap_ext, "
+                                 "float temperature, Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor, Tensor)",
+    "soft_nw_affine_hvp": "soft_nw_affine_hvp(Tensor scores, Tensor tangent, float gap_open, float gap_ext, "
+                          "float temperature, Tensor? lengths) -> Tensor",
+    "soft_nw_affine_param_jacobian": "soft_nw_affine_param_jacobian(Tensor scores, int param_type, "
+                                     "float gap_open, float gap_ext, float temperature, Tensor? lengths) -> Tensor",
+    "soft_nw_affine_backward_full": "soft_nw_affine_backward_full(Tensor scores, Tensor grad_alignment, "
+                                    "float gap_open, float gap_ext, float temperature, Tensor? lengths) "
+                                    "-> (Tensor, Tensor, Tensor, Tensor)",
 }
 LEGACY_DEFINED_HERE = []
 if DEFINED_HERE:
@@ -747,6 +801,11 @@ def _legacy_with_grads_linear(scores, gap, temperature, lengths):
 def _legacy_with_grads_nw(scores, gap, temperature, lengths):
     ln = _prep(scores, lengths, "nw")
     return tuple(run_linear(scores, ln, gap, temperature, family="nw"))
+
+
+def _legacy_with_grads_nw_affine(scores, gap_open, gap_ext, temperature, lengths):
+    ln = _prep(scores, lengths, "nw_affine")
+    return tuple(run_affine(scores, ln, gap_open, gap_ext, temperature, family="nw_affine"))
 
 
 def _legacy_with_grads_affine(scores, gap_open, gap_ext, temperature, lengths):
@@ -786,12 +845,20 @@ LEGACY_IMPLS = {
     "soft_nw_hvp": nw_marginals_hvp,
     "soft_nw_param_jacobian": _legacy_jacobian("nw", 2),
     "soft_nw_backward_full": nw_marginals_backward,
+    "soft_nw_affine_float": nw_affine_forward,
+    "soft_nw_affine": nw_affine_forward_t,
+    "soft_nw_affine_with_grads": _legacy_with_grads_nw_affine,
+    "soft_nw_affine_hvp": nw_affine_marginals_hvp,
+    "soft_nw_affine_param_jacobian": _legacy_jacobian("nw_affine", 3),
+    "soft_nw_affine_backward_full": nw_affine_marginals_backward,
 }
 for _name in LEGACY_DEFINED_HERE:
     _IMPL_LIB.impl(_name, LEGACY_IMPLS[_name], "CUDA")
 for _name, _fam, _t in (("soft_sw_float", "sw", False), ("soft_sw", "sw", True),
                         ("soft_sw_affine_float", "sw_affine", False), ("soft_sw_affine", "sw_affine", True),
-                        ("soft_nw_float", "nw", False), ("soft_nw", "nw", True)):
+                        ("soft_nw_float", "nw", False), ("soft_nw", "nw", True),
+                        ("soft_nw_affine_float", "nw_affine", False),
+                        ("soft_nw_affine", "nw_affine", True)):
     if _name in LEGACY_DEFINED_HERE:   # differentiable like the reference (AutogradCUDA)
         _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
 

@@ -75,7 +75,7 @@ def _fake_for(name: str):
     if name.endswith("_forward") or name.endswith("_forward_t"):
         return _fake_forward
     if name.endswith("_value_grad_params"):
-        # nw_affine's also returns the value first (src/nw_affine/registry.cpp:39)
+        # nw_affine's also returns the value first (src/nw_affine/registry.cpp:45)
         return _fake_grad_params(n + 1 if name.startswith("nw_affine") else n)
     if name.endswith("_marginals_backward"):
         return _fake_backward(n)

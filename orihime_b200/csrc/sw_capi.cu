@@ -347,23 +347,24 @@ struct XLayout {
   size_t sent_bytes, total;
 };
 
-template <int NS>
+template <int NS, bool G = false>
 XLayout xlayout(long long B, long long L1m, long long L2m) {
   XLayout l{};
   l.R = xpick_r(B, L2m);
   l.nb = (int)std::max(1LL, (L2m + 32 * l.R - 1) / (32 * l.R));
   l.nsteps = (int)((L1m + 31 + swb::XC - 1) / swb::XC * swb::XC);
   const size_t slots = (size_t)B * l.nb;
-  const size_t step = (size_t)l.R * swb::XShape<NS>::G * 128;
+  using XS = swb::XShape<NS, G>;
+  const size_t step = (size_t)l.R * XS::G * 128;
   size_t o = align_up(64);   // counters [0, 1], status [4]
   l.off_pair_done = o; o = align_up(o + sizeof(unsigned) * (size_t)B);
-  l.off_part = o;      o = align_up(o + sizeof(float) * 4 * slots);
+  l.off_part = o;      o = align_up(o + sizeof(float) * swb::XPART * slots);
   l.off_gpart = o;     o = align_up(o + sizeof(float) * 4 * slots);
   l.off_cmax = o;      o = align_up(o + sizeof(float) * slots * (size_t)(l.nsteps / swb::XC));
   l.off_sent = o;
-  l.off_edge = o;      o = align_up(o + sizeof(float) * slots * swb::XShape<NS>::NE * (size_t)L1m);
+  l.off_edge = o;      o = align_up(o + sizeof(float) * slots * XS::NE * (size_t)L1m);
   l.off_bpush = o;
-  o = align_up(o + sizeof(float) * slots * 2 * swb::XShape<NS>::NP * (size_t)(L1m + 1));
+  o = align_up(o + sizeof(float) * slots * 2 * XS::NP * (size_t)(L1m + 1));
   l.sent_bytes = o - l.off_sent;
   l.off_fld = o;       o = align_up(o + sizeof(float) * slots * (size_t)l.nsteps * step);
   l.total = o;
@@ -375,7 +376,7 @@ struct XOcc {
   int f = 0, b = 0;
   bool ready = false;
 };
-XOcc g_xocc[64][3][2][4];   // [device][model: linear, affine, global linear][R == 4?][mode]
+XOcc g_xocc[64][4][2][4];   // [device][model: linear, affine, global linear, global affine][R == 4?][mode]
 
 template <int NS, int R, int MODE, bool G = false>
 int launch_xband_r(swb::XArgs a, cudaStream_t st) {
@@ -384,7 +385,7 @@ int launch_xband_r(swb::XArgs a, cudaStream_t st) {
   if (rc != SWB_OK) return rc;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWB_ERR_CUDA;
-  const size_t smem = sizeof(float) * swb::XSTAGES * swb::xstep_floats<NS, R>();
+  const size_t smem = sizeof(float) * swb::XSTAGES * swb::xstep_floats<NS, R, G>();
   XOcc& o = g_xocc[dev][model_index<NS, G>()][R == 4][MODE];
   {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -416,7 +417,7 @@ int launch_xband(const float* scores, const float* v, const int* lengths, int B,
   if (B == 0) return SWB_OK;
   const size_t map_elems = (size_t)B * L1m * L2m;
   if (map_elems > 0 && (!scores || !out || (MODE == swb::AUX_HVP && !v))) return SWB_ERR_ARG;
-  const XLayout l = xlayout<NS>(B, L1m, L2m);
+  const XLayout l = xlayout<NS, G>(B, L1m, L2m);
   if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream_v);
   char* w = static_cast<char*>(ws);
@@ -496,6 +497,35 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
   }
 }
 
+
+size_t swb_nw_affine_aux_workspace_bytes(int B, int L1max, int L2max) {
+  return B > 0 ? xlayout<3, true>(B, L1max, L2max).total : 0;
+}
+
+int swb_nw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
+                      int L2max, float gap_open, float gap_ext, float temp, float* out,
+                      float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_xband<3, swb::AUX_HVP, true>(scores, v, lengths, B, L1max, L2max, gap_open, gap_ext,
+                                             temp, out, grad_tangents, workspace, workspace_bytes,
+                                             stream);
+}
+
+int swb_nw_affine_param_jacobian(const float* scores, const int* lengths, int B, int L1max,
+                                 int L2max, float gap_open, float gap_ext, float temp, int param,
+                                 float* out, void* workspace, size_t workspace_bytes, void* stream) {
+  switch (param) {
+    case 0: return launch_xband<3, swb::AUX_P0, true>(scores, nullptr, lengths, B, L1max, L2max,
+                                                      gap_open, gap_ext, temp, out, nullptr,
+                                                      workspace, workspace_bytes, stream);
+    case 1: return launch_xband<3, swb::AUX_P1, true>(scores, nullptr, lengths, B, L1max, L2max,
+                                                      gap_open, gap_ext, temp, out, nullptr,
+                                                      workspace, workspace_bytes, stream);
+    case 2: return launch_xband<3, swb::AUX_PT, true>(scores, nullptr, lengths, B, L1max, L2max,
+                                                      gap_open, gap_ext, temp, out, nullptr,
+                                                      workspace, workspace_bytes, stream);
+    default: return SWB_ERR_ARG;
+  }
+}
 
 size_t swb_nw_aux_workspace_bytes(int B, int L1max, int L2max) {
   return swb_sw_aux_workspace_bytes(B, L1max, L2max);

@@ -47,12 +47,20 @@ constexpr float LN2 = 0.69314718055994531f;
 // MUFU lg2 flushes a subnormal input to 0 and would return -inf.
 constexpr float W_TINY = 1.17549435e-38f;
 
-template <int NS> struct XShape;
+template <int NS, bool GL = false> struct XShape;
 // G: float4 field groups per cell; NE: floats per row crossing a band edge
 // forward (hi, lo, tangent of each state); NP: value push channels crossing a
-// lane or band edge backward (their tangents double it).
-template <> struct XShape<3> { static constexpr int G = 6, NE = 9, NP = 5; };
-template <> struct XShape<1> { static constexpr int G = 3, NE = 3, NP = 2; };
+// lane or band edge backward (their tangents double it); NL of them are left
+// pushes.  Global affine: nine weights and their tangents, no per-cell
+// alpha (its only beta-init, at the terminal, travels in the partial slot).
+template <> struct XShape<3, false> { static constexpr int G = 6, NE = 9, NP = 5, NL = 2; };
+template <> struct XShape<3, true> { static constexpr int G = 5, NE = 9, NP = 6, NL = 3; };
+template <> struct XShape<1, false> { static constexpr int G = 3, NE = 3, NP = 2, NL = 1; };
+template <> struct XShape<1, true> { static constexpr int G = 3, NE = 3, NP = 2, NL = 1; };
+// floats of the forward's per-band partial slot: (ref or S hi, sum or S lo,
+// U-sum or dS, log-sum), then the global affine terminal's beta-inits and
+// their tangents (w_M, w_I, w_D, dw_M, dw_I, dw_D), padded to 12
+constexpr int XPART = 12;
 
 constexpr int XC = 4;   // steps per edge / push prefetch chunk
 #ifndef SWB_XPF
@@ -72,8 +80,8 @@ constexpr int XSTAGES = SWB_XSTAGES;   // field steps in flight per backward war
 #endif
 
 // floats of one step of fields for one warp
-template <int NS, int R>
-__host__ __device__ constexpr int xstep_floats() { return R * XShape<NS>::G * 128; }
+template <int NS, int R, bool GL = false>
+__host__ __device__ constexpr int xstep_floats() { return R * XShape<NS, GL>::G * 128; }
 
 struct XArgs {
   const float* scores;     // [B, L1m, L2m]
@@ -122,13 +130,21 @@ __device__ __forceinline__ Pair xpair_of(const XArgs& a, int p, int L1, int L2, 
 }
 
 // Weight tangents dw_k = w_k (c_k - cbar [+ (-ln w_k - H)]) / T; returns the
-// cell's tangent cbar [+ H].
+// cell's tangent cbar [+ H].  The mean is taken as c_0 + sum w_k (c_k - c_0):
+// the weights sum to 1 only up to the approximate reciprocal (~1e-7), and
+// that error then scales the candidates' small differences instead of their
+// magnitude (tangents along a gap grow with the number of gaps on a path,
+// and a bias of ~1e-7 of them per cell accumulates along the DP).
 template <int N, bool TM>
 __device__ __forceinline__ float xwtan(const float (&w)[N], const float (&c)[N], float iT,
                                        float (&dw)[N]) {
-  float cb = 0.f;
+  const float c0 = c[0];
+  float d[N];
 #pragma unroll
-  for (int q = 0; q < N; ++q) cb = fmaf(w[q], c[q], cb);
+  for (int q = 0; q < N; ++q) d[q] = c[q] - c0;
+  float cb = 0.f;   // sum w (c - c0)
+#pragma unroll
+  for (int q = 0; q < N; ++q) cb = fmaf(w[q], d[q], cb);
   float h = 0.f, nl[N];
   if (TM) {
 #pragma unroll
@@ -139,11 +155,11 @@ __device__ __forceinline__ float xwtan(const float (&w)[N], const float (&c)[N],
   }
 #pragma unroll
   for (int q = 0; q < N; ++q) {
-    float x = c[q] - cb;
+    float x = d[q] - cb;
     if (TM) x += nl[q] - h;
     dw[q] = w[q] * x * iT;
   }
-  return TM ? cb + h : cb;
+  return TM ? (c0 + cb) + h : c0 + cb;
 }
 
 // One affine cell of the forward: new alpha pairs and tangents of M, I, D in
@@ -208,6 +224,64 @@ __device__ __forceinline__ void xcell3(const float (&dh)[3], const float (&dl)[3
   f[5] = make_float4(uM, uI, uD, 0.f);
 }
 
+// One global affine cell: M = s + LSE(M, I, D at diag); I = LSE(M + go,
+// I + ge, D + go) from above; D = LSE(M + go, I + go, D + ge) from the left.
+// o as xcell3; fields
+//   f0 = (wMM, wMI, wMD, wIM)   f1 = (wII, wID, wDM, wDI)
+//   f2 = (wDD, dwMM, dwMI, dwMD)  f3 = (dwIM, dwII, dwID, dwDM)  f4 = (dwDI, dwDD, 0, 0)
+template <int MODE>
+__device__ __forceinline__ void xcell3g(const float (&dh)[3], const float (&dl)[3],
+                                        const float (&du)[3], const float (&uh)[3],
+                                        const float (&ul)[3], const float (&uu)[3],
+                                        const float (&lh)[3], const float (&ll)[3],
+                                        const float (&lu)[3], float s, float vv, float g0, float g1,
+                                        float iT, float (&o)[9], float4 (&f)[5]) {
+  constexpr bool TM = (MODE == AUX_PT);
+  const float r = fmaxf(fmaxf(dh[0], dh[1]), dh[2]);
+  const float tM = ex2((dh[0] - r) + dl[0]), tI = ex2((dh[1] - r) + dl[1]);
+  const float tD = ex2((dh[2] - r) + dl[2]);
+  const float sm = (tM + tI) + tD;
+  float Mh, Ml;
+  two_sum(r, s, Mh, Ml);
+  Ml += lg2(sm);
+  const float vm = recip(sm);
+  const float wm[3] = {tM * vm, tI * vm, tD * vm};
+  const float ru = fmaxf(fmaxf(uh[0] + g0, uh[1] + g1), uh[2] + g0);
+  const float ta = ex2(((uh[0] - ru) + g0) + ul[0]), tb = ex2(((uh[1] - ru) + g1) + ul[1]);
+  const float tc = ex2(((uh[2] - ru) + g0) + ul[2]);
+  const float si = (ta + tb) + tc;
+  float Ih, Il;
+  fast2(ru, lg2(si), Ih, Il);
+  const float vi = recip(si);
+  const float wi[3] = {ta * vi, tb * vi, tc * vi};
+  const float rl = fmaxf(fmaxf(lh[0] + g0, lh[1] + g0), lh[2] + g1);
+  const float td = ex2(((lh[0] - rl) + g0) + ll[0]), te = ex2(((lh[1] - rl) + g0) + ll[1]);
+  const float tf = ex2(((lh[2] - rl) + g1) + ll[2]);
+  const float sd = (td + te) + tf;
+  float Dh, Dl;
+  fast2(rl, lg2(sd), Dh, Dl);
+  const float vd = recip(sd);
+  const float wd[3] = {td * vd, te * vd, tf * vd};
+  // candidate tangents: predecessors' U, the score direction on all of M's
+  // terms (its weights sum to 1), 1 on the terms of the differentiated gap
+  float cm[3] = {du[0], du[1], du[2]}, ci[3] = {uu[0], uu[1], uu[2]}, cd[3] = {lu[0], lu[1], lu[2]};
+  if (MODE == AUX_HVP) { cm[0] += vv; cm[1] += vv; cm[2] += vv; }
+  if (MODE == AUX_P0) { ci[0] += 1.f; ci[2] += 1.f; cd[0] += 1.f; cd[1] += 1.f; }
+  if (MODE == AUX_P1) { ci[1] += 1.f; cd[2] += 1.f; }
+  float dwm[3], dwi[3], dwd[3];
+  const float uM = xwtan<3, TM>(wm, cm, iT, dwm);
+  const float uI = xwtan<3, TM>(wi, ci, iT, dwi);
+  const float uD = xwtan<3, TM>(wd, cd, iT, dwd);
+  o[0] = Mh; o[1] = Ml; o[2] = uM;
+  o[3] = Ih; o[4] = Il; o[5] = uI;
+  o[6] = Dh; o[7] = Dl; o[8] = uD;
+  f[0] = make_float4(wm[0], wm[1], wm[2], wi[0]);
+  f[1] = make_float4(wi[1], wi[2], wd[0], wd[1]);
+  f[2] = make_float4(wd[2], dwm[0], dwm[1], dwm[2]);
+  f[3] = make_float4(dwi[0], dwi[1], dwi[2], dwd[0]);
+  f[4] = make_float4(dwd[1], dwd[2], 0.f, 0.f);
+}
+
 // One linear cell: o = (Ah, Al, U); fields
 //   f0 = (w_diag, w_up, w_left, w_diag + w_start)
 //   f1 = (dw_diag, dw_up, dw_left, dw_diag + dw_start)   f2 = (Ah, Al, U, 0)
@@ -270,6 +344,66 @@ __device__ __forceinline__ void xcombine(float& r1, float& s1, float& u1, float&
   r1 = m;
 }
 
+// Tangents of a global alignment's row-0 values at column j along the
+// differentiated direction: linear j * gap -> j (gap); affine D(0,j) =
+// go + (j-1) ge -> 1 (gap open) or j - 1 (gap extend); 0 otherwise.
+template <int NS, int MODE>
+__device__ __forceinline__ void xrow0_tan(int j, float (&u)[NS]) {
+#pragma unroll
+  for (int q = 0; q < NS; ++q) u[q] = 0.f;
+  if constexpr (NS == 1) {
+    if (MODE == AUX_P0) u[0] = (float)j;
+  } else {
+    if (j >= 1 && MODE == AUX_P0) u[2] = 1.f;
+    if (j >= 1 && MODE == AUX_P1) u[2] = (float)(j - 1);
+  }
+}
+
+// Column-0 edge record at row i (hi, lo, tangent of each state): linear
+// i * gap; affine I(i,0) = go + (i-1) ge, M and D NEG.
+template <int NS, int MODE>
+__device__ __forceinline__ void xcol0_edge(int i, float g0, float g1, float (&e)[3 * NS]) {
+  float hl[2 * NS];
+  col0_edge<NS>(i, g0, g1, hl);
+#pragma unroll
+  for (int f = 0; f < 2 * NS; ++f) e[f] = hl[f];
+  if constexpr (NS == 1) {
+    e[2] = MODE == AUX_P0 ? (float)i : 0.f;
+  } else {
+    e[6] = 0.f;
+    e[7] = MODE == AUX_P0 ? 1.f : (MODE == AUX_P1 ? (float)(i - 1) : 0.f);
+    e[8] = 0.f;
+  }
+}
+
+// The terminal of a global alignment (column c of the lane): part = (S hi,
+// S lo, dS, 0, then for the affine model the beta-inits w_q = 2^(x_q - S)
+// of M, I, D and their tangents).
+template <int NS, int MODE, int R>
+__device__ __forceinline__ void xterminal(const float (&ph)[NS][R], const float (&pl)[NS][R],
+                                          const float (&pu)[NS][R], int c, float iT, float* part) {
+  if constexpr (NS == 1) {
+    part[0] = ph[0][c]; part[1] = pl[0][c]; part[2] = pu[0][c]; part[3] = 0.f;
+  } else {
+    constexpr bool TM = (MODE == AUX_PT);
+    const float r = fmaxf(fmaxf(ph[0][c], ph[1][c]), ph[2][c]);
+    float e[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) e[q] = ex2((ph[q][c] - r) + pl[q][c]);
+    const float sm = (e[0] + e[1]) + e[2];
+    float Sh, Sl;
+    fast2(r, lg2(sm), Sh, Sl);
+    const float v = recip(sm);
+    const float w[3] = {e[0] * v, e[1] * v, e[2] * v};
+    const float u[3] = {pu[0][c], pu[1][c], pu[2][c]};
+    float dw[3];
+    const float dS = xwtan<3, TM>(w, u, iT, dw);
+    part[0] = Sh; part[1] = Sl; part[2] = dS; part[3] = 0.f;
+    part[4] = w[0]; part[5] = w[1]; part[6] = w[2];
+    part[7] = dw[0]; part[8] = dw[1]; part[9] = dw[2];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // forward band task
 // ---------------------------------------------------------------------------
@@ -282,15 +416,14 @@ __device__ __forceinline__ void xcombine(float& r1, float& s1, float& u1, float&
 // the chunk holding the terminal and NEG elsewhere.
 template <int NS, int R, int MODE, bool GL = false>
 __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t deadline) {
-  static_assert(!GL || NS == 1, "global alignment is built for the linear model");
-  using XS = XShape<NS>;
+  using XS = XShape<NS, GL>;
   constexpr int G = XS::G, NE = XS::NE;
-  constexpr int XSTEP = xstep_floats<NS, R>();
+  constexpr int XSTEP = xstep_floats<NS, R, GL>();
   constexpr bool HV = (MODE == AUX_HVP);
   int L1, L2;
   xlengths(a, p, L1, L2);
   const size_t slot = (size_t)p * a.nb + band;
-  float* part = a.part + 4 * slot;
+  float* part = a.part + XPART * slot;
   const int col0 = band * 32 * R;
   if (!(L1 > 0 && col0 < L2)) {
     if (!GL && lane == 0) { part[0] = 0.f; part[1] = (band == 0) ? 1.f : 0.f; part[2] = 0.f; part[3] = 0.f; }
@@ -313,14 +446,16 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
 #pragma unroll
     for (int c = 0; c < R; ++c) { ph[q][c] = NEG; pl[q][c] = 0.f; pu[q][c] = 0.f; }
   }
-  constexpr bool GAPDIR = (MODE == AUX_P0);   // tangent of a boundary n * gap is n
-  if constexpr (GL) {
-    nmul(jl, g0, lh[0], ll[0]);
-    lu[0] = GAPDIR ? (float)jl : 0.f;
+  if constexpr (GL) {   // row 0 and its tangents (the boundaries' gap derivatives)
+    row0<NS>(jl, g0, g1, lh, ll);
+    xrow0_tan<NS, MODE>(jl, lu);
 #pragma unroll
     for (int c = 0; c < R; ++c) {
-      nmul(jl + c + 1, g0, ph[0][c], pl[0][c]);
-      pu[0][c] = GAPDIR ? (float)(jl + c + 1) : 0.f;
+      float h[NS], l[NS], u[NS];
+      row0<NS>(jl + c + 1, g0, g1, h, l);
+      xrow0_tan<NS, MODE>(jl + c + 1, u);
+#pragma unroll
+      for (int q = 0; q < NS; ++q) { ph[q][c] = h[q]; pl[q][c] = l[q]; pu[q][c] = u[q]; }
     }
   }
   const bool term_lane = GL && jl < L2 && L2 <= jl + R;   // holds the pair's last column
@@ -338,10 +473,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
     const bool ok = ein && lane < XC && i <= L1;
 #pragma unroll
     for (int f = 0; f < NE; ++f) dst[f] = ok ? ld_poll(ein + f * Lm + (i - 1)) : 0.f;
-    if (left_bnd) {
-      nmul(i, g0, dst[0], dst[1]);
-      dst[2] = GAPDIR ? (float)i : 0.f;
-    }
+    if (left_bnd) xcol0_edge<NS, MODE>(i, g0, g1, dst);
   };
   load_edge(0, eb);
   float sb[XPF][R], vb[XPF][R];
@@ -421,7 +553,28 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
         for (int q = 0; q < NS; ++q) { wh[q] = lh[q]; wl[q] = ll[q]; wu[q] = lu[q]; }
 #pragma unroll
         for (int c = 0; c < R; ++c) {
-          if constexpr (NS == 3) {
+          if constexpr (NS == 3 && GL) {
+            const float uh3[3] = {ph[0][c], ph[1][c], ph[2][c]};
+            const float ul3[3] = {pl[0][c], pl[1][c], pl[2][c]};
+            const float uu3[3] = {pu[0][c], pu[1][c], pu[2][c]};
+            float o[9];
+            float4 f[G];
+            xcell3g<MODE>(dgh, dgl, dgu, uh3, ul3, uu3, wh, wl, wu, s[c], vv[c], g0, g1, iT, o, f);
+            if (i < 1) {   // boundary row: keep the values, no fields
+#pragma unroll
+              for (int q = 0; q < 3; ++q) { o[3 * q] = uh3[q]; o[3 * q + 1] = ul3[q]; o[3 * q + 2] = uu3[q]; }
+#pragma unroll
+              for (int g = 0; g < G; ++g) f[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int g = 0; g < G; ++g) reinterpret_cast<float4*>(Fs + (c * G + g) * 128)[lane] = f[g];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              dgh[q] = uh3[q]; dgl[q] = ul3[q]; dgu[q] = uu3[q];
+              wh[q] = o[3 * q]; wl[q] = o[3 * q + 1]; wu[q] = o[3 * q + 2];
+              ph[q][c] = o[3 * q]; pl[q][c] = o[3 * q + 1]; pu[q][c] = o[3 * q + 2];
+            }
+          } else if constexpr (NS == 3) {
             const float uMh = ph[0][c], uMl = pl[0][c], uMu = pu[0][c];
             const float uIh = ph[1][c], uIl = pl[1][c], uIu = pu[1][c];
             const float uDh = ph[2][c], uDl = pl[2][c], uDu = pu[2][c];
@@ -458,18 +611,19 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
           }
         }
         if (GL && act) {
-          if (term_lane && i == L1) {   // the terminal A[L1, L2] with its tangent
-            float th = 0.f, tl = 0.f, tu = 0.f;
+          if (term_lane && i == L1) {   // the terminal with its tangent (affine: LSE of M, I, D)
 #pragma unroll
             for (int c = 0; c < R; ++c)
-              if (jl + c == L2 - 1) { th = ph[0][c]; tl = pl[0][c]; tu = pu[0][c]; }
-            part[0] = th; part[1] = tl; part[2] = tu; part[3] = 0.f;
+              if (jl + c == L2 - 1) xterminal<NS, MODE>(ph, pl, pu, c, iT, part);
             cmx = 1e30f;
           }
           if (lane == 31) {
-            eout[(i - 1)] = ph[0][R - 1];
-            eout[Lm + (i - 1)] = pl[0][R - 1];
-            eout[2 * Lm + (i - 1)] = pu[0][R - 1];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+              eout[q * Lm + (i - 1)] = ph[q][R - 1];
+              eout[(NS + q) * Lm + (i - 1)] = pl[q][R - 1];
+              eout[(2 * NS + q) * Lm + (i - 1)] = pu[q][R - 1];
+            }
           }
         }
         if (!GL && act) {
@@ -566,7 +720,7 @@ __device__ __forceinline__ void xpair_stats(const XArgs& a, int p, int lane, flo
       dS = 0.f;
       return;
     }
-    const float* q = a.part + 4 * ((size_t)p * a.nb + (L2 - 1) / (32 * R));
+    const float* q = a.part + XPART * ((size_t)p * a.nb + (L2 - 1) / (32 * R));
     Sh = q[0];
     Sl = q[1];
     dS = q[2];
@@ -574,7 +728,7 @@ __device__ __forceinline__ void xpair_stats(const XArgs& a, int p, int lane, flo
   }
   float ref = NEG, s = 0.f, su = 0.f, sx = 0.f;
   for (int b = lane; b < a.nb; b += 32) {
-    const float* q = a.part + 4 * ((size_t)p * a.nb + b);
+    const float* q = a.part + XPART * ((size_t)p * a.nb + b);
     const float r2 = q[0], s2 = q[1], u2 = q[2], x2 = q[3];
     if (s2 > 0.f) xcombine(ref, s, su, sx, r2, s2, u2, x2);
   }
@@ -655,9 +809,9 @@ __device__ void xfinish(const XArgs& a, int p, int band, int lane, bool empty, f
 template <int NS, int R, int MODE, bool GL = false>
 __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring,
                           uint64_t deadline) {
-  using XS = XShape<NS>;
-  constexpr int G = XS::G, NP = XS::NP, NQ = 2 * NP;
-  constexpr int XSTEP = xstep_floats<NS, R>();
+  using XS = XShape<NS, GL>;
+  constexpr int G = XS::G, NP = XS::NP, NQ = 2 * NP, NL = XS::NL;
+  constexpr int XSTEP = xstep_floats<NS, R, GL>();
   constexpr bool TM = (MODE == AUX_PT), HV = (MODE == AUX_HVP);
   int L1, L2;
   xlengths(a, p, L1, L2);
@@ -673,6 +827,15 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   const Pair pv = xpair_of(a, p, L1, L2, HV ? a.v : a.scores, nullptr);
   const int jl = col0 + lane * R;
   const bool term_lane = GL && jl < L2 && L2 <= jl + R;   // holds the pair's last column
+  // the terminal's beta-inits and their tangents (linear: 1 and 0)
+  float tw[NS], tdw[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) { tw[q] = 1.f; tdw[q] = 0.f; }
+  if (NS == 3 && term_lane) {
+    const float* q = a.part + XPART * ((size_t)p * a.nb + band);
+#pragma unroll
+    for (int st = 0; st < NS; ++st) { tw[st] = q[4 + st]; tdw[st] = q[7 + st]; }
+  }
   const float iT = 1.f / a.T;
   const size_t Lm = (size_t)a.L1m;
   float* pout = (band > 0) ? a.bpush + slot * NQ * (Lm + 1) : nullptr;
@@ -703,7 +866,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
 #pragma unroll
     for (int f = 0; f < NQ; ++f) {
       const int fc = f % NP;
-      const bool left = (NS == 3) ? (fc < 2) : (fc < 1);
+      const bool left = fc < NL;
       dst[f] = (ok && (left || i < L1)) ? ld_poll(pin + f * (Lm + 1) + i) : 0.f;
     }
   };
@@ -776,7 +939,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
 #pragma unroll
           for (int f = 0; f < NQ; ++f) {
             const int fc = f % NP;
-            const bool left = (NS == 3) ? (fc < 2) : (fc < 1);
+            const bool left = fc < NL;
             pout[f * (Lm + 1) + (left ? i : i - 1)] = 0.f;
           }
         }
@@ -836,7 +999,31 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
         }
         // pushes arriving at column R-1 of row i: from the right lane (or band)
         // into the left of this cell, and into its diagonal from (i+1, j+1)
-        if constexpr (NS == 3) {
+        if constexpr (NS == 3 && GL) {
+          float iL[3], tL[3], iD[3], tD[3];
+          if (lane == 31) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              iL[q] = pw[q]; tL[q] = pw[NP + q]; iD[q] = pw[NL + q]; tD[q] = pw[NP + NL + q];
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              iL[q] = r[q]; tL[q] = r[NP + q];
+              iD[q] = hold[q]; hold[q] = r[NL + q];
+              tD[q] = holdt[q]; holdt[q] = r[NP + NL + q];
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < 3; ++q) { ac[q][R - 1] += iL[q] + iD[q]; at[q][R - 1] += tL[q] + tD[q]; }
+          if (term_lane && i == L1) {   // the terminal's beta-inits and their tangents
+#pragma unroll
+            for (int c = 0; c < R; ++c)
+              if (jl + c == L2 - 1)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) { ac[q][c] += tw[q]; at[q][c] += tdw[q]; }
+          }
+        } else if constexpr (NS == 3) {
           float iL0, iL1, tL0, tL1, iD[3], tD[3];
           if (lane == 31) {
             iL0 = pw[0]; iL1 = pw[1]; tL0 = pw[NP + 0]; tL1 = pw[NP + 1];
@@ -887,7 +1074,51 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
 #pragma unroll
           for (int g = 0; g < G; ++g) f[g] = *reinterpret_cast<const float4*>(E + (c * G + g) * 128);
           const bool live = act && (jl + c < L2);
-          if constexpr (NS == 3) {
+          if constexpr (NS == 3 && GL) {
+            // f0 = (wMM, wMI, wMD, wIM) f1 = (wII, wID, wDM, wDI) f2 = (wDD, dwMM, dwMI, dwMD)
+            // f3 = (dwIM, dwII, dwID, dwDM) f4 = (dwDI, dwDD, -, -)
+            const float bM = ac[0][c], bI = ac[1][c], bD = ac[2][c];
+            const float tgM = at[0][c], tgI = at[1][c], tgD = at[2][c];
+            const float qM = bM * f[0].x, qI = bM * f[0].y, qD = bM * f[0].z;
+            const float tqM = fmaf(tgM, f[0].x, bM * f[2].y);
+            const float tqI = fmaf(tgM, f[0].y, bM * f[2].z);
+            const float tqD = fmaf(tgM, f[0].z, bM * f[2].w);
+            const float pIM = bI * f[0].w, pII = bI * f[1].x, pID = bI * f[1].y;
+            const float tIM = fmaf(tgI, f[0].w, bI * f[3].x);
+            const float tII = fmaf(tgI, f[1].x, bI * f[3].y);
+            const float tID = fmaf(tgI, f[1].y, bI * f[3].z);
+            const float pDM = bD * f[1].z, pDI = bD * f[1].w, pDD = bD * f[2].x;
+            const float tDM = fmaf(tgD, f[1].z, bD * f[3].w);
+            const float tDI = fmaf(tgD, f[1].w, bD * f[4].x);
+            const float tDD = fmaf(tgD, f[2].x, bD * f[4].y);
+            pm[c] = tgM;
+            if (HV) {
+              cA += (tIM + tID) + (tDM + tDI);
+              cB += tII + tDD;
+              cC = fmaf(tgM, sc[c], fmaf(bM, vv[c], cC));
+              // tangents pushed into the boundary states D(0, j) and I(i, 0)
+              if (i == 1) {
+                cA += tID + tqD;
+                cB += (float)(jl + c) * tID + (float)(jl + c - 1) * tqD;
+              }
+              if (band == 0 && lane == 0 && c == 0) {
+                cA += tDI + tqI;
+                cB += (float)(i - 1) * tDI + (float)(i - 2) * tqI;
+              }
+            }
+            nx[0][c] += pIM; nx[1][c] += pII; nx[2][c] += pID;
+            nt[0][c] += tIM; nt[1][c] += tII; nt[2][c] += tID;
+            if (c > 0) {
+              nx[0][c - 1] += qM; nx[1][c - 1] += qI; nx[2][c - 1] += qD;
+              nt[0][c - 1] += tqM; nt[1][c - 1] += tqI; nt[2][c - 1] += tqD;
+              ac[0][c - 1] += pDM; ac[1][c - 1] += pDI; ac[2][c - 1] += pDD;
+              at[0][c - 1] += tDM; at[1][c - 1] += tDI; at[2][c - 1] += tDD;
+            } else {
+              outp[0] = pDM; outp[1] = pDI; outp[2] = pDD; outp[3] = qM; outp[4] = qI; outp[5] = qD;
+              outp[NP + 0] = tDM; outp[NP + 1] = tDI; outp[NP + 2] = tDD;
+              outp[NP + 3] = tqM; outp[NP + 4] = tqI; outp[NP + 5] = tqD;
+            }
+          } else if constexpr (NS == 3) {
             const float xs[3] = {(f[3].z - Sh) + (f[4].y - Sl), (f[3].w - Sh) + (f[4].z - Sl),
                                  (f[4].x - Sh) + (f[4].w - Sl)};
             const float us[3] = {f[5].x, f[5].y, f[5].z};
@@ -970,7 +1201,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
 #pragma unroll
             for (int f = 0; f < NQ; ++f) {
               const int fc = f % NP;
-              const bool left = (NS == 3) ? (fc < 2) : (fc < 1);
+              const bool left = fc < NL;
               pout[f * (Lm + 1) + (left ? i : i - 1)] = outp[f];
             }
           }

@@ -205,3 +205,119 @@ def test_nw_affine_public_value_and_map():
     x = s.clone().requires_grad_(True)
     (dx,) = torch.autograd.grad(ob.nw_affine_value(x, **kw).sum(), x)
     np.testing.assert_allclose(dx.cpu().numpy(), o["map"], atol=1e-5)
+
+
+# ---- second-order ops: HVP, parameter Jacobians, map VJP --------------------
+
+def _check2(name, got, r32, r64, rel_floor=1e-4):
+    """Second-order bar: error vs fp64 within the reference's own fp32 error,
+    floor 1e-4 of the largest exact entry."""
+    got, r32, r64 = (np.asarray(x, np.float64) for x in (got, r32, r64))
+    scale = max(float(np.abs(r64).max()), 1e-12)
+    e64 = float(np.abs(got - r64).max())
+    eref = float(np.abs(r32 - r64).max())
+    bound = max(rel_floor * scale, eref)
+    print(f"  {name:14s} ours-fp64 {e64:.2e}  ref32-fp64 {eref:.2e}  bound {bound:.2e}  scale {scale:.2e}")
+    assert e64 <= bound, f"{name}: {e64:.3e} > {bound:.3e}"
+
+
+SECOND = [
+    # (B, L1, L2, lengths or None, go, ge, T, seed)
+    (2, 24, 31, None, -2.0, -0.5, 0.7, 1),
+    (4, 10, 12, [[8, 10], [10, 12], [0, 5], [7, 0]], -1.0, -0.3, 1.0, 2),
+    (2, 64, 48, None, -2.0, -0.5, 0.3, 3),
+    (1, 130, 300, None, -3.0, -1.0, 0.5, 4),
+    (3, 5, 7, None, -1.0, -0.3, 1.0, 7),     # boundary-heavy
+]
+
+
+def _second_inputs(B, L1, L2, seed):
+    s = _gen((B, L1, L2), seed, 1.5)
+    if seed == 7:
+        s[:, 0, :] -= 2.5
+        s[:, :, 0] -= 2.5
+    return s, _gen((B, L1, L2), seed + 100)
+
+
+@pytest.mark.parametrize("B,L1,L2,lengths,go,ge,T,seed", SECOND)
+def test_nw_affine_hvp_matches_oracle(B, L1, L2, lengths, go, ge, T, seed):
+    s, v = _second_inputs(B, L1, L2, seed)
+    ln = None if lengths is None else torch.tensor(lengths, dtype=torch.int32)
+    lnd = None if ln is None else ln.cuda()
+    lnn = None if ln is None else ln.numpy()
+    got = torch.ops.orihime.nw_affine_marginals_hvp(s.cuda(), v.cuda(), go, ge, T, lnd).cpu().numpy()
+    _check2("hvp", got, O.nw_affine_hvp(s.numpy(), v.numpy(), lnn, go, ge, T),
+            O.nw_affine_hvp(s.numpy(), v.numpy(), lnn, go, ge, T, dtype=np.float64))
+    if lengths is not None:
+        for b, (l1, l2) in enumerate(lengths):
+            assert not got[b, l1:, :].any() and not got[b, :, l2:].any()
+
+
+@pytest.mark.parametrize("B,L1,L2,lengths,go,ge,T,seed", SECOND)
+@pytest.mark.parametrize("param", [0, 1, 2])
+def test_nw_affine_param_jacobian_matches_oracle(param, B, L1, L2, lengths, go, ge, T, seed):
+    s, _ = _second_inputs(B, L1, L2, seed)
+    ln = None if lengths is None else torch.tensor(lengths, dtype=torch.int32)
+    lnd = None if ln is None else ln.cuda()
+    lnn = None if ln is None else ln.numpy()
+    ops = torch.ops.orihime
+    fn = (ops.nw_affine_marginals_grad_gap_open, ops.nw_affine_marginals_grad_gap_ext,
+          ops.nw_affine_marginals_grad_temp)[param]
+    got = fn(s.cuda(), go, ge, T, lnd).cpu().numpy()
+    _check2(f"dP/dtheta{param}", got, O.nw_affine_param_grad(s.numpy(), lnn, go, ge, T, param),
+            O.nw_affine_param_grad(s.numpy(), lnn, go, ge, T, param, dtype=np.float64))
+
+
+def test_nw_affine_marginals_backward_matches_oracle_contractions():
+    B, L1, L2, go, ge, T = 3, 37, 145, -2.0, -0.5, 0.6
+    s, gm = _second_inputs(B, L1, L2, 11)
+    ln = torch.tensor([[37, 145], [20, 45], [37, 9]], dtype=torch.int32)
+    sn, gn, lnn = s.numpy(), gm.numpy(), ln.numpy()
+    out = torch.ops.orihime.nw_affine_marginals_backward(s.cuda(), gm.cuda(), go, ge, T, ln.cuda())
+    _check2("grad_scores", out[0].cpu().numpy(), O.nw_affine_hvp(sn, gn, lnn, go, ge, T),
+            O.nw_affine_hvp(sn, gn, lnn, go, ge, T, dtype=np.float64))
+    for k in range(3):
+        r64 = (gn.astype(np.float64) * O.nw_affine_param_grad(sn, lnn, go, ge, T, k, dtype=np.float64)).sum()
+        r32 = (gn.astype(np.float64) * O.nw_affine_param_grad(sn, lnn, go, ge, T, k)).sum()
+        got = float(out[1 + k].item())
+        bound = max(abs(r32 - r64), 1e-4 * (1 + abs(r64)))
+        print(f"  param {k}: ours {got:.6f} fp64 {r64:.6f} ref32 {r32:.6f}")
+        assert abs(got - r64) <= bound
+
+
+def test_nw_affine_public_autograd_and_legacy():
+    import orihime_b200 as ob
+    s = _gen((2, 30, 41), 31, 1.5).cuda()
+    cot = _gen((2, 30, 41), 32).cuda()
+    ln = torch.tensor([[30, 41], [22, 17]], dtype=torch.int32).cuda()
+    kw = dict(gap_open_score=-2.0, gap_extend_score=-0.5, temperature=0.7, lengths=ln)
+    x = s.clone().requires_grad_(True)
+    (dm,) = torch.autograd.grad((ob.nw_affine(x, **kw) * cot).sum(), x)
+    ref = torch.ops.orihime.nw_affine_marginals_hvp(s, cot, -2.0, -0.5, 0.7, ln)
+    assert torch.allclose(dm, ref, rtol=1e-6, atol=1e-7)
+    x = s.clone().requires_grad_(True)
+    (de,) = torch.autograd.grad(ob.nw_affine_entropy(x, **kw).sum(), x)
+    assert torch.allclose(de, torch.ops.orihime.nw_affine_marginals_grad_temp(s, -2.0, -0.5, 0.7, ln),
+                          rtol=1e-6, atol=1e-7)
+    # tensor parameters through the AutogradCUDA forward
+    go = torch.tensor(-2.0, device="cuda", requires_grad=True)
+    ge = torch.tensor(-0.5, device="cuda", requires_grad=True)
+    tp = torch.tensor(0.7, device="cuda", requires_grad=True)
+    x = s.clone().requires_grad_(True)
+    v, m = torch.ops.orihime.nw_affine_forward_t(x, go, ge, tp, ln)
+    (v.sum() + (m * cot).sum()).backward()
+    _, g0, g1, gT = torch.ops.orihime.nw_affine_value_grad_params(s, -2.0, -0.5, 0.7, ln)
+    mb = torch.ops.orihime.nw_affine_marginals_backward(s, cot, -2.0, -0.5, 0.7, ln)
+    assert torch.allclose(go.grad, g0.sum() + mb[1][0], rtol=1e-5, atol=1e-5)
+    assert torch.allclose(ge.grad, g1.sum() + mb[2][0], rtol=1e-5, atol=1e-5)
+    assert torch.allclose(tp.grad, gT.sum() + mb[3][0], rtol=1e-5, atol=1e-5)
+    from orihime_b200 import _ops
+    if len(_ops.LEGACY_DEFINED_HERE) == len(_ops.LEGACY_SCHEMAS):
+        o = torch.ops.orihime
+        assert all(torch.equal(a, b) for a, b in zip(o.soft_nw_affine_float(s, -2.0, -0.5, 0.7, ln),
+                                                      o.nw_affine_forward(s, -2.0, -0.5, 0.7, ln)))
+        for k, name in enumerate(("gap_open", "gap_ext", "temp")):
+            assert torch.equal(o.soft_nw_affine_param_jacobian(s, k, -2.0, -0.5, 0.7, ln),
+                               getattr(o, f"nw_affine_marginals_grad_{name}")(s, -2.0, -0.5, 0.7, ln))
+        with pytest.raises(RuntimeError, match="param_type must be 0, 1, or 2"):
+            o.soft_nw_affine_param_jacobian(s, 3, -2.0, -0.5, 0.7, ln)
