@@ -369,7 +369,8 @@ def second_order(args):
 # ---------------------------------------------------------------------------
 
 def global_alignment(args):
-    """Soft Needleman-Wunsch (linear gap) at three workloads: 64 pairs of
+    """Soft Needleman-Wunsch (linear gap, then affine gaps with gap_open -2,
+    gap_ext -0.5) at three workloads: 64 pairs of
     1024 x 1024 (scores 3 <e_i, f_j> / sqrt(64), gap -1, T 0.5) for the
     forward + adjoint (value, map, dS/dgap, dS/dT) and the value alone;
     256 pairs of 512 x 512 (N(0, 1) embeddings, d = 128) for the HVP, dP/dT
@@ -462,6 +463,57 @@ def global_alignment(args):
     ms = timed(lambda: (plan.values(flat, gap=gap, temp=temp, out=vals), 0)[1])
     res["ragged_value_only"] = {"ms": round(ms, 3), "gcups": round(rcells / ms / 1e6, 2)}
     del flat, plan, outr
+
+    # affine gaps: the same three workloads
+    aff = {}
+    go, ge = -2.0, -0.5
+    g.manual_seed(1)
+    e = torch.randn(B, N, d, generator=g, device="cuda")
+    f = torch.randn(B, N, d, generator=g, device="cuda")
+    s = (3.0 * torch.bmm(e, f.transpose(1, 2)) / d ** 0.5).contiguous()
+    del e, f
+    amap = torch.empty_like(s)
+    go_, ge_ = torch.empty(B, device="cuda"), torch.empty(B, device="cuda")
+    nb = int(lib.swb_nw_affine_workspace_bytes(B, N, N))
+    ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    nbv = int(lib.swb_nw_affine_value_workspace_bytes(B, N, N))
+    wsv = torch.empty(nbv, dtype=torch.uint8, device="cuda")
+    ms = timed(lambda: lib.swb_nw_affine_forward(P(s), None, B, N, N, go, ge, temp, P(val), P(amap),
+                                                 P(go_), P(ge_), P(gT), P(ws), nb, st, None))
+    aff["forward_adjoint"] = {"ms": round(ms, 3), "gcups": round(cells / ms / 1e6, 2)}
+    ms = timed(lambda: lib.swb_nw_affine_value(P(s), None, B, N, N, go, ge, temp, P(val), P(wsv),
+                                               nbv, st))
+    aff["value_only"] = {"ms": round(ms, 3), "gcups": round(cells / ms / 1e6, 2)}
+    del s, amap, ws, wsv
+    g.manual_seed(5)
+    e = torch.randn(B5, N5, d5, generator=g, device="cuda")
+    f = torch.randn(B5, N5, d5, generator=g, device="cuda")
+    s5 = (torch.bmm(e, f.transpose(1, 2)) / d5 ** 0.5).contiguous()
+    v5 = torch.randn(B5, N5, N5, generator=g, device="cuda")
+    del e, f
+    out = torch.empty_like(s5)
+    nx = int(lib.swb_nw_affine_aux_workspace_bytes(B5, N5, N5))
+    wx = torch.empty(nx, dtype=torch.uint8, device="cuda")
+    for name, fn in (
+            ("hvp", lambda: lib.swb_nw_affine_hvp(P(s5), P(v5), None, B5, N5, N5, go, ge, temp,
+                                                  P(out), None, P(wx), nx, st)),
+            ("grad_temp", lambda: lib.swb_nw_affine_param_jacobian(P(s5), None, B5, N5, N5, go, ge,
+                                                                   temp, 2, P(out), P(wx), nx, st)),
+            ("marginals_backward", lambda: lib.swb_nw_affine_hvp(P(s5), P(v5), None, B5, N5, N5, go,
+                                                                 ge, temp, P(out), P(gt), P(wx), nx,
+                                                                 st))):
+        ms = timed(fn)
+        aff[name] = {"ms": round(ms, 3), "gcups": round(c5 / ms / 1e6, 2), "shape": [B5, N5, N5]}
+    del s5, v5, out, wx
+    flat = make_scores(torch, lengths, offsets, 3, "cuda")
+    plan = ragged.Plan(ln32, offsets, family="global_affine", device="cuda")
+    outr = plan.outputs()
+    ms = timed(lambda: (plan.run(flat, gap_open=go, gap_ext=ge, temp=temp, out=outr), 0)[1])
+    aff["ragged_forward_adjoint"] = {"ms": round(ms, 3), "gcups": round(rcells / ms / 1e6, 2)}
+    ms = timed(lambda: (plan.values(flat, gap_open=go, gap_ext=ge, temp=temp, out=vals), 0)[1])
+    aff["ragged_value_only"] = {"ms": round(ms, 3), "gcups": round(rcells / ms / 1e6, 2)}
+    del flat, plan, outr
+    res["affine"] = dict(aff, params={"gap_open": go, "gap_ext": ge, "temp": temp})
 
     line = {"global_alignment": res, "shape": [B, N, N], "params": {"gap": gap, "temp": temp}}
     try:

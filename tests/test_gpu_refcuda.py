@@ -1,9 +1,9 @@
 """Our CUDA path against the reference's own CUDA path on the same GPU.
 
 The reference CUDA extension is built by ``make -C oracle refcuda`` from
-``src/sw*/kernels_gpu.cu``, ``src/nw/kernels_gpu.cu`` and the op bodies beside
-them.  It has to be loaded before orihime_b200, which then takes over the
-namespaced ``sw*`` / ``nw*`` ops; the reference's legacy ``soft_sw*`` /
+``src/sw*/kernels_gpu.cu``, ``src/nw*/kernels_gpu.cu`` and the op bodies
+beside them.  It has to be loaded before orihime_b200, which then takes over
+the namespaced ``sw*`` / ``nw*`` ops; the reference's legacy ``soft_sw*`` /
 ``soft_nw*`` ops stay the reference's CUDA path.  That
 order is fixed per process, so the comparison runs in a child process.
 
@@ -83,6 +83,24 @@ def _worker():
                         hvp_ref_64=dist(rh.cpu(), h64), hvp_scale=float(np.abs(h64).max()),
                         dpdt_ours_ref=dist(op_.cpu(), rp.cpu()), dpdt_ours_64=dist(op_.cpu(), p64),
                         dpdt_ref_64=dist(rp.cpu(), p64), dpdt_scale=float(np.abs(p64).max())))
+        # global alignment with affine gaps, same inputs
+        rv, rm = ops.soft_nw_affine_float(sd, -2.0, -0.5, T, ln.cuda())[:2]
+        ov, om = ops.nw_affine_forward(sd, -2.0, -0.5, T, ln.cuda())
+        t64 = O.nw_affine(s.numpy(), ln.numpy(), -2.0, -0.5, T, dtype=np.float64)
+        rel = float(((ov - rv).abs() / rv.abs().clamp_min(1.0)).max())
+        rh = ops.soft_nw_affine_hvp(sd, v.cuda(), -2.0, -0.5, T, ln.cuda())
+        oh = ops.nw_affine_marginals_hvp(sd, v.cuda(), -2.0, -0.5, T, ln.cuda())
+        h64 = O.nw_affine_hvp(s.numpy(), v.numpy(), ln.numpy(), -2.0, -0.5, T, dtype=np.float64)
+        rp = ops.soft_nw_affine_param_jacobian(sd, 2, -2.0, -0.5, T, ln.cuda())
+        op_ = ops.nw_affine_marginals_grad_temp(sd, -2.0, -0.5, T, ln.cuda())
+        p64 = O.nw_affine_param_grad(s.numpy(), ln.numpy(), -2.0, -0.5, T, 2, dtype=np.float64)
+        out.append(dict(case=["nw_affine", B, N, M, T], value_rel=rel,
+                        map_ours_ref=dist(om.cpu(), rm.cpu()), map_ours_64=dist(om.cpu(), t64["map"]),
+                        map_ref_64=dist(rm.cpu(), t64["map"]),
+                        hvp_ours_ref=dist(oh.cpu(), rh.cpu()), hvp_ours_64=dist(oh.cpu(), h64),
+                        hvp_ref_64=dist(rh.cpu(), h64), hvp_scale=float(np.abs(h64).max()),
+                        dpdt_ours_ref=dist(op_.cpu(), rp.cpu()), dpdt_ours_64=dist(op_.cpu(), p64),
+                        dpdt_ref_64=dist(rp.cpu(), p64), dpdt_scale=float(np.abs(p64).max())))
     # timing: C2 (64 x 1024^2) on both CUDA paths
     s = emb(64, 1024, 1024, 1).cuda()
 
@@ -102,6 +120,10 @@ def _worker():
     tr = t(lambda: ops.soft_nw_float(s, -1.0, 0.5, None), 2)
     to = t(lambda: ops.nw_forward(s, -1.0, 0.5, None), 5)
     out.append(dict(timing="NW (global) 64x1024^2 value+map", ref_ms=tr, ours_ms=to,
+                    ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
+    tr = t(lambda: ops.soft_nw_affine_float(s, -2.0, -0.5, 0.5, None), 2)
+    to = t(lambda: ops.nw_affine_forward(s, -2.0, -0.5, 0.5, None), 5)
+    out.append(dict(timing="NW affine 64x1024^2 value+map", ref_ms=tr, ours_ms=to,
                     ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
     del s
     # C1: linear, 8 x 128^2, N(0,1) scores, gap -1, T 1
@@ -131,7 +153,14 @@ def _worker():
             ("NW dP/dT", lambda: ops.soft_nw_param_jacobian(s5, 1, -1.0, 0.5, None),
              lambda: ops.nw_marginals_grad_temp(s5, -1.0, 0.5, None)),
             ("NW marginals_backward", lambda: ops.soft_nw_backward_full(s5, v5, -1.0, 0.5, None),
-             lambda: ops.nw_marginals_backward(s5, v5, -1.0, 0.5, None))):
+             lambda: ops.nw_marginals_backward(s5, v5, -1.0, 0.5, None)),
+            ("NW affine HVP", lambda: ops.soft_nw_affine_hvp(s5, v5, -2.0, -0.5, 0.5, None),
+             lambda: ops.nw_affine_marginals_hvp(s5, v5, -2.0, -0.5, 0.5, None)),
+            ("NW affine dP/dT", lambda: ops.soft_nw_affine_param_jacobian(s5, 2, -2.0, -0.5, 0.5, None),
+             lambda: ops.nw_affine_marginals_grad_temp(s5, -2.0, -0.5, 0.5, None)),
+            ("NW affine marginals_backward",
+             lambda: ops.soft_nw_affine_backward_full(s5, v5, -2.0, -0.5, 0.5, None),
+             lambda: ops.nw_affine_marginals_backward(s5, v5, -2.0, -0.5, 0.5, None))):
         tr, to = t(rf, 1), t(of, 3)
         out.append(dict(timing=name + " 256x512^2", ref_ms=tr, ours_ms=to,
                         ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
