@@ -7,11 +7,12 @@ directory under /tmp, compiles the reference's CPU extension there with g++
 the public soft Smith-Waterman API's outputs on small seeded inputs:
 
 * ``ohm.sw`` / ``sw_value`` / ``sw_entropy``, the ``sw_affine`` trio and the
-  global-alignment ``nw`` trio: forward results and the gradients of value,
-  map (against a fixed cotangent) and entropy with respect to the pair scores;
+  global-alignment ``nw`` and ``nw_affine`` trios: forward results and the
+  gradients of value, map (against a fixed cotangent) and entropy with respect
+  to the pair scores;
 * lengths-ragged and boolean-mask batches;
 * tensor-valued (learnable) gap parameters and their gradients;
-* ``ohm.ops.sw*.backward`` / ``ohm.ops.nw.backward`` (map VJP) and
+* ``ohm.ops.sw*.backward`` / ``ohm.ops.nw*.backward`` (map VJP) and
   ``.sensitivity`` (parameter fields).
 
 Output: ``sw_golden.npz`` (float32 arrays, a few hundred KB).
@@ -109,10 +110,14 @@ def main() -> None:
         for fam, kw in (("lin", dict(gap_score=-1.0, temperature=0.7)),
                         ("aff", dict(gap_open_score=-2.0, gap_extend_score=-0.5,
                                      temperature=0.7)),
-                        ("nw", dict(gap_score=-1.0, temperature=0.7))):
+                        ("nw", dict(gap_score=-1.0, temperature=0.7)),
+                        ("nwa", dict(gap_open_score=-2.0, gap_extend_score=-0.5,
+                                     temperature=0.7))):
             fmap, fval, fent = {"lin": (ohm.sw, ohm.sw_value, ohm.sw_entropy),
                                 "aff": (ohm.sw_affine, ohm.sw_affine_value, ohm.sw_affine_entropy),
-                                "nw": (ohm.nw, ohm.nw_value, ohm.nw_entropy)}[fam]
+                                "nw": (ohm.nw, ohm.nw_value, ohm.nw_entropy),
+                                "nwa": (ohm.nw_affine, ohm.nw_affine_value,
+                                        ohm.nw_affine_entropy)}[fam]
             key = f"{name}/{fam}"
             x = x0.clone().requires_grad_(True)
             v = fval(x, lengths=lt, **kw)
@@ -129,7 +134,8 @@ def main() -> None:
             (g,) = torch.autograd.grad(h.sum(), x)
             put(f"{key}/entropy", h)
             put(f"{key}/dentropy", g)
-            op = {"lin": ohm.ops.sw, "aff": ohm.ops.sw_affine, "nw": ohm.ops.nw}[fam]
+            op = {"lin": ohm.ops.sw, "aff": ohm.ops.sw_affine, "nw": ohm.ops.nw,
+                  "nwa": ohm.ops.nw_affine}[fam]
             sens = op.sensitivity(x0, lengths=lt, **kw)
             for k2, t in sens.items():
                 put(f"{key}/sens_{k2}", t)

@@ -321,3 +321,33 @@ def test_nw_affine_public_autograd_and_legacy():
                                getattr(o, f"nw_affine_marginals_grad_{name}")(s, -2.0, -0.5, 0.7, ln))
         with pytest.raises(RuntimeError, match="param_type must be 0, 1, or 2"):
             o.soft_nw_affine_param_jacobian(s, 3, -2.0, -0.5, 0.7, ln)
+
+
+def test_nw_affine_public_api_vs_golden(golden):
+    """ohm.nw_affine / nw_affine_value / nw_affine_entropy and the map VJP,
+    against fixtures recorded from the reference's public API."""
+    import orihime_b200 as ob
+    for case in ("sq", "rect", "ragged", "unit", "row"):
+        s = torch.from_numpy(golden[f"{case}/scores"]).cuda()
+        cot = torch.from_numpy(golden[f"{case}/cot"]).cuda()
+        ln = (torch.from_numpy(golden[f"{case}/lengths"]).to(torch.int32).cuda()
+              if f"{case}/lengths" in golden.files else None)
+        g = lambda k: golden[f"{case}/nwa/{k}"]  # noqa: E731
+        kw = dict(gap_open_score=-2.0, gap_extend_score=-0.5, temperature=0.7, lengths=ln)
+        np.testing.assert_allclose(ob.nw_affine_value(s, **kw).cpu().numpy(), g("value"), rtol=1e-5,
+                                   atol=1e-5)
+        x = s.clone().requires_grad_(True)
+        (dx,) = torch.autograd.grad(-ob.nw_affine_value(x, **kw).mean(), x)
+        np.testing.assert_allclose(dx.cpu().numpy(), g("dvalue"), atol=1e-5)
+        x = s.clone().requires_grad_(True)
+        (dm,) = torch.autograd.grad((ob.nw_affine(x, **kw) * cot).sum(), x)
+        np.testing.assert_allclose(dm.cpu().numpy(), g("dmap"), atol=1e-5)
+        x = s.clone().requires_grad_(True)
+        h = ob.nw_affine_entropy(x, **kw)
+        np.testing.assert_allclose(h.detach().cpu().numpy(), g("entropy"), atol=2e-5)
+        (de,) = torch.autograd.grad(h.sum(), x)
+        np.testing.assert_allclose(de.cpu().numpy(), g("dentropy"), atol=1e-5)
+        bw = torch.ops.orihime.nw_affine_marginals_backward(s, cot, -2.0, -0.5, 0.7, ln)
+        np.testing.assert_allclose(bw[0].cpu().numpy(), g("bw_pair_scores"), atol=1e-5)
+        for k, name in enumerate(("gap_open_score", "gap_extend_score", "temperature")):
+            np.testing.assert_allclose(bw[1 + k].item(), g(f"bw_{name}"), atol=1e-4)

@@ -93,6 +93,31 @@ def test_nw_oracle_vs_golden(golden, case):
     _close((cot * sens[1]).sum(), g("bw_temperature"), atol=1e-4)
 
 
+@pytest.mark.parametrize("case", CASES)
+def test_nw_affine_oracle_vs_golden(golden, case):
+    """Global alignment with affine gaps (ohm.nw_affine trio, ohm.ops.nw_affine)
+    against the recorded fixtures."""
+    s, ln, cot = _case(golden, case)
+    g = lambda k: golden[f"{case}/nwa/{k}"]
+    B = s.shape[0]
+    o = O.nw_affine(s, ln, -2.0, -0.5, T0)
+    _close(o["value"], g("value"))
+    _close(o["map"], g("map"))
+    _close(-o["map"] / B, g("dvalue"))
+    _close(o["grad_temp"], g("entropy"), atol=2e-5)
+    sens = {p: O.nw_affine_param_grad(s, ln, -2.0, -0.5, T0, p) for p in range(3)}
+    _close(sens[0], g("sens_gap_open_score"), atol=1e-5)
+    _close(sens[1], g("sens_gap_extend_score"), atol=1e-5)
+    _close(sens[2], g("sens_temperature"), atol=1e-5)
+    _close(sens[2], g("dentropy"), atol=1e-5)
+    hv = O.nw_affine_hvp(s, cot, ln, -2.0, -0.5, T0)
+    _close(hv, g("dmap"), atol=1e-5)
+    _close(hv, g("bw_pair_scores"), atol=1e-5)
+    _close((cot * sens[0]).sum(), g("bw_gap_open_score"), atol=1e-4)
+    _close((cot * sens[1]).sum(), g("bw_gap_extend_score"), atol=1e-4)
+    _close((cot * sens[2]).sum(), g("bw_temperature"), atol=1e-4)
+
+
 def _mask_sentinel(scores, mask, T):
     """orihime/operator.py:334-386: masked cells -> amax - (sum(shape[1:])*80 + 200)*T."""
     x = np.where(mask, -np.inf, scores).astype(np.float32)
@@ -165,6 +190,14 @@ def test_oracle_bit_exact_vs_reference_kernels(seed):
             for p in range(2):
                 assert np.array_equal(O.linear_param_grad(s, lens, -1.0, T, p),
                                       O.ref_linear_param_grad(s, lens, -1.0, T, p))
+            a, r = O.nw_affine(s, lens, -2.0, -0.5, T), O.ref_nw_affine(s, lens, -2.0, -0.5, T)
+            for k in a:
+                assert np.array_equal(a[k], r[k]), k
+            assert np.array_equal(O.nw_affine_hvp(s, V, lens, -2.0, -0.5, T),
+                                  O.ref_nw_affine_hvp(s, V, lens, -2.0, -0.5, T))
+            for p in range(3):
+                assert np.array_equal(O.nw_affine_param_grad(s, lens, -2.0, -0.5, T, p),
+                                      O.ref_nw_affine_param_grad(s, lens, -2.0, -0.5, T, p))
             a, r = O.nw(s, lens, -1.0, T), O.ref_nw(s, lens, -1.0, T)
             for k in a:
                 assert np.array_equal(a[k], r[k]), k
