@@ -184,6 +184,34 @@ int swb_nw_affine_ragged_value(const float* scores, const void* host_plan, const
                                float gap_open, float gap_ext, float temp, float* value,
                                void* workspace, size_t workspace_bytes, void* stream);
 
+/*
+ * Saigo–Vert local alignment, affine gaps: value S = LSE(0, M cells), marginal
+ * map (posterior of M), dS/dgap_open, dS/dgap_ext, dS/dT.  The local affine
+ * model with one more transition, D <- I (gap open) from the left; only M
+ * ends an alignment.  Replaces soft_sv_affine_cuda_float /
+ * soft_sv_affine_cuda_with_grads (src/sv_affine/torch_cuda.cpp), restating
+ * src/sv_affine/kernels_cpu.cpp:81-365.  The linear model
+ * (src/sv_linear) is this one with gap_open = gap_ext = gap and
+ * dS/dgap = dS/dgap_open + dS/dgap_ext.  Value-only and packed ragged calls
+ * (plan family 5) as for the other families.
+ */
+size_t swb_sv_affine_workspace_bytes(int B, int L1max, int L2max);
+int swb_sv_affine_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap_open, float gap_ext, float temp, float* value, float* map,
+                          float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                          size_t workspace_bytes, void* stream, const swb_options* opt);
+size_t swb_sv_affine_value_workspace_bytes(int B, int L1max, int L2max);
+int swb_sv_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                        float gap_open, float gap_ext, float temp, float* value, void* workspace,
+                        size_t workspace_bytes, void* stream);
+int swb_sv_affine_ragged(const float* scores, const void* host_plan, const void* dev_plan,
+                         float gap_open, float gap_ext, float temp, float* value, float* map,
+                         float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                         size_t workspace_bytes, void* stream, const swb_options* opt);
+int swb_sv_affine_ragged_value(const float* scores, const void* host_plan, const void* dev_plan,
+                               float gap_open, float gap_ext, float temp, float* value,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
 /* Value only (forward wavefront alone; equals swb_nw_forward's value bit for bit). */
 size_t swb_nw_value_workspace_bytes(int B, int L1max, int L2max);
 int swb_nw_value(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
@@ -206,8 +234,8 @@ int swb_nw_value(const float* scores, const int* lengths, int B, int L1max, int 
  * *plan_bytes (and *workspace_bytes), then with a buffer of that size; copy
  * the plan bytes to the device unchanged and pass both copies to the launch.
  * family: 3 = affine, 1 = linear, 2 = global alignment (soft Needleman–Wunsch,
- * linear gap), 4 = global alignment with affine gaps; cols_per_lane: 2 or 4
- * (0 = default).
+ * linear gap), 4 = global alignment with affine gaps, 5 = Saigo–Vert;
+ * cols_per_lane: 2 or 4 (0 = default).
  * host lengths [B, 2], host offsets [B+1].
  */
 int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const long long* offsets,
@@ -314,6 +342,17 @@ size_t swb_nw_aux_workspace_bytes(int B, int L1max, int L2max);
  * replacing soft_nw_affine_hvp_cuda and soft_nw_affine_param_jacobian_cuda
  * (src/nw_affine/torch_cuda.cpp:435, :484; backward_full :555). */
 size_t swb_nw_affine_aux_workspace_bytes(int B, int L1max, int L2max);
+/* Saigo–Vert: the same two ops (param 0 / 1 / 2 = gap_open / gap_ext / temp;
+ * the linear model's gap direction is the sum of 0 and 1), replacing
+ * soft_sv_affine_hvp_cuda and soft_sv_affine_param_jacobian_cuda
+ * (src/sv_affine/torch_cuda.cpp; restating src/sv_affine/kernels_cpu.cpp:369-934). */
+size_t swb_sv_affine_aux_workspace_bytes(int B, int L1max, int L2max);
+int swb_sv_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
+                      int L2max, float gap_open, float gap_ext, float temp, float* out,
+                      float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream);
+int swb_sv_affine_param_jacobian(const float* scores, const int* lengths, int B, int L1max,
+                                 int L2max, float gap_open, float gap_ext, float temp, int param,
+                                 float* out, void* workspace, size_t workspace_bytes, void* stream);
 int swb_nw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
                       int L2max, float gap_open, float gap_ext, float temp, float* out,
                       float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream);

@@ -260,9 +260,54 @@ def nw_affine_param_grad(scores, lengths, gap_open, gap_ext, temp, param: int,
     return out
 
 
+def sv(scores, lengths, gap_open, gap_ext, temp, linear=False, dtype=np.float32) -> dict:
+    """Saigo-Vert local alignment: value [B], map, grad_open/grad_ext/grad_temp
+    [B]; linear=True (go = ge = gap) reports dS/dgap as grad_open."""
+    s, ln = _prep(scores, lengths, dtype)
+    B, L1, L2 = s.shape
+    out = {k: np.zeros(B, dtype) for k in ("value", "grad_open", "grad_ext", "grad_temp")}
+    out["map"] = np.zeros_like(s)
+    sc = _scal(dtype)
+    rc = getattr(lib(), "oracle_sv_forward" + _sfx(dtype))(
+        _ptr(s), _ptr(ln), _I(B), _I(L1), _I(L2), sc(gap_open), sc(gap_ext), sc(temp), _I(int(linear)),
+        _ptr(out["value"]), _ptr(out["map"]), _ptr(out["grad_open"]), _ptr(out["grad_ext"]),
+        _ptr(out["grad_temp"]))
+    assert rc == 0
+    return out
+
+
+def sv_hvp(scores, v, lengths, gap_open, gap_ext, temp, dtype=np.float32) -> np.ndarray:
+    s, ln = _prep(scores, lengths, dtype)
+    vv = np.ascontiguousarray(v, dtype=dtype)
+    B, L1, L2 = s.shape
+    out = np.zeros_like(s)
+    sc = _scal(dtype)
+    rc = getattr(lib(), "oracle_sv_hvp" + _sfx(dtype))(
+        _ptr(s), _ptr(vv), _ptr(ln), _I(B), _I(L1), _I(L2), sc(gap_open), sc(gap_ext), sc(temp),
+        _ptr(out))
+    assert rc == 0
+    return out
+
+
+def sv_param_grad(scores, lengths, gap_open, gap_ext, temp, param: int, linear=False,
+                  dtype=np.float32) -> np.ndarray:
+    """d(map)/d(theta); affine: 0 = gap_open, 1 = gap_ext, 2 = temperature;
+    linear (go = ge = gap): 0 = gap, 1 = temperature."""
+    s, ln = _prep(scores, lengths, dtype)
+    B, L1, L2 = s.shape
+    out = np.zeros_like(s)
+    sc = _scal(dtype)
+    pt = ((3, 2)[param]) if linear else param
+    rc = getattr(lib(), "oracle_sv_param_grad" + _sfx(dtype))(
+        _ptr(s), _ptr(ln), _I(B), _I(L1), _I(L2), sc(gap_open), sc(gap_ext), sc(temp),
+        _I(int(linear)), _I(pt), _ptr(out))
+    assert rc == 0
+    return out
+
+
 # ---------------------------------------------------------------------------
 # the reference's own CPU kernels (src/sw*/kernels_cpu.cpp,
-# src/nw*/kernels_cpu.cpp), float32 only
+# src/nw*/kernels_cpu.cpp, src/sv_*/kernels_cpu.cpp), float32 only
 # ---------------------------------------------------------------------------
 
 def _full_lengths(B, L1, L2, ln):
@@ -491,4 +536,71 @@ def ref_nw_affine_param_grad(scores, lengths, gap_open, gap_ext, temp, param: in
     r.nw_affine_forward_cpu(_ptr(s), _ptr(alpha), _ptr(part), _ptr(ln), *a)
     r.nw_affine_param_grad_cpu(_ptr(alpha), _ptr(s), _ptr(part), _ptr(dS), _ptr(U), _ptr(be), _ptr(W),
                                _ptr(out), _ptr(ln), *a, _I(param))
+    return out
+
+
+def _ref_sv_prefix(linear):
+    return "sv_linear" if linear else "sv_affine"
+
+
+def ref_sv(scores, lengths, gap_open, gap_ext, temp, linear=False) -> dict:
+    """sv_{affine,linear}_forward_cpu + _backward_cpu (src/sv_*/kernels_cpu.cpp)."""
+    s, ln = _prep(scores, lengths, np.float32)
+    B, L1, L2 = s.shape
+    ln = _full_lengths(B, L1, L2, ln)
+    n_alpha = 3 * (L1 + 1) * (L2 + 1)
+    alpha = np.empty((B, n_alpha), np.float32)
+    beta = np.empty((B, n_alpha), np.float32)
+    out = {k: np.zeros(B, np.float32) for k in ("value", "grad_open", "grad_ext", "grad_temp")}
+    out["map"] = np.zeros_like(s)
+    r = ref_lib()
+    pre = _ref_sv_prefix(linear)
+    prm = (_F(gap_open), _F(temp)) if linear else (_F(gap_open), _F(gap_ext), _F(temp))
+    a = (_I(B), _I(L1), _I(L2), *prm)
+    getattr(r, pre + "_forward_cpu")(_ptr(s), _ptr(alpha), _ptr(out["value"]), _ptr(ln), *a)
+    grads = ((out["grad_open"], out["grad_temp"]) if linear
+             else (out["grad_open"], out["grad_ext"], out["grad_temp"]))
+    getattr(r, pre + "_backward_cpu")(_ptr(alpha), _ptr(s), _ptr(out["value"]), _ptr(beta),
+                                      _ptr(out["map"]), *map(_ptr, grads), _ptr(ln), *a)
+    return out
+
+
+def ref_sv_hvp(scores, v, lengths, gap_open, gap_ext, temp, linear=False) -> np.ndarray:
+    s, ln = _prep(scores, lengths, np.float32)
+    vv = np.ascontiguousarray(v, dtype=np.float32)
+    B, L1, L2 = s.shape
+    ln = _full_lengths(B, L1, L2, ln)
+    n_alpha = 3 * (L1 + 1) * (L2 + 1)
+    alpha, da, dbe = (np.empty((B, n_alpha), np.float32) for _ in range(3))
+    part = np.zeros(B, np.float32)
+    dpart = np.zeros(B, np.float32)
+    out = np.zeros_like(s)
+    r = ref_lib()
+    pre = _ref_sv_prefix(linear)
+    prm = (_F(gap_open), _F(temp)) if linear else (_F(gap_open), _F(gap_ext), _F(temp))
+    a = (_I(B), _I(L1), _I(L2), *prm)
+    getattr(r, pre + "_forward_cpu")(_ptr(s), _ptr(alpha), _ptr(part), _ptr(ln), *a)
+    getattr(r, pre + "_hvp_cpu")(_ptr(alpha), _ptr(s), _ptr(part), _ptr(vv), _ptr(da), _ptr(dpart),
+                                 _ptr(dbe), _ptr(out), _ptr(ln), *a)
+    return out
+
+
+def ref_sv_param_grad(scores, lengths, gap_open, gap_ext, temp, param: int, linear=False) -> np.ndarray:
+    s, ln = _prep(scores, lengths, np.float32)
+    B, L1, L2 = s.shape
+    ln = _full_lengths(B, L1, L2, ln)
+    base = ref_sv(s, ln, gap_open, gap_ext, temp, linear)
+    key = (("grad_open", "grad_temp") if linear else ("grad_open", "grad_ext", "grad_temp"))[param]
+    n_alpha = 3 * (L1 + 1) * (L2 + 1)
+    alpha, U, be, W = (np.empty((B, n_alpha), np.float32) for _ in range(4))
+    part = np.zeros(B, np.float32)
+    out = np.zeros_like(s)
+    dS = np.ascontiguousarray(base[key])
+    r = ref_lib()
+    pre = _ref_sv_prefix(linear)
+    prm = (_F(gap_open), _F(temp)) if linear else (_F(gap_open), _F(gap_ext), _F(temp))
+    a = (_I(B), _I(L1), _I(L2), *prm)
+    getattr(r, pre + "_forward_cpu")(_ptr(s), _ptr(alpha), _ptr(part), _ptr(ln), *a)
+    getattr(r, pre + "_param_grad_cpu")(_ptr(alpha), _ptr(s), _ptr(part), _ptr(dS), _ptr(U), _ptr(be),
+                                        _ptr(W), _ptr(out), _ptr(ln), *a, _I(param))
     return out

@@ -1216,6 +1216,346 @@ static void FN(nwa_param)(FN(aff_t) *c, int pt, REAL *u, REAL *be, REAL *wt, REA
     }
 }
 
+/* ---- Saigo-Vert local alignment (affine gaps; linear = go = ge = gap) ----
+ * src/sv_affine/kernels_cpu.cpp and src/sv_linear/kernels_cpu.cpp: the local
+ * affine model with one more transition, D <- I (gap open) from the left,
+ * and S = LSE(0, M cells) -- only M states end an alignment, so only M has a
+ * beta-init.  M's candidates add the score inside each term (diag + s and the
+ * start term s), as the reference writes them.  `lin` selects the linear
+ * file's accumulation of dS/dgap (one Kahan sum) and its gap direction (every
+ * gap term). */
+
+static void FN(sv_cands)(const FN(aff_t) *c, const REAL *t, int i, int j, REAL v[9]) {
+    REAL s = SC(c, i, j);
+    int dg = i > 1 && j > 1;
+    v[0] = dg ? t[AIX(c, 0, i - 1, j - 1)] + s : (REAL)NEG_BIG;
+    v[1] = dg ? t[AIX(c, 1, i - 1, j - 1)] + s : (REAL)NEG_BIG;
+    v[2] = dg ? t[AIX(c, 2, i - 1, j - 1)] + s : (REAL)NEG_BIG;
+    v[3] = s;
+    v[4] = i > 1 ? t[AIX(c, 0, i - 1, j)] + c->go : (REAL)NEG_BIG;
+    v[5] = i > 1 ? t[AIX(c, 1, i - 1, j)] + c->ge : (REAL)NEG_BIG;
+    v[6] = j > 1 ? t[AIX(c, 0, i, j - 1)] + c->go : (REAL)NEG_BIG;
+    v[7] = j > 1 ? t[AIX(c, 1, i, j - 1)] + c->go : (REAL)NEG_BIG;
+    v[8] = j > 1 ? t[AIX(c, 2, i, j - 1)] + c->ge : (REAL)NEG_BIG;
+}
+
+/* src/sv_affine/kernels_cpu.cpp:81-196 */
+static REAL FN(sv_forward)(FN(aff_t) *c) {
+    for (int st = 0; st < 3; ++st)
+        for (int i = 0; i <= c->L1; ++i)
+            for (int j = 0; j <= c->L2; ++j) c->a[AIX(c, st, i, j)] = (REAL)NEG_BIG;
+    c->a[AIX(c, 0, 0, 0)] = 0;
+    REAL v[9];
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            FN(sv_cands)(c, c->a, i, j, v);
+            c->a[AIX(c, 0, i, j)] = FN(tlse)(v, 4, c->T);
+            c->a[AIX(c, 1, i, j)] = FN(tlse)(v + 4, 2, c->T);
+            c->a[AIX(c, 2, i, j)] = FN(tlse)(v + 6, 3, c->T);
+        }
+    }
+    REAL m = 0;   /* the empty alignment (score 0) */
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j)
+            if (c->a[AIX(c, 0, i, j)] > m) m = c->a[AIX(c, 0, i, j)];
+    FN(ksum_t) k = {0, 0};
+    FN(kadd)(&k, FN(clip_exp)((0 - m) / c->T));
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            REAL x = c->a[AIX(c, 0, i, j)];
+            if (x > (REAL)NEG_BIG) FN(kadd)(&k, FN(clip_exp)((x - m) / c->T));
+        }
+    return m + c->T * LOGF(k.s);
+}
+
+#define SV_LIVE(b) (!isinf(b) && !isnan(b) && (b) != 0)
+
+/* src/sv_affine/kernels_cpu.cpp:200-365, src/sv_linear/kernels_cpu.cpp:207-370;
+ * affine g = dS/d(go, ge, T); linear g[0] = dS/dgap, g[2] = dS/dT. */
+static void FN(sv_adjoint)(const FN(aff_t) *c, REAL S, REAL *be, REAL *post, int L1max, int lin,
+                           REAL g[3]) {
+    size_t nsc = (size_t)L1max * c->ld;
+    for (size_t q = 0; q < nsc; ++q) post[q] = 0;
+    for (int st = 0; st < 3; ++st)
+        for (int i = 0; i <= c->L1; ++i)
+            for (int j = 0; j <= c->L2; ++j) be[AIX(c, st, i, j)] = 0;
+    const REAL T = c->T;
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            REAL lp = (c->a[AIX(c, 0, i, j)] - S) / T;
+            if (lp > 0) lp = 0;
+            be[AIX(c, 0, i, j)] = FN(clip_exp)(lp);
+        }
+    REAL so = 0, se = 0, w[4], v[9];
+    FN(ksum_t) gk = {0, 0};
+    NW_DIAGS(c, k, i, j) {
+        FN(sv_cands)(c, c->a, i, j, v);
+        REAL bM = be[AIX(c, 0, i, j)];
+        if (SV_LIVE(bM)) {
+            FN(tsoftmax)(v, 4, T, w);
+            post[(size_t)(i - 1) * c->ld + (j - 1)] += bM * (w[0] + w[1] + w[2] + w[3]);
+            if (i > 1 && j > 1)
+                for (int st = 0; st < 3; ++st)
+                    if (w[st] > 0) be[AIX(c, st, i - 1, j - 1)] += bM * w[st];
+        }
+        REAL bI = be[AIX(c, 1, i, j)];
+        if (SV_LIVE(bI)) {
+            FN(tsoftmax)(v + 4, 2, T, w);
+            if (i > 1) {
+                if (w[0] > 0) {
+                    be[AIX(c, 0, i - 1, j)] += bI * w[0];
+                    if (lin) FN(kadd)(&gk, bI * w[0]); else so += bI * w[0];
+                }
+                if (w[1] > 0) {
+                    be[AIX(c, 1, i - 1, j)] += bI * w[1];
+                    if (lin) FN(kadd)(&gk, bI * w[1]); else se += bI * w[1];
+                }
+            }
+        }
+        REAL bD = be[AIX(c, 2, i, j)];
+        if (SV_LIVE(bD)) {
+            FN(tsoftmax)(v + 6, 3, T, w);
+            if (j > 1) {
+                if (w[0] > 0) {
+                    be[AIX(c, 0, i, j - 1)] += bD * w[0];
+                    if (lin) FN(kadd)(&gk, bD * w[0]); else so += bD * w[0];
+                }
+                if (w[1] > 0) {
+                    be[AIX(c, 1, i, j - 1)] += bD * w[1];
+                    if (lin) FN(kadd)(&gk, bD * w[1]); else so += bD * w[1];
+                }
+                if (w[2] > 0) {
+                    be[AIX(c, 2, i, j - 1)] += bD * w[2];
+                    if (lin) FN(kadd)(&gk, bD * w[2]); else se += bD * w[2];
+                }
+            }
+        }
+    }
+    FN(ksum_t) ms = {0, 0};
+    for (size_t q = 0; q < nsc; ++q) FN(kadd)(&ms, post[q] * c->s[q]);
+    if (lin) {
+        REAL gc = gk.s;
+        FN(ksum_t) et = {0, 0};
+        FN(kadd)(&et, ms.s);
+        FN(kadd)(&et, gc * c->go);
+        g[0] = gc; g[1] = 0; g[2] = (S - et.s) / T;
+    } else {
+        REAL egc = so * c->go + se * c->ge;
+        REAL et = ms.s + egc;
+        g[0] = so; g[1] = se; g[2] = (S - et) / T;
+    }
+}
+
+/* src/sv_affine/kernels_cpu.cpp:369-620 (HVP; the linear file's is the same). */
+static void FN(sv_hvp)(FN(aff_t) *c, REAL S, const REAL *V, REAL *da, REAL *dbe, REAL *be,
+                       REAL *H, int L1max) {
+    size_t nsc = (size_t)L1max * c->ld;
+    for (int st = 0; st < 3; ++st)
+        for (int i = 0; i <= c->L1; ++i)
+            for (int j = 0; j <= c->L2; ++j) {
+                size_t o = AIX(c, st, i, j);
+                da[o] = 0; dbe[o] = 0; be[o] = 0;
+            }
+    for (size_t q = 0; q < nsc; ++q) H[q] = 0;
+    const REAL T = c->T;
+    REAL w[4], v[9], t[4], dw[4];
+#define VV(i, j) V[(size_t)((i) - 1) * c->ld + (size_t)((j) - 1)]
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            REAL vv = VV(i, j);
+            int dg = i > 1 && j > 1;
+            FN(sv_cands)(c, c->a, i, j, v);
+            FN(tsoftmax)(v, 4, T, w);
+            for (int st = 0; st < 3; ++st) t[st] = dg ? da[AIX(c, st, i - 1, j - 1)] + vv : 0;
+            t[3] = vv;
+            da[AIX(c, 0, i, j)] = w[0] * t[0] + w[1] * t[1] + w[2] * t[2] + w[3] * t[3];
+            FN(tsoftmax)(v + 4, 2, T, w);
+            da[AIX(c, 1, i, j)] = w[0] * (i > 1 ? da[AIX(c, 0, i - 1, j)] : 0) +
+                                  w[1] * (i > 1 ? da[AIX(c, 1, i - 1, j)] : 0);
+            FN(tsoftmax)(v + 6, 3, T, w);
+            da[AIX(c, 2, i, j)] = w[0] * (j > 1 ? da[AIX(c, 0, i, j - 1)] : 0) +
+                                  w[1] * (j > 1 ? da[AIX(c, 1, i, j - 1)] : 0) +
+                                  w[2] * (j > 1 ? da[AIX(c, 2, i, j - 1)] : 0);
+        }
+    }
+    FN(ksum_t) dk = {0, 0};
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j)
+            FN(kadd)(&dk, FN(end_weight)(c->a[AIX(c, 0, i, j)], S, T) * da[AIX(c, 0, i, j)]);
+    REAL dS = dk.s;
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) be[AIX(c, 0, i, j)] = FN(end_weight)(c->a[AIX(c, 0, i, j)], S, T);
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) {
+            size_t o = AIX(c, 0, i, j);
+            dbe[o] = be[o] * (da[o] - dS) / T;
+        }
+    NW_DIAGS(c, k, i, j) {
+        REAL vv = VV(i, j);
+        int dg = i > 1 && j > 1;
+        FN(sv_cands)(c, c->a, i, j, v);
+        REAL bM = be[AIX(c, 0, i, j)], dM = dbe[AIX(c, 0, i, j)];
+        FN(tsoftmax)(v, 4, T, w);
+        for (int st = 0; st < 3; ++st) t[st] = dg ? da[AIX(c, st, i - 1, j - 1)] + vv : 0;
+        t[3] = vv;
+        REAL e = w[0] * t[0] + w[1] * t[1] + w[2] * t[2] + w[3] * t[3];
+        for (int q = 0; q < 4; ++q) dw[q] = w[q] * (t[q] - e) / T;
+        H[(size_t)(i - 1) * c->ld + (j - 1)] += dM * (w[0] + w[1] + w[2] + w[3]) +
+                                                bM * (dw[0] + dw[1] + dw[2] + dw[3]);
+        if (dg)
+            for (int st = 0; st < 3; ++st) be[AIX(c, st, i - 1, j - 1)] += bM * w[st];
+        if (dg)
+            for (int st = 0; st < 3; ++st)
+                dbe[AIX(c, st, i - 1, j - 1)] += dM * w[st] + bM * dw[st];
+        REAL bI = be[AIX(c, 1, i, j)], dI = dbe[AIX(c, 1, i, j)];
+        FN(tsoftmax)(v + 4, 2, T, w);
+        t[0] = i > 1 ? da[AIX(c, 0, i - 1, j)] : 0;
+        t[1] = i > 1 ? da[AIX(c, 1, i - 1, j)] : 0;
+        e = w[0] * t[0] + w[1] * t[1];
+        dw[0] = w[0] * (t[0] - e) / T;
+        dw[1] = w[1] * (t[1] - e) / T;
+        if (i > 1) {
+            be[AIX(c, 0, i - 1, j)] += bI * w[0];
+            be[AIX(c, 1, i - 1, j)] += bI * w[1];
+        }
+        if (i > 1) {
+            dbe[AIX(c, 0, i - 1, j)] += dI * w[0] + bI * dw[0];
+            dbe[AIX(c, 1, i - 1, j)] += dI * w[1] + bI * dw[1];
+        }
+        REAL bD = be[AIX(c, 2, i, j)], dD = dbe[AIX(c, 2, i, j)];
+        FN(tsoftmax)(v + 6, 3, T, w);
+        for (int st = 0; st < 3; ++st) t[st] = j > 1 ? da[AIX(c, st, i, j - 1)] : 0;
+        e = w[0] * t[0] + w[1] * t[1] + w[2] * t[2];
+        for (int q = 0; q < 3; ++q) dw[q] = w[q] * (t[q] - e) / T;
+        if (j > 1)
+            for (int st = 0; st < 3; ++st) be[AIX(c, st, i, j - 1)] += bD * w[st];
+        if (j > 1)
+            for (int st = 0; st < 3; ++st) dbe[AIX(c, st, i, j - 1)] += dD * w[st] + bD * dw[st];
+    }
+#undef VV
+}
+
+/* src/sv_affine/kernels_cpu.cpp:630-934 (dP/dtheta); pt 0 = gap_open, 1 =
+ * gap_ext, 2 = temperature, 3 = the linear model's single gap (every gap term). */
+static void FN(sv_param)(FN(aff_t) *c, REAL S, REAL dSdt, int pt, REAL *u, REAL *be, REAL *wt,
+                         REAL *dP, int L1max) {
+    size_t nsc = (size_t)L1max * c->ld;
+    for (int st = 0; st < 3; ++st)
+        for (int i = 0; i <= c->L1; ++i)
+            for (int j = 0; j <= c->L2; ++j) {
+                size_t o = AIX(c, st, i, j);
+                u[o] = 0; be[o] = 0; wt[o] = 0;
+            }
+    for (size_t q = 0; q < nsc; ++q) dP[q] = 0;
+    const REAL T = c->T;
+    const int TM = pt == 2;
+    /* direct tangents: I <- (M open, I ext); D <- (M open, I open, D ext) */
+    const REAL dI[2] = {(pt == 0 || pt == 3) ? 1 : 0, (pt == 1 || pt == 3) ? 1 : 0};
+    const REAL dD[3] = {(pt == 0 || pt == 3) ? 1 : 0, (pt == 0 || pt == 3) ? 1 : 0,
+                        (pt == 1 || pt == 3) ? 1 : 0};
+    REAL w[4], v[9], t[4], dw[4];
+    for (int k = 2; k <= c->L1 + c->L2; ++k) {
+        int i0 = (k - c->L2 > 1) ? k - c->L2 : 1;
+        int i1 = (c->L1 < k - 1) ? c->L1 : k - 1;
+        for (int i = i0; i <= i1; ++i) {
+            int j = k - i;
+            int dg = i > 1 && j > 1;
+            FN(sv_cands)(c, c->a, i, j, v);
+            FN(tsoftmax)(v, 4, T, w);
+            REAL U = w[0] * (dg ? u[AIX(c, 0, i - 1, j - 1)] : 0) + w[1] * (dg ? u[AIX(c, 1, i - 1, j - 1)] : 0) +
+                     w[2] * (dg ? u[AIX(c, 2, i - 1, j - 1)] : 0);
+            if (TM) {
+                REAL e = w[0] * v[0] + w[1] * v[1] + w[2] * v[2] + w[3] * v[3];
+                U += (c->a[AIX(c, 0, i, j)] - e) / T;
+            }
+            u[AIX(c, 0, i, j)] = U;
+            FN(tsoftmax)(v + 4, 2, T, w);
+            t[0] = (i > 1 ? u[AIX(c, 0, i - 1, j)] : 0) + dI[0];
+            t[1] = (i > 1 ? u[AIX(c, 1, i - 1, j)] : 0) + dI[1];
+            U = w[0] * t[0] + w[1] * t[1];
+            if (TM) {
+                REAL e = w[0] * v[4] + w[1] * v[5];
+                U += (c->a[AIX(c, 1, i, j)] - e) / T;
+            }
+            u[AIX(c, 1, i, j)] = U;
+            FN(tsoftmax)(v + 6, 3, T, w);
+            for (int st = 0; st < 3; ++st) t[st] = (j > 1 ? u[AIX(c, st, i, j - 1)] : 0) + dD[st];
+            U = w[0] * t[0] + w[1] * t[1] + w[2] * t[2];
+            if (TM) {
+                REAL e = w[0] * v[6] + w[1] * v[7] + w[2] * v[8];
+                U += (c->a[AIX(c, 2, i, j)] - e) / T;
+            }
+            u[AIX(c, 2, i, j)] = U;
+        }
+    }
+    for (int i = 1; i <= c->L1; ++i)
+        for (int j = 1; j <= c->L2; ++j) be[AIX(c, 0, i, j)] = FN(end_weight)(c->a[AIX(c, 0, i, j)], S, T);
+    REAL it2 = (REAL)1 / (T * T);
+    NW_DIAGS(c, k, i, j) {
+        int dg = i > 1 && j > 1;
+        size_t oM = AIX(c, 0, i, j), oI = AIX(c, 1, i, j), oD = AIX(c, 2, i, j);
+        FN(sv_cands)(c, c->a, i, j, v);
+        REAL bM = be[oM];
+        REAL b0 = FN(end_weight)(c->a[oM], S, T);
+        REAL WM = wt[oM] + b0 * (u[oM] - dSdt) / T;
+        if (TM && c->a[oM] > (REAL)NEG_BIG) WM -= b0 * (c->a[oM] - S) / (T * T);
+        FN(tsoftmax)(v, 4, T, w);
+        for (int st = 0; st < 3; ++st) t[st] = dg ? u[AIX(c, st, i - 1, j - 1)] : 0;
+        t[3] = 0;
+        REAL e = w[0] * t[0] + w[1] * t[1] + w[2] * t[2] + w[3] * t[3];
+        for (int q = 0; q < 4; ++q) dw[q] = w[q] * (t[q] - e) / T;
+        if (TM) {
+            REAL ev = w[0] * v[0] + w[1] * v[1] + w[2] * v[2] + w[3] * v[3];
+            for (int q = 0; q < 4; ++q) dw[q] += w[q] * (ev - v[q]) * it2;
+        }
+        dP[(size_t)(i - 1) * c->ld + (j - 1)] += WM;
+        if (dg)
+            for (int st = 0; st < 3; ++st) {
+                be[AIX(c, st, i - 1, j - 1)] += bM * w[st];
+                wt[AIX(c, st, i - 1, j - 1)] += WM * w[st] + bM * dw[st];
+            }
+        REAL bI = be[oI], WI = wt[oI];
+        if (i > 1) {
+            FN(tsoftmax)(v + 4, 2, T, w);
+            t[0] = u[AIX(c, 0, i - 1, j)] + dI[0];
+            t[1] = u[AIX(c, 1, i - 1, j)] + dI[1];
+            e = w[0] * t[0] + w[1] * t[1];
+            dw[0] = w[0] * (t[0] - e) / T;
+            dw[1] = w[1] * (t[1] - e) / T;
+            if (TM) {
+                REAL ev = w[0] * v[4] + w[1] * v[5];
+                dw[0] += w[0] * (ev - v[4]) * it2;
+                dw[1] += w[1] * (ev - v[5]) * it2;
+            }
+            for (int st = 0; st < 2; ++st) {
+                be[AIX(c, st, i - 1, j)] += bI * w[st];
+                wt[AIX(c, st, i - 1, j)] += WI * w[st] + bI * dw[st];
+            }
+        }
+        REAL bD = be[oD], WD = wt[oD];
+        if (j > 1) {
+            FN(tsoftmax)(v + 6, 3, T, w);
+            for (int st = 0; st < 3; ++st) t[st] = u[AIX(c, st, i, j - 1)] + dD[st];
+            e = w[0] * t[0] + w[1] * t[1] + w[2] * t[2];
+            for (int q = 0; q < 3; ++q) dw[q] = w[q] * (t[q] - e) / T;
+            if (TM) {
+                REAL ev = w[0] * v[6] + w[1] * v[7] + w[2] * v[8];
+                for (int q = 0; q < 3; ++q) dw[q] += w[q] * (ev - v[6 + q]) * it2;
+            }
+            for (int st = 0; st < 3; ++st) {
+                be[AIX(c, st, i, j - 1)] += bD * w[st];
+                wt[AIX(c, st, i, j - 1)] += WD * w[st] + bD * dw[st];
+            }
+        }
+    }
+}
+
 /* ---- batched entry points (padded [B, L1max, L2max] layout) ------------ */
 
 static int FN(pair_len)(const int *lengths, int b, int which, int dflt) {
@@ -1486,6 +1826,62 @@ int FN(oracle_nw_affine_param_grad)(const REAL *scores, const int *lengths, int 
     return 0;
 }
 
+/* Saigo-Vert: lin = 0 affine (go, ge), 1 linear (go = ge = gap; grads in
+ * gopen and gT, gext set to 0). */
+int FN(oracle_sv_forward)(const REAL *scores, const int *lengths, int B, int L1m, int L2m, REAL go,
+                          REAL ge, REAL T, int lin, REAL *value, REAL *map, REAL *gopen,
+                          REAL *gext, REAL *gT) {
+    size_t slab = (size_t)L1m * L2m, plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 6 * plane);
+    if (!a) return -1;
+    for (int b = 0; b < B; ++b) {
+        NWA_PAIR();
+        REAL S = FN(sv_forward)(&c);
+        REAL g[3];
+        FN(sv_adjoint)(&c, S, a + 3 * plane, map + b * slab, L1m, lin, g);
+        value[b] = S;
+        if (gopen) gopen[b] = g[0];
+        if (gext) gext[b] = g[1];
+        if (gT) gT[b] = g[2];
+    }
+    free(a);
+    return 0;
+}
+
+int FN(oracle_sv_hvp)(const REAL *scores, const REAL *V, const int *lengths, int B, int L1m,
+                      int L2m, REAL go, REAL ge, REAL T, REAL *out) {
+    size_t slab = (size_t)L1m * L2m, plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 12 * plane);
+    if (!a) return -1;
+    for (int b = 0; b < B; ++b) {
+        NWA_PAIR();
+        REAL S = FN(sv_forward)(&c);
+        FN(sv_hvp)(&c, S, V + b * slab, a + 3 * plane, a + 6 * plane, a + 9 * plane, out + b * slab, L1m);
+    }
+    free(a);
+    return 0;
+}
+
+/* pt: 0 = gap_open, 1 = gap_ext, 2 = temperature, 3 = linear gap. */
+int FN(oracle_sv_param_grad)(const REAL *scores, const int *lengths, int B, int L1m, int L2m,
+                             REAL go, REAL ge, REAL T, int lin, int pt, REAL *out) {
+    size_t slab = (size_t)L1m * L2m, plane = (size_t)(L1m + 1) * (L2m + 1);
+    REAL *a = (REAL *)malloc(sizeof(REAL) * 15 * plane + sizeof(REAL) * slab);
+    if (!a) return -1;
+    REAL *post = a + 15 * plane;
+    for (int b = 0; b < B; ++b) {
+        NWA_PAIR();
+        REAL S = FN(sv_forward)(&c);
+        REAL g[3];
+        FN(sv_adjoint)(&c, S, a + 12 * plane, post, L1m, lin, g);
+        REAL dS = pt == 2 ? g[2] : (pt == 1 ? g[1] : g[0]);
+        FN(sv_param)(&c, S, dS, pt, a + 3 * plane, a + 6 * plane, a + 9 * plane, out + b * slab, L1m);
+    }
+    free(a);
+    return 0;
+}
+
+#undef SV_LIVE
 #undef NWA_PAIR
 #undef NWA_TH
 #undef NW_DIAGS

@@ -146,6 +146,26 @@ def load() -> ctypes.CDLL:
     lib.swb_nw_affine_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, f, vp, vp, vp, sz, vp]
     lib.swb_nw_affine_param_jacobian.restype = i
     lib.swb_nw_affine_param_jacobian.argtypes = [vp, vp, i, i, i, f, f, f, i, vp, vp, sz, vp]
+    lib.swb_sv_affine_workspace_bytes.restype = sz
+    lib.swb_sv_affine_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sv_affine_forward.restype = i
+    lib.swb_sv_affine_forward.argtypes = [vp, vp, i, i, i, f, f, f, vp, vp, vp, vp, vp, vp, sz,
+                                          vp, ctypes.POINTER(Options)]
+    lib.swb_sv_affine_value_workspace_bytes.restype = sz
+    lib.swb_sv_affine_value_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sv_affine_value.restype = i
+    lib.swb_sv_affine_value.argtypes = [vp, vp, i, i, i, f, f, f, vp, vp, sz, vp]
+    lib.swb_sv_affine_ragged.restype = i
+    lib.swb_sv_affine_ragged.argtypes = [vp, vp, vp, f, f, f, vp, vp, vp, vp, vp, vp, sz, vp,
+                                         ctypes.POINTER(Options)]
+    lib.swb_sv_affine_ragged_value.restype = i
+    lib.swb_sv_affine_ragged_value.argtypes = [vp, vp, vp, f, f, f, vp, vp, sz, vp]
+    lib.swb_sv_affine_aux_workspace_bytes.restype = sz
+    lib.swb_sv_affine_aux_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sv_affine_hvp.restype = i
+    lib.swb_sv_affine_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, f, vp, vp, vp, sz, vp]
+    lib.swb_sv_affine_param_jacobian.restype = i
+    lib.swb_sv_affine_param_jacobian.argtypes = [vp, vp, i, i, i, f, f, f, i, vp, vp, sz, vp]
     lib.swb_mufu_probe.restype = i
     lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()

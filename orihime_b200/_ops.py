@@ -59,6 +59,23 @@ SCHEMAS = {
     "nw_affine_marginals_grad_gap_open": "nw_affine_marginals_grad_gap_open(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
     "nw_affine_marginals_grad_gap_ext": "nw_affine_marginals_grad_gap_ext(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
     "nw_affine_marginals_grad_temp": "nw_affine_marginals_grad_temp(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    # src/sv_linear/registry.cpp:28-34
+    "sv_linear_forward": "sv_linear_forward(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor[]",
+    "sv_linear_forward_t": "sv_linear_forward_t(Tensor scores, Tensor gap, Tensor temp, Tensor lengths) -> Tensor[]",
+    "sv_linear_value_grad_params": "sv_linear_value_grad_params(Tensor scores, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor)",
+    "sv_linear_marginals_backward": "sv_linear_marginals_backward(Tensor scores, Tensor grad_marginals, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
+    "sv_linear_marginals_hvp": "sv_linear_marginals_hvp(Tensor scores, Tensor v, float gap, float temp, Tensor? lengths) -> Tensor",
+    "sv_linear_marginals_grad_gap": "sv_linear_marginals_grad_gap(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
+    "sv_linear_marginals_grad_temp": "sv_linear_marginals_grad_temp(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
+    # src/sv_affine/registry.cpp:37-44
+    "sv_affine_forward": "sv_affine_forward(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor[]",
+    "sv_affine_forward_t": "sv_affine_forward_t(Tensor scores, Tensor gap_open, Tensor gap_ext, Tensor temp, Tensor lengths) -> Tensor[]",
+    "sv_affine_value_grad_params": "sv_affine_value_grad_params(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
+    "sv_affine_marginals_backward": "sv_affine_marginals_backward(Tensor scores, Tensor grad_marginals, float gap_open, float gap_ext, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
+    "sv_affine_marginals_hvp": "sv_affine_marginals_hvp(Tensor scores, Tensor v, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "sv_affine_marginals_grad_gap_open": "sv_affine_marginals_grad_gap_open(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "sv_affine_marginals_grad_gap_ext": "sv_affine_marginals_grad_gap_ext(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
+    "sv_affine_marginals_grad_temp": "sv_affine_marginals_grad_temp(Tensor scores, float gap_open, float gap_ext, float temp, Tensor? lengths) -> Tensor",
     # src/nw/registry.cpp:48-51
     "nw_marginals_backward": "nw_marginals_backward(Tensor scores, Tensor grad_marginals, float gap, float temp, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
     "nw_marginals_hvp": "nw_marginals_hvp(Tensor scores, Tensor v, float gap, float temp, Tensor? lengths) -> Tensor",
@@ -187,7 +204,8 @@ def run_affine(scores, lengths, go, ge, temp, options=None, family="sw_affine"):
     g_T = torch.empty(B, dtype=torch.float32, device=dev)
     if B == 0:
         return value, amap, g_open, g_ext, g_T
-    name = "swb_nw_affine_forward" if family == "nw_affine" else "swb_sw_affine_forward"
+    name = {"sw_affine": "swb_sw_affine_forward", "nw_affine": "swb_nw_affine_forward",
+            "sv_affine": "swb_sv_affine_forward"}[family]
     nbytes = getattr(_LIB, name.replace("_forward", "_workspace_bytes"))(B, L1, L2)
     ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
     with torch.cuda.device(dev):
@@ -249,8 +267,10 @@ def run_value(fam, scores, lengths, params):
     value = torch.empty(B, dtype=torch.float32, device=dev)
     if B == 0:
         return value
+    if fam == "sv_linear":   # the Saigo-Vert affine model with gap_open = gap_ext = gap
+        fam, params = "sv_affine", (params[0], params[0], params[1])
     name = {"sw": "swb_sw_value", "sw_affine": "swb_sw_affine_value", "nw": "swb_nw_value",
-            "nw_affine": "swb_nw_affine_value"}[fam]
+            "nw_affine": "swb_nw_affine_value", "sv_affine": "swb_sv_affine_value"}[fam]
     nbytes = int(getattr(_LIB, name + "_workspace_bytes")(B, L1, L2))
     ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     with torch.cuda.device(dev):
@@ -414,6 +434,8 @@ _AUX = {  # family -> (workspace bytes, HVP, parameter Jacobian) entry points
     "nw": ("swb_nw_aux_workspace_bytes", "swb_nw_hvp", "swb_nw_param_jacobian"),
     "nw_affine": ("swb_nw_affine_aux_workspace_bytes", "swb_nw_affine_hvp",
                   "swb_nw_affine_param_jacobian"),
+    "sv_affine": ("swb_sv_affine_aux_workspace_bytes", "swb_sv_affine_hvp",
+                  "swb_sv_affine_param_jacobian"),
 }
 
 
@@ -513,6 +535,10 @@ def marginals_backward_per_pair(fam, scores, grad_marginals, params, lengths):
                            f"{grad_marginals.device} vs {scores.device}")
     g = grad_marginals.contiguous().to(torch.float32)
     ln = _prep(scores, lengths, fam)
+    if fam == "sv_linear":   # via the affine model: tangent of dS/dgap = open + ext
+        gap, temp = params
+        out, gt = run_hvp("sv_affine", scores, g, ln, (gap, gap, temp), want_grads=True)
+        return out, torch.stack([gt[:, 0] + gt[:, 1], gt[:, 2], torch.zeros_like(gt[:, 0]), gt[:, 3]], 1)
     return run_hvp(fam, scores, g, ln, params, want_grads=True)
 
 
@@ -606,7 +632,127 @@ def nw_affine_marginals_backward(scores, grad_marginals, gap_open, gap_ext, temp
     return out, tot[0:1].clone(), tot[1:2].clone(), tot[2:3].clone()
 
 
+# ---- Saigo-Vert (local; affine, and linear as affine with one gap) -------------
+# src/sv_affine/torch_cuda.cpp and src/sv_linear/torch_cuda.cpp bodies; the
+# linear model runs the affine kernels with gap_open = gap_ext = gap and
+# reports dS/dgap = dS/dgap_open + dS/dgap_ext.
+
+def sv_affine_forward(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::sv_affine_forward -> [value [B], marginals [B, L1, L2]]."""
+    ln = _prep(scores, lengths, "sv_affine")
+    v, m, *_ = run_affine(scores, ln, gap_open, gap_ext, temp, family="sv_affine")
+    return [v, m]
+
+
+def sv_affine_forward_t(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::sv_affine_forward_t (tensor parameters)."""
+    check_input_cuda(scores, "scores")
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    go = _scalar_param(gap_open, "gap_open")
+    ge = _scalar_param(gap_ext, "gap_ext")
+    T = _scalar_param(temp, "temperature")
+    B, L1, L2 = check_shape(scores, "sv_affine")
+    ln = resolve_lengths(lengths, B, L1, L2, scores.device)
+    v, m, *_ = run_affine(scores, ln, go, ge, T, family="sv_affine")
+    return [v, m]
+
+
+def sv_affine_value_grad_params(scores, gap_open, gap_ext, temp, lengths):
+    """orihime::sv_affine_value_grad_params -> (dS/dgo, dS/dge, dS/dT), each [B]."""
+    ln = _prep(scores, lengths, "sv_affine")
+    _, _, go, ge, gT = run_affine(scores, ln, gap_open, gap_ext, temp, family="sv_affine")
+    return go, ge, gT
+
+
+def sv_affine_marginals_hvp(scores, v, gap_open, gap_ext, temp, lengths):
+    check_input_cuda(scores, "scores")
+    _check_like(scores, v, "tangent", "scores and tangent must have same shape")
+    ln = _prep(scores, lengths, "sv_affine")
+    return run_hvp("sv_affine", scores, v, ln, (gap_open, gap_ext, temp))[0]
+
+
+def _sv_affine_param(which):
+    def op(scores, gap_open, gap_ext, temp, lengths):
+        ln = _prep(scores, lengths, "sv_affine")
+        return run_param_jacobian("sv_affine", scores, ln, (gap_open, gap_ext, temp), which)
+    op.__doc__ = f"orihime::sv_affine_marginals_grad_* param {which}"
+    return op
+
+
+def sv_affine_marginals_backward(scores, grad_marginals, gap_open, gap_ext, temp, lengths):
+    out, gt = marginals_backward_per_pair("sv_affine", scores, grad_marginals,
+                                          (gap_open, gap_ext, temp), lengths)
+    tot = gt[:, :3].sum(0)
+    return out, tot[0:1].clone(), tot[1:2].clone(), tot[2:3].clone()
+
+
+def sv_linear_forward(scores, gap, temp, lengths):
+    """orihime::sv_linear_forward -> [value [B], marginals [B, L1, L2]]."""
+    ln = _prep(scores, lengths, "sv_linear")
+    v, m, *_ = run_affine(scores, ln, gap, gap, temp, family="sv_affine")
+    return [v, m]
+
+
+def sv_linear_forward_t(scores, gap, temp, lengths):
+    check_input_cuda(scores, "scores")
+    if scores.dim() != 3:
+        raise RuntimeError("scores must be 3D (B, L1, L2)")
+    g = _scalar_param(gap, "gap")
+    T = _scalar_param(temp, "temperature")
+    B, L1, L2 = check_shape(scores, "sv_linear")
+    ln = resolve_lengths(lengths, B, L1, L2, scores.device)
+    v, m, *_ = run_affine(scores, ln, g, g, T, family="sv_affine")
+    return [v, m]
+
+
+def sv_linear_value_grad_params(scores, gap, temp, lengths):
+    """orihime::sv_linear_value_grad_params -> (dS/dgap, dS/dT), each [B]."""
+    ln = _prep(scores, lengths, "sv_linear")
+    _, _, go, ge, gT = run_affine(scores, ln, gap, gap, temp, family="sv_affine")
+    return go + ge, gT
+
+
+def sv_linear_marginals_hvp(scores, v, gap, temp, lengths):
+    check_input_cuda(scores, "scores")
+    _check_like(scores, v, "tangent", "scores and tangent must have same shape")
+    ln = _prep(scores, lengths, "sv_linear")
+    return run_hvp("sv_affine", scores, v, ln, (gap, gap, temp))[0]
+
+
+def _sv_linear_param(which):
+    def op(scores, gap, temp, lengths):
+        ln = _prep(scores, lengths, "sv_linear")
+        if which == 1:
+            return run_param_jacobian("sv_affine", scores, ln, (gap, gap, temp), 2)
+        return (run_param_jacobian("sv_affine", scores, ln, (gap, gap, temp), 0) +
+                run_param_jacobian("sv_affine", scores, ln, (gap, gap, temp), 1))
+    op.__doc__ = f"orihime::sv_linear_marginals_grad_* param {which} (gap = open + ext directions)"
+    return op
+
+
+def sv_linear_marginals_backward(scores, grad_marginals, gap, temp, lengths):
+    out, gt = marginals_backward_per_pair("sv_linear", scores, grad_marginals, (gap, temp), lengths)
+    tot = gt[:, :2].sum(0)
+    return out, tot[0:1].clone(), tot[1:2].clone()
+
+
 IMPLS = {
+    "sv_affine_forward": sv_affine_forward,
+    "sv_affine_forward_t": sv_affine_forward_t,
+    "sv_affine_value_grad_params": sv_affine_value_grad_params,
+    "sv_affine_marginals_hvp": sv_affine_marginals_hvp,
+    "sv_affine_marginals_grad_gap_open": _sv_affine_param(0),
+    "sv_affine_marginals_grad_gap_ext": _sv_affine_param(1),
+    "sv_affine_marginals_grad_temp": _sv_affine_param(2),
+    "sv_affine_marginals_backward": sv_affine_marginals_backward,
+    "sv_linear_forward": sv_linear_forward,
+    "sv_linear_forward_t": sv_linear_forward_t,
+    "sv_linear_value_grad_params": sv_linear_value_grad_params,
+    "sv_linear_marginals_hvp": sv_linear_marginals_hvp,
+    "sv_linear_marginals_grad_gap": _sv_linear_param(0),
+    "sv_linear_marginals_grad_temp": _sv_linear_param(1),
+    "sv_linear_marginals_backward": sv_linear_marginals_backward,
     "nw_affine_marginals_hvp": nw_affine_marginals_hvp,
     "nw_affine_marginals_grad_gap_open": _nw_affine_param(0),
     "nw_affine_marginals_grad_gap_ext": _nw_affine_param(1),
@@ -721,7 +867,11 @@ for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True
                         ("sw_affine_forward_t", "sw_affine", True),
                         ("nw_forward", "nw", False), ("nw_forward_t", "nw", True),
                         ("nw_affine_forward", "nw_affine", False),
-                        ("nw_affine_forward_t", "nw_affine", True)):
+                        ("nw_affine_forward_t", "nw_affine", True),
+                        ("sv_affine_forward", "sv_affine", False),
+                        ("sv_affine_forward_t", "sv_affine", True),
+                        ("sv_linear_forward", "sv_linear", False),
+                        ("sv_linear_forward_t", "sv_linear", True)):
     _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
 
 
@@ -730,7 +880,7 @@ for _name, _fam, _t in (("sw_forward", "sw", False), ("sw_forward_t", "sw", True
 # src/sw_affine/registry.cpp:27-32, src/nw/registry.cpp:34-39,
 # src/nw_affine/registry.cpp:35-40)
 # ---------------------------------------------------------------------------
-# The reference keeps 24 older schemas beside the namespaced ones; its Python
+# The reference keeps 36 older schemas beside the namespaced ones; its Python
 # package no longer calls them.  Each is one of the namespaced op bodies under
 # another name (src/sw*/torch_cuda.cpp:803-830, :917-946,
 # src/nw*/torch_cuda.cpp:795-821, :763-786).  They are defined
@@ -784,6 +934,31 @@ LEGACY_SCHEMAS = {
     "soft_nw_affine_backward_full": "soft_nw_affine_backward_full(Tensor scores, Tensor grad_alignment, "
                                     "float gap_open, float gap_ext, float temperature, Tensor? lengths) "
                                     "-> (Tensor, Tensor, Tensor, Tensor)",
+    # src/sv_linear/registry.cpp:20-25, src/sv_affine/registry.cpp:29-34
+    "soft_sv_linear": "soft_sv_linear(Tensor scores, Tensor gap, Tensor temperature, Tensor lengths) -> Tensor[]",
+    "soft_sv_linear_float": "soft_sv_linear_float(Tensor scores, float gap, float temperature, "
+                            "Tensor? lengths) -> Tensor[]",
+    "soft_sv_linear_with_grads": "soft_sv_linear_with_grads(Tensor scores, float gap, float temperature, "
+                                 "Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
+    "soft_sv_linear_hvp": "soft_sv_linear_hvp(Tensor scores, Tensor tangent, float gap, float temperature, "
+                          "Tensor? lengths) -> Tensor",
+    "soft_sv_linear_param_jacobian": "soft_sv_linear_param_jacobian(Tensor scores, int param_type, float gap, "
+                                     "float temperature, Tensor? lengths) -> Tensor",
+    "soft_sv_linear_backward_full": "soft_sv_linear_backward_full(Tensor scores, Tensor grad_alignment, "
+                                    "float gap, float temperature, Tensor? lengths) -> (Tensor, Tensor, Tensor)",
+    "soft_sv_affine": "soft_sv_affine(Tensor scores, Tensor gap_open, Tensor gap_ext, Tensor temperature, "
+                      "Tensor lengths) -> Tensor[]",
+    "soft_sv_affine_float": "soft_sv_affine_float(Tensor scores, float gap_open, float gap_ext, "
+                            "float temperature, Tensor? lengths) -> Tensor[]",
+    "soft_sv_affine_with_grads": "soft_sv_affine_with_grads(Tensor scores, float gap_open, float gap_ext, "
+                                 "float temperature, Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor, Tensor)",
+    "soft_sv_affine_hvp": "soft_sv_affine_hvp(Tensor scores, Tensor tangent, float gap_open, float gap_ext, "
+                          "float temperature, Tensor? lengths) -> Tensor",
+    "soft_sv_affine_param_jacobian": "soft_sv_affine_param_jacobian(Tensor scores, int param_type, "
+                                     "float gap_open, float gap_ext, float temperature, Tensor? lengths) -> Tensor",
+    "soft_sv_affine_backward_full": "soft_sv_affine_backward_full(Tensor scores, Tensor grad_alignment, "
+                                    "float gap_open, float gap_ext, float temperature, Tensor? lengths) "
+                                    "-> (Tensor, Tensor, Tensor, Tensor)",
 }
 LEGACY_DEFINED_HERE = []
 if DEFINED_HERE:
@@ -801,6 +976,23 @@ def _legacy_with_grads_linear(scores, gap, temperature, lengths):
 def _legacy_with_grads_nw(scores, gap, temperature, lengths):
     ln = _prep(scores, lengths, "nw")
     return tuple(run_linear(scores, ln, gap, temperature, family="nw"))
+
+
+def _legacy_with_grads_sv_affine(scores, gap_open, gap_ext, temperature, lengths):
+    ln = _prep(scores, lengths, "sv_affine")
+    return tuple(run_affine(scores, ln, gap_open, gap_ext, temperature, family="sv_affine"))
+
+
+def _legacy_with_grads_sv_linear(scores, gap, temperature, lengths):
+    ln = _prep(scores, lengths, "sv_linear")
+    v, m, go, ge, gT = run_affine(scores, ln, gap, gap, temperature, family="sv_affine")
+    return v, m, go + ge, gT
+
+
+def _legacy_sv_linear_jacobian(scores, param_type, gap, temperature, lengths):
+    if not 0 <= int(param_type) < 2:
+        raise RuntimeError("param_type must be 0 or 1")
+    return _sv_linear_param(int(param_type))(scores, gap, temperature, lengths)
 
 
 def _legacy_with_grads_nw_affine(scores, gap_open, gap_ext, temperature, lengths):
@@ -851,6 +1043,18 @@ LEGACY_IMPLS = {
     "soft_nw_affine_hvp": nw_affine_marginals_hvp,
     "soft_nw_affine_param_jacobian": _legacy_jacobian("nw_affine", 3),
     "soft_nw_affine_backward_full": nw_affine_marginals_backward,
+    "soft_sv_linear_float": sv_linear_forward,
+    "soft_sv_linear": sv_linear_forward_t,
+    "soft_sv_linear_with_grads": _legacy_with_grads_sv_linear,
+    "soft_sv_linear_hvp": sv_linear_marginals_hvp,
+    "soft_sv_linear_param_jacobian": _legacy_sv_linear_jacobian,
+    "soft_sv_linear_backward_full": sv_linear_marginals_backward,
+    "soft_sv_affine_float": sv_affine_forward,
+    "soft_sv_affine": sv_affine_forward_t,
+    "soft_sv_affine_with_grads": _legacy_with_grads_sv_affine,
+    "soft_sv_affine_hvp": sv_affine_marginals_hvp,
+    "soft_sv_affine_param_jacobian": _legacy_jacobian("sv_affine", 3),
+    "soft_sv_affine_backward_full": sv_affine_marginals_backward,
 }
 for _name in LEGACY_DEFINED_HERE:
     _IMPL_LIB.impl(_name, LEGACY_IMPLS[_name], "CUDA")
@@ -858,7 +1062,9 @@ for _name, _fam, _t in (("soft_sw_float", "sw", False), ("soft_sw", "sw", True),
                         ("soft_sw_affine_float", "sw_affine", False), ("soft_sw_affine", "sw_affine", True),
                         ("soft_nw_float", "nw", False), ("soft_nw", "nw", True),
                         ("soft_nw_affine_float", "nw_affine", False),
-                        ("soft_nw_affine", "nw_affine", True)):
+                        ("soft_nw_affine", "nw_affine", True),
+                        ("soft_sv_linear_float", "sv_linear", False), ("soft_sv_linear", "sv_linear", True),
+                        ("soft_sv_affine_float", "sv_affine", False), ("soft_sv_affine", "sv_affine", True)):
     if _name in LEGACY_DEFINED_HERE:   # differentiable like the reference (AutogradCUDA)
         _IMPL_LIB.impl(_name, _autograd_forward(_fam, _t), "AutogradCUDA")
 
@@ -875,6 +1081,9 @@ OWN_SCHEMAS = {
                        "Tensor? lengths) -> Tensor",
     "nw_value": "nw_value(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
     "nw_affine_value": "nw_affine_value(Tensor scores, float gap_open, float gap_ext, float temp, "
+                       "Tensor? lengths) -> Tensor",
+    "sv_linear_value": "sv_linear_value(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
+    "sv_affine_value": "sv_affine_value(Tensor scores, float gap_open, float gap_ext, float temp, "
                        "Tensor? lengths) -> Tensor",
 }
 _OWN_LIB = torch.library.Library("orihime_b200", "DEF")
@@ -905,7 +1114,19 @@ def _own_nw_affine_value(scores, gap_open, gap_ext, temp, lengths):
 
 
 _OWN_LIB.impl("nw_value", _own_nw_value, "CUDA")
+def _own_sv_linear_value(scores, gap, temp, lengths):
+    ln = _prep(scores, lengths, "sv_linear")
+    return run_value("sv_linear", scores, ln, (gap, temp))
+
+
+def _own_sv_affine_value(scores, gap_open, gap_ext, temp, lengths):
+    ln = _prep(scores, lengths, "sv_affine")
+    return run_value("sv_affine", scores, ln, (gap_open, gap_ext, temp))
+
+
 _OWN_LIB.impl("nw_affine_value", _own_nw_affine_value, "CUDA")
+_OWN_LIB.impl("sv_linear_value", _own_sv_linear_value, "CUDA")
+_OWN_LIB.impl("sv_affine_value", _own_sv_affine_value, "CUDA")
 
 # Meta shapes, FP32 autocast and vmap rules for the ops defined here (when the
 # reference extension defined them, its own Python package registers these).

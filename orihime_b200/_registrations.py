@@ -31,11 +31,11 @@ import torch
 from . import _ops
 
 _BATCH_ARGS = frozenset({"scores", "v", "grad_marginals", "lengths"})
-_NPARAMS = {"sw": 2, "sw_affine": 3, "nw": 2, "nw_affine": 3}
+_NPARAMS = {"sw": 2, "sw_affine": 3, "nw": 2, "nw_affine": 3, "sv_linear": 2, "sv_affine": 3}
 
 
 def _fam(name: str) -> str:
-    for f in ("sw_affine", "nw_affine", "nw"):
+    for f in ("sw_affine", "nw_affine", "sv_affine", "sv_linear", "nw"):
         if name.startswith(f):
             return f
     return "sw"

@@ -36,7 +36,7 @@ constexpr size_t kAlign = 256;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
-template <int NS, bool G = false> constexpr int np() { return swb::push_channels<NS, G>(); }
+template <int NS, int G = 0> constexpr int np() { return swb::push_channels<NS, G>(); }
 template <int NS, int R> constexpr int ckrs() { return swb::Dims<NS, R>::CKRS; }
 template <int NS, int R> constexpr int ne() { return swb::Dims<NS, R>::NE; }
 
@@ -73,7 +73,7 @@ Layout layout_sizes(long long B, size_t slots, size_t edge_floats, size_t bp_flo
 int chunks_for(long long L1) { return (int)((L1 + 31 + swb::C_STEPS - 1) / swb::C_STEPS); }
 
 // Padded batch: every pair gets the slices of a Lmax1 x Lmax2 pair.
-template <int NS, int R, bool G = false>
+template <int NS, int R, int G = 0>
 Layout layout_for(long long B, long long L1m, long long L2m) {
   int nb = (int)((L2m + 32 * R - 1) / (32 * R));
   if (nb < 1) nb = 1;
@@ -103,7 +103,7 @@ size_t plan_bytes_for(long long B, long long ntasks) {
 // Occupancy of each kernel instantiation on one device, computed once.
 struct DevInfo {
   int sms = 0;
-  int occ[2][4][2] = {};   // [kernel fwd/bwd][model: linear, affine, global linear, global affine][R == 4?]
+  int occ[2][5][2] = {};   // [kernel fwd/bwd][model_index][R == 4?]
   bool ready = false;
 };
 DevInfo g_dev[64];
@@ -112,9 +112,12 @@ std::mutex g_mu;
 template <int NS, int R>
 size_t bwd_smem() { return (size_t)kWarpsBwd * swb::bwd_smem_floats<NS, R>() * sizeof(float); }
 
-template <int NS, bool G> constexpr int model_index() { return NS == 3 ? (G ? 3 : 1) : (G ? 2 : 0); }
+// occupancy slots: linear, affine, global linear, global affine, Saigo-Vert
+template <int NS, int G> constexpr int model_index() {
+  return NS == 3 ? (G == 1 ? 3 : (G == 2 ? 4 : 1)) : (G == 1 ? 2 : 0);
+}
 
-template <int NS, int R, bool G = false>
+template <int NS, int R, int G = 0>
 cudaError_t setup_pair(DevInfo& d) {
   constexpr int m = model_index<NS, G>();
   cudaError_t e = cudaFuncSetAttribute(swb::bwd_kernel<NS, R, kWarpsBwd, G>,
@@ -138,8 +141,8 @@ int dev_info(DevInfo** out) {
     if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       return SWB_ERR_CUDA;
     if (setup_pair<1, 2>(d) || setup_pair<1, 4>(d) || setup_pair<3, 2>(d) || setup_pair<3, 4>(d) ||
-        setup_pair<1, 2, true>(d) || setup_pair<1, 4, true>(d) || setup_pair<3, 2, true>(d) ||
-        setup_pair<3, 4, true>(d))
+        setup_pair<1, 2, 1>(d) || setup_pair<1, 4, 1>(d) || setup_pair<3, 2, 1>(d) ||
+        setup_pair<3, 4, 1>(d) || setup_pair<3, 2, 2>(d) || setup_pair<3, 4, 2>(d))
       return SWB_ERR_CUDA;
     d.ready = true;
   }
@@ -165,7 +168,7 @@ int static_scratch(void** out) {
 }
 
 // Common launch: per-call resets, then the forward and adjoint kernels.
-template <int NS, int R, bool G = false>
+template <int NS, int R, int G = 0>
 int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool clear_map, void* ws,
            size_t ws_bytes, void* stream_v, const swb_options* opt, bool value_only = false) {
   if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
@@ -223,7 +226,7 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   return SWB_OK;
 }
 
-template <int NS, int R, bool G = false>
+template <int NS, int R, int G = 0>
 int launch_padded_r(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
                     float ge, float T, float* value, float* map, float* g_open, float* g_ext,
                     float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
@@ -243,7 +246,7 @@ int launch_padded_r(const float* scores, const int* lengths, int B, int L1m, int
   return launch<NS, R, G>(a, l, (long long)B * l.nb, map_elems, true, ws, ws_bytes, stream, opt);
 }
 
-template <int NS, bool G = false>
+template <int NS, int G = 0>
 int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
                   float ge, float T, float* value, float* map, float* g_open, float* g_ext,
                   float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
@@ -258,7 +261,7 @@ int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L
 }
 
 // Padded value-only batch: the forward wavefront, no checkpoints, no adjoint.
-template <int NS, bool G = false>
+template <int NS, int G = 0>
 Layout value_layout(long long B, long long L1m, long long L2m) {
   constexpr int R = kDefaultR;
   int nb = (int)((L2m + 32 * R - 1) / (32 * R));
@@ -271,7 +274,7 @@ Layout value_layout(long long B, long long L1m, long long L2m) {
   return l;
 }
 
-template <int NS, bool G = false>
+template <int NS, int G = 0>
 int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
                  float ge, float T, float* value, void* ws, size_t ws_bytes, void* stream) {
   if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
@@ -289,15 +292,16 @@ int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2
                                   nullptr, true);
 }
 
-template <int NS, bool G = false>
+template <int NS, int G = 0>
 int launch_ragged(const float* scores, const void* host_plan, const void* dev_plan, float go,
                   float ge, float T, float* value, float* map, float* g_open, float* g_ext,
                   float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt,
                   bool value_only = false) {
   if (!host_plan || !dev_plan) return SWB_ERR_ARG;
   const long long* h = static_cast<const long long*>(host_plan);
-  if (h[HW_MAGIC] != kPlanMagic || (h[HW_FAMILY] & 0xff) != (G ? (NS == 3 ? 4 : 2) : NS))
-    return SWB_ERR_ARG;
+  // plan families: 1 linear, 3 affine, 2 global linear, 4 global affine, 5 Saigo-Vert
+  constexpr int fam = G == 2 ? 5 : (G == 1 ? (NS == 3 ? 4 : 2) : NS);
+  if (h[HW_MAGIC] != kPlanMagic || (h[HW_FAMILY] & 0xff) != fam) return SWB_ERR_ARG;
   const int r = (int)(h[HW_FAMILY] >> 8);
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   const long long B = h[HW_B], ntasks = h[HW_NTASKS];
@@ -347,7 +351,7 @@ struct XLayout {
   size_t sent_bytes, total;
 };
 
-template <int NS, bool G = false>
+template <int NS, int G = 0>
 XLayout xlayout(long long B, long long L1m, long long L2m) {
   XLayout l{};
   l.R = xpick_r(B, L2m);
@@ -376,9 +380,9 @@ struct XOcc {
   int f = 0, b = 0;
   bool ready = false;
 };
-XOcc g_xocc[64][4][2][4];   // [device][model: linear, affine, global linear, global affine][R == 4?][mode]
+XOcc g_xocc[64][5][2][4];   // [device][model_index][R == 4?][mode]
 
-template <int NS, int R, int MODE, bool G = false>
+template <int NS, int R, int MODE, int G = 0>
 int launch_xband_r(swb::XArgs a, cudaStream_t st) {
   DevInfo* d = nullptr;
   int rc = dev_info(&d);
@@ -408,7 +412,7 @@ int launch_xband_r(swb::XArgs a, cudaStream_t st) {
   return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
 }
 
-template <int NS, int MODE, bool G = false>
+template <int NS, int MODE, int G = 0>
 int launch_xband(const float* scores, const float* v, const int* lengths, int B, int L1m, int L2m,
                  float go, float ge, float T, float* out, float* gt, void* ws, size_t ws_bytes,
                  void* stream_v) {
@@ -499,13 +503,13 @@ int swb_sw_param_jacobian(const float* scores, const int* lengths, int B, int L1
 
 
 size_t swb_nw_affine_aux_workspace_bytes(int B, int L1max, int L2max) {
-  return B > 0 ? xlayout<3, true>(B, L1max, L2max).total : 0;
+  return B > 0 ? xlayout<3, 1>(B, L1max, L2max).total : 0;
 }
 
 int swb_nw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
                       int L2max, float gap_open, float gap_ext, float temp, float* out,
                       float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream) {
-  return launch_xband<3, swb::AUX_HVP, true>(scores, v, lengths, B, L1max, L2max, gap_open, gap_ext,
+  return launch_xband<3, swb::AUX_HVP, 1>(scores, v, lengths, B, L1max, L2max, gap_open, gap_ext,
                                              temp, out, grad_tangents, workspace, workspace_bytes,
                                              stream);
 }
@@ -514,15 +518,44 @@ int swb_nw_affine_param_jacobian(const float* scores, const int* lengths, int B,
                                  int L2max, float gap_open, float gap_ext, float temp, int param,
                                  float* out, void* workspace, size_t workspace_bytes, void* stream) {
   switch (param) {
-    case 0: return launch_xband<3, swb::AUX_P0, true>(scores, nullptr, lengths, B, L1max, L2max,
+    case 0: return launch_xband<3, swb::AUX_P0, 1>(scores, nullptr, lengths, B, L1max, L2max,
                                                       gap_open, gap_ext, temp, out, nullptr,
                                                       workspace, workspace_bytes, stream);
-    case 1: return launch_xband<3, swb::AUX_P1, true>(scores, nullptr, lengths, B, L1max, L2max,
+    case 1: return launch_xband<3, swb::AUX_P1, 1>(scores, nullptr, lengths, B, L1max, L2max,
                                                       gap_open, gap_ext, temp, out, nullptr,
                                                       workspace, workspace_bytes, stream);
-    case 2: return launch_xband<3, swb::AUX_PT, true>(scores, nullptr, lengths, B, L1max, L2max,
+    case 2: return launch_xband<3, swb::AUX_PT, 1>(scores, nullptr, lengths, B, L1max, L2max,
                                                       gap_open, gap_ext, temp, out, nullptr,
                                                       workspace, workspace_bytes, stream);
+    default: return SWB_ERR_ARG;
+  }
+}
+
+size_t swb_sv_affine_aux_workspace_bytes(int B, int L1max, int L2max) {
+  return B > 0 ? xlayout<3, 2>(B, L1max, L2max).total : 0;
+}
+
+int swb_sv_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
+                      int L2max, float gap_open, float gap_ext, float temp, float* out,
+                      float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_xband<3, swb::AUX_HVP, 2>(scores, v, lengths, B, L1max, L2max, gap_open, gap_ext,
+                                          temp, out, grad_tangents, workspace, workspace_bytes,
+                                          stream);
+}
+
+int swb_sv_affine_param_jacobian(const float* scores, const int* lengths, int B, int L1max,
+                                 int L2max, float gap_open, float gap_ext, float temp, int param,
+                                 float* out, void* workspace, size_t workspace_bytes, void* stream) {
+  switch (param) {
+    case 0: return launch_xband<3, swb::AUX_P0, 2>(scores, nullptr, lengths, B, L1max, L2max,
+                                                   gap_open, gap_ext, temp, out, nullptr, workspace,
+                                                   workspace_bytes, stream);
+    case 1: return launch_xband<3, swb::AUX_P1, 2>(scores, nullptr, lengths, B, L1max, L2max,
+                                                   gap_open, gap_ext, temp, out, nullptr, workspace,
+                                                   workspace_bytes, stream);
+    case 2: return launch_xband<3, swb::AUX_PT, 2>(scores, nullptr, lengths, B, L1max, L2max,
+                                                   gap_open, gap_ext, temp, out, nullptr, workspace,
+                                                   workspace_bytes, stream);
     default: return SWB_ERR_ARG;
   }
 }
@@ -534,7 +567,7 @@ size_t swb_nw_aux_workspace_bytes(int B, int L1max, int L2max) {
 int swb_nw_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max, int L2max,
                float gap, float temp, float* out, float* grad_tangents, void* workspace,
                size_t workspace_bytes, void* stream) {
-  return launch_xband<1, swb::AUX_HVP, true>(scores, v, lengths, B, L1max, L2max, gap, 0.f, temp,
+  return launch_xband<1, swb::AUX_HVP, 1>(scores, v, lengths, B, L1max, L2max, gap, 0.f, temp,
                                              out, grad_tangents, workspace, workspace_bytes, stream);
 }
 
@@ -542,10 +575,10 @@ int swb_nw_param_jacobian(const float* scores, const int* lengths, int B, int L1
                           float gap, float temp, int param, float* out, void* workspace,
                           size_t workspace_bytes, void* stream) {
   switch (param) {
-    case 0: return launch_xband<1, swb::AUX_P0, true>(scores, nullptr, lengths, B, L1max, L2max, gap,
+    case 0: return launch_xband<1, swb::AUX_P0, 1>(scores, nullptr, lengths, B, L1max, L2max, gap,
                                                       0.f, temp, out, nullptr, workspace,
                                                       workspace_bytes, stream);
-    case 1: return launch_xband<1, swb::AUX_PT, true>(scores, nullptr, lengths, B, L1max, L2max, gap,
+    case 1: return launch_xband<1, swb::AUX_PT, 1>(scores, nullptr, lengths, B, L1max, L2max, gap,
                                                       0.f, temp, out, nullptr, workspace,
                                                       workspace_bytes, stream);
     default: return SWB_ERR_ARG;
@@ -653,34 +686,34 @@ int swb_nw_forward(const float* scores, const int* lengths, int B, int L1max, in
                    float temp, float* value, float* map, float* grad_gap, float* grad_temp,
                    void* workspace, size_t workspace_bytes, void* stream,
                    const swb_options* opt) {
-  return launch_padded<1, true>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, map,
+  return launch_padded<1, 1>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, map,
                                 grad_gap, nullptr, grad_temp, workspace, workspace_bytes, stream,
                                 opt);
 }
 
 size_t swb_nw_affine_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;
-  return std::max(layout_for<3, 2, true>(B, L1max, L2max).total,
-                  layout_for<3, 4, true>(B, L1max, L2max).total);
+  return std::max(layout_for<3, 2, 1>(B, L1max, L2max).total,
+                  layout_for<3, 4, 1>(B, L1max, L2max).total);
 }
 
 int swb_nw_affine_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
                           float gap_open, float gap_ext, float temp, float* value, float* map,
                           float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
                           size_t workspace_bytes, void* stream, const swb_options* opt) {
-  return launch_padded<3, true>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value,
+  return launch_padded<3, 1>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value,
                                 map, grad_open, grad_ext, grad_temp, workspace, workspace_bytes,
                                 stream, opt);
 }
 
 size_t swb_nw_affine_value_workspace_bytes(int B, int L1max, int L2max) {
-  return B > 0 ? value_layout<3, true>(B, L1max, L2max).total : 0;
+  return B > 0 ? value_layout<3, 1>(B, L1max, L2max).total : 0;
 }
 
 int swb_nw_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
                         float gap_open, float gap_ext, float temp, float* value, void* workspace,
                         size_t workspace_bytes, void* stream) {
-  return launch_value<3, true>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value,
+  return launch_value<3, 1>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value,
                                workspace, workspace_bytes, stream);
 }
 
@@ -688,7 +721,7 @@ int swb_nw_affine_ragged(const float* scores, const void* host_plan, const void*
                          float gap_open, float gap_ext, float temp, float* value, float* map,
                          float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
                          size_t workspace_bytes, void* stream, const swb_options* opt) {
-  return launch_ragged<3, true>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value, map,
+  return launch_ragged<3, 1>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value, map,
                                 grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream,
                                 opt);
 }
@@ -696,9 +729,51 @@ int swb_nw_affine_ragged(const float* scores, const void* host_plan, const void*
 int swb_nw_affine_ragged_value(const float* scores, const void* host_plan, const void* dev_plan,
                                float gap_open, float gap_ext, float temp, float* value,
                                void* workspace, size_t workspace_bytes, void* stream) {
-  return launch_ragged<3, true>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value,
+  return launch_ragged<3, 1>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value,
                                 nullptr, nullptr, nullptr, nullptr, workspace, workspace_bytes,
                                 stream, nullptr, true);
+}
+
+size_t swb_sv_affine_workspace_bytes(int B, int L1max, int L2max) {
+  if (B <= 0) return 0;
+  return std::max(layout_for<3, 2, 2>(B, L1max, L2max).total,
+                  layout_for<3, 4, 2>(B, L1max, L2max).total);
+}
+
+int swb_sv_affine_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap_open, float gap_ext, float temp, float* value, float* map,
+                          float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                          size_t workspace_bytes, void* stream, const swb_options* opt) {
+  return launch_padded<3, 2>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value, map,
+                             grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream,
+                             opt);
+}
+
+size_t swb_sv_affine_value_workspace_bytes(int B, int L1max, int L2max) {
+  return B > 0 ? value_layout<3, 2>(B, L1max, L2max).total : 0;
+}
+
+int swb_sv_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                        float gap_open, float gap_ext, float temp, float* value, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+  return launch_value<3, 2>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, value,
+                            workspace, workspace_bytes, stream);
+}
+
+int swb_sv_affine_ragged(const float* scores, const void* host_plan, const void* dev_plan,
+                         float gap_open, float gap_ext, float temp, float* value, float* map,
+                         float* grad_open, float* grad_ext, float* grad_temp, void* workspace,
+                         size_t workspace_bytes, void* stream, const swb_options* opt) {
+  return launch_ragged<3, 2>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value, map,
+                             grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream, opt);
+}
+
+int swb_sv_affine_ragged_value(const float* scores, const void* host_plan, const void* dev_plan,
+                               float gap_open, float gap_ext, float temp, float* value,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_ragged<3, 2>(scores, host_plan, dev_plan, gap_open, gap_ext, temp, value, nullptr,
+                             nullptr, nullptr, nullptr, workspace, workspace_bytes, stream, nullptr,
+                             true);
 }
 
 size_t swb_nw_value_workspace_bytes(int B, int L1max, int L2max) {
@@ -707,7 +782,7 @@ size_t swb_nw_value_workspace_bytes(int B, int L1max, int L2max) {
 
 int swb_nw_value(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
                  float temp, float* value, void* workspace, size_t workspace_bytes, void* stream) {
-  return launch_value<1, true>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, workspace,
+  return launch_value<1, 1>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, value, workspace,
                                workspace_bytes, stream);
 }
 
@@ -715,11 +790,11 @@ int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const lon
                     int B, void* plan, size_t plan_capacity, size_t* plan_bytes,
                     size_t* workspace_bytes) {
   const int R = cols_per_lane ? cols_per_lane : kDefaultR;
-  // family: 1 linear, 3 affine, 2 global linear, 4 global affine
-  if ((family < 1 || family > 4) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
+  // family: 1 linear, 3 affine, 2 global linear, 4 global affine, 5 Saigo-Vert
+  if ((family < 1 || family > 5) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
     return SWB_ERR_ARG;
-  const int ns = (family == 3 || family == 4) ? 3 : 1;
-  const int NE = 2 * ns, NP = family == 4 ? 6 : (ns == 3 ? 5 : 2);
+  const int ns = (family >= 3) ? 3 : 1;
+  const int NE = 2 * ns, NP = family >= 4 ? 6 : (ns == 3 ? 5 : 2);
   const int CKRS = (2 * ns * R + 2 * ns) * 32 + 4;
   // validate the packing: row pitch round4(L2), offsets multiples of 4 floats
   long long ntasks = 0;
@@ -829,14 +904,14 @@ int swb_nw_ragged(const float* scores, const void* host_plan, const void* dev_pl
                   float temp, float* value, float* map, float* grad_gap, float* grad_temp,
                   void* workspace, size_t workspace_bytes, void* stream,
                   const swb_options* opt) {
-  return launch_ragged<1, true>(scores, host_plan, dev_plan, gap, 0.f, temp, value, map, grad_gap,
+  return launch_ragged<1, 1>(scores, host_plan, dev_plan, gap, 0.f, temp, value, map, grad_gap,
                                 nullptr, grad_temp, workspace, workspace_bytes, stream, opt);
 }
 
 int swb_nw_ragged_value(const float* scores, const void* host_plan, const void* dev_plan, float gap,
                         float temp, float* value, void* workspace, size_t workspace_bytes,
                         void* stream) {
-  return launch_ragged<1, true>(scores, host_plan, dev_plan, gap, 0.f, temp, value, nullptr,
+  return launch_ragged<1, 1>(scores, host_plan, dev_plan, gap, 0.f, temp, value, nullptr,
                                 nullptr, nullptr, nullptr, workspace, workspace_bytes, stream,
                                 nullptr, true);
 }

@@ -138,16 +138,20 @@ struct Place {
 // Push channels crossing a lane or band edge backward: local affine 5 (left
 // M, D; diagonal M, I, D), global affine 6 (left M, I, D; diagonal M, I, D),
 // linear 2 (left, diagonal); the first push_left of them are left pushes.
-template <int NS, bool G> __host__ __device__ constexpr int push_channels() {
-  return NS == 3 ? (G ? 6 : 5) : 2;
+// Model variants of the band kernels (template argument GM): 0 the local
+// alignments (soft Smith-Waterman), 1 the global ones (soft Needleman-
+// Wunsch), 2 Saigo-Vert (local, affine states with D <- I, only M ends).
+// Global and Saigo-Vert affine take six push channels (D pushes to M, I, D).
+template <int NS, int GM> __host__ __device__ constexpr int push_channels() {
+  return NS == 3 ? (GM ? 6 : 5) : 2;
 }
-template <int NS, bool G> __host__ __device__ constexpr int push_left() {
-  return NS == 3 ? (G ? 3 : 2) : 1;
+template <int NS, int GM> __host__ __device__ constexpr int push_left() {
+  return NS == 3 ? (GM ? 3 : 2) : 1;
 }
 
-template <int NS, int R, bool G = false>
+template <int NS, int R, int GM = 0>
 __device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_band) {
-  constexpr int NE = 2 * NS, NP = push_channels<NS, G>(), CKRS = (2 * NS * R + 2 * NS) * 32 + 4;
+  constexpr int NE = 2 * NS, NP = push_channels<NS, GM>(), CKRS = (2 * NS * R + 2 * NS) * 32 + 4;
   Place w;
   Pair& r = w.pr;
   if (a.layout == 0) {
@@ -416,6 +420,22 @@ __device__ __forceinline__ void put_inits(float* ent, int lane, int c, float b0,
     col[160 + lane] = b0;
   }
 }
+// Saigo-Vert: the D <- I weight lives in the slot the local affine model
+// uses for D's beta-init (its only beta-init is M's, in the first of the
+// init pair).
+template <int R>
+__device__ __forceinline__ void put_wdi(float* ent, int lane, int c, float w) {
+  ent[c * Shape<3>::WF * 32 + 320 + lane] = w;
+}
+template <int R>
+__device__ __forceinline__ float get_wdi(const float* ent, int lane, int c) {
+  return ent[c * Shape<3>::WF * 32 + 320 + lane];
+}
+template <int R>
+__device__ __forceinline__ void put_init_m(float* ent, int lane, int c, float b0) {
+  reinterpret_cast<float2*>(ent + c * Shape<3>::WF * 32 + 256)[lane] = make_float2(b0, 0.f);
+}
+
 template <int NS, int R>
 __device__ __forceinline__ void get_weights(const float* ent, int lane, int c, float4& A, float4& B,
                                             float& sc) {
@@ -460,13 +480,15 @@ __device__ __forceinline__ void get_inits(const float* ent, int lane, int c, flo
 // no local start, no beta-inits.  `hold` (a row before the lane's first)
 // keeps (ph, pl) at the row-0 boundary values and writes zero weights, so the
 // boundary cells neither change nor push.
-template <int NS, int R, bool WT = false, bool G = false>
+template <int NS, int R, bool WT = false, int GM = 0>
 __device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R],
                                           const float (&lfh)[NS], const float (&lfl)[NS],
                                           const float (&dgh0)[NS], const float (&dgl0)[NS],
                                           const float (&s)[R], float g0, float g1,
                                           float Sh = 0.f, float Sl = 0.f, int nlive = 0,
                                           float* went = nullptr, int lane = 0, bool hold = false) {
+  constexpr bool G = GM == 1;
+  [[maybe_unused]] constexpr bool SV = GM == 2;
   // G, NS == 3 (global affine): M = s + LSE(M, I, D at diag);
   // I = LSE(M + go, I + ge, D + go) from above; D = LSE(M + go, I + go, D + ge)
   // from the left.  Fields: A = (wMM, wMI, wMD, wIM), B = (wII, wDM, wDD, s),
@@ -528,16 +550,19 @@ __device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
       const float si = ta + tb;
       float Ih, Il;
       fast2(ru, lg2(si), Ih, Il);
-      // D = LSE(M left + go, D left + ge)
-      const float rl = fmaxf(lh[0] + g0, lh[2] + g1);
+      // D = LSE(M left + go, D left + ge); Saigo-Vert adds I left + go
+      const float rl = SV ? fmaxf(fmaxf(lh[0] + g0, lh[1] + g0), lh[2] + g1)
+                          : fmaxf(lh[0] + g0, lh[2] + g1);
       const float tc = ex2(((lh[0] - rl) + g0) + ll[0]), td = ex2(((lh[2] - rl) + g1) + ll[2]);
-      const float sd = tc + td;
+      const float te = SV ? ex2(((lh[1] - rl) + g0) + ll[1]) : 0.f;
+      const float sd = SV ? (tc + te) + td : tc + td;
       float Dh, Dl;
       fast2(rl, lg2(sd), Dh, Dl);
       if constexpr (WT) {
         const float vm = recip(sm), vi = recip(si), vd = recip(sd);
         put_weights<NS, R>(went, lane, c, make_float4(tM * vm, tI * vm, tD * vm, ta * vi),
                            make_float4(tb * vi, tc * vd, td * vd, 0.f), s[c]);
+        if constexpr (SV) put_wdi<R>(went, lane, c, te * vd);
       }
       dgh[0] = uMh; dgl[0] = uMl; dgh[1] = uIh; dgl[1] = uIl; dgh[2] = uDh; dgl[2] = uDl;
       lh[0] = Mh; ll[0] = Ml; lh[1] = Ih; ll[1] = Il; lh[2] = Dh; ll[2] = Dl;
@@ -590,19 +615,21 @@ __device__ __forceinline__ bool fwd_cells(float (&ph)[NS][R], float (&pl)[NS][R]
     // terms <= 1), so a hi part below S - 135 gives an exponent below -130
     // and an init of exactly 0 (ex2.approx.ftz flushes it): when that holds
     // for every lane the step's inits are not computed or stored.
+    constexpr int NI = SV ? 1 : NS;   // states that end an alignment (Saigo-Vert: M only)
     bool near = false;
 #pragma unroll
     for (int c = 0; c < R; ++c)
 #pragma unroll
-      for (int q = 0; q < NS; ++q) near |= (c < nlive) && (ph[q][c] - Sh > -135.f);
+      for (int q = 0; q < NI; ++q) near |= (c < nlive) && (ph[q][c] - Sh > -135.f);
     if (!__any_sync(FULL, near)) return false;
 #pragma unroll
     for (int c = 0; c < R; ++c) {
       const bool lv = c < nlive;
-      float b[NS];
+      float b[NI];
 #pragma unroll
-      for (int q = 0; q < NS; ++q) b[q] = lv ? ex2(fminf((ph[q][c] - Sh) + (pl[q][c] - Sl), 0.f)) : 0.f;
-      if constexpr (NS == 3) put_inits<NS, R>(went, lane, c, b[0], b[1], b[2]);
+      for (int q = 0; q < NI; ++q) b[q] = lv ? ex2(fminf((ph[q][c] - Sh) + (pl[q][c] - Sl), 0.f)) : 0.f;
+      if constexpr (SV) put_init_m<R>(went, lane, c, b[0]);
+      else if constexpr (NS == 3) put_inits<NS, R>(went, lane, c, b[0], b[1], b[2]);
       else put_inits<NS, R>(went, lane, c, b[0], 0.f, 0.f);
     }
     return true;
@@ -640,8 +667,10 @@ __device__ __forceinline__ int band_chunks(int L1) { return (L1 + 31 + C_STEPS -
 // terminal value A[L1,L2] (hi, lo) to its partial slot.  The chunk maximum
 // becomes a marker: +1e30 for the chunk holding the terminal, NEG elsewhere,
 // so the adjoint's quiet-chunk test sees the one beta-init there is.
-template <int NS, int R, bool G = false>
+template <int NS, int R, int GM = 0>
 __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadline) {
+  constexpr bool G = GM == 1;
+  [[maybe_unused]] constexpr bool SV = GM == 2;
   using D = Dims<NS, R>;
   constexpr int NE = D::NE;
   const Pair& pr = w.pr;
@@ -774,8 +803,8 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
       if constexpr (G) {
-        fwd_cells<NS, R, false, true>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, 0.f, 0.f, 0, nullptr,
-                                      lane, i < 1);
+        fwd_cells<NS, R, false, GM>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, 0.f, 0.f, 0, nullptr,
+                                    lane, i < 1);
         if (act) {
           if (term_lane && i == L1) {   // the terminal: A[L1, L2], affine LSE of M, I, D there
             float th = 0.f, tl = 0.f;
@@ -796,16 +825,19 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
         }
         continue;
       }
-      fwd_cells<NS, R>(ph, pl, lh, ll, dgh, dgl, s, g0, g1);
+      fwd_cells<NS, R, false, GM>(ph, pl, lh, ll, dgh, dgl, s, g0, g1);
       if (act) {
         // partition: lazily rescaled Kahan sum of ex2(x - ref); exponents stay
         // <= 8 so (hi - ref) + lo rounds at <= 2^-21 absolute
+        // the partition's terms: every state of the local models, M alone
+        // for Saigo-Vert (S = LSE(0, M cells))
+        constexpr int NT = SV ? 1 : NS;
         float mx = NEG;
 #pragma unroll
         for (int c = 0; c < R; ++c)
           if (jl + c < L2)
 #pragma unroll
-            for (int q = 0; q < NS; ++q) mx = fmaxf(mx, ph[q][c]);
+            for (int q = 0; q < NT; ++q) mx = fmaxf(mx, ph[q][c]);
         cmx = fmaxf(cmx, mx);
         if (mx > ref + 8.f) {
           float f = ex2(ref - mx);
@@ -818,7 +850,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
         for (int c = 0; c < R; ++c)
           if (jl + c < L2)
 #pragma unroll
-            for (int q = 0; q < NS; ++q) tsum += ex2((ph[q][c] - ref) + pl[q][c]);
+            for (int q = 0; q < NT; ++q) tsum += ex2((ph[q][c] - ref) + pl[q][c]);
         acc.add(tsum);
         if (lane == 31) {
 #pragma unroll
@@ -849,7 +881,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
   if (lane == 0) { part[0] = ref; part[1] = s_; }
 }
 
-template <int NS, int R, bool G = false>
+template <int NS, int R, int GM = 0>
 __global__ void __launch_bounds__(128) fwd_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
@@ -859,7 +891,7 @@ __global__ void __launch_bounds__(128) fwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 0, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    fwd_band<NS, R, G>(a, place_of<NS, R, G>(a, task, false), lane, deadline);
+    fwd_band<NS, R, GM>(a, place_of<NS, R, GM>(a, task, false), lane, deadline);
   }
 }
 
@@ -947,14 +979,15 @@ __device__ __forceinline__ float empty_global_value(const Args& a, int n, float&
 // S, as finish_pair does after a full adjoint (4 warps per CTA).  Only the
 // pair's band count and first partial slot (and, for a global alignment, its
 // lengths) are needed.
-template <int NS, int R, bool G = false>
+template <int NS, int R, int GM = 0>
 __global__ void __launch_bounds__(128) value_kernel(Args a) {
+  constexpr bool G = GM == 1;
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (q >= a.B) return;
   Place w;
   if (a.layout == 0) {
-    w = place_of<NS, R, G>(a, q * a.nb, false);
+    w = place_of<NS, R, GM>(a, q * a.nb, false);
   } else {
     const long long* pw = a.plan_pairs + (size_t)q * PLAN_PAIR_WORDS;
     w.p = q;
@@ -982,9 +1015,10 @@ __global__ void __launch_bounds__(128) value_kernel(Args a) {
 
 // Last band task of a pair to finish folds the per-band gradient partials (in
 // band order, so the result is deterministic) into the outputs.
-template <int NS, bool G = false>
+template <int NS, int GM = 0>
 __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, float Sl,
                             float g0sum, float g1sum, float pssum) {
+  constexpr bool G = GM == 1;
   const int p = w.p;
   if (lane == 0) {
     float* gp = a.gpart + 4 * (w.slot0 + w.band);
@@ -1041,10 +1075,12 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
 // G (global alignment): the only beta-init is beta = 1 at the terminal cell
 // A[L1, L2]; pushes that leave the grid into the row-0 and column-0 boundary
 // cells (values j * gap and i * gap) add index * push to dS/dgap there.
-template <int NS, int R, bool G = false>
+template <int NS, int R, int GM = 0>
 __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uint64_t deadline) {
+  constexpr bool G = GM == 1;
+  [[maybe_unused]] constexpr bool SV = GM == 2;
   using D = Dims<NS, R>;
-  constexpr int NP = push_channels<NS, G>(), NL = push_left<NS, G>();
+  constexpr int NP = push_channels<NS, GM>(), NL = push_left<NS, GM>();
   constexpr int EW = D::EW, CKF = D::CKF, CKRS = D::CKRS, NE = D::NE;
   const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
@@ -1054,7 +1090,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
   if constexpr (G) pair_term<NS, R>(a, w, Sh, Sl);
   else pair_logz(a, w, lane, Sh, Sl);
   if (!(L1 > 0 && col0 < L2)) {
-    finish_pair<NS, G>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f);
+    finish_pair<NS, GM>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f);
     return;
   }
   const int jl = col0 + lane * R;
@@ -1272,7 +1308,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
         const int ip = i + PF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
-      if (fwd_cells<NS, R, true, G>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, Sh, Sl, act ? ncols : 0,
+      if (fwd_cells<NS, R, true, GM>(ph, pl, lh, ll, dgh, dgl, s, g0, g1, Sh, Sl, act ? ncols : 0,
                                     sm + (size_t)cu * EW * 32, lane, G && i < 1))
         initbits |= 1u << cu;
       if (G && term_lane && i == L1) {
@@ -1335,7 +1371,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
 #pragma unroll
         for (int q = 0; q < NS; ++q) { inD[q] = hold[q]; hold[q] = r[NL + q]; }
       }
-      if constexpr (NS == 3 && G) {
+      if constexpr (NS == 3 && (G || SV)) {
         ac[0][R - 1] += inL[0] + inD[0];
         ac[1][R - 1] += inL[1] + inD[1];
         ac[2][R - 1] += inL[2] + inD[2];
@@ -1389,6 +1425,32 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
             cB += (float)(i - 1) * pDI + (float)(i - 2) * qI;
           }
           nx[0][c] += pIM; nx[1][c] += pII; nx[2][c] += pID;
+          if (c > 0) {
+            nx[0][c - 1] += qM; nx[1][c - 1] += qI; nx[2][c - 1] += qD;
+            ac[0][c - 1] += pDM; ac[1][c - 1] += pDI; ac[2][c - 1] += pDD;
+          } else {
+            outp[0] = pDM; outp[1] = pDI; outp[2] = pDD; outp[3] = qM; outp[4] = qI; outp[5] = qD;
+          }
+        } else if constexpr (NS == 3 && SV) {
+          float4 f0, f1;
+          float sc;
+          get_weights<NS, R>(E, lane, c, f0, f1, sc);
+          const float wDI = get_wdi<R>(E, lane, c);
+          // f0 = (wMM, wMI, wMD, wIM), f1 = (wII, wDM, wDD, s), wDI; M's beta-init
+          float i0 = 0.f, i1 = 0.f, unused = 0.f;
+          if (hasinit) get_inits<NS, R>(E, lane, c, i0, i1, unused);
+          const float bM = i0 + ac[0][c];
+          const float bI = ac[1][c];
+          const float bD = ac[2][c];
+          pm[c] = bM;
+          const float pIM = bI * f0.w, pII = bI * f1.x;
+          const float pDM = bD * f1.y, pDI = bD * wDI, pDD = bD * f1.z;
+          cA += (pIM + pDM) + pDI;
+          cB += pII + pDD;
+          cS += bM * sc;
+          nx[0][c] += pIM;
+          nx[1][c] += pII;
+          const float qM = bM * f0.x, qI = bM * f0.y, qD = bM * f0.z;
           if (c > 0) {
             nx[0][c - 1] += qM; nx[1][c - 1] += qI; nx[2][c - 1] += qD;
             ac[0][c - 1] += pDM; ac[1][c - 1] += pDI; ac[2][c - 1] += pDD;
@@ -1475,7 +1537,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
   }
-  finish_pair<NS, G>(a, w, lane, Sh, Sl, v0, v1, v2);
+  finish_pair<NS, GM>(a, w, lane, Sh, Sl, v0, v1, v2);
 }
 
 // Shared memory per adjoint warp (floats): one chunk of adjoint fields.
@@ -1484,7 +1546,7 @@ __host__ __device__ constexpr int bwd_smem_floats() {
   return C_STEPS * Dims<NS, R>::EW * 32;
 }
 
-template <int NS, int R, int WARPS, bool G = false>
+template <int NS, int R, int WARPS, int GM = 0>
 __global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31;
@@ -1497,7 +1559,7 @@ __global__ void __launch_bounds__(32 * WARPS) bwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    bwd_band<NS, R, G>(a, place_of<NS, R, G>(a, task, true), lane, sm, deadline);
+    bwd_band<NS, R, GM>(a, place_of<NS, R, GM>(a, task, true), lane, sm, deadline);
   }
 }
 

@@ -47,16 +47,19 @@ constexpr float LN2 = 0.69314718055994531f;
 // MUFU lg2 flushes a subnormal input to 0 and would return -inf.
 constexpr float W_TINY = 1.17549435e-38f;
 
-template <int NS, bool GL = false> struct XShape;
+template <int NS, int GM = 0> struct XShape;
 // G: float4 field groups per cell; NE: floats per row crossing a band edge
 // forward (hi, lo, tangent of each state); NP: value push channels crossing a
 // lane or band edge backward (their tangents double it); NL of them are left
 // pushes.  Global affine: nine weights and their tangents, no per-cell
 // alpha (its only beta-init, at the terminal, travels in the partial slot).
-template <> struct XShape<3, false> { static constexpr int G = 6, NE = 9, NP = 5, NL = 2; };
-template <> struct XShape<3, true> { static constexpr int G = 5, NE = 9, NP = 6, NL = 3; };
-template <> struct XShape<1, false> { static constexpr int G = 3, NE = 3, NP = 2, NL = 1; };
-template <> struct XShape<1, true> { static constexpr int G = 3, NE = 3, NP = 2, NL = 1; };
+// (GM: 0 local, 1 global, 2 Saigo-Vert; Saigo-Vert keeps only M's alpha and
+// tangent per cell, the one state with a beta-init)
+template <> struct XShape<3, 0> { static constexpr int G = 6, NE = 9, NP = 5, NL = 2; };
+template <> struct XShape<3, 1> { static constexpr int G = 5, NE = 9, NP = 6, NL = 3; };
+template <> struct XShape<3, 2> { static constexpr int G = 5, NE = 9, NP = 6, NL = 3; };
+template <> struct XShape<1, 0> { static constexpr int G = 3, NE = 3, NP = 2, NL = 1; };
+template <> struct XShape<1, 1> { static constexpr int G = 3, NE = 3, NP = 2, NL = 1; };
 // floats of the forward's per-band partial slot: (ref or S hi, sum or S lo,
 // U-sum or dS, log-sum), then the global affine terminal's beta-inits and
 // their tangents (w_M, w_I, w_D, dw_M, dw_I, dw_D), padded to 12
@@ -80,8 +83,8 @@ constexpr int XSTAGES = SWB_XSTAGES;   // field steps in flight per backward war
 #endif
 
 // floats of one step of fields for one warp
-template <int NS, int R, bool GL = false>
-__host__ __device__ constexpr int xstep_floats() { return R * XShape<NS, GL>::G * 128; }
+template <int NS, int R, int GM = 0>
+__host__ __device__ constexpr int xstep_floats() { return R * XShape<NS, GM>::G * 128; }
 
 struct XArgs {
   const float* scores;     // [B, L1m, L2m]
@@ -282,6 +285,62 @@ __device__ __forceinline__ void xcell3g(const float (&dh)[3], const float (&dl)[
   f[4] = make_float4(dwd[1], dwd[2], 0.f, 0.f);
 }
 
+// One Saigo-Vert cell: M as the local affine cell; I = LSE(M + go, I + ge)
+// from above; D = LSE(M + go, I + go, D + ge) from the left.  o as xcell3;
+// fields
+//   f0 = (wMM, wMI, wMD, wIM)   f1 = (wII, wDM, wDI, wDD)
+//   f2 = (dwMM, dwMI, dwMD, dwIM)  f3 = (dwII, dwDM, dwDI, dwDD)  f4 = (Mh, Ml, uM, 0)
+template <int MODE>
+__device__ __forceinline__ void xcell3v(const float (&dh)[3], const float (&dl)[3],
+                                        const float (&du)[3], const float (&uh)[3],
+                                        const float (&ul)[3], const float (&uu)[3],
+                                        const float (&lh)[3], const float (&ll)[3],
+                                        const float (&lu)[3], float s, float vv, float g0, float g1,
+                                        float iT, float (&o)[9], float4 (&f)[5]) {
+  constexpr bool TM = (MODE == AUX_PT);
+  const float r = fmaxf(fmaxf(dh[0], dh[1]), fmaxf(dh[2], 0.f));
+  const float tM = ex2((dh[0] - r) + dl[0]), tI = ex2((dh[1] - r) + dl[1]);
+  const float tD = ex2((dh[2] - r) + dl[2]), tZ = ex2(-r);
+  const float sm = (tM + tI) + (tD + tZ);
+  float Mh, Ml;
+  two_sum(r, s, Mh, Ml);
+  Ml += lg2(sm);
+  const float vm = recip(sm);
+  const float wm[4] = {tM * vm, tI * vm, tD * vm, tZ * vm};
+  const float ru = fmaxf(uh[0] + g0, uh[1] + g1);
+  const float ta = ex2(((uh[0] - ru) + g0) + ul[0]), tb = ex2(((uh[1] - ru) + g1) + ul[1]);
+  const float si = ta + tb;
+  float Ih, Il;
+  fast2(ru, lg2(si), Ih, Il);
+  const float vi = recip(si);
+  const float wi[2] = {ta * vi, tb * vi};
+  const float rl = fmaxf(fmaxf(lh[0] + g0, lh[1] + g0), lh[2] + g1);
+  const float tc = ex2(((lh[0] - rl) + g0) + ll[0]), te = ex2(((lh[1] - rl) + g0) + ll[1]);
+  const float td = ex2(((lh[2] - rl) + g1) + ll[2]);
+  const float sd = (tc + te) + td;
+  float Dh, Dl;
+  fast2(rl, lg2(sd), Dh, Dl);
+  const float vd = recip(sd);
+  const float wd[3] = {tc * vd, te * vd, td * vd};
+  float cm[4] = {du[0], du[1], du[2], 0.f};
+  if (MODE == AUX_HVP) { cm[0] += vv; cm[1] += vv; cm[2] += vv; cm[3] = vv; }
+  float ci[2] = {uu[0], uu[1]}, cd[3] = {lu[0], lu[1], lu[2]};
+  if (MODE == AUX_P0) { ci[0] += 1.f; cd[0] += 1.f; cd[1] += 1.f; }
+  if (MODE == AUX_P1) { ci[1] += 1.f; cd[2] += 1.f; }
+  float dwm[4], dwi[2], dwd[3];
+  const float uM = xwtan<4, TM>(wm, cm, iT, dwm);
+  const float uI = xwtan<2, TM>(wi, ci, iT, dwi);
+  const float uD = xwtan<3, TM>(wd, cd, iT, dwd);
+  o[0] = Mh; o[1] = Ml; o[2] = uM;
+  o[3] = Ih; o[4] = Il; o[5] = uI;
+  o[6] = Dh; o[7] = Dl; o[8] = uD;
+  f[0] = make_float4(wm[0], wm[1], wm[2], wi[0]);
+  f[1] = make_float4(wi[1], wd[0], wd[1], wd[2]);
+  f[2] = make_float4(dwm[0], dwm[1], dwm[2], dwi[0]);
+  f[3] = make_float4(dwi[1], dwd[0], dwd[1], dwd[2]);
+  f[4] = make_float4(Mh, Ml, uM, 0.f);
+}
+
 // One linear cell: o = (Ah, Al, U); fields
 //   f0 = (w_diag, w_up, w_left, w_diag + w_start)
 //   f1 = (dw_diag, dw_up, dw_left, dw_diag + dw_start)   f2 = (Ah, Al, U, 0)
@@ -414,11 +473,12 @@ __device__ __forceinline__ void xterminal(const float (&ph)[NS][R], const float 
 // fields.  The band holding the pair's last column writes the terminal
 // (hi, lo, U) to its partial slot; the chunk maximum is a marker, +1e30 in
 // the chunk holding the terminal and NEG elsewhere.
-template <int NS, int R, int MODE, bool GL = false>
+template <int NS, int R, int MODE, int GM = 0>
 __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t deadline) {
-  using XS = XShape<NS, GL>;
+  constexpr bool GL = GM == 1, SV = GM == 2;
+  using XS = XShape<NS, GM>;
   constexpr int G = XS::G, NE = XS::NE;
-  constexpr int XSTEP = xstep_floats<NS, R, GL>();
+  constexpr int XSTEP = xstep_floats<NS, R, GM>();
   constexpr bool HV = (MODE == AUX_HVP);
   int L1, L2;
   xlengths(a, p, L1, L2);
@@ -553,14 +613,17 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
         for (int q = 0; q < NS; ++q) { wh[q] = lh[q]; wl[q] = ll[q]; wu[q] = lu[q]; }
 #pragma unroll
         for (int c = 0; c < R; ++c) {
-          if constexpr (NS == 3 && GL) {
+          if constexpr (NS == 3 && (GL || SV)) {
             const float uh3[3] = {ph[0][c], ph[1][c], ph[2][c]};
             const float ul3[3] = {pl[0][c], pl[1][c], pl[2][c]};
             const float uu3[3] = {pu[0][c], pu[1][c], pu[2][c]};
             float o[9];
             float4 f[G];
-            xcell3g<MODE>(dgh, dgl, dgu, uh3, ul3, uu3, wh, wl, wu, s[c], vv[c], g0, g1, iT, o, f);
-            if (i < 1) {   // boundary row: keep the values, no fields
+            if constexpr (SV)
+              xcell3v<MODE>(dgh, dgl, dgu, uh3, ul3, uu3, wh, wl, wu, s[c], vv[c], g0, g1, iT, o, f);
+            else
+              xcell3g<MODE>(dgh, dgl, dgu, uh3, ul3, uu3, wh, wl, wu, s[c], vv[c], g0, g1, iT, o, f);
+            if (GL && i < 1) {   // boundary row: keep the values, no fields
 #pragma unroll
               for (int q = 0; q < 3; ++q) { o[3 * q] = uh3[q]; o[3 * q + 1] = ul3[q]; o[3 * q + 2] = uu3[q]; }
 #pragma unroll
@@ -629,12 +692,13 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
         if (!GL && act) {
           // partition with its U- and log-weighted sums, lazily rescaled:
           // exponents stay <= 8 so (hi - ref) + lo rounds at <= 2^-21
+          constexpr int NT = SV ? 1 : NS;   // Saigo-Vert: S = LSE(0, M cells)
           float mx = NEG;
 #pragma unroll
           for (int c = 0; c < R; ++c)
             if (jl + c < L2)
 #pragma unroll
-              for (int q = 0; q < NS; ++q) mx = fmaxf(mx, ph[q][c]);
+              for (int q = 0; q < NT; ++q) mx = fmaxf(mx, ph[q][c]);
           cmx = fmaxf(cmx, mx);
           if (mx > ref + 8.f) {
             const float d = ref - mx, f = ex2(d);
@@ -649,7 +713,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
           for (int c = 0; c < R; ++c)
             if (jl + c < L2)
 #pragma unroll
-              for (int q = 0; q < NS; ++q) {
+              for (int q = 0; q < NT; ++q) {
                 const float x = (ph[q][c] - ref) + pl[q][c];
                 const float e = ex2(x);
                 ts += e;
@@ -687,7 +751,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
   if (lane == 0) { part[0] = ref; part[1] = s_; part[2] = su; part[3] = sx; }
 }
 
-template <int NS, int R, int MODE, bool GL = false>
+template <int NS, int R, int MODE, int GM = 0>
 __global__ void __launch_bounds__(128, SWB_XFWD_MINB) xfwd_kernel(XArgs a) {
   const int lane = threadIdx.x & 31;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
@@ -698,7 +762,7 @@ __global__ void __launch_bounds__(128, SWB_XFWD_MINB) xfwd_kernel(XArgs a) {
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
     const int p = task / a.nb;
-    xfwd_band<NS, R, MODE, GL>(a, p, task - p * a.nb, lane, deadline);
+    xfwd_band<NS, R, MODE, GM>(a, p, task - p * a.nb, lane, deadline);
   }
 }
 
@@ -806,12 +870,13 @@ __device__ void xfinish(const XArgs& a, int p, int band, int lane, bool empty, f
 
 // GL: the only beta-init is 1 at the terminal (tangent 0); pushes into the
 // row-0 / column-0 boundary add index * tangent to the gap tangent (HVP).
-template <int NS, int R, int MODE, bool GL = false>
+template <int NS, int R, int MODE, int GM = 0>
 __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring,
                           uint64_t deadline) {
-  using XS = XShape<NS, GL>;
+  constexpr bool GL = GM == 1, SV = GM == 2;
+  using XS = XShape<NS, GM>;
   constexpr int G = XS::G, NP = XS::NP, NQ = 2 * NP, NL = XS::NL;
-  constexpr int XSTEP = xstep_floats<NS, R, GL>();
+  constexpr int XSTEP = xstep_floats<NS, R, GM>();
   constexpr bool TM = (MODE == AUX_PT), HV = (MODE == AUX_HVP);
   int L1, L2;
   xlengths(a, p, L1, L2);
@@ -999,7 +1064,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
         }
         // pushes arriving at column R-1 of row i: from the right lane (or band)
         // into the left of this cell, and into its diagonal from (i+1, j+1)
-        if constexpr (NS == 3 && GL) {
+        if constexpr (NS == 3 && (GL || SV)) {
           float iL[3], tL[3], iD[3], tD[3];
           if (lane == 31) {
 #pragma unroll
@@ -1016,7 +1081,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
           }
 #pragma unroll
           for (int q = 0; q < 3; ++q) { ac[q][R - 1] += iL[q] + iD[q]; at[q][R - 1] += tL[q] + tD[q]; }
-          if (term_lane && i == L1) {   // the terminal's beta-inits and their tangents
+          if (GL && term_lane && i == L1) {   // the terminal's beta-inits and their tangents
 #pragma unroll
             for (int c = 0; c < R; ++c)
               if (jl + c == L2 - 1)
@@ -1074,7 +1139,45 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
 #pragma unroll
           for (int g = 0; g < G; ++g) f[g] = *reinterpret_cast<const float4*>(E + (c * G + g) * 128);
           const bool live = act && (jl + c < L2);
-          if constexpr (NS == 3 && GL) {
+          if constexpr (NS == 3 && SV) {
+            // f0 = (wMM, wMI, wMD, wIM) f1 = (wII, wDM, wDI, wDD) f2 = (dwMM, dwMI, dwMD, dwIM)
+            // f3 = (dwII, dwDM, dwDI, dwDD) f4 = (Mh, Ml, uM, -); M's beta-init only
+            const float xs = (f[4].x - Sh) + (f[4].y - Sl);
+            const float e0 = live ? ex2(fminf(xs, 0.f)) : 0.f;
+            float x = f[4].z - dS;
+            if (TM) x -= (e0 > 0.f ? xs * LN2 : 0.f);
+            const float bM = ac[0][c] + e0, tgM = at[0][c] + e0 * x * iT;
+            const float bI = ac[1][c], tgI = at[1][c], bD = ac[2][c], tgD = at[2][c];
+            const float qM = bM * f[0].x, qI = bM * f[0].y, qD = bM * f[0].z;
+            const float tqM = fmaf(tgM, f[0].x, bM * f[2].x);
+            const float tqI = fmaf(tgM, f[0].y, bM * f[2].y);
+            const float tqD = fmaf(tgM, f[0].z, bM * f[2].z);
+            const float pIM = bI * f[0].w, pII = bI * f[1].x;
+            const float tIM = fmaf(tgI, f[0].w, bI * f[2].w);
+            const float tII = fmaf(tgI, f[1].x, bI * f[3].x);
+            const float pDM = bD * f[1].y, pDI = bD * f[1].z, pDD = bD * f[1].w;
+            const float tDM = fmaf(tgD, f[1].y, bD * f[3].y);
+            const float tDI = fmaf(tgD, f[1].z, bD * f[3].z);
+            const float tDD = fmaf(tgD, f[1].w, bD * f[3].w);
+            pm[c] = tgM;
+            if (HV) {
+              cA += (tIM + tDM) + tDI;
+              cB += tII + tDD;
+              cC = fmaf(tgM, sc[c], fmaf(bM, vv[c], cC));
+            }
+            nx[0][c] += pIM; nx[1][c] += pII;
+            nt[0][c] += tIM; nt[1][c] += tII;
+            if (c > 0) {
+              nx[0][c - 1] += qM; nx[1][c - 1] += qI; nx[2][c - 1] += qD;
+              nt[0][c - 1] += tqM; nt[1][c - 1] += tqI; nt[2][c - 1] += tqD;
+              ac[0][c - 1] += pDM; ac[1][c - 1] += pDI; ac[2][c - 1] += pDD;
+              at[0][c - 1] += tDM; at[1][c - 1] += tDI; at[2][c - 1] += tDD;
+            } else {
+              outp[0] = pDM; outp[1] = pDI; outp[2] = pDD; outp[3] = qM; outp[4] = qI; outp[5] = qD;
+              outp[NP + 0] = tDM; outp[NP + 1] = tDI; outp[NP + 2] = tDD;
+              outp[NP + 3] = tqM; outp[NP + 4] = tqI; outp[NP + 5] = tqD;
+            }
+          } else if constexpr (NS == 3 && GL) {
             // f0 = (wMM, wMI, wMD, wIM) f1 = (wII, wID, wDM, wDI) f2 = (wDD, dwMM, dwMI, dwMD)
             // f3 = (dwIM, dwII, dwID, dwDM) f4 = (dwDI, dwDD, -, -)
             const float bM = ac[0][c], bI = ac[1][c], bD = ac[2][c];
@@ -1231,7 +1334,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   xfinish<NS, MODE>(a, p, band, lane, false, dS, v0, v1, v2);
 }
 
-template <int NS, int R, int MODE, bool GL = false>
+template <int NS, int R, int MODE, int GM = 0>
 __global__ void __launch_bounds__(32, SWB_XBWD_MINB) xbwd_kernel(XArgs a) {
   extern __shared__ __align__(16) float xring[];
   const int lane = threadIdx.x & 31;
@@ -1243,7 +1346,7 @@ __global__ void __launch_bounds__(32, SWB_XBWD_MINB) xbwd_kernel(XArgs a) {
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
     const int p = task / a.nb;
-    xbwd_band<NS, R, MODE, GL>(a, p, a.nb - 1 - (task - p * a.nb), lane, xring, deadline);
+    xbwd_band<NS, R, MODE, GM>(a, p, a.nb - 1 - (task - p * a.nb), lane, xring, deadline);
   }
 }
 

@@ -217,6 +217,27 @@ NW_AFFINE = Family(
     value=lambda *a: torch.ops.orihime_b200.nw_affine_value(*a),
 )
 
+SV_LINEAR = Family(
+    "sv_linear", ("gap", "temp"),
+    forward=lambda *a: _ops().sv_linear_forward(*a),
+    grads=lambda *a: _ops().sv_linear_value_grad_params(*a),
+    hvp=lambda *a: _ops().sv_linear_marginals_hvp(*a),
+    sens=(lambda *a: _ops().sv_linear_marginals_grad_gap(*a),
+          lambda *a: _ops().sv_linear_marginals_grad_temp(*a)),
+    value=lambda *a: torch.ops.orihime_b200.sv_linear_value(*a),
+)
+
+SV_AFFINE = Family(
+    "sv_affine", ("gap_open", "gap_ext", "temp"),
+    forward=lambda *a: _ops().sv_affine_forward(*a),
+    grads=lambda *a: _ops().sv_affine_value_grad_params(*a),
+    hvp=lambda *a: _ops().sv_affine_marginals_hvp(*a),
+    sens=(lambda *a: _ops().sv_affine_marginals_grad_gap_open(*a),
+          lambda *a: _ops().sv_affine_marginals_grad_gap_ext(*a),
+          lambda *a: _ops().sv_affine_marginals_grad_temp(*a)),
+    value=lambda *a: torch.ops.orihime_b200.sv_affine_value(*a),
+)
+
 
 # ---------------------------------------------------------------------------
 # autograd functions

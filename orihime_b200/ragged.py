@@ -18,8 +18,9 @@ flat float32 buffer.  The map comes back in the same packing.
 
 Families: "affine" and "linear" (local alignment), "global" (soft
 Needleman-Wunsch, linear gap; parameters gap and temp as for "linear") and
-"global_affine" (soft Needleman-Wunsch, affine gaps; parameters as for
-"affine").
+"global_affine" (soft Needleman-Wunsch, affine gaps) and "saigo_vert"
+(Saigo-Vert, affine gaps; its linear model is gap_open = gap_ext); the last
+two take the parameters of "affine".
 """
 
 from __future__ import annotations
@@ -33,8 +34,10 @@ import torch
 
 from . import _lib
 
-_FAMILY = {"affine": 3, "linear": 1, "global": 2, "global_affine": 4}
-_AFFINE = ("affine", "global_affine")
+_FAMILY = {"affine": 3, "linear": 1, "global": 2, "global_affine": 4, "saigo_vert": 5}
+_AFFINE = ("affine", "global_affine", "saigo_vert")
+_AFFINE_FN = {"affine": "swb_sw_affine_ragged", "global_affine": "swb_nw_affine_ragged",
+              "saigo_vert": "swb_sv_affine_ragged"}
 
 
 def pitch_of(L2: int) -> int:
@@ -152,8 +155,7 @@ class Plan:
         ws = self.workspace.data_ptr()
         with torch.cuda.device(self.device):
             if self.family in _AFFINE:
-                fn = (self.lib.swb_nw_affine_ragged if self.family == "global_affine"
-                      else self.lib.swb_sw_affine_ragged)
+                fn = getattr(self.lib, _AFFINE_FN[self.family])
                 rc = fn(
                     flat.data_ptr(), hp, dp, float(gap_open), float(gap_ext), float(temp),
                     out.value.data_ptr(), out.map.data_ptr(), out.grad_open.data_ptr(),
@@ -186,8 +188,7 @@ class Plan:
         ws = self.workspace.data_ptr()
         with torch.cuda.device(self.device):
             if self.family in _AFFINE:
-                fn = (self.lib.swb_nw_affine_ragged_value if self.family == "global_affine"
-                      else self.lib.swb_sw_affine_ragged_value)
+                fn = getattr(self.lib, _AFFINE_FN[self.family] + "_value")
                 rc = fn(
                     flat.data_ptr(), hp, dp, float(gap_open), float(gap_ext), float(temp),
                     out.data_ptr(), ws, self.workspace_bytes, st)

@@ -6,13 +6,13 @@ directory under /tmp, compiles the reference's CPU extension there with g++
 (the source list of meson.build's ``cpp_sources``), imports it, and records
 the public soft Smith-Waterman API's outputs on small seeded inputs:
 
-* ``ohm.sw`` / ``sw_value`` / ``sw_entropy``, the ``sw_affine`` trio and the
-  global-alignment ``nw`` and ``nw_affine`` trios: forward results and the
-  gradients of value, map (against a fixed cotangent) and entropy with respect
-  to the pair scores;
+* ``ohm.sw`` / ``sw_value`` / ``sw_entropy``, the ``sw_affine`` trio, the
+  global-alignment ``nw`` and ``nw_affine`` trios and the Saigo-Vert ``sv``
+  and ``sv_affine`` trios: forward results and the gradients of value, map
+  (against a fixed cotangent) and entropy with respect to the pair scores;
 * lengths-ragged and boolean-mask batches;
 * tensor-valued (learnable) gap parameters and their gradients;
-* ``ohm.ops.sw*.backward`` / ``ohm.ops.nw*.backward`` (map VJP) and
+* ``ohm.ops.{sw,nw,sv}*.backward`` (map VJP) and
   ``.sensitivity`` (parameter fields).
 
 Output: ``sw_golden.npz`` (float32 arrays, a few hundred KB).
@@ -112,12 +112,18 @@ def main() -> None:
                                      temperature=0.7)),
                         ("nw", dict(gap_score=-1.0, temperature=0.7)),
                         ("nwa", dict(gap_open_score=-2.0, gap_extend_score=-0.5,
+                                     temperature=0.7)),
+                        ("svl", dict(gap_score=-1.0, temperature=0.7)),
+                        ("sva", dict(gap_open_score=-2.0, gap_extend_score=-0.5,
                                      temperature=0.7))):
             fmap, fval, fent = {"lin": (ohm.sw, ohm.sw_value, ohm.sw_entropy),
                                 "aff": (ohm.sw_affine, ohm.sw_affine_value, ohm.sw_affine_entropy),
                                 "nw": (ohm.nw, ohm.nw_value, ohm.nw_entropy),
                                 "nwa": (ohm.nw_affine, ohm.nw_affine_value,
-                                        ohm.nw_affine_entropy)}[fam]
+                                        ohm.nw_affine_entropy),
+                                "svl": (ohm.sv, ohm.sv_value, ohm.sv_entropy),
+                                "sva": (ohm.sv_affine, ohm.sv_affine_value,
+                                        ohm.sv_affine_entropy)}[fam]
             key = f"{name}/{fam}"
             x = x0.clone().requires_grad_(True)
             v = fval(x, lengths=lt, **kw)
@@ -135,7 +141,8 @@ def main() -> None:
             put(f"{key}/entropy", h)
             put(f"{key}/dentropy", g)
             op = {"lin": ohm.ops.sw, "aff": ohm.ops.sw_affine, "nw": ohm.ops.nw,
-                  "nwa": ohm.ops.nw_affine}[fam]
+                  "nwa": ohm.ops.nw_affine, "svl": ohm.ops.sv,
+                  "sva": ohm.ops.sv_affine}[fam]
             sens = op.sensitivity(x0, lengths=lt, **kw)
             for k2, t in sens.items():
                 put(f"{key}/sens_{k2}", t)

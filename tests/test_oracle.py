@@ -118,6 +118,32 @@ def test_nw_affine_oracle_vs_golden(golden, case):
     _close((cot * sens[2]).sum(), g("bw_temperature"), atol=1e-4)
 
 
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("fam", ["svl", "sva"])
+def test_sv_oracle_vs_golden(golden, case, fam):
+    """Saigo-Vert, linear (ohm.sv trio, ohm.ops.sv) and affine (ohm.sv_affine
+    trio, ohm.ops.sv_affine), against the recorded fixtures."""
+    s, ln, cot = _case(golden, case)
+    g = lambda k: golden[f"{case}/{fam}/{k}"]
+    B = s.shape[0]
+    lin = fam == "svl"
+    go, ge = (-1.0, -1.0) if lin else (-2.0, -0.5)
+    o = O.sv(s, ln, go, ge, T0, linear=lin)
+    _close(o["value"], g("value"))
+    _close(o["map"], g("map"))
+    _close(-o["map"] / B, g("dvalue"))
+    _close(o["grad_temp"], g("entropy"), atol=2e-5)
+    names = ("gap_score", "temperature") if lin else ("gap_open_score", "gap_extend_score", "temperature")
+    sens = {p: O.sv_param_grad(s, ln, go, ge, T0, p, linear=lin) for p in range(len(names))}
+    for p, n in enumerate(names):
+        _close(sens[p], g(f"sens_{n}"), atol=1e-5)
+        _close((cot * sens[p]).sum(), g(f"bw_{n}"), atol=1e-4)
+    _close(sens[len(names) - 1], g("dentropy"), atol=1e-5)
+    hv = O.sv_hvp(s, cot, ln, go, ge, T0)
+    _close(hv, g("dmap"), atol=1e-5)
+    _close(hv, g("bw_pair_scores"), atol=1e-5)
+
+
 def _mask_sentinel(scores, mask, T):
     """orihime/operator.py:334-386: masked cells -> amax - (sum(shape[1:])*80 + 200)*T."""
     x = np.where(mask, -np.inf, scores).astype(np.float32)
@@ -198,6 +224,15 @@ def test_oracle_bit_exact_vs_reference_kernels(seed):
             for p in range(3):
                 assert np.array_equal(O.nw_affine_param_grad(s, lens, -2.0, -0.5, T, p),
                                       O.ref_nw_affine_param_grad(s, lens, -2.0, -0.5, T, p))
+            for lin, (go, ge) in ((False, (-2.0, -0.5)), (True, (-1.0, -1.0))):
+                a, r = O.sv(s, lens, go, ge, T, linear=lin), O.ref_sv(s, lens, go, ge, T, linear=lin)
+                for k in (("value", "map", "grad_open", "grad_temp") if lin else a):
+                    assert np.array_equal(a[k], r[k]), (lin, k)
+                assert np.array_equal(O.sv_hvp(s, V, lens, go, ge, T),
+                                      O.ref_sv_hvp(s, V, lens, go, ge, T, linear=lin))
+                for p in range(2 if lin else 3):
+                    assert np.array_equal(O.sv_param_grad(s, lens, go, ge, T, p, linear=lin),
+                                          O.ref_sv_param_grad(s, lens, go, ge, T, p, linear=lin))
             a, r = O.nw(s, lens, -1.0, T), O.ref_nw(s, lens, -1.0, T)
             for k in a:
                 assert np.array_equal(a[k], r[k]), k

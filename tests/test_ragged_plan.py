@@ -87,7 +87,7 @@ def test_global_alignment_plan_uses_the_linear_layout():
     assert rc1 == 0 and rc2 == 0
     assert np.array_equal(lin[1:7], glob[1:7])          # B, tasks, slots, ck, edge, push
     assert glob[7] & 0xff == 2 and lin[7] & 0xff == 1   # family word
-    assert _plan(lengths, off, family=5)[0] != 0
+    assert _plan(lengths, off, family=6)[0] != 0
     assert _plan(lengths, off, family=0)[0] != 0
 
 
@@ -102,3 +102,5 @@ def test_global_affine_plan_has_six_push_channels():
     assert np.array_equal(loc[1:6], glob[1:6])          # B, tasks, slots, ck, edge
     assert glob[6] * 5 == loc[6] * 6                    # push floats: 6 vs 5 channels
     assert glob[7] & 0xff == 4
+    rc5, sv = _plan(lengths, off, family=5)        # Saigo-Vert: the same six-channel layout
+    assert rc5 == 0 and np.array_equal(sv[1:7], glob[1:7]) and sv[7] & 0xff == 5

@@ -82,4 +82,4 @@ def test_legacy_schemas_defined():
 
 
 def test_legacy_schema_count():
-    assert len(_ops.LEGACY_SCHEMAS) == 24
+    assert len(_ops.LEGACY_SCHEMAS) == 36
