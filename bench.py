@@ -532,6 +532,117 @@ def global_alignment(args):
     return 0
 
 
+def saigo_vert(args):
+    """Saigo-Vert local alignment, affine gaps (gap_open -2, gap_ext -0.5,
+    T 0.5), through the C ABI: the contract line's ragged batch (4096 pairs)
+    as one packed plan (family 5), forward + adjoint and value alone; 64
+    pairs of 1024 x 1024 (scores 3 <e_i, f_j> / sqrt(64)) padded; and the
+    HVP / dP/dT / map VJP at 256 x 512 x 512.  CUDA events on the launching
+    stream, `--warmup` untimed and `--steps` timed calls each.  The
+    reference's CPU kernels (src/sv_affine/kernels_cpu.cpp) run 2 of the 64
+    pairs on all host threads for the CPU line.  Prints one JSON line."""
+    import torch
+
+    import orihime_b200  # noqa: F401
+    from orihime_b200 import _lib, ragged
+
+    lib = _lib.load()
+    st = torch.cuda.current_stream().cuda_stream
+    P = lambda t: t.data_ptr()  # noqa: E731
+    go, ge, temp = -2.0, -0.5, 0.5
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            if fn() != 0:
+                raise RuntimeError("Saigo-Vert call failed")
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / args.steps
+
+    res = {}
+    lengths = workload_lengths(3)
+    offsets, ln32 = ragged.layout(lengths)
+    flat = make_scores(torch, lengths, offsets, 3, "cuda")
+    plan = ragged.Plan(ln32, offsets, family="saigo_vert", device="cuda")
+    outr = plan.outputs()
+    vals = torch.empty(plan.B, device="cuda")
+    rc = plan.cells
+    ms = timed(lambda: (plan.run(flat, gap_open=go, gap_ext=ge, temp=temp, out=outr), 0)[1])
+    res["ragged_forward_adjoint"] = {"ms": round(ms, 3), "gcups": round(rc / ms / 1e6, 2),
+                                     "pairs": plan.B, "cells": rc}
+    ms = timed(lambda: (plan.values(flat, gap_open=go, gap_ext=ge, temp=temp, out=vals), 0)[1])
+    res["ragged_value_only"] = {"ms": round(ms, 3), "gcups": round(rc / ms / 1e6, 2)}
+    del flat, plan, outr
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    B, N, d = 64, 1024, 64
+    e = torch.randn(B, N, d, generator=g, device="cuda")
+    f = torch.randn(B, N, d, generator=g, device="cuda")
+    s = (3.0 * torch.bmm(e, f.transpose(1, 2)) / d ** 0.5).contiguous()
+    del e, f
+    val, amap = torch.empty(B, device="cuda"), torch.empty_like(s)
+    go_, ge_, gT = (torch.empty(B, device="cuda") for _ in range(3))
+    nb = int(lib.swb_sv_affine_workspace_bytes(B, N, N))
+    ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    nbv = int(lib.swb_sv_affine_value_workspace_bytes(B, N, N))
+    wsv = torch.empty(nbv, dtype=torch.uint8, device="cuda")
+    cells = B * N * N
+    ms = timed(lambda: lib.swb_sv_affine_forward(P(s), None, B, N, N, go, ge, temp, P(val), P(amap),
+                                                 P(go_), P(ge_), P(gT), P(ws), nb, st, None))
+    res["forward_adjoint"] = {"ms": round(ms, 3), "gcups": round(cells / ms / 1e6, 2),
+                              "shape": [B, N, N]}
+    ms = timed(lambda: lib.swb_sv_affine_value(P(s), None, B, N, N, go, ge, temp, P(val), P(wsv),
+                                               nbv, st))
+    res["value_only"] = {"ms": round(ms, 3), "gcups": round(cells / ms / 1e6, 2)}
+    sample = s[:2].cpu().numpy()
+    del s, amap, ws, wsv
+
+    B5, N5, d5 = 256, 512, 128
+    g.manual_seed(5)
+    e = torch.randn(B5, N5, d5, generator=g, device="cuda")
+    f = torch.randn(B5, N5, d5, generator=g, device="cuda")
+    s5 = (torch.bmm(e, f.transpose(1, 2)) / d5 ** 0.5).contiguous()
+    v5 = torch.randn(B5, N5, N5, generator=g, device="cuda")
+    del e, f
+    out, gt = torch.empty_like(s5), torch.zeros(B5, 4, device="cuda")
+    nx = int(lib.swb_sv_affine_aux_workspace_bytes(B5, N5, N5))
+    wx = torch.empty(nx, dtype=torch.uint8, device="cuda")
+    c5 = B5 * N5 * N5
+    for name, fn in (
+            ("hvp", lambda: lib.swb_sv_affine_hvp(P(s5), P(v5), None, B5, N5, N5, go, ge, temp,
+                                                  P(out), None, P(wx), nx, st)),
+            ("grad_temp", lambda: lib.swb_sv_affine_param_jacobian(P(s5), None, B5, N5, N5, go, ge,
+                                                                   temp, 2, P(out), P(wx), nx, st)),
+            ("marginals_backward", lambda: lib.swb_sv_affine_hvp(P(s5), P(v5), None, B5, N5, N5, go,
+                                                                 ge, temp, P(out), P(gt), P(wx), nx,
+                                                                 st))):
+        ms = timed(fn)
+        res[name] = {"ms": round(ms, 3), "gcups": round(c5 / ms / 1e6, 2), "shape": [B5, N5, N5]}
+    del s5, v5, out, wx
+
+    line = {"saigo_vert": res, "params": {"gap_open": go, "gap_ext": ge, "temp": temp}}
+    try:
+        from oracle import oracle as O   # the reference's CPU kernels, as a baseline
+        if O.ref_available():
+            torch.set_num_threads(os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            O.ref_sv(sample, None, go, ge, temp)
+            sec = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": round(sample.size / sec / 1e9, 4), "unit": "GCUPS",
+                                    "cores": torch.get_num_threads(), "kind": "reference",
+                                    "sample": "2 of the 64 pairs of 1024 x 1024, forward + backward"}
+    except ImportError:
+        pass
+    print(json.dumps(line))
+    return 0
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -550,6 +661,8 @@ def main():
                     help="timed steps only: no e2e, plain, CPU legs (profiling cases)")
     ap.add_argument("--global-alignment", action="store_true",
                     help="time the soft Needleman-Wunsch (global alignment) ops instead")
+    ap.add_argument("--saigo-vert", action="store_true",
+                    help="time the Saigo-Vert (affine gaps) ops instead")
     ap.add_argument("--second-order", action="store_true",
                     help="time the second-order ops at the training-step shapes instead")
     args = ap.parse_args()
@@ -559,6 +672,8 @@ def main():
         return global_alignment(args)
     if args.second_order:
         return second_order(args)
+    if args.saigo_vert:
+        return saigo_vert(args)
 
     import torch
 
