@@ -1,10 +1,10 @@
 """Our CUDA path against the reference's own CUDA path on the same GPU.
 
 The reference CUDA extension is built by ``make -C oracle refcuda`` from
-``src/sw*/kernels_gpu.cu``, ``src/nw*/kernels_gpu.cu`` and the op bodies
-beside them.  It has to be loaded before orihime_b200, which then takes over
-the namespaced ``sw*`` / ``nw*`` ops; the reference's legacy ``soft_sw*`` /
-``soft_nw*`` ops stay the reference's CUDA path.  That
+``src/sw*/kernels_gpu.cu``, ``src/nw*/kernels_gpu.cu``,
+``src/sv_*/kernels_gpu.cu`` and the op bodies beside them.  It has to be loaded before orihime_b200, which then takes over
+the namespaced ``sw*`` / ``nw*`` / ``sv*`` ops; the reference's legacy
+``soft_sw*`` / ``soft_nw*`` / ``soft_sv*`` ops stay the reference's CUDA path.  That
 order is fixed per process, so the comparison runs in a child process.
 
 Bar: values within rel 1e-5 of the reference CUDA path.  Maps and
@@ -101,6 +101,36 @@ def _worker():
                         hvp_ref_64=dist(rh.cpu(), h64), hvp_scale=float(np.abs(h64).max()),
                         dpdt_ours_ref=dist(op_.cpu(), rp.cpu()), dpdt_ours_64=dist(op_.cpu(), p64),
                         dpdt_ref_64=dist(rp.cpu(), p64), dpdt_scale=float(np.abs(p64).max())))
+        # Saigo-Vert, affine and linear gaps, same inputs
+        for lin in (False, True):
+            if lin:
+                rv, rm = ops.soft_sv_linear_float(sd, -1.0, T, ln.cuda())[:2]
+                ov, om = ops.sv_linear_forward(sd, -1.0, T, ln.cuda())
+                rh = ops.soft_sv_linear_hvp(sd, v.cuda(), -1.0, T, ln.cuda())
+                oh = ops.sv_linear_marginals_hvp(sd, v.cuda(), -1.0, T, ln.cuda())
+                rp = ops.soft_sv_linear_param_jacobian(sd, 1, -1.0, T, ln.cuda())
+                op_ = ops.sv_linear_marginals_grad_temp(sd, -1.0, T, ln.cuda())
+                g3 = (-1.0, -1.0, T)
+            else:
+                rv, rm = ops.soft_sv_affine_float(sd, -2.0, -0.5, T, ln.cuda())[:2]
+                ov, om = ops.sv_affine_forward(sd, -2.0, -0.5, T, ln.cuda())
+                rh = ops.soft_sv_affine_hvp(sd, v.cuda(), -2.0, -0.5, T, ln.cuda())
+                oh = ops.sv_affine_marginals_hvp(sd, v.cuda(), -2.0, -0.5, T, ln.cuda())
+                rp = ops.soft_sv_affine_param_jacobian(sd, 2, -2.0, -0.5, T, ln.cuda())
+                op_ = ops.sv_affine_marginals_grad_temp(sd, -2.0, -0.5, T, ln.cuda())
+                g3 = (-2.0, -0.5, T)
+            t64 = O.sv(s.numpy(), ln.numpy(), *g3, linear=lin, dtype=np.float64)
+            rel = float(((ov - rv).abs() / rv.abs().clamp_min(1.0)).max())
+            h64 = O.sv_hvp(s.numpy(), v.numpy(), ln.numpy(), *g3, dtype=np.float64)
+            p64 = O.sv_param_grad(s.numpy(), ln.numpy(), *g3, 1 if lin else 2, linear=lin,
+                                  dtype=np.float64)
+            out.append(dict(case=["sv_linear" if lin else "sv_affine", B, N, M, T], value_rel=rel,
+                            map_ours_ref=dist(om.cpu(), rm.cpu()), map_ours_64=dist(om.cpu(), t64["map"]),
+                            map_ref_64=dist(rm.cpu(), t64["map"]),
+                            hvp_ours_ref=dist(oh.cpu(), rh.cpu()), hvp_ours_64=dist(oh.cpu(), h64),
+                            hvp_ref_64=dist(rh.cpu(), h64), hvp_scale=float(np.abs(h64).max()),
+                            dpdt_ours_ref=dist(op_.cpu(), rp.cpu()), dpdt_ours_64=dist(op_.cpu(), p64),
+                            dpdt_ref_64=dist(rp.cpu(), p64), dpdt_scale=float(np.abs(p64).max())))
     # timing: C2 (64 x 1024^2) on both CUDA paths
     s = emb(64, 1024, 1024, 1).cuda()
 
@@ -124,6 +154,10 @@ def _worker():
     tr = t(lambda: ops.soft_nw_affine_float(s, -2.0, -0.5, 0.5, None), 2)
     to = t(lambda: ops.nw_affine_forward(s, -2.0, -0.5, 0.5, None), 5)
     out.append(dict(timing="NW affine 64x1024^2 value+map", ref_ms=tr, ours_ms=to,
+                    ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
+    tr = t(lambda: ops.soft_sv_affine_float(s, -2.0, -0.5, 0.5, None), 2)
+    to = t(lambda: ops.sv_affine_forward(s, -2.0, -0.5, 0.5, None), 5)
+    out.append(dict(timing="Saigo-Vert affine 64x1024^2 value+map", ref_ms=tr, ours_ms=to,
                     ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
     del s
     # C1: linear, 8 x 128^2, N(0,1) scores, gap -1, T 1
@@ -160,7 +194,14 @@ def _worker():
              lambda: ops.nw_affine_marginals_grad_temp(s5, -2.0, -0.5, 0.5, None)),
             ("NW affine marginals_backward",
              lambda: ops.soft_nw_affine_backward_full(s5, v5, -2.0, -0.5, 0.5, None),
-             lambda: ops.nw_affine_marginals_backward(s5, v5, -2.0, -0.5, 0.5, None))):
+             lambda: ops.nw_affine_marginals_backward(s5, v5, -2.0, -0.5, 0.5, None)),
+            ("SV affine HVP", lambda: ops.soft_sv_affine_hvp(s5, v5, -2.0, -0.5, 0.5, None),
+             lambda: ops.sv_affine_marginals_hvp(s5, v5, -2.0, -0.5, 0.5, None)),
+            ("SV affine dP/dT", lambda: ops.soft_sv_affine_param_jacobian(s5, 2, -2.0, -0.5, 0.5, None),
+             lambda: ops.sv_affine_marginals_grad_temp(s5, -2.0, -0.5, 0.5, None)),
+            ("SV affine marginals_backward",
+             lambda: ops.soft_sv_affine_backward_full(s5, v5, -2.0, -0.5, 0.5, None),
+             lambda: ops.sv_affine_marginals_backward(s5, v5, -2.0, -0.5, 0.5, None))):
         tr, to = t(rf, 1), t(of, 3)
         out.append(dict(timing=name + " 256x512^2", ref_ms=tr, ours_ms=to,
                         ref_gcups=cells / tr / 1e6, ours_gcups=cells / to / 1e6))
