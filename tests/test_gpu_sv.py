@@ -185,19 +185,25 @@ def test_sv_second_order_matches_oracle(lin, B, L1, L2, lengths, T, seed):
             O.sv_hvp(sn, v.numpy(), lnn, *og, T, dtype=np.float64))
     vn = v.numpy().astype(np.float64)
     # The temperature tangent comes from homogeneity in (s, go, ge, T) in the
-    # same pass: T g_T = -sum(s * HG) - go * o - ge * e.  An error D in the
-    # returned HG therefore moves it by -sum(s * D) / T; the check is that the
-    # scalar is consistent with the identity given our HG (which is bounded
-    # above on its own).
+    # same pass: T g_T = -sum(s * HG) - go * o - ge * e.  Errors D in the
+    # returned HG and in the gap tangents o, e therefore move it by
+    # -(sum(s * D) + go * Do + ge * De) / T; the check is that the scalar is
+    # consistent with the identity given our other outputs (each bounded on
+    # its own above and below).
     h64 = O.sv_hvp(sn, v.numpy(), lnn, *og, T, dtype=np.float64)
     dh = bw[0].cpu().numpy().astype(np.float64) - h64
     if lnn is not None:
         for b, (l1, l2) in enumerate(lnn.tolist()):
             dh[b, l1:, :] = 0.0
             dh[b, :, l2:] = 0.0
-    shift_T = -(sn.astype(np.float64) * dh).sum() / T
+    r64s = [(vn * O.sv_param_grad(sn, lnn, *og, T, p, linear=lin, dtype=np.float64)).sum()
+            for p in range(len(fns))]
+    shift_T = -(sn.astype(np.float64) * dh).sum()
+    for p, g in enumerate(gaps):
+        shift_T -= g * (float(bw[1 + p].item()) - r64s[p])
+    shift_T /= T
     for p in range(len(fns)):
-        r64 = (vn * O.sv_param_grad(sn, lnn, *og, T, p, linear=lin, dtype=np.float64)).sum()
+        r64 = r64s[p]
         r32 = (vn * O.sv_param_grad(sn, lnn, *og, T, p, linear=lin)).sum()
         want = r64 + (shift_T if p == len(fns) - 1 else 0.0)
         got = float(bw[1 + p].item())
