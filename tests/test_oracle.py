@@ -280,3 +280,41 @@ def test_nw_finite_differences_of_fp64_value():
     assert abs((f(s, -0.7 + eps, 0.6) - f(s, -0.7 - eps, 0.6)) / (2 * eps) - base["grad_gap"][0]) < 1e-6
     assert abs((f(s, -0.7, 0.6 + eps) - f(s, -0.7, 0.6 - eps)) / (2 * eps) - base["grad_temp"][0]) < 1e-5
     assert np.all(base["map"][0, 5:, :] == 0) and np.all(base["map"][0, :, 6:] == 0)
+
+
+@pytest.mark.parametrize("fam", ["sw", "sw_affine", "nw", "nw_affine", "sv_linear", "sv_affine"])
+def test_second_order_homogeneity_identity(fam):
+    """S is 1-homogeneous in (scores, gaps, T), so along any score direction v
+    T * <v, dP/dT> = -<s, H v> - sum_k gap_k * <v, dP/dgap_k>: the identity
+    from which the marginals_backward ops take their temperature tangent in
+    the same pass as H v.  Checked on the fp64 oracle."""
+    rng = np.random.default_rng(7)
+    B, L1, L2, T = 2, 13, 17, 0.6
+    s = (1.5 * rng.standard_normal((B, L1, L2))).astype(np.float32)
+    v = rng.standard_normal((B, L1, L2)).astype(np.float32)
+    ln = np.array([[13, 17], [9, 12]], np.int32)
+    d = np.float64
+    if fam == "sw":
+        gaps = (-1.0,)
+        hv = O.linear_hvp(s, v, ln, *gaps, T, dtype=d)
+        jac = [O.linear_param_grad(s, ln, *gaps, T, p, dtype=d) for p in range(2)]
+    elif fam == "nw":
+        gaps = (-1.0,)
+        hv = O.nw_hvp(s, v, ln, *gaps, T, dtype=d)
+        jac = [O.nw_param_grad(s, ln, *gaps, T, p, dtype=d) for p in range(2)]
+    elif fam == "sv_linear":
+        gaps = (-1.0,)
+        hv = O.sv_hvp(s, v, ln, -1.0, -1.0, T, dtype=d)
+        jac = [O.sv_param_grad(s, ln, -1.0, -1.0, T, p, linear=True, dtype=d) for p in range(2)]
+    else:
+        gaps = (-2.0, -0.5)
+        hvp, pg = {"sw_affine": (O.affine_hvp, O.affine_param_grad),
+                   "nw_affine": (O.nw_affine_hvp, O.nw_affine_param_grad),
+                   "sv_affine": (O.sv_hvp, O.sv_param_grad)}[fam]
+        hv = hvp(s, v, ln, *gaps, T, dtype=d)
+        jac = [pg(s, ln, *gaps, T, p, dtype=d) for p in range(3)]
+    vd, sd = v.astype(d), s.astype(d)
+    tan = [(vd * j).sum() for j in jac]
+    lhs = T * tan[-1]
+    rhs = -(sd * hv).sum() - sum(g * t for g, t in zip(gaps, tan[:-1]))
+    assert abs(lhs - rhs) <= 1e-9 * (1 + abs(lhs) + np.abs(sd * hv).sum()), (fam, lhs, rhs)
