@@ -79,3 +79,28 @@ def test_argument_errors_return_before_any_launch(lib):
     rc = lib.swb_sw_affine_forward(p, None, 1, 4, 4, f(-2), f(-0.5), f(1.0), p, p, p, p, p, p, 16,
                                    None, None)
     assert rc == -2  # workspace too small
+
+
+@pytest.mark.parametrize("fam", ["nw", "nw_affine", "sv_affine"])
+def test_other_families_argument_errors_and_workspaces(lib, fam):
+    """The global and Saigo-Vert entry points validate like the local ones,
+    before touching CUDA: temperature <= 0 and B < 0 are argument errors, an
+    empty batch is a no-op, a short workspace is refused."""
+    f = ctypes.c_float
+    ws = getattr(lib, f"swb_{fam}_workspace_bytes")
+    a, b = ws(4, 100, 100), ws(8, 100, 100)
+    assert 0 < a < b and ws(0, 10, 10) == 0
+    assert getattr(lib, f"swb_{fam}_value_workspace_bytes")(4, 100, 100) > 0
+    assert getattr(lib, f"swb_{fam}_aux_workspace_bytes")(4, 100, 100) > 0
+    fwd = getattr(lib, f"swb_{fam}_forward")
+    buf = (ctypes.c_float * 16)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    if fam == "nw":
+        call = lambda B, T, w, n: fwd(w, None, B, 4, 4, f(-1), f(T), w, w, w, w, w, n, None, None)  # noqa: E731
+    else:
+        call = lambda B, T, w, n: fwd(w, None, B, 4, 4, f(-2), f(-0.5), f(T), w, w, w, w, w, w, n,  # noqa: E731
+                                      None, None)
+    assert call(1, 0.0, None, 0) == -1
+    assert call(-1, 1.0, None, 0) == -1
+    assert call(0, 1.0, None, 0) == 0
+    assert call(1, 1.0, p, 16) == -2
