@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SWB_ABI_VERSION 1
+#define SWB_ABI_VERSION 2
 
 #define SWB_OK 0
 #define SWB_ERR_ARG (-1)
@@ -52,7 +52,18 @@ typedef struct swb_options {
     void* split_event;                 /* cudaEvent_t recorded between the forward and the
                                           adjoint kernel (per-kernel timing), or NULL     */
     int cols_per_lane;                 /* columns per lane of a band: 2 or 4 (0 = default) */
+    int domain;                        /* local models: SWB_DOMAIN_AUTO (0), _LOG or _LINEAR */
 } swb_options;
+
+/* Arithmetic of the local-alignment kernels (swb_options.domain).  AUTO runs
+ * the scaled linear domain (one ex2 per cell, multiply-adds, power-of-two
+ * frames per lane) whenever every gap parameter is <= 0, else the scaled log
+ * domain (double-float log-sum-exp); LOG forces the latter; LINEAR requires
+ * the former and returns SWB_ERR_ARG when a gap parameter is positive.  The
+ * global and Saigo-Vert families always run in the log domain. */
+#define SWB_DOMAIN_AUTO 0
+#define SWB_DOMAIN_LOG 1
+#define SWB_DOMAIN_LINEAR 2
 
 /* Workspace bytes for swb_sw_affine_forward on a [B, L1max, L2max] batch. */
 size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max);

@@ -12,7 +12,9 @@ import os
 
 _SO = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_swb.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
+
+DOMAIN_AUTO, DOMAIN_LOG, DOMAIN_LINEAR = 0, 1, 2
 
 OK = 0
 ERR_ARG = -1
@@ -31,6 +33,7 @@ class Options(ctypes.Structure):
         ("fault_inject", ctypes.c_int),
         ("split_event", ctypes.c_void_p),
         ("cols_per_lane", ctypes.c_int),
+        ("domain", ctypes.c_int),
     ]
 
 

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "sw_kernels.cu"
+#include "sw_lin.cu"
 #include "sw_xband.cu"
 #include "sw_prelude.cuh"
 #include "sw_probe.cuh"
@@ -36,8 +37,8 @@ constexpr size_t kAlign = 256;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
-template <int NS, int G = 0> constexpr int np() { return swb::push_channels<NS, G>(); }
-template <int NS, int R> constexpr int ckrs() { return swb::Dims<NS, R>::CKRS; }
+template <int NS, int G = 0> constexpr int np() { return swb::push_fields<NS, G>(); }
+template <int NS, int R> constexpr int ckrs() { return swb::ck_record_floats<NS, R>(); }
 template <int NS, int R> constexpr int ne() { return swb::Dims<NS, R>::NE; }
 
 bool valid_r(int r) { return r == 2 || r == 4; }
@@ -104,6 +105,7 @@ size_t plan_bytes_for(long long B, long long ntasks) {
 struct DevInfo {
   int sms = 0;
   int occ[2][5][2] = {};   // [kernel fwd/bwd][model_index][R == 4?]
+  int locc[2][2][2] = {};  // linear-domain kernels: [fwd/bwd][NS == 3?][R == 4?]
   bool ready = false;
 };
 DevInfo g_dev[64];
@@ -115,6 +117,23 @@ size_t bwd_smem() { return (size_t)kWarpsBwd * swb::bwd_smem_floats<NS, R>() * s
 // occupancy slots: linear, affine, global linear, global affine, Saigo-Vert
 template <int NS, int G> constexpr int model_index() {
   return NS == 3 ? (G == 1 ? 3 : (G == 2 ? 4 : 1)) : (G == 1 ? 2 : 0);
+}
+
+template <int NS, int R>
+size_t lbwd_smem() { return (size_t)kWarpsBwd * swb::lbwd_smem_floats<NS, R>() * sizeof(float); }
+
+template <int NS, int R>
+cudaError_t setup_lin(DevInfo& d) {
+  cudaError_t e = cudaFuncSetAttribute(swb::lbwd_kernel<NS, R, kWarpsBwd>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)lbwd_smem<NS, R>());
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.locc[0][NS == 3][R == 4],
+                                                    swb::lfwd_kernel<NS, R>, 32 * kWarpsFwd, 0);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &d.locc[1][NS == 3][R == 4], swb::lbwd_kernel<NS, R, kWarpsBwd>, 32 * kWarpsBwd,
+      lbwd_smem<NS, R>());
 }
 
 template <int NS, int R, int G = 0>
@@ -142,7 +161,8 @@ int dev_info(DevInfo** out) {
       return SWB_ERR_CUDA;
     if (setup_pair<1, 2>(d) || setup_pair<1, 4>(d) || setup_pair<3, 2>(d) || setup_pair<3, 4>(d) ||
         setup_pair<1, 2, 1>(d) || setup_pair<1, 4, 1>(d) || setup_pair<3, 2, 1>(d) ||
-        setup_pair<3, 4, 1>(d) || setup_pair<3, 2, 2>(d) || setup_pair<3, 4, 2>(d))
+        setup_pair<3, 4, 1>(d) || setup_pair<3, 2, 2>(d) || setup_pair<3, 4, 2>(d) ||
+        setup_lin<1, 2>(d) || setup_lin<1, 4>(d) || setup_lin<3, 2>(d) || setup_lin<3, 4>(d))
       return SWB_ERR_CUDA;
     d.ready = true;
   }
@@ -189,6 +209,14 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   a.ckpt = value_only ? nullptr : reinterpret_cast<float*>(w + l.off_ckpt);
   a.spin_limit_ns = (opt && opt->spin_limit_ns) ? opt->spin_limit_ns : 20ull * 1000000000ull;
   a.fault_inject = opt ? opt->fault_inject : 0;
+  // the local models run in the scaled linear domain (sw_lin.cu) when every
+  // transition factor 2^(gap k) is at most 1, else in the log domain
+  const double xo = (double)a.go * (double)a.k, xe = NS == 3 ? (double)a.ge * (double)a.k : 0.0;
+  const int domain = opt ? opt->domain : SWB_DOMAIN_AUTO;
+  const bool lin = G == 0 && domain != SWB_DOMAIN_LOG && xo <= 0.0 && xe <= 0.0;
+  if (G == 0 && domain == SWB_DOMAIN_LINEAR && !lin) return SWB_ERR_ARG;
+  a.xgo = (float)exp2(xo);
+  a.xge = (float)exp2(xe);
 
   // per-call resets: counters, status and completion counts to 0, cross-band
   // buffers to the NaN sentinel, the map to 0 (cells outside lengths stay 0)
@@ -199,7 +227,8 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
     return SWB_ERR_CUDA;
 
   constexpr int m = model_index<NS, G>();
-  const int of = d->occ[0][m][R == 4], ob = d->occ[1][m][R == 4];
+  const int of = lin ? d->locc[0][NS == 3][R == 4] : d->occ[0][m][R == 4];
+  const int ob = lin ? d->locc[1][NS == 3][R == 4] : d->occ[1][m][R == 4];
   const int cta_cap_f = d->sms * (of > 0 ? of : 1);
   const int cta_cap_b = d->sms * (ob > 0 ? ob : 1);
   const long long need_f = (ntasks + kWarpsFwd - 1) / kWarpsFwd;
@@ -212,6 +241,21 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   }
   if (grid_f < 1) grid_f = 1;
   if (grid_b < 1) grid_b = 1;
+  if (lin) {
+    if constexpr (G == 0) {
+      swb::lfwd_kernel<NS, R><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
+      if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
+      if (opt && opt->split_event &&
+          cudaEventRecord(reinterpret_cast<cudaEvent_t>(opt->split_event), st) != cudaSuccess)
+        return SWB_ERR_CUDA;
+      if (value_only) {
+        swb::lvalue_kernel<NS, R><<<(a.B + 3) / 4, 128, 0, st>>>(a);
+        return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+      }
+      swb::lbwd_kernel<NS, R, kWarpsBwd><<<grid_b, 32 * kWarpsBwd, lbwd_smem<NS, R>(), st>>>(a);
+      return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+    }
+  }
   swb::fwd_kernel<NS, R, G><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
   if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   if (opt && opt->split_event &&
@@ -794,8 +838,11 @@ int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const lon
   if ((family < 1 || family > 5) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
     return SWB_ERR_ARG;
   const int ns = (family >= 3) ? 3 : 1;
-  const int NE = 2 * ns, NP = family >= 4 ? 6 : (ns == 3 ? 5 : 2);
-  const int CKRS = (2 * ns * R + 2 * ns) * 32 + 4;
+  const int NE = 2 * ns;
+  const int NP = family >= 4 ? swb::push_fields<3, 1>()
+                             : (ns == 3 ? swb::push_fields<3, 0>() : swb::push_fields<1, 0>());
+  const int CKRS = ns == 3 ? (R == 2 ? swb::ck_record_floats<3, 2>() : swb::ck_record_floats<3, 4>())
+                           : (R == 2 ? swb::ck_record_floats<1, 2>() : swb::ck_record_floats<1, 4>());
   // validate the packing: row pitch round4(L2), offsets multiples of 4 floats
   long long ntasks = 0;
   for (int b = 0; b < B; ++b) {

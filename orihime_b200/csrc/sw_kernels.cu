@@ -148,10 +148,24 @@ template <int NS, int GM> __host__ __device__ constexpr int push_channels() {
 template <int NS, int GM> __host__ __device__ constexpr int push_left() {
   return NS == 3 ? (GM ? 3 : 2) : 1;
 }
+// Floats per row of a band's push buffer in the workspace: the push channels
+// of the log-domain adjoint, or the 3 fields (beta_D or beta, t, frame) the
+// linear-domain adjoint of the local models passes, whichever is more.
+template <int NS, int GM> __host__ __device__ constexpr int push_fields() {
+  return push_channels<NS, GM>() > 3 ? push_channels<NS, GM>() : 3;
+}
+// Floats of one checkpoint chunk record: the larger of the log-domain record
+// (double-float values) and the linear-domain one (sw_lin.cu), so one
+// workspace layout serves both kernel families.
+template <int NS, int R> __host__ __device__ constexpr int ck_record_floats() {
+  constexpr int lg = (2 * NS * R + 2 * NS) * 32 + 4;
+  constexpr int lv = ((NS * R + NS + 3 + 3) / 4 * 4) * 32 + 4;
+  return lg > lv ? lg : lv;
+}
 
 template <int NS, int R, int GM = 0>
 __device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_band) {
-  constexpr int NE = 2 * NS, NP = push_channels<NS, GM>(), CKRS = (2 * NS * R + 2 * NS) * 32 + 4;
+  constexpr int NE = 2 * NS, NP = push_fields<NS, GM>(), CKRS = ck_record_floats<NS, R>();
   Place w;
   Pair& r = w.pr;
   if (a.layout == 0) {

@@ -93,6 +93,7 @@ struct Args {
   int B, Lmax1, Lmax2;
   int layout;                 // 0 padded, 1 ragged packed via plan (row pitch = round4(L2))
   float go, ge, T, k;         // gaps in natural units, temperature, k = log2(e)/T
+  float xgo, xge;             // linear-domain kernels: transition factors 2^(go k), 2^(ge k)
   int nb;                     // bands per pair (uniform, >= ceil(max L2 / 32R))
   int nchunks;                // checkpoint chunks per band (>= ceil((max L1+31)/C))
   // outputs [B]

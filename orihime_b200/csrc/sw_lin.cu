@@ -1,0 +1,866 @@
+// Soft Smith-Waterman forward / adjoint in the scaled linear domain (sm_100a),
+// local alignment with linear or affine gaps.  Compiled as part of sw_capi.cu
+// after sw_kernels.cu, whose band decomposition, task queue, cross-band
+// buffers, polling and pair finish this file reuses.
+//
+// Why a linear domain
+// -------------------
+// Every term of the reference recurrence is positive, so instead of
+// log-sum-exp over scaled log values (one ex2 per term, one lg2 per state:
+// 14 MUFU ops per affine cell forward, 15 more in the adjoint) the DP can run
+// on the exponentials themselves.  With E = 2^(s k) (k = log2(e) / T),
+// G_o = 2^(go k), G_e = 2^(ge k) the local affine recurrence of
+// src/sw_affine/kernels_cpu.cpp:94-196 becomes
+//     M[i,j] = E[i,j] * (M + I + D)[i-1,j-1] + E[i,j]      (the "+ E": a fresh start)
+//     I[i,j] = G_o * M[i-1,j] + G_e * I[i-1,j]
+//     D[i,j] = G_o * M[i,j-1] + G_e * D[i,j-1]
+//     Z      = 1 + sum over all cells and states,  S = T ln Z,
+// and the linear one (src/sw/kernels_cpu.cpp:70-160)
+//     A[i,j] = E[i,j] * (A[i-1,j-1] + 1) + G (A[i-1,j] + A[i,j-1]).
+// The adjoint is the outside recursion beta = dZ/d(cell) over the successors,
+//     beta_M = 1 + t(i+1,j+1) + G_o (beta_I(i+1,j) + beta_D(i,j+1)),  t = E * beta_M,
+//     beta_I = 1 + t(i+1,j+1) + G_e beta_I(i+1,j),   beta_D = 1 + t + G_e beta_D(i,j+1),
+// with the map P = M beta_M / Z (linear: E (A_diag + 1) beta / Z) and the
+// parameter gradients as expected transition counts.  One ex2 per cell
+// (the emission E), the rest multiply-adds.
+//
+// Range
+// -----
+// Values span far more than fp32's exponent range, so each lane keeps its R
+// columns of a row as float mantissas under one power-of-two frame:
+// value = m * 2^e.  A step computes its row in the frame et = max of its
+// inputs' normalised frames (the lane's previous row, the left lane's row and
+// the left lane's previous row), which makes every converted input <= 1;
+// then the row maximum gives the normalised frame n = et + exponent(max) in
+// which the row is <= 1.  Rows are never rescaled: the raw values keep the
+// compute frame et and every use scales them by 2^(frame - target) (a
+// power-of-two factor built from the exponent bits, folded into the gap
+// factors).  Frames are floored at 0: the empty alignment's weight 1 is
+// always representable and Z >= 1, so values below 2^-149 of it are dropped,
+// as the reference drops exponentials below e^-88 of their LSE's maximum.
+// Scores are within |s|/T <= 80 (the host's domain check), so E <= 2^115.4
+// and a step's raw values stay below 2^122.
+//
+// The kernels run when every transition factor is at most 1 (gaps <= 0);
+// otherwise the host uses the log-domain kernels of sw_kernels.cu.
+#include "sw_kernels.cuh"
+
+namespace swb {
+
+// 2^d for an integer d <= 127 (0 for d < -126): frame conversion factors.
+// Conversions go to a frame at least as large as the source's normalised
+// frame, so d <= 126 always (a raw value's frame exceeds its normalised frame
+// by at most 126, when the values are below 1).
+__device__ __forceinline__ float p2i(int d) {
+  d = max(d, -127);
+  return __int_as_float((d + 127) << 23);
+}
+// 2^d for any integer d, saturated to [0, 2^127].
+__device__ __forceinline__ float p2any(int d) {
+  d = min(max(d, -127), 127);
+  return __int_as_float((d + 127) << 23);
+}
+// Upper bound k of log2 of a non-negative float: m <= 2^k, tight within a
+// factor 2 for normal m (0 and subnormals give -126).
+__device__ __forceinline__ int fexp(float m) {
+  return (int)((__float_as_uint(m) >> 23) & 0xffu) - 126;
+}
+
+constexpr float XMAX = 118.f;   // scaled scores above this are clamped (|s|/T <= 80 gives 115.4)
+
+// Checkpoint floats per lane (LCKF, padded to float4), chunk record floats
+// (LCKRS: checkpoint groups, then the chunk's largest normalised frame, then
+// padding) and adjoint shared-memory floats per lane per step (LFW).
+template <int NS, int R> struct LDims {
+  static constexpr int CKV = NS * R + NS + 3;          // raw row, left values, e, n, nl
+  static constexpr int CKF = (CKV + 3) / 4 * 4;
+  static constexpr int CK4 = CKF / 4;
+  static constexpr int CKRS = CKF * 32 + 4;
+  // affine: M, I, D (raw) and the scaled score per column; linear: A, the
+  // emission part E (A_diag + 1), and the scaled score; then e and n
+  static constexpr int NF = NS == 3 ? 4 : 3;
+  static constexpr int FW = NF * R + 2;
+};
+
+// Lane state of the forward wavefront.
+template <int NS, int R> struct LState {
+  float v[NS][R];   // raw values of the lane's latest row (frame e)
+  float lv[NS];     // the left lane's latest row, last column (normalised frame nl)
+  float vs[NS];     // the lane's last column in its normalised frame n
+  int e, n, nl;
+};
+
+template <int NS, int R>
+__device__ __forceinline__ void lstate_zero(LState<NS, R>& s) {
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    s.lv[q] = 0.f; s.vs[q] = 0.f;
+#pragma unroll
+    for (int c = 0; c < R; ++c) s.v[q][c] = 0.f;
+  }
+  s.e = 0; s.n = 0; s.nl = 0;
+}
+
+template <int NS, int R>
+__device__ __forceinline__ void lck_store(float* rec, int lane, const LState<NS, R>& s) {
+  using L = LDims<NS, R>;
+  float x[L::CKF];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+#pragma unroll
+    for (int c = 0; c < R; ++c) x[q * R + c] = s.v[q][c];
+    x[NS * R + q] = s.lv[q];
+  }
+  x[NS * R + NS] = __int_as_float(s.e);
+  x[NS * R + NS + 1] = __int_as_float(s.n);
+  x[NS * R + NS + 2] = __int_as_float(s.nl);
+#pragma unroll
+  for (int f = L::CKV; f < L::CKF; ++f) x[f] = 0.f;
+#pragma unroll
+  for (int g = 0; g < L::CK4; ++g)
+    reinterpret_cast<float4*>(rec + g * 128)[lane] = make_float4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
+}
+
+template <int NS, int R>
+__device__ __forceinline__ void lck_load(const float* rec, int lane, float (&x)[LDims<NS, R>::CKF]) {
+  using L = LDims<NS, R>;
+#pragma unroll
+  for (int g = 0; g < L::CK4; ++g) {
+    const float4 y = reinterpret_cast<const float4*>(rec + g * 128)[lane];
+    x[4 * g] = y.x; x[4 * g + 1] = y.y; x[4 * g + 2] = y.z; x[4 * g + 3] = y.w;
+  }
+}
+
+template <int NS, int R>
+__device__ __forceinline__ void lck_unpack(const float (&x)[LDims<NS, R>::CKF], LState<NS, R>& s) {
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+#pragma unroll
+    for (int c = 0; c < R; ++c) s.v[q][c] = x[q * R + c];
+    s.lv[q] = x[NS * R + q];
+  }
+  s.e = __float_as_int(x[NS * R + NS]);
+  s.n = __float_as_int(x[NS * R + NS + 1]);
+  s.nl = __float_as_int(x[NS * R + NS + 2]);
+  const float f = p2i(s.e - s.n);
+#pragma unroll
+  for (int q = 0; q < NS; ++q) s.vs[q] = s.v[q][R - 1] * f;
+}
+
+// One step of the forward wavefront for one lane: (xl, xn) is the left
+// lane's last column of this row (normalised frame xn), xs the scaled scores
+// (NEG where the cell does not exist).  Updates the state to this row;
+// returns the step's compute frame in `et` (the raw values' frame).
+// Affine: M, I, D; linear: A (and, for the adjoint, the emission part em).
+template <int NS, int R>
+__device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], int xn,
+                                       const float (&xs)[R], float gO, float gE, int nlive,
+                                       bool has_dead, int& et, float (&em)[R]) {
+  // diagonal inputs of column 0: the left lane's previous row
+  const int nd = s.nl;
+  float dg[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) { dg[q] = s.lv[q]; s.lv[q] = xl[q]; }
+  s.nl = xn;
+  et = max(max(s.n, xn), nd);
+  const float fU = p2i(s.e - et), fL = p2i(xn - et), fD = p2i(nd - et), st = p2i(-et);
+  float E[R];
+#pragma unroll
+  for (int c = 0; c < R; ++c) E[c] = ex2(xs[c]);
+  if constexpr (NS == 3) {
+    const float gOu = gO * fU, gEu = gE * fU, gOl = gO * fL, gEl = gE * fL;
+    float pM = dg[0], pI = dg[1], pD = dg[2], fP = fD;
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      const float oM = s.v[0][c], oI = s.v[1][c], oD = s.v[2][c];
+      const float m = E[c] * fmaf(fP, (pM + pI) + pD, st);
+      const float iv = fmaf(gOu, oM, gEu * oI);
+      const float dv = c == 0 ? fmaf(gOl, s.lv[0], gEl * s.lv[2])
+                              : fmaf(gO, s.v[0][c - 1], gE * s.v[2][c - 1]);
+      s.v[0][c] = m; s.v[1][c] = iv; s.v[2][c] = dv;
+      pM = oM; pI = oI; pD = oD; fP = fU;
+      em[c] = 0.f;
+    }
+    if (has_dead) {   // columns past the pair: D would run on from the last live column
+#pragma unroll
+      for (int c = 0; c < R; ++c)
+        if (c >= nlive) s.v[2][c] = 0.f;
+    }
+  } else {
+    const float gU = gO * fU, gL = gO * fL;
+    float pA = dg[0], fP = fD;
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      const float oA = s.v[0][c];
+      const float m = E[c] * fmaf(fP, pA, st);
+      const float left = c == 0 ? gL * s.lv[0] : gO * s.v[0][c - 1];
+      const float a = fmaf(gU, oA, m + left);
+      em[c] = m;
+      s.v[0][c] = a;
+      pA = oA; fP = fU;
+    }
+    if (has_dead) {
+#pragma unroll
+      for (int c = 0; c < R; ++c)
+        if (c >= nlive) { s.v[0][c] = 0.f; em[c] = 0.f; }
+    }
+  }
+  float mx = 0.f;
+#pragma unroll
+  for (int q = 0; q < NS; ++q)
+#pragma unroll
+    for (int c = 0; c < R; ++c) mx = fmaxf(mx, s.v[q][c]);
+  s.e = et;
+  s.n = max(et + fexp(mx), 0);
+  const float f = p2i(et - s.n);
+#pragma unroll
+  for (int q = 0; q < NS; ++q) s.vs[q] = s.v[q][R - 1] * f;
+}
+
+// Scaled scores of one step: NEG before the lane's first row and in columns
+// past the pair (E = 0 there), clamped at XMAX.
+template <int R>
+__device__ __forceinline__ void lscores(const float (&sb)[R], int i, float k, int nlive, bool has_dead,
+                                        float (&xs)[R]) {
+#pragma unroll
+  for (int c = 0; c < R; ++c) xs[c] = i >= 1 ? fminf(__fmul_rn(sb[c], k), XMAX) : NEG;
+  if (has_dead) {
+#pragma unroll
+    for (int c = 0; c < R; ++c)
+      if (c >= nlive) xs[c] = NEG;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// forward band task
+// ---------------------------------------------------------------------------
+
+// Forward wavefront of one band: per-lane partition sums (Kahan, in the
+// lane's largest normalised frame), the left-to-right edge records
+// (last column normalised, then its frame) and, every C steps, a checkpoint
+// of the lane state plus the chunk's largest normalised frame.  The band's
+// partition partial is (frame, mantissa sum): Z_band = sum * 2^frame.
+template <int NS, int R>
+__device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t deadline) {
+  using LD = LDims<NS, R>;
+  const Pair& pr = w.pr;
+  const int L1 = pr.L1, L2 = pr.L2;
+  const int band = w.band;
+  const size_t slot = w.slot0 + band;
+  const int col0 = band * 32 * R;
+  float* part = a.part + 2 * (size_t)slot;
+  if (!(L1 > 0 && col0 < L2)) {
+    if (lane == 0) { part[0] = 0.f; part[1] = (band == 0) ? 1.f : 0.f; }
+    return;
+  }
+  const int jl = col0 + lane * R;
+  const int nlive = min(max(L2 - jl, 0), R);
+  const bool has_dead = __any_sync(FULL, nlive < R);
+  const float k = a.k, gO = a.xgo, gE = a.xge;
+  const size_t Lm = (size_t)w.Lm;
+  float* eout = a.edge + w.ed0 + (size_t)band * w.edb;
+  const float* ein = (band > 0) ? eout - w.edb : nullptr;
+  const bool fault = a.fault_inject && band > 0;
+  if (fault) ein = nullptr;
+  const bool keep_ck = a.ckpt != nullptr;
+  float* ck = keep_ck ? a.ckpt + w.ck0 + (size_t)band * w.ckb : nullptr;
+  const int nch = band_chunks(L1);
+
+  LState<NS, R> s;
+  lstate_zero(s);
+  float zm = (band == 0 && lane == 0) ? 1.f : 0.f, zc = 0.f;   // M[0,0]: the empty alignment
+  int ze = 0;
+
+  // lane u < C holds the left band's edge record lane 0 needs at step u of a
+  // chunk (NS values, then the frame), loaded one chunk ahead
+  constexpr int NEF = NS + 1;
+  float eb[NEF], ebn[NEF];
+  auto load_edge = [&](int kc, float (&dst)[NEF]) {
+    const int i = kc * C_STEPS + lane + 1;
+    const bool ok = ein && lane < C_STEPS && i <= L1;
+#pragma unroll
+    for (int f = 0; f < NEF; ++f) dst[f] = ok ? ld_poll(ein + f * Lm + (i - 1)) : 0.f;
+  };
+  load_edge(0, eb);
+#pragma unroll
+  for (int f = 0; f < NEF; ++f) ebn[f] = 0.f;
+  float sb[PF][R];
+#pragma unroll
+  for (int u = 0; u < PF; ++u) {
+    const int i = u - lane + 1;
+    load_row<R>(pr, i, jl, i >= 1 && i <= L1, sb[u]);
+  }
+
+  for (int kc = 0; kc < nch; ++kc) {
+    if (keep_ck) lck_store<NS, R>(ck + (size_t)kc * LD::CKRS, lane, s);
+    int cmx = -(1 << 30);   // largest normalised frame of the lane's live rows in this chunk
+    if (kc + 1 < nch) load_edge(kc + 1, ebn);
+#pragma unroll 1
+    for (int u0 = 0; u0 < C_STEPS; u0 += PF)
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int cu = u0 + u;
+      const int t = kc * C_STEPS + cu;
+      const int i = t - lane + 1;
+      const bool act = (i >= 1) && (i <= L1);
+      float xl[NS], ev[NEF];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) xl[q] = __shfl_up_sync(FULL, s.vs[q], 1);
+      int xn = __shfl_up_sync(FULL, s.n, 1);
+#pragma unroll
+      for (int f = 0; f < NEF; ++f) ev[f] = __shfl_sync(FULL, eb[f], cu);
+      bool miss = false;
+#pragma unroll
+      for (int f = 0; f < NEF; ++f) miss |= is_sentinel(ev[f]);
+      miss = (lane == 0) && ein && act && miss;
+      if (__any_sync(FULL, miss) || fault) {
+        if (lane == 0 && fault && act) {
+          const float v = poll_value(a.never_written, ld_poll(a.never_written), deadline, a.status, 0.f);
+#pragma unroll
+          for (int f = 0; f < NEF; ++f) ev[f] = (f < NS) ? v : 0.f;
+        } else if (miss) {
+          FieldVec<NEF> x;
+#pragma unroll
+          for (int f = 0; f < NEF; ++f) x.v[f] = ev[f];
+          x = poll_fields_v<NEF, 0>(x, ein + (i - 1), Lm, deadline, a.status);
+#pragma unroll
+          for (int f = 0; f < NEF; ++f) ev[f] = x.v[f];
+        }
+      }
+      if (lane == 0) {
+        const bool take = act && (ein || fault);
+#pragma unroll
+        for (int q = 0; q < NS; ++q) xl[q] = take ? ev[q] : 0.f;
+        xn = take ? __float_as_int(ev[NS]) : 0;
+      }
+      float xs[R];
+      lscores<R>(sb[u], i, k, nlive, has_dead, xs);
+      {
+        const int ip = i + PF;
+        load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
+      }
+      int et;
+      float em[R];
+      lcells<NS, R>(s, xl, xn, xs, gO, gE, nlive, has_dead, et, em);
+      if (act) {
+        // partition: the row's live values in the frame ze (the largest
+        // normalised frame so far), Kahan-compensated
+        float rs = 0.f;
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+          if constexpr (NS == 3) rs += (s.v[0][c] + s.v[1][c]) + s.v[2][c];
+          else rs += s.v[0][c];
+        }
+        if (s.n > ze) {
+          const float f = p2i(ze - s.n);
+          zm *= f; zc *= f; ze = s.n;
+        }
+        const float y = rs * p2i(et - ze) - zc;
+        const float tt = zm + y;
+        zc = (tt - zm) - y;
+        zm = tt;
+        cmx = max(cmx, s.n);
+        if (lane == 31) {
+#pragma unroll
+          for (int q = 0; q < NS; ++q) eout[q * Lm + (i - 1)] = s.vs[q];
+          eout[NS * Lm + (i - 1)] = __int_as_float(s.n);
+        }
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < NEF; ++f) eb[f] = ebn[f];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cmx = max(cmx, __shfl_xor_sync(FULL, cmx, o));
+    if (keep_ck && lane == 0) ck[(size_t)kc * LD::CKRS + LD::CKF * 32] = __int_as_float(cmx);
+  }
+  // warp-combine (frame, sum) pairs, fixed shuffle tree
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const int z2 = __shfl_xor_sync(FULL, ze, o);
+    const float m2 = __shfl_xor_sync(FULL, zm, o);
+    const int m = max(ze, z2);
+    zm = zm * p2i(ze - m) + m2 * p2i(z2 - m);
+    ze = m;
+  }
+  if (lane == 0) { part[0] = (float)ze; part[1] = zm; }
+}
+
+template <int NS, int R>
+__global__ void __launch_bounds__(128) lfwd_kernel(Args a) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t deadline = gtimer() + a.spin_limit_ns;
+  const int ntasks = (a.layout == 0) ? a.B * a.nb : a.ntasks;
+  while (true) {
+    int task = 0;
+    if (lane == 0) task = (int)atomicAdd(a.counters + 0, 1u);
+    task = __shfl_sync(FULL, task, 0);
+    if (task >= ntasks) break;
+    lfwd_band<NS, R>(a, place_of<NS, R>(a, task, false), lane, deadline);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// partition of a pair
+// ---------------------------------------------------------------------------
+
+// Z of pair w as (integer frame ze, mantissa zm): Z = zm * 2^ze, combined
+// from the band partials in a fixed order (deterministic).
+__device__ __forceinline__ void lpair_z(const Args& a, const Place& w, int lane, int& ze, float& zm) {
+  int ref = 0;
+  float s = 0.f;
+  for (int b = lane; b < w.nb; b += 32) {
+    const float* q = a.part + 2 * (w.slot0 + b);
+    const int r2 = (int)q[0];
+    const float s2 = q[1];
+    if (s2 > 0.f) {
+      const int m = max(ref, r2);
+      s = s * p2i(ref - m) + s2 * p2i(r2 - m);
+      ref = m;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const int r2 = __shfl_xor_sync(FULL, ref, o);
+    const float s2 = __shfl_xor_sync(FULL, s, o);
+    const int m = max(ref, r2);
+    s = s * p2i(ref - m) + s2 * p2i(r2 - m);
+    ref = m;
+  }
+  ze = ref;
+  zm = s;
+}
+
+// S' = log2 Z as a double-float (Sh, Sl): the integer part joins the frame
+// exactly and lg2 sees only the mantissa.
+__device__ __forceinline__ void lz_log2(int ze, float zm, float& Sh, float& Sl) {
+  const unsigned bits = __float_as_uint(zm);
+  const int e = (int)((bits >> 23) & 0xffu) - 127;
+  if (zm > 0.f && e > -127 && e < 128) {
+    float h, l;
+    two_sum((float)ze, (float)e, h, l);
+    Sh = h;
+    Sl = l + lg2(__uint_as_float((bits & 0x7fffffu) | 0x3f800000u));
+  } else {
+    Sh = (float)ze;
+    Sl = lg2(zm);
+  }
+}
+
+// Value-only calls: one warp per pair folds the band partials into S.
+template <int NS, int R>
+__global__ void __launch_bounds__(128) lvalue_kernel(Args a) {
+  const int lane = threadIdx.x & 31;
+  const int q = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (q >= a.B) return;
+  Place w;
+  if (a.layout == 0) {
+    w = place_of<NS, R>(a, q * a.nb, false);
+  } else {
+    const long long* pw = a.plan_pairs + (size_t)q * PLAN_PAIR_WORDS;
+    w.p = q;
+    w.nb = (int)pw[PW_NB];
+    w.slot0 = (size_t)pw[PW_SLOT0];
+  }
+  int ze;
+  float zm, Sh, Sl;
+  lpair_z(a, w, lane, ze, zm);
+  lz_log2(ze, zm, Sh, Sl);
+  if (lane == 0) a.value[w.p] = (Sh + Sl) * (1.f / a.k);
+}
+
+// ---------------------------------------------------------------------------
+// adjoint band task
+// ---------------------------------------------------------------------------
+
+// Shared memory per adjoint warp (floats): one chunk of recomputed fields.
+template <int NS, int R>
+__host__ __device__ constexpr int lbwd_smem_floats() {
+  return C_STEPS * LDims<NS, R>::FW * 32;
+}
+
+// Per band, checkpoint chunks in reverse.  Each chunk restores its checkpoint
+// and recomputes C steps of the forward, keeping every cell's raw values and
+// scaled score (and each step's frames) in shared memory; then the outside
+// recursion runs the same C steps backwards.  Lane l + 1 is one step ahead of
+// lane l (it processes row i one step earlier); a lane receives from its right
+// neighbour that row's beta_D (beta, linear) of column 0 in the neighbour's
+// normalised frame, its t = E beta_M of column 0 and the frame, and holds
+// the t for one more step (it is the diagonal successor of the next row).
+// Lane 0 passes the same three values to the left band through the push
+// buffer; lane 31 reads the right band's.  No atomics; the map is written row
+// by row; the gradient sums are folded per pair in band order.
+template <int NS, int R>
+__device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, uint64_t deadline) {
+  using LD = LDims<NS, R>;
+  constexpr int CKF = LD::CKF, CKRS = LD::CKRS, FW = LD::FW, NEF = NS + 1, NPF = 3;
+  const Pair& pr = w.pr;
+  const int L1 = pr.L1, L2 = pr.L2;
+  const int band = w.band;
+  const int col0 = band * 32 * R;
+  int ze;
+  float zm, Sh, Sl;
+  lpair_z(a, w, lane, ze, zm);
+  lz_log2(ze, zm, Sh, Sl);
+  if (!(L1 > 0 && col0 < L2)) {
+    finish_pair<NS>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f);
+    return;
+  }
+  const float invZ = 1.f / zm;
+  const int jl = col0 + lane * R;
+  const int nlive = min(max(L2 - jl, 0), R);
+  const bool has_dead = __any_sync(FULL, nlive < R);
+  const float k = a.k, gO = a.xgo, gE = a.xge;
+  const size_t Lm = (size_t)w.Lm;
+  const float* ein = (band > 0) ? a.edge + w.ed0 + (size_t)(band - 1) * w.edb : nullptr;
+  float* pout = (band > 0) ? a.bpush + w.bp0 + (size_t)band * w.bpb : nullptr;
+  const bool right_live = (col0 + 32 * R) < L2 && (band + 1) < w.nb;
+  const float* pin = right_live ? a.bpush + w.bp0 + (size_t)(band + 1) * w.bpb : nullptr;
+  const float* ck = a.ckpt + w.ck0 + (size_t)band * w.ckb;
+  const int nch = band_chunks(L1);
+
+  // ---- chunk-ahead prefetch state ----
+  float ckr[CKF];          // checkpoint of the next chunk to recompute
+  int ckm;                 // ... and the chunk's largest normalised alpha frame
+  float ebr[NEF];          // lane u < C: left-band edge record of lane 0's row at recompute step u
+  float pbc[NPF], pbn[NPF];// lane u < C: right-band record lane 31 needs at backward step u
+  float sb[PF][R];         // per-lane scores of the first PF recompute steps
+  auto load_ck = [&](int kc) {
+    lck_load<NS, R>(ck + (size_t)kc * CKRS, lane, ckr);
+    ckm = __float_as_int(ck[(size_t)kc * CKRS + CKF * 32]);
+  };
+  auto load_eb = [&](int kc) {
+    const int i = kc * C_STEPS + lane + 1;
+    const bool ok = ein && lane < C_STEPS && i <= L1;
+#pragma unroll
+    for (int f = 0; f < NEF; ++f) ebr[f] = ok ? ein[f * Lm + (i - 1)] : 0.f;
+  };
+  auto load_pb = [&](int kc, float (&dst)[NPF]) {
+    const int i = kc * C_STEPS + C_STEPS - 1 - lane - 30;   // lane 31's row at backward step lane
+    const bool ok = pin && lane < C_STEPS && i >= 1 && i <= L1;
+#pragma unroll
+    for (int f = 0; f < NPF; ++f) dst[f] = ok ? ld_poll(pin + f * (Lm + 1) + i) : 0.f;
+  };
+  auto load_sb = [&](int kc) {
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int i = kc * C_STEPS + u - lane + 1;
+      load_row<R>(pr, i, jl, i >= 1 && i <= L1, sb[u]);
+    }
+  };
+  load_ck(nch - 1);
+  load_eb(nch - 1);
+  load_sb(nch - 1);
+  load_pb(nch - 1, pbc);
+#pragma unroll
+  for (int f = 0; f < NPF; ++f) pbn[f] = 0.f;
+
+  // ---- outside-recursion state: the row below (raw beta_I / beta in frame
+  // fb, t = E beta_M in frame nb), the right neighbour's held t and frame,
+  // and this lane's outputs of its latest row (for the left neighbour) ----
+  float bdn[R], tdn[R];
+#pragma unroll
+  for (int c = 0; c < R; ++c) { bdn[c] = 0.f; tdn[c] = 0.f; }
+  int fb = 0, nb = 0;
+  float ht = 0.f;
+  int hn = 0;
+  float o_b = 0.f, o_t = 0.f;
+  int o_n = 0;
+  KSum gA, gB, gS;
+
+  // log2 of Z is at least zlog; a chunk is quiet (below) when every cell's
+  // posterior and every flow out of it is below 2^-60
+  const int zlog = ze + fexp(zm) - 1;
+  for (int kc = nch - 1; kc >= 0; --kc) {
+    const int t0 = kc * C_STEPS;
+    // ---- quiet chunk.  For a cell u of the chunk, alpha_u beta_u / Z sums,
+    // over the chunk cells x where u's continuations stay inside, terms
+    // alpha_x (1 + w beta_out) / Z (alpha_u W(u -> x) <= alpha_x: all weights
+    // are positive), where beta_out are the successors outside the chunk: the
+    // row below, the right neighbour's held t and, for lane 31, the right
+    // band's records.  With at most 2^9 cells, alpha_x <= 2^ckm and
+    // 1 + w beta_out <= 4 max(1, inflow), every posterior in the chunk and
+    // every flow across its top and left edges is below 2^-60 when
+    // ckm + 11 + max(log2 inflow, 0) < log2 Z - 60.  Such a chunk writes zero
+    // map rows and zero records to the left band, and passes zero beta up:
+    // the flows it drops are among those bounded.  The right band's records
+    // are resolved first, so the decision does not depend on timing. ----
+    {
+      {
+        bool miss = false;
+#pragma unroll
+        for (int f = 0; f < NPF; ++f) miss |= is_sentinel(pbc[f]);
+        if (__any_sync(FULL, miss) && miss) {
+          const int ir = kc * C_STEPS + C_STEPS - 1 - lane - 30;   // as in load_pb
+          FieldVec<NPF> x;
+#pragma unroll
+          for (int f = 0; f < NPF; ++f) x.v[f] = pbc[f];
+          x = poll_fields_v<NPF, 0>(x, pin + ir, Lm + 1, deadline, a.status);
+#pragma unroll
+          for (int f = 0; f < NPF; ++f) pbc[f] = x.v[f];
+        }
+      }
+      int inl = hn + fexp(ht);
+#pragma unroll
+      for (int c = 0; c < R; ++c) inl = max(inl, max(fb + fexp(bdn[c]), nb + fexp(tdn[c])));
+      if (lane < C_STEPS) {
+        const int pn = __float_as_int(pbc[2]);
+        inl = max(inl, pn + fexp(fmaxf(pbc[0], pbc[1])));
+      }
+      const bool ok = ckm + 11 + max(inl, 0) < zlog - 60;
+      if (__all_sync(FULL, ok)) {
+        float z[R];
+#pragma unroll
+        for (int c = 0; c < R; ++c) z[c] = 0.f;
+        for (int cu = 0; cu < C_STEPS; ++cu) {
+          const int i = t0 + cu - lane + 1;
+          if (i >= 1 && i <= L1) {
+            store_row<R>(pr, i, jl, z);
+            if (lane == 0 && pout) {
+              pout[0 * (Lm + 1) + i] = 0.f;
+              pout[1 * (Lm + 1) + i] = 0.f;
+              pout[2 * (Lm + 1) + i] = 0.f;
+            }
+          }
+        }
+        // the row above the chunk sees zero beta; lane 31 keeps the right
+        // band's t of its top chunk row as the held diagonal successor
+        const float pt = __shfl_sync(FULL, pbc[1], C_STEPS - 1);
+        const int pn = __shfl_sync(FULL, __float_as_int(pbc[2]), C_STEPS - 1);
+#pragma unroll
+        for (int c = 0; c < R; ++c) { bdn[c] = 0.f; tdn[c] = 0.f; }
+        fb = 0; nb = 0;
+        o_b = 0.f; o_t = 0.f; o_n = 0;
+        ht = lane == 31 ? pt : 0.f;
+        hn = lane == 31 ? pn : 0;
+        if (kc > 0) {
+          load_ck(kc - 1);
+          load_eb(kc - 1);
+          load_sb(kc - 1);
+          load_pb(kc - 1, pbc);
+        }
+        continue;
+      }
+    }
+    // ---- restore the checkpoint and recompute the chunk ----
+    LState<NS, R> st;
+    lck_unpack<NS, R>(ckr, st);
+#pragma unroll 1
+    for (int u0 = 0; u0 < C_STEPS; u0 += PF)
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int cu = u0 + u;
+      const int t = t0 + cu;
+      const int i = t - lane + 1;
+      const bool act = (i >= 1) && (i <= L1);
+      float xl[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) xl[q] = __shfl_up_sync(FULL, st.vs[q], 1);
+      int xn = __shfl_up_sync(FULL, st.n, 1);
+      float ev[NEF];
+#pragma unroll
+      for (int f = 0; f < NEF; ++f) ev[f] = __shfl_sync(FULL, ebr[f], cu);
+      if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NS; ++q) xl[q] = act ? ev[q] : 0.f;
+        xn = act ? __float_as_int(ev[NS]) : 0;
+      }
+      float xs[R];
+      lscores<R>(sb[u], i, k, nlive, has_dead, xs);
+      if (cu + PF < C_STEPS) {
+        const int ip = i + PF;
+        load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
+      }
+      int et;
+      float em[R];
+      lcells<NS, R>(st, xl, xn, xs, gO, gE, nlive, has_dead, et, em);
+      float* ent = sm + (size_t)cu * FW * 32;
+      if constexpr (R == 4) {
+        reinterpret_cast<float4*>(ent)[lane] = make_float4(st.v[0][0], st.v[0][1], st.v[0][2], st.v[0][3]);
+        if constexpr (NS == 3) {
+          reinterpret_cast<float4*>(ent + 128)[lane] = make_float4(st.v[1][0], st.v[1][1], st.v[1][2], st.v[1][3]);
+          reinterpret_cast<float4*>(ent + 256)[lane] = make_float4(st.v[2][0], st.v[2][1], st.v[2][2], st.v[2][3]);
+        } else {
+          reinterpret_cast<float4*>(ent + 128)[lane] = make_float4(em[0], em[1], em[2], em[3]);
+        }
+        reinterpret_cast<float4*>(ent + (LD::NF - 1) * 128)[lane] = make_float4(xs[0], xs[1], xs[2], xs[3]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+          ent[(0 * R + c) * 32 + lane] = st.v[0][c];
+          if constexpr (NS == 3) {
+            ent[(1 * R + c) * 32 + lane] = st.v[1][c];
+            ent[(2 * R + c) * 32 + lane] = st.v[2][c];
+          } else {
+            ent[(1 * R + c) * 32 + lane] = em[c];
+          }
+          ent[((LD::NF - 1) * R + c) * 32 + lane] = xs[c];
+        }
+      }
+      ent[LD::NF * R * 32 + lane] = __int_as_float(et);
+      ent[LD::NF * R * 32 + 32 + lane] = __int_as_float(st.n);
+    }
+    if (kc > 0) {   // prefetch the next chunk's inputs while the outside recursion runs
+      load_ck(kc - 1);
+      load_eb(kc - 1);
+      load_sb(kc - 1);
+      load_pb(kc - 1, pbn);
+    }
+    __syncwarp();
+    float cA = 0.f, cB = 0.f, cS = 0.f;   // this chunk's plain sums
+    // ---- outside recursion over the chunk, last step first ----
+#pragma unroll 1
+    for (int cu = 0; cu < C_STEPS; ++cu) {
+      const int ent_i = C_STEPS - 1 - cu;
+      const int t = t0 + ent_i;
+      const int i = t - lane + 1;
+      const bool act = (i >= 1) && (i <= L1);
+      const float* ent = sm + (size_t)ent_i * FW * 32;
+      // the right neighbour's latest row (row i): beta_D / beta of its column
+      // 0, its t and frame; lane 31 takes the right band's record of row i
+      float rb = __shfl_down_sync(FULL, o_b, 1);
+      float rt = __shfl_down_sync(FULL, o_t, 1);
+      int rn = __shfl_down_sync(FULL, o_n, 1);
+      {
+        float pw[NPF];
+#pragma unroll
+        for (int f = 0; f < NPF; ++f) pw[f] = __shfl_sync(FULL, pbc[f], cu);
+        bool miss = false;
+#pragma unroll
+        for (int f = 0; f < NPF; ++f) miss |= is_sentinel(pw[f]);
+        miss = miss && (lane == 31);
+        if (__any_sync(FULL, miss) && miss) {
+          FieldVec<NPF> x;
+#pragma unroll
+          for (int f = 0; f < NPF; ++f) x.v[f] = pw[f];
+          x = poll_fields_v<NPF, 0>(x, pin + i, Lm + 1, deadline, a.status);
+#pragma unroll
+          for (int f = 0; f < NPF; ++f) pw[f] = x.v[f];
+        }
+        if (lane == 31) { rb = pw[0]; rt = pw[1]; rn = __float_as_int(pw[2]); }
+      }
+      // frames: the row is computed in ft >= every input's normalised frame
+      const int ft = max(max(nb, rn), hn);
+      const float fBd = p2i(fb - ft), fTd = p2i(nb - ft), fR = p2i(rn - ft), fH = p2i(hn - ft);
+      const float st1 = p2i(-ft);
+      const int ea = __float_as_int(ent[LD::NF * R * 32 + lane]);
+      const int na = __float_as_int(ent[LD::NF * R * 32 + 32 + lane]);
+      const float as = p2i(ea - na);                       // raw alpha -> normalised
+      const float sc = p2any(na + ft - ze) * invZ; // real alpha * beta / Z factor
+      float fa[LD::NF][R];
+      if constexpr (R == 4) {
+#pragma unroll
+        for (int g = 0; g < LD::NF; ++g) {
+          const float4 y = reinterpret_cast<const float4*>(ent + g * 128)[lane];
+          fa[g][0] = y.x; fa[g][1] = y.y; fa[g][2] = y.z; fa[g][3] = y.w;
+        }
+      } else {
+#pragma unroll
+        for (int g = 0; g < LD::NF; ++g)
+#pragma unroll
+          for (int c = 0; c < R; ++c) fa[g][c] = ent[(g * R + c) * 32 + lane];
+      }
+      const float one = act ? st1 : 0.f;
+      float br = fR * rb;   // right successor's beta_D (beta)
+      float td = fH * ht;   // diagonal successor's t
+      float nbv[R], nmv[R], pm[R];
+      float mx = 0.f, so = 0.f, sx = 0.f, sp = 0.f;
+#pragma unroll
+      for (int c = R - 1; c >= 0; --c) {
+        const float oc = c < nlive ? one : 0.f;
+        const float bd = fBd * bdn[c];   // beta_I (beta) of the cell below
+        const float base = oc + td;
+        if constexpr (NS == 3) {
+          const float sr = bd + br;
+          const float vm = fmaf(gO, sr, base);
+          const float vi = fmaf(gE, bd, base);
+          const float vd = fmaf(gE, br, base);
+          const float am = fa[0][c] * as, ai = fa[1][c] * as, ad = fa[2][c] * as;
+          const float P = fminf((am * sc) * vm, 1.f);   // a posterior: rounding may pass 1
+          pm[c] = P;
+          so = fmaf(am, sr, so);
+          sx = fmaf(ai, bd, fmaf(ad, br, sx));
+          sp = fmaf(P, fa[3][c], sp);
+          nbv[c] = vi;
+          nmv[c] = vm;
+          mx = fmaxf(fmaxf(mx, vm), fmaxf(vi, vd));
+          br = vd;
+        } else {
+          const float sr = bd + br;
+          const float vb = fmaf(gO, sr, base);
+          const float P = fminf(((fa[1][c] * as) * sc) * vb, 1.f);
+          pm[c] = P;
+          so = fmaf(fa[0][c] * as, sr, so);
+          sp = fmaf(P, fa[2][c], sp);
+          nbv[c] = vb;
+          nmv[c] = vb;
+          mx = fmaxf(mx, vb);
+          br = vb;
+        }
+        td = fTd * tdn[c];
+      }
+      // normalise: t = E beta_M in the row's normalised frame
+      const int nn = max(ft + fexp(mx), 0);
+      const float bs = p2i(ft - nn);
+#pragma unroll
+      for (int c = 0; c < R; ++c) {
+        tdn[c] = (nmv[c] * bs) * ex2(fa[LD::NF - 1][c]);
+        bdn[c] = nbv[c];
+      }
+      fb = ft;
+      nb = nn;
+      o_b = br * bs;   // column 0's beta_D (beta), normalised
+      o_t = tdn[0];
+      o_n = nn;
+      ht = rt;
+      hn = rn;
+      if constexpr (NS == 3) {
+        cA = fmaf(so * sc, gO, cA);
+        cB = fmaf(sx * sc, gE, cB);
+      } else {
+        cA = fmaf(so * sc, gO, cA);
+      }
+      cS += sp;
+      if (act) {
+        store_row<R>(pr, i, jl, pm);
+        if (lane == 0 && pout) {
+          pout[0 * (Lm + 1) + i] = o_b;
+          pout[1 * (Lm + 1) + i] = o_t;
+          pout[2 * (Lm + 1) + i] = __int_as_float(o_n);
+        }
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < NPF; ++f) pbc[f] = pbn[f];
+    gA.add(cA);
+    gB.add(cB);
+    gS.add(cS);
+    __syncwarp();
+  }
+  float v0 = gA.s, v1 = gB.s, v2 = gS.s;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 += __shfl_xor_sync(FULL, v0, o);
+    v1 += __shfl_xor_sync(FULL, v1, o);
+    v2 += __shfl_xor_sync(FULL, v2, o);
+  }
+  finish_pair<NS>(a, w, lane, Sh, Sl, v0, v1, v2);
+}
+
+template <int NS, int R, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) lbwd_kernel(Args a) {
+  extern __shared__ float smem[];
+  const int lane = threadIdx.x & 31;
+  const int wi = threadIdx.x >> 5;
+  float* sm = smem + (size_t)wi * lbwd_smem_floats<NS, R>();
+  const uint64_t deadline = gtimer() + a.spin_limit_ns;
+  const int ntasks = (a.layout == 0) ? a.B * a.nb : a.ntasks;
+  while (true) {
+    int task = 0;
+    if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
+    task = __shfl_sync(FULL, task, 0);
+    if (task >= ntasks) break;
+    lbwd_band<NS, R>(a, place_of<NS, R>(a, task, true), lane, sm, deadline);
+  }
+}
+
+}  // namespace swb

@@ -43,7 +43,7 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_abi_version_and_errors(lib):
-    assert lib.swb_abi_version() == 1
+    assert lib.swb_abi_version() == 2
     assert lib.swb_error_string(0) == b"ok"
     assert b"workspace" in lib.swb_error_string(-2)
 
