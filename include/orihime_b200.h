@@ -23,7 +23,8 @@
  *     (dS/dscores; exactly 0 outside lengths), and per-pair dS/dparameter [B].
  *   - Return value: SWB_OK or a negative SWB_ERR_* code (nothing launched).
  *     A bounded cross-warp wait that expires inside a kernel is reported in the
- *     workspace status word (swb_read_status), not by the return value.
+ *     workspace status word (swb_read_status), not by the return value, and
+ *     the affected pairs' value and gradients come back NaN.
  */
 #ifndef ORIHIME_B200_H
 #define ORIHIME_B200_H
@@ -104,13 +105,16 @@ int swb_sw_affine_forward(const float* scores, const int* lengths, int B, int L1
  *     12 x 512 x 512 or one 2048 x 2048 pair fit.
  *   - The first call on each device looks up the array's device address
  *     (cudaGetSymbolAddress, which may load the module) and sets up the
- *     kernels; make that first call before any stream capture.
+ *     kernels; make that first call before any stream capture.  The address
+ *     is cached per device and CUDA context: after cudaDeviceReset (or a
+ *     re-created primary context) the next call looks it up again.
  *   - All calls of one process on one device share the array: calls that
  *     overlap in time (on different streams, or from several host threads,
  *     without ordering) race and corrupt each other's results.  Order them on
  *     one stream.
- *   - The wait-timeout status word lives in the shared array and is not
- *     readable with swb_read_status.
+ *   - A bounded wait that expires makes the affected pairs' value and
+ *     gradients NaN; the status word in the shared array records it too and
+ *     is read with swb_static_read_status (not swb_read_status).
  * Arguments and outputs as swb_sw_affine_forward.
  */
 int swb_sw_affine_forward_static(const float* scores, const int* lengths, int B, int L1max,
@@ -390,8 +394,16 @@ int swb_scan_scores(const float* x, int B, long long per_item, float limit, floa
                     unsigned* words, float* amax, void* stream);
 
 /* Copies the workspace status word to *status (synchronises `stream`).
- * No reference counterpart: the reference synchronises inside every op. */
+ * No reference counterpart: the reference synchronises inside every op.
+ * A bounded wait that expires also shows in the results without this call:
+ * the affected pairs' value and dS/dparameters (second-order ops: their
+ * output map) are NaN. */
 int swb_read_status(const void* workspace, void* stream, unsigned* status);
+
+/* The status word of swb_sw_affine_forward_static's shared scratch on the
+ * current device (synchronises `stream`; allocates nothing).  No reference
+ * counterpart. */
+int swb_static_read_status(void* stream, unsigned* status);
 
 /* Human-readable text for a SWB_ERR_* code. */
 const char* swb_error_string(int code);

@@ -37,13 +37,20 @@ _I = ctypes.c_int
 _P = ctypes.c_void_p
 
 
+# Root of the reference sources (megure-labs/orihime) that the checkers are
+# compiled from: the environment variable ORIHIME_REFERENCE, default
+# /root/reference.  Where it is absent (a GPU box), only prebuilt checkers
+# under _ref/ are used.
+REFERENCE = os.environ.get("ORIHIME_REFERENCE", "/root/reference")
+
+
 def build(ref: bool = True) -> None:
     """Compile the oracle (and the reference CPU kernels and CUDA extension
-    when their sources exist)."""
+    when their sources exist under ``REFERENCE``)."""
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
-    if ref and os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
-        subprocess.run(["make", "-s", "-C", _HERE, "refcuda"], check=True)
+    if ref and os.path.isdir(os.path.join(REFERENCE, "src")):
+        for target in ("ref", "refcuda"):
+            subprocess.run(["make", "-s", "-C", _HERE, target, f"REF={REFERENCE}"], check=True)
 
 
 def ref_cuda_path() -> Optional[str]:

@@ -74,6 +74,8 @@ def load() -> ctypes.CDLL:
                                    ctypes.POINTER(Options)]
     lib.swb_read_status.restype = i
     lib.swb_read_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_uint)]
+    lib.swb_static_read_status.restype = i
+    lib.swb_static_read_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
     ll = ctypes.c_longlong
     lib.swb_ragged_plan.restype = i
     lib.swb_ragged_plan.argtypes = [i, i, vp, vp, i, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]

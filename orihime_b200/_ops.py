@@ -1085,6 +1085,23 @@ OWN_SCHEMAS = {
     "sv_linear_value": "sv_linear_value(Tensor scores, float gap, float temp, Tensor? lengths) -> Tensor",
     "sv_affine_value": "sv_affine_value(Tensor scores, float gap_open, float gap_ext, float temp, "
                        "Tensor? lengths) -> Tensor",
+    # value, map and dS/dparameters from ONE forward + adjoint call (the
+    # reference's forward op and its value_grad_params op each run both passes)
+    "sw_forward_with_grads": "sw_forward_with_grads(Tensor scores, float gap, float temp, "
+                             "Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
+    "sw_affine_forward_with_grads": "sw_affine_forward_with_grads(Tensor scores, float gap_open, "
+                                    "float gap_ext, float temp, Tensor? lengths) -> "
+                                    "(Tensor, Tensor, Tensor, Tensor, Tensor)",
+    "nw_forward_with_grads": "nw_forward_with_grads(Tensor scores, float gap, float temp, "
+                             "Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
+    "nw_affine_forward_with_grads": "nw_affine_forward_with_grads(Tensor scores, float gap_open, "
+                                    "float gap_ext, float temp, Tensor? lengths) -> "
+                                    "(Tensor, Tensor, Tensor, Tensor, Tensor)",
+    "sv_linear_forward_with_grads": "sv_linear_forward_with_grads(Tensor scores, float gap, float temp, "
+                                    "Tensor? lengths) -> (Tensor, Tensor, Tensor, Tensor)",
+    "sv_affine_forward_with_grads": "sv_affine_forward_with_grads(Tensor scores, float gap_open, "
+                                    "float gap_ext, float temp, Tensor? lengths) -> "
+                                    "(Tensor, Tensor, Tensor, Tensor, Tensor)",
 }
 _OWN_LIB = torch.library.Library("orihime_b200", "DEF")
 for _name, _schema in OWN_SCHEMAS.items():
@@ -1127,6 +1144,30 @@ def _own_sv_affine_value(scores, gap_open, gap_ext, temp, lengths):
 _OWN_LIB.impl("nw_affine_value", _own_nw_affine_value, "CUDA")
 _OWN_LIB.impl("sv_linear_value", _own_sv_linear_value, "CUDA")
 _OWN_LIB.impl("sv_affine_value", _own_sv_affine_value, "CUDA")
+
+
+def _own_linear_with_grads(fam):
+    def impl(scores, gap, temp, lengths):
+        ln = _prep(scores, lengths, fam)
+        if fam == "sv_linear":   # the Saigo-Vert affine model with gap_open = gap_ext = gap
+            v, m, go, ge, gT = run_affine(scores, ln, gap, gap, temp, family="sv_affine")
+            return v, m, go + ge, gT
+        v, m, gg, gT = run_linear(scores, ln, gap, temp, family=fam)
+        return v, m, gg, gT
+    return impl
+
+
+def _own_affine_with_grads(fam):
+    def impl(scores, gap_open, gap_ext, temp, lengths):
+        ln = _prep(scores, lengths, fam)
+        return run_affine(scores, ln, gap_open, gap_ext, temp, family=fam)
+    return impl
+
+
+for _fam_name in ("sw", "nw", "sv_linear"):
+    _OWN_LIB.impl(f"{_fam_name}_forward_with_grads", _own_linear_with_grads(_fam_name), "CUDA")
+for _fam_name in ("sw_affine", "nw_affine", "sv_affine"):
+    _OWN_LIB.impl(f"{_fam_name}_forward_with_grads", _own_affine_with_grads(_fam_name), "CUDA")
 
 # Meta shapes, FP32 autocast and vmap rules for the ops defined here (when the
 # reference extension defined them, its own Python package registers these).

@@ -171,17 +171,41 @@ int dev_info(DevInfo** out) {
 }
 
 // Device address of g_static_scratch on the current device, looked up once
-// per device (the first lookup may load the module on that device).
+// per device context (the first lookup may load the module on that device).
+// The cache is keyed on the current CUDA context as well as the device: a
+// device reset or a re-created primary context makes the old address
+// invalid, and the next call looks it up again.  The context comes from the
+// driver's cuCtxGetCurrent, reached through cudaGetDriverEntryPoint, so the
+// library needs no link against the driver library.
 void* g_static_ptr[64];
+void* g_static_ctx[64];
+
+using CtxGetCurrentFn = int (*)(void**);
+
+void* current_context() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 int static_scratch(void** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWB_ERR_CUDA;
+  void* ctx = current_context();   // null before the runtime first touches the device
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_static_ptr[dev]) {
-    void* p = nullptr;
+  if (!g_static_ptr[dev] || !ctx || ctx != g_static_ctx[dev]) {
+    void* p = nullptr;   // the lookup initialises the device's primary context if needed
     if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess || !p) return SWB_ERR_CUDA;
     g_static_ptr[dev] = p;
+    g_static_ctx[dev] = current_context();
   }
   *out = g_static_ptr[dev];
   return SWB_OK;
@@ -961,6 +985,14 @@ int swb_nw_ragged_value(const float* scores, const void* host_plan, const void* 
   return launch_ragged<1, 1>(scores, host_plan, dev_plan, gap, 0.f, temp, value, nullptr,
                                 nullptr, nullptr, nullptr, workspace, workspace_bytes, stream,
                                 nullptr, true);
+}
+
+int swb_static_read_status(void* stream, unsigned* status) {
+  if (!status) return SWB_ERR_ARG;
+  void* ws = nullptr;
+  const int rc = static_scratch(&ws);
+  if (rc != SWB_OK) return rc;
+  return swb_read_status(ws, stream, status);
 }
 
 int swb_read_status(const void* workspace, void* stream, unsigned* status) {

@@ -70,15 +70,29 @@ struct KSum {
 #ifndef SWB_POLL_SLEEP
 #define SWB_POLL_SLEEP 128
 #endif
+// A bounded wait that expires marks its pair: bit 31 of the pair's
+// completion word (zeroed with the workspace header at every call).  The
+// pair's finisher then writes NaN into its value and gradients (second-order
+// ops: into its output map), so a timeout shows in the results without any
+// host synchronisation; the status word records it as well.
+constexpr unsigned PAIR_TIMEOUT = 0x80000000u;
+
+__device__ __forceinline__ void mark_timeout(unsigned* status, unsigned* flag) {
+  atomicOr(status, ERR_WAIT_TIMEOUT);
+  if (flag) atomicOr(flag, PAIR_TIMEOUT);
+}
+
 // Bounded wait until none of x.v[0..N) is the sentinel, x.v[f] read from
 // base[f * stride].  Every round re-reads all missing fields together, so their
 // load latencies overlap.  The fields travel by value (the caller's values
-// need no memory address).  On timeout it records the error and substitutes
-// NEG for the missing fields f < NSV, 0 for the others.
+// need no memory address).  On timeout it records the error (status word and
+// the pair's flag) and substitutes NEG for the missing fields f < NSV, 0 for
+// the others.
 template <int N> struct FieldVec { float v[N]; };
 template <int N, int NSV>
 __device__ __noinline__ FieldVec<N> poll_fields_v(FieldVec<N> x, const float* base, size_t stride,
-                                                  uint64_t deadline, unsigned* status) {
+                                                  uint64_t deadline, unsigned* status,
+                                                  unsigned* flag) {
   while (true) {
     bool miss = false;
 #pragma unroll
@@ -88,7 +102,7 @@ __device__ __noinline__ FieldVec<N> poll_fields_v(FieldVec<N> x, const float* ba
     for (int f = 0; f < N; ++f) miss |= is_sentinel(x.v[f]);
     if (!miss) return x;
     if (gtimer() > deadline) {
-      atomicOr(status, ERR_WAIT_TIMEOUT);
+      mark_timeout(status, flag);
 #pragma unroll
       for (int f = 0; f < N; ++f)
         if (is_sentinel(x.v[f])) x.v[f] = f < NSV ? NEG : 0.f;
@@ -98,13 +112,13 @@ __device__ __noinline__ FieldVec<N> poll_fields_v(FieldVec<N> x, const float* ba
   }
 }
 
-// Bounded wait until *p is not the sentinel.  On timeout records the error and
-// returns `fallback`.
+// Bounded wait until *p is not the sentinel.  On timeout records the error
+// (status word and the pair's flag) and returns `fallback`.
 __device__ __noinline__ float poll_value(const float* p, float v, uint64_t deadline,
-                                         unsigned* status, float fallback) {
+                                         unsigned* status, unsigned* flag, float fallback) {
   while (is_sentinel(v)) {
     if (gtimer() > deadline) {
-      atomicOr(status, ERR_WAIT_TIMEOUT);
+      mark_timeout(status, flag);
       return fallback;
     }
     __nanosleep(SWB_POLL_SLEEP);
@@ -783,14 +797,15 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
       miss = (lane == 0) && ein && act && miss;
       if (__any_sync(FULL, miss) || fault) {
         if (lane == 0 && fault && act) {
-          float v = poll_value(a.never_written, ld_poll(a.never_written), deadline, a.status, NEG);
+          float v = poll_value(a.never_written, ld_poll(a.never_written), deadline, a.status,
+                               a.pair_done + w.p, NEG);
 #pragma unroll
           for (int f = 0; f < NE; ++f) ev[f] = (f < NS) ? v : 0.f;
         } else if (miss) {
           FieldVec<NE> x;
 #pragma unroll
           for (int f = 0; f < NE; ++f) x.v[f] = ev[f];
-          x = poll_fields_v<NE, NS>(x, ein + (i - 1), Lm, deadline, a.status);
+          x = poll_fields_v<NE, NS>(x, ein + (i - 1), Lm, deadline, a.status, a.pair_done + w.p);
 #pragma unroll
           for (int f = 0; f < NE; ++f) ev[f] = x.v[f];
         }
@@ -1011,6 +1026,10 @@ __global__ void __launch_bounds__(128) value_kernel(Args a) {
     w.pr.L2 = (int)pw[PW_L2];
   }
   float Sh, Sl;
+  if (a.pair_done[w.p] & PAIR_TIMEOUT) {   // a bounded wait of this pair expired
+    if (lane == 0) a.value[w.p] = __int_as_float(0x7fc00000);
+    return;
+  }
   if constexpr (G) {
     if (lane == 0) {
       if (w.pr.L1 == 0 || w.pr.L2 == 0) {   // exactly the boundary cell's value
@@ -1039,8 +1058,14 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
     gp[0] = g0sum; gp[1] = g1sum; gp[2] = pssum; gp[3] = 0.f;
     __threadfence();
     unsigned done = atomicAdd(a.pair_done + p, 1u);
-    if (done == (unsigned)w.nb - 1) {
+    if ((done & ~PAIR_TIMEOUT) == (unsigned)w.nb - 1) {
       __threadfence();
+      if (done & PAIR_TIMEOUT) {   // a bounded wait of this pair expired
+        const float nan = __int_as_float(0x7fc00000);
+        a.value[p] = nan; a.g_open[p] = nan; a.g_T[p] = nan;
+        if (a.g_ext) a.g_ext[p] = nan;
+        return;
+      }
       float o = 0.f, e = 0.f, ps = 0.f;
       for (int b = 0; b < w.nb; ++b) {
         const float* q = a.gpart + 4 * (w.slot0 + b);
@@ -1193,7 +1218,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
           for (int q = 0; q < NP; ++q)
             if (is_sentinel(pbc[q]))
               pbc[q] = poll_value(pin + q * (Lm + 1) + ir, ld_poll(pin + q * (Lm + 1) + ir), deadline,
-                                  a.status, 0.f);
+                                  a.status, a.pair_done + w.p, 0.f);
         }
       }
       float inmax = 0.f;
@@ -1369,7 +1394,7 @@ __device__ void bwd_band(const Args& a, const Place& w, int lane, float* sm, uin
           for (int q = 0; q < NP; ++q)
             if (is_sentinel(pw[q]))
               pw[q] = poll_value(pin + q * (Lm + 1) + i, ld_poll(pin + q * (Lm + 1) + i), deadline,
-                                 a.status, 0.f);
+                                 a.status, a.pair_done + w.p, 0.f);
         }
       }
 #pragma unroll

@@ -68,6 +68,53 @@ __device__ __forceinline__ int fexp(float m) {
 
 constexpr float XMAX = 118.f;   // scaled scores above this are clamped (|s|/T <= 80 gives 115.4)
 
+// Quiet chunks of the adjoint: every posterior in the chunk and every flow
+// out of it below 2^-SWB_LQUIET (relative to Z).  At 45 or more the posterior mass a
+// pair can lose over all its chunks stays below ~1e-9.
+#ifndef SWB_LQUIET
+#define SWB_LQUIET 60
+#endif
+
+// Asynchronous global -> shared copies (cp.async): the adjoint stages the
+// next chunk's checkpoint and first score rows while it runs the current
+// chunk, so they occupy no registers in between.  A copy with src_size 0
+// writes zeros and reads nothing.
+__device__ __forceinline__ void lcp16(float* dst, const float* src, int src_size) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_size)
+               : "memory");
+}
+__device__ __forceinline__ void lcp8(float* dst, const float* src, int src_size) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_size)
+               : "memory");
+}
+__device__ __forceinline__ void lcp4(float* dst, const float* src, int src_size) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(src_size)
+               : "memory");
+}
+__device__ __forceinline__ void lcp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void lcp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Stage row i (1-based) of the lane's R columns into dst (R floats, aligned
+// to 4R bytes); cells outside the pair or rows outside [1, L1] (ok false)
+// become 0, as load_row gives.
+template <int R>
+__device__ __forceinline__ void stage_row(float* dst, const Pair& pr, int i, int jl, bool ok) {
+  const float* src = pr.s + (size_t)(ok ? i - 1 : 0) * pr.ld + jl;
+  if (ok && pr.vec && jl + R <= pr.L2 && (R == 4 || R == 2)) {
+    if constexpr (R == 4) lcp16(dst, src, 16);
+    else lcp8(dst, src, 8);
+  } else {
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      const bool v = ok && jl + c < pr.L2;
+      lcp4(dst + c, v ? src + c : pr.s, v ? 4 : 0);
+    }
+  }
+}
+
 // Checkpoint floats per lane (LCKF, padded to float4), chunk record floats
 // (LCKRS: checkpoint groups, then the chunk's largest normalised frame, then
 // padding) and adjoint shared-memory floats per lane per step (LFW).
@@ -150,12 +197,13 @@ __device__ __forceinline__ void lck_unpack(const float (&x)[LDims<NS, R>::CKF], 
 // One step of the forward wavefront for one lane: (xl, xn) is the left
 // lane's last column of this row (normalised frame xn), xs the scaled scores
 // (NEG where the cell does not exist).  Updates the state to this row;
-// returns the step's compute frame in `et` (the raw values' frame).
+// returns the step's compute frame in `et` (the raw values' frame) and the
+// row's sum over its columns and states in `rs` (frame et).
 // Affine: M, I, D; linear: A (and, for the adjoint, the emission part em).
 template <int NS, int R>
 __device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], int xn,
                                        const float (&xs)[R], float gO, float gE, int nlive,
-                                       bool has_dead, int& et, float (&em)[R]) {
+                                       bool has_dead, int& et, float (&em)[R], float& rs) {
   // diagonal inputs of column 0: the left lane's previous row
   const int nd = s.nl;
   float dg[NS];
@@ -205,11 +253,17 @@ __device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], 
         if (c >= nlive) { s.v[0][c] = 0.f; em[c] = 0.f; }
     }
   }
+  // the largest column sum bounds every value of the row (all are >= 0);
+  // the sums are also the row's partition terms
   float mx = 0.f;
+  rs = 0.f;
 #pragma unroll
-  for (int q = 0; q < NS; ++q)
-#pragma unroll
-    for (int c = 0; c < R; ++c) mx = fmaxf(mx, s.v[q][c]);
+  for (int c = 0; c < R; ++c) {
+    float cs = s.v[0][c];
+    if constexpr (NS == 3) cs = (cs + s.v[1][c]) + s.v[2][c];
+    mx = fmaxf(mx, cs);
+    rs += cs;
+  }
   s.e = et;
   s.n = max(et + fexp(mx), 0);
   const float f = p2i(et - s.n);
@@ -284,7 +338,7 @@ __device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t dead
   load_edge(0, eb);
 #pragma unroll
   for (int f = 0; f < NEF; ++f) ebn[f] = 0.f;
-  float sb[PF][R];
+  float sb[PF][R];   // per-lane score ring, PF steps ahead
 #pragma unroll
   for (int u = 0; u < PF; ++u) {
     const int i = u - lane + 1;
@@ -292,6 +346,33 @@ __device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t dead
   }
 
   for (int kc = 0; kc < nch; ++kc) {
+    // resolve this chunk's edge records before its first step: lane u < C
+    // polls its own record until the left band has written it (one bounded
+    // wait per chunk, not per row); fault injection waits on a word nobody
+    // writes and substitutes zeros
+    {
+      const int ie = kc * C_STEPS + lane + 1;
+      const bool mine = lane < C_STEPS && ie <= L1;
+      bool miss = false;
+#pragma unroll
+      for (int f = 0; f < NEF; ++f) miss |= is_sentinel(eb[f]);
+      miss = miss && ein && mine;
+      if (__any_sync(FULL, miss || (fault && mine))) {
+        if (fault && mine) {
+          poll_value(a.never_written, ld_poll(a.never_written), deadline, a.status, a.pair_done + w.p,
+                     0.f);
+#pragma unroll
+          for (int f = 0; f < NEF; ++f) eb[f] = 0.f;
+        } else if (miss) {
+          FieldVec<NEF> x;
+#pragma unroll
+          for (int f = 0; f < NEF; ++f) x.v[f] = eb[f];
+          x = poll_fields_v<NEF, 0>(x, ein + (ie - 1), Lm, deadline, a.status, a.pair_done + w.p);
+#pragma unroll
+          for (int f = 0; f < NEF; ++f) eb[f] = x.v[f];
+        }
+      }
+    }
     if (keep_ck) lck_store<NS, R>(ck + (size_t)kc * LD::CKRS, lane, s);
     int cmx = -(1 << 30);   // largest normalised frame of the lane's live rows in this chunk
     if (kc + 1 < nch) load_edge(kc + 1, ebn);
@@ -309,29 +390,10 @@ __device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t dead
       int xn = __shfl_up_sync(FULL, s.n, 1);
 #pragma unroll
       for (int f = 0; f < NEF; ++f) ev[f] = __shfl_sync(FULL, eb[f], cu);
-      bool miss = false;
+      if (lane == 0) {   // the chunk's records are resolved (0 where there is no left band)
 #pragma unroll
-      for (int f = 0; f < NEF; ++f) miss |= is_sentinel(ev[f]);
-      miss = (lane == 0) && ein && act && miss;
-      if (__any_sync(FULL, miss) || fault) {
-        if (lane == 0 && fault && act) {
-          const float v = poll_value(a.never_written, ld_poll(a.never_written), deadline, a.status, 0.f);
-#pragma unroll
-          for (int f = 0; f < NEF; ++f) ev[f] = (f < NS) ? v : 0.f;
-        } else if (miss) {
-          FieldVec<NEF> x;
-#pragma unroll
-          for (int f = 0; f < NEF; ++f) x.v[f] = ev[f];
-          x = poll_fields_v<NEF, 0>(x, ein + (i - 1), Lm, deadline, a.status);
-#pragma unroll
-          for (int f = 0; f < NEF; ++f) ev[f] = x.v[f];
-        }
-      }
-      if (lane == 0) {
-        const bool take = act && (ein || fault);
-#pragma unroll
-        for (int q = 0; q < NS; ++q) xl[q] = take ? ev[q] : 0.f;
-        xn = take ? __float_as_int(ev[NS]) : 0;
+        for (int q = 0; q < NS; ++q) xl[q] = act ? ev[q] : 0.f;
+        xn = act ? __float_as_int(ev[NS]) : 0;
       }
       float xs[R];
       lscores<R>(sb[u], i, k, nlive, has_dead, xs);
@@ -340,17 +402,11 @@ __device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t dead
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
       int et;
-      float em[R];
-      lcells<NS, R>(s, xl, xn, xs, gO, gE, nlive, has_dead, et, em);
+      float em[R], rs;
+      lcells<NS, R>(s, xl, xn, xs, gO, gE, nlive, has_dead, et, em, rs);
       if (act) {
-        // partition: the row's live values in the frame ze (the largest
-        // normalised frame so far), Kahan-compensated
-        float rs = 0.f;
-#pragma unroll
-        for (int c = 0; c < R; ++c) {
-          if constexpr (NS == 3) rs += (s.v[0][c] + s.v[1][c]) + s.v[2][c];
-          else rs += s.v[0][c];
-        }
+        // partition: the row's live values (dead columns are 0) in the frame
+        // ze (the largest normalised frame so far), Kahan-compensated
         if (s.n > ze) {
           const float f = p2i(ze - s.n);
           zm *= f; zc *= f; ze = s.n;
@@ -385,8 +441,11 @@ __device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t dead
   if (lane == 0) { part[0] = (float)ze; part[1] = zm; }
 }
 
+#ifndef SWB_LFWD_MINB
+#define SWB_LFWD_MINB 5
+#endif
 template <int NS, int R>
-__global__ void __launch_bounds__(128) lfwd_kernel(Args a) {
+__global__ void __launch_bounds__(128, SWB_LFWD_MINB) lfwd_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
   const int ntasks = (a.layout == 0) ? a.B * a.nb : a.ntasks;
@@ -461,6 +520,10 @@ __global__ void __launch_bounds__(128) lvalue_kernel(Args a) {
     w.nb = (int)pw[PW_NB];
     w.slot0 = (size_t)pw[PW_SLOT0];
   }
+  if (a.pair_done[w.p] & PAIR_TIMEOUT) {   // a bounded wait of this pair expired
+    if (lane == 0) a.value[w.p] = __int_as_float(0x7fc00000);
+    return;
+  }
   int ze;
   float zm, Sh, Sl;
   lpair_z(a, w, lane, ze, zm);
@@ -472,10 +535,11 @@ __global__ void __launch_bounds__(128) lvalue_kernel(Args a) {
 // adjoint band task
 // ---------------------------------------------------------------------------
 
-// Shared memory per adjoint warp (floats): one chunk of recomputed fields.
+// Shared memory per adjoint warp (floats): one chunk of recomputed fields,
+// then the staged checkpoint and first PF score rows of the next chunk.
 template <int NS, int R>
 __host__ __device__ constexpr int lbwd_smem_floats() {
-  return C_STEPS * LDims<NS, R>::FW * 32;
+  return (C_STEPS * LDims<NS, R>::FW + LDims<NS, R>::CKF + PF * R) * 32;
 }
 
 // Per band, checkpoint chunks in reverse.  Each chunk restores its checkpoint
@@ -509,7 +573,7 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
   const int jl = col0 + lane * R;
   const int nlive = min(max(L2 - jl, 0), R);
   const bool has_dead = __any_sync(FULL, nlive < R);
-  const float k = a.k, gO = a.xgo, gE = a.xge;
+  const float k = a.k, gO = a.xgo, gE = a.xge, gX = fmaxf(gO, gE);
   const size_t Lm = (size_t)w.Lm;
   const float* ein = (band > 0) ? a.edge + w.ed0 + (size_t)(band - 1) * w.edb : nullptr;
   float* pout = (band > 0) ? a.bpush + w.bp0 + (size_t)band * w.bpb : nullptr;
@@ -518,15 +582,18 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
   const float* ck = a.ckpt + w.ck0 + (size_t)band * w.ckb;
   const int nch = band_chunks(L1);
 
-  // ---- chunk-ahead prefetch state ----
-  float ckr[CKF];          // checkpoint of the next chunk to recompute
-  int ckm;                 // ... and the chunk's largest normalised alpha frame
+  // ---- chunk-ahead prefetch state: the next chunk's checkpoint and first
+  // PF score rows are staged in shared memory (cp.async), the rest here ----
+  float* stg_ck = sm + C_STEPS * FW * 32;   // [CK4][lane][4]
+  float* stg_sc = stg_ck + CKF * 32;        // [PF][lane][R]
+  int ckm;                 // the next chunk's largest normalised alpha frame
   float ebr[NEF];          // lane u < C: left-band edge record of lane 0's row at recompute step u
   float pbc[NPF], pbn[NPF];// lane u < C: right-band record lane 31 needs at backward step u
-  float sb[PF][R];         // per-lane scores of the first PF recompute steps
   auto load_ck = [&](int kc) {
-    lck_load<NS, R>(ck + (size_t)kc * CKRS, lane, ckr);
-    ckm = __float_as_int(ck[(size_t)kc * CKRS + CKF * 32]);
+    const float* rec = ck + (size_t)kc * CKRS;
+#pragma unroll
+    for (int g = 0; g < LD::CK4; ++g) lcp16(stg_ck + g * 128 + lane * 4, rec + g * 128 + lane * 4, 16);
+    ckm = __float_as_int(rec[CKF * 32]);
   };
   auto load_eb = [&](int kc) {
     const int i = kc * C_STEPS + lane + 1;
@@ -544,8 +611,9 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int i = kc * C_STEPS + u - lane + 1;
-      load_row<R>(pr, i, jl, i >= 1 && i <= L1, sb[u]);
+      stage_row<R>(stg_sc + (u * 32 + lane) * R, pr, i, jl, i >= 1 && i <= L1);
     }
+    lcp_commit();
   };
   load_ck(nch - 1);
   load_eb(nch - 1);
@@ -568,10 +636,12 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
   KSum gA, gB, gS;
 
   // log2 of Z is at least zlog; a chunk is quiet (below) when every cell's
-  // posterior and every flow out of it is below 2^-60
-  const int zlog = ze + fexp(zm) - 1;
+  // posterior and every flow out of it is below 2^-SWB_LQUIET
+  const int zlog = ze + fexp(zm) - 1 - SWB_LQUIET;
   for (int kc = nch - 1; kc >= 0; --kc) {
     const int t0 = kc * C_STEPS;
+    lcp_wait_all();   // this chunk's staged checkpoint and score rows
+    __syncwarp();
     // ---- quiet chunk.  For a cell u of the chunk, alpha_u beta_u / Z sums,
     // over the chunk cells x where u's continuations stay inside, terms
     // alpha_x (1 + w beta_out) / Z (alpha_u W(u -> x) <= alpha_x: all weights
@@ -579,8 +649,8 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
     // row below, the right neighbour's held t and, for lane 31, the right
     // band's records.  With at most 2^9 cells, alpha_x <= 2^ckm and
     // 1 + w beta_out <= 4 max(1, inflow), every posterior in the chunk and
-    // every flow across its top and left edges is below 2^-60 when
-    // ckm + 11 + max(log2 inflow, 0) < log2 Z - 60.  Such a chunk writes zero
+    // every flow across its top and left edges is below 2^-SWB_LQUIET when
+    // ckm + 11 + max(log2 inflow, 0) < log2 Z - SWB_LQUIET.  Such a chunk writes zero
     // map rows and zero records to the left band, and passes zero beta up:
     // the flows it drops are among those bounded.  The right band's records
     // are resolved first, so the decision does not depend on timing. ----
@@ -594,7 +664,7 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
           FieldVec<NPF> x;
 #pragma unroll
           for (int f = 0; f < NPF; ++f) x.v[f] = pbc[f];
-          x = poll_fields_v<NPF, 0>(x, pin + ir, Lm + 1, deadline, a.status);
+          x = poll_fields_v<NPF, 0>(x, pin + ir, Lm + 1, deadline, a.status, a.pair_done + w.p);
 #pragma unroll
           for (int f = 0; f < NPF; ++f) pbc[f] = x.v[f];
         }
@@ -606,44 +676,110 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
         const int pn = __float_as_int(pbc[2]);
         inl = max(inl, pn + fexp(fmaxf(pbc[0], pbc[1])));
       }
-      const bool ok = ckm + 11 + max(inl, 0) < zlog - 60;
+      const bool ok = ckm + 11 + max(inl, 0) < zlog;
+#ifdef SWB_COUNT_QUIET   // measurement builds: quiet and computed chunks in header words 8, 9
+      {
+        const bool all_ok = __all_sync(FULL, ok);   // the vote runs on every lane
+        if (lane == 0) atomicAdd(a.counters + (all_ok ? 8 : 9), 1u);
+      }
+#endif
       if (__all_sync(FULL, ok)) {
-        float z[R];
+        // zero map rows and left-band records for the rows of chunk kq
+        auto zero_chunk = [&](int kq) {
+          float z[R];
 #pragma unroll
-        for (int c = 0; c < R; ++c) z[c] = 0.f;
-        for (int cu = 0; cu < C_STEPS; ++cu) {
-          const int i = t0 + cu - lane + 1;
-          if (i >= 1 && i <= L1) {
-            store_row<R>(pr, i, jl, z);
-            if (lane == 0 && pout) {
-              pout[0 * (Lm + 1) + i] = 0.f;
-              pout[1 * (Lm + 1) + i] = 0.f;
-              pout[2 * (Lm + 1) + i] = 0.f;
+          for (int c = 0; c < R; ++c) z[c] = 0.f;
+          for (int cu = 0; cu < C_STEPS; ++cu) {
+            const int i = kq * C_STEPS + cu - lane + 1;
+            if (i >= 1 && i <= L1) {
+              store_row<R>(pr, i, jl, z);
+              if (lane == 0 && pout) {
+                pout[0 * (Lm + 1) + i] = 0.f;
+                pout[1 * (Lm + 1) + i] = 0.f;
+                pout[2 * (Lm + 1) + i] = 0.f;
+              }
             }
           }
-        }
+        };
+        zero_chunk(kc);
         // the row above the chunk sees zero beta; lane 31 keeps the right
         // band's t of its top chunk row as the held diagonal successor
-        const float pt = __shfl_sync(FULL, pbc[1], C_STEPS - 1);
-        const int pn = __shfl_sync(FULL, __float_as_int(pbc[2]), C_STEPS - 1);
+        float pt = __shfl_sync(FULL, pbc[1], C_STEPS - 1);
+        int pn = __shfl_sync(FULL, __float_as_int(pbc[2]), C_STEPS - 1);
+        // ---- quiet run.  After a quiet chunk only lane 31's held t and the
+        // right band's records enter the chunks above, so one round of loads
+        // decides the next 32 / C chunks: lane l takes chunk kn - l / C at
+        // backward step l % C (lane 31's row there), checking that record
+        // and the one of the row below (lane l - 1's; lane 0: the held t).
+        // A record not written yet ends the run; that chunk is then decided
+        // as above from the same values, so results do not depend on timing. ----
+        constexpr int RUN = 32 / C_STEPS;
+        int kn = kc - 1;
+        while (kn >= 0) {
+          const int j = lane / C_STEPS, u = lane - j * C_STEPS;
+          const int kq = kn - j;
+          float r0 = 0.f, r1 = 0.f;
+          int rn2 = 0, cm = -(1 << 30);
+          bool written = true;
+          if (kq >= 0) {
+            const int ir = kq * C_STEPS + C_STEPS - 1 - u - 30;
+            if (pin && ir >= 1 && ir <= L1) {
+              r0 = ld_poll(pin + 0 * (Lm + 1) + ir);
+              r1 = ld_poll(pin + 1 * (Lm + 1) + ir);
+              const float r2 = ld_poll(pin + 2 * (Lm + 1) + ir);
+              written = !is_sentinel(r0) && !is_sentinel(r1) && !is_sentinel(r2);
+              rn2 = __float_as_int(r2);
+            }
+            cm = __float_as_int(ck[(size_t)kq * CKRS + CKF * 32]);
+          }
+          const int lg = written ? rn2 + fexp(fmaxf(r0, r1)) : 0;
+          const int lgu = __shfl_up_sync(FULL, lg, 1);
+          const bool wu = __shfl_up_sync(FULL, (int)written, 1) != 0;
+          const int lgb = lane == 0 ? pn + fexp(pt) : lgu;
+          const bool wb = lane == 0 || wu;
+          const bool q = kq >= 0 && written && wb && cm + 11 + max(max(lg, lgb), 0) < zlog;
+          const unsigned ball = __ballot_sync(FULL, q);
+          constexpr unsigned grp = (1u << C_STEPS) - 1u;
+          int n = 0;
+          while (n < RUN && kn - n >= 0 && ((ball >> (n * C_STEPS)) & grp) == grp) ++n;
+          for (int m = 0; m < n; ++m) zero_chunk(kn - m);
+          if (n > 0) {   // lane 31's held t: the record of its top row of the last zeroed chunk
+            const int src = (n - 1) * C_STEPS + C_STEPS - 1;
+            pt = __shfl_sync(FULL, r1, src);
+            pn = __shfl_sync(FULL, rn2, src);
+          }
+          kn -= n;
+          if (n < RUN) break;
+        }
 #pragma unroll
         for (int c = 0; c < R; ++c) { bdn[c] = 0.f; tdn[c] = 0.f; }
         fb = 0; nb = 0;
         o_b = 0.f; o_t = 0.f; o_n = 0;
         ht = lane == 31 ? pt : 0.f;
         hn = lane == 31 ? pn : 0;
-        if (kc > 0) {
-          load_ck(kc - 1);
-          load_eb(kc - 1);
-          load_sb(kc - 1);
-          load_pb(kc - 1, pbc);
+        if (kn >= 0) {   // inputs of the next chunk to run
+          load_ck(kn);
+          load_eb(kn);
+          load_sb(kn);
+          load_pb(kn, pbc);
         }
+        kc = kn + 1;   // the loop continues with chunk kn
         continue;
       }
     }
     // ---- restore the checkpoint and recompute the chunk ----
     LState<NS, R> st;
-    lck_unpack<NS, R>(ckr, st);
+    float sb[PF][R];   // per-lane score ring, PF steps ahead
+    {
+      float ckr[CKF];
+      lck_load<NS, R>(stg_ck, lane, ckr);
+      lck_unpack<NS, R>(ckr, st);
+#pragma unroll
+      for (int u = 0; u < PF; ++u)
+#pragma unroll
+        for (int c = 0; c < R; ++c) sb[u][c] = stg_sc[(u * 32 + lane) * R + c];
+    }
+    __syncwarp();   // the stage is read before the next chunk's copies are issued
 #pragma unroll 1
     for (int u0 = 0; u0 < C_STEPS; u0 += PF)
 #pragma unroll
@@ -671,8 +807,8 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
       int et;
-      float em[R];
-      lcells<NS, R>(st, xl, xn, xs, gO, gE, nlive, has_dead, et, em);
+      float em[R], rs;
+      lcells<NS, R>(st, xl, xn, xs, gO, gE, nlive, has_dead, et, em, rs);
       float* ent = sm + (size_t)cu * FW * 32;
       if constexpr (R == 4) {
         reinterpret_cast<float4*>(ent)[lane] = make_float4(st.v[0][0], st.v[0][1], st.v[0][2], st.v[0][3]);
@@ -720,22 +856,10 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
       float rb = __shfl_down_sync(FULL, o_b, 1);
       float rt = __shfl_down_sync(FULL, o_t, 1);
       int rn = __shfl_down_sync(FULL, o_n, 1);
-      {
+      {   // resolved at the chunk's start (the quiet-chunk test polls them)
         float pw[NPF];
 #pragma unroll
         for (int f = 0; f < NPF; ++f) pw[f] = __shfl_sync(FULL, pbc[f], cu);
-        bool miss = false;
-#pragma unroll
-        for (int f = 0; f < NPF; ++f) miss |= is_sentinel(pw[f]);
-        miss = miss && (lane == 31);
-        if (__any_sync(FULL, miss) && miss) {
-          FieldVec<NPF> x;
-#pragma unroll
-          for (int f = 0; f < NPF; ++f) x.v[f] = pw[f];
-          x = poll_fields_v<NPF, 0>(x, pin + i, Lm + 1, deadline, a.status);
-#pragma unroll
-          for (int f = 0; f < NPF; ++f) pw[f] = x.v[f];
-        }
         if (lane == 31) { rb = pw[0]; rt = pw[1]; rn = __float_as_int(pw[2]); }
       }
       // frames: the row is computed in ft >= every input's normalised frame
@@ -782,7 +906,7 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
           sp = fmaf(P, fa[3][c], sp);
           nbv[c] = vi;
           nmv[c] = vm;
-          mx = fmaxf(fmaxf(mx, vm), fmaxf(vi, vd));
+          mx = fmaxf(mx, fmaf(gX, sr, base));   // >= vm, vi, vd
           br = vd;
         } else {
           const float sr = bd + br;

@@ -575,7 +575,7 @@ __device__ void xfwd_band(const XArgs& a, int p, int band, int lane, uint64_t de
           FieldVec<NE> x;
 #pragma unroll
           for (int f = 0; f < NE; ++f) x.v[f] = ev[f];
-          x = poll_fields_v<NE, NS>(x, ein + (i - 1), Lm, deadline, a.status);
+          x = poll_fields_v<NE, NS>(x, ein + (i - 1), Lm, deadline, a.status, a.pair_done + p);
 #pragma unroll
           for (int f = 0; f < NE; ++f) ev[f] = x.v[f];
         }
@@ -835,17 +835,34 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Band partials of the HVP's parameter tangents; the last band of a pair to
-// finish folds them (in band order: deterministic) into grad_tangents.
+// finish folds them (in band order: deterministic) into grad_tangents.  When
+// a bounded wait of the pair expired (PAIR_TIMEOUT in its completion word),
+// the last band fills the pair's output map (and grad_tangents) with NaN.
 template <int NS, int MODE>
 __device__ void xfinish(const XArgs& a, int p, int band, int lane, bool empty, float dS, float ga,
-                        float gb, float gc) {
-  if (MODE != AUX_HVP || !a.gt) return;
+                        float gb, float gc, int L1, int L2) {
+  const bool tangents = MODE == AUX_HVP && a.gt;
+  unsigned done = 0;
   if (lane == 0) {
-    float* gp = a.gpart + 4 * ((size_t)p * a.nb + band);
-    gp[0] = ga; gp[1] = gb; gp[2] = gc; gp[3] = 0.f;
-    __threadfence();
-    const unsigned done = atomicAdd(a.pair_done + p, 1u);
-    if (done == (unsigned)a.nb - 1) {
+    if (tangents) {
+      float* gp = a.gpart + 4 * ((size_t)p * a.nb + band);
+      gp[0] = ga; gp[1] = gb; gp[2] = gc; gp[3] = 0.f;
+      __threadfence();
+    }
+    done = atomicAdd(a.pair_done + p, 1u);
+  }
+  done = __shfl_sync(FULL, done, 0);
+  if ((done & ~PAIR_TIMEOUT) == (unsigned)a.nb - 1 && (done & PAIR_TIMEOUT)) {
+    const float nan = __int_as_float(0x7fc00000);
+    float* o = a.out + (size_t)p * a.L1m * a.L2m;
+    for (int i = 0; i < L1; ++i)
+      for (int j = lane; j < L2; j += 32) o[(size_t)i * a.L2m + j] = nan;
+    if (tangents && lane < 4) a.gt[4 * p + lane] = nan;
+    return;
+  }
+  if (!tangents) return;
+  if (lane == 0) {
+    if ((done & ~PAIR_TIMEOUT) == (unsigned)a.nb - 1) {
       __threadfence();
       float o = 0.f, e = 0.f, c = 0.f;
       for (int b = 0; b < a.nb; ++b) {
@@ -884,7 +901,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
   float Sh, Sl, dS;
   xpair_stats<TM, R, GL>(a, p, lane, Sh, Sl, dS);
   if (!(L1 > 0 && col0 < L2)) {
-    xfinish<NS, MODE>(a, p, band, lane, L1 == 0 || L2 == 0, dS, 0.f, 0.f, 0.f);
+    xfinish<NS, MODE>(a, p, band, lane, L1 == 0 || L2 == 0, dS, 0.f, 0.f, 0.f, L1, L2);
     return;
   }
   const size_t slot = (size_t)p * a.nb + band;
@@ -979,7 +996,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
         for (int q = 0; q < NQ; ++q)
           if (is_sentinel(pbc[q]))
             pbc[q] = poll_value(pin + q * (Lm + 1) + ir, ld_poll(pin + q * (Lm + 1) + ir), deadline,
-                                a.status, 0.f);
+                                a.status, a.pair_done + p, 0.f);
       }
     }
     float inmax = 0.f;
@@ -1059,7 +1076,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
             for (int q = 0; q < NQ; ++q)
               if (is_sentinel(pw[q]))
                 pw[q] = poll_value(pin + q * (Lm + 1) + i, ld_poll(pin + q * (Lm + 1) + i), deadline,
-                                   a.status, 0.f);
+                                   a.status, a.pair_done + p, 0.f);
           }
         }
         // pushes arriving at column R-1 of row i: from the right lane (or band)
@@ -1331,7 +1348,7 @@ __device__ void xbwd_band(const XArgs& a, int p, int band, int lane, float* ring
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
   }
-  xfinish<NS, MODE>(a, p, band, lane, false, dS, v0, v1, v2);
+  xfinish<NS, MODE>(a, p, band, lane, false, dS, v0, v1, v2, L1, L2);
 }
 
 template <int NS, int R, int MODE, int GM = 0>

@@ -168,6 +168,7 @@ class Family:
     hvp: Callable                # (scores, v, *floats, lengths) -> [B, L1, L2]
     sens: tuple[Callable, ...]   # per param: (scores, *floats, lengths) -> dP/dtheta
     value: Callable = None       # (scores, *floats, lengths) -> [B], forward wavefront only
+    full: Callable = None        # (scores, *floats, lengths) -> (value, map, *dS/dtheta), one call
 
 
 def _ops():
@@ -182,6 +183,7 @@ SW = Family(
     sens=(lambda *a: _ops().sw_marginals_grad_gap(*a),
           lambda *a: _ops().sw_marginals_grad_temp(*a)),
     value=lambda *a: torch.ops.orihime_b200.sw_value(*a),
+    full=lambda *a: torch.ops.orihime_b200.sw_forward_with_grads(*a),
 )
 
 SW_AFFINE = Family(
@@ -193,6 +195,7 @@ SW_AFFINE = Family(
           lambda *a: _ops().sw_affine_marginals_grad_gap_ext(*a),
           lambda *a: _ops().sw_affine_marginals_grad_temp(*a)),
     value=lambda *a: torch.ops.orihime_b200.sw_affine_value(*a),
+    full=lambda *a: torch.ops.orihime_b200.sw_affine_forward_with_grads(*a),
 )
 
 NW = Family(
@@ -203,6 +206,7 @@ NW = Family(
     sens=(lambda *a: _ops().nw_marginals_grad_gap(*a),
           lambda *a: _ops().nw_marginals_grad_temp(*a)),
     value=lambda *a: torch.ops.orihime_b200.nw_value(*a),
+    full=lambda *a: torch.ops.orihime_b200.nw_forward_with_grads(*a),
 )
 
 NW_AFFINE = Family(
@@ -215,6 +219,7 @@ NW_AFFINE = Family(
           lambda *a: _ops().nw_affine_marginals_grad_gap_ext(*a),
           lambda *a: _ops().nw_affine_marginals_grad_temp(*a)),
     value=lambda *a: torch.ops.orihime_b200.nw_affine_value(*a),
+    full=lambda *a: torch.ops.orihime_b200.nw_affine_forward_with_grads(*a),
 )
 
 SV_LINEAR = Family(
@@ -225,6 +230,7 @@ SV_LINEAR = Family(
     sens=(lambda *a: _ops().sv_linear_marginals_grad_gap(*a),
           lambda *a: _ops().sv_linear_marginals_grad_temp(*a)),
     value=lambda *a: torch.ops.orihime_b200.sv_linear_value(*a),
+    full=lambda *a: torch.ops.orihime_b200.sv_linear_forward_with_grads(*a),
 )
 
 SV_AFFINE = Family(
@@ -236,6 +242,7 @@ SV_AFFINE = Family(
           lambda *a: _ops().sv_affine_marginals_grad_gap_ext(*a),
           lambda *a: _ops().sv_affine_marginals_grad_temp(*a)),
     value=lambda *a: torch.ops.orihime_b200.sv_affine_value(*a),
+    full=lambda *a: torch.ops.orihime_b200.sv_affine_forward_with_grads(*a),
 )
 
 
@@ -253,9 +260,13 @@ class _ValueFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, fam, lengths, scores, *params):
         vals = [_as_float(p) for p in params]
-        value, smap = fam.forward(scores, *vals, lengths)
         needs_params = any(isinstance(p, Tensor) and p.requires_grad for p in params)
-        grads = fam.grads(scores, *vals, lengths) if needs_params else None
+        if needs_params:
+            # one forward + adjoint gives the value, the map and dS/dtheta
+            value, smap, *grads = fam.full(scores, *vals, lengths)
+        else:
+            value, smap = fam.forward(scores, *vals, lengths)
+            grads = None
         ctx.fam, ctx.params = fam, params
         ctx.save_for_backward(smap)
         ctx.param_grads = grads

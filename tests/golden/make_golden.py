@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
-Run here (not on a GPU box): it needs the reference sources under
-/root/reference.  It copies the reference's Python package to a scratch
+Run where the reference sources are (not on a GPU box): their root is the
+environment variable ORIHIME_REFERENCE (default /root/reference).  It copies the reference's Python package to a scratch
 directory under /tmp, compiles the reference's CPU extension there with g++
 (the source list of meson.build's ``cpp_sources``), imports it, and records
 the public soft Smith-Waterman API's outputs on small seeded inputs:
@@ -31,7 +31,7 @@ import sysconfig
 
 import numpy as np
 
-REF = "/root/reference"
+REF = os.environ.get("ORIHIME_REFERENCE", "/root/reference")
 WORK = "/tmp/orihime_refpkg"
 HERE = os.path.dirname(os.path.abspath(__file__))
 

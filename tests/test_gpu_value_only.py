@@ -75,3 +75,38 @@ def test_value_ops_under_vmap_and_compile():
         assert torch.equal(got[k], torch.ops.orihime_b200.sw_affine_value(s[k].contiguous(), *AFF, None))
     f = torch.compile(lambda a: torch.ops.orihime_b200.sw_value(a, *LIN, None).sum(), fullgraph=True)
     assert torch.allclose(f(s[0]), torch.ops.orihime_b200.sw_value(s[0], *LIN, None).sum())
+
+
+@pytest.mark.parametrize("fam", ["sw_affine", "sw", "nw", "nw_affine", "sv_affine", "sv_linear"])
+def test_value_with_tensor_params_runs_one_native_call(fam, monkeypatch):
+    """value(...).backward() with learnable gaps and temperature: the value,
+    the map and dS/dparameters come from ONE forward + adjoint call, equal
+    bit for bit to the op's value and value_grad_params."""
+    import orihime_b200 as ohm
+    from orihime_b200 import _ops
+
+    s = _scores(3, 40, 57, seed=4).requires_grad_(True)
+    affine = fam in ("sw_affine", "nw_affine", "sv_affine")
+    names = ("gap_open", "gap_ext", "temp") if affine else ("gap", "temp")
+    vals = (-2.0, -0.5, 0.5) if affine else (-1.0, 0.5)
+    params = [torch.tensor(v, device="cuda", requires_grad=True) for v in vals]
+    calls = []
+    real_a, real_l = _ops.run_affine, _ops.run_linear
+    monkeypatch.setattr(_ops, "run_affine", lambda *a, **k: calls.append(1) or real_a(*a, **k))
+    monkeypatch.setattr(_ops, "run_linear", lambda *a, **k: calls.append(1) or real_l(*a, **k))
+    op = getattr(ohm, {"sw_affine": "sw_affine_value", "sw": "sw_value", "nw": "nw_value",
+                       "nw_affine": "nw_affine_value", "sv_affine": "sv_affine_value",
+                       "sv_linear": "sv_value"}[fam])
+    kw = {"gap_open": "gap_open_score", "gap_ext": "gap_extend_score", "gap": "gap_score",
+          "temp": "temperature"}
+    v = op(s, **{kw[n]: p for n, p in zip(names, params)})
+    v.sum().backward()
+    torch.cuda.synchronize()
+    assert len(calls) == 1, f"{len(calls)} native forward+adjoint calls"
+    monkeypatch.undo()
+    sd = s.detach()
+    full = getattr(torch.ops.orihime_b200, f"{fam}_forward_with_grads")(sd, *vals, None)
+    assert torch.equal(v.detach(), full[0])
+    assert torch.equal(s.grad, full[1])
+    for p, g in zip(params, full[2:]):
+        assert torch.equal(p.grad.reshape(()), g.sum())

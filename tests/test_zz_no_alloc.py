@@ -89,3 +89,37 @@ def test_static_matches_workspace_entry_point_twice():
             torch.testing.assert_close(g[k], w[k], rtol=1e-5, atol=1e-6, msg=k)
     # pair 3 of call 2 is empty: value, map and gradients are exactly 0
     assert float(got[1]["value"][3]) == 0.0 and not got[1]["map"][3].any()
+
+
+@pytest.mark.gpu
+def test_static_timeout_shows_in_results_and_status():
+    """A bounded cross-band wait that expires (injected on the host: bands
+    after the first wait on a word nobody writes, for at most 2 ms) marks the
+    affected pairs NaN and sets the shared scratch's status word, which
+    swb_static_read_status reads; the next call starts clean."""
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA not available")
+    lib = _lib.load()
+    s = _scores(3, 64, 300, 13).cuda()          # 300 columns: three bands of 128
+    ln = torch.tensor([[64, 300], [64, 100], [20, 300]], dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    o = _outputs(3, 64, 300)
+    opt = _lib.Options(0, 2_000_000, 1, None, 0, 0)
+    rc = lib.swb_sw_affine_forward_static(s.data_ptr(), ln.data_ptr(), 3, 64, 300, GO, GE, T,
+                                          *_ptrs(o), st, ctypes.byref(opt))
+    _lib.check(rc, "swb_sw_affine_forward_static")
+    torch.cuda.synchronize()
+    status = ctypes.c_uint(0)
+    _lib.check(lib.swb_static_read_status(st, ctypes.byref(status)), "swb_static_read_status")
+    assert status.value & _lib.STATUS_WAIT_TIMEOUT
+    # pairs 0 and 2 have bands that waited: NaN; pair 1 (one band) is unaffected
+    for k in ("value", "go", "ge", "gt"):
+        assert torch.isnan(o[k][0]) and torch.isnan(o[k][2]), k
+        assert torch.isfinite(o[k][1]), k
+    # the next call resets the scratch: correct results, status clear
+    got = _static(lib, s, ln)
+    want = _with_workspace(lib, s, ln)
+    _lib.check(lib.swb_static_read_status(st, ctypes.byref(status)), "swb_static_read_status")
+    assert status.value == 0
+    for k in ("value", "map", "go", "ge", "gt"):
+        torch.testing.assert_close(got[k], want[k], rtol=1e-5, atol=1e-6, msg=k)
