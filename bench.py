@@ -38,7 +38,6 @@ MUFU_PER_CELL = 21      # algorithmic MUFU ops per cell, forward 11 + adjoint 10
 MUFU_PER_CELL_BWD = 10  # adjoint kernel alone
 BYTES_PER_CELL = 8      # compulsory HBM bytes per cell (score read + map write)
 E2E_PARTS = 8           # pair groups of the end-to-end pipeline
-BWD_DRAM_BYTES_PER_CELL = 13.33  # measured adjoint DRAM traffic: scores + checkpoints + map
 
 
 def workload_lengths(seed: int, n: int = NPAIRS) -> np.ndarray:
@@ -647,6 +646,33 @@ def saigo_vert(args):
 # our arm
 # ---------------------------------------------------------------------------
 
+def profile_traffic(name="lbwd_kernel_affine_r4_dram.md"):
+    """DRAM bytes per useful cell of one adjoint launch, from the committed
+    ncu summary profiles/<name> (its line 'dram_bytes_per_cell: X'), with the
+    summary's own description of the build and capture it came from."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None, None
+    val = None
+    for line in txt.splitlines():
+        if line.strip().startswith("dram_bytes_per_cell:"):
+            val = float(line.split(":", 1)[1].split()[0])
+    return val, f"profiles/{name}"
+
+
+def time_steps(torch, fn, steps, stream=None):
+    """Milliseconds of `steps` calls of fn, CUDA events on the current stream."""
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -690,55 +716,77 @@ def main():
     cells = int((lengths[:, 0] * lengths[:, 1]).sum())
     flat = make_scores(torch, lengths, offsets, 3 + rank, dev)
     plan = ragged.Plan(ln32, offsets, family="affine", device=dev, cols_per_lane=args.cols_per_lane)
-    out = plan.outputs()
+    params = dict(gap_open=GO, gap_ext=GE, temp=T)
 
-    def step():
-        plan.run(flat, gap_open=GO, gap_ext=GE, temp=T, out=out)
-
+    # ---- headline: the packed plan captured in a CUDA graph, replayed ----
+    graph, gout = plan.graph(flat, **params)
     for _ in range(max(args.warmup, 3)):
-        step()
+        graph.replay()
     torch.cuda.synchronize()
     if plan.status() != 0:
         raise RuntimeError("kernel reported a bounded-wait timeout")
+    with ClockSampler(local) as clk:
+        barrier(torch, world)
+        torch.cuda.synchronize()
+        total_ms = time_steps(torch, graph.replay, args.steps)
+        barrier(torch, world)
+    total_ms = max_over_ranks(torch, world, total_ms)
+    ms = total_ms / args.steps
+    gcups_all = cells * world / (ms * 1e-3) / 1e9
+    if not bool(torch.isfinite(gout.value).all()):
+        raise RuntimeError("non-finite values")
 
-    # ---- timed region: K steps, events on the launching stream ----
-    # Each step records three events: before the call, between the forward and
-    # the adjoint kernel (recorded by the library on the launch stream), after.
+    # ---- the same step through plan.run (no graph), with the forward /
+    # adjoint split recorded by the library between the two kernels ----
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     for trio in ev:           # create the underlying CUDA events before timing
         for e_ in trio:
             e_.record()
     torch.cuda.synchronize()
-    opts = [_lib.Options(0, 0, 0, trio[1].cuda_event, 0) for trio in ev]
-    with ClockSampler(local) as clk:
-        barrier(torch, world)
-        torch.cuda.synchronize()
-        t_start = torch.cuda.Event(enable_timing=True)
-        t_end = torch.cuda.Event(enable_timing=True)
-        t_start.record()
-        for k in range(args.steps):
-            ev[k][0].record()
-            plan.run(flat, gap_open=GO, gap_ext=GE, temp=T, out=out, options=opts[k])
-            ev[k][2].record()
-        t_end.record()
-        torch.cuda.synchronize()
-        barrier(torch, world)
-    total_ms = max_over_ranks(torch, world, t_start.elapsed_time(t_end))
-    ms = total_ms / args.steps
-    gcups_all = cells * world / (ms * 1e-3) / 1e9
+    opts = [_lib.Options(0, 0, 0, trio[1].cuda_event, 0, 0) for trio in ev]
+    out = plan.outputs()
+    for _ in range(2):
+        plan.run(flat, out=out, **params)
+    torch.cuda.synchronize()
+    barrier(torch, world)
+    for k in range(args.steps):
+        ev[k][0].record()
+        plan.run(flat, out=out, options=opts[k], **params)
+        ev[k][2].record()
+    torch.cuda.synchronize()
+    barrier(torch, world)
     per_step = sorted(ev[k][0].elapsed_time(ev[k][2]) for k in range(args.steps))
+    eager_ms = max_over_ranks(torch, world, float(np.mean(per_step)))
     kernel_split = {
         "fwd_ms": float(np.mean([ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)])),
         "bwd_ms": float(np.mean([ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps)])),
-        "note": "fwd_ms includes the per-call workspace memsets",
+        "note": "plan.run without a graph; fwd_ms includes the per-call workspace memsets",
     }
+    del graph, gout, out
 
     if args.quick:
         if rank == 0:
             print(json.dumps({"quick": True, "pairs": args.pairs, "cols_per_lane": args.cols_per_lane,
-                              "cells": cells, "ms_per_step": ms,
+                              "cells": cells, "ms_per_step": ms, "eager_ms_per_step": eager_ms,
                               "gcups": gcups_all, "kernel_ms": kernel_split}))
         return 0
+
+    # ---- dense posteriors: the same lengths with N(0, 1) scores at T = 1
+    # (few cells are negligible, so the adjoint's quiet-chunk skip rarely
+    # applies) ----
+    g = torch.Generator(device=dev)
+    g.manual_seed(11 + rank)
+    dense = torch.randn(flat.numel(), generator=g, device=dev)
+    dgraph, _ = plan.graph(dense, gap_open=GO, gap_ext=GE, temp=1.0)
+    for _ in range(2):
+        dgraph.replay()
+    torch.cuda.synchronize()
+    barrier(torch, world)
+    dense_ms = max_over_ranks(torch, world, time_steps(torch, dgraph.replay, args.steps)) / args.steps
+    barrier(torch, world)
+    dense_line = {"value": cells * world / (dense_ms * 1e-3) / 1e9, "unit": "GCUPS", "ms_per_step": dense_ms,
+                  "workload": "the same lengths, scores N(0, 1), gap_open -2, gap_ext -0.5, T 1.0 (CUDA graph)"}
+    del dgraph, dense
 
     # ---- e2e through the public API: pinned host scores in, values out ----
     # StreamedPlan copies the batch in E2E_PARTS pair groups on a copy stream
@@ -746,7 +794,7 @@ def main():
     host = torch.empty(flat.numel(), dtype=torch.float32, pin_memory=True)
     host.copy_(flat.cpu())
     host_val = torch.empty(plan.B, dtype=torch.float32, pin_memory=True)
-    del plan, out
+    del plan
     torch.cuda.empty_cache()
     splan = ragged.StreamedPlan(ln32, offsets, family="affine", device=dev, parts=E2E_PARTS,
                                 cols_per_lane=args.cols_per_lane)
@@ -771,29 +819,33 @@ def main():
            "ms_per_step": e2e_ms, "pipeline": f"{len(splan.groups)} pair groups, copy/compute overlapped"}
     del splan, sout, host
 
-    # ---- plain padded launch on a sample of the same pairs ----
+    # ---- the plain padded drop-in over the same pairs ----
     plain = None if args.no_plain else plain_padded(torch, lengths, offsets, flat, ms, cells)
 
     line = None
     if rank == 0:
         peak = mufu_peak(torch, lib)
         bwd_ms = kernel_split.get("bwd_ms")
+        hbm = measured_peaks().get("hbm_gbs")
         roof = None
         if bwd_ms:
             achieved = MUFU_PER_CELL_BWD * cells / (bwd_ms * 1e-3)
+            tpc, tsrc = profile_traffic()
             roof = {"bound": "mufu", "achieved": achieved / 1e9, "peak": peak / 1e9,
-                    "unit": "Gop/s", "frac": achieved / peak, "traffic": None,
-                    "kernel": "bwd_kernel<3,4,1> (checkpointed adjoint)",
-                    "algorithmic": f"{MUFU_PER_CELL_BWD} ex2/lg2 per cell x {cells} cells",
+                    "unit": "Gop/s", "frac": achieved / peak,
+                    "traffic": None if tpc is None else tpc * cells,
+                    "traffic_source": tsrc,
+                    "kernel": "lbwd_kernel<3,4,1> (checkpointed adjoint, scaled linear domain)",
+                    "algorithmic": (f"{MUFU_PER_CELL_BWD} ex2/lg2 per cell (the log-domain adjoint's "
+                                    f"count) x {cells} cells"),
                     "peak_source": "measured in-bench (swb_mufu_probe: ex2.approx throughput)",
                     "step_frac": (MUFU_PER_CELL * cells / (ms * 1e-3)) / peak,
-                    "hbm_frac_of_measured": (BYTES_PER_CELL * cells / (ms * 1e-3)) /
-                                            (measured_peaks().get("hbm_gbs", 6550.0) * 1e9)}
-            # DRAM bytes of one adjoint launch: ncu's dram__bytes_read + write per
-            # cell on a 256-pair capture of this kernel, times this launch's cells
-            roof["traffic"] = BWD_DRAM_BYTES_PER_CELL * cells
-            roof["traffic_source"] = ("ncu capture (1 pass) of bwd_kernel<3,4,1> on this 4096-pair "
-                                      f"batch: {BWD_DRAM_BYTES_PER_CELL} B/cell")
+                    "hbm_frac_of_measured": (None if not hbm else
+                                             (BYTES_PER_CELL * cells / (ms * 1e-3)) / (hbm * 1e9)),
+                    "note": ("the linear-domain kernels issue about 1 ex2 per cell instead of the "
+                             "21 the log-sum-exp recurrence needs, so they can exceed this roofline; "
+                             "the fraction is throughput relative to the MUFU bound of the reference's "
+                             "formulation")}
         cpu = None if args.no_cpu_baseline else cpu_baseline(lengths)
         clocks = clk.summary()
         line = {"metric": METRIC, "value": gcups_all, "unit": "GCUPS", "n_gpus": world,
@@ -803,12 +855,14 @@ def main():
                 "config": {"workload": f"ragged C3: {args.pairs} affine pairs per GPU, N,M log-uniform "
                                        f"[{LMIN},{LMAX}] (seed 3+rank), scores 3<e,f>/sqrt(64)",
                            "cells_per_gpu": cells, "gap_open": GO, "gap_ext": GE, "temp": T,
+                           "timed": "CUDA graph replay of the packed plan (forward + adjoint)",
                            "l2": "inputs (3.9 GB) larger than L2; no flush",
                            "parallelism": f"replicas x{world} (independent pairs)"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * args.steps, "clocks": clocks,
-                "kernel_ms": kernel_split, "step_ms_spread": [per_step[0], per_step[-1]],
-                "plain_padded": plain}
+                "eager_ms_per_step": eager_ms, "kernel_ms": kernel_split,
+                "step_ms_spread_eager": [per_step[0], per_step[-1]],
+                "dense_posteriors": dense_line, "plain_padded": plain}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
@@ -817,47 +871,53 @@ def main():
     return 0
 
 
-def plain_padded(torch, lengths, offsets, flat, ragged_ms, cells_all, sample_pairs=64):
-    """The plain drop-in on a padded [B, 2048, 2048] batch of the first
-    `sample_pairs` pairs, masked (excluded cells get the mask sentinel, so the
-    full padded area is computed, as ohm.sw_affine(mask=...) does) and with
-    lengths (the kernel skips cells outside each pair)."""
+def plain_padded(torch, lengths, offsets, flat, ragged_ms, cells_all, chunk=64):
+    """The plain padded drop-in (torch.ops.orihime.sw_affine_forward) over
+    ALL pairs of the batch: pairs grouped by size in chunks of `chunk`, each
+    chunk padded to its own largest L1 x L2, the kernel times of
+    the chunks summed.  Two variants: masked (cells outside each pair at the
+    mask sentinel, as ohm.sw_affine(mask=...) passes them: the whole padded
+    area is computed) and lengths (the kernel skips cells outside each
+    pair)."""
     from orihime_b200 import operator as op
     from orihime_b200 import ragged
 
-    pick = list(range(sample_pairs))
-    L1m, L2m = LMAX, LMAX
     dev = flat.device
-    x = torch.zeros(len(pick), L1m, L2m, device=dev)
-    mask = torch.ones(len(pick), L1m, L2m, dtype=torch.bool, device=dev)
-    for k, b in enumerate(pick):
-        L1, L2 = int(lengths[b, 0]), int(lengths[b, 1])
-        p = ragged.pitch_of(L2)
-        x[k, :L1, :L2] = flat[int(offsets[b]):int(offsets[b]) + L1 * p].view(L1, p)[:, :L2]
-        mask[k, :L1, :L2] = False
-    useful = int(sum(int(lengths[b, 0]) * int(lengths[b, 1]) for b in pick))
-    xm = op.normalize_mask(x.masked_fill(mask, float("-inf")), T).contiguous()
-    ln = torch.tensor([[int(lengths[b, 0]), int(lengths[b, 1])] for b in pick], dtype=torch.int32,
-                      device=dev)
-    res = {}
-    for name, fn in (("masked", lambda: torch.ops.orihime.sw_affine_forward(xm, GO, GE, T, None)),
-                     ("lengths", lambda: torch.ops.orihime.sw_affine_forward(x, GO, GE, T, ln))):
-        fn()
-        torch.cuda.synchronize()
-        a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        fn()
-        b2.record()
-        torch.cuda.synchronize()
-        t = a.elapsed_time(b2)
-        res[name] = {"ms": t, "gcups_useful": useful / (t * 1e-3) / 1e9}
-    ragged_gcups = cells_all / (ragged_ms * 1e-3) / 1e9
-    res["sample"] = f"first {sample_pairs} pairs padded to {L1m}x{L2m} ({useful} useful cells)"
-    res["ragged_over_plain_masked"] = ragged_gcups / res["masked"]["gcups_useful"]
-    res["ragged_over_plain_lengths"] = ragged_gcups / res["lengths"]["gcups_useful"]
-    del x, mask, xm
+    # grouping with little padding: by L2 in half-octave buckets, then by L1
+    # (2.2x padded cells on this batch; sorting by L1 alone pads 4.1x)
+    order = np.lexsort((lengths[:, 0], np.floor(np.log2(lengths[:, 1]) * 2)))[::-1]
+    res = {"masked": 0.0, "lengths": 0.0}
+    padded_cells = 0
+    for c0 in range(0, len(order), chunk):
+        pick = order[c0:c0 + chunk]
+        L1m = int(lengths[pick, 0].max())
+        L2m = int(lengths[pick, 1].max())
+        padded_cells += len(pick) * L1m * L2m
+        x = torch.zeros(len(pick), L1m, L2m, device=dev)
+        mask = torch.ones(len(pick), L1m, L2m, dtype=torch.bool, device=dev)
+        for k, b in enumerate(pick):
+            L1, L2 = int(lengths[b, 0]), int(lengths[b, 1])
+            p = ragged.pitch_of(L2)
+            x[k, :L1, :L2] = flat[int(offsets[b]):int(offsets[b]) + L1 * p].view(L1, p)[:, :L2]
+            mask[k, :L1, :L2] = False
+        xm = op.normalize_mask(x.masked_fill(mask, float("-inf")), T).contiguous()
+        ln = torch.tensor([[int(lengths[b, 0]), int(lengths[b, 1])] for b in pick], dtype=torch.int32,
+                          device=dev)
+        for name, fn in (("masked", lambda: torch.ops.orihime.sw_affine_forward(xm, GO, GE, T, None)),
+                         ("lengths", lambda: torch.ops.orihime.sw_affine_forward(x, GO, GE, T, ln))):
+            fn()
+            torch.cuda.synchronize()
+            res[name] += time_steps(torch, fn, 1)
+        del x, mask, xm
     torch.cuda.empty_cache()
-    return res
+    ragged_gcups = cells_all / (ragged_ms * 1e-3) / 1e9
+    out = {"sample": (f"all {len(order)} pairs grouped by size (L2 half-octave, then L1) in padded chunks of {chunk} "
+                      f"({padded_cells:.4g} padded cells for {cells_all:.4g} useful)")}
+    for name in ("masked", "lengths"):
+        out[name] = {"ms": res[name], "gcups_useful": cells_all / (res[name] * 1e-3) / 1e9}
+    out["ragged_over_plain_masked"] = ragged_gcups / out["masked"]["gcups_useful"]
+    out["ragged_over_plain_lengths"] = ragged_gcups / out["lengths"]["gcups_useful"]
+    return out
 
 
 def cpu_baseline(lengths):

@@ -69,10 +69,10 @@ __device__ __forceinline__ int fexp(float m) {
 constexpr float XMAX = 118.f;   // scaled scores above this are clamped (|s|/T <= 80 gives 115.4)
 
 // Quiet chunks of the adjoint: every posterior in the chunk and every flow
-// out of it below 2^-SWB_LQUIET (relative to Z).  At 45 or more the posterior mass a
+// out of it below 2^-SWB_LQUIET (relative to Z).  At 45 the posterior mass a
 // pair can lose over all its chunks stays below ~1e-9.
 #ifndef SWB_LQUIET
-#define SWB_LQUIET 60
+#define SWB_LQUIET 45
 #endif
 
 // Asynchronous global -> shared copies (cp.async): the adjoint stages the
