@@ -11,9 +11,11 @@ scores) are larger than L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Multi-GPU (torchrun): every rank runs its own batch (seed 3 + rank): weak
-scaling, no collective on the data path; rank 0 prints the line with the
-max-over-ranks time.
+Multi-GPU (torchrun): the job is N x 4096 pairs drawn the same way (seed 3),
+split across the ranks by LPT on each pair's computed cells (weak scaling:
+about 4096 pairs per GPU); each rank runs its shard, no collective touches
+the data path, and rank 0 prints the line with the max-over-ranks time and
+the whole job's cells; the values are gathered once after timing.
 """
 
 from __future__ import annotations
@@ -46,14 +48,26 @@ def workload_lengths(seed: int, n: int = NPAIRS) -> np.ndarray:
     return np.rint(ln).astype(np.int64)
 
 
-def make_scores(torch, lengths, offsets, seed, device):
-    """Packed C2-generator scores, built on the device pair by pair."""
+def shard_of(world: int, rank: int, pairs: int = NPAIRS):
+    """This rank's pairs of the whole job: N x `pairs` pairs (seed 3) split
+    across the N ranks by LPT on their computed cells.  Returns (lengths,
+    global pair indices, all shards); one rank gets the whole batch."""
+    from orihime_b200 import ragged
+
+    lengths = workload_lengths(3, pairs * world)
+    shards = ragged.lpt_partition(lengths, world)
+    return lengths[shards[rank]], shards[rank], shards
+
+
+def make_scores(torch, lengths, offsets, seed, device, index=None):
+    """Packed C2-generator scores, built on the device pair by pair; pair b
+    is seeded by its index in the whole job (`index[b]`, default b)."""
     from orihime_b200 import ragged
 
     flat = torch.zeros(int(offsets[-1]), dtype=torch.float32, device=device)
     g = torch.Generator(device=device)
     for b, (L1, L2) in enumerate(lengths.tolist()):
-        g.manual_seed(seed * 100003 + b)
+        g.manual_seed(seed * 100003 + (int(index[b]) if index is not None else b))
         e = torch.randn(L1, D, generator=g, device=device)
         f = torch.randn(L2, D, generator=g, device=device)
         p = ragged.pitch_of(L2)
@@ -711,10 +725,12 @@ def main():
     dev = torch.device("cuda", local)
     lib = _lib.load()
 
-    lengths = workload_lengths(3 + rank, args.pairs)
+    # one pair list for the whole job, LPT-sharded over the ranks (one rank:
+    # the whole batch); no collective touches the data
+    lengths, gidx, shards = shard_of(world, rank, args.pairs)
     offsets, ln32 = ragged.layout(lengths)
     cells = int((lengths[:, 0] * lengths[:, 1]).sum())
-    flat = make_scores(torch, lengths, offsets, 3 + rank, dev)
+    flat = make_scores(torch, lengths, offsets, 3, dev, index=gidx)
     plan = ragged.Plan(ln32, offsets, family="affine", device=dev, cols_per_lane=args.cols_per_lane)
     params = dict(gap_open=GO, gap_ext=GE, temp=T)
 
@@ -732,8 +748,14 @@ def main():
         barrier(torch, world)
     total_ms = max_over_ranks(torch, world, total_ms)
     ms = total_ms / args.steps
-    gcups_all = cells * world / (ms * 1e-3) / 1e9
-    if not bool(torch.isfinite(gout.value).all()):
+    job = workload_lengths(3, args.pairs * world)
+    all_cells = int((job[:, 0] * job[:, 1]).sum())   # every shard's cells: the whole job
+    gcups_all = all_cells / (ms * 1e-3) / 1e9
+    if world > 1:   # the job's values in pair order (one all_gather, outside the timed region)
+        vals = ragged.all_gather_values(gout.value, shards, sum(len(x) for x in shards))
+    else:
+        vals = gout.value
+    if not bool(torch.isfinite(vals).all()):
         raise RuntimeError("non-finite values")
 
     # ---- the same step through plan.run (no graph), with the forward /
@@ -784,7 +806,7 @@ def main():
     barrier(torch, world)
     dense_ms = max_over_ranks(torch, world, time_steps(torch, dgraph.replay, args.steps)) / args.steps
     barrier(torch, world)
-    dense_line = {"value": cells * world / (dense_ms * 1e-3) / 1e9, "unit": "GCUPS", "ms_per_step": dense_ms,
+    dense_line = {"value": all_cells / (dense_ms * 1e-3) / 1e9, "unit": "GCUPS", "ms_per_step": dense_ms,
                   "workload": "the same lengths, scores N(0, 1), gap_open -2, gap_ext -0.5, T 1.0 (CUDA graph)"}
     del dgraph, dense
 
@@ -814,7 +836,7 @@ def main():
     if splan.status() != 0:
         raise RuntimeError("kernel reported a bounded-wait timeout")
     e2e_ms = max_over_ranks(torch, world, e0.elapsed_time(e1)) / args.steps
-    e2e = {"value": cells * world / (e2e_ms * 1e-3) / 1e9, "unit": "GCUPS",
+    e2e = {"value": all_cells / (e2e_ms * 1e-3) / 1e9, "unit": "GCUPS",
            "h2d_bytes_per_step": flat.numel() * 4, "d2h_bytes_per_step": splan.B * 4,
            "ms_per_step": e2e_ms, "pipeline": f"{len(splan.groups)} pair groups, copy/compute overlapped"}
     del splan, sout, host
@@ -852,12 +874,15 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"ragged C3: {args.pairs} affine pairs per GPU, N,M log-uniform "
-                                       f"[{LMIN},{LMAX}] (seed 3+rank), scores 3<e,f>/sqrt(64)",
-                           "cells_per_gpu": cells, "gap_open": GO, "gap_ext": GE, "temp": T,
+                "config": {"workload": f"ragged C3: {args.pairs * world} affine pairs, N,M log-uniform "
+                                       f"[{LMIN},{LMAX}] (seed 3), scores 3<e,f>/sqrt(64)"
+                                       + (f", LPT-sharded over {world} GPUs" if world > 1 else ""),
+                           "cells": all_cells, "cells_rank0": cells,
+                           "gap_open": GO, "gap_ext": GE, "temp": T,
                            "timed": "CUDA graph replay of the packed plan (forward + adjoint)",
                            "l2": "inputs (3.9 GB) larger than L2; no flush",
-                           "parallelism": f"replicas x{world} (independent pairs)"},
+                           "parallelism": (f"LPT shards x{world} of one pair list, no collective on "
+                                           "the data path" if world > 1 else "one GPU")},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * args.steps, "clocks": clocks,
                 "eager_ms_per_step": eager_ms, "kernel_ms": kernel_split,

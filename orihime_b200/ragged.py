@@ -310,3 +310,143 @@ class StreamedPlan:
         for p in self.plans:
             st |= p.status()
         return st
+
+
+# ---------------------------------------------------------------------------
+# one pair list across several GPUs
+# ---------------------------------------------------------------------------
+
+def pair_cost(lengths, cols_per_lane: int = 4) -> np.ndarray:
+    """Work of each pair for load balancing: the cells its bands compute, i.e.
+    the band count times the band's wavefront steps (L1 + 31) times the band
+    width, which counts the partly dead last band and the fill and drain of
+    every band, not just L1 * L2."""
+    ln = np.asarray(lengths, dtype=np.int64).reshape(-1, 2)
+    w = 32 * int(cols_per_lane or 4)
+    nb = np.maximum(1, (ln[:, 1] + w - 1) // w)
+    cost = nb * (ln[:, 0] + 31) * w
+    return np.where((ln[:, 0] > 0) & (ln[:, 1] > 0), cost, 0)
+
+
+def lpt_partition(lengths, parts: int, cost=None) -> list[np.ndarray]:
+    """Pair indices of each of `parts` shards, longest processing time first:
+    pairs in decreasing cost, each to the shard with the least cost so far
+    (ties: the lowest shard).  Deterministic, so every rank computes the same
+    partition from the same lengths.  Each shard's indices are ascending."""
+    import heapq
+
+    c = pair_cost(lengths) if cost is None else np.asarray(cost, dtype=np.float64)
+    parts = max(1, int(parts))
+    heap = [(0, g) for g in range(parts)]
+    buckets = [[] for _ in range(parts)]
+    for b in np.argsort(-c, kind="stable"):
+        load, g = heapq.heappop(heap)
+        buckets[g].append(int(b))
+        heapq.heappush(heap, (load + int(c[b]), g))
+    return [np.array(sorted(x), dtype=np.int64) for x in buckets]
+
+
+def shard_scores(flat: torch.Tensor, offsets, lengths, idx, device=None) -> tuple[torch.Tensor, np.ndarray, np.ndarray]:
+    """The packed buffer of pairs `idx` of a packed batch: (flat, offsets,
+    lengths) of the shard in the same packing, copied to `device`."""
+    off = np.asarray(offsets, dtype=np.int64)
+    ln = np.asarray(lengths).reshape(-1, 2)
+    sub_off, sub_ln = layout(ln[idx])
+    dev = flat.device if device is None else torch.device(device)
+    out = torch.empty(max(int(sub_off[-1]), 1), dtype=torch.float32, device=dev)
+    for k, b in enumerate(np.asarray(idx).tolist()):
+        n = int(sub_off[k + 1] - sub_off[k])
+        if n:
+            out[int(sub_off[k]):int(sub_off[k]) + n].copy_(flat[int(off[b]):int(off[b]) + n],
+                                                            non_blocking=True)
+    return out, sub_off, sub_ln
+
+
+class ShardedPlan:
+    """One packed batch split across GPUs by LPT on the pairs' computed cells
+    (`pair_cost`), one persistent forward + adjoint launch per GPU and no
+    collective on the data path: pairs are independent.
+
+    Single process, several devices:
+
+        sp = ragged.ShardedPlan(lengths, devices=["cuda:0", "cuda:1"])
+        flats = sp.scatter(flat_host)            # each shard's packed scores on its device
+        outs = sp.run(flats, gap_open=-2.0, gap_ext=-0.5, temp=0.5)
+        values = sp.gather_values(outs)          # [B], in the batch's pair order
+
+    One process per GPU (torchrun): every rank builds the same partition and
+    runs only its shard (``rank``/``world``); ``all_gather_values`` assembles
+    the values of all ranks with one all_gather (optional, for reporting).
+    """
+
+    def __init__(self, lengths, offsets=None, family: str = "affine", devices=None,
+                 rank: Optional[int] = None, world: Optional[int] = None, cols_per_lane: int = 0):
+        ln = np.asarray(lengths, dtype=np.int32).reshape(-1, 2)
+        self.B = ln.shape[0]
+        self.lengths = ln
+        self.offsets = layout(ln)[0] if offsets is None else np.asarray(offsets, dtype=np.int64)
+        self.family = family
+        if world is not None:
+            self.world, self.rank = int(world), int(rank or 0)
+            self.devices = [torch.device(devices) if devices is not None else
+                            torch.device("cuda", torch.cuda.current_device())]
+            self.local = [self.rank]
+        else:
+            devs = devices or ["cuda"]
+            self.devices = [torch.device(d) for d in devs]
+            self.world, self.rank = len(self.devices), 0
+            self.local = list(range(self.world))
+        self.shards = lpt_partition(ln, self.world, pair_cost(ln, cols_per_lane or 4))
+        self.plans = {}
+        for k, g in enumerate(self.local):
+            idx = self.shards[g]
+            sub_off, sub_ln = layout(ln[idx])
+            self.plans[g] = Plan(sub_ln, sub_off, family=family, device=self.devices[k],
+                                 cols_per_lane=cols_per_lane)
+
+    def cost(self) -> list[int]:
+        """Computed cells of each shard (the LPT loads)."""
+        c = pair_cost(self.lengths)
+        return [int(c[idx].sum()) for idx in self.shards]
+
+    def scatter(self, flat: torch.Tensor) -> dict:
+        """Each local shard's packed scores on its device, from the whole
+        batch's packed buffer (host or device)."""
+        return {g: shard_scores(flat, self.offsets, self.lengths, self.shards[g],
+                                self.plans[g].device)[0] for g in self.local}
+
+    def run(self, flats: dict, **params) -> dict:
+        """One forward + adjoint per local shard, asynchronous on each
+        device's current stream; returns {shard: Result}."""
+        return {g: self.plans[g].run(flats[g], **params) for g in self.local}
+
+    def gather_values(self, outs: dict, device=None) -> torch.Tensor:
+        """Values of the local shards, in the batch's pair order ([B])."""
+        dev = torch.device(device) if device is not None else self.devices[0]
+        v = torch.full((self.B,), float("nan"), dtype=torch.float32, device=dev)
+        for g, r in outs.items():
+            v[torch.as_tensor(self.shards[g], device=dev)] = r.value.to(dev)
+        return v
+
+    def all_gather_values(self, value_local: torch.Tensor, group=None) -> torch.Tensor:
+        """[B] values of every rank's shard from this rank's [len(shard)]
+        values (a collective: every rank calls it)."""
+        return all_gather_values(value_local, self.shards, self.B, group)
+
+
+def all_gather_values(value_local: torch.Tensor, shards, B: int, group=None) -> torch.Tensor:
+    """Assemble per-pair values computed shard by shard on the ranks of a
+    process group: one all_gather of equally padded blocks, then a scatter
+    into the batch's pair order.  `shards[g]` are rank g's pair indices."""
+    import torch.distributed as dist
+
+    n = max(len(x) for x in shards)
+    pad = torch.zeros(n, dtype=value_local.dtype, device=value_local.device)
+    pad[:value_local.numel()] = value_local
+    blocks = [torch.empty_like(pad) for _ in range(len(shards))]
+    dist.all_gather(blocks, pad, group=group)
+    out = torch.empty(B, dtype=value_local.dtype, device=value_local.device)
+    for g, blk in enumerate(blocks):
+        idx = torch.as_tensor(shards[g], device=value_local.device)
+        out[idx] = blk[:len(shards[g])]
+    return out

@@ -1,8 +1,9 @@
 """Multi-process host logic of bench.py on CPU ranks (gloo, world size 2).
 
-Pairs are independent, so N GPUs run N replicas: every rank draws its own
-batch (seed 3 + rank), no collective touches the data, and the reported time
-is the max over ranks.  These tests run that host logic with gloo.
+Pairs are independent, so N GPUs split one pair list of N x 4096 pairs by
+LPT on the pairs' computed cells: every rank computes the same partition and
+runs its shard, no collective touches the data, and the reported time is the
+max over ranks.  These tests run that host logic with gloo.
 """
 
 import json
@@ -33,7 +34,7 @@ def _rank_main(rank, world, port, outdir):
 
     w, r, local = bench.dist_init(torch, backend="gloo")
     assert (w, r, local) == (world, rank, rank)
-    ln = bench.workload_lengths(3 + r, 64)
+    ln, idx, shards = bench.shard_of(w, r, 64)
     bench.barrier(torch, w)
     t_max = bench.max_over_ranks(torch, w, 10.0 + r)
     # every rank takes the same collective steps: a second reduction agrees
@@ -41,12 +42,16 @@ def _rank_main(rank, world, port, outdir):
     # the reference arm is rank 0's alone: other ranks return at once
     rc_ref = bench.run_reference(type("A", (), {"steps": 1, "warmup": 0})()) if r != 0 else 0
     with open(os.path.join(outdir, f"rank{r}.json"), "w") as f:
-        json.dump({"lengths": ln.tolist(), "t_max": t_max, "t_max2": t_max2, "rc_ref": rc_ref}, f)
+        json.dump({"lengths": ln.tolist(), "index": idx.tolist(), "shards": [x.tolist() for x in shards],
+                   "t_max": t_max, "t_max2": t_max2, "rc_ref": rc_ref}, f)
     dist.destroy_process_group()
 
 
 @pytest.mark.timeout(120)
-def test_two_rank_replicas(tmp_path):
+def test_two_rank_shards(tmp_path):
+    sys.path.insert(0, ROOT)
+    import bench
+
     world = 2
     mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world,
                        join=True, start_method="spawn")
@@ -54,10 +59,13 @@ def test_two_rank_replicas(tmp_path):
     assert all(x["t_max"] == 11.0 for x in res)      # max over ranks
     assert all(x["t_max2"] == 0.0 for x in res)
     assert all(x["rc_ref"] == 0 for x in res)
-    a, b = (np.array(x["lengths"]) for x in res)
-    assert a.shape == b.shape == (64, 2) and not np.array_equal(a, b)  # independent batches
-    for x in (a, b):
-        assert x.min() >= 32 and x.max() <= 2048
+    # both ranks computed the same partition of the 128-pair job, and each ran its own shard
+    assert res[0]["shards"] == res[1]["shards"]
+    i0, i1 = (np.array(x["index"]) for x in res)
+    assert len(np.intersect1d(i0, i1)) == 0 and len(i0) + len(i1) == 128
+    job = bench.workload_lengths(3, 128)
+    for x, i in zip(res, (i0, i1)):
+        assert np.array_equal(np.array(x["lengths"]), job[i])
 
 
 def test_single_rank_needs_no_process_group():
