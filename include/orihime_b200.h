@@ -42,8 +42,11 @@ extern "C" {
 #define SWB_ERR_WORKSPACE (-2)
 #define SWB_ERR_CUDA (-3)
 
-/* Status bits written by kernels into the workspace status word. */
+/* Status bits written by kernels into the workspace status word.  The pairs
+ * concerned also come back NaN (value, dS/dparameters). */
 #define SWB_STATUS_WAIT_TIMEOUT 1u
+#define SWB_STATUS_BAD_LENGTHS 2u   /* lengths outside [0, padded size], checked on the device */
+#define SWB_STATUS_BAD_PARAMS 4u    /* device parameters invalid (params_device) */
 
 /* Optional launch knobs (pass NULL for defaults). */
 typedef struct swb_options {
@@ -54,6 +57,15 @@ typedef struct swb_options {
                                           adjoint kernel (per-kernel timing), or NULL     */
     int cols_per_lane;                 /* columns per lane of a band: 2 or 4 (0 = default) */
     int domain;                        /* local models: SWB_DOMAIN_AUTO (0), _LOG or _LINEAR */
+    const float* params_device;        /* local models, linear domain: device array
+                                          (gap_open, gap_ext, temp) or (gap, temp) that the
+                                          kernels read at run time instead of the float
+                                          arguments (a CUDA graph captured with tensor
+                                          parameters reads their current values at each
+                                          replay); NULL = use the floats.  The floats still
+                                          choose the domain: keep the gaps <= 0.  Invalid
+                                          device values give NaN results and
+                                          SWB_STATUS_BAD_PARAMS. */
 } swb_options;
 
 /* Arithmetic of the local-alignment kernels (swb_options.domain).  AUTO runs

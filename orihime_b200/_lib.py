@@ -22,6 +22,8 @@ ERR_WORKSPACE = -2
 ERR_CUDA = -3
 
 STATUS_WAIT_TIMEOUT = 1
+STATUS_BAD_LENGTHS = 2
+STATUS_BAD_PARAMS = 4
 
 
 class Options(ctypes.Structure):
@@ -34,6 +36,7 @@ class Options(ctypes.Structure):
         ("split_event", ctypes.c_void_p),
         ("cols_per_lane", ctypes.c_int),
         ("domain", ctypes.c_int),
+        ("params_device", ctypes.c_void_p),
     ]
 
 

@@ -148,9 +148,22 @@ def check_shape(scores: torch.Tensor, family: str) -> tuple[int, int, int]:
     return B, L1, L2
 
 
+def _capturing() -> bool:
+    """A CUDA graph is being captured on the current stream: no host
+    synchronisation is allowed, so range checks move to the device."""
+    return torch.cuda.is_available() and torch.cuda.is_current_stream_capturing()
+
+
 def resolve_lengths(lengths, B: int, L1: int, L2: int, device) -> torch.Tensor:
-    """Default or validate [B, 2] int32 lengths (validate_sw_affine_lengths_cuda)."""
+    """Default or validate [B, 2] int32 lengths (validate_sw_affine_lengths_cuda).
+
+    The value range check reads the lengths on the host, as the reference
+    does (same messages).  While a CUDA graph is being captured that read is
+    not allowed: the kernels then check the range on the device, clamp, and
+    return NaN for the pairs concerned (status bit SWB_STATUS_BAD_LENGTHS)."""
     if lengths is None:
+        if _capturing():   # torch.tensor from a host list would copy host -> device
+            return torch.tensor([L1, L2], dtype=torch.int32).to(device).expand(B, 2).contiguous()
         return torch.tensor([[L1, L2]] * B, dtype=torch.int32, device=device).reshape(B, 2)
     if not lengths.is_cuda:
         raise RuntimeError("lengths must be a CUDA tensor")
@@ -165,6 +178,8 @@ def resolve_lengths(lengths, B: int, L1: int, L2: int, device) -> torch.Tensor:
         raise RuntimeError("lengths must be int32")
     if lengths.device != device:
         raise RuntimeError(f"lengths must be on same device as scores, got {lengths.device} vs {device}")
+    if _capturing():
+        return lengths
     host = lengths.cpu().tolist()
     for b, (l1, l2) in enumerate(host):
         if not (0 <= l1 <= L1):
@@ -178,6 +193,23 @@ def _scalar_param(t: torch.Tensor, name: str) -> float:
     if t.numel() != 1:
         raise RuntimeError(f"{name} must be a scalar tensor")
     return float(t.detach().cpu().reshape(()).item())
+
+
+def _device_params(scores, *params):
+    """Under stream capture, the `_t` ops' tensor parameters as one float32
+    device array the kernels read at each replay (no .item()): returns
+    (options, placeholder floats).  Local families only (the linear-domain
+    kernels): the placeholders choose that domain, and the kernels mark every
+    pair NaN if a replayed value is not valid there (a positive gap or a
+    temperature that is not finite and > 0)."""
+    for t, n in zip(params, ("parameter",) * len(params)):
+        if t.numel() != 1:
+            raise RuntimeError(f"{n} must be a scalar tensor")
+    arr = torch.stack([t.detach().reshape(()).to(device=scores.device, dtype=torch.float32)
+                       for t in params]).contiguous()
+    opt = _lib.Options(0, 0, 0, None, 0, _lib.DOMAIN_LINEAR, arr.data_ptr())
+    opt._keep = arr   # the array must live as long as the captured graph uses it
+    return opt, [-1.0] * (len(params) - 1) + [1.0]
 
 
 # ---------------------------------------------------------------------------
@@ -301,6 +333,12 @@ def sw_affine_forward_t(scores, gap_open, gap_ext, temp, lengths):
     check_input_cuda(scores, "scores")
     if scores.dim() != 3:
         raise RuntimeError("scores must be 3D (B, L1, L2)")
+    if _capturing():
+        opt, (go, ge, T) = _device_params(scores, gap_open, gap_ext, temp)
+        B, L1, L2 = check_shape(scores, "sw_affine")
+        ln = resolve_lengths(lengths, B, L1, L2, scores.device)
+        v, m, *_ = run_affine(scores, ln, go, ge, T, options=opt)
+        return [v, m]
     go = _scalar_param(gap_open, "gap_open")
     ge = _scalar_param(gap_ext, "gap_ext")
     T = _scalar_param(temp, "temperature")
@@ -332,6 +370,12 @@ def sw_forward_t(scores, gap, temp, lengths):
     check_input_cuda(scores, "scores")
     if scores.dim() != 3:
         raise RuntimeError("scores must be 3D (B, L1, L2)")
+    if _capturing():
+        opt, (g, T) = _device_params(scores, gap, temp)
+        B, L1, L2 = check_shape(scores, "sw")
+        ln = resolve_lengths(lengths, B, L1, L2, scores.device)
+        v, m, *_ = run_linear(scores, ln, g, T, options=opt)
+        return [v, m]
     g = _scalar_param(gap, "gap")
     T = _scalar_param(temp, "temperature")
     B, L1, L2 = check_shape(scores, "sw")
@@ -446,7 +490,8 @@ def _aux_plan(fam, B, L1, L2, dev):
     max(2 GiB, half the free device memory))."""
     fn = getattr(_LIB, _AUX[fam][0])
     nbytes = int(fn(B, L1, L2))
-    free = torch.cuda.mem_get_info(dev)[0]
+    # the free-memory query is a host call; under stream capture use the floor
+    free = 0 if _capturing() else torch.cuda.mem_get_info(dev)[0]
     budget = min(AUX_BUDGET_MAX, max(2 << 30, free // 2))
     g = B
     if nbytes > budget:
@@ -816,7 +861,10 @@ class _ForwardFn(torch.autograd.Function):
         name = f"{fam}_forward" + ("_t" if tensor_params else "")
         v, m = _below(getattr(torch.ops.orihime, name), scores, *params, lengths)
         ctx.fam, ctx.tensor_params, ctx.lengths = fam, tensor_params, lengths
-        ctx.vals = tuple(_scalar_param(p, "param") if tensor_params else float(p) for p in params)
+        # the parameter values the backward ops take as floats; under stream
+        # capture a host read is not allowed, so the backward reads them
+        ctx.vals = (None if tensor_params and _capturing() else
+                    tuple(_scalar_param(p, "param") if tensor_params else float(p) for p in params))
         ctx.params = params
         ctx.save_for_backward(scores, m)
         return v, m
@@ -825,6 +873,8 @@ class _ForwardFn(torch.autograd.Function):
     def backward(ctx, gv, gm):
         scores, m = ctx.saved_tensors
         fam, vals, ln = ctx.fam, ctx.vals, ctx.lengths
+        if vals is None:
+            vals = tuple(_scalar_param(p, "param") for p in ctx.params)
         ops = torch.ops.orihime
         gs = torch.zeros_like(scores) if ctx.needs_input_grad[2] else None
         pg = [None] * len(ctx.params)

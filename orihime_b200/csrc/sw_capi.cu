@@ -241,6 +241,8 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   if (G == 0 && domain == SWB_DOMAIN_LINEAR && !lin) return SWB_ERR_ARG;
   a.xgo = (float)exp2(xo);
   a.xge = (float)exp2(xe);
+  a.dparams = opt ? opt->params_device : nullptr;
+  if (a.dparams && !lin) return SWB_ERR_ARG;   // device parameters: linear-domain kernels only
 
   // per-call resets: counters, status and completion counts to 0, cross-band
   // buffers to the NaN sentinel, the map to 0 (cells outside lengths stay 0)

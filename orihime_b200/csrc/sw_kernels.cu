@@ -235,6 +235,20 @@ __device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_
   return w;
 }
 
+// Lengths of pair p in a padded batch outside [0, padded size]: the kernels
+// clamp them (so nothing is read or written out of bounds); the first band
+// task of the pair marks it so its outputs come back NaN, and sets the
+// status bit.  (The host range-checks lengths with the reference's messages
+// before launching, except while a stream is being captured.)
+__device__ __forceinline__ void check_lengths(const Args& a, const Place& w, int lane) {
+  if (a.layout != 0 || !a.lengths || w.band != 0 || lane != 0) return;
+  const int l1 = a.lengths[2 * w.p], l2 = a.lengths[2 * w.p + 1];
+  if (l1 < 0 || l1 > a.Lmax1 || l2 < 0 || l2 > a.Lmax2) {
+    atomicOr(a.status, ERR_BAD_LENGTHS);
+    atomicOr(a.pair_done + w.p, PAIR_TIMEOUT);
+  }
+}
+
 template <int R>
 __device__ __forceinline__ void load_row(const Pair& pr, int i, int jl, bool ok, float (&o)[R]) {
   // i: 1-based row; jl: 0-based first column of the lane
@@ -701,6 +715,7 @@ __device__ void fwd_band(const Args& a, const Place& w, int lane, uint64_t deadl
   [[maybe_unused]] constexpr bool SV = GM == 2;
   using D = Dims<NS, R>;
   constexpr int NE = D::NE;
+  check_lengths(a, w, lane);
   const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
   const int band = w.band;
@@ -1046,11 +1061,24 @@ __global__ void __launch_bounds__(128) value_kernel(Args a) {
   if (lane == 0) a.value[w.p] = (Sh + Sl) * (1.f / a.k);
 }
 
+// Parameters a pair's finish needs (natural units, and k = log2(e) / T).
+struct PParams { float go, ge, T, k; };
+
 // Last band task of a pair to finish folds the per-band gradient partials (in
 // band order, so the result is deterministic) into the outputs.
 template <int NS, int GM = 0>
+__device__ void finish_pair_p(const Args& a, const Place& w, int lane, float Sh, float Sl,
+                              float g0sum, float g1sum, float pssum, PParams pp);
+
+template <int NS, int GM = 0>
 __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, float Sl,
                             float g0sum, float g1sum, float pssum) {
+  finish_pair_p<NS, GM>(a, w, lane, Sh, Sl, g0sum, g1sum, pssum, PParams{a.go, a.ge, a.T, a.k});
+}
+
+template <int NS, int GM>
+__device__ void finish_pair_p(const Args& a, const Place& w, int lane, float Sh, float Sl,
+                              float g0sum, float g1sum, float pssum, PParams pp) {
   constexpr bool G = GM == 1;
   const int p = w.p;
   if (lane == 0) {
@@ -1073,7 +1101,7 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
         e += ld_poll(q + 1);
         ps += ld_poll(q + 2);
       }
-      const float inv_k = 1.f / a.k;          // = T * ln 2
+      const float inv_k = 1.f / pp.k;         // = T * ln 2
       const float S = (Sh + Sl) * inv_k;
       const float match = ps * inv_k;
       if (G && (w.pr.L1 == 0 || w.pr.L2 == 0)) {
@@ -1089,11 +1117,11 @@ __device__ void finish_pair(const Args& a, const Place& w, int lane, float Sh, f
       if (NS == 3) {
         a.g_open[p] = o;
         a.g_ext[p] = e;
-        a.g_T[p] = (S - (match + (o * a.go + e * a.ge))) / a.T;
+        a.g_T[p] = (S - (match + (o * pp.go + e * pp.ge))) / pp.T;
       } else {
         a.g_open[p] = o;
         if (a.g_ext) a.g_ext[p] = 0.f;
-        a.g_T[p] = (S - (match + o * a.go)) / a.T;
+        a.g_T[p] = (S - (match + o * pp.go)) / pp.T;
       }
     }
   }

@@ -78,6 +78,8 @@ enum PlanWord : int {
 
 enum : unsigned {
   ERR_WAIT_TIMEOUT = 1u,
+  ERR_BAD_LENGTHS = 2u,      // a pair's lengths outside [0, padded size] (checked on the device)
+  ERR_BAD_PARAMS = 4u,       // device parameters: temperature not finite > 0, or a positive gap
 };
 
 // Launch arguments shared by the forward and adjoint kernels.
@@ -94,6 +96,8 @@ struct Args {
   int layout;                 // 0 padded, 1 ragged packed via plan (row pitch = round4(L2))
   float go, ge, T, k;         // gaps in natural units, temperature, k = log2(e)/T
   float xgo, xge;             // linear-domain kernels: transition factors 2^(go k), 2^(ge k)
+  const float* dparams;       // linear-domain kernels: (go, ge, T) or (gap, T) read on the device
+                              // instead of go, ge, T (graph capture with tensor parameters), or null
   int nb;                     // bands per pair (uniform, >= ceil(max L2 / 32R))
   int nchunks;                // checkpoint chunks per band (>= ceil((max L1+31)/C))
   // outputs [B]

@@ -285,6 +285,31 @@ __device__ __forceinline__ void lscores(const float (&sb)[R], int i, float k, in
   }
 }
 
+// Parameters of a linear-domain launch: the launch's floats, or read from the
+// device parameter array when there is one (a stream capture with tensor
+// parameters: each replay reads their current values).  k and the transition
+// factors are formed exactly as the host forms them.  ok is false for a
+// temperature that is not finite and positive or a positive gap: the linear
+// domain needs every transition factor <= 1.
+struct LParams {
+  float go, ge, T, k, xgo, xge;
+  bool ok;
+};
+template <int NS>
+__device__ __forceinline__ LParams lparams(const Args& a) {
+  LParams p{a.go, a.ge, a.T, a.k, a.xgo, a.xge, true};
+  if (a.dparams) {
+    p.go = a.dparams[0];
+    p.ge = NS == 3 ? a.dparams[1] : 0.f;
+    p.T = a.dparams[NS == 3 ? 2 : 1];
+    p.k = 1.4426950408889634f / p.T;
+    p.xgo = (float)exp2((double)p.go * (double)p.k);
+    p.xge = (float)exp2((double)p.ge * (double)p.k);
+    p.ok = p.T > 0.f && p.T < INFINITY && p.go * p.k <= 0.f && p.ge * p.k <= 0.f;
+  }
+  return p;
+}
+
 // ---------------------------------------------------------------------------
 // forward band task
 // ---------------------------------------------------------------------------
@@ -295,8 +320,14 @@ __device__ __forceinline__ void lscores(const float (&sb)[R], int i, float k, in
 // of the lane state plus the chunk's largest normalised frame.  The band's
 // partition partial is (frame, mantissa sum): Z_band = sum * 2^frame.
 template <int NS, int R>
-__device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t deadline) {
+__device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int lane,
+                          uint64_t deadline) {
   using LD = LDims<NS, R>;
+  check_lengths(a, w, lane);
+  if (!lp.ok && w.band == 0 && lane == 0) {
+    atomicOr(a.status, ERR_BAD_PARAMS);
+    atomicOr(a.pair_done + w.p, PAIR_TIMEOUT);
+  }
   const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
   const int band = w.band;
@@ -310,7 +341,7 @@ __device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t dead
   const int jl = col0 + lane * R;
   const int nlive = min(max(L2 - jl, 0), R);
   const bool has_dead = __any_sync(FULL, nlive < R);
-  const float k = a.k, gO = a.xgo, gE = a.xge;
+  const float k = lp.k, gO = lp.xgo, gE = lp.xge;
   const size_t Lm = (size_t)w.Lm;
   float* eout = a.edge + w.ed0 + (size_t)band * w.edb;
   const float* ein = (band > 0) ? eout - w.edb : nullptr;
@@ -447,6 +478,7 @@ __device__ void lfwd_band(const Args& a, const Place& w, int lane, uint64_t dead
 template <int NS, int R>
 __global__ void __launch_bounds__(128, SWB_LFWD_MINB) lfwd_kernel(Args a) {
   const int lane = threadIdx.x & 31;
+  const LParams lp = lparams<NS>(a);
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
   const int ntasks = (a.layout == 0) ? a.B * a.nb : a.ntasks;
   while (true) {
@@ -454,7 +486,7 @@ __global__ void __launch_bounds__(128, SWB_LFWD_MINB) lfwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 0, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    lfwd_band<NS, R>(a, place_of<NS, R>(a, task, false), lane, deadline);
+    lfwd_band<NS, R>(a, lp, place_of<NS, R>(a, task, false), lane, deadline);
   }
 }
 
@@ -528,7 +560,7 @@ __global__ void __launch_bounds__(128) lvalue_kernel(Args a) {
   float zm, Sh, Sl;
   lpair_z(a, w, lane, ze, zm);
   lz_log2(ze, zm, Sh, Sl);
-  if (lane == 0) a.value[w.p] = (Sh + Sl) * (1.f / a.k);
+  if (lane == 0) a.value[w.p] = (Sh + Sl) * (1.f / lparams<NS>(a).k);
 }
 
 // ---------------------------------------------------------------------------
@@ -554,7 +586,8 @@ __host__ __device__ constexpr int lbwd_smem_floats() {
 // buffer; lane 31 reads the right band's.  No atomics; the map is written row
 // by row; the gradient sums are folded per pair in band order.
 template <int NS, int R>
-__device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, uint64_t deadline) {
+__device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int lane, float* sm,
+                          uint64_t deadline) {
   using LD = LDims<NS, R>;
   constexpr int CKF = LD::CKF, CKRS = LD::CKRS, FW = LD::FW, NEF = NS + 1, NPF = 3;
   const Pair& pr = w.pr;
@@ -565,15 +598,16 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
   float zm, Sh, Sl;
   lpair_z(a, w, lane, ze, zm);
   lz_log2(ze, zm, Sh, Sl);
+  const PParams pp{lp.go, lp.ge, lp.T, lp.k};
   if (!(L1 > 0 && col0 < L2)) {
-    finish_pair<NS>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f);
+    finish_pair_p<NS>(a, w, lane, Sh, Sl, 0.f, 0.f, 0.f, pp);
     return;
   }
   const float invZ = 1.f / zm;
   const int jl = col0 + lane * R;
   const int nlive = min(max(L2 - jl, 0), R);
   const bool has_dead = __any_sync(FULL, nlive < R);
-  const float k = a.k, gO = a.xgo, gE = a.xge, gX = fmaxf(gO, gE);
+  const float k = lp.k, gO = lp.xgo, gE = lp.xge, gX = fmaxf(gO, gE);
   const size_t Lm = (size_t)w.Lm;
   const float* ein = (band > 0) ? a.edge + w.ed0 + (size_t)(band - 1) * w.edb : nullptr;
   float* pout = (band > 0) ? a.bpush + w.bp0 + (size_t)band * w.bpb : nullptr;
@@ -967,7 +1001,7 @@ __device__ void lbwd_band(const Args& a, const Place& w, int lane, float* sm, ui
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
   }
-  finish_pair<NS>(a, w, lane, Sh, Sl, v0, v1, v2);
+  finish_pair_p<NS>(a, w, lane, Sh, Sl, v0, v1, v2, pp);
 }
 
 template <int NS, int R, int WARPS>
@@ -976,6 +1010,7 @@ __global__ void __launch_bounds__(32 * WARPS) lbwd_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const int wi = threadIdx.x >> 5;
   float* sm = smem + (size_t)wi * lbwd_smem_floats<NS, R>();
+  const LParams lp = lparams<NS>(a);
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
   const int ntasks = (a.layout == 0) ? a.B * a.nb : a.ntasks;
   while (true) {
@@ -983,7 +1018,7 @@ __global__ void __launch_bounds__(32 * WARPS) lbwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    lbwd_band<NS, R>(a, place_of<NS, R>(a, task, true), lane, sm, deadline);
+    lbwd_band<NS, R>(a, lp, place_of<NS, R>(a, task, true), lane, sm, deadline);
   }
 }
 
