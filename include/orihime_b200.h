@@ -405,6 +405,39 @@ int swb_nw_param_jacobian(const float* scores, const int* lengths, int B, int L1
 int swb_scan_scores(const float* x, int B, long long per_item, float limit, float sentinel,
                     unsigned* words, float* amax, void* stream);
 
+/*
+ * Checkpointed value, in two launches (no reference counterpart: the
+ * reference's forward op runs the forward and the backward together and
+ * keeps the full alpha table for the map).  swb_*_checkpoint runs the
+ * forward wavefront alone: it writes the value and leaves in the workspace
+ * the DP state of every `ck_every`-th checkpoint chunk (4 wavefront steps
+ * per chunk), the band partials and the cross-band edge records; nothing
+ * else is kept.  swb_*_adjoint, later, on the same workspace, scores,
+ * lengths and parameters, runs the checkpointed adjoint: the marginal map
+ * and dS/dparameters (and the value again).  It can run more than once.
+ * ck_every in [1, 16]: 1 keeps a checkpoint per chunk (the fastest
+ * adjoint); 4 keeps about 1.3 bytes per cell of the padded batch, and the
+ * adjoint recomputes the chunks in between from the nearest checkpoint.
+ * The local families in the linear domain only: gaps must be <= 0, else
+ * SWB_ERR_ARG.  4 columns per lane.  Workspace from
+ * swb_*_checkpoint_workspace_bytes(B, L1max, L2max, ck_every).
+ */
+size_t swb_sw_affine_checkpoint_workspace_bytes(int B, int L1max, int L2max, int ck_every);
+int swb_sw_affine_checkpoint(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                             float gap_open, float gap_ext, float temp, int ck_every, float* value,
+                             void* workspace, size_t workspace_bytes, void* stream);
+int swb_sw_affine_adjoint(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap_open, float gap_ext, float temp, int ck_every, float* value,
+                          float* map, float* grad_open, float* grad_ext, float* grad_temp,
+                          void* workspace, size_t workspace_bytes, void* stream);
+size_t swb_sw_checkpoint_workspace_bytes(int B, int L1max, int L2max, int ck_every);
+int swb_sw_checkpoint(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                      float gap, float temp, int ck_every, float* value, void* workspace,
+                      size_t workspace_bytes, void* stream);
+int swb_sw_adjoint(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
+                   float temp, int ck_every, float* value, float* map, float* grad_gap,
+                   float* grad_temp, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Copies the workspace status word to *status (synchronises `stream`).
  * No reference counterpart: the reference synchronises inside every op.
  * A bounded wait that expires also shows in the results without this call:

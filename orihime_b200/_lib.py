@@ -174,6 +174,18 @@ def load() -> ctypes.CDLL:
     lib.swb_sv_affine_hvp.argtypes = [vp, vp, vp, i, i, i, f, f, f, vp, vp, vp, sz, vp]
     lib.swb_sv_affine_param_jacobian.restype = i
     lib.swb_sv_affine_param_jacobian.argtypes = [vp, vp, i, i, i, f, f, f, i, vp, vp, sz, vp]
+    lib.swb_sw_affine_checkpoint_workspace_bytes.restype = sz
+    lib.swb_sw_affine_checkpoint_workspace_bytes.argtypes = [i, i, i, i]
+    lib.swb_sw_checkpoint_workspace_bytes.restype = sz
+    lib.swb_sw_checkpoint_workspace_bytes.argtypes = [i, i, i, i]
+    lib.swb_sw_affine_checkpoint.restype = i
+    lib.swb_sw_affine_checkpoint.argtypes = [vp, vp, i, i, i, f, f, f, i, vp, vp, sz, vp]
+    lib.swb_sw_affine_adjoint.restype = i
+    lib.swb_sw_affine_adjoint.argtypes = [vp, vp, i, i, i, f, f, f, i, vp, vp, vp, vp, vp, vp, sz, vp]
+    lib.swb_sw_checkpoint.restype = i
+    lib.swb_sw_checkpoint.argtypes = [vp, vp, i, i, i, f, f, i, vp, vp, sz, vp]
+    lib.swb_sw_adjoint.restype = i
+    lib.swb_sw_adjoint.argtypes = [vp, vp, i, i, i, f, f, i, vp, vp, vp, vp, vp, sz, vp]
     lib.swb_mufu_probe.restype = i
     lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()

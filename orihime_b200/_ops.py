@@ -312,6 +312,57 @@ def run_value(fam, scores, lengths, params):
     return value
 
 
+# ---- checkpointed value: forward now, adjoint in the backward ---------------
+
+def run_checkpoint(fam, scores, lengths, params, ck_every):
+    """Forward wavefront only (local families, gaps <= 0): value [B] and the
+    workspace holding the checkpoints the adjoint needs later, or None when
+    the parameters need the log-domain kernels (a positive gap)."""
+    B, L1, L2 = scores.shape
+    dev = scores.device
+    value = torch.empty(B, dtype=torch.float32, device=dev)
+    affine = fam == "sw_affine"
+    if any(float(p) > 0 for p in params[:-1]) or B == 0:
+        return None
+    nbytes = int((_LIB.swb_sw_affine_checkpoint_workspace_bytes if affine
+                  else _LIB.swb_sw_checkpoint_workspace_bytes)(B, L1, L2, ck_every))
+    ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    with torch.cuda.device(dev):
+        if affine:
+            rc = _LIB.swb_sw_affine_checkpoint(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params),
+                                               int(ck_every), _ptr(value), _ptr(ws), nbytes, _stream(dev))
+        else:
+            rc = _LIB.swb_sw_checkpoint(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params),
+                                        int(ck_every), _ptr(value), _ptr(ws), nbytes, _stream(dev))
+    _lib.check(rc, "swb_sw_checkpoint")
+    return value, ws
+
+
+def run_adjoint(fam, scores, lengths, params, ck_every, ws):
+    """The checkpointed adjoint on a run_checkpoint workspace: (value, map,
+    dS/dparameters...)."""
+    B, L1, L2 = scores.shape
+    dev = scores.device
+    e = lambda: torch.empty(B, dtype=torch.float32, device=dev)  # noqa: E731
+    value, amap = e(), torch.empty_like(scores)
+    nbytes = ws.numel()
+    with torch.cuda.device(dev):
+        if fam == "sw_affine":
+            go, ge, gT = e(), e(), e()
+            rc = _LIB.swb_sw_affine_adjoint(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params),
+                                            int(ck_every), _ptr(value), _ptr(amap), _ptr(go), _ptr(ge),
+                                            _ptr(gT), _ptr(ws), nbytes, _stream(dev))
+            grads = (go, ge, gT)
+        else:
+            gg, gT = e(), e()
+            rc = _LIB.swb_sw_adjoint(_ptr(scores), _ptr(lengths), B, L1, L2, *map(float, params),
+                                     int(ck_every), _ptr(value), _ptr(amap), _ptr(gg), _ptr(gT), _ptr(ws),
+                                     nbytes, _stream(dev))
+            grads = (gg, gT)
+    _lib.check(rc, "swb_sw_adjoint")
+    return (value, amap, *grads)
+
+
 def _prep(scores, lengths, family):
     check_input_cuda(scores, "scores")
     B, L1, L2 = check_shape(scores, family)

@@ -51,6 +51,7 @@ struct Layout {
   size_t off_hdr, off_pair_done, off_part, off_gpart, off_sent, off_edge, off_bpush, off_ckpt;
   size_t sent_bytes;   // sentinel-initialised span (never_written + edge + bpush)
   size_t total;
+  size_t ck_band = 0;  // checkpoint floats per band slot when not nchunks records
 };
 
 // Workspace layout for `slots` band slots and the given buffer sizes (floats).
@@ -106,6 +107,7 @@ struct DevInfo {
   int sms = 0;
   int occ[2][5][2] = {};   // [kernel fwd/bwd][model_index][R == 4?]
   int locc[2][2][2] = {};  // linear-domain kernels: [fwd/bwd][NS == 3?][R == 4?]
+  int locc_sparse[2] = {}; // linear-domain adjoint with sparse checkpoints (R = 4): [NS == 3?]
   bool ready = false;
 };
 DevInfo g_dev[64];
@@ -131,8 +133,15 @@ cudaError_t setup_lin(DevInfo& d) {
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.locc[0][NS == 3][R == 4],
                                                     swb::lfwd_kernel<NS, R>, 32 * kWarpsFwd, 0);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &d.locc[1][NS == 3][R == 4], swb::lbwd_kernel<NS, R, kWarpsBwd>, 32 * kWarpsBwd,
+      lbwd_smem<NS, R>());
+  if (e != cudaSuccess || R != kDefaultR) return e;
+  e = cudaFuncSetAttribute(swb::lbwd_kernel<NS, R, kWarpsBwd, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lbwd_smem<NS, R>());
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &d.locc_sparse[NS == 3], swb::lbwd_kernel<NS, R, kWarpsBwd, true>, 32 * kWarpsBwd,
       lbwd_smem<NS, R>());
 }
 
@@ -241,6 +250,7 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
   if (G == 0 && domain == SWB_DOMAIN_LINEAR && !lin) return SWB_ERR_ARG;
   a.xgo = (float)exp2(xo);
   a.xge = (float)exp2(xe);
+  if (a.ck_every < 1) a.ck_every = 1;
   a.dparams = opt ? opt->params_device : nullptr;
   if (a.dparams && !lin) return SWB_ERR_ARG;   // device parameters: linear-domain kernels only
 
@@ -519,9 +529,167 @@ int launch_xband(const float* scores, const float* v, const int* lengths, int B,
   return l.R == 4 ? launch_xband_r<NS, 4, MODE, G>(a, st) : launch_xband_r<NS, 2, MODE, G>(a, st);
 }
 
+// ---- checkpointed value: forward now (checkpoints kept), adjoint later ----
+
+constexpr int kMaxCkEvery = 16;
+
+template <int NS>
+Layout ck_layout(long long B, long long L1m, long long L2m, int kc) {
+  constexpr int R = kDefaultR;
+  using LD = swb::LDims<NS, R>;
+  int nb = (int)((L2m + 32 * R - 1) / (32 * R));
+  if (nb < 1) nb = 1;
+  const int nch = chunks_for(L1m);
+  const size_t band = ((size_t)((nch + kc - 1) / kc) * LD::LREC + (size_t)nch + 3) / 4 * 4;
+  const size_t slots = (size_t)B * nb;
+  Layout l = layout_sizes(B, slots, slots * ne<NS, R>() * (size_t)L1m,
+                          slots * np<NS, 0>() * (size_t)(L1m + 1), slots * band);
+  l.nb = nb;
+  l.nchunks = nch;
+  l.ck_band = band;
+  return l;
+}
+
+// Shared set-up of the two halves: argument checks, parameters (linear
+// domain only), workspace pointers.  Returns SWB_OK or an error code.
+template <int NS>
+int ck_setup(Args& a, Layout& l, const float* scores, const int* lengths, int B, int L1m, int L2m,
+             float go, float ge, float T, int kc, void* ws, size_t ws_bytes) {
+  if (B < 0 || L1m < 0 || L2m < 0 || kc < 1 || kc > kMaxCkEvery) return SWB_ERR_ARG;
+  if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
+  if ((size_t)B * L1m * L2m > 0 && !scores) return SWB_ERR_ARG;
+  a = Args{};
+  a.k = 1.4426950408889634f / T;
+  const double xo = (double)go * (double)a.k, xe = NS == 3 ? (double)ge * (double)a.k : 0.0;
+  if (!(xo <= 0.0 && xe <= 0.0)) return SWB_ERR_ARG;   // the linear domain needs gaps <= 0
+  l = ck_layout<NS>(B, L1m, L2m, kc);
+  if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
+  char* w = static_cast<char*>(ws);
+  a.scores = scores; a.lengths = lengths;
+  a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
+  a.go = go; a.ge = NS == 3 ? ge : 0.f; a.T = T;
+  a.xgo = (float)exp2(xo);
+  a.xge = (float)exp2(xe);
+  a.nb = l.nb; a.nchunks = l.nchunks;
+  a.ck_every = kc;
+  a.ck_band_floats = l.ck_band;
+  a.counters = reinterpret_cast<unsigned*>(w + l.off_hdr);
+  a.status = a.counters + 4;
+  a.pair_done = reinterpret_cast<unsigned*>(w + l.off_pair_done);
+  a.part = reinterpret_cast<float*>(w + l.off_part);
+  a.gpart = reinterpret_cast<float*>(w + l.off_gpart);
+  a.never_written = reinterpret_cast<float*>(w + l.off_sent);
+  a.edge = reinterpret_cast<float*>(w + l.off_edge);
+  a.bpush = reinterpret_cast<float*>(w + l.off_bpush);
+  a.ckpt = reinterpret_cast<float*>(w + l.off_ckpt);
+  a.spin_limit_ns = 20ull * 1000000000ull;
+  return SWB_OK;
+}
+
+template <int NS>
+int ck_forward(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
+               float T, int kc, float* value, void* ws, size_t ws_bytes, void* stream_v) {
+  constexpr int R = kDefaultR;
+  Args a;
+  Layout l;
+  int rc = ck_setup<NS>(a, l, scores, lengths, B, L1m, L2m, go, ge, T, kc, ws, ws_bytes);
+  if (rc != SWB_OK) return rc;
+  if (B == 0) return SWB_OK;
+  if (!value) return SWB_ERR_ARG;
+  a.value = value;
+  DevInfo* d = nullptr;
+  if ((rc = dev_info(&d)) != SWB_OK) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream_v);
+  char* w = static_cast<char*>(ws);
+  if (cudaMemsetAsync(w, 0, l.off_part, st) != cudaSuccess) return SWB_ERR_CUDA;
+  if (cudaMemsetAsync(w + l.off_sent, 0xff, l.sent_bytes, st) != cudaSuccess) return SWB_ERR_CUDA;
+  const long long ntasks = (long long)B * l.nb;
+  const int of = d->locc[0][NS == 3][1];
+  const long long cap = (long long)d->sms * (of > 0 ? of : 1);
+  const int grid = (int)std::max(1LL, std::min((ntasks + kWarpsFwd - 1) / kWarpsFwd, cap));
+  swb::lfwd_kernel<NS, R><<<grid, 32 * kWarpsFwd, 0, st>>>(a);
+  swb::lvalue_kernel<NS, R><<<(B + 3) / 4, 128, 0, st>>>(a);
+  return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+}
+
+template <int NS>
+int ck_adjoint(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
+               float T, int kc, float* value, float* map, float* g_open, float* g_ext, float* g_T,
+               void* ws, size_t ws_bytes, void* stream_v) {
+  constexpr int R = kDefaultR;
+  Args a;
+  Layout l;
+  int rc = ck_setup<NS>(a, l, scores, lengths, B, L1m, L2m, go, ge, T, kc, ws, ws_bytes);
+  if (rc != SWB_OK) return rc;
+  if (B == 0) return SWB_OK;
+  const size_t map_elems = (size_t)B * L1m * L2m;
+  if (!value || !g_open || !g_T || (NS == 3 && !g_ext) || (map_elems > 0 && !map)) return SWB_ERR_ARG;
+  a.value = value; a.map = map; a.g_open = g_open; a.g_ext = g_ext; a.g_T = g_T;
+  DevInfo* d = nullptr;
+  if ((rc = dev_info(&d)) != SWB_OK) return rc;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream_v);
+  char* w = static_cast<char*>(ws);
+  // the forward's edge records, partials and checkpoints stay; the adjoint's
+  // counter, the completion counts (not the failure flags) and the push
+  // records are reset, so the adjoint can run more than once
+  swb::adjoint_reset_kernel<<<(B + 255) / 256, 256, 0, st>>>(a.counters, a.pair_done, B);
+  if (cudaMemsetAsync(w + l.off_bpush, 0xff, l.off_ckpt - l.off_bpush, st) != cudaSuccess)
+    return SWB_ERR_CUDA;
+  if (map_elems > 0 && cudaMemsetAsync(map, 0, map_elems * sizeof(float), st) != cudaSuccess)
+    return SWB_ERR_CUDA;
+  const long long ntasks = (long long)B * l.nb;
+  const int ob = kc > 1 ? d->locc_sparse[NS == 3] : d->locc[1][NS == 3][1];
+  const long long cap = (long long)d->sms * (ob > 0 ? ob : 1);
+  const int grid = (int)std::max(1LL, std::min((ntasks + kWarpsBwd - 1) / kWarpsBwd, cap));
+  if (kc > 1)
+    swb::lbwd_kernel<NS, R, kWarpsBwd, true><<<grid, 32 * kWarpsBwd, lbwd_smem<NS, R>(), st>>>(a);
+  else
+    swb::lbwd_kernel<NS, R, kWarpsBwd><<<grid, 32 * kWarpsBwd, lbwd_smem<NS, R>(), st>>>(a);
+  return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+}
+
 }  // namespace
 
 extern "C" {
+
+size_t swb_sw_affine_checkpoint_workspace_bytes(int B, int L1max, int L2max, int ck_every) {
+  if (B <= 0 || ck_every < 1 || ck_every > kMaxCkEvery) return 0;
+  return ck_layout<3>(B, L1max, L2max, ck_every).total;
+}
+
+size_t swb_sw_checkpoint_workspace_bytes(int B, int L1max, int L2max, int ck_every) {
+  if (B <= 0 || ck_every < 1 || ck_every > kMaxCkEvery) return 0;
+  return ck_layout<1>(B, L1max, L2max, ck_every).total;
+}
+
+int swb_sw_affine_checkpoint(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                             float gap_open, float gap_ext, float temp, int ck_every, float* value,
+                             void* workspace, size_t workspace_bytes, void* stream) {
+  return ck_forward<3>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, ck_every, value,
+                       workspace, workspace_bytes, stream);
+}
+
+int swb_sw_affine_adjoint(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                          float gap_open, float gap_ext, float temp, int ck_every, float* value,
+                          float* map, float* grad_open, float* grad_ext, float* grad_temp,
+                          void* workspace, size_t workspace_bytes, void* stream) {
+  return ck_adjoint<3>(scores, lengths, B, L1max, L2max, gap_open, gap_ext, temp, ck_every, value,
+                       map, grad_open, grad_ext, grad_temp, workspace, workspace_bytes, stream);
+}
+
+int swb_sw_checkpoint(const float* scores, const int* lengths, int B, int L1max, int L2max,
+                      float gap, float temp, int ck_every, float* value, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+  return ck_forward<1>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, ck_every, value, workspace,
+                       workspace_bytes, stream);
+}
+
+int swb_sw_adjoint(const float* scores, const int* lengths, int B, int L1max, int L2max, float gap,
+                   float temp, int ck_every, float* value, float* map, float* grad_gap,
+                   float* grad_temp, void* workspace, size_t workspace_bytes, void* stream) {
+  return ck_adjoint<1>(scores, lengths, B, L1max, L2max, gap, 0.f, temp, ck_every, value, map,
+                       grad_gap, nullptr, grad_temp, workspace, workspace_bytes, stream);
+}
 
 size_t swb_sw_affine_aux_workspace_bytes(int B, int L1max, int L2max) {
   return B > 0 ? xlayout<3>(B, L1max, L2max).total : 0;

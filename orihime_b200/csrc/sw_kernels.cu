@@ -191,7 +191,7 @@ __device__ __forceinline__ Place place_of(const Args& a, int task, bool reverse_
     w.band = reverse_band ? a.nb - 1 - j : j;
     w.slot0 = (size_t)p * a.nb;
     w.Lm = a.Lmax1;
-    w.ckb = (size_t)a.nchunks * CKRS;
+    w.ckb = a.ck_band_floats ? a.ck_band_floats : (size_t)a.nchunks * CKRS;
     w.edb = (size_t)NE * a.Lmax1;
     w.bpb = (size_t)NP * (a.Lmax1 + 1);
     w.ck0 = w.slot0 * w.ckb;

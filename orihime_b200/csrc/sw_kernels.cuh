@@ -100,6 +100,8 @@ struct Args {
                               // instead of go, ge, T (graph capture with tensor parameters), or null
   int nb;                     // bands per pair (uniform, >= ceil(max L2 / 32R))
   int nchunks;                // checkpoint chunks per band (>= ceil((max L1+31)/C))
+  int ck_every;               // linear-domain kernels: a checkpoint every ck_every chunks (>= 1)
+  size_t ck_band_floats;      // layout 0: checkpoint floats per band slot (0: nchunks records)
   // outputs [B]
   float* value;
   float* g_open;              // affine: dS/dgo ; linear: dS/dgap

@@ -115,14 +115,16 @@ __device__ __forceinline__ void stage_row(float* dst, const Pair& pr, int i, int
   }
 }
 
-// Checkpoint floats per lane (LCKF, padded to float4), chunk record floats
-// (LCKRS: checkpoint groups, then the chunk's largest normalised frame, then
-// padding) and adjoint shared-memory floats per lane per step (LFW).
+// Checkpoint floats per lane (CKF, padded to float4), one checkpoint record
+// (LREC: CK4 groups of [lane][4]) and adjoint shared-memory floats per lane
+// per step (FW).  A band's checkpoint region holds ceil(nchunks / ck_every)
+// records, then one float per chunk: the chunk's largest normalised alpha
+// frame (the adjoint's quiet-chunk test).
 template <int NS, int R> struct LDims {
   static constexpr int CKV = NS * R + NS + 3;          // raw row, left values, e, n, nl
   static constexpr int CKF = (CKV + 3) / 4 * 4;
   static constexpr int CK4 = CKF / 4;
-  static constexpr int CKRS = CKF * 32 + 4;
+  static constexpr int LREC = CKF * 32;
   // affine: M, I, D (raw) and the scaled score per column; linear: A, the
   // emission part E (A_diag + 1), and the scaled score; then e and n
   static constexpr int NF = NS == 3 ? 4 : 3;
@@ -350,6 +352,8 @@ __device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int 
   const bool keep_ck = a.ckpt != nullptr;
   float* ck = keep_ck ? a.ckpt + w.ck0 + (size_t)band * w.ckb : nullptr;
   const int nch = band_chunks(L1);
+  const int KC = a.ck_every;
+  float* ckmax = keep_ck ? ck + (size_t)((nch + KC - 1) / KC) * LD::LREC : nullptr;
 
   LState<NS, R> s;
   lstate_zero(s);
@@ -404,7 +408,7 @@ __device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int 
         }
       }
     }
-    if (keep_ck) lck_store<NS, R>(ck + (size_t)kc * LD::CKRS, lane, s);
+    if (keep_ck && kc % KC == 0) lck_store<NS, R>(ck + (size_t)(kc / KC) * LD::LREC, lane, s);
     int cmx = -(1 << 30);   // largest normalised frame of the lane's live rows in this chunk
     if (kc + 1 < nch) load_edge(kc + 1, ebn);
 #pragma unroll 1
@@ -458,7 +462,7 @@ __device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int 
     for (int f = 0; f < NEF; ++f) eb[f] = ebn[f];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cmx = max(cmx, __shfl_xor_sync(FULL, cmx, o));
-    if (keep_ck && lane == 0) ck[(size_t)kc * LD::CKRS + LD::CKF * 32] = __int_as_float(cmx);
+    if (keep_ck && lane == 0) ckmax[kc] = __int_as_float(cmx);
   }
   // warp-combine (frame, sum) pairs, fixed shuffle tree
 #pragma unroll
@@ -585,11 +589,11 @@ __host__ __device__ constexpr int lbwd_smem_floats() {
 // Lane 0 passes the same three values to the left band through the push
 // buffer; lane 31 reads the right band's.  No atomics; the map is written row
 // by row; the gradient sums are folded per pair in band order.
-template <int NS, int R>
+template <int NS, int R, bool SPARSE = false>
 __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int lane, float* sm,
                           uint64_t deadline) {
   using LD = LDims<NS, R>;
-  constexpr int CKF = LD::CKF, CKRS = LD::CKRS, FW = LD::FW, NEF = NS + 1, NPF = 3;
+  constexpr int CKF = LD::CKF, LREC = LD::LREC, FW = LD::FW, NEF = NS + 1, NPF = 3;
   const Pair& pr = w.pr;
   const int L1 = pr.L1, L2 = pr.L2;
   const int band = w.band;
@@ -615,6 +619,8 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
   const float* pin = right_live ? a.bpush + w.bp0 + (size_t)(band + 1) * w.bpb : nullptr;
   const float* ck = a.ckpt + w.ck0 + (size_t)band * w.ckb;
   const int nch = band_chunks(L1);
+  const int KC = SPARSE ? a.ck_every : 1;   // checkpoint records every KC chunks
+  const float* ckmax = ck + (size_t)((nch + KC - 1) / KC) * LREC;
 
   // ---- chunk-ahead prefetch state: the next chunk's checkpoint and first
   // PF score rows are staged in shared memory (cp.async), the rest here ----
@@ -623,11 +629,11 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
   int ckm;                 // the next chunk's largest normalised alpha frame
   float ebr[NEF];          // lane u < C: left-band edge record of lane 0's row at recompute step u
   float pbc[NPF], pbn[NPF];// lane u < C: right-band record lane 31 needs at backward step u
-  auto load_ck = [&](int kc) {
-    const float* rec = ck + (size_t)kc * CKRS;
+  auto load_ck = [&](int kc) {   // the record at or before chunk kc, and kc's alpha frame
+    const float* rec = ck + (size_t)(kc / KC) * LREC;
 #pragma unroll
     for (int g = 0; g < LD::CK4; ++g) lcp16(stg_ck + g * 128 + lane * 4, rec + g * 128 + lane * 4, 16);
-    ckm = __float_as_int(rec[CKF * 32]);
+    ckm = __float_as_int(ckmax[kc]);
   };
   auto load_eb = [&](int kc) {
     const int i = kc * C_STEPS + lane + 1;
@@ -764,7 +770,7 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
               written = !is_sentinel(r0) && !is_sentinel(r1) && !is_sentinel(r2);
               rn2 = __float_as_int(r2);
             }
-            cm = __float_as_int(ck[(size_t)kq * CKRS + CKF * 32]);
+            cm = __float_as_int(ckmax[kq]);
           }
           const int lg = written ? rn2 + fexp(fmaxf(r0, r1)) : 0;
           const int lgu = __shfl_up_sync(FULL, lg, 1);
@@ -814,6 +820,56 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
         for (int c = 0; c < R; ++c) sb[u][c] = stg_sc[(u * 32 + lane) * R + c];
     }
     __syncwarp();   // the stage is read before the next chunk's copies are issued
+    if (SPARSE && kc % KC != 0) {
+      // sparse checkpoints: the restored state is that of chunk kc - kc % KC;
+      // run the forward over the chunks in between (the same steps as the
+      // forward kernel, so the state reached is bit for bit the same)
+      const int k0 = kc - kc % KC;
+      float ab[PF][R];
+#pragma unroll
+      for (int u = 0; u < PF; ++u) {
+        const int i = k0 * C_STEPS + u - lane + 1;
+        load_row<R>(pr, i, jl, i >= 1 && i <= L1, ab[u]);
+      }
+      for (int ka = k0; ka < kc; ++ka) {
+        float er[NEF];
+        {
+          const int ie = ka * C_STEPS + lane + 1;
+          const bool ok = ein && lane < C_STEPS && ie <= L1;
+#pragma unroll
+          for (int f = 0; f < NEF; ++f) er[f] = ok ? ein[f * Lm + (ie - 1)] : 0.f;
+        }
+#pragma unroll 1
+        for (int u0 = 0; u0 < C_STEPS; u0 += PF)
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+          const int cu = u0 + u;
+          const int i = ka * C_STEPS + cu - lane + 1;
+          const bool act = (i >= 1) && (i <= L1);
+          float xl[NS];
+#pragma unroll
+          for (int q = 0; q < NS; ++q) xl[q] = __shfl_up_sync(FULL, st.vs[q], 1);
+          int xn = __shfl_up_sync(FULL, st.n, 1);
+          float ev[NEF];
+#pragma unroll
+          for (int f = 0; f < NEF; ++f) ev[f] = __shfl_sync(FULL, er[f], cu);
+          if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < NS; ++q) xl[q] = act ? ev[q] : 0.f;
+            xn = act ? __float_as_int(ev[NS]) : 0;
+          }
+          float xs[R];
+          lscores<R>(ab[u], i, k, nlive, has_dead, xs);
+          {
+            const int ip = i + PF;
+            load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, ab[u]);
+          }
+          int et;
+          float em[R], rs;
+          lcells<NS, R>(st, xl, xn, xs, gO, gE, nlive, has_dead, et, em, rs);
+        }
+      }
+    }
 #pragma unroll 1
     for (int u0 = 0; u0 < C_STEPS; u0 += PF)
 #pragma unroll
@@ -1004,7 +1060,18 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
   finish_pair_p<NS>(a, w, lane, Sh, Sl, v0, v1, v2, pp);
 }
 
-template <int NS, int R, int WARPS>
+// Before a separate adjoint launch on a workspace the forward filled: the
+// adjoint task counter to 0 and the pairs' completion counts to 0, keeping
+// the failure flags the forward set.
+__global__ void adjoint_reset_kernel(unsigned* counters, unsigned* pair_done, int B) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) counters[1] = 0u;
+  if (i < B) pair_done[i] &= PAIR_TIMEOUT;
+}
+
+// SPARSE: checkpoints every a.ck_every chunks (the chunks between are
+// recomputed); otherwise every chunk (a.ck_every must be 1).
+template <int NS, int R, int WARPS, bool SPARSE = false>
 __global__ void __launch_bounds__(32 * WARPS) lbwd_kernel(Args a) {
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31;
@@ -1018,7 +1085,7 @@ __global__ void __launch_bounds__(32 * WARPS) lbwd_kernel(Args a) {
     if (lane == 0) task = (int)atomicAdd(a.counters + 1, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    lbwd_band<NS, R>(a, lp, place_of<NS, R>(a, task, true), lane, sm, deadline);
+    lbwd_band<NS, R, SPARSE>(a, lp, place_of<NS, R>(a, task, true), lane, sm, deadline);
   }
 }
 

@@ -285,6 +285,59 @@ class _ValueFn(torch.autograd.Function):
         return tuple(out)
 
 
+# Checkpoint stride of the checkpointed value op: the forward keeps the DP
+# state of every CHECKPOINT_EVERY-th chunk of 4 wavefront steps (about 5 / k
+# bytes per computed cell at k = CHECKPOINT_EVERY), and the adjoint recomputes
+# the chunks in between.  4 keeps ~1.3 B/cell, a third of the map's 4 B/cell.
+CHECKPOINT_EVERY = 4
+
+
+class _CheckpointedValueFn(torch.autograd.Function):
+    """value with a deferred adjoint (local families, gaps <= 0): forward
+    runs only the forward wavefront and keeps its sparse checkpoints in a
+    workspace; backward runs the checkpointed adjoint on them and scales the
+    map and dS/dtheta by the value's cotangent.  Nothing of size [B, L1, L2]
+    is kept between the two."""
+
+    @staticmethod
+    def forward(ctx, fam, lengths, ws_value, scores, *params):
+        value, ws = ws_value
+        ctx.fam, ctx.params, ctx.lengths, ctx.ws = fam, params, lengths, ws
+        ctx.vals = [_as_float(p) for p in params]
+        ctx.save_for_backward(scores)
+        return value
+
+    @staticmethod
+    def backward(ctx, gv):
+        from . import _ops as ops_mod
+
+        (scores,) = ctx.saved_tensors
+        _, smap, *grads = ops_mod.run_adjoint(ctx.fam.name, scores, ctx.lengths, ctx.vals,
+                                              CHECKPOINT_EVERY, ctx.ws)
+        gs = gv.view(-1, 1, 1) * smap if ctx.needs_input_grad[3] else None
+        out = [None, None, None, gs]
+        for k, p in enumerate(ctx.params):
+            g = None
+            if isinstance(p, Tensor) and p.requires_grad:
+                g = _param_grad((gv * grads[k]).sum(), p)
+            out.append(g)
+        return tuple(out)
+
+
+def _checkpointed_value(fam, lengths, scores, params):
+    """The checkpointed value op, or None where it does not apply (another
+    family, a positive gap, under stream capture)."""
+    if fam.name not in ("sw", "sw_affine") or torch.cuda.is_current_stream_capturing():
+        return None
+    from . import _ops as ops_mod
+
+    vals = [_as_float(p) for p in params]
+    got = ops_mod.run_checkpoint(fam.name, scores.detach(), lengths, vals, CHECKPOINT_EVERY)
+    if got is None:
+        return None
+    return _CheckpointedValueFn.apply(fam, lengths, got, scores, *params)
+
+
 class _MapFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, fam, lengths, scores, *params):
@@ -418,6 +471,9 @@ class Operator:
             # no gradient can flow: the forward wavefront alone (same values,
             # no marginal map, about half the work)
             return self.fam.value(x, *[_as_float(p) for p in params], lengths)
+        v = _checkpointed_value(self.fam, lengths, x, params)
+        if v is not None:
+            return v
         return _ValueFn.apply(self.fam, lengths, x, *params)
 
     def entropy(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:

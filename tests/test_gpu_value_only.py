@@ -80,8 +80,10 @@ def test_value_ops_under_vmap_and_compile():
 @pytest.mark.parametrize("fam", ["sw_affine", "sw", "nw", "nw_affine", "sv_affine", "sv_linear"])
 def test_value_with_tensor_params_runs_one_native_call(fam, monkeypatch):
     """value(...).backward() with learnable gaps and temperature: the value,
-    the map and dS/dparameters come from ONE forward + adjoint call, equal
-    bit for bit to the op's value and value_grad_params."""
+    the map and dS/dparameters come from ONE forward pass (one forward +
+    adjoint call, or, for the local families, the checkpointed forward and
+    its adjoint in the backward), equal bit for bit to the op's value and
+    value_grad_params."""
     import orihime_b200 as ohm
     from orihime_b200 import _ops
 
@@ -90,10 +92,11 @@ def test_value_with_tensor_params_runs_one_native_call(fam, monkeypatch):
     names = ("gap_open", "gap_ext", "temp") if affine else ("gap", "temp")
     vals = (-2.0, -0.5, 0.5) if affine else (-1.0, 0.5)
     params = [torch.tensor(v, device="cuda", requires_grad=True) for v in vals]
-    calls = []
-    real_a, real_l = _ops.run_affine, _ops.run_linear
+    calls = []   # native forward passes: one-call forward + adjoint, or the checkpointed forward
+    real_a, real_l, real_c = _ops.run_affine, _ops.run_linear, _ops.run_checkpoint
     monkeypatch.setattr(_ops, "run_affine", lambda *a, **k: calls.append(1) or real_a(*a, **k))
     monkeypatch.setattr(_ops, "run_linear", lambda *a, **k: calls.append(1) or real_l(*a, **k))
+    monkeypatch.setattr(_ops, "run_checkpoint", lambda *a, **k: calls.append(1) or real_c(*a, **k))
     op = getattr(ohm, {"sw_affine": "sw_affine_value", "sw": "sw_value", "nw": "nw_value",
                        "nw_affine": "nw_affine_value", "sv_affine": "sv_affine_value",
                        "sv_linear": "sv_value"}[fam])
