@@ -731,8 +731,24 @@ def main():
     offsets, ln32 = ragged.layout(lengths)
     cells = int((lengths[:, 0] * lengths[:, 1]).sum())
     flat = make_scores(torch, lengths, offsets, 3, dev, index=gidx)
-    plan = ragged.Plan(ln32, offsets, family="affine", device=dev, cols_per_lane=args.cols_per_lane)
     params = dict(gap_open=GO, gap_ext=GE, temp=T)
+    # launch configuration: columns per lane chosen by timing the candidates
+    # (2, 4, 8 for every pair, or per length bucket) on this batch and GPU
+    if args.cols_per_lane:
+        plan = ragged.Plan(ln32, offsets, family="affine", device=dev, cols_per_lane=args.cols_per_lane)
+        tuning = {"choice": f"R{args.cols_per_lane}", "fixed": True}
+    else:
+        plan, tuning = ragged.autotune_plan(ln32, offsets, "affine", dev, flat=flat, **params)
+    cols = int(tuning["choice"][1:]) if tuning["choice"].startswith("R") else 0
+    if cols:
+        plan_cols = np.full(len(lengths), cols)
+    else:
+        plan_cols = plan.cols
+    w = 32 * plan_cols
+    computed = int((np.maximum(1, (lengths[:, 1] + w - 1) // w) * (lengths[:, 0] + 31) * w).sum())
+    # the eager leg records the forward / adjoint split inside one uniform plan
+    eplan = plan if isinstance(plan, ragged.Plan) else ragged.Plan(ln32, offsets, family="affine",
+                                                                   device=dev, cols_per_lane=4)
 
     # ---- headline: the packed plan captured in a CUDA graph, replayed ----
     graph, gout = plan.graph(flat, **params)
@@ -766,14 +782,14 @@ def main():
             e_.record()
     torch.cuda.synchronize()
     opts = [_lib.Options(0, 0, 0, trio[1].cuda_event, 0, 0) for trio in ev]
-    out = plan.outputs()
+    out = eplan.outputs()
     for _ in range(2):
-        plan.run(flat, out=out, **params)
+        eplan.run(flat, out=out, **params)
     torch.cuda.synchronize()
     barrier(torch, world)
     for k in range(args.steps):
         ev[k][0].record()
-        plan.run(flat, out=out, options=opts[k], **params)
+        eplan.run(flat, out=out, options=opts[k], **params)
         ev[k][2].record()
     torch.cuda.synchronize()
     barrier(torch, world)
@@ -816,10 +832,10 @@ def main():
     host = torch.empty(flat.numel(), dtype=torch.float32, pin_memory=True)
     host.copy_(flat.cpu())
     host_val = torch.empty(plan.B, dtype=torch.float32, pin_memory=True)
-    del plan
+    del plan, eplan
     torch.cuda.empty_cache()
     splan = ragged.StreamedPlan(ln32, offsets, family="affine", device=dev, parts=E2E_PARTS,
-                                cols_per_lane=args.cols_per_lane)
+                                cols_per_lane=cols or 4)
     sout = splan.outputs()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for _ in range(2):
@@ -857,7 +873,7 @@ def main():
                     "unit": "Gop/s", "frac": achieved / peak,
                     "traffic": None if tpc is None else tpc * cells,
                     "traffic_source": tsrc,
-                    "kernel": "lbwd_kernel<3,4,1> (checkpointed adjoint, scaled linear domain)",
+                    "kernel": f"lbwd_kernel<3,{cols or 4},1> (checkpointed adjoint, scaled linear domain)",
                     "algorithmic": (f"{MUFU_PER_CELL_BWD} ex2/lg2 per cell (the log-domain adjoint's "
                                     f"count) x {cells} cells"),
                     "peak_source": "measured in-bench (swb_mufu_probe: ex2.approx throughput)",
@@ -880,6 +896,11 @@ def main():
                            "cells": all_cells, "cells_rank0": cells,
                            "gap_open": GO, "gap_ext": GE, "temp": T,
                            "timed": "CUDA graph replay of the packed plan (forward + adjoint)",
+                           "launch": {"columns_per_lane": tuning["choice"],
+                                      "tuning_ms": tuning.get("ms"),
+                                      "how": "ragged.autotune_plan: candidates timed on this batch"
+                                             if not tuning.get("fixed") else "--cols-per-lane",
+                                      "computed_over_useful_cells": computed / cells},
                            "l2": "inputs (3.9 GB) larger than L2; no flush",
                            "parallelism": (f"LPT shards x{world} of one pair list, no collective on "
                                            "the data path" if world > 1 else "one GPU")},

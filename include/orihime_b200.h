@@ -55,7 +55,8 @@ typedef struct swb_options {
     int fault_inject;                  /* 1: band>0 waits on a word nobody writes (tests) */
     void* split_event;                 /* cudaEvent_t recorded between the forward and the
                                           adjoint kernel (per-kernel timing), or NULL     */
-    int cols_per_lane;                 /* columns per lane of a band: 2 or 4 (0 = default) */
+    int cols_per_lane;                 /* columns per lane of a band: 2, 4 or (local families,
+                                          linear domain) 8; 0 = swb_cols_per_lane's default */
     int domain;                        /* local models: SWB_DOMAIN_AUTO (0), _LOG or _LINEAR */
     const float* params_device;        /* local models, linear domain: device array
                                           (gap_open, gap_ext, temp) or (gap, temp) that the
@@ -77,6 +78,15 @@ typedef struct swb_options {
 #define SWB_DOMAIN_AUTO 0
 #define SWB_DOMAIN_LOG 1
 #define SWB_DOMAIN_LINEAR 2
+
+/* Columns per lane the padded entry points use when swb_options does not
+ * set one: 8 for the local families (family 1 linear gap, 3 affine gaps) in
+ * the linear domain on batches with L2max >= 256, else 4 (families 2, 4, 5:
+ * the global and Saigo-Vert models, always 4).  Results depend on it bit for
+ * bit (the band decomposition orders each pair's sums), so a packed plan
+ * built with the same value reproduces a padded call exactly.  No reference
+ * counterpart. */
+int swb_cols_per_lane(int family, int L2max, float gap_open, float gap_ext, float temp);
 
 /* Workspace bytes for swb_sw_affine_forward on a [B, L1max, L2max] batch. */
 size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max);

@@ -186,6 +186,8 @@ def load() -> ctypes.CDLL:
     lib.swb_sw_checkpoint.argtypes = [vp, vp, i, i, i, f, f, i, vp, vp, sz, vp]
     lib.swb_sw_adjoint.restype = i
     lib.swb_sw_adjoint.argtypes = [vp, vp, i, i, i, f, f, i, vp, vp, vp, vp, vp, sz, vp]
+    lib.swb_cols_per_lane.restype = i
+    lib.swb_cols_per_lane.argtypes = [i, i, f, f, f]
     lib.swb_mufu_probe.restype = i
     lib.swb_mufu_probe.argtypes = [vp, i, i, vp]
     got = lib.swb_abi_version()

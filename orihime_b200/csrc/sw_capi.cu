@@ -42,8 +42,26 @@ template <int NS, int R> constexpr int ckrs() { return swb::ck_record_floats<NS,
 template <int NS, int R> constexpr int ne() { return swb::Dims<NS, R>::NE; }
 
 bool valid_r(int r) { return r == 2 || r == 4; }
-int pick_r(const swb_options* opt) {
-  return (opt && opt->cols_per_lane) ? opt->cols_per_lane : kDefaultR;
+// 8 columns per lane: the linear-domain kernels of the local families only
+bool valid_r_local(int r) { return r == 2 || r == 4 || r == 8; }
+constexpr int ridx(int r) { return r == 2 ? 0 : (r == 4 ? 1 : 2); }
+// Whether a launch with these parameters runs the linear-domain kernels
+// (the local families, gaps <= 0, not forced to the log domain).
+template <int NS, int G>
+bool lin_eligible(float go, float ge, float T, const swb_options* opt) {
+  if (G != 0 || !(T > 0.f) || !(T < INFINITY)) return false;
+  if (opt && opt->domain == SWB_DOMAIN_LOG) return false;
+  const float k = 1.4426950408889634f / T;
+  const double xo = (double)go * (double)k, xe = NS == 3 ? (double)ge * (double)k : 0.0;
+  return xo <= 0.0 && xe <= 0.0;
+}
+// Default columns per lane of the padded entry points: 8 for the
+// linear-domain kernels on batches at least 256 columns wide (half the bands,
+// each step's fixed work spread over twice the cells: measured faster from
+// 64 x 1024^2 to 4 x 4096^2), else 4.
+int default_r(long long L2m, bool lin) { return lin && L2m >= 256 ? 8 : kDefaultR; }
+int pick_r(const swb_options* opt, long long L2m, bool lin) {
+  return (opt && opt->cols_per_lane) ? opt->cols_per_lane : default_r(L2m, lin);
 }
 
 struct Layout {
@@ -106,8 +124,8 @@ size_t plan_bytes_for(long long B, long long ntasks) {
 struct DevInfo {
   int sms = 0;
   int occ[2][5][2] = {};   // [kernel fwd/bwd][model_index][R == 4?]
-  int locc[2][2][2] = {};  // linear-domain kernels: [fwd/bwd][NS == 3?][R == 4?]
-  int locc_sparse[2] = {}; // linear-domain adjoint with sparse checkpoints (R = 4): [NS == 3?]
+  int locc[2][2][3] = {};  // linear-domain kernels: [fwd/bwd][NS == 3?][R: 2, 4, 8]
+  int locc_sparse[2][3] = {};  // linear-domain adjoint, sparse checkpoints: [NS == 3?][R: 2, 4, 8]
   bool ready = false;
 };
 DevInfo g_dev[64];
@@ -130,18 +148,18 @@ cudaError_t setup_lin(DevInfo& d) {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)lbwd_smem<NS, R>());
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.locc[0][NS == 3][R == 4],
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.locc[0][NS == 3][ridx(R)],
                                                     swb::lfwd_kernel<NS, R>, 32 * kWarpsFwd, 0);
   if (e != cudaSuccess) return e;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &d.locc[1][NS == 3][R == 4], swb::lbwd_kernel<NS, R, kWarpsBwd>, 32 * kWarpsBwd,
+      &d.locc[1][NS == 3][ridx(R)], swb::lbwd_kernel<NS, R, kWarpsBwd>, 32 * kWarpsBwd,
       lbwd_smem<NS, R>());
-  if (e != cudaSuccess || R != kDefaultR) return e;
+  if (e != cudaSuccess || R == 2) return e;   // the checkpointed op runs 4 or 8 columns per lane
   e = cudaFuncSetAttribute(swb::lbwd_kernel<NS, R, kWarpsBwd, true>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lbwd_smem<NS, R>());
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &d.locc_sparse[NS == 3], swb::lbwd_kernel<NS, R, kWarpsBwd, true>, 32 * kWarpsBwd,
+      &d.locc_sparse[NS == 3][ridx(R)], swb::lbwd_kernel<NS, R, kWarpsBwd, true>, 32 * kWarpsBwd,
       lbwd_smem<NS, R>());
 }
 
@@ -171,7 +189,8 @@ int dev_info(DevInfo** out) {
     if (setup_pair<1, 2>(d) || setup_pair<1, 4>(d) || setup_pair<3, 2>(d) || setup_pair<3, 4>(d) ||
         setup_pair<1, 2, 1>(d) || setup_pair<1, 4, 1>(d) || setup_pair<3, 2, 1>(d) ||
         setup_pair<3, 4, 1>(d) || setup_pair<3, 2, 2>(d) || setup_pair<3, 4, 2>(d) ||
-        setup_lin<1, 2>(d) || setup_lin<1, 4>(d) || setup_lin<3, 2>(d) || setup_lin<3, 4>(d))
+        setup_lin<1, 2>(d) || setup_lin<1, 4>(d) || setup_lin<3, 2>(d) || setup_lin<3, 4>(d) ||
+        setup_lin<1, 8>(d) || setup_lin<3, 8>(d))
       return SWB_ERR_CUDA;
     d.ready = true;
   }
@@ -262,9 +281,10 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
       cudaMemsetAsync(a.map, 0, map_elems * sizeof(float), st) != cudaSuccess)
     return SWB_ERR_CUDA;
 
+  if (R == 8 && !lin) return SWB_ERR_ARG;   // 8 columns per lane: linear domain only
   constexpr int m = model_index<NS, G>();
-  const int of = lin ? d->locc[0][NS == 3][R == 4] : d->occ[0][m][R == 4];
-  const int ob = lin ? d->locc[1][NS == 3][R == 4] : d->occ[1][m][R == 4];
+  const int of = lin ? d->locc[0][NS == 3][ridx(R)] : d->occ[0][m][R == 4];
+  const int ob = lin ? d->locc[1][NS == 3][ridx(R)] : d->occ[1][m][R == 4];
   const int cta_cap_f = d->sms * (of > 0 ? of : 1);
   const int cta_cap_b = d->sms * (ob > 0 ? ob : 1);
   const long long need_f = (ntasks + kWarpsFwd - 1) / kWarpsFwd;
@@ -292,17 +312,19 @@ int launch(Args a, const Layout& l, long long ntasks, size_t map_elems, bool cle
       return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
     }
   }
-  swb::fwd_kernel<NS, R, G><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
-  if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
-  if (opt && opt->split_event &&
-      cudaEventRecord(reinterpret_cast<cudaEvent_t>(opt->split_event), st) != cudaSuccess)
-    return SWB_ERR_CUDA;
-  if (value_only) {
-    swb::value_kernel<NS, R, G><<<(a.B + 3) / 4, 128, 0, st>>>(a);
-    return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+  if constexpr (R != 8) {   // the log-domain kernels have 2 or 4 columns per lane
+    swb::fwd_kernel<NS, R, G><<<grid_f, 32 * kWarpsFwd, 0, st>>>(a);
+    if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
+    if (opt && opt->split_event &&
+        cudaEventRecord(reinterpret_cast<cudaEvent_t>(opt->split_event), st) != cudaSuccess)
+      return SWB_ERR_CUDA;
+    if (value_only) {
+      swb::value_kernel<NS, R, G><<<(a.B + 3) / 4, 128, 0, st>>>(a);
+      return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+    }
+    swb::bwd_kernel<NS, R, kWarpsBwd, G><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS, R>(), st>>>(a);
+    if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   }
-  swb::bwd_kernel<NS, R, kWarpsBwd, G><<<grid_b, 32 * kWarpsBwd, bwd_smem<NS, R>(), st>>>(a);
-  if (cudaPeekAtLastError() != cudaSuccess) return SWB_ERR_CUDA;
   return SWB_OK;
 }
 
@@ -330,20 +352,26 @@ template <int NS, int G = 0>
 int launch_padded(const float* scores, const int* lengths, int B, int L1m, int L2m, float go,
                   float ge, float T, float* value, float* map, float* g_open, float* g_ext,
                   float* g_T, void* ws, size_t ws_bytes, void* stream, const swb_options* opt) {
-  const int r = pick_r(opt);
+  const int r = pick_r(opt, L2m, lin_eligible<NS, G>(go, ge, T, opt));
   if (r == 2)
     return launch_padded_r<NS, 2, G>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
                                      g_ext, g_T, ws, ws_bytes, stream, opt);
   if (r == 4)
     return launch_padded_r<NS, 4, G>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
                                      g_ext, g_T, ws, ws_bytes, stream, opt);
+  if constexpr (G == 0) {   // 8 columns per lane: the local families' linear-domain kernels
+    if (r == 8)
+      return launch_padded_r<NS, 8, G>(scores, lengths, B, L1m, L2m, go, ge, T, value, map, g_open,
+                                       g_ext, g_T, ws, ws_bytes, stream, opt);
+  }
   return SWB_ERR_ARG;
 }
 
 // Padded value-only batch: the forward wavefront, no checkpoints, no adjoint.
-template <int NS, int G = 0>
+// Columns per lane as the full call's default (the values are equal bit for
+// bit only for equal band decompositions).
+template <int NS, int G = 0, int R = kDefaultR>
 Layout value_layout(long long B, long long L1m, long long L2m) {
-  constexpr int R = kDefaultR;
   int nb = (int)((L2m + 32 * R - 1) / (32 * R));
   if (nb < 1) nb = 1;
   const size_t slots = (size_t)B * nb;
@@ -361,15 +389,29 @@ int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   if (B == 0) return SWB_OK;
   if (!value || ((size_t)B * L1m * L2m > 0 && !scores)) return SWB_ERR_ARG;
-  const Layout l = value_layout<NS, G>(B, L1m, L2m);
-  Args a{};
-  a.scores = scores; a.map = nullptr; a.lengths = lengths;
-  a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
-  a.go = go; a.ge = ge; a.T = T;
-  a.nb = l.nb; a.nchunks = l.nchunks;
-  a.value = value;
-  return launch<NS, kDefaultR, G>(a, l, (long long)B * l.nb, 0, false, ws, ws_bytes, stream,
-                                  nullptr, true);
+  auto run = [&](auto rt) {
+    constexpr int R = decltype(rt)::value;
+    const Layout l = value_layout<NS, G, R>(B, L1m, L2m);
+    Args a{};
+    a.scores = scores; a.map = nullptr; a.lengths = lengths;
+    a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
+    a.go = go; a.ge = ge; a.T = T;
+    a.nb = l.nb; a.nchunks = l.nchunks;
+    a.value = value;
+    return launch<NS, R, G>(a, l, (long long)B * l.nb, 0, false, ws, ws_bytes, stream, nullptr, true);
+  };
+  if constexpr (G == 0) {
+    if (default_r(L2m, lin_eligible<NS, G>(go, ge, T, nullptr)) == 8)
+      return run(std::integral_constant<int, 8>{});
+  }
+  return run(std::integral_constant<int, kDefaultR>{});
+}
+
+template <int NS, int G = 0>
+size_t value_workspace(long long B, long long L1m, long long L2m) {
+  size_t n = value_layout<NS, G, kDefaultR>(B, L1m, L2m).total;
+  if constexpr (G == 0) n = std::max(n, value_layout<NS, G, 8>(B, L1m, L2m).total);
+  return n;
 }
 
 template <int NS, int G = 0>
@@ -406,6 +448,11 @@ int launch_ragged(const float* scores, const void* host_plan, const void* dev_pl
   if (r == 4)
     return launch<NS, 4, G>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream,
                             opt, value_only);
+  if constexpr (G == 0) {
+    if (r == 8)
+      return launch<NS, 8, G>(a, l, ntasks, (size_t)h[HW_MAP_ELEMS], false, ws, ws_bytes, stream,
+                              opt, value_only);
+  }
   return SWB_ERR_ARG;
 }
 
@@ -533,9 +580,8 @@ int launch_xband(const float* scores, const float* v, const int* lengths, int B,
 
 constexpr int kMaxCkEvery = 16;
 
-template <int NS>
+template <int NS, int R>
 Layout ck_layout(long long B, long long L1m, long long L2m, int kc) {
-  constexpr int R = kDefaultR;
   using LD = swb::LDims<NS, R>;
   int nb = (int)((L2m + 32 * R - 1) / (32 * R));
   if (nb < 1) nb = 1;
@@ -552,7 +598,7 @@ Layout ck_layout(long long B, long long L1m, long long L2m, int kc) {
 
 // Shared set-up of the two halves: argument checks, parameters (linear
 // domain only), workspace pointers.  Returns SWB_OK or an error code.
-template <int NS>
+template <int NS, int R>
 int ck_setup(Args& a, Layout& l, const float* scores, const int* lengths, int B, int L1m, int L2m,
              float go, float ge, float T, int kc, void* ws, size_t ws_bytes) {
   if (B < 0 || L1m < 0 || L2m < 0 || kc < 1 || kc > kMaxCkEvery) return SWB_ERR_ARG;
@@ -562,7 +608,7 @@ int ck_setup(Args& a, Layout& l, const float* scores, const int* lengths, int B,
   a.k = 1.4426950408889634f / T;
   const double xo = (double)go * (double)a.k, xe = NS == 3 ? (double)ge * (double)a.k : 0.0;
   if (!(xo <= 0.0 && xe <= 0.0)) return SWB_ERR_ARG;   // the linear domain needs gaps <= 0
-  l = ck_layout<NS>(B, L1m, L2m, kc);
+  l = ck_layout<NS, R>(B, L1m, L2m, kc);
   if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
   char* w = static_cast<char*>(ws);
   a.scores = scores; a.lengths = lengths;
@@ -586,13 +632,12 @@ int ck_setup(Args& a, Layout& l, const float* scores, const int* lengths, int B,
   return SWB_OK;
 }
 
-template <int NS>
-int ck_forward(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
-               float T, int kc, float* value, void* ws, size_t ws_bytes, void* stream_v) {
-  constexpr int R = kDefaultR;
+template <int NS, int R>
+int ck_forward_r(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
+                 float T, int kc, float* value, void* ws, size_t ws_bytes, void* stream_v) {
   Args a;
   Layout l;
-  int rc = ck_setup<NS>(a, l, scores, lengths, B, L1m, L2m, go, ge, T, kc, ws, ws_bytes);
+  int rc = ck_setup<NS, R>(a, l, scores, lengths, B, L1m, L2m, go, ge, T, kc, ws, ws_bytes);
   if (rc != SWB_OK) return rc;
   if (B == 0) return SWB_OK;
   if (!value) return SWB_ERR_ARG;
@@ -604,7 +649,7 @@ int ck_forward(const float* scores, const int* lengths, int B, int L1m, int L2m,
   if (cudaMemsetAsync(w, 0, l.off_part, st) != cudaSuccess) return SWB_ERR_CUDA;
   if (cudaMemsetAsync(w + l.off_sent, 0xff, l.sent_bytes, st) != cudaSuccess) return SWB_ERR_CUDA;
   const long long ntasks = (long long)B * l.nb;
-  const int of = d->locc[0][NS == 3][1];
+  const int of = d->locc[0][NS == 3][ridx(R)];
   const long long cap = (long long)d->sms * (of > 0 ? of : 1);
   const int grid = (int)std::max(1LL, std::min((ntasks + kWarpsFwd - 1) / kWarpsFwd, cap));
   swb::lfwd_kernel<NS, R><<<grid, 32 * kWarpsFwd, 0, st>>>(a);
@@ -612,14 +657,13 @@ int ck_forward(const float* scores, const int* lengths, int B, int L1m, int L2m,
   return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
 }
 
-template <int NS>
-int ck_adjoint(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
-               float T, int kc, float* value, float* map, float* g_open, float* g_ext, float* g_T,
-               void* ws, size_t ws_bytes, void* stream_v) {
-  constexpr int R = kDefaultR;
+template <int NS, int R>
+int ck_adjoint_r(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
+                 float T, int kc, float* value, float* map, float* g_open, float* g_ext, float* g_T,
+                 void* ws, size_t ws_bytes, void* stream_v) {
   Args a;
   Layout l;
-  int rc = ck_setup<NS>(a, l, scores, lengths, B, L1m, L2m, go, ge, T, kc, ws, ws_bytes);
+  int rc = ck_setup<NS, R>(a, l, scores, lengths, B, L1m, L2m, go, ge, T, kc, ws, ws_bytes);
   if (rc != SWB_OK) return rc;
   if (B == 0) return SWB_OK;
   const size_t map_elems = (size_t)B * L1m * L2m;
@@ -638,7 +682,7 @@ int ck_adjoint(const float* scores, const int* lengths, int B, int L1m, int L2m,
   if (map_elems > 0 && cudaMemsetAsync(map, 0, map_elems * sizeof(float), st) != cudaSuccess)
     return SWB_ERR_CUDA;
   const long long ntasks = (long long)B * l.nb;
-  const int ob = kc > 1 ? d->locc_sparse[NS == 3] : d->locc[1][NS == 3][1];
+  const int ob = kc > 1 ? d->locc_sparse[NS == 3][ridx(R)] : d->locc[1][NS == 3][ridx(R)];
   const long long cap = (long long)d->sms * (ob > 0 ? ob : 1);
   const int grid = (int)std::max(1LL, std::min((ntasks + kWarpsBwd - 1) / kWarpsBwd, cap));
   if (kc > 1)
@@ -648,18 +692,52 @@ int ck_adjoint(const float* scores, const int* lengths, int B, int L1m, int L2m,
   return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
 }
 
+// The checkpointed op's columns per lane: the padded default for the linear
+// domain (its results then equal the one-call entry points' bit for bit).
+template <int NS>
+int ck_forward(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
+               float T, int kc, float* value, void* ws, size_t ws_bytes, void* stream_v) {
+  if (default_r(L2m, true) == 8)
+    return ck_forward_r<NS, 8>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, ws, ws_bytes, stream_v);
+  return ck_forward_r<NS, 4>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, ws, ws_bytes, stream_v);
+}
+
+template <int NS>
+int ck_adjoint(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
+               float T, int kc, float* value, float* map, float* g_open, float* g_ext, float* g_T,
+               void* ws, size_t ws_bytes, void* stream_v) {
+  if (default_r(L2m, true) == 8)
+    return ck_adjoint_r<NS, 8>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, map, g_open, g_ext,
+                               g_T, ws, ws_bytes, stream_v);
+  return ck_adjoint_r<NS, 4>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, map, g_open, g_ext,
+                             g_T, ws, ws_bytes, stream_v);
+}
+
+template <int NS>
+size_t ck_workspace(long long B, long long L1m, long long L2m, int kc) {
+  return default_r(L2m, true) == 8 ? ck_layout<NS, 8>(B, L1m, L2m, kc).total
+                                   : ck_layout<NS, 4>(B, L1m, L2m, kc).total;
+}
+
 }  // namespace
 
 extern "C" {
 
+int swb_cols_per_lane(int family, int L2max, float gap_open, float gap_ext, float temp) {
+  // family: 1 linear, 3 affine (local); 2, 4, 5 global and Saigo-Vert
+  if (family == 1) return default_r(L2max, lin_eligible<1, 0>(gap_open, 0.f, temp, nullptr));
+  if (family == 3) return default_r(L2max, lin_eligible<3, 0>(gap_open, gap_ext, temp, nullptr));
+  return (family >= 1 && family <= 5) ? kDefaultR : SWB_ERR_ARG;
+}
+
 size_t swb_sw_affine_checkpoint_workspace_bytes(int B, int L1max, int L2max, int ck_every) {
   if (B <= 0 || ck_every < 1 || ck_every > kMaxCkEvery) return 0;
-  return ck_layout<3>(B, L1max, L2max, ck_every).total;
+  return ck_workspace<3>(B, L1max, L2max, ck_every);
 }
 
 size_t swb_sw_checkpoint_workspace_bytes(int B, int L1max, int L2max, int ck_every) {
   if (B <= 0 || ck_every < 1 || ck_every > kMaxCkEvery) return 0;
-  return ck_layout<1>(B, L1max, L2max, ck_every).total;
+  return ck_workspace<1>(B, L1max, L2max, ck_every);
 }
 
 int swb_sw_affine_checkpoint(const float* scores, const int* lengths, int B, int L1max, int L2max,
@@ -825,7 +903,8 @@ int swb_nw_param_jacobian(const float* scores, const int* lengths, int B, int L1
 
 size_t swb_sw_affine_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;
-  return std::max(layout_for<3, 2>(B, L1max, L2max).total, layout_for<3, 4>(B, L1max, L2max).total);
+  return std::max({layout_for<3, 2>(B, L1max, L2max).total, layout_for<3, 4>(B, L1max, L2max).total,
+                   layout_for<3, 8>(B, L1max, L2max).total});
 }
 
 int swb_scan_scores(const float* x, int B, long long per_item, float limit, float sentinel,
@@ -854,11 +933,11 @@ int swb_scan_scores(const float* x, int B, long long per_item, float limit, floa
 }
 
 size_t swb_sw_affine_value_workspace_bytes(int B, int L1max, int L2max) {
-  return B > 0 ? value_layout<3>(B, L1max, L2max).total : 0;
+  return B > 0 ? value_workspace<3>(B, L1max, L2max) : 0;
 }
 
 size_t swb_sw_value_workspace_bytes(int B, int L1max, int L2max) {
-  return B > 0 ? value_layout<1>(B, L1max, L2max).total : 0;
+  return B > 0 ? value_workspace<1>(B, L1max, L2max) : 0;
 }
 
 int swb_sw_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
@@ -876,7 +955,8 @@ int swb_sw_value(const float* scores, const int* lengths, int B, int L1max, int 
 
 size_t swb_sw_workspace_bytes(int B, int L1max, int L2max) {
   if (B <= 0) return 0;
-  return std::max(layout_for<1, 2>(B, L1max, L2max).total, layout_for<1, 4>(B, L1max, L2max).total);
+  return std::max({layout_for<1, 2>(B, L1max, L2max).total, layout_for<1, 4>(B, L1max, L2max).total,
+                   layout_for<1, 8>(B, L1max, L2max).total});
 }
 
 int swb_sw_affine_forward(const float* scores, const int* lengths, int B, int L1max, int L2max,
@@ -892,10 +972,11 @@ int swb_sw_affine_forward_static(const float* scores, const int* lengths, int B,
                                  float* value, float* map, float* grad_open, float* grad_ext,
                                  float* grad_temp, void* stream, const swb_options* opt) {
   // size check first: an oversize batch is rejected before any CUDA call
-  const int r = pick_r(opt);
-  if (B > 0 && L1max >= 0 && L2max >= 0 && valid_r(r)) {
+  const int r = pick_r(opt, L2max, lin_eligible<3, 0>(gap_open, gap_ext, temp, opt));
+  if (B > 0 && L1max >= 0 && L2max >= 0 && valid_r_local(r)) {
     const size_t need = r == 2 ? layout_for<3, 2>(B, L1max, L2max).total
-                               : layout_for<3, 4>(B, L1max, L2max).total;
+                               : (r == 4 ? layout_for<3, 4>(B, L1max, L2max).total
+                                         : layout_for<3, 8>(B, L1max, L2max).total);
     if (need > (size_t)SWB_STATIC_SCRATCH_BYTES) return SWB_ERR_WORKSPACE;
   }
   void* ws = nullptr;
@@ -945,7 +1026,7 @@ int swb_nw_affine_forward(const float* scores, const int* lengths, int B, int L1
 }
 
 size_t swb_nw_affine_value_workspace_bytes(int B, int L1max, int L2max) {
-  return B > 0 ? value_layout<3, 1>(B, L1max, L2max).total : 0;
+  return B > 0 ? value_workspace<3, 1>(B, L1max, L2max) : 0;
 }
 
 int swb_nw_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
@@ -988,7 +1069,7 @@ int swb_sv_affine_forward(const float* scores, const int* lengths, int B, int L1
 }
 
 size_t swb_sv_affine_value_workspace_bytes(int B, int L1max, int L2max) {
-  return B > 0 ? value_layout<3, 2>(B, L1max, L2max).total : 0;
+  return B > 0 ? value_workspace<3, 2>(B, L1max, L2max) : 0;
 }
 
 int swb_sv_affine_value(const float* scores, const int* lengths, int B, int L1max, int L2max,
@@ -1029,14 +1110,18 @@ int swb_ragged_plan(int family, int cols_per_lane, const int* lengths, const lon
                     size_t* workspace_bytes) {
   const int R = cols_per_lane ? cols_per_lane : kDefaultR;
   // family: 1 linear, 3 affine, 2 global linear, 4 global affine, 5 Saigo-Vert
-  if ((family < 1 || family > 5) || !valid_r(R) || B < 0 || (B > 0 && (!lengths || !offsets)))
+  const bool local = family == 1 || family == 3;
+  if ((family < 1 || family > 5) || !(local ? valid_r_local(R) : valid_r(R)) || B < 0 ||
+      (B > 0 && (!lengths || !offsets)))
     return SWB_ERR_ARG;
   const int ns = (family >= 3) ? 3 : 1;
   const int NE = 2 * ns;
   const int NP = family >= 4 ? swb::push_fields<3, 1>()
                              : (ns == 3 ? swb::push_fields<3, 0>() : swb::push_fields<1, 0>());
-  const int CKRS = ns == 3 ? (R == 2 ? swb::ck_record_floats<3, 2>() : swb::ck_record_floats<3, 4>())
-                           : (R == 2 ? swb::ck_record_floats<1, 2>() : swb::ck_record_floats<1, 4>());
+  const int CKRS = ns == 3 ? (R == 2 ? swb::ck_record_floats<3, 2>()
+                                     : (R == 4 ? swb::ck_record_floats<3, 4>() : swb::ck_record_floats<3, 8>()))
+                           : (R == 2 ? swb::ck_record_floats<1, 2>()
+                                     : (R == 4 ? swb::ck_record_floats<1, 4>() : swb::ck_record_floats<1, 8>()));
   // validate the packing: row pitch round4(L2), offsets multiples of 4 floats
   long long ntasks = 0;
   for (int b = 0; b < B; ++b) {

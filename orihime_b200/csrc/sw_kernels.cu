@@ -258,7 +258,12 @@ __device__ __forceinline__ void load_row(const Pair& pr, int i, int jl, bool ok,
     return;
   }
   const float* src = pr.s + (size_t)(i - 1) * pr.ld + jl;
-  if (R == 4 && pr.vec && jl + 4 <= pr.L2) {
+  if (R == 8 && pr.vec && jl + 8 <= pr.L2) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(src));
+    const float4 u = __ldg(reinterpret_cast<const float4*>(src) + 1);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    o[R > 4 ? 4 : 0] = u.x; o[R > 5 ? 5 : 0] = u.y; o[R > 6 ? 6 : 0] = u.z; o[R > 7 ? 7 : 0] = u.w;
+  } else if (R == 4 && pr.vec && jl + 4 <= pr.L2) {
     float4 v = __ldg(reinterpret_cast<const float4*>(src));
     o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
   } else if (R == 2 && pr.vec && jl + 2 <= pr.L2) {
@@ -275,7 +280,13 @@ __device__ __forceinline__ void load_row(const Pair& pr, int i, int jl, bool ok,
 template <int R>
 __device__ __forceinline__ void store_row(const Pair& pr, int i, int jl, const float (&v)[R]) {
   float* dst = pr.m + (size_t)(i - 1) * pr.ld + jl;
-  if (R == 4 && pr.vec && jl + 4 <= pr.ld) {
+  if (R == 8 && pr.vec && jl + 8 <= pr.ld) {
+    float z[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) z[c] = (c < R && jl + c < pr.L2) ? v[c < R ? c : 0] : 0.f;
+    reinterpret_cast<float4*>(dst)[0] = make_float4(z[0], z[1], z[2], z[3]);
+    reinterpret_cast<float4*>(dst)[1] = make_float4(z[4], z[5], z[6], z[7]);
+  } else if (R == 4 && pr.vec && jl + 4 <= pr.ld) {
     *reinterpret_cast<float4*>(dst) = make_float4(jl + 0 < pr.L2 ? v[0] : 0.f, jl + 1 < pr.L2 ? v[1] : 0.f,
                                                   jl + 2 < pr.L2 ? v[2] : 0.f, jl + 3 < pr.L2 ? v[3] : 0.f);
   } else if (R == 2 && pr.vec && jl + 2 <= pr.ld) {

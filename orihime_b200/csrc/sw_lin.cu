@@ -103,9 +103,15 @@ __device__ __forceinline__ void lcp_wait_all() { asm volatile("cp.async.wait_all
 template <int R>
 __device__ __forceinline__ void stage_row(float* dst, const Pair& pr, int i, int jl, bool ok) {
   const float* src = pr.s + (size_t)(ok ? i - 1 : 0) * pr.ld + jl;
-  if (ok && pr.vec && jl + R <= pr.L2 && (R == 4 || R == 2)) {
-    if constexpr (R == 4) lcp16(dst, src, 16);
-    else lcp8(dst, src, 8);
+  if (ok && pr.vec && jl + R <= pr.L2 && (R == 8 || R == 4 || R == 2)) {
+    if constexpr (R == 8) {
+      lcp16(dst, src, 16);
+      lcp16(dst + 4, src + 4, 16);
+    } else if constexpr (R == 4) {
+      lcp16(dst, src, 16);
+    } else {
+      lcp8(dst, src, 8);
+    }
   } else {
 #pragma unroll
     for (int c = 0; c < R; ++c) {
@@ -480,7 +486,7 @@ __device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int 
 #define SWB_LFWD_MINB 5
 #endif
 template <int NS, int R>
-__global__ void __launch_bounds__(128, SWB_LFWD_MINB) lfwd_kernel(Args a) {
+__global__ void __launch_bounds__(128, (R >= 8 ? 4 : SWB_LFWD_MINB)) lfwd_kernel(Args a) {
   const int lane = threadIdx.x & 31;
   const LParams lp = lparams<NS>(a);
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
@@ -900,15 +906,22 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
       float em[R], rs;
       lcells<NS, R>(st, xl, xn, xs, gO, gE, nlive, has_dead, et, em, rs);
       float* ent = sm + (size_t)cu * FW * 32;
-      if constexpr (R == 4) {
-        reinterpret_cast<float4*>(ent)[lane] = make_float4(st.v[0][0], st.v[0][1], st.v[0][2], st.v[0][3]);
+      if constexpr (R % 4 == 0) {
+        // field g's R columns as R / 4 float4 per lane: [g][quad][lane][4]
+        auto put = [&](int g, const float (&x)[R]) {
+#pragma unroll
+          for (int h = 0; h < R / 4; ++h)
+            reinterpret_cast<float4*>(ent + g * R * 32 + h * 128)[lane] =
+                make_float4(x[4 * h], x[4 * h + 1], x[4 * h + 2], x[4 * h + 3]);
+        };
+        put(0, st.v[0]);
         if constexpr (NS == 3) {
-          reinterpret_cast<float4*>(ent + 128)[lane] = make_float4(st.v[1][0], st.v[1][1], st.v[1][2], st.v[1][3]);
-          reinterpret_cast<float4*>(ent + 256)[lane] = make_float4(st.v[2][0], st.v[2][1], st.v[2][2], st.v[2][3]);
+          put(1, st.v[1]);
+          put(2, st.v[2]);
         } else {
-          reinterpret_cast<float4*>(ent + 128)[lane] = make_float4(em[0], em[1], em[2], em[3]);
+          put(1, em);
         }
-        reinterpret_cast<float4*>(ent + (LD::NF - 1) * 128)[lane] = make_float4(xs[0], xs[1], xs[2], xs[3]);
+        put(LD::NF - 1, xs);
       } else {
 #pragma unroll
         for (int c = 0; c < R; ++c) {
@@ -961,12 +974,14 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
       const float as = p2i(ea - na);                       // raw alpha -> normalised
       const float sc = p2any(na + ft - ze) * invZ; // real alpha * beta / Z factor
       float fa[LD::NF][R];
-      if constexpr (R == 4) {
+      if constexpr (R % 4 == 0) {
 #pragma unroll
-        for (int g = 0; g < LD::NF; ++g) {
-          const float4 y = reinterpret_cast<const float4*>(ent + g * 128)[lane];
-          fa[g][0] = y.x; fa[g][1] = y.y; fa[g][2] = y.z; fa[g][3] = y.w;
-        }
+        for (int g = 0; g < LD::NF; ++g)
+#pragma unroll
+          for (int h = 0; h < R / 4; ++h) {
+            const float4 y = reinterpret_cast<const float4*>(ent + g * R * 32 + h * 128)[lane];
+            fa[g][4 * h] = y.x; fa[g][4 * h + 1] = y.y; fa[g][4 * h + 2] = y.z; fa[g][4 * h + 3] = y.w;
+          }
       } else {
 #pragma unroll
         for (int g = 0; g < LD::NF; ++g)

@@ -450,3 +450,307 @@ def all_gather_values(value_local: torch.Tensor, shards, B: int, group=None) -> 
         idx = torch.as_tensor(shards[g], device=value_local.device)
         out[idx] = blk[:len(shards[g])]
     return out
+
+
+# ---------------------------------------------------------------------------
+# columns per lane chosen per length bucket
+# ---------------------------------------------------------------------------
+
+# Length buckets of the autotuner: L2 in octaves from 32 (the band width is
+# 32 x columns per lane, so L2 sets the dead columns of a pair's last band)
+# times L1 below / from 256 (a band's 31 fill and drain steps weigh more on
+# short pairs).  Key "l2lo:l1lo", e.g. "512:256".
+L2_EDGES = (0, 64, 128, 256, 512, 1024)
+L1_EDGES = (0, 256)
+
+# Columns per lane per bucket, measured on a B200 (the local families in the
+# linear domain, 2048 pairs per bucket filling the GPU, N(0, 1) * 1.5 scores at
+# T 0.5): used when no tuned table is cached for this GPU.
+DEFAULT_COLS = {"0:0": 2, "0:256": 2, "64:0": 4, "64:256": 2, "128:0": 8, "128:256": 2,
+                "256:0": 8, "256:256": 4, "512:0": 8, "512:256": 8, "1024:0": 8, "1024:256": 8}
+
+
+def bucket_of(L1: int, L2: int) -> str:
+    l2 = max(e for e in L2_EDGES if L2 >= e)
+    l1 = max(e for e in L1_EDGES if L1 >= e)
+    return f"{l2}:{l1}"
+
+
+def _cache_path(device) -> str:
+    import os
+    import re
+
+    name = torch.cuda.get_device_name(device) if torch.cuda.is_available() else "cpu"
+    d = os.environ.get("ORIHIME_B200_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "orihime_b200"))
+    return os.path.join(d, "cols_" + re.sub(r"[^A-Za-z0-9]+", "_", name) + ".json")
+
+
+def cols_table(device=None) -> dict:
+    """Columns per lane per bucket: the environment variable
+    ORIHIME_B200_COLS (a JSON object, or "bucket=R,..." pairs, or a path to a
+    JSON file) overrides; else the table `tune` cached for this GPU; else
+    DEFAULT_COLS.  Buckets missing from a table take DEFAULT_COLS' entry."""
+    import json
+    import os
+
+    table = dict(DEFAULT_COLS)
+    spec = os.environ.get("ORIHIME_B200_COLS")
+    if spec:
+        if os.path.exists(spec):
+            table.update(json.load(open(spec)))
+        elif spec.lstrip().startswith("{"):
+            table.update(json.loads(spec))
+        else:
+            for kv in spec.split(","):
+                k, v = kv.split("=")
+                table[k.strip()] = int(v)
+        return table
+    try:
+        path = _cache_path(device)
+        if os.path.exists(path):
+            table.update(json.load(open(path))["table"])
+    except Exception:
+        pass
+    return table
+
+
+def tune(family: str = "affine", device="cuda", pairs: int = 2048, reps: int = 5,
+         choices=(2, 4, 8), save: bool = True, seed: int = 0) -> dict:
+    """Time every length bucket at each columns-per-lane choice on this GPU
+    and keep the fastest: per bucket, `pairs` pairs with lengths log-uniform
+    in the bucket (N(0, 1) * 1.5 scores, gap_open -2, gap_ext -0.5 or gap -1,
+    T 0.5), one packed plan per choice, CUDA-graph replays timed with CUDA
+    events.  The table is cached as JSON per GPU name (see cols_table)."""
+    import json
+    import os
+
+    dev = torch.device(device)
+    rng = np.random.default_rng(seed)
+    params = dict(gap_open=-2.0, gap_ext=-0.5, temp=0.5) if family in _AFFINE else dict(gap=-1.0, temp=0.5)
+    table, times = {}, {}
+    l2e = list(L2_EDGES) + [2049]
+    l1e = list(L1_EDGES) + [2049]
+    for a2, b2 in zip(l2e[:-1], l2e[1:]):
+        for a1, b1 in zip(l1e[:-1], l1e[1:]):
+            key = f"{a2}:{a1}"
+            lo2, lo1 = max(a2, 16), max(a1, 16)
+            ln = np.stack([np.exp(rng.uniform(np.log(lo1), np.log(b1), pairs)),
+                           np.exp(rng.uniform(np.log(lo2), np.log(b2), pairs))], 1)
+            ln = np.clip(np.floor(ln), [lo1, lo2], [b1 - 1, b2 - 1]).astype(np.int64)
+            off, ln32 = layout(ln)
+            g = torch.Generator(device=dev)
+            g.manual_seed(seed + a2 * 7 + a1)
+            flat = torch.randn(int(off[-1]), generator=g, device=dev) * 1.5
+            best = None
+            for R in choices:
+                plan = Plan(ln32, off, family=family, device=dev, cols_per_lane=R)
+                gr, _ = plan.graph(flat, **params)
+                for _ in range(2):
+                    gr.replay()
+                torch.cuda.synchronize(dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    gr.replay()
+                e1.record()
+                torch.cuda.synchronize(dev)
+                ms = e0.elapsed_time(e1) / reps
+                times[f"{key}:R{R}"] = ms
+                if best is None or ms < best[1]:
+                    best = (R, ms)
+                del gr, plan
+            table[key] = best[0]
+    if save:
+        path = _cache_path(dev)
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        json.dump({"gpu": torch.cuda.get_device_name(dev), "family": family, "table": table,
+                   "ms": times}, open(path, "w"), indent=1)
+    return {"table": table, "ms": times}
+
+
+class MixedPlan:
+    """A packed batch run with a columns-per-lane choice per pair (the bucket
+    table of cols_table, or `table`): one Plan per choice over its pairs, all
+    on the batch's own packed score and map buffers (the original offsets,
+    no copies), launched on parallel streams that join before `run` returns
+    (graph-capturable); per-pair outputs are scattered into [B] arrays.  Same
+    interface as Plan.  The local families ("affine", "linear") in the
+    linear domain take 2, 4 or 8; the others 2 or 4."""
+
+    def __init__(self, lengths, offsets, family: str = "affine", device="cuda", table=None):
+        ln = np.ascontiguousarray(np.asarray(lengths, dtype=np.int32).reshape(-1, 2))
+        off = np.ascontiguousarray(np.asarray(offsets, dtype=np.int64).reshape(-1))
+        self.B = ln.shape[0]
+        self.lengths, self.offsets, self.family = ln, off, family
+        self.device = torch.device(device)
+        if self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.table = dict(table) if table is not None else cols_table(self.device)
+        local = family in ("affine", "linear")
+        cols = np.array([self.table.get(bucket_of(int(a), int(b)), 4) for a, b in ln.tolist()], dtype=np.int64)
+        if not local:
+            cols = np.where(cols == 8, 4, cols)
+        self.cols = cols
+        self.cells = int((ln[:, 0].astype(np.int64) * ln[:, 1]).sum())
+        self.map_elems = int(off[-1]) if self.B else 0
+        self.subs = []   # (R, pair indices, index tensor, Plan)
+        for R in sorted(set(cols.tolist())):
+            idx = np.nonzero(cols == R)[0]
+            sub_off = np.concatenate([off[idx], [off[idx[-1] + 1]]])
+            plan = Plan(ln[idx], sub_off, family=family, device=self.device, cols_per_lane=int(R))
+            self.subs.append((int(R), idx, torch.as_tensor(idx, device=self.device), plan))
+        self.streams = [torch.cuda.Stream(self.device) for _ in self.subs[1:]]
+        self.workspace_bytes = sum(p.workspace_bytes for *_, p in self.subs)
+
+    def computed_cells(self) -> int:
+        """Cells the bands compute (dead columns and fill/drain included)."""
+        w = 32 * self.cols
+        nb = np.maximum(1, (self.lengths[:, 1] + w - 1) // w)
+        c = nb * (self.lengths[:, 0] + 31) * w
+        return int(np.where((self.lengths[:, 0] > 0) & (self.lengths[:, 1] > 0), c, 0).sum())
+
+    def outputs(self) -> Result:
+        dev = self.device
+        e = lambda: torch.empty(self.B, dtype=torch.float32, device=dev)  # noqa: E731
+        return Result(e(), torch.empty(self.map_elems, dtype=torch.float32, device=dev), e(),
+                      e() if self.family in _AFFINE else None, e())
+
+    def _fanout(self, fns):
+        """Run fns[k] on stream k (the current stream for k = 0, side streams
+        forked from it for the others) and join them back."""
+        main = torch.cuda.current_stream(self.device)
+        for s in self.streams:
+            s.wait_stream(main)
+        for k, fn in enumerate(fns):
+            with torch.cuda.stream(main if k == 0 else self.streams[k - 1]):
+                fn()
+        for s in self.streams:
+            main.wait_stream(s)
+
+    def run(self, flat: torch.Tensor, *, out: Optional[Result] = None, **params) -> Result:
+        """One forward + adjoint over the batch (asynchronous): the sub-plans
+        write their pairs' cells into out.map and their per-pair outputs are
+        scattered into out's [B] arrays."""
+        out = out or self.outputs()
+        dev = self.device
+        e = lambda n: torch.empty(n, dtype=torch.float32, device=dev)  # noqa: E731
+        # per-pair outputs of each sub-plan, allocated on the current stream
+        subs_out = [Result(e(len(idx)), out.map, e(len(idx)), e(len(idx)) if out.grad_ext is not None else None,
+                           e(len(idx))) for _, idx, _, _ in self.subs]
+        self._fanout([lambda p=plan, o=o: p.run(flat, out=o, **params)
+                      for (_, _, _, plan), o in zip(self.subs, subs_out)])
+        for (R, idx, it, plan), r in zip(self.subs, subs_out):
+            out.value.index_copy_(0, it, r.value)
+            out.grad_open.index_copy_(0, it, r.grad_open)
+            if out.grad_ext is not None:
+                out.grad_ext.index_copy_(0, it, r.grad_ext)
+            out.grad_temp.index_copy_(0, it, r.grad_temp)
+        return out
+
+    def values(self, flat: torch.Tensor, *, out: Optional[torch.Tensor] = None, **params) -> torch.Tensor:
+        """S per pair without map or gradients (the forward wavefront alone)."""
+        if out is None:
+            out = torch.empty(self.B, dtype=torch.float32, device=self.device)
+        vals = [torch.empty(len(idx), dtype=torch.float32, device=self.device) for _, idx, _, _ in self.subs]
+        self._fanout([lambda p=plan, v=v: p.values(flat, out=v, **params)
+                      for (_, _, _, plan), v in zip(self.subs, vals)])
+        for (R, idx, it, plan), v in zip(self.subs, vals):
+            out.index_copy_(0, it, v)
+        return out
+
+    def status(self) -> int:
+        st = 0
+        for *_, p in self.subs:
+            st |= p.status()
+        return st
+
+    def graph(self, flat: torch.Tensor, **params) -> tuple[torch.cuda.CUDAGraph, Result]:
+        """Capture one call on static buffers; replay with ``g.replay()``."""
+        out = self.outputs()
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.run(flat, out=out, **params)
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.run(flat, out=out, **params)
+        return g, out
+
+
+def _signature(lengths, family) -> str:
+    """A coarse key of a batch for the tuning cache: the family, the pair
+    count's power of two and the cells per length bucket as a share of the
+    batch, in tenths."""
+    ln = np.asarray(lengths, dtype=np.int64).reshape(-1, 2)
+    cells = ln[:, 0] * ln[:, 1]
+    tot = max(int(cells.sum()), 1)
+    share = {}
+    for (a, b), c in zip(ln.tolist(), cells.tolist()):
+        k = bucket_of(a, b)
+        share[k] = share.get(k, 0) + c
+    hist = ",".join(f"{k}={round(10 * v / tot)}" for k, v in sorted(share.items()) if round(10 * v / tot))
+    return f"{family}|B{int(np.log2(max(len(ln), 1)))}|{hist}"
+
+
+def autotune_plan(lengths, offsets, family: str = "affine", device="cuda", flat=None, reps: int = 3,
+                  use_cache: bool = True, **params):
+    """The fastest launch configuration for this batch on this GPU, chosen by
+    timing: one Plan per columns-per-lane choice (2, 4 and, for the local
+    families, 8) and the MixedPlan of the bucket table, each captured in a
+    CUDA graph and replayed on `flat` (the batch's packed scores; N(0, 1) *
+    1.5 if None) with CUDA events.  The choice is cached per GPU and batch
+    signature (see cols_table for the cache folder).  Returns (plan, report)
+    where report = {"choice": ..., "ms": {candidate: ms}, "cached": bool}."""
+    import json
+    import os
+
+    dev = torch.device(device)
+    if dev.type == "cuda" and dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    ln = np.asarray(lengths, dtype=np.int32).reshape(-1, 2)
+    local = family in ("affine", "linear")
+    cands = {f"R{r}": (lambda r=r: Plan(ln, offsets, family=family, device=dev, cols_per_lane=r))
+             for r in ((2, 4, 8) if local else (2, 4))}
+    cands["mixed"] = lambda: MixedPlan(ln, offsets, family=family, device=dev)
+    sig = _signature(ln, family)
+    path = _cache_path(dev).replace("cols_", "plans_")
+    cache = {}
+    if use_cache and os.path.exists(path):
+        try:
+            cache = json.load(open(path))
+        except Exception:
+            cache = {}
+    if use_cache and sig in cache and cache[sig]["choice"] in cands:
+        return cands[cache[sig]["choice"]](), dict(cache[sig], cached=True)
+    if not params:
+        params = dict(gap_open=-2.0, gap_ext=-0.5, temp=0.5) if family in _AFFINE else dict(gap=-1.0, temp=0.5)
+    if flat is None:
+        g = torch.Generator(device=dev)
+        g.manual_seed(0)
+        off = np.asarray(offsets, dtype=np.int64)
+        flat = torch.randn(max(int(off[-1]), 1), generator=g, device=dev) * 1.5
+    times, best = {}, None
+    for name, make in cands.items():
+        plan = make()
+        gr, _ = plan.graph(flat, **params)
+        gr.replay()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            gr.replay()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        times[name] = e0.elapsed_time(e1) / reps
+        if best is None or times[name] < times[best[0]]:
+            best = (name, plan)
+        del gr
+        if best[1] is not plan:
+            del plan
+    report = {"choice": best[0], "ms": times, "signature": sig}
+    if use_cache:
+        cache[sig] = report
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        json.dump(cache, open(path, "w"), indent=1)
+    return best[1], dict(report, cached=False)

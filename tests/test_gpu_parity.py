@@ -179,12 +179,22 @@ def test_scale_invariance_bitwise():
     assert torch.equal(m1, m2)
 
 
-def test_padding_invariance_bitwise():
-    """A pair inside a padded batch (lengths) equals the cropped pair bit for bit."""
-    s = _emb_scores(3, 300, 420, 64, 4).cuda()
-    ln = torch.tensor([[300, 420], [211, 137], [64, 399]], dtype=torch.int32, device="cuda")
+@pytest.mark.parametrize("width, pairs", [
+    (420, [[300, 420], [211, 300], [64, 399]]),   # 8 columns per lane, padded and cropped
+    (200, [[300, 200], [211, 137], [64, 199]]),   # 4 columns per lane
+])
+def test_padding_invariance_bitwise(width, pairs):
+    """A pair inside a padded batch (lengths) equals the cropped pair bit for
+    bit when both run at the same columns per lane (the default depends on
+    the padded width: swb_cols_per_lane)."""
+    from orihime_b200 import _lib
+
+    lib = _lib.load()
+    s = _emb_scores(3, 300, width, 64, 4).cuda()
+    ln = torch.tensor(pairs, dtype=torch.int32, device="cuda")
     v, m = torch.ops.orihime.sw_affine_forward(s, -2.0, -0.5, 0.5, ln)
     for b, (l1, l2) in enumerate(ln.tolist()):
+        assert lib.swb_cols_per_lane(3, l2, -2.0, -0.5, 0.5) == lib.swb_cols_per_lane(3, width, -2.0, -0.5, 0.5)
         vc, mc = torch.ops.orihime.sw_affine_forward(s[b:b + 1, :l1, :l2].contiguous(), -2.0, -0.5,
                                                      0.5, None)
         assert torch.equal(vc[0], v[b])

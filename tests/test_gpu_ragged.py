@@ -31,8 +31,15 @@ def _lengths(B, seed, lo=1, hi=400):
     return ln
 
 
+def _lib_cols(fam_code, L2, params):
+    from orihime_b200 import _lib
+
+    return _lib.load().swb_cols_per_lane(fam_code, int(L2), params.get("gap_open", params.get("gap", 0.0)),
+                                         params.get("gap_ext", 0.0), params["temp"])
+
+
 @pytest.mark.parametrize("family", ["affine", "linear"])
-@pytest.mark.parametrize("cols", [2, 4])
+@pytest.mark.parametrize("cols", [2, 4, 8])
 def test_ragged_matches_oracle_and_padded(family, cols):
     from orihime_b200 import ragged
 
@@ -62,7 +69,9 @@ def test_ragged_matches_oracle_and_padded(family, cols):
             v, m = torch.ops.orihime.sw_forward(s.cuda(), -1.0, 0.5, None)
             r32 = O.linear(s.numpy(), None, -1.0, 0.5)
             r64 = O.linear(s.numpy(), None, -1.0, 0.5, dtype=np.float64)
-        if cols == 4:  # same per-pair schedule as the padded drop-in: identical bits
+        fam_code = 3 if family == "affine" else 1
+        pad_cols = _lib_cols(fam_code, L2, params)
+        if cols == pad_cols:  # same per-pair schedule as the padded drop-in: identical bits
             assert torch.equal(v.cpu()[0], out.value.cpu()[b])
             assert torch.equal(m.cpu()[0], maps[b])
         rel = abs(float(out.value[b]) - r32["value"][0]) / abs(r32["value"][0])
