@@ -660,10 +660,17 @@ def saigo_vert(args):
 # our arm
 # ---------------------------------------------------------------------------
 
-def profile_traffic(name="lbwd_kernel_affine_r4_dram.md"):
-    """DRAM bytes per useful cell of one adjoint launch, from the committed
-    ncu summary profiles/<name> (its line 'dram_bytes_per_cell: X'), with the
-    summary's own description of the build and capture it came from."""
+TRAFFIC_PROFILES = {4: "lbwd_kernel_affine_r4_dram.md", 8: "lfwd_lbwd_kernels_affine_r8_1024pairs.md"}
+
+
+def profile_traffic(cols):
+    """DRAM bytes per useful cell of one adjoint launch with `cols` columns
+    per lane, from the committed ncu summary of that kernel (its line
+    'dram_bytes_per_cell: X'), and the summary's path; (None, None) when no
+    capture of that kernel is committed."""
+    name = TRAFFIC_PROFILES.get(cols)
+    if name is None:
+        return None, None
     path = os.path.join(ROOT, "profiles", name)
     try:
         txt = open(path).read()
@@ -696,7 +703,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--pairs", type=int, default=NPAIRS, help="pairs per GPU (profiling cases)")
-    ap.add_argument("--cols-per-lane", type=int, default=0, help="band columns per lane (2 or 4)")
+    ap.add_argument("--cols-per-lane", type=int, default=0, help="band columns per lane (2, 4 or 8; 0 = timed choice)")
     ap.add_argument("--quick", action="store_true",
                     help="timed steps only: no e2e, plain, CPU legs (profiling cases)")
     ap.add_argument("--global-alignment", action="store_true",
@@ -868,12 +875,12 @@ def main():
         roof = None
         if bwd_ms:
             achieved = MUFU_PER_CELL_BWD * cells / (bwd_ms * 1e-3)
-            tpc, tsrc = profile_traffic()
+            tpc, tsrc = profile_traffic(cols or 4)
             roof = {"bound": "mufu", "achieved": achieved / 1e9, "peak": peak / 1e9,
                     "unit": "Gop/s", "frac": achieved / peak,
                     "traffic": None if tpc is None else tpc * cells,
                     "traffic_source": tsrc,
-                    "kernel": f"lbwd_kernel<3,{cols or 4},1> (checkpointed adjoint, scaled linear domain)",
+                    "kernel": f"lbwd_kernel<3,{cols or 4},1,0> (checkpointed adjoint, scaled linear domain)",
                     "algorithmic": (f"{MUFU_PER_CELL_BWD} ex2/lg2 per cell (the log-domain adjoint's "
                                     f"count) x {cells} cells"),
                     "peak_source": "measured in-bench (swb_mufu_probe: ex2.approx throughput)",

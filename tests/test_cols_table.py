@@ -60,3 +60,15 @@ def test_bench_batch_computed_cells_reported():
     mixed = (nb * (ln[:, 0] + 31) * w).sum() / useful
     print(f"  computed / useful cells: 4 columns per lane {r4:.3f}, bucket table {mixed:.3f}")
     assert 1.0 < r4 < 1.3 and 1.0 < mixed < 1.4
+
+
+def test_bench_traffic_profile_per_cols():
+    """The bench's roofline traffic comes from the committed DRAM capture of
+    the adjoint it launched: one per columns-per-lane choice."""
+    import bench
+
+    for cols in (4, 8):
+        v, src = bench.profile_traffic(cols)
+        assert v is not None and 8.0 <= v <= 20.0, (cols, v)
+        assert os.path.exists(os.path.join(ROOT, src))
+    assert bench.profile_traffic(2) == (None, None)
