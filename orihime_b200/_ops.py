@@ -1276,3 +1276,21 @@ from . import _registrations  # noqa: E402
 
 _registrations.register(DEFINED_HERE)
 _registrations.register(list(OWN_SCHEMAS), namespace="orihime_b200")
+
+
+def _tell_reference_loader() -> None:
+    """The reference's loader looks up a CUDA kernel for ``orihime::sw_forward``
+    once, when its extension loads, and keeps the answer
+    (orihime/_ops.py:42-47, :92); a build of it without CUDA keeps False and
+    then refuses CUDA tensors (:161-170).  Once the kernels above are
+    registered on its schemas, the answer is True."""
+    import sys
+
+    ref = sys.modules.get("orihime._ops")
+    if ref is None or getattr(ref, "_cuda_dispatch_available", None) is not False:
+        return
+    if torch._C._dispatch_has_kernel_for_dispatch_key("orihime::sw_forward", "CUDA"):
+        ref._cuda_dispatch_available = True
+
+
+_tell_reference_loader()

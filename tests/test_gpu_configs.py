@@ -38,15 +38,22 @@ def test_c5_training_step_grads_match_oracle(T):
     E = torch.randn(B, N, d, generator=g).cuda().requires_grad_(True)
     F = torch.randn(B, N, d, generator=g).cuda().requires_grad_(True)
     kw = dict(gap_open_score=-2.0, gap_extend_score=-0.5, temperature=T)
+
+    def step():
+        E.grad = F.grad = None
+        s = torch.bmm(E, F.transpose(1, 2)) / d ** 0.5
+        s.retain_grad()
+        out = -ohm.sw_affine_value(s, **kw).mean() + 0.01 * ohm.sw_affine_entropy(s, **kw).mean()
+        out.backward()
+        return s, out
+
+    step()                       # warm-up: first-call setup stays out of the timing
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record()
-    scores = torch.bmm(E, F.transpose(1, 2)) / d ** 0.5
-    scores.retain_grad()
-    loss = -ohm.sw_affine_value(scores, **kw).mean() + 0.01 * ohm.sw_affine_entropy(scores, **kw).mean()
-    loss.backward()
+    scores, loss = step()
     t1.record()
     torch.cuda.synchronize()
-    print(f"  C5 T={T}: forward+backward {t0.elapsed_time(t1):.1f} ms, loss {float(loss):.4f}")
+    print(f"  C5 T={T}: forward+backward {t0.elapsed_time(t1):.1f} ms, loss {float(loss.detach()):.4f}")
     assert torch.isfinite(loss)
     assert torch.isfinite(E.grad).all() and torch.isfinite(F.grad).all()
     # chain rule into E, F
