@@ -426,10 +426,11 @@ int swb_scan_scores(const float* x, int B, long long per_item, float limit, floa
  * lengths and parameters, runs the checkpointed adjoint: the marginal map
  * and dS/dparameters (and the value again).  It can run more than once.
  * ck_every in [1, 16]: 1 keeps a checkpoint per chunk (the fastest
- * adjoint); 4 keeps about 1.3 bytes per cell of the padded batch, and the
+ * adjoint); 4 keeps about 1.2 bytes per cell of a large padded batch, and the
  * adjoint recomputes the chunks in between from the nearest checkpoint.
  * The local families in the linear domain only: gaps must be <= 0, else
- * SWB_ERR_ARG.  4 columns per lane.  Workspace from
+ * SWB_ERR_ARG.  Columns per lane as swb_cols_per_lane gives for L2max (8 at
+ * L2max >= 256, else 4).  Workspace from
  * swb_*_checkpoint_workspace_bytes(B, L1max, L2max, ck_every).
  */
 size_t swb_sw_affine_checkpoint_workspace_bytes(int B, int L1max, int L2max, int ck_every);
