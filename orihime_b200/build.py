@@ -11,6 +11,7 @@ so it builds in seconds and loads with ctypes.
 
 from __future__ import annotations
 
+import glob
 import os
 import shutil
 import subprocess
@@ -20,14 +21,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 SO = os.path.join(PKG, "_swb.so")
 SOURCES = [os.path.join(PKG, "csrc", "sw_capi.cu")]
-DEPS = SOURCES + [
-    os.path.join(PKG, "csrc", "sw_kernels.cu"),
-    os.path.join(PKG, "csrc", "sw_kernels.cuh"),
-    os.path.join(PKG, "csrc", "sw_xband.cu"),
-    os.path.join(PKG, "csrc", "sw_prelude.cuh"),
-    os.path.join(PKG, "csrc", "sw_probe.cuh"),
-    os.path.join(ROOT, "include", "orihime_b200.h"),
-]
+# every file under csrc/ (sw_capi.cu includes the others) and the public header
+DEPS = sorted(glob.glob(os.path.join(PKG, "csrc", "*.cu")) + glob.glob(os.path.join(PKG, "csrc", "*.cuh"))
+              + [os.path.join(ROOT, "include", "orihime_b200.h"), os.path.abspath(__file__)])
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -31,7 +31,7 @@
 // value = m * 2^e.  A step computes its row in the frame et = max of its
 // inputs' normalised frames (the lane's previous row, the left lane's row and
 // the left lane's previous row), which makes every converted input <= 1;
-// then the row maximum gives the normalised frame n = et + exponent(max) in
+// then the row's sum gives the normalised frame n = et + exponent(sum) in
 // which the row is <= 1.  Rows are never rescaled: the raw values keep the
 // compute frame et and every use scales them by 2^(frame - target) (a
 // power-of-two factor built from the exponent bits, folded into the gap
@@ -75,51 +75,16 @@ constexpr float XMAX = 118.f;   // scaled scores above this are clamped (|s|/T <
 #define SWB_LQUIET 45
 #endif
 
-// Asynchronous global -> shared copies (cp.async): the adjoint stages the
-// next chunk's checkpoint and first score rows while it runs the current
-// chunk, so they occupy no registers in between.  A copy with src_size 0
-// writes zeros and reads nothing.
+// Asynchronous global -> shared copy (cp.async): the adjoint stages the next
+// chunk's checkpoint while it runs the current chunk, so it occupies no
+// registers in between.
 __device__ __forceinline__ void lcp16(float* dst, const float* src, int src_size) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_size)
                : "memory");
 }
-__device__ __forceinline__ void lcp8(float* dst, const float* src, int src_size) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_size)
-               : "memory");
-}
-__device__ __forceinline__ void lcp4(float* dst, const float* src, int src_size) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(src_size)
-               : "memory");
-}
 __device__ __forceinline__ void lcp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void lcp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// Stage row i (1-based) of the lane's R columns into dst (R floats, aligned
-// to 4R bytes); cells outside the pair or rows outside [1, L1] (ok false)
-// become 0, as load_row gives.
-template <int R>
-__device__ __forceinline__ void stage_row(float* dst, const Pair& pr, int i, int jl, bool ok) {
-  const float* src = pr.s + (size_t)(ok ? i - 1 : 0) * pr.ld + jl;
-  if (ok && pr.vec && jl + R <= pr.L2 && (R == 8 || R == 4 || R == 2)) {
-    if constexpr (R == 8) {
-      lcp16(dst, src, 16);
-      lcp16(dst + 4, src + 4, 16);
-    } else if constexpr (R == 4) {
-      lcp16(dst, src, 16);
-    } else {
-      lcp8(dst, src, 8);
-    }
-  } else {
-#pragma unroll
-    for (int c = 0; c < R; ++c) {
-      const bool v = ok && jl + c < pr.L2;
-      lcp4(dst + c, v ? src + c : pr.s, v ? 4 : 0);
-    }
-  }
-}
 
 // Checkpoint floats per lane (CKF, padded to float4), one checkpoint record
 // (LREC: CK4 groups of [lane][4]) and adjoint shared-memory floats per lane
@@ -210,7 +175,7 @@ __device__ __forceinline__ void lck_unpack(const float (&x)[LDims<NS, R>::CKF], 
 // Affine: M, I, D; linear: A (and, for the adjoint, the emission part em).
 template <int NS, int R>
 __device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], int xn,
-                                       const float (&xs)[R], float gO, float gE, int nlive,
+                                       const float (&xs)[R], bool live, float gO, float gE, int nlive,
                                        bool has_dead, int& et, float (&em)[R], float& rs) {
   // diagonal inputs of column 0: the left lane's previous row
   const int nd = s.nl;
@@ -219,7 +184,10 @@ __device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], 
   for (int q = 0; q < NS; ++q) { dg[q] = s.lv[q]; s.lv[q] = xl[q]; }
   s.nl = xn;
   et = max(max(s.n, xn), nd);
-  const float fU = p2i(s.e - et), fL = p2i(xn - et), fD = p2i(nd - et), st = p2i(-et);
+  // st: the fresh-start term 1 in frame et.  Before the lane's first row every
+  // input of the step is 0, so st = 0 keeps the whole row at 0 (E is finite:
+  // the scores of such rows are 0)
+  const float fU = p2i(s.e - et), fL = p2i(xn - et), fD = p2i(nd - et), st = live ? p2i(-et) : 0.f;
   float E[R];
 #pragma unroll
   for (int c = 0; c < R; ++c) E[c] = ex2(xs[c]);
@@ -231,8 +199,9 @@ __device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], 
       const float oM = s.v[0][c], oI = s.v[1][c], oD = s.v[2][c];
       const float m = E[c] * fmaf(fP, (pM + pI) + pD, st);
       const float iv = fmaf(gOu, oM, gEu * oI);
-      const float dv = c == 0 ? fmaf(gOl, s.lv[0], gEl * s.lv[2])
-                              : fmaf(gO, s.v[0][c - 1], gE * s.v[2][c - 1]);
+      // D runs along the lane's columns: one fma per column on that chain
+      const float dv = c == 0 ? fmaf(gEl, s.lv[2], gOl * s.lv[0])
+                              : fmaf(gE, s.v[2][c - 1], gO * s.v[0][c - 1]);
       s.v[0][c] = m; s.v[1][c] = iv; s.v[2][c] = dv;
       pM = oM; pI = oI; pD = oD; fP = fU;
       em[c] = 0.f;
@@ -261,31 +230,34 @@ __device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], 
         if (c >= nlive) { s.v[0][c] = 0.f; em[c] = 0.f; }
     }
   }
-  // the largest column sum bounds every value of the row (all are >= 0);
-  // the sums are also the row's partition terms
-  float mx = 0.f;
-  rs = 0.f;
+  // the row sum over columns and states bounds every value of the row (all
+  // are >= 0; it exceeds the largest by at most a factor 3R) and is the row's
+  // partition term
+  float cs[R];
 #pragma unroll
   for (int c = 0; c < R; ++c) {
-    float cs = s.v[0][c];
-    if constexpr (NS == 3) cs = (cs + s.v[1][c]) + s.v[2][c];
-    mx = fmaxf(mx, cs);
-    rs += cs;
+    cs[c] = s.v[0][c];
+    if constexpr (NS == 3) cs[c] = (cs[c] + s.v[1][c]) + s.v[2][c];
   }
+#pragma unroll
+  for (int h = 1; h < R; h *= 2)   // pairwise: a short dependency chain
+#pragma unroll
+    for (int c = 0; c + h < R; c += 2 * h) cs[c] += cs[c + h];
+  rs = cs[0];
   s.e = et;
-  s.n = max(et + fexp(mx), 0);
+  s.n = max(et + fexp(rs), 0);
   const float f = p2i(et - s.n);
 #pragma unroll
   for (int q = 0; q < NS; ++q) s.vs[q] = s.v[q][R - 1] * f;
 }
 
-// Scaled scores of one step: NEG before the lane's first row and in columns
-// past the pair (E = 0 there), clamped at XMAX.
+// Scaled scores of one step, clamped at XMAX; NEG in columns past the pair
+// (E = 0 there).  Rows outside the pair hold scores 0 (load_row).
 template <int R>
-__device__ __forceinline__ void lscores(const float (&sb)[R], int i, float k, int nlive, bool has_dead,
+__device__ __forceinline__ void lscores(const float (&sb)[R], float k, int nlive, bool has_dead,
                                         float (&xs)[R]) {
 #pragma unroll
-  for (int c = 0; c < R; ++c) xs[c] = i >= 1 ? fminf(__fmul_rn(sb[c], k), XMAX) : NEG;
+  for (int c = 0; c < R; ++c) xs[c] = fminf(__fmul_rn(sb[c], k), XMAX);
   if (has_dead) {
 #pragma unroll
     for (int c = 0; c < R; ++c)
@@ -322,6 +294,16 @@ __device__ __forceinline__ LParams lparams(const Args& a) {
 // forward band task
 // ---------------------------------------------------------------------------
 
+// Score prefetch distance of the forward (steps; C_STEPS % SWB_FPF == 0).  A
+// whole chunk: each row is requested a chunk before its step (measured on the
+// 4096-pair bench batch at 8 columns per lane: forward 2.27 ms at 4 steps,
+// 2.59 at 2, 3.05 at 1).
+#ifndef SWB_FPF
+#define SWB_FPF SWB_C_STEPS
+#endif
+constexpr int FPF = SWB_FPF;
+static_assert(C_STEPS % FPF == 0, "the forward's prefetch distance must divide the chunk");
+
 // Forward wavefront of one band: per-lane partition sums (Kahan, in the
 // lane's largest normalised frame), the left-to-right edge records
 // (last column normalised, then its frame) and, every C steps, a checkpoint
@@ -329,7 +311,7 @@ __device__ __forceinline__ LParams lparams(const Args& a) {
 // partition partial is (frame, mantissa sum): Z_band = sum * 2^frame.
 template <int NS, int R>
 __device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int lane,
-                          uint64_t deadline) {
+                          uint64_t deadline, float4* sedge) {
   using LD = LDims<NS, R>;
   check_lengths(a, w, lane);
   if (!lp.ok && w.band == 0 && lane == 0) {
@@ -379,9 +361,9 @@ __device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int 
   load_edge(0, eb);
 #pragma unroll
   for (int f = 0; f < NEF; ++f) ebn[f] = 0.f;
-  float sb[PF][R];   // per-lane score ring, PF steps ahead
+  float sb[FPF][R];   // per-lane score ring, FPF steps ahead
 #pragma unroll
-  for (int u = 0; u < PF; ++u) {
+  for (int u = 0; u < FPF; ++u) {
     const int i = u - lane + 1;
     load_row<R>(pr, i, jl, i >= 1 && i <= L1, sb[u]);
   }
@@ -414,37 +396,42 @@ __device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int 
         }
       }
     }
+    // the resolved records go to shared memory, where lane 0 reads the one of
+    // each step (one load instead of NS + 1 shuffles per step)
+    __syncwarp();
+    if (lane < C_STEPS) sedge[lane] = make_float4(eb[0], eb[1], eb[NEF > 2 ? 2 : 0], eb[NEF > 3 ? 3 : 0]);
+    __syncwarp();
     if (keep_ck && kc % KC == 0) lck_store<NS, R>(ck + (size_t)(kc / KC) * LD::LREC, lane, s);
     int cmx = -(1 << 30);   // largest normalised frame of the lane's live rows in this chunk
     if (kc + 1 < nch) load_edge(kc + 1, ebn);
 #pragma unroll 1
-    for (int u0 = 0; u0 < C_STEPS; u0 += PF)
+    for (int u0 = 0; u0 < C_STEPS; u0 += FPF)
 #pragma unroll
-    for (int u = 0; u < PF; ++u) {
+    for (int u = 0; u < FPF; ++u) {
       const int cu = u0 + u;
       const int t = kc * C_STEPS + cu;
       const int i = t - lane + 1;
       const bool act = (i >= 1) && (i <= L1);
-      float xl[NS], ev[NEF];
+      float xl[NS];
 #pragma unroll
       for (int q = 0; q < NS; ++q) xl[q] = __shfl_up_sync(FULL, s.vs[q], 1);
       int xn = __shfl_up_sync(FULL, s.n, 1);
-#pragma unroll
-      for (int f = 0; f < NEF; ++f) ev[f] = __shfl_sync(FULL, eb[f], cu);
       if (lane == 0) {   // the chunk's records are resolved (0 where there is no left band)
+        const float4 e4 = sedge[cu];
+        const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
 #pragma unroll
         for (int q = 0; q < NS; ++q) xl[q] = act ? ev[q] : 0.f;
         xn = act ? __float_as_int(ev[NS]) : 0;
       }
       float xs[R];
-      lscores<R>(sb[u], i, k, nlive, has_dead, xs);
+      lscores<R>(sb[u], k, nlive, has_dead, xs);
       {
-        const int ip = i + PF;
+        const int ip = i + FPF;
         load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
       }
       int et;
       float em[R], rs;
-      lcells<NS, R>(s, xl, xn, xs, gO, gE, nlive, has_dead, et, em, rs);
+      lcells<NS, R>(s, xl, xn, xs, i >= 1, gO, gE, nlive, has_dead, et, em, rs);
       if (act) {
         // partition: the row's live values (dead columns are 0) in the frame
         // ze (the largest normalised frame so far), Kahan-compensated
@@ -487,6 +474,7 @@ __device__ void lfwd_band(const Args& a, const LParams& lp, const Place& w, int 
 #endif
 template <int NS, int R>
 __global__ void __launch_bounds__(128, (R >= 8 ? 4 : SWB_LFWD_MINB)) lfwd_kernel(Args a) {
+  __shared__ float4 s_edge[4][C_STEPS];   // per warp: the left band's records of a chunk
   const int lane = threadIdx.x & 31;
   const LParams lp = lparams<NS>(a);
   const uint64_t deadline = gtimer() + a.spin_limit_ns;
@@ -496,7 +484,7 @@ __global__ void __launch_bounds__(128, (R >= 8 ? 4 : SWB_LFWD_MINB)) lfwd_kernel
     if (lane == 0) task = (int)atomicAdd(a.counters + 0, 1u);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ntasks) break;
-    lfwd_band<NS, R>(a, lp, place_of<NS, R>(a, task, false), lane, deadline);
+    lfwd_band<NS, R>(a, lp, place_of<NS, R>(a, task, false), lane, deadline, s_edge[threadIdx.x >> 5]);
   }
 }
 
@@ -578,10 +566,13 @@ __global__ void __launch_bounds__(128) lvalue_kernel(Args a) {
 // ---------------------------------------------------------------------------
 
 // Shared memory per adjoint warp (floats): one chunk of recomputed fields,
-// then the staged checkpoint and first PF score rows of the next chunk.
+// the staged checkpoint of the next chunk, then the chunk's cross-band
+// records as float4 per step: the left band's edge records (lane 0,
+// recompute) and the right band's push records (lane 31, outside recursion).
+// The next chunk's score rows wait in registers.
 template <int NS, int R>
 __host__ __device__ constexpr int lbwd_smem_floats() {
-  return (C_STEPS * LDims<NS, R>::FW + LDims<NS, R>::CKF + PF * R) * 32;
+  return (C_STEPS * LDims<NS, R>::FW + LDims<NS, R>::CKF) * 32 + 2 * C_STEPS * 4;
 }
 
 // Per band, checkpoint chunks in reverse.  Each chunk restores its checkpoint
@@ -628,10 +619,12 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
   const int KC = SPARSE ? a.ck_every : 1;   // checkpoint records every KC chunks
   const float* ckmax = ck + (size_t)((nch + KC - 1) / KC) * LREC;
 
-  // ---- chunk-ahead prefetch state: the next chunk's checkpoint and first
-  // PF score rows are staged in shared memory (cp.async), the rest here ----
+  // ---- chunk-ahead prefetch state: the next chunk's checkpoint is staged in
+  // shared memory (cp.async), its score rows and records wait in registers ----
   float* stg_ck = sm + C_STEPS * FW * 32;   // [CK4][lane][4]
-  float* stg_sc = stg_ck + CKF * 32;        // [PF][lane][R]
+  float4* s_eb = reinterpret_cast<float4*>(stg_ck + CKF * 32);   // [C] edge records
+  float4* s_pb = s_eb + C_STEPS;                                 // [C] push records
+  float nsb[C_STEPS][R];   // the next chunk's score rows, requested a chunk ahead
   int ckm;                 // the next chunk's largest normalised alpha frame
   float ebr[NEF];          // lane u < C: left-band edge record of lane 0's row at recompute step u
   float pbc[NPF], pbn[NPF];// lane u < C: right-band record lane 31 needs at backward step u
@@ -639,6 +632,7 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
     const float* rec = ck + (size_t)(kc / KC) * LREC;
 #pragma unroll
     for (int g = 0; g < LD::CK4; ++g) lcp16(stg_ck + g * 128 + lane * 4, rec + g * 128 + lane * 4, 16);
+    lcp_commit();
     ckm = __float_as_int(ckmax[kc]);
   };
   auto load_eb = [&](int kc) {
@@ -655,11 +649,10 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
   };
   auto load_sb = [&](int kc) {
 #pragma unroll
-    for (int u = 0; u < PF; ++u) {
+    for (int u = 0; u < C_STEPS; ++u) {
       const int i = kc * C_STEPS + u - lane + 1;
-      stage_row<R>(stg_sc + (u * 32 + lane) * R, pr, i, jl, i >= 1 && i <= L1);
+      load_row<R>(pr, i, jl, i >= 1 && i <= L1, nsb[u]);
     }
-    lcp_commit();
   };
   load_ck(nch - 1);
   load_eb(nch - 1);
@@ -815,16 +808,12 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
     }
     // ---- restore the checkpoint and recompute the chunk ----
     LState<NS, R> st;
-    float sb[PF][R];   // per-lane score ring, PF steps ahead
     {
       float ckr[CKF];
       lck_load<NS, R>(stg_ck, lane, ckr);
       lck_unpack<NS, R>(ckr, st);
-#pragma unroll
-      for (int u = 0; u < PF; ++u)
-#pragma unroll
-        for (int c = 0; c < R; ++c) sb[u][c] = stg_sc[(u * 32 + lane) * R + c];
     }
+    if (lane < C_STEPS) s_eb[lane] = make_float4(ebr[0], ebr[1], ebr[NEF > 2 ? 2 : 0], ebr[NEF > 3 ? 3 : 0]);
     __syncwarp();   // the stage is read before the next chunk's copies are issued
     if (SPARSE && kc % KC != 0) {
       // sparse checkpoints: the restored state is that of chunk kc - kc % KC;
@@ -865,22 +854,19 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
             xn = act ? __float_as_int(ev[NS]) : 0;
           }
           float xs[R];
-          lscores<R>(ab[u], i, k, nlive, has_dead, xs);
+          lscores<R>(ab[u], k, nlive, has_dead, xs);
           {
             const int ip = i + PF;
             load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, ab[u]);
           }
           int et;
           float em[R], rs;
-          lcells<NS, R>(st, xl, xn, xs, gO, gE, nlive, has_dead, et, em, rs);
+          lcells<NS, R>(st, xl, xn, xs, i >= 1, gO, gE, nlive, has_dead, et, em, rs);
         }
       }
     }
-#pragma unroll 1
-    for (int u0 = 0; u0 < C_STEPS; u0 += PF)
 #pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      const int cu = u0 + u;
+    for (int cu = 0; cu < C_STEPS; ++cu) {
       const int t = t0 + cu;
       const int i = t - lane + 1;
       const bool act = (i >= 1) && (i <= L1);
@@ -888,23 +874,18 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
 #pragma unroll
       for (int q = 0; q < NS; ++q) xl[q] = __shfl_up_sync(FULL, st.vs[q], 1);
       int xn = __shfl_up_sync(FULL, st.n, 1);
-      float ev[NEF];
-#pragma unroll
-      for (int f = 0; f < NEF; ++f) ev[f] = __shfl_sync(FULL, ebr[f], cu);
       if (lane == 0) {
+        const float4 e4 = s_eb[cu];
+        const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
 #pragma unroll
         for (int q = 0; q < NS; ++q) xl[q] = act ? ev[q] : 0.f;
         xn = act ? __float_as_int(ev[NS]) : 0;
       }
       float xs[R];
-      lscores<R>(sb[u], i, k, nlive, has_dead, xs);
-      if (cu + PF < C_STEPS) {
-        const int ip = i + PF;
-        load_row<R>(pr, ip, jl, ip >= 1 && ip <= L1, sb[u]);
-      }
+      lscores<R>(nsb[cu], k, nlive, has_dead, xs);
       int et;
       float em[R], rs;
-      lcells<NS, R>(st, xl, xn, xs, gO, gE, nlive, has_dead, et, em, rs);
+      lcells<NS, R>(st, xl, xn, xs, i >= 1, gO, gE, nlive, has_dead, et, em, rs);
       float* ent = sm + (size_t)cu * FW * 32;
       if constexpr (R % 4 == 0) {
         // field g's R columns as R / 4 float4 per lane: [g][quad][lane][4]
@@ -944,6 +925,7 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
       load_sb(kc - 1);
       load_pb(kc - 1, pbn);
     }
+    if (lane < C_STEPS) s_pb[lane] = make_float4(pbc[0], pbc[1], pbc[2], 0.f);
     __syncwarp();
     float cA = 0.f, cB = 0.f, cS = 0.f;   // this chunk's plain sums
     // ---- outside recursion over the chunk, last step first ----
@@ -959,11 +941,9 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
       float rb = __shfl_down_sync(FULL, o_b, 1);
       float rt = __shfl_down_sync(FULL, o_t, 1);
       int rn = __shfl_down_sync(FULL, o_n, 1);
-      {   // resolved at the chunk's start (the quiet-chunk test polls them)
-        float pw[NPF];
-#pragma unroll
-        for (int f = 0; f < NPF; ++f) pw[f] = __shfl_sync(FULL, pbc[f], cu);
-        if (lane == 31) { rb = pw[0]; rt = pw[1]; rn = __float_as_int(pw[2]); }
+      if (lane == 31) {   // resolved at the chunk's start (the quiet-chunk test polls them)
+        const float4 p4 = s_pb[cu];
+        rb = p4.x; rt = p4.y; rn = __float_as_int(p4.z);
       }
       // frames: the row is computed in ft >= every input's normalised frame
       const int ft = max(max(nb, rn), hn);
@@ -991,8 +971,8 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
       const float one = act ? st1 : 0.f;
       float br = fR * rb;   // right successor's beta_D (beta)
       float td = fH * ht;   // diagonal successor's t
-      float nbv[R], nmv[R], pm[R];
-      float mx = 0.f, so = 0.f, sx = 0.f, sp = 0.f;
+      float nbv[R], nmv[R], pm[R], mxv[R];
+      float so = 0.f, sx = 0.f, sp = 0.f;
 #pragma unroll
       for (int c = R - 1; c >= 0; --c) {
         const float oc = c < nlive ? one : 0.f;
@@ -1011,24 +991,28 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
           sp = fmaf(P, fa[3][c], sp);
           nbv[c] = vi;
           nmv[c] = vm;
-          mx = fmaxf(mx, fmaf(gX, sr, base));   // >= vm, vi, vd
+          mxv[c] = fmaf(gX, sr, base);   // >= vm, vi, vd
           br = vd;
         } else {
           const float sr = bd + br;
-          const float vb = fmaf(gO, sr, base);
+          const float vb = fmaf(gO, br, fmaf(gO, bd, base));   // one fma on the column chain
           const float P = fminf(((fa[1][c] * as) * sc) * vb, 1.f);
           pm[c] = P;
           so = fmaf(fa[0][c] * as, sr, so);
           sp = fmaf(P, fa[2][c], sp);
           nbv[c] = vb;
           nmv[c] = vb;
-          mx = fmaxf(mx, vb);
+          mxv[c] = vb;
           br = vb;
         }
         td = fTd * tdn[c];
       }
       // normalise: t = E beta_M in the row's normalised frame
-      const int nn = max(ft + fexp(mx), 0);
+#pragma unroll
+      for (int h = 1; h < R; h *= 2)   // pairwise maximum: a short dependency chain
+#pragma unroll
+        for (int c = 0; c + h < R; c += 2 * h) mxv[c] = fmaxf(mxv[c], mxv[c + h]);
+      const int nn = max(ft + fexp(mxv[0]), 0);
       const float bs = p2i(ft - nn);
 #pragma unroll
       for (int c = 0; c < R; ++c) {
