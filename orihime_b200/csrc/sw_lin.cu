@@ -105,10 +105,21 @@ template <int NS, int R> struct LDims {
 // Lane state of the forward wavefront.
 template <int NS, int R> struct LState {
   float v[NS][R];   // raw values of the lane's latest row (frame e)
+  float cs[NS == 3 ? R : 1];   // affine: their column sums (M + I) + D (frame e)
   float lv[NS];     // the left lane's latest row, last column (normalised frame nl)
   float vs[NS];     // the lane's last column in its normalised frame n
   int e, n, nl;
 };
+
+// Affine: the column sums of the lane's row, the diagonal inputs of the next
+// row's M (formed once per row, not once per cell).
+template <int NS, int R>
+__device__ __forceinline__ void lstate_sums(LState<NS, R>& s) {
+  if constexpr (NS == 3) {
+#pragma unroll
+    for (int c = 0; c < R; ++c) s.cs[c] = (s.v[0][c] + s.v[1][c]) + s.v[2][c];
+  }
+}
 
 template <int NS, int R>
 __device__ __forceinline__ void lstate_zero(LState<NS, R>& s) {
@@ -118,6 +129,7 @@ __device__ __forceinline__ void lstate_zero(LState<NS, R>& s) {
 #pragma unroll
     for (int c = 0; c < R; ++c) s.v[q][c] = 0.f;
   }
+  lstate_sums(s);
   s.e = 0; s.n = 0; s.nl = 0;
 }
 
@@ -162,6 +174,7 @@ __device__ __forceinline__ void lck_unpack(const float (&x)[LDims<NS, R>::CKF], 
   s.e = __float_as_int(x[NS * R + NS]);
   s.n = __float_as_int(x[NS * R + NS + 1]);
   s.nl = __float_as_int(x[NS * R + NS + 2]);
+  lstate_sums(s);
   const float f = p2i(s.e - s.n);
 #pragma unroll
   for (int q = 0; q < NS; ++q) s.vs[q] = s.v[q][R - 1] * f;
@@ -193,17 +206,17 @@ __device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], 
   for (int c = 0; c < R; ++c) E[c] = ex2(xs[c]);
   if constexpr (NS == 3) {
     const float gOu = gO * fU, gEu = gE * fU, gOl = gO * fL, gEl = gE * fL;
-    float pM = dg[0], pI = dg[1], pD = dg[2], fP = fD;
+    float pS = (dg[0] + dg[1]) + dg[2], fP = fD;   // diagonal (M + I) + D of column 0
 #pragma unroll
     for (int c = 0; c < R; ++c) {
-      const float oM = s.v[0][c], oI = s.v[1][c], oD = s.v[2][c];
-      const float m = E[c] * fmaf(fP, (pM + pI) + pD, st);
+      const float oM = s.v[0][c], oI = s.v[1][c];
+      const float m = E[c] * fmaf(fP, pS, st);
       const float iv = fmaf(gOu, oM, gEu * oI);
       // D runs along the lane's columns: one fma per column on that chain
       const float dv = c == 0 ? fmaf(gEl, s.lv[2], gOl * s.lv[0])
                               : fmaf(gE, s.v[2][c - 1], gO * s.v[0][c - 1]);
       s.v[0][c] = m; s.v[1][c] = iv; s.v[2][c] = dv;
-      pM = oM; pI = oI; pD = oD; fP = fU;
+      pS = s.cs[c]; fP = fU;   // the previous row's column sum: column c + 1's diagonal
       em[c] = 0.f;
     }
     if (has_dead) {   // columns past the pair: D would run on from the last live column
@@ -233,11 +246,12 @@ __device__ __forceinline__ void lcells(LState<NS, R>& s, const float (&xl)[NS], 
   // the row sum over columns and states bounds every value of the row (all
   // are >= 0; it exceeds the largest by at most a factor 3R) and is the row's
   // partition term
+  lstate_sums(s);
   float cs[R];
 #pragma unroll
   for (int c = 0; c < R; ++c) {
-    cs[c] = s.v[0][c];
-    if constexpr (NS == 3) cs[c] = (cs[c] + s.v[1][c]) + s.v[2][c];
+    if constexpr (NS == 3) cs[c] = s.cs[c];
+    else cs[c] = s.v[0][c];
   }
 #pragma unroll
   for (int h = 1; h < R; h *= 2)   // pairwise: a short dependency chain
@@ -969,43 +983,43 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
           for (int c = 0; c < R; ++c) fa[g][c] = ent[(g * R + c) * 32 + lane];
       }
       const float one = act ? st1 : 0.f;
+      // per-row factors folded out of the cells: the frame of the row below
+      // (fBd), alpha's normalisation (as) and the posterior scale (sc)
+      const float asc = as * sc, gEb = gE * fBd, gOb = gO * fBd;
       float br = fR * rb;   // right successor's beta_D (beta)
-      float td = fH * ht;   // diagonal successor's t
       float nbv[R], nmv[R], pm[R], mxv[R];
-      float so = 0.f, sx = 0.f, sp = 0.f;
+      float so = 0.f, sxi = 0.f, sxd = 0.f, sp = 0.f;   // sums of raw alpha x beta
 #pragma unroll
       for (int c = R - 1; c >= 0; --c) {
         const float oc = c < nlive ? one : 0.f;
-        const float bd = fBd * bdn[c];   // beta_I (beta) of the cell below
-        const float base = oc + td;
+        // plus the diagonal successor's t
+        const float base = c == R - 1 ? fmaf(fH, ht, oc) : fmaf(fTd, tdn[c + 1], oc);
+        const float sr = fmaf(fBd, bdn[c], br);   // beta_I (beta) below + beta_D right
         if constexpr (NS == 3) {
-          const float sr = bd + br;
           const float vm = fmaf(gO, sr, base);
-          const float vi = fmaf(gE, bd, base);
+          const float vi = fmaf(gEb, bdn[c], base);
           const float vd = fmaf(gE, br, base);
-          const float am = fa[0][c] * as, ai = fa[1][c] * as, ad = fa[2][c] * as;
-          const float P = fminf((am * sc) * vm, 1.f);   // a posterior: rounding may pass 1
+          const float P = fminf((fa[0][c] * asc) * vm, 1.f);   // a posterior: rounding may pass 1
           pm[c] = P;
-          so = fmaf(am, sr, so);
-          sx = fmaf(ai, bd, fmaf(ad, br, sx));
+          so = fmaf(fa[0][c], sr, so);
+          sxi = fmaf(fa[1][c], bdn[c], sxi);
+          sxd = fmaf(fa[2][c], br, sxd);
           sp = fmaf(P, fa[3][c], sp);
           nbv[c] = vi;
           nmv[c] = vm;
           mxv[c] = fmaf(gX, sr, base);   // >= vm, vi, vd
           br = vd;
         } else {
-          const float sr = bd + br;
-          const float vb = fmaf(gO, br, fmaf(gO, bd, base));   // one fma on the column chain
-          const float P = fminf(((fa[1][c] * as) * sc) * vb, 1.f);
+          const float vb = fmaf(gO, br, fmaf(gOb, bdn[c], base));   // one fma on the column chain
+          const float P = fminf((fa[1][c] * asc) * vb, 1.f);
           pm[c] = P;
-          so = fmaf(fa[0][c] * as, sr, so);
+          so = fmaf(fa[0][c], sr, so);
           sp = fmaf(P, fa[2][c], sp);
           nbv[c] = vb;
           nmv[c] = vb;
           mxv[c] = vb;
           br = vb;
         }
-        td = fTd * tdn[c];
       }
       // normalise: t = E beta_M in the row's normalised frame
 #pragma unroll
@@ -1027,10 +1041,10 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
       ht = rt;
       hn = rn;
       if constexpr (NS == 3) {
-        cA = fmaf(so * sc, gO, cA);
-        cB = fmaf(sx * sc, gE, cB);
+        cA = fmaf(so * asc, gO, cA);
+        cB = fmaf(fmaf(sxi, fBd, sxd) * asc, gE, cB);
       } else {
-        cA = fmaf(so * sc, gO, cA);
+        cA = fmaf(so * asc, gO, cA);
       }
       cS += sp;
       if (act) {
