@@ -86,6 +86,56 @@ __device__ __forceinline__ void lcp16(float* dst, const float* src, int src_size
 __device__ __forceinline__ void lcp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void lcp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// ---------------------------------------------------------------------------
+// whole-chunk row pieces
+// ---------------------------------------------------------------------------
+// In the skewed wavefront lane l works on row t - l + 1 at step t, so one
+// store of every lane touches 32 rows: 32 cache lines per warp instruction.
+// Over a checkpoint chunk (C steps), though, row i is worked on by C
+// adjacent lanes, whose columns are one contiguous piece of 4 C R bytes.  The
+// adjoint writes the map rows of a quiet chunk (zeros) in whole row pieces:
+// round `it`, item k = 32 it + lane is float4 h of lane l at step cu with
+// q = k % NI, rho = k / NI, cu = q / HR, h = q % HR, l = rho - (C - 1) + cu;
+// its row is kc C + cu - l + 1.  Every (cu, l, h) is one item; NI
+// consecutive items are one row piece.
+template <int R> struct Pieces {
+  static constexpr int HR = R / 4;                    // float4 per lane and row
+  static constexpr int NI = C_STEPS * HR;             // items per row piece
+  static constexpr int ROWS = 32 + C_STEPS - 1;       // rows a chunk touches
+  static constexpr int ROUNDS = (ROWS * NI + 31) / 32;
+};
+
+// Zero chunk kc's map rows of a band (a quiet chunk) in whole row pieces.
+// Rows outside [1, L1] are not written; every column up to the row pitch is.
+// The rounds run as a loop: unrolled, their per-lane item indices would stay
+// live in registers across the adjoint.
+template <int R>
+__device__ __forceinline__ void zero_chunk_rows(const Pair& pr, int kc, int col0, int lane) {
+  using P = Pieces<R>;
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 1
+  for (int it = 0; it < P::ROUNDS; ++it) {
+    const int k = it * 32 + lane;
+    const int rho = k / P::NI, q = k - rho * P::NI;
+    const int cu = q / P::HR, h = q - cu * P::HR;
+    const int l = rho - (C_STEPS - 1) + cu;
+    if (rho < P::ROWS && l >= 0 && l < 32) {
+      const int i = kc * C_STEPS + cu - l + 1;
+      const int col = col0 + R * l + 4 * h;
+      if (i >= 1 && i <= pr.L1 && col < pr.ld) {
+        float* dst = pr.m + (size_t)(i - 1) * pr.ld + col;
+        if (pr.vec) {
+          *reinterpret_cast<float4*>(dst) = z;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (col + e < pr.ld) dst[e] = 0.f;
+        }
+      }
+    }
+  }
+}
+
 // Checkpoint floats per lane (CKF, padded to float4), one checkpoint record
 // (LREC: CK4 groups of [lane][4]) and adjoint shared-memory floats per lane
 // per step (FW).  A band's checkpoint region holds ceil(nchunks / ck_every)
@@ -739,13 +789,16 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
       if (__all_sync(FULL, ok)) {
         // zero map rows and left-band records for the rows of chunk kq
         auto zero_chunk = [&](int kq) {
-          float z[R];
-#pragma unroll
-          for (int c = 0; c < R; ++c) z[c] = 0.f;
+          if constexpr (R % 4 == 0) zero_chunk_rows<R>(pr, kq, col0, lane);
           for (int cu = 0; cu < C_STEPS; ++cu) {
             const int i = kq * C_STEPS + cu - lane + 1;
             if (i >= 1 && i <= L1) {
-              store_row<R>(pr, i, jl, z);
+              if constexpr (R % 4 != 0) {
+                float z[R];
+#pragma unroll
+                for (int c = 0; c < R; ++c) z[c] = 0.f;
+                store_row<R>(pr, i, jl, z);
+              }
               if (lane == 0 && pout) {
                 pout[0 * (Lm + 1) + i] = 0.f;
                 pout[1 * (Lm + 1) + i] = 0.f;
