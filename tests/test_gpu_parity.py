@@ -257,6 +257,18 @@ def test_quiet_chunks_stay_within_tolerance(fam):
     assert float(m1.cpu().numpy()[tiny].max()) < 1e-12
 
 
+@pytest.mark.parametrize("fam", ["aff", "lin"])
+def test_quiet_chunks_with_unaligned_rows(fam):
+    """Quiet chunks write their zero map rows in whole row pieces; with a
+    padded width that is not a multiple of 4 the rows are not 16-byte aligned
+    and the pieces are written element by element.  Ragged lengths put the
+    pairs' right edges (pitch padding written as 0) inside those pieces."""
+    s = _emb_scores(3, 1100, 1001, 64, 9)
+    ln = torch.tensor([[1100, 1001], [1037, 998], [640, 733]], dtype=torch.int32)
+    params = (-2.0, -0.5, 0.5) if fam == "aff" else (-1.0, 0.5)
+    _cmp(fam, s, ln, params)
+
+
 # ---- through the C ABI directly ----
 
 def test_c_abi_direct_call():
