@@ -649,7 +649,8 @@ __host__ __device__ constexpr int lbwd_smem_floats() {
 // the t for one more step (it is the diagonal successor of the next row).
 // Lane 0 passes the same three values to the left band through the push
 // buffer; lane 31 reads the right band's.  No atomics; the map is written row
-// by row; the gradient sums are folded per pair in band order.
+// by row (a quiet chunk writes its zero rows in whole row pieces); the
+// gradient sums are folded per pair in band order.
 template <int NS, int R, bool SPARSE = false>
 __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int lane, float* sm,
                           uint64_t deadline) {
@@ -743,7 +744,7 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
   const int zlog = ze + fexp(zm) - 1 - SWB_LQUIET;
   for (int kc = nch - 1; kc >= 0; --kc) {
     const int t0 = kc * C_STEPS;
-    lcp_wait_all();   // this chunk's staged checkpoint and score rows
+    lcp_wait_all();   // this chunk's staged checkpoint
     __syncwarp();
     // ---- quiet chunk.  For a cell u of the chunk, alpha_u beta_u / Z sums,
     // over the chunk cells x where u's continuations stay inside, terms
@@ -881,7 +882,7 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
       lck_unpack<NS, R>(ckr, st);
     }
     if (lane < C_STEPS) s_eb[lane] = make_float4(ebr[0], ebr[1], ebr[NEF > 2 ? 2 : 0], ebr[NEF > 3 ? 3 : 0]);
-    __syncwarp();   // the stage is read before the next chunk's copies are issued
+    __syncwarp();   // the staged checkpoint is read before the next chunk's copy is issued
     if (SPARSE && kc % KC != 0) {
       // sparse checkpoints: the restored state is that of chunk kc - kc % KC;
       // run the forward over the chunks in between (the same steps as the
