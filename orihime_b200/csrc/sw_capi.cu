@@ -15,6 +15,7 @@
 
 #include "sw_kernels.cu"
 #include "sw_lin.cu"
+#include "sw_tan.cu"
 #include "sw_xband.cu"
 #include "sw_prelude.cuh"
 #include "sw_probe.cuh"
@@ -539,6 +540,115 @@ int launch_xband_r(swb::XArgs a, cudaStream_t st) {
   return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
 }
 
+// ---- second-order ops of the local models in the linear domain ----
+
+constexpr int kTanR = 4;   // columns per lane of the tangent kernels
+static_assert((int)swb::TM_SCORE == (int)swb::AUX_HVP && (int)swb::TM_G0 == (int)swb::AUX_P0 &&
+                  (int)swb::TM_G1 == (int)swb::AUX_P1 && (int)swb::TM_T == (int)swb::AUX_PT,
+              "tangent directions follow the second-order op modes");
+
+// Workspace of the tangent kernels: counters and status, per-pair completion
+// counts, per-band (frame, Z) and (frame, Z') partials and parameter-tangent
+// partials, then (sentinel-filled) edge and push records, then checkpoints.
+struct TLayout {
+  size_t off_pair_done, off_part, off_zdot, off_gpart, off_edge, off_bpush, off_ckpt, total;
+  int nb, nchunks;
+};
+
+template <int NS>
+TLayout tlayout(long long B, long long L1m, long long L2m) {
+  using D = swb::TDims<NS, kTanR>;
+  TLayout l{};
+  l.nb = (int)std::max(1LL, (L2m + 32 * kTanR - 1) / (32 * kTanR));
+  l.nchunks = chunks_for(L1m);
+  const size_t slots = (size_t)B * l.nb;
+  size_t o = align_up(64);   // counters [0, 1], status [4]
+  l.off_pair_done = o; o = align_up(o + sizeof(unsigned) * (size_t)B);
+  l.off_part = o;      o = align_up(o + sizeof(float) * 2 * slots);
+  l.off_zdot = o;      o = align_up(o + sizeof(float) * 2 * slots);
+  l.off_gpart = o;     o = align_up(o + sizeof(float) * 8 * slots);
+  l.off_edge = o;      o = align_up(o + sizeof(float) * slots * D::NEF * (size_t)L1m);
+  l.off_bpush = o;     o = align_up(o + sizeof(float) * slots * D::NPF * (size_t)(L1m + 1));
+  l.off_ckpt = o;      o = align_up(o + sizeof(float) * slots * (size_t)l.nchunks * D::LREC);
+  l.total = o;
+  return l;
+}
+
+// The linear-domain tangent kernels serve the local models when every gap is
+// <= 0 and T is finite and positive (the first-order linear domain's range).
+bool tan_eligible(float go, float ge, float T) {
+  if (!SWB_TAN || !(T > 0.f) || !(T < INFINITY)) return false;
+  const float k = 1.4426950408889634f / T;
+  return (double)go * k <= 0.0 && (double)ge * k <= 0.0;
+}
+
+struct TOcc {
+  int f = 0, b = 0;
+  bool ready = false;
+};
+TOcc g_tocc[64][2][4];   // [device][affine?][mode]
+
+template <int NS, int MODE>
+int launch_tan(const float* scores, const float* v, const int* lengths, int B, int L1m, int L2m,
+               float go, float ge, float T, float* out, float* gt, void* ws, size_t ws_bytes,
+               cudaStream_t st) {
+  constexpr int R = kTanR;
+  const TLayout l = tlayout<NS>(B, L1m, L2m);
+  if (!ws || ws_bytes < l.total) return SWB_ERR_WORKSPACE;
+  DevInfo* d = nullptr;
+  int rc = dev_info(&d);
+  if (rc != SWB_OK) return rc;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWB_ERR_CUDA;
+  const size_t smem = sizeof(float) * swb::ltbwd_smem_floats<NS, R>();
+  TOcc& o = g_tocc[dev][NS == 3][MODE];
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!o.ready) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.f, swb::ltfwd_kernel<NS, R, MODE>, 128, 0) !=
+              cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.b, swb::ltbwd_kernel<NS, R, MODE>, 32, smem) !=
+              cudaSuccess)
+        return SWB_ERR_CUDA;
+      o.ready = true;
+    }
+  }
+  char* w = static_cast<char*>(ws);
+  // per-call resets: header, completion counts and partials to 0; the edge and
+  // push records to the NaN sentinel; the output to 0 (cells outside lengths)
+  if (cudaMemsetAsync(w, 0, l.off_edge, st) != cudaSuccess) return SWB_ERR_CUDA;
+  if (cudaMemsetAsync(w + l.off_edge, 0xff, l.off_ckpt - l.off_edge, st) != cudaSuccess) return SWB_ERR_CUDA;
+  const size_t map_elems = (size_t)B * L1m * L2m;
+  if (map_elems > 0 && cudaMemsetAsync(out, 0, map_elems * sizeof(float), st) != cudaSuccess)
+    return SWB_ERR_CUDA;
+  swb::Args a{};
+  a.scores = scores; a.map = out; a.lengths = lengths;
+  a.B = B; a.Lmax1 = L1m; a.Lmax2 = L2m; a.layout = 0;
+  a.go = go; a.ge = ge; a.T = T; a.k = 1.4426950408889634f / T;
+  a.xgo = (float)exp2((double)go * (double)a.k);
+  a.xge = (float)exp2((double)ge * (double)a.k);
+  a.nb = l.nb; a.nchunks = l.nchunks;
+  a.counters = reinterpret_cast<unsigned*>(w);
+  a.status = a.counters + 4;
+  a.pair_done = reinterpret_cast<unsigned*>(w + l.off_pair_done);
+  a.part = reinterpret_cast<float*>(w + l.off_part);
+  a.zdot = reinterpret_cast<float*>(w + l.off_zdot);
+  a.gpart = reinterpret_cast<float*>(w + l.off_gpart);
+  a.edge = reinterpret_cast<float*>(w + l.off_edge);
+  a.bpush = reinterpret_cast<float*>(w + l.off_bpush);
+  a.ckpt = reinterpret_cast<float*>(w + l.off_ckpt);
+  a.tdir = v; a.tgt = gt; a.tmode = MODE;
+  a.spin_limit_ns = 20ull * 1000000000ull;
+  const long long ntasks = (long long)B * l.nb;
+  const long long cap_f = (long long)d->sms * (o.f > 0 ? o.f : 1);
+  const long long cap_b = (long long)d->sms * (o.b > 0 ? o.b : 1);
+  const int grid_f = (int)std::min((ntasks + 3) / 4, cap_f);
+  const int grid_b = (int)std::min(ntasks, cap_b);
+  swb::ltfwd_kernel<NS, R, MODE><<<grid_f, 128, 0, st>>>(a);
+  swb::ltbwd_kernel<NS, R, MODE><<<grid_b, 32, smem, st>>>(a);
+  return cudaPeekAtLastError() == cudaSuccess ? SWB_OK : SWB_ERR_CUDA;
+}
+
 template <int NS, int MODE, int G = 0>
 int launch_xband(const float* scores, const float* v, const int* lengths, int B, int L1m, int L2m,
                  float go, float ge, float T, float* out, float* gt, void* ws, size_t ws_bytes,
@@ -546,6 +656,14 @@ int launch_xband(const float* scores, const float* v, const int* lengths, int B,
   if (B < 0 || L1m < 0 || L2m < 0) return SWB_ERR_ARG;
   if (!(T > 0.f) || !(T < INFINITY)) return SWB_ERR_ARG;
   if (B == 0) return SWB_OK;
+  if constexpr (G == 0) {
+    if (tan_eligible(go, NS == 3 ? ge : 0.f, T)) {
+      const size_t map_elems = (size_t)B * L1m * L2m;
+      if (map_elems > 0 && (!scores || !out || (MODE == swb::AUX_HVP && !v))) return SWB_ERR_ARG;
+      return launch_tan<NS, MODE>(scores, v, lengths, B, L1m, L2m, go, ge, T, out, gt, ws, ws_bytes,
+                                  reinterpret_cast<cudaStream_t>(stream_v));
+    }
+  }
   const size_t map_elems = (size_t)B * L1m * L2m;
   if (map_elems > 0 && (!scores || !out || (MODE == swb::AUX_HVP && !v))) return SWB_ERR_ARG;
   const XLayout l = xlayout<NS, G>(B, L1m, L2m);
@@ -770,11 +888,11 @@ int swb_sw_adjoint(const float* scores, const int* lengths, int B, int L1max, in
 }
 
 size_t swb_sw_affine_aux_workspace_bytes(int B, int L1max, int L2max) {
-  return B > 0 ? xlayout<3>(B, L1max, L2max).total : 0;
+  return B > 0 ? std::max(xlayout<3>(B, L1max, L2max).total, tlayout<3>(B, L1max, L2max).total) : 0;
 }
 
 size_t swb_sw_aux_workspace_bytes(int B, int L1max, int L2max) {
-  return B > 0 ? xlayout<1>(B, L1max, L2max).total : 0;
+  return B > 0 ? std::max(xlayout<1>(B, L1max, L2max).total, tlayout<1>(B, L1max, L2max).total) : 0;
 }
 
 int swb_sw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,

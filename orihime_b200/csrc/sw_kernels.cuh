@@ -119,6 +119,11 @@ struct Args {
   unsigned long long spin_limit_ns;
   int fault_inject;           // 1: band>0 waits on a word nobody writes (tests only)
   float* never_written;       // target of fault_inject polls
+  // tangent (second-order) kernels of the linear domain, layout 0 only
+  const float* tdir;          // tmode 0: the score direction [B, Lmax1, Lmax2]
+  float* tgt;                 // tmode 0: per pair tangents of (g0, g1, g_T, S) [B][4], or null
+  float* zdot;                // [B*nb][2] per band: frame, tangent of the partition sum
+  int tmode;                  // 0 score direction, 1 gap_open (linear: gap), 2 gap_ext, 3 temperature
 };
 
 }  // namespace swb

@@ -10,14 +10,22 @@ arguments on CUDA tensors: square, rectangular, ragged (``lengths=``),
 1 x 1 and one-row batches, a boolean ``mask=`` batch, and learnable
 (tensor, requires_grad) gap and temperature parameters.
 
-Tolerances are those of the reference's CPU-vs-CUDA tests
-(tests/test_soft_sw_affine.py:425-575): values rtol 1e-5, maps and score
-gradients atol 1e-5, parameter contractions atol 1e-4, entropy atol 2e-5.
+First-order outputs are held to values rtol 1e-5, maps and score gradients
+atol 1e-5, parameter gradients atol 1e-4, entropy atol 2e-5: tighter than the
+reference's own CPU-vs-CUDA tests (tests/test_soft_sw_affine.py:425-575).
+Second-order outputs (the named operations' sensitivities and backward
+fields) are held as every second-order test here: to the fp64 oracle, no
+further than max(1e-4 of the field's largest exact entry, the reference's own
+recorded distance from fp64); and to the reference's recorded outputs at the
+reference's own CPU-vs-CUDA tolerance for these fields (rtol 1e-2, atol 5e-3,
+tests/test_soft_sw_affine.py:536-542).
 """
 
 import numpy as np
 import pytest
 import torch
+
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -72,6 +80,34 @@ def test_public_functions_match_reference(golden, fam, case):
     np.testing.assert_allclose(dh.cpu().numpy(), g("dentropy"), atol=1e-4)
 
 
+def _second_order_close(tag, got, ref_out, exact):
+    """got within max(1e-4 of the largest exact entry, the reference's own
+    distance from fp64) of fp64, and within the reference's CPU-vs-CUDA
+    tolerance of its recorded output."""
+    got, ref_out, exact = (np.asarray(x, np.float64) for x in (got, ref_out, exact))
+    scale = float(np.abs(exact).max()) if exact.size else 0.0
+    bound = max(1e-4 * scale, float(np.abs(ref_out - exact).max()) if exact.size else 0.0, 1e-7)
+    err = float(np.abs(got - exact).max()) if exact.size else 0.0
+    assert err <= bound, f"{tag}: ours-fp64 {err:.2e} > bound {bound:.2e}"
+    np.testing.assert_allclose(got, ref_out, rtol=1e-2, atol=5e-3, err_msg=tag)
+
+
+def _exact_second_order(fam, s, cot, ln, kw):
+    """fp64 oracle: per parameter the map's sensitivity, and the map's VJP."""
+    sn = s.cpu().numpy()
+    lnn = None if ln is None else ln.cpu().numpy()
+    cn = cot.cpu().numpy().astype(np.float64)
+    if fam == "aff":
+        p = (kw["gap_open_score"], kw["gap_extend_score"], kw["temperature"])
+        sens = [O.affine_param_grad(sn, lnn, *p, k, dtype=np.float64) for k in range(3)]
+        hv = O.affine_hvp(sn, cn, lnn, *p, dtype=np.float64)
+    else:
+        p = (kw["gap_score"], kw["temperature"])
+        sens = [O.linear_param_grad(sn, lnn, *p, k, dtype=np.float64) for k in range(2)]
+        hv = O.linear_hvp(sn, cn, lnn, *p, dtype=np.float64)
+    return sens, hv, [float((cn * x).sum()) for x in sens]
+
+
 @pytest.mark.parametrize("fam", list(FAMS))
 @pytest.mark.parametrize("case", CASES)
 def test_named_operations_match_reference(golden, fam, case):
@@ -81,20 +117,21 @@ def test_named_operations_match_reference(golden, fam, case):
     op = getattr(ob.ops, name)
     s, cot, ln = _inputs(golden, case)
     g = lambda k: golden[f"{case}/{fam}/{k}"]  # noqa: E731
+    sens64, hv64, bw64 = _exact_second_order(fam, s, cot, ln, kw)
 
     sens = op.sensitivity(s, lengths=ln, **kw)
     assert tuple(sens) == op.sensitivity_fields
-    for k, t in sens.items():
-        np.testing.assert_allclose(t.cpu().numpy(), g(f"sens_{k}"), atol=1e-5)
+    for (k, t), e64 in zip(sens.items(), sens64):
+        _second_order_close(f"sens_{k}", t.cpu().numpy(), g(f"sens_{k}"), e64)
     bw = op.backward(s, grad_map=cot, lengths=ln, **kw)
     assert tuple(bw) == op.backward_fields
-    np.testing.assert_allclose(bw["pair_scores"].cpu().numpy(), g("bw_pair_scores"), atol=1e-5)
-    for k in op.parameter_fields:
+    _second_order_close("bw_pair_scores", bw["pair_scores"].cpu().numpy(), g("bw_pair_scores"), hv64)
+    for k, e64 in zip(op.parameter_fields, bw64):
         assert bw[k].shape == ()
-        np.testing.assert_allclose(bw[k].item(), g(f"bw_{k}"), atol=1e-4)
+        _second_order_close(f"bw_{k}", bw[k].item(), g(f"bw_{k}"), e64)
     # one field selected by name comes back bare; forward selects observables
     t = op.sensitivity(s, lengths=ln, output="temperature", **kw)
-    np.testing.assert_allclose(t.cpu().numpy(), g("sens_temperature"), atol=1e-5)
+    assert torch.equal(t, sens["temperature"])
     fw = op.forward(s, lengths=ln, output=("value", "map"), **kw)
     np.testing.assert_allclose(fw["value"].cpu().numpy(), g("value"), rtol=1e-5, atol=1e-5)
     np.testing.assert_allclose(fw["map"].cpu().numpy(), g("map"), atol=1e-5)
