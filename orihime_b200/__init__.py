@@ -12,7 +12,8 @@ operations ``ops.<family>.forward / backward / sensitivity``.
 from . import _lib as _lib
 from . import _ops as _ops
 from .nw import nw, nw_affine, nw_affine_entropy, nw_affine_value, nw_entropy, nw_value
-from .sv import sv, sv_affine, sv_affine_entropy, sv_affine_value, sv_entropy, sv_value
+from .sv import (sv, sv_affine, sv_affine_entropy, sv_affine_value, sv_entropy, sv_linear,
+                 sv_linear_entropy, sv_linear_value, sv_value)
 from .sw import sw, sw_affine, sw_affine_entropy, sw_affine_value, sw_entropy, sw_value
 from . import ops as ops
 

@@ -23,6 +23,7 @@ from typing import Callable, Optional, Sequence, Union
 
 import torch
 from torch import Tensor
+from torch.autograd.function import once_differentiable
 
 Param = Union[float, int, Tensor]
 
@@ -250,39 +251,198 @@ SV_AFFINE = Family(
 # autograd functions
 # ---------------------------------------------------------------------------
 
-def _param_grad(total: Tensor, like: Param) -> Optional[Tensor]:
-    if isinstance(like, Tensor) and like.requires_grad:
-        return total.reshape(like.shape).to(device=like.device, dtype=like.dtype)
+def _param_grad(total: Tensor, meta, needed: bool) -> Optional[Tensor]:
+    """dS/dtheta summed over the batch, shaped like the parameter tensor
+    (meta = its shape, dtype, device), or None for a float parameter."""
+    if needed and meta is not None:
+        shape, dtype, device = meta
+        return total.reshape(shape).to(device=device, dtype=dtype)
     return None
 
 
+def _param_meta(params):
+    return [(p.shape, p.dtype, p.device) if isinstance(p, Tensor) else None for p in params]
+
+
+# ---------------------------------------------------------------------------
+# autograd Functions (eager autograd and torch.func: vjp, jvp, jacrev, vmap)
+# ---------------------------------------------------------------------------
+# Each observable is one torch.autograd.Function in the setup_context form,
+# which torch.func can transform (the reference registers its observables the
+# same way, orihime/operator.py:1288-1570):
+# * vjp / jacrev: backward is written with torch ops and the native ops,
+#   whose vmap rules fold a mapped cotangent into the native batch;
+# * jvp: a forward-mode rule per observable -- value: <map, ds> + sum_k
+#   dS/dtheta_k dtheta_k; map: HVP(ds) + sum_k dP/dtheta_k dtheta_k;
+#   entropy: <dP/dT, ds> (its parameter directions are not available, as in
+#   the reference);
+# * vmap: the mapped dimension is folded into the native batch and the
+#   Function runs once over vmap_size * B pairs; a mapped scalar parameter is
+#   an error, with the native ops' message.
+# Eager calls run the value-dependent part of the input contract (lengths
+# range, temperature, numerical domain, -inf masks) before the Function, so
+# the mask normalisation is ordinary autograd.  Under a transform the inputs
+# may be wrapped tensors that cannot be inspected, so forward runs it on the
+# plain tensors and its -inf cells get zero derivatives (their sentinel is a
+# constant).  forward returns the normalised scores and the -inf mask as
+# extra, non-differentiable outputs: setup_context may save only inputs and
+# outputs.
+
+_PUBLIC_PARAM = {"gap": "gap_score", "gap_open": "gap_open_score", "gap_ext": "gap_extend_score",
+                 "temp": "temperature"}
+
+
+def _interpreters() -> tuple:
+    return tuple(torch._C._functorch.get_interpreter_stack() or ())
+
+
+def _transforms_active() -> bool:
+    return bool(_interpreters())
+
+
+def _vmap_active() -> bool:
+    vm = torch._C._functorch.TransformType.Vmap
+    return any(i.key() == vm for i in _interpreters())
+
+
+def _strip(t):
+    """t without its grad-tracking wrappers: the native ops read storage,
+    which those wrappers do not expose.  Batching wrappers stay; the native
+    ops' vmap rules fold them."""
+    if isinstance(t, Tensor):
+        f = torch._C._functorch
+        while f.is_gradtrackingtensor(t):
+            t = f.get_unwrapped(t)
+    return t
+
+
+def _no_forward_mode_under_vmap(op, observable: str) -> None:
+    if _vmap_active():
+        raise NotImplementedError(
+            f"{op.name}{observable} has no batched forward-mode rule: its jvp function runs once per "
+            "call and cannot take mapped tangents (torch.func.jacfwd, or vmap over jvp); use "
+            "torch.func.jacrev or vmap over vjp")
+
+
+def _entropy_direction_error(op, pname: str) -> NotImplementedError:
+    return NotImplementedError(
+        f"{op.name}_entropy is differentiable only w.r.t. its primary {op.primary_name} input in "
+        f"this release; the entropy gradient w.r.t. parameter {_PUBLIC_PARAM.get(pname, pname)} "
+        "(a second derivative involving temperature) is not available -- see "
+        "DERIVATIVE_COVERAGE.md. Detach the parameter or use finite differences.")
+
+
+def _checked(op, x: Tensor, params, lengths):
+    """The value-dependent part of the input contract on plain tensors:
+    lengths within the padded shape, the temperature, the FP32 numerical
+    domain and -inf masks.  Returns (normalised scores, the -inf cells or
+    None)."""
+    if lengths is not None:
+        lim = torch.tensor(x.shape[1:], device=lengths.device, dtype=torch.int32)
+        if not bool(((lengths >= 0) & (lengths <= lim)).all()):
+            raise RuntimeError("lengths entries must lie within the padded input shape")
+    xn = _validate_and_normalize(op.primary_name, x, params, op.params)
+    neg = torch.isneginf(x) if xn is not x else None
+    return (xn if xn.is_contiguous() else xn.contiguous()), neg
+
+
+def _fold_vmap(fn, info, in_dims, op, validate, lengths, scores, params):
+    """vmap rule shared by the observables: fold the mapped dimension of the
+    scores (and lengths) into the native batch, run fn once, unfold."""
+    for pname, d in zip(op.params, in_dims[4:]):
+        if d is not None:
+            raise RuntimeError(f"orihime::{op.name}_forward_t does not support mapping scalar argument "
+                               f"{pname!r}; keep scalar parameters unbatched")
+    V = info.batch_size
+    ld, sd = in_dims[2], in_dims[3]
+    s = scores.movedim(sd, 0) if sd is not None else scores.unsqueeze(0).expand(V, *scores.shape)
+    B = s.shape[1]
+    s = s.reshape(V * B, *s.shape[2:]).contiguous()
+    if lengths is not None:
+        ln = lengths.movedim(ld, 0) if ld is not None else lengths.unsqueeze(0).expand(V, *lengths.shape)
+        lengths = ln.reshape(V * B, 2).contiguous()
+    out = fn.apply(op, validate, lengths, s, *params)
+    out = tuple(o.reshape(V, B, *o.shape[1:]) for o in out)
+    return out, tuple(0 for _ in out)
+
+
+def _saved(ctx):
+    """(scores, lengths, -inf mask or None) saved by setup_context."""
+    saved = ctx.saved_tensors
+    scores = saved[0]
+    lengths = saved[1] if ctx.has_lengths else None
+    neg = saved[-1] if ctx.has_neg else None
+    return scores, lengths, neg
+
+
+def _save_inputs(ctx, inputs, output, nlead: int):
+    """Save the scores the native ops need (the input, or the normalised
+    copy forward returned), the lengths and the -inf mask, for backward and
+    for jvp; output[:nlead] are the observable's own outputs."""
+    op, validate, lengths, scores, *params = inputs
+    extra = output[nlead:]
+    if validate:
+        scores = extra[0]
+    neg = extra[1] if validate and len(extra) > 1 else None
+    ctx.op, ctx.validate = op, validate
+    ctx.vals = [_as_float(p) for p in params]
+    ctx.pmeta = _param_meta(params)
+    ctx.has_lengths, ctx.has_neg = lengths is not None, neg is not None
+    tensors = (scores,) + ((lengths,) if lengths is not None else ()) + ((neg,) if neg is not None else ())
+    return tensors, extra
+
+
 class _ValueFn(torch.autograd.Function):
-    @staticmethod
-    def forward(ctx, fam, lengths, scores, *params):
-        vals = [_as_float(p) for p in params]
-        needs_params = any(isinstance(p, Tensor) and p.requires_grad for p in params)
-        if needs_params:
-            # one forward + adjoint gives the value, the map and dS/dtheta
-            value, smap, *grads = fam.full(scores, *vals, lengths)
-        else:
-            value, smap = fam.forward(scores, *vals, lengths)
-            grads = None
-        ctx.fam, ctx.params = fam, params
-        ctx.save_for_backward(smap)
-        ctx.param_grads = grads
-        return value
+    """value S [B]; backward: cotangent x map, and cotangent . dS/dtheta."""
 
     @staticmethod
-    def backward(ctx, gv):
-        (smap,) = ctx.saved_tensors
-        gs = gv.view(-1, 1, 1) * smap if ctx.needs_input_grad[2] else None
-        out = [None, None, gs]
-        for k, p in enumerate(ctx.params):
-            g = None
-            if ctx.param_grads is not None and isinstance(p, Tensor) and p.requires_grad:
-                g = _param_grad((gv * ctx.param_grads[k]).sum(), p)
-            out.append(g)
+    def forward(op, validate, lengths, scores, *params):
+        neg = None
+        if validate:
+            scores, neg = _checked(op, scores, params, lengths)
+        vals = [_as_float(p) for p in params]
+        value, smap, *grads = op.fam.full(scores, *vals, lengths)
+        if neg is not None:
+            smap = smap.masked_fill(neg, 0.0)
+        return (value, smap, *grads)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        value, smap, *grads = output
+        ctx.mark_non_differentiable(smap, *grads)
+        ctx.save_for_backward(smap, *grads)
+        ctx.save_for_forward(smap, *grads)
+        ctx.pmeta = _param_meta(inputs[4:])
+        ctx.op = inputs[0]
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, gv, *_):
+        smap, *grads = ctx.saved_tensors
+        gs = gv.reshape(-1, 1, 1) * smap if ctx.needs_input_grad[3] else None
+        out = [None, None, None, gs]
+        for k, meta in enumerate(ctx.pmeta):
+            out.append(_param_grad((gv * grads[k]).sum(), meta, ctx.needs_input_grad[4 + k]))
         return tuple(out)
+
+    @staticmethod
+    def jvp(ctx, _op, _validate, _lengths, t_scores, *t_params):
+        _no_forward_mode_under_vmap(ctx.op, "_value")
+        smap, *grads = ctx.saved_tensors
+        t = None
+        if t_scores is not None:
+            t = (smap * t_scores).sum(dim=(1, 2))
+        for g, tp in zip(grads, t_params):
+            if tp is not None:
+                d = g * tp.reshape(())
+                t = d if t is None else t + d
+        if t is None:
+            t = torch.zeros_like(grads[0])
+        return (t, None, *(None for _ in grads))
+
+    @staticmethod
+    def vmap(info, in_dims, op, validate, lengths, scores, *params):
+        return _fold_vmap(_ValueFn, info, in_dims, op, validate, lengths, scores, params)
 
 
 # Checkpoint stride of the checkpointed value op: the forward keeps the DP
@@ -293,21 +453,23 @@ CHECKPOINT_EVERY = 4
 
 
 class _CheckpointedValueFn(torch.autograd.Function):
-    """value with a deferred adjoint (local families, gaps <= 0): forward
-    runs only the forward wavefront and keeps its sparse checkpoints in a
-    workspace; backward runs the checkpointed adjoint on them and scales the
-    map and dS/dtheta by the value's cotangent.  Nothing of size [B, L1, L2]
-    is kept between the two."""
+    """value with a deferred adjoint (local families, gaps <= 0, eager calls):
+    forward runs only the forward wavefront and keeps its sparse checkpoints
+    in a workspace; backward runs the checkpointed adjoint on them and scales
+    the map and dS/dtheta by the value's cotangent.  Nothing of size
+    [B, L1, L2] is kept between the two."""
 
     @staticmethod
     def forward(ctx, fam, lengths, ws_value, scores, *params):
         value, ws = ws_value
-        ctx.fam, ctx.params, ctx.lengths, ctx.ws = fam, params, lengths, ws
+        ctx.fam, ctx.lengths, ctx.ws = fam, lengths, ws
         ctx.vals = [_as_float(p) for p in params]
+        ctx.pmeta = _param_meta(params)
         ctx.save_for_backward(scores)
         return value
 
     @staticmethod
+    @once_differentiable
     def backward(ctx, gv):
         from . import _ops as ops_mod
 
@@ -316,18 +478,16 @@ class _CheckpointedValueFn(torch.autograd.Function):
                                               CHECKPOINT_EVERY, ctx.ws)
         gs = gv.view(-1, 1, 1) * smap if ctx.needs_input_grad[3] else None
         out = [None, None, None, gs]
-        for k, p in enumerate(ctx.params):
-            g = None
-            if isinstance(p, Tensor) and p.requires_grad:
-                g = _param_grad((gv * grads[k]).sum(), p)
-            out.append(g)
+        for k, meta in enumerate(ctx.pmeta):
+            out.append(_param_grad((gv * grads[k]).sum(), meta, ctx.needs_input_grad[4 + k]))
         return tuple(out)
 
 
 def _checkpointed_value(fam, lengths, scores, params):
     """The checkpointed value op, or None where it does not apply (another
-    family, a positive gap, under stream capture)."""
-    if fam.name not in ("sw", "sw_affine") or torch.cuda.is_current_stream_capturing():
+    family, a positive gap, a tensor off CUDA, under stream capture)."""
+    if (fam.name not in ("sw", "sw_affine") or not scores.is_cuda
+            or torch.cuda.is_current_stream_capturing()):
         return None
     from . import _ops as ops_mod
 
@@ -339,46 +499,139 @@ def _checkpointed_value(fam, lengths, scores, params):
 
 
 class _MapFn(torch.autograd.Function):
-    @staticmethod
-    def forward(ctx, fam, lengths, scores, *params):
-        vals = [_as_float(p) for p in params]
-        _, smap = fam.forward(scores, *vals, lengths)
-        ctx.fam, ctx.params, ctx.vals, ctx.lengths = fam, params, vals, lengths
-        ctx.save_for_backward(scores)
-        return smap
+    """map dS/dscores; backward: HVP of the cotangent and cotangent . dP/dtheta."""
 
     @staticmethod
-    def backward(ctx, gm):
-        (scores,) = ctx.saved_tensors
-        gm = gm.contiguous()
-        gs = ctx.fam.hvp(scores, gm, *ctx.vals, ctx.lengths) if ctx.needs_input_grad[2] else None
-        out = [None, None, gs]
-        for k, p in enumerate(ctx.params):
-            g = None
-            if isinstance(p, Tensor) and p.requires_grad:
-                field = ctx.fam.sens[k](scores, *ctx.vals, ctx.lengths)
-                g = _param_grad((gm * field).sum(), p)
-            out.append(g)
+    def forward(op, validate, lengths, scores, *params):
+        neg = None
+        if validate:
+            scores, neg = _checked(op, scores, params, lengths)
+        vals = [_as_float(p) for p in params]
+        _, smap = op.fam.forward(scores, *vals, lengths)
+        if neg is not None:
+            smap = smap.masked_fill(neg, 0.0)
+        # the normalised scores may be the input itself: return a view of it
+        extra = (scores.view_as(scores),) if validate else ()
+        if neg is not None:
+            extra += (neg,)
+        return (smap, *extra)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        tensors, extra = _save_inputs(ctx, inputs, output, 1)
+        if extra:
+            ctx.mark_non_differentiable(*extra)
+        ctx.save_for_backward(*tensors)
+        ctx.save_for_forward(*tensors)
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, gm, *_):
+        scores, lengths, neg = _saved(ctx)
+        fam, vals = ctx.op.fam, ctx.vals
+        sc = _strip(scores)
+        g = _strip(gm)
+        if neg is not None:
+            g = g.masked_fill(neg, 0.0)
+        g = g.contiguous()
+        gs = None
+        if ctx.needs_input_grad[3]:
+            gs = fam.hvp(sc, g, *vals, lengths)
+            if neg is not None:
+                gs = gs.masked_fill(neg, 0.0)
+        out = [None, None, None, gs]
+        for k, meta in enumerate(ctx.pmeta):
+            need = ctx.needs_input_grad[4 + k]
+            total = (g * fam.sens[k](sc, *vals, lengths)).sum() if need else None
+            out.append(_param_grad(total, meta, need))
         return tuple(out)
+
+    @staticmethod
+    def jvp(ctx, _op, _validate, _lengths, t_scores, *t_params):
+        _no_forward_mode_under_vmap(ctx.op, "")
+        scores, lengths, neg = _saved(ctx)
+        fam, vals = ctx.op.fam, ctx.vals
+        sc = _strip(scores)
+        t = None
+        if t_scores is not None:
+            d = _strip(t_scores)
+            if neg is not None:
+                d = d.masked_fill(neg, 0.0)
+            t = fam.hvp(sc, d.contiguous(), *vals, lengths)
+        for k, tp in enumerate(t_params):
+            if tp is not None:
+                d = fam.sens[k](sc, *vals, lengths) * _strip(tp).reshape(())
+                t = d if t is None else t + d
+        if t is None:
+            t = torch.zeros_like(sc)
+        elif neg is not None:
+            t = t.masked_fill(neg, 0.0)
+        return (t,) + (None,) * (1 + ctx.has_neg if ctx.validate else 0)
+
+    @staticmethod
+    def vmap(info, in_dims, op, validate, lengths, scores, *params):
+        return _fold_vmap(_MapFn, info, in_dims, op, validate, lengths, scores, params)
 
 
 class _EntropyFn(torch.autograd.Function):
-    @staticmethod
-    def forward(ctx, fam, lengths, scores, *params):
-        vals = [_as_float(p) for p in params]
-        grads = fam.grads(scores, *vals, lengths)
-        ctx.fam, ctx.vals, ctx.lengths, ctx.nparams = fam, vals, lengths, len(params)
-        ctx.save_for_backward(scores)
-        return grads[-1]
+    """entropy dS/dT [B]; backward: cotangent x dP/dT through the scores only
+    (a parameter direction raises, as in the reference)."""
 
     @staticmethod
-    def backward(ctx, ge):
-        (scores,) = ctx.saved_tensors
+    def forward(op, validate, lengths, scores, *params):
+        neg = None
+        if validate:
+            scores, neg = _checked(op, scores, params, lengths)
+        vals = [_as_float(p) for p in params]
+        ent = op.fam.grads(scores, *vals, lengths)[-1]
+        extra = (scores.view_as(scores),) if validate else ()
+        if neg is not None:
+            extra += (neg,)
+        return (ent, *extra)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        tensors, extra = _save_inputs(ctx, inputs, output, 1)
+        if extra:
+            ctx.mark_non_differentiable(*extra)
+        ctx.save_for_backward(*tensors)
+        ctx.save_for_forward(*tensors)
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, ge, *_):
+        for k, pname in enumerate(ctx.op.params):
+            if ctx.needs_input_grad[4 + k] and ctx.pmeta[k] is not None:
+                raise _entropy_direction_error(ctx.op, pname)
+        scores, lengths, neg = _saved(ctx)
         gs = None
-        if ctx.needs_input_grad[2]:
-            field = ctx.fam.sens[-1](scores, *ctx.vals, ctx.lengths)
-            gs = ge.view(-1, 1, 1) * field
-        return (None, None, gs) + (None,) * ctx.nparams
+        if ctx.needs_input_grad[3]:
+            field = ctx.op.fam.sens[-1](_strip(scores), *ctx.vals, lengths)
+            gs = _strip(ge).reshape(-1, 1, 1) * field
+            if neg is not None:
+                gs = gs.masked_fill(neg, 0.0)
+        return (None, None, None, gs) + (None,) * len(ctx.pmeta)
+
+    @staticmethod
+    def jvp(ctx, _op, _validate, _lengths, t_scores, *t_params):
+        for pname, tp in zip(ctx.op.params, t_params):
+            if tp is not None:
+                raise _entropy_direction_error(ctx.op, pname)
+        _no_forward_mode_under_vmap(ctx.op, "_entropy")
+        scores, lengths, neg = _saved(ctx)
+        sc = _strip(scores)
+        if t_scores is None:
+            t = sc.new_zeros(sc.shape[0])
+        else:
+            d = _strip(t_scores)
+            if neg is not None:
+                d = d.masked_fill(neg, 0.0)
+            t = (ctx.op.fam.sens[-1](sc, *ctx.vals, lengths) * d).sum(dim=(1, 2))
+        return (t,) + (None,) * (1 + ctx.has_neg if ctx.validate else 0)
+
+    @staticmethod
+    def vmap(info, in_dims, op, validate, lengths, scores, *params):
+        return _fold_vmap(_EntropyFn, info, in_dims, op, validate, lengths, scores, params)
 
 
 # ---------------------------------------------------------------------------
@@ -386,8 +639,8 @@ class _EntropyFn(torch.autograd.Function):
 # ---------------------------------------------------------------------------
 
 class Operator:
-    """One soft alignment family (Smith-Waterman or Needleman-Wunsch) with map /
-    value / entropy observables."""
+    """One soft alignment family (Smith-Waterman, Needleman-Wunsch or
+    Saigo-Vert) with map / value / entropy observables."""
 
     def __init__(self, fam: Family, primary_name: str = "pair_scores"):
         self.fam = fam
@@ -396,7 +649,10 @@ class Operator:
         self.primary_name = primary_name
 
     # -- input contract (orihime/operator.py:1948-2074, :2178-2206) --
-    def _prepare(self, primary, params, lengths, mask, dtype):
+    def _prepare_shapes(self, primary, params, lengths, mask, dtype):
+        """The checks that read no tensor values (types, shapes, dtypes,
+        devices) and the mask and dtype conversions: safe on tensors that a
+        torch.func transform wraps."""
         name = self.primary_name
         if not isinstance(primary, Tensor):
             raise TypeError(f"{name} must be a tensor")
@@ -448,22 +704,27 @@ class Operator:
                                  f"{lengths.device} and {primary.device}")
             if not lengths.is_contiguous():
                 raise ValueError("lengths must be contiguous")
-            lim = torch.tensor(primary.shape[1:], device=lengths.device, dtype=torch.int32)
-            if not bool(((lengths >= 0) & (lengths <= lim)).all()):
-                raise RuntimeError("lengths entries must lie within the padded input shape")
-        primary = _validate_and_normalize(name, primary, params, self.params)
-        if not primary.is_contiguous():
-            primary = primary.contiguous()
+        return primary, params, lengths
+
+    def _prepare(self, primary, params, lengths, mask, dtype):
+        primary, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
+        primary, _ = _checked(self, primary, params, lengths)
         if lengths is None:
             B, L1, L2 = primary.shape
             lengths = torch.tensor([[L1, L2]] * B, dtype=torch.int32, device=primary.device)
         return primary, params, lengths
 
     def __call__(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:
+        if _transforms_active():
+            x, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
+            return _MapFn.apply(self, True, lengths, x, *params)[0]
         x, params, lengths = self._prepare(primary, params, lengths, mask, dtype)
-        return _MapFn.apply(self.fam, lengths, x, *params)
+        return _MapFn.apply(self, False, lengths, x, *params)[0]
 
     def value(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:
+        if _transforms_active():
+            x, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
+            return _ValueFn.apply(self, True, lengths, x, *params)[0]
         x, params, lengths = self._prepare(primary, params, lengths, mask, dtype)
         needs_grad = torch.is_grad_enabled() and (
             x.requires_grad or any(isinstance(p, Tensor) and p.requires_grad for p in params))
@@ -474,11 +735,14 @@ class Operator:
         v = _checkpointed_value(self.fam, lengths, x, params)
         if v is not None:
             return v
-        return _ValueFn.apply(self.fam, lengths, x, *params)
+        return _ValueFn.apply(self, False, lengths, x, *params)[0]
 
     def entropy(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:
+        if _transforms_active():
+            x, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
+            return _EntropyFn.apply(self, True, lengths, x, *params)[0]
         x, params, lengths = self._prepare(primary, params, lengths, mask, dtype)
-        return _EntropyFn.apply(self.fam, lengths, x, *params)
+        return _EntropyFn.apply(self, False, lengths, x, *params)[0]
 
     # -- named ops tier (orihime/operator.py:2312-2400) --
     def vjp(self, primary, *params, grad_map, wrt, lengths=None, mask=None, dtype=None) -> Tensor:

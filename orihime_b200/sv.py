@@ -63,3 +63,9 @@ def sv_affine_entropy(pair_scores: Tensor, *, gap_open_score=0.0, gap_extend_sco
 
 
 __all__ = ["sv", "sv_value", "sv_entropy", "sv_affine", "sv_affine_value", "sv_affine_entropy"]
+
+
+# The linear-gap family's kernel name, kept as aliases as in orihime/sv.py:117-122.
+sv_linear = sv
+sv_linear_value = sv_value
+sv_linear_entropy = sv_entropy
