@@ -638,6 +638,10 @@ class _EntropyFn(torch.autograd.Function):
 # the operator
 # ---------------------------------------------------------------------------
 
+# Operator of each family by name (the compile path's ops look them up).
+OPERATORS: dict = {}
+
+
 class Operator:
     """One soft alignment family (Smith-Waterman, Needleman-Wunsch or
     Saigo-Vert) with map / value / entropy observables."""
@@ -647,6 +651,7 @@ class Operator:
         self.name = fam.name
         self.params = fam.params
         self.primary_name = primary_name
+        OPERATORS[fam.name] = self
 
     # -- input contract (orihime/operator.py:1948-2074, :2178-2206) --
     def _prepare_shapes(self, primary, params, lengths, mask, dtype):
@@ -714,7 +719,16 @@ class Operator:
             lengths = torch.tensor([[L1, L2]] * B, dtype=torch.int32, device=primary.device)
         return primary, params, lengths
 
+    def _compiled(self, kind, primary, params, lengths, mask, dtype) -> Tensor:
+        """While Dynamo traces: the observable as one opaque op (_pt2)."""
+        from . import _pt2
+
+        x, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
+        return _pt2.observable(kind, self, x, lengths, params)
+
     def __call__(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:
+        if torch.compiler.is_compiling():
+            return self._compiled("map", primary, params, lengths, mask, dtype)
         if _transforms_active():
             x, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
             return _MapFn.apply(self, True, lengths, x, *params)[0]
@@ -722,6 +736,8 @@ class Operator:
         return _MapFn.apply(self, False, lengths, x, *params)[0]
 
     def value(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:
+        if torch.compiler.is_compiling():
+            return self._compiled("value", primary, params, lengths, mask, dtype)
         if _transforms_active():
             x, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
             return _ValueFn.apply(self, True, lengths, x, *params)[0]
@@ -738,6 +754,8 @@ class Operator:
         return _ValueFn.apply(self, False, lengths, x, *params)[0]
 
     def entropy(self, primary, *params, lengths=None, mask=None, dtype=None) -> Tensor:
+        if torch.compiler.is_compiling():
+            return self._compiled("entropy", primary, params, lengths, mask, dtype)
         if _transforms_active():
             x, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
             return _EntropyFn.apply(self, True, lengths, x, *params)[0]
