@@ -17,6 +17,7 @@ from .sv import (sv, sv_affine, sv_affine_entropy, sv_affine_value, sv_entropy, 
 from .sw import sw, sw_affine, sw_affine_entropy, sw_affine_value, sw_entropy, sw_value
 from . import ops as ops
 from . import _pt2 as _pt2
+from . import raw as raw
 
 __version__ = "0.1.0"
 
