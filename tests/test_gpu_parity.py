@@ -3,7 +3,7 @@
 The oracle's float restatement reproduces the reference CPU kernels bit for
 bit ("ref32"); its double instantiation is the truth ("fp64").
 
-Parity bar (north star): value relative error <= 1e-5 against ref32.  For the
+Parity bar: value relative error <= 1e-5 against ref32.  For the
 marginal map the bar is absolute error <= 1e-5, measured against the FP64
 truth: on long pairs an FP32 forward-backward (the reference included) drifts
 further than that from the truth, so the map must be within
