@@ -247,3 +247,7 @@ def check_masked_and_ragged(name, device):
         (ge,) = torch.autograd.grad(f(xe), (xe,), grad_outputs=cot)
         _close(g, ge)
         assert bool((g[mask] == 0).all()) and bool((ge[mask] == 0).all())
+        # vmap over the lengths (the scores unmapped), an empty pair included
+        lns = torch.tensor([[[3, 3], [2, 3]], [[3, 2], [0, 3]]], dtype=torch.int32, device=device)
+        got = torch.vmap(lambda l: fn(x, lengths=l, **kw))(lns)
+        _close(got, torch.stack([fn(x, lengths=l.contiguous(), **kw) for l in lns]))
