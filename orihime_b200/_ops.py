@@ -21,6 +21,8 @@ read ``lengths`` on the host to range-check them.
 
 from __future__ import annotations
 
+from typing import Optional
+
 import torch
 
 from . import _lib
@@ -154,17 +156,17 @@ def _capturing() -> bool:
     return torch.cuda.is_available() and torch.cuda.is_current_stream_capturing()
 
 
-def resolve_lengths(lengths, B: int, L1: int, L2: int, device) -> torch.Tensor:
-    """Default or validate [B, 2] int32 lengths (validate_sw_affine_lengths_cuda).
+def resolve_lengths(lengths, B: int, L1: int, L2: int, device) -> Optional[torch.Tensor]:
+    """Validate [B, 2] int32 lengths (validate_sw_affine_lengths_cuda), or
+    None for full lengths: the C ABI takes a null lengths pointer as the
+    padded shape, so no default tensor is copied to the device.
 
     The value range check reads the lengths on the host, as the reference
     does (same messages).  While a CUDA graph is being captured that read is
     not allowed: the kernels then check the range on the device, clamp, and
     return NaN for the pairs concerned (status bit SWB_STATUS_BAD_LENGTHS)."""
     if lengths is None:
-        if _capturing():   # torch.tensor from a host list would copy host -> device
-            return torch.tensor([L1, L2], dtype=torch.int32).to(device).expand(B, 2).contiguous()
-        return torch.tensor([[L1, L2]] * B, dtype=torch.int32, device=device).reshape(B, 2)
+        return None
     if not lengths.is_cuda:
         raise RuntimeError("lengths must be a CUDA tensor")
     if not lengths.is_contiguous():

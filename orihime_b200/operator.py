@@ -712,11 +712,10 @@ class Operator:
         return primary, params, lengths
 
     def _prepare(self, primary, params, lengths, mask, dtype):
+        """The whole input contract.  lengths stays None when the caller gave
+        none: the ops take that as full lengths, with no host round trip."""
         primary, params, lengths = self._prepare_shapes(primary, params, lengths, mask, dtype)
         primary, _ = _checked(self, primary, params, lengths)
-        if lengths is None:
-            B, L1, L2 = primary.shape
-            lengths = torch.tensor([[L1, L2]] * B, dtype=torch.int32, device=primary.device)
         return primary, params, lengths
 
     def _compiled(self, kind, primary, params, lengths, mask, dtype) -> Tensor:
