@@ -80,9 +80,10 @@ typedef struct swb_options {
 #define SWB_DOMAIN_LINEAR 2
 
 /* Columns per lane the padded entry points use when swb_options does not
- * set one: 8 for the local families (family 1 linear gap, 3 affine gaps) in
- * the linear domain on batches with L2max >= 256, else 4 (families 2, 4, 5:
- * the global and Saigo-Vert models, always 4).  Results depend on it bit for
+ * set one: for the local families (family 1 linear gap, 3 affine gaps) in
+ * the linear domain, 8 on batches with L2max >= 256, 2 on batches with
+ * L2max <= 64, else 4; in the log domain and for families 2, 4, 5 (the
+ * global and Saigo-Vert models) always 4.  Results depend on it bit for
  * bit (the band decomposition orders each pair's sums), so a packed plan
  * built with the same value reproduces a padded call exactly.  No reference
  * counterpart. */
@@ -430,7 +431,7 @@ int swb_scan_scores(const float* x, int B, long long per_item, float limit, floa
  * adjoint recomputes the chunks in between from the nearest checkpoint.
  * The local families in the linear domain only: gaps must be <= 0, else
  * SWB_ERR_ARG.  Columns per lane as swb_cols_per_lane gives for L2max (8 at
- * L2max >= 256, else 4).  Workspace from
+ * L2max >= 256, 2 at L2max <= 64, else 4).  Workspace from
  * swb_*_checkpoint_workspace_bytes(B, L1max, L2max, ck_every).
  */
 size_t swb_sw_affine_checkpoint_workspace_bytes(int B, int L1max, int L2max, int ck_every);

@@ -56,11 +56,16 @@ bool lin_eligible(float go, float ge, float T, const swb_options* opt) {
   const double xo = (double)go * (double)k, xe = NS == 3 ? (double)ge * (double)k : 0.0;
   return xo <= 0.0 && xe <= 0.0;
 }
-// Default columns per lane of the padded entry points: 8 for the
-// linear-domain kernels on batches at least 256 columns wide (half the bands,
-// each step's fixed work spread over twice the cells: measured faster from
-// 64 x 1024^2 to 4 x 4096^2), else 4.
-int default_r(long long L2m, bool lin) { return lin && L2m >= 256 ? 8 : kDefaultR; }
+// Default columns per lane of the padded entry points, for the linear-domain
+// kernels: 8 on batches at least 256 columns wide (half the bands, each
+// step's fixed work spread over twice the cells: measured faster from
+// 64 x 1024^2 to 4 x 4096^2); 2 on batches at most 64 columns wide (one band
+// with every lane live: forward + adjoint of 1 x 64^2 in 84 us against 105 at
+// 4, 128 x 64^2 in 87 against 106); else 4.  The log domain always takes 4.
+int default_r(long long L2m, bool lin) {
+  if (!lin) return kDefaultR;
+  return L2m >= 256 ? 8 : (L2m <= 64 ? 2 : kDefaultR);
+}
 int pick_r(const swb_options* opt, long long L2m, bool lin) {
   return (opt && opt->cols_per_lane) ? opt->cols_per_lane : default_r(L2m, lin);
 }
@@ -402,8 +407,9 @@ int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2
     return launch<NS, R, G>(a, l, (long long)B * l.nb, 0, false, ws, ws_bytes, stream, nullptr, true);
   };
   if constexpr (G == 0) {
-    if (default_r(L2m, lin_eligible<NS, G>(go, ge, T, nullptr)) == 8)
-      return run(std::integral_constant<int, 8>{});
+    const int r = default_r(L2m, lin_eligible<NS, G>(go, ge, T, nullptr));
+    if (r == 8) return run(std::integral_constant<int, 8>{});
+    if (r == 2) return run(std::integral_constant<int, 2>{});
   }
   return run(std::integral_constant<int, kDefaultR>{});
 }
@@ -411,7 +417,8 @@ int launch_value(const float* scores, const int* lengths, int B, int L1m, int L2
 template <int NS, int G = 0>
 size_t value_workspace(long long B, long long L1m, long long L2m) {
   size_t n = value_layout<NS, G, kDefaultR>(B, L1m, L2m).total;
-  if constexpr (G == 0) n = std::max(n, value_layout<NS, G, 8>(B, L1m, L2m).total);
+  if constexpr (G == 0)
+    n = std::max({n, value_layout<NS, G, 8>(B, L1m, L2m).total, value_layout<NS, G, 2>(B, L1m, L2m).total});
   return n;
 }
 
@@ -815,8 +822,11 @@ int ck_adjoint_r(const float* scores, const int* lengths, int B, int L1m, int L2
 template <int NS>
 int ck_forward(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
                float T, int kc, float* value, void* ws, size_t ws_bytes, void* stream_v) {
-  if (default_r(L2m, true) == 8)
+  const int r = default_r(L2m, true);
+  if (r == 8)
     return ck_forward_r<NS, 8>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, ws, ws_bytes, stream_v);
+  if (r == 2)
+    return ck_forward_r<NS, 2>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, ws, ws_bytes, stream_v);
   return ck_forward_r<NS, 4>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, ws, ws_bytes, stream_v);
 }
 
@@ -824,8 +834,12 @@ template <int NS>
 int ck_adjoint(const float* scores, const int* lengths, int B, int L1m, int L2m, float go, float ge,
                float T, int kc, float* value, float* map, float* g_open, float* g_ext, float* g_T,
                void* ws, size_t ws_bytes, void* stream_v) {
-  if (default_r(L2m, true) == 8)
+  const int r = default_r(L2m, true);
+  if (r == 8)
     return ck_adjoint_r<NS, 8>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, map, g_open, g_ext,
+                               g_T, ws, ws_bytes, stream_v);
+  if (r == 2)
+    return ck_adjoint_r<NS, 2>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, map, g_open, g_ext,
                                g_T, ws, ws_bytes, stream_v);
   return ck_adjoint_r<NS, 4>(scores, lengths, B, L1m, L2m, go, ge, T, kc, value, map, g_open, g_ext,
                              g_T, ws, ws_bytes, stream_v);
@@ -833,8 +847,9 @@ int ck_adjoint(const float* scores, const int* lengths, int B, int L1m, int L2m,
 
 template <int NS>
 size_t ck_workspace(long long B, long long L1m, long long L2m, int kc) {
-  return default_r(L2m, true) == 8 ? ck_layout<NS, 8>(B, L1m, L2m, kc).total
-                                   : ck_layout<NS, 4>(B, L1m, L2m, kc).total;
+  const int r = default_r(L2m, true);
+  return r == 8 ? ck_layout<NS, 8>(B, L1m, L2m, kc).total
+                : (r == 2 ? ck_layout<NS, 2>(B, L1m, L2m, kc).total : ck_layout<NS, 4>(B, L1m, L2m, kc).total);
 }
 
 }  // namespace
