@@ -140,9 +140,13 @@ __device__ __forceinline__ void zero_chunk_rows(const Pair& pr, int kc, int col0
 // (LREC: CK4 groups of [lane][4]) and adjoint shared-memory floats per lane
 // per step (FW).  A band's checkpoint region holds ceil(nchunks / ck_every)
 // records, then one float per chunk: the chunk's largest normalised alpha
-// frame (the adjoint's quiet-chunk test).
+// frame (the adjoint's quiet-chunk test).  An affine record keeps M and I of
+// the lane's row but not D: D is rebuilt from M, the left lane's values and
+// the frames with the forward's own operations (lck_unpack), bit for bit, so
+// a record is 24 floats per lane instead of 32 at 8 columns per lane.
 template <int NS, int R> struct LDims {
-  static constexpr int CKV = NS * R + NS + 3;          // raw row, left values, e, n, nl
+  static constexpr int NSTORE = NS == 3 ? 2 : 1;         // states stored per column
+  static constexpr int CKV = NSTORE * R + NS + 3;        // raw row, left values, e, n, nl
   static constexpr int CKF = (CKV + 3) / 4 * 4;
   static constexpr int CK4 = CKF / 4;
   static constexpr int LREC = CKF * 32;
@@ -186,16 +190,17 @@ __device__ __forceinline__ void lstate_zero(LState<NS, R>& s) {
 template <int NS, int R>
 __device__ __forceinline__ void lck_store(float* rec, int lane, const LState<NS, R>& s) {
   using L = LDims<NS, R>;
+  constexpr int V = L::NSTORE * R;   // where the left values start
   float x[L::CKF];
 #pragma unroll
-  for (int q = 0; q < NS; ++q) {
+  for (int q = 0; q < L::NSTORE; ++q)
 #pragma unroll
     for (int c = 0; c < R; ++c) x[q * R + c] = s.v[q][c];
-    x[NS * R + q] = s.lv[q];
-  }
-  x[NS * R + NS] = __int_as_float(s.e);
-  x[NS * R + NS + 1] = __int_as_float(s.n);
-  x[NS * R + NS + 2] = __int_as_float(s.nl);
+#pragma unroll
+  for (int q = 0; q < NS; ++q) x[V + q] = s.lv[q];
+  x[V + NS] = __int_as_float(s.e);
+  x[V + NS + 1] = __int_as_float(s.n);
+  x[V + NS + 2] = __int_as_float(s.nl);
 #pragma unroll
   for (int f = L::CKV; f < L::CKF; ++f) x[f] = 0.f;
 #pragma unroll
@@ -213,17 +218,37 @@ __device__ __forceinline__ void lck_load(const float* rec, int lane, float (&x)[
   }
 }
 
+// Restores the lane state of a record.  Affine: D is rebuilt as lcells
+// computed it for that row -- column 0 from the left lane's values (in its
+// frame nl, converted to the row's frame e), column c > 0 from column c - 1
+// of M and D, then zero past the pair -- with the same operations in the
+// same order, so the restored state equals the forward's bit for bit.
 template <int NS, int R>
-__device__ __forceinline__ void lck_unpack(const float (&x)[LDims<NS, R>::CKF], LState<NS, R>& s) {
+__device__ __forceinline__ void lck_unpack(const float (&x)[LDims<NS, R>::CKF], LState<NS, R>& s,
+                                           float gO, float gE, int nlive, bool has_dead) {
+  using L = LDims<NS, R>;
+  constexpr int V = L::NSTORE * R;
 #pragma unroll
-  for (int q = 0; q < NS; ++q) {
+  for (int q = 0; q < L::NSTORE; ++q)
 #pragma unroll
     for (int c = 0; c < R; ++c) s.v[q][c] = x[q * R + c];
-    s.lv[q] = x[NS * R + q];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) s.lv[q] = x[V + q];
+  s.e = __float_as_int(x[V + NS]);
+  s.n = __float_as_int(x[V + NS + 1]);
+  s.nl = __float_as_int(x[V + NS + 2]);
+  if constexpr (NS == 3) {
+    const float fL = p2i(s.nl - s.e);
+    const float gOl = gO * fL, gEl = gE * fL;
+#pragma unroll
+    for (int c = 0; c < R; ++c)
+      s.v[2][c] = c == 0 ? fmaf(gEl, s.lv[2], gOl * s.lv[0]) : fmaf(gE, s.v[2][c - 1], gO * s.v[0][c - 1]);
+    if (has_dead) {
+#pragma unroll
+      for (int c = 0; c < R; ++c)
+        if (c >= nlive) s.v[2][c] = 0.f;
+    }
   }
-  s.e = __float_as_int(x[NS * R + NS]);
-  s.n = __float_as_int(x[NS * R + NS + 1]);
-  s.nl = __float_as_int(x[NS * R + NS + 2]);
   lstate_sums(s);
   const float f = p2i(s.e - s.n);
 #pragma unroll
@@ -879,7 +904,7 @@ __device__ void lbwd_band(const Args& a, const LParams& lp, const Place& w, int 
     {
       float ckr[CKF];
       lck_load<NS, R>(stg_ck, lane, ckr);
-      lck_unpack<NS, R>(ckr, st);
+      lck_unpack<NS, R>(ckr, st, gO, gE, nlive, has_dead);
     }
     if (lane < C_STEPS) s_eb[lane] = make_float4(ebr[0], ebr[1], ebr[NEF > 2 ? 2 : 0], ebr[NEF > 3 ? 3 : 0]);
     __syncwarp();   // the staged checkpoint is read before the next chunk's copy is issued
