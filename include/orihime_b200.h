@@ -427,7 +427,7 @@ int swb_scan_scores(const float* x, int B, long long per_item, float limit, floa
  * lengths and parameters, runs the checkpointed adjoint: the marginal map
  * and dS/dparameters (and the value again).  It can run more than once.
  * ck_every in [1, 16]: 1 keeps a checkpoint per chunk (the fastest
- * adjoint); 4 keeps about 1.2 bytes per cell of a large padded batch, and the
+ * adjoint); 4 keeps about 0.93 bytes per cell of a large padded batch, and the
  * adjoint recomputes the chunks in between from the nearest checkpoint.
  * The local families in the linear domain only: gaps must be <= 0, else
  * SWB_ERR_ARG.  Columns per lane as swb_cols_per_lane gives for L2max (8 at

@@ -446,9 +446,10 @@ class _ValueFn(torch.autograd.Function):
 
 
 # Checkpoint stride of the checkpointed value op: the forward keeps the DP
-# state of every CHECKPOINT_EVERY-th chunk of 4 wavefront steps (about 5 / k
+# state of every CHECKPOINT_EVERY-th chunk of 4 wavefront steps (about 3.7 / k
 # bytes per computed cell at k = CHECKPOINT_EVERY), and the adjoint recomputes
-# the chunks in between.  4 keeps ~1.3 B/cell, a third of the map's 4 B/cell.
+# the chunks in between.  4 keeps ~0.93 B/cell, under a quarter of the map's
+# 4 B/cell.
 CHECKPOINT_EVERY = 4
 
 
