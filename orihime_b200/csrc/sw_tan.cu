@@ -68,8 +68,13 @@ __device__ __forceinline__ TConst tconst(float go, float ge, float T) {
 // and step (affine: M, I, D, their tangents, the scaled score and e; linear:
 // A, A', the emission part E (A_diag + 1) and its tangent, the scaled score
 // and e; then the two frames).
+// An affine record keeps M, I and their tangents but not D and D': restoring
+// it rebuilds them from M, M', the left lane's values and tangents and the
+// frames with tcells' own operations, bit for bit (28 floats per lane at 4
+// columns per lane instead of 36).
 template <int NS, int R> struct TDims {
-  static constexpr int CKV = 2 * NS * R + 2 * NS + 3;
+  static constexpr int NSTORE = NS == 3 ? 2 : 1;   // states stored per column
+  static constexpr int CKV = 2 * NSTORE * R + 2 * NS + 3;
   static constexpr int CKF = (CKV + 3) / 4 * 4;
   static constexpr int CK4 = CKF / 4;
   static constexpr int LREC = CKF * 32;
@@ -113,17 +118,20 @@ __device__ __forceinline__ void tstate_zero(TState<NS, R>& s) {
 template <int NS, int R>
 __device__ __forceinline__ void tck_store(float* rec, int lane, const TState<NS, R>& s) {
   using D = TDims<NS, R>;
+  constexpr int K = D::NSTORE, V = 2 * K * R;   // V: where the left column starts
   float x[D::CKF];
 #pragma unroll
-  for (int q = 0; q < NS; ++q) {
+  for (int q = 0; q < K; ++q)
 #pragma unroll
-    for (int c = 0; c < R; ++c) { x[q * R + c] = s.v[q][c]; x[(NS + q) * R + c] = s.w[q][c]; }
-    x[2 * NS * R + q] = s.lv[q];
-    x[2 * NS * R + NS + q] = s.lw[q];
+    for (int c = 0; c < R; ++c) { x[q * R + c] = s.v[q][c]; x[(K + q) * R + c] = s.w[q][c]; }
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    x[V + q] = s.lv[q];
+    x[V + NS + q] = s.lw[q];
   }
-  x[2 * NS * R + 2 * NS] = __int_as_float(s.e);
-  x[2 * NS * R + 2 * NS + 1] = __int_as_float(s.n);
-  x[2 * NS * R + 2 * NS + 2] = __int_as_float(s.nl);
+  x[V + 2 * NS] = __int_as_float(s.e);
+  x[V + 2 * NS + 1] = __int_as_float(s.n);
+  x[V + 2 * NS + 2] = __int_as_float(s.nl);
 #pragma unroll
   for (int f = D::CKV; f < D::CKF; ++f) x[f] = 0.f;
 #pragma unroll
@@ -131,9 +139,15 @@ __device__ __forceinline__ void tck_store(float* rec, int lane, const TState<NS,
     reinterpret_cast<float4*>(rec + g * 128)[lane] = make_float4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
 }
 
+// Restores a record.  Affine: D and D' are rebuilt as tcells computed them
+// for that row (column 0 from the left lane's values and tangents converted
+// to the row's frame, column c > 0 from column c - 1 of M, D and their
+// tangents, zero past the pair), with the same operations in the same order.
 template <int NS, int R>
-__device__ __forceinline__ void tck_restore(const float* rec, int lane, TState<NS, R>& s) {
+__device__ __forceinline__ void tck_restore(const float* rec, int lane, TState<NS, R>& s, float gO,
+                                            float gE, const TConst& tc, int nlive, bool has_dead) {
   using D = TDims<NS, R>;
+  constexpr int K = D::NSTORE, V = 2 * K * R;
   float x[D::CKF];
 #pragma unroll
   for (int g = 0; g < D::CK4; ++g) {
@@ -141,15 +155,37 @@ __device__ __forceinline__ void tck_restore(const float* rec, int lane, TState<N
     x[4 * g] = y.x; x[4 * g + 1] = y.y; x[4 * g + 2] = y.z; x[4 * g + 3] = y.w;
   }
 #pragma unroll
-  for (int q = 0; q < NS; ++q) {
+  for (int q = 0; q < K; ++q)
 #pragma unroll
-    for (int c = 0; c < R; ++c) { s.v[q][c] = x[q * R + c]; s.w[q][c] = x[(NS + q) * R + c]; }
-    s.lv[q] = x[2 * NS * R + q];
-    s.lw[q] = x[2 * NS * R + NS + q];
+    for (int c = 0; c < R; ++c) { s.v[q][c] = x[q * R + c]; s.w[q][c] = x[(K + q) * R + c]; }
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    s.lv[q] = x[V + q];
+    s.lw[q] = x[V + NS + q];
   }
-  s.e = __float_as_int(x[2 * NS * R + 2 * NS]);
-  s.n = __float_as_int(x[2 * NS * R + 2 * NS + 1]);
-  s.nl = __float_as_int(x[2 * NS * R + 2 * NS + 2]);
+  s.e = __float_as_int(x[V + 2 * NS]);
+  s.n = __float_as_int(x[V + 2 * NS + 1]);
+  s.nl = __float_as_int(x[V + 2 * NS + 2]);
+  if constexpr (NS == 3) {
+    const float fL = p2i(s.nl - s.e);
+    const float gOl = gO * fL, gEl = gE * fL;
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      if (c == 0) {
+        s.v[2][c] = fmaf(gEl, s.lv[2], gOl * s.lv[0]);
+        s.w[2][c] = fmaf(gEl, fmaf(tc.gEd, s.lv[2], s.lw[2]), gOl * fmaf(tc.gOd, s.lv[0], s.lw[0]));
+      } else {
+        s.v[2][c] = fmaf(gE, s.v[2][c - 1], gO * s.v[0][c - 1]);
+        s.w[2][c] = fmaf(gE, fmaf(tc.gEd, s.v[2][c - 1], s.w[2][c - 1]),
+                         gO * fmaf(tc.gOd, s.v[0][c - 1], s.w[0][c - 1]));
+      }
+    }
+    if (has_dead) {
+#pragma unroll
+      for (int c = 0; c < R; ++c)
+        if (c >= nlive) { s.v[2][c] = 0.f; s.w[2][c] = 0.f; }
+    }
+  }
   tstate_sums(s);
   const float f = p2i(s.e - s.n);
 #pragma unroll
@@ -633,7 +669,7 @@ __device__ void ltbwd_band(const Args& a, const LParams& lp, const TConst& tc, c
     // ---- restore and recompute the chunk (values and tangents) ----
     {
       TState<NS, R> st;
-      tck_restore<NS, R>(ck + (size_t)kc * D::LREC, lane, st);
+      tck_restore<NS, R>(ck + (size_t)kc * D::LREC, lane, st, gO, gE, tc, nlive, has_dead);
 #pragma unroll
       for (int cu = 0; cu < C_STEPS; ++cu) {
         const int i = t0 + cu - lane + 1;
