@@ -60,8 +60,9 @@ def shard_of(world: int, rank: int, pairs: int = NPAIRS):
 
 
 def make_scores(torch, lengths, offsets, seed, device, index=None):
-    """Packed C2-generator scores, built on the device pair by pair; pair b
-    is seeded by its index in the whole job (`index[b]`, default b)."""
+    """Packed scores 3 <e_i, f_j> / sqrt(64) (e, f ~ N(0, 1) in 64 dimensions),
+    built on the device pair by pair; pair b is seeded by its index in the
+    whole job (`index[b]`, default b)."""
     from orihime_b200 import ragged
 
     flat = torch.zeros(int(offsets[-1]), dtype=torch.float32, device=device)
@@ -307,7 +308,7 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"ragged C3: {NPAIRS} affine pairs, N,M log-uniform "
+            "config": {"workload": f"ragged batch: {NPAIRS} affine pairs, N,M log-uniform "
                                    f"[{LMIN},{LMAX}], go {GO} ge {GE} T {T}", "sample": sample},
             "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": kind,
                              "sample": sample},
@@ -910,7 +911,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"ragged C3: {args.pairs * world} affine pairs, N,M log-uniform "
+                "config": {"workload": f"ragged batch: {args.pairs * world} affine pairs, N,M log-uniform "
                                        f"[{LMIN},{LMAX}] (seed 3), scores 3<e,f>/sqrt(64)"
                                        + (f", LPT-sharded over {world} GPUs" if world > 1 else ""),
                            "cells": all_cells, "cells_rank0": cells,

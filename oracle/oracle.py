@@ -1,4 +1,4 @@
-"""TEST INFRASTRUCTURE ONLY: the CPU checker for the soft Smith-Waterman path.
+"""TEST INFRASTRUCTURE ONLY: the CPU oracle for the soft Smith-Waterman path.
 
 Two libraries sit behind this module, both built by ``oracle/Makefile``:
 
@@ -37,10 +37,10 @@ _I = ctypes.c_int
 _P = ctypes.c_void_p
 
 
-# Root of the reference sources (megure-labs/orihime) that the checkers are
+# Root of the reference sources (megure-labs/orihime) that the oracle libraries are
 # compiled from: the environment variable ORIHIME_REFERENCE, default
-# /root/reference.  Where it is absent (a GPU box), only prebuilt checkers
-# under _ref/ are used.
+# /root/reference.  On a machine without those sources only the prebuilt
+# libraries under _ref/ are used.
 REFERENCE = os.environ.get("ORIHIME_REFERENCE", "/root/reference")
 
 

@@ -5,7 +5,7 @@
  * Hessian-vector product and parameter Jacobians.
  *
  * The product (orihime_b200) never loads this library: only tests/, the CPU
- * legs of bench.py and __graft_entry__.smoke() do, as the checker.
+ * legs of bench.py and __graft_entry__.smoke() do, as the oracle.
  *
  * Symbols ending in _f32 follow the reference CPU kernels
  * (src/sw/kernels_cpu.cpp, src/sw_affine/kernels_cpu.cpp,

@@ -1,7 +1,8 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
-Run where the reference sources are (not on a GPU box): their root is the
-environment variable ORIHIME_REFERENCE (default /root/reference).  It copies the reference's Python package to a scratch
+Run on a machine that holds the reference sources: their root is the
+environment variable ORIHIME_REFERENCE (default /root/reference).  It
+copies the reference's Python package to a scratch
 directory under /tmp, compiles the reference's CPU extension there with g++
 (the source list of meson.build's ``cpp_sources``), imports it, and records
 the public soft Smith-Waterman API's outputs on small seeded inputs:
