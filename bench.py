@@ -346,7 +346,7 @@ def second_order(args):
     del e, f
     out = torch.empty_like(s)
     gt = torch.zeros(B, 4, device="cuda")
-    nbytes = int(lib.swb_sw_affine_aux_workspace_bytes(B, N, N))
+    nbytes = int(lib.swb_sw_affine_aux_workspace_bytes_for(B, N, N, GO, GE, T))
     ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
     P = lambda t: t.data_ptr()  # noqa: E731

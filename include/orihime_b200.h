@@ -318,14 +318,24 @@ int swb_nw_ragged_value(const float* scores, const void* host_plan, const void* 
 
 /*
  * Second-order ops (band wavefronts: a forward kernel carrying alpha and its
- * tangent, then a backward kernel carrying beta and its tangent).  The
- * workspace holds, for every cell the wavefront visits, the fields the
- * backward reads: 24 floats affine (weights, weight tangents, alpha hi/lo,
- * tangents), 12 linear, plus per-band edge, push and partial buffers; about
- * 100 (affine) or 50 (linear) bytes per cell of the padded batch.  Callers
- * that bound memory split the batch into pair groups.
+ * tangent, then a backward kernel carrying beta and its tangent).  Two kernel
+ * pairs serve them, chosen per call from the parameters:
+ *   - every gap <= 0 and 0 < T < inf: the scaled linear-domain dual-number
+ *     kernels, whose workspace holds per-chunk checkpoints of values and
+ *     tangents plus per-band edge, push and partial buffers (about 7 B per
+ *     cell of the padded batch at 4 columns per lane);
+ *   - otherwise the log-domain kernels, whose workspace holds, for every cell
+ *     the wavefront visits, the fields the backward reads: 24 floats affine
+ *     (weights, weight tangents, alpha hi/lo, tangents), 12 linear; about 100
+ *     (affine) or 50 (linear) bytes per cell.
+ * swb_sw_affine_aux_workspace_bytes is enough for any parameters (the larger
+ * of the two); swb_sw_affine_aux_workspace_bytes_for is enough for the given
+ * ones (what the call with them launches).  Callers that bound memory split
+ * the batch into pair groups.
  */
 size_t swb_sw_affine_aux_workspace_bytes(int B, int L1max, int L2max);
+size_t swb_sw_affine_aux_workspace_bytes_for(int B, int L1max, int L2max, float gap_open,
+                                             float gap_ext, float temp);
 
 /*
  * Hessian-vector product of the marginal map: out = d(map)/d(scores) . v
@@ -351,6 +361,7 @@ int swb_sw_affine_param_jacobian(const float* scores, const int* lengths, int B,
                                  float* out, void* workspace, size_t workspace_bytes, void* stream);
 
 size_t swb_sw_aux_workspace_bytes(int B, int L1max, int L2max);
+size_t swb_sw_aux_workspace_bytes_for(int B, int L1max, int L2max, float gap, float temp);
 
 /* Linear-gap HVP (src/sw/torch_cuda.cpp marginals_hvp body); grad_tangents
  * [B][4] = tangents of (dS/dgap, dS/dT, 0, S). */

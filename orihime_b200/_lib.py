@@ -93,6 +93,10 @@ def load() -> ctypes.CDLL:
     lib.swb_sw_affine_aux_workspace_bytes.argtypes = [i, i, i]
     lib.swb_sw_aux_workspace_bytes.restype = sz
     lib.swb_sw_aux_workspace_bytes.argtypes = [i, i, i]
+    lib.swb_sw_affine_aux_workspace_bytes_for.restype = sz
+    lib.swb_sw_affine_aux_workspace_bytes_for.argtypes = [i, i, i, f, f, f]
+    lib.swb_sw_aux_workspace_bytes_for.restype = sz
+    lib.swb_sw_aux_workspace_bytes_for.argtypes = [i, i, i, f, f]
     lib.swb_sw_affine_value_workspace_bytes.restype = sz
     lib.swb_sw_affine_value_workspace_bytes.argtypes = [i, i, i]
     lib.swb_sw_value_workspace_bytes.restype = sz

@@ -536,12 +536,23 @@ _AUX = {  # family -> (workspace bytes, HVP, parameter Jacobian) entry points
 }
 
 
-def _aux_plan(fam, B, L1, L2, dev):
-    """(pairs per group, workspace bytes) for a second-order call: the field
-    table of the band wavefront is about 100 (affine) / 50 (linear) bytes per
-    cell, so large batches are split to stay within min(AUX_BUDGET_MAX,
-    max(2 GiB, half the free device memory))."""
-    fn = getattr(_LIB, _AUX[fam][0])
+# Local families: the workspace the call with given parameters launches (the
+# linear-domain tangent kernels' checkpoints, about 7 B per cell, when every
+# gap is <= 0), instead of the larger log-domain field table.
+_AUX_FOR = {"sw": "swb_sw_aux_workspace_bytes_for", "sw_affine": "swb_sw_affine_aux_workspace_bytes_for"}
+
+
+def _aux_plan(fam, B, L1, L2, dev, params):
+    """(pairs per group, workspace bytes) for a second-order call with these
+    parameters.  The log-domain kernels' field table is about 100 (affine) /
+    50 (linear) bytes per cell, so large batches are split to stay within
+    min(AUX_BUDGET_MAX, max(2 GiB, half the free device memory))."""
+    if fam in _AUX_FOR:
+        f = getattr(_LIB, _AUX_FOR[fam])
+        vals = [float(p) for p in params]
+        fn = lambda b, l1, l2: f(b, l1, l2, *vals)  # noqa: E731
+    else:
+        fn = getattr(_LIB, _AUX[fam][0])
     nbytes = int(fn(B, L1, L2))
     # the free-memory query is a host call; under stream capture use the floor
     free = 0 if _capturing() else torch.cuda.mem_get_info(dev)[0]
@@ -568,7 +579,7 @@ def run_hvp(fam, scores, v, lengths, params, want_grads=False):
     gt = torch.zeros(B, 4, dtype=torch.float32, device=dev) if want_grads else None
     if B == 0:
         return out, gt
-    g, nbytes = _aux_plan(fam, B, L1, L2, dev)
+    g, nbytes = _aux_plan(fam, B, L1, L2, dev, params)
     ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     fn = getattr(_LIB, _AUX[fam][1])
     with torch.cuda.device(dev):
@@ -587,7 +598,7 @@ def run_param_jacobian(fam, scores, lengths, params, which):
     out = torch.empty_like(scores)
     if B == 0:
         return out
-    g, nbytes = _aux_plan(fam, B, L1, L2, dev)
+    g, nbytes = _aux_plan(fam, B, L1, L2, dev, params)
     ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     fn = getattr(_LIB, _AUX[fam][2])
     with torch.cuda.device(dev):

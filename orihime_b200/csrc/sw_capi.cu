@@ -910,6 +910,22 @@ size_t swb_sw_aux_workspace_bytes(int B, int L1max, int L2max) {
   return B > 0 ? std::max(xlayout<1>(B, L1max, L2max).total, tlayout<1>(B, L1max, L2max).total) : 0;
 }
 
+// What the second-order call with these parameters launches: the tangent
+// kernels' layout when tan_eligible holds (launch_xband's own test), else the
+// log-domain kernels'.
+size_t swb_sw_affine_aux_workspace_bytes_for(int B, int L1max, int L2max, float gap_open,
+                                             float gap_ext, float temp) {
+  if (B <= 0) return 0;
+  return tan_eligible(gap_open, gap_ext, temp) ? tlayout<3>(B, L1max, L2max).total
+                                               : xlayout<3>(B, L1max, L2max).total;
+}
+
+size_t swb_sw_aux_workspace_bytes_for(int B, int L1max, int L2max, float gap, float temp) {
+  if (B <= 0) return 0;
+  return tan_eligible(gap, 0.f, temp) ? tlayout<1>(B, L1max, L2max).total
+                                      : xlayout<1>(B, L1max, L2max).total;
+}
+
 int swb_sw_affine_hvp(const float* scores, const float* v, const int* lengths, int B, int L1max,
                       int L2max, float gap_open, float gap_ext, float temp, float* out,
                       float* grad_tangents, void* workspace, size_t workspace_bytes, void* stream) {

@@ -104,3 +104,24 @@ def test_other_families_argument_errors_and_workspaces(lib, fam):
     assert call(-1, 1.0, None, 0) == -1
     assert call(0, 1.0, None, 0) == 0
     assert call(1, 1.0, p, 16) == -2
+
+
+@pytest.mark.parametrize("fam", ["sw_affine", "sw"])
+def test_aux_workspace_for_parameters(lib, fam):
+    """Second-order workspace sizes (host arithmetic only): with every gap <= 0
+    and 0 < T < inf the linear-domain tangent kernels run, and their
+    checkpoints need a small fraction of the log-domain field table that the
+    any-parameters size covers; other parameters get that table's size."""
+    f = ctypes.c_float
+    any_ = getattr(lib, f"swb_{fam}_aux_workspace_bytes")
+    for_ = getattr(lib, f"swb_{fam}_aux_workspace_bytes_for")
+    gaps = (f(-2.0), f(-0.5)) if fam == "sw_affine" else (f(-1.0),)
+    pos = (f(-2.0), f(0.25)) if fam == "sw_affine" else (f(0.25),)
+    B, L1, L2 = 256, 512, 512
+    n_any = int(any_(B, L1, L2))
+    n_lin = int(for_(B, L1, L2, *gaps, f(0.5)))
+    assert 0 < n_lin * 8 < n_any
+    assert int(for_(B, L1, L2, *pos, f(0.5))) == n_any          # a positive gap: log domain
+    assert int(for_(B, L1, L2, *gaps, f(0.0))) == n_any         # T <= 0: no tangent kernels
+    assert int(for_(0, L1, L2, *gaps, f(0.5))) == 0
+    assert int(for_(2 * B, L1, L2, *gaps, f(0.5))) > n_lin

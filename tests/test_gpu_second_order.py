@@ -215,7 +215,7 @@ def test_pair_groups_match_single_call(monkeypatch):
     want, want_gt = _ops.run_hvp("sw_affine", s, v, ln, (*AFF, 0.6), want_grads=True)
     want_p = _ops.run_param_jacobian("sw", s, ln, (*LIN, 0.6), 1)
     monkeypatch.setattr(_ops, "AUX_BUDGET_MAX", 1)
-    assert _ops._aux_plan("sw_affine", 5, 40, 70, s.device)[0] == 1
+    assert _ops._aux_plan("sw_affine", 5, 40, 70, s.device, (*AFF, 0.6))[0] == 1
     got, got_gt = _ops.run_hvp("sw_affine", s, v, ln, (*AFF, 0.6), want_grads=True)
     got_p = _ops.run_param_jacobian("sw", s, ln, (*LIN, 0.6), 1)
     assert torch.equal(got, want) and torch.equal(got_gt, want_gt) and torch.equal(got_p, want_p)
@@ -250,3 +250,44 @@ def test_long_pair_quiet_chunks(fam):
         _check("dP/dT", pt.cpu().numpy(), O.linear_param_grad(sn, None, *LIN, T, 1),
                O.linear_param_grad(sn, None, *LIN, T, 1, dtype=np.float64))
     assert torch.equal(got, again)
+
+
+@pytest.mark.parametrize("fam", ["affine", "linear"])
+def test_workspace_for_parameters(fam):
+    """The parameter-aware workspace size is exactly what the call launches:
+    an HVP and a parameter Jacobian with that many bytes give the outputs of
+    a call with the any-parameters size bit for bit, and one byte less is
+    refused before anything runs (SWB_ERR_WORKSPACE, output untouched)."""
+    import ctypes
+
+    from orihime_b200 import _lib
+
+    lib = _lib.load()
+    s = _scores(3, 40, 70, 31).cuda()
+    v = _scores(3, 40, 70, 32, scale=1.0).cuda()
+    B, L1, L2 = s.shape
+    f = ctypes.c_float
+    if fam == "affine":
+        ps, pfx = (f(AFF[0]), f(AFF[1]), f(0.6)), "swb_sw_affine"
+    else:
+        ps, pfx = (f(LIN[0]), f(0.6)), "swb_sw"
+    n_for = int(getattr(lib, f"{pfx}_aux_workspace_bytes_for")(B, L1, L2, *ps))
+    n_any = int(getattr(lib, f"{pfx}_aux_workspace_bytes")(B, L1, L2))
+    assert 0 < n_for < n_any
+    st = torch.cuda.current_stream().cuda_stream
+    hvp, jac = getattr(lib, f"{pfx}_hvp"), getattr(lib, f"{pfx}_param_jacobian")
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    outs = {}
+    for n in (n_any, n_for):
+        ws = torch.empty(n, dtype=torch.uint8, device="cuda")
+        o1, o2 = torch.empty_like(s), torch.empty_like(s)
+        assert hvp(P(s), P(v), None, B, L1, L2, *ps, P(o1), None, P(ws), ctypes.c_size_t(n), ctypes.c_void_p(st)) == 0
+        assert jac(P(s), None, B, L1, L2, *ps, 0, P(o2), P(ws), ctypes.c_size_t(n), ctypes.c_void_p(st)) == 0
+        torch.cuda.synchronize()
+        outs[n] = (o1, o2)
+    assert torch.equal(outs[n_for][0], outs[n_any][0]) and torch.equal(outs[n_for][1], outs[n_any][1])
+    ws = torch.empty(n_for, dtype=torch.uint8, device="cuda")
+    o = torch.full_like(s, 7.0)
+    rc = hvp(P(s), P(v), None, B, L1, L2, *ps, P(o), None, P(ws), ctypes.c_size_t(n_for - 1), ctypes.c_void_p(st))
+    torch.cuda.synchronize()
+    assert rc == -2 and bool((o == 7.0).all())
