@@ -521,7 +521,10 @@ def _check_like(scores, other, name, msg_shape):
 
 # Largest workspace one second-order call takes at once; a batch needing more
 # is processed in pair groups (results identical: pairs are independent).
-AUX_BUDGET_MAX = 16 << 30
+# Fewer, larger groups are faster: the log-domain HVP at 4096 pairs of
+# 512 x 512 takes 31 ms in groups of 3060 pairs (64 GiB) and 34 ms in groups
+# of 765 (16 GiB).  Half the free device memory still bounds it.
+AUX_BUDGET_MAX = 64 << 30
 
 
 _AUX = {  # family -> (workspace bytes, HVP, parameter Jacobian) entry points
