@@ -125,3 +125,38 @@ def test_aux_workspace_for_parameters(lib, fam):
     assert int(for_(B, L1, L2, *gaps, f(0.0))) == n_any         # T <= 0: no tangent kernels
     assert int(for_(0, L1, L2, *gaps, f(0.5))) == 0
     assert int(for_(2 * B, L1, L2, *gaps, f(0.5))) > n_lin
+
+
+@pytest.mark.parametrize("fam,params", [("sw_affine", (-2.0, -0.5, 0.5)), ("sw", (-1.0, 0.5)),
+                                        ("sw_affine", (-2.0, 0.25, 0.5)), ("nw_affine", (-2.0, -0.5, 0.5)),
+                                        ("sv_affine", (-2.0, -0.5, 0.5))])
+def test_second_order_pair_groups(monkeypatch, fam, params):
+    """The op layer's pair-group plan for second-order calls (host logic):
+    under stream capture there is no free-memory query and the budget is the
+    2 GiB floor.  Groups then fit the budget, cover the batch, and the
+    workspace fits every group; the local models with every gap <= 0 are
+    sized for their tangent kernels (far fewer groups), the others for the
+    log-domain field table."""
+    from orihime_b200 import _ops
+
+    monkeypatch.setattr(_ops, "_capturing", lambda: True)
+    B, L = 4096, 512
+    g, nbytes = _ops._aux_plan(fam, B, L, L, None, params)
+    if fam in _ops._AUX_FOR:
+        size = lambda b: int(getattr(_ops._LIB, _ops._AUX_FOR[fam])(b, L, L, *map(float, params)))  # noqa: E731
+    else:
+        size = lambda b: int(getattr(_ops._LIB, _ops._AUX[fam][0])(b, L, L))  # noqa: E731
+    budget = 2 << 30
+    assert 1 <= g <= B and nbytes <= budget
+    groups = list(_ops._groups(B, g))
+    assert groups[0][0] == 0 and groups[-1][1] == B
+    assert all(b1 > b0 and b1 - b0 <= g for b0, b1 in groups)
+    assert all(groups[k][1] == groups[k + 1][0] for k in range(len(groups) - 1))
+    assert all(size(b1 - b0) <= nbytes for b0, b1 in groups)
+    if fam in ("sw_affine", "sw") and all(p <= 0 for p in params[:-1]):
+        assert len(groups) <= 5            # about 7 B per cell: 8.4 GB affine
+    else:
+        assert len(groups) >= 40           # about 100 B per cell: 92 GB affine
+    # a batch within the budget is one group
+    g1, n1 = _ops._aux_plan(fam, 8, L, L, None, params)
+    assert g1 == 8 and n1 == size(8)
